@@ -1,0 +1,391 @@
+"""Benchmark of the H-matrix MVM (y += alpha A x) on B200.
+
+Default workload (one step = one product on one GPU): FP64 H-matrix of the 3D
+exponential covariance exp(-r/0.1) + 1e-4 nugget on n = 131072 points
+uniform in [0,1]^3 (seed 1), BSP cluster tree leaf 64, eta = 2, ACA + SVD
+eps = 1e-6, one right-hand side x ~ N(0,1).  Synthetic inputs, built on the
+host by the library's own construction.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2|c1|c3|c2s|c4] [--no-cpu-baseline]
+
+Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
+independent replica of the product on its own GPU (the MVM has no exchange
+step on one matrix; weak scaling), time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "H-MVM/s & HBM GB/s vs roofline; FP64 vs mixed-precision at rel.err ≤1e-6"
+
+CONFIGS = {
+    # name: (description, problem kwargs, uniform, precision, nrhs)
+    "c1": ("FP64 H-MVM, 1D log kernel n=8192, leaf 64, eta 2, eps 1e-6, nrhs 1",
+           dict(kind=0, n=8192), False, "f64", 1),
+    "c2": ("FP64 H-MVM, 3D exp(-r/0.1)+1e-4 nugget, n=131072 U[0,1]^3, BSP leaf 64, eta 2, eps 1e-6, nrhs 1",
+           dict(kind=1, n=131072, ell=0.1, nugget=1e-4), False, "f64", 1),
+    "c2s": ("FP64 H-MVM, 3D exp(-r/0.1)+1e-4 nugget, n=32768 (profiling size), leaf 64, eta 2, eps 1e-6, nrhs 1",
+            dict(kind=1, n=32768, ell=0.1, nugget=1e-4), False, "f64", 1),
+    "c3": ("FP64 uniform-H MVM, 1/(4 pi r)*area on octahedron sphere refined 6x (32768 triangles), leaf 64, "
+           "eta 2, eps 1e-6, nrhs 1", dict(kind=2, refine=6, uniform=True), True, "f64", 1),
+    "c4": ("FP64 H-MVM, 3D exp(-r/0.1)+1e-4 nugget, n=262144, leaf 64, eta 2, eps 1e-6, nrhs 1",
+           dict(kind=1, n=262144, ell=0.1, nugget=1e-4), False, "f64", 1),
+}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", self.gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_uuid(dev: int) -> str:
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(dev)
+
+
+def make_problem(cfg, nthreads):
+    import hlr_b200 as hlr
+    desc, kw, uniform, prec, nrhs = CONFIGS[cfg]
+    kw = dict(kw)
+    kw.setdefault("leaf_size", 64)
+    kw.setdefault("eta", 2.0)
+    kw.setdefault("eps", 1e-6)
+    kw["nthreads"] = nthreads
+    return hlr.Problem(**kw), desc, uniform, prec, nrhs
+
+
+def cpu_mvm(hm, uniform, desc_obj, x, y, nthreads):
+    import oracle
+    if uniform:
+        st = oracle.uniform_mvm(desc_obj, 1.0, 0, x, y, nthreads)
+        assert st == 0
+    else:
+        oracle.hmvm_chunk(desc_obj, 1.0, 0, x, y, nthreads)
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of HLR's TBB MVM (oracle port) on the host cores."""
+    if rank != 0:
+        return
+    import hlr_b200 as hlr
+    import oracle
+    nthreads = os.cpu_count() or 1
+    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads)
+    hm = hlr.build(prob)
+    d = hm.uniform_desc() if uniform else hm.h_desc()
+    x = np.random.default_rng(2).standard_normal(hm.n)
+    y = np.zeros(hm.n)
+    t0 = time.perf_counter()
+    cpu_mvm(hm, uniform, d, x, y, nthreads)
+    t_full = time.perf_counter() - t0
+    # bound the run: a step is a sample of the leaves when K full products would exceed ~120 s
+    frac = 1.0
+    dd = d
+    if not uniform and args.steps * t_full > 120.0:
+        stride = int(np.ceil(args.steps * t_full / 120.0))
+        sub = [d.blocks[i] for i in range(0, d.nblocks, stride)]
+        import ctypes as C
+        from hlr_b200 import _capi
+        arr = (_capi.hlrc_block * len(sub))(*sub)
+        dd = _capi.hlrc_h_desc()
+        dd.nrows, dd.ncols, dd.nblocks = d.nrows, d.ncols, len(sub)
+        dd.blocks = C.cast(arr, C.POINTER(_capi.hlrc_block))
+        dd._keep = (arr, d)
+        sub_bytes = sum(8 * (b.nrows * b.ncols if b.kind == 0 else b.rank * (b.nrows + b.ncols)) for b in sub)
+        all_bytes = sum(8 * (d.blocks[i].nrows * d.blocks[i].ncols if d.blocks[i].kind == 0 else
+                             d.blocks[i].rank * (d.blocks[i].nrows + d.blocks[i].ncols)) for i in range(d.nblocks))
+        frac = sub_bytes / all_bytes
+    for _ in range(args.warmup):
+        cpu_mvm(hm, uniform, dd, x, y, nthreads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_mvm(hm, uniform, dd, x, y, nthreads)
+    el = time.perf_counter() - t0
+    value = frac * args.steps / el
+    sample = ("full product per step" if frac == 1.0 else
+              f"every {int(round(1 / frac))}-th leaf per step ({frac * 100:.1f}% of matrix bytes), scaled")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "n": hm.n},
+        "cpu_baseline": {"value": value, "unit": "MVM/s", "cores": nthreads, "kind": "port",
+                         "sample": sample + "; oracle/oracle.c oracle_hmvm_chunk (restated hlr::tbb::mul_vec, "
+                                            "64-row chunk locks, OpenMP)"},
+        "e2e": {"value": value, "unit": "MVM/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import hlr_b200 as hlr
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ncpu = os.cpu_count() or 1
+    nthreads = max(1, ncpu // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", world))))
+    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads)
+    tb = time.perf_counter()
+    hm = hlr.build(prob)
+    t_build = time.perf_counter() - tb
+    tu = time.perf_counter()
+    M = hlr.upload(hm, precision=prec, uniform=uniform)
+    t_upload = time.perf_counter() - tu
+    info = M.info
+    n = hm.n
+    xh = np.random.default_rng(2).standard_normal(n)
+    x = torch.from_numpy(xh).to(dev)
+    y = torch.zeros(n, dtype=torch.float64, device=dev)
+    alpha = 2.0
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        hlr.mul_vec(alpha, hlr.apply_normal, M, x, y)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    M.set_profiling(True)
+    M.last_profile()  # clear
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_uuid(local_rank)) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    prof = M.last_profile()
+    M.set_profiling(False)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+
+    # correctness of the timed path: one product from zero, against the oracle
+    yc = torch.zeros(n, dtype=torch.float64, device=dev)
+    hlr.mul_vec(1.0, hlr.apply_normal, M, x, yc)
+    torch.cuda.synchronize()
+    ygpu = yc.cpu().numpy()
+
+    # end to end through the C ABI with pinned host buffers (copies inside)
+    xp = torch.from_numpy(xh.copy()).pin_memory()
+    yp = torch.zeros(n, dtype=torch.float64).pin_memory()
+    xpn, ypn = xp.numpy(), yp.numpy()
+    for _ in range(max(1, args.warmup // 2)):
+        hlr.mul_vec(alpha, hlr.apply_normal, M, xpn, ypn)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ksteps = args.steps
+    h0.record()
+    for _ in range(ksteps):
+        hlr.mul_vec(alpha, hlr.apply_normal, M, xpn, ypn)
+    h1.record()
+    torch.cuda.synchronize()
+    e2e_ms = h0.elapsed_time(h1)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_ms = float(te.item())
+    if rank != 0:
+        return
+
+    hbm_peak, peak_kind = peaks()
+    value = world * args.steps / (ms_max / 1e3)
+    alg = info["algorithmic_bytes"]
+    gbs = alg / (ms_max / 1e3 / args.steps) / 1e9
+    # dominant kernel = pass with the largest device time
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if dom:
+        name, (cnt, tot_ms, by) = dom
+        avg_ms = tot_ms / max(1, cnt)
+        achieved = by / (avg_ms / 1e3) / 1e9
+        traffic = traffic_from_profiles(name, args.config)
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                "bytes_per_launch": by, "avg_ms": avg_ms,
+                "share_of_step": tot_ms / sum(v[1] for v in prof.values())}
+    line = {
+        "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == "f64" else prec, "data": "synthetic",
+        "config": {"workload": desc, "n": n, "nrhs": nrhs, "precision": prec, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 ({info['matrix_bytes'] / 1e9:.2f} GB matrix streamed per step)",
+                   "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": alg, "flops": info["flops"],
+                   "leaves": info["n_dense"] + info["n_lowrank"], "max_rank": info["max_rank"],
+                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2)},
+        "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
+        "roofline": roof,
+        "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
+                   for k, v in prof.items()},
+        "gpu_launches": info["launches"][0] * args.steps,
+        "e2e": {"value": world * ksteps / (e2e_ms / 1e3), "unit": "MVM/s",
+                "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
+        "clocks": clocks.summary(),
+    }
+    # CPU baseline (oracle port on the host cores, bounded sample) and error
+    if not args.no_cpu_baseline and world == 1:
+        d = hm.uniform_desc() if uniform else hm.h_desc()
+        ncores = os.cpu_count() or 1
+        yo = np.zeros(n)
+        t0 = time.perf_counter()
+        cpu_mvm(hm, uniform, d, xh, yo, ncores)
+        t1 = time.perf_counter() - t0
+        line["rel_err_vs_oracle"] = float(np.linalg.norm(ygpu - yo) / np.linalg.norm(yo))
+        reps, el = 0, 0.0
+        budget = 15.0
+        while el < budget and reps < 50:
+            yy = np.zeros(n)
+            t0 = time.perf_counter()
+            cpu_mvm(hm, uniform, d, xh, yy, ncores)
+            el += time.perf_counter() - t0
+            reps += 1
+        line["cpu_baseline"] = {"value": reps / el, "unit": "MVM/s", "cores": ncores, "kind": "port",
+                                "sample": f"{reps} full products of the same matrix and x after 1 warm-up "
+                                          f"({el:.1f} s); oracle/oracle.c restatement of hlr::tbb::mul_vec"}
+    print(json.dumps(line), flush=True)
+
+
+def traffic_from_profiles(kernel: str, config: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.md"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        parts = [s.strip() for s in ln.strip().strip("|").split("|")]
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == config:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,330 @@
+"""hlr_b200 — B200-native H-matrix / uniform-H matrix-vector product.
+
+Host-side mirror of HLR's MVM interface:
+
+    hlr::tbb::mul_vec(alpha, op_M, M, x, y)            -> hlr_b200.mul_vec(alpha, op, M, x, y)
+    hlr::tbb::uniform::mul_vec(alpha, op_M, M, x, y,
+                               rowcb, colcb)           -> hlr_b200.uniform.mul_vec(alpha, op, M, x, y)
+
+``M`` is a :class:`DeviceMatrix` (the flattened, device-resident copy made
+once by :func:`upload`), ``x``/``y`` are float64 CUDA tensors (or numpy arrays
+for the host-buffer path).  ``y`` is accumulated: ``y += alpha * op(M) x``.
+
+Matrices come either from a caller's own leaf list (:class:`LeafList`,
+the shape HLR's block tree flattens to) or from the host construction
+:func:`build` (clustering, admissibility, ACA + SVD, uniform bases in C++).
+Everything runs through ``libhlrc.so``; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+from ._capi import HLRCError, check, lib
+
+# HLIBpro matop_t
+apply_normal = 0
+apply_transposed = 1
+apply_adjoint = 2
+
+# storage precisions (hlrc_precision)
+PREC_F64, PREC_F32, PREC_BF16, PREC_F16, PREC_MIXED = 0, 1, 2, 3, 4
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "bf16": PREC_BF16, "f16": PREC_F16, "mixed": PREC_MIXED}
+
+LEAF_DENSE, LEAF_LOWRANK = 0, 1
+PROBLEM_LOG1D, PROBLEM_EXP3D, PROBLEM_LAPLACE_SPH = 0, 1, 2
+
+
+@dataclass
+class Problem:
+    """A test matrix definition (point set + kernel + H parameters)."""
+    kind: int
+    n: int = 0
+    leaf_size: int = 64
+    eta: float = 2.0
+    eps: float = 1e-6
+    seed: int = 1
+    ell: float = 0.1
+    nugget: float = 0.0
+    refine: int = 6
+    uniform: bool = False
+    nthreads: int = 0
+
+    @staticmethod
+    def log1d(n: int, **kw) -> "Problem":
+        """A_ij = log|x_i - x_j|, A_ii = h(log h - 1), x_i ~ U[0,1]."""
+        return Problem(kind=PROBLEM_LOG1D, n=n, **kw)
+
+    @staticmethod
+    def exp3d(n: int, ell: float = 0.1, nugget: float = 1e-4, **kw) -> "Problem":
+        """Exponential covariance exp(-r/ell) (+ nugget) on U[0,1]^3 points."""
+        return Problem(kind=PROBLEM_EXP3D, n=n, ell=ell, nugget=nugget, **kw)
+
+    @staticmethod
+    def laplace_sphere(refine: int = 6, **kw) -> "Problem":
+        """Collocation of 1/(4 pi r) on a refined octahedron sphere mesh."""
+        return Problem(kind=PROBLEM_LAPLACE_SPH, refine=refine, **kw)
+
+    def to_c(self) -> _capi.hlrc_problem:
+        p = _capi.hlrc_problem()
+        p.kind, p.leaf_size, p.n, p.refine = self.kind, self.leaf_size, self.n, self.refine
+        p.uniform, p.seed, p.eta, p.eps = int(self.uniform), self.seed, self.eta, self.eps
+        p.ell, p.nugget, p.nthreads = self.ell, self.nugget, self.nthreads
+        return p
+
+
+class HostMatrix:
+    """Host-built H-matrix (and optionally its uniform-H form) owned by C++."""
+
+    def __init__(self, problem: Problem):
+        self.problem = problem
+        h = C.c_void_p()
+        pc = problem.to_c()
+        check(lib().hlrc_build(C.byref(pc), C.byref(h)), "hlrc_build")
+        self._h = h
+        pts, dim, n = _capi.pdbl(), C.c_int(), C.c_int64()
+        check(lib().hlrc_build_points(h, C.byref(pts), C.byref(dim), C.byref(n)), "hlrc_build_points")
+        self.n = n.value
+        self.dim = dim.value
+        self.points = np.ctypeslib.as_array(pts, shape=(self.n * self.dim,)).reshape(self.n, self.dim).copy()
+        w = _capi.pdbl()
+        check(lib().hlrc_build_weights(h, C.byref(w)), "hlrc_build_weights")
+        self.weights = np.ctypeslib.as_array(w, shape=(self.n,)).copy() if bool(w) else None
+        perm = C.POINTER(C.c_int64)()
+        check(lib().hlrc_build_perm(h, C.byref(perm)), "hlrc_build_perm")
+        self.perm_i2e = np.ctypeslib.as_array(perm, shape=(self.n,)).copy()
+        secs, nl, mr, by = C.c_double(), C.c_int64(), C.c_int32(), C.c_int64()
+        check(lib().hlrc_build_stats(h, C.byref(secs), C.byref(nl), C.byref(mr), C.byref(by)), "hlrc_build_stats")
+        self.build_seconds, self.nleaves, self.max_rank, self.bytes = secs.value, nl.value, mr.value, by.value
+
+    def h_desc(self) -> _capi.hlrc_h_desc:
+        d = _capi.hlrc_h_desc()
+        check(lib().hlrc_build_h_desc(self._h, C.byref(d)), "hlrc_build_h_desc")
+        d._owner = self
+        return d
+
+    def uniform_desc(self) -> _capi.hlrc_uniform_desc:
+        d = _capi.hlrc_uniform_desc()
+        check(lib().hlrc_build_uniform_desc(self._h, C.byref(d)), "hlrc_build_uniform_desc")
+        d._owner = self
+        return d
+
+    def entry(self, i: int, j: int) -> float:
+        return lib().hlrc_build_entry(self._h, i, j)
+
+    def close(self) -> None:
+        if self._h:
+            lib().hlrc_build_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build(problem: Problem) -> HostMatrix:
+    """Host construction: cluster tree, block tree, ACA + SVD (C++, OpenMP)."""
+    return HostMatrix(problem)
+
+
+class LeafList:
+    """An H-matrix given as a flat list of leaves (numpy, column-major).
+
+    ``add_dense(row0, col0, D)`` and ``add_lowrank(row0, col0, U, V)`` (M = U V^T)
+    mirror dense_matrix / lrmatrix; the list keeps the arrays alive.
+    """
+
+    def __init__(self, nrows: int, ncols: int):
+        self.nrows, self.ncols = nrows, ncols
+        self._keep = []
+        self._blocks = []
+
+    def _arr(self, a) -> np.ndarray:
+        a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+        self._keep.append(a)
+        return a
+
+    def add_dense(self, row0: int, col0: int, D) -> None:
+        D = self._arr(D)
+        b = _capi.hlrc_block()
+        b.row0, b.nrows, b.col0, b.ncols = row0, D.shape[0], col0, D.shape[1]
+        b.kind, b.rank = LEAF_DENSE, 0
+        b.D = D.ctypes.data_as(_capi.pdbl)
+        b.ldd = max(1, D.shape[0])
+        self._blocks.append(b)
+
+    def add_lowrank(self, row0: int, col0: int, U, V) -> None:
+        U, V = self._arr(U), self._arr(V)
+        assert U.shape[1] == V.shape[1]
+        b = _capi.hlrc_block()
+        b.row0, b.nrows, b.col0, b.ncols = row0, U.shape[0], col0, V.shape[0]
+        b.kind, b.rank = LEAF_LOWRANK, U.shape[1]
+        b.U = U.ctypes.data_as(_capi.pdbl)
+        b.ldu = max(1, U.shape[0])
+        b.V = V.ctypes.data_as(_capi.pdbl)
+        b.ldv = max(1, V.shape[0])
+        self._blocks.append(b)
+
+    def h_desc(self) -> _capi.hlrc_h_desc:
+        arr = (_capi.hlrc_block * max(1, len(self._blocks)))(*self._blocks)
+        d = _capi.hlrc_h_desc()
+        d.nrows, d.ncols, d.nblocks = self.nrows, self.ncols, len(self._blocks)
+        d.blocks = C.cast(arr, C.POINTER(_capi.hlrc_block))
+        d._owner = (self, arr)
+        return d
+
+
+def _options(precision="f64", max_nrhs: int = 1, mixed_eps: float = 1e-6, device: int = -1):
+    o = _capi.hlrc_options()
+    lib().hlrc_default_options(C.byref(o))
+    o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    o.max_nrhs, o.mixed_eps, o.device = max_nrhs, mixed_eps, device
+    return o
+
+
+class DeviceMatrix:
+    """Device-resident flattened H / uniform-H matrix (an ``hlrc_hmat``)."""
+
+    def __init__(self, handle: C.c_void_p, uniform: bool):
+        self._h = handle
+        self.uniform = uniform
+        inf = _capi.hlrc_info()
+        check(lib().hlrc_get_info(self._h, C.byref(inf)), "hlrc_get_info")
+        self.info = {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
+        self.info["launches"] = list(inf.launches)
+        self.nrows, self.ncols = inf.n_rows, inf.n_cols
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def set_profiling(self, on: bool = True) -> None:
+        check(lib().hlrc_set_profiling(self._h, int(on)), "hlrc_set_profiling")
+
+    def last_profile(self) -> dict:
+        """{pass name: (launches, total ms, algorithmic bytes per launch)} since the last read."""
+        names = (C.c_char_p * 64)()
+        cnt = (C.c_int * 64)()
+        ms = (C.c_double * 64)()
+        by = (C.c_int64 * 64)()
+        k = lib().hlrc_last_profile(self._h, names, cnt, ms, by, 64)
+        return {names[i].decode(): (cnt[i], ms[i], by[i]) for i in range(k)}
+
+    def free(self) -> None:
+        if self._h:
+            lib().hlrc_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
+           mixed_eps: float = 1e-6, device: int = -1) -> DeviceMatrix:
+    """Flatten and upload a matrix: ``src`` is a HostMatrix, LeafList or descriptor."""
+    if uniform is None:
+        uniform = isinstance(src, HostMatrix) and src.problem.uniform
+    o = _options(precision, max_nrhs, mixed_eps, device)
+    h = C.c_void_p()
+    if uniform:
+        d = src.uniform_desc() if hasattr(src, "uniform_desc") else src
+        check(lib().hlrc_upload_uniform(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_uniform")
+    else:
+        d = src.h_desc() if hasattr(src, "h_desc") else src
+        check(lib().hlrc_upload_h(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_h")
+    return DeviceMatrix(h, uniform)
+
+
+def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
+              mixed_eps: float = 1e-6) -> dict:
+    """Dry run of :func:`upload`: validates and flattens on the host only."""
+    if uniform is None:
+        uniform = isinstance(src, HostMatrix) and src.problem.uniform
+    o = _options(precision, max_nrhs, mixed_eps, -1)
+    inf = _capi.hlrc_info()
+    if uniform:
+        d = src.uniform_desc() if hasattr(src, "uniform_desc") else src
+        check(lib().hlrc_plan_info_uniform(C.byref(d), C.byref(o), C.byref(inf)), "hlrc_plan_info_uniform")
+    else:
+        d = src.h_desc() if hasattr(src, "h_desc") else src
+        check(lib().hlrc_plan_info_h(C.byref(d), C.byref(o), C.byref(inf)), "hlrc_plan_info_h")
+    return {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
+
+
+def _vec_args(v, n: int):
+    """(pointer, nrhs, ld, is_device) for a 1-D (n,) or column-major (n, nrhs) float64 array."""
+    if hasattr(v, "data_ptr"):  # torch tensor
+        import torch
+        if v.dtype != torch.float64:
+            raise TypeError("vectors must be float64")
+        if v.dim() == 1:
+            if v.stride(0) != 1 and v.numel() > 1:
+                raise ValueError("vector must be contiguous")
+            return v.data_ptr(), 1, max(1, v.shape[0]), v.is_cuda
+        if v.stride(0) != 1:
+            raise ValueError("multi-RHS arrays must be column-major (n, nrhs) with stride(0) == 1")
+        return v.data_ptr(), v.shape[1], v.stride(1), v.is_cuda
+    a = v
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64:
+        raise TypeError("vectors must be float64 numpy arrays or torch tensors")
+    if a.ndim == 1:
+        if not a.flags.c_contiguous:
+            raise ValueError("vector must be contiguous")
+        return a.ctypes.data, 1, max(1, a.shape[0]), False
+    if not a.flags.f_contiguous:
+        raise ValueError("multi-RHS arrays must be Fortran-ordered (n, nrhs)")
+    return a.ctypes.data, a.shape[1], a.shape[0], False
+
+
+def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
+    """y += alpha * op(M) x  (drop-in for hlr::tbb::mul_vec / hlr::seq::mul_vec).
+
+    Device tensors run on ``stream`` (default: torch's current stream) without
+    synchronising; numpy arrays take the host-buffer path (copies included).
+    """
+    xp, xn, ldx, xdev = _vec_args(x, 0)
+    yp, yn, ldy, ydev = _vec_args(y, 0)
+    if xn != yn:
+        raise ValueError("x and y have different numbers of right-hand sides")
+    if xdev != ydev:
+        raise ValueError("x and y must both be device or both be host arrays")
+    nx = M.ncols if op == apply_normal else M.nrows
+    ny = M.nrows if op == apply_normal else M.ncols
+    if (x.shape[0] != nx) or (y.shape[0] != ny):
+        raise ValueError(f"shape mismatch: op(M) is {ny}x{nx}, x has {x.shape[0]}, y has {y.shape[0]} rows")
+    if xdev:
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+        check(lib().hlrc_mvm(M.handle, float(alpha), int(op), C.c_void_p(xp), C.c_void_p(yp), xn, ldx, ldy,
+                             C.c_void_p(stream)), "hlrc_mvm")
+    else:
+        check(lib().hlrc_mvm_host(M.handle, float(alpha), int(op), C.c_void_p(xp), C.c_void_p(yp), xn, ldx, ldy),
+              "hlrc_mvm_host")
+
+
+mvm = mul_vec
+
+
+class uniform:  # namespace mirroring hlr::tbb::uniform
+    @staticmethod
+    def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
+        """y += alpha * op(M) x for a uniform-H matrix (op N or adjoint)."""
+        if not M.uniform:
+            raise ValueError("uniform.mul_vec needs a uniform-H DeviceMatrix")
+        mul_vec(alpha, op, M, x, y, stream)
+
+
+__all__ = [
+    "apply_normal", "apply_transposed", "apply_adjoint", "Problem", "HostMatrix", "LeafList", "DeviceMatrix",
+    "build", "upload", "mul_vec", "mvm", "uniform", "HLRCError", "PRECISIONS",
+]

@@ -1,0 +1,474 @@
+// Device handle, upload and the product entry points of the hlrc C ABI.
+//
+// hlrc_mvm replaces hlr::tbb::mul_vec (include/hlr/tbb/arith.hh:312-340) and
+// hlr::tbb::uniform::mul_vec (include/hlr/tbb/arith_uniform.hh:36-96).  The
+// CPU versions recurse over the block tree, apply each leaf into a temporary
+// and add it under 64-row chunk locks (tbb/detail/arith.hh:95-175); here the
+// product is a fixed sequence of 2-4 batched passes over a flattened layout,
+// and every output tile is written by exactly one CTA, so the result is
+// deterministic and needs no atomics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.hpp"
+#include "hlrc.h"
+#include "kernels_f64.cuh"
+#include "plan.hpp"
+
+namespace hlrc {
+
+struct DevTPass {
+    const TUnit* units = nullptr;
+    const TSlab* slabs = nullptr;
+    const TGroup* groups = nullptr;
+    int cls_begin[4] = {0, 0, 0, 0};
+    int ngroups = 0;
+    int in = V_X, out = V_T, mode = OUT_SET;
+    int64_t bytes = 0, alg_bytes = 0;
+    int launches() const {
+        int n = ngroups > 0 ? 1 : 0;
+        for (int c = 0; c < 3; ++c) n += cls_begin[c + 1] > cls_begin[c] ? 1 : 0;
+        return n;
+    }
+};
+
+struct DevNPass {
+    const NSeg* segs = nullptr;
+    const NChunk* chunks = nullptr;
+    int nsegs = 0;
+    int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
+    int64_t bytes = 0, alg_bytes = 0;
+    int launches() const { return nsegs > 0 ? 1 : 0; }
+};
+
+struct ProfileRec {
+    const char* name;
+    cudaEvent_t e0, e1;
+    int64_t alg_bytes;
+};
+
+}  // namespace hlrc
+
+using namespace hlrc;
+
+struct hlrc_hmat_s {
+    int device = 0;
+    int kind = 0;
+    int precision = HLRC_PREC_F64;
+    int64_t nrows = 0, ncols = 0;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    const double* store = nullptr;
+    double* ws_t = nullptr;
+    double* ws_t2 = nullptr;
+    double* part = nullptr;
+    int64_t n_t = 0, n_t2 = 0;
+    std::vector<DevTPass> t;
+    std::vector<DevNPass> n;
+    std::vector<Stage> stages[3];
+    hlrc_info info{};
+    // host-pointer entry point staging
+    double* hx = nullptr;
+    double* hy = nullptr;
+    size_t hx_elems = 0, hy_elems = 0;
+    // profiling
+    bool profiling = false;
+    std::vector<ProfileRec> prof;
+    int nprof = 0;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
+        if (dev >= 0 && dev != prev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+#define HLRC_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(HLRC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+const char* stage_name(int kind, int nk, int idx) {
+    // names used in profiles: kind 0 = H, 1 = uniform
+    static const char* hn[] = {"tform_VtX", "tform_UtX", "tform_DtX"};
+    static const char* hnn[] = {"nform_Ut_Dx", "nform_Vt"};
+    static const char* un[] = {"tform_fwd_col", "tform_fwd_row", "tform_coupT", "tform_DtX"};
+    static const char* unn[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col"};
+    if (kind == 0) return nk == 0 ? hn[idx] : hnn[idx];
+    return nk == 0 ? un[idx] : unn[idx];
+}
+
+// Offsets of every array inside the single device arena of a handle.
+struct ArenaLayout {
+    size_t store = 0;
+    std::vector<size_t> tu, ts, tg, ns, nc;
+    size_t t = 0, t2 = 0, part = 0, total = 0;
+};
+
+ArenaLayout arena_layout(const Plan& p) {
+    ArenaLayout L;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o_ = off; off = align_up(off + bytes, 256); return o_; };
+    L.store = take(p.store.size() * sizeof(double));
+    uint32_t max_slots = 0;
+    for (const TPass& tp : p.tpasses) {
+        L.tu.push_back(take(tp.units.size() * sizeof(TUnit)));
+        L.ts.push_back(take(tp.slabs.size() * sizeof(TSlab)));
+        L.tg.push_back(take(tp.groups.size() * sizeof(TGroup)));
+        max_slots = std::max(max_slots, tp.nslots);
+    }
+    for (const NPass& np : p.npasses) {
+        L.ns.push_back(take(np.segs.size() * sizeof(NSeg)));
+        L.nc.push_back(take(np.chunks.size() * sizeof(NChunk)));
+    }
+    L.t = take(size_t(std::max<int64_t>(1, p.n_t)) * sizeof(double));
+    L.t2 = take(size_t(std::max<int64_t>(1, p.n_t2)) * sizeof(double));
+    L.part = take(size_t(std::max<uint32_t>(1, max_slots)) * 32 * sizeof(double));
+    L.total = off;
+    return L;
+}
+
+void fill_info(const Plan& p, const ArenaLayout& L, hlrc_info& in) {
+    std::memset(&in, 0, sizeof(in));
+    in.n_rows = p.nrows; in.n_cols = p.ncols;
+    in.n_dense = p.n_dense; in.n_lowrank = p.n_lowrank;
+    in.n_row_tiles = p.n_row_tiles; in.n_col_tiles = p.n_col_tiles;
+    in.matrix_bytes = p.matrix_bytes;
+    in.algorithmic_bytes = p.algorithmic_bytes;
+    in.flops = p.flops;
+    in.workspace_bytes = int64_t(L.total - L.t);
+    in.device_bytes = int64_t(L.total);
+    in.precision = p.precision;
+    in.kind = p.kind;
+    in.max_rank = p.max_rank;
+}
+
+hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
+    auto h = std::make_unique<hlrc_hmat_s>();
+    int dev = o.device;
+    if (dev < 0) HLRC_CUDA(cudaGetDevice(&dev));
+    DeviceGuard g(dev);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", dev);
+    h->device = dev;
+    h->kind = p.kind;
+    h->precision = p.precision;
+    h->nrows = p.nrows;
+    h->ncols = p.ncols;
+    h->n_t = p.n_t;
+    h->n_t2 = p.n_t2;
+
+    const ArenaLayout L = arena_layout(p);
+    const size_t o_store = L.store, o_t = L.t, o_t2 = L.t2, o_part = L.part;
+    const std::vector<size_t>&o_tu = L.tu, &o_ts = L.ts, &o_tg = L.tg, &o_ns = L.ns, &o_nc = L.nc;
+    h->arena_bytes = L.total;
+    cudaError_t e = cudaMalloc(&h->arena, h->arena_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HLRC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", h->arena_bytes, cudaGetErrorString(e));
+    }
+    hlrc_hmat_s* hp = h.get();
+    auto cleanup = [&]() { cudaFree(hp->arena); hp->arena = nullptr; };
+    auto put = [&](size_t o_, const void* src, size_t bytes) -> cudaError_t {
+        if (bytes == 0) return cudaSuccess;
+        return cudaMemcpy(hp->arena + o_, src, bytes, cudaMemcpyHostToDevice);
+    };
+    e = put(o_store, p.store.data(), p.store.size() * sizeof(double));
+    for (size_t i = 0; e == cudaSuccess && i < p.tpasses.size(); ++i) {
+        const TPass& tp = p.tpasses[i];
+        e = put(o_tu[i], tp.units.data(), tp.units.size() * sizeof(TUnit));
+        if (e == cudaSuccess) e = put(o_ts[i], tp.slabs.data(), tp.slabs.size() * sizeof(TSlab));
+        if (e == cudaSuccess) e = put(o_tg[i], tp.groups.data(), tp.groups.size() * sizeof(TGroup));
+        DevTPass d;
+        d.units = reinterpret_cast<const TUnit*>(hp->arena + o_tu[i]);
+        d.slabs = reinterpret_cast<const TSlab*>(hp->arena + o_ts[i]);
+        d.groups = reinterpret_cast<const TGroup*>(hp->arena + o_tg[i]);
+        std::memcpy(d.cls_begin, tp.cls_begin, sizeof(d.cls_begin));
+        d.ngroups = int(tp.groups.size());
+        d.in = tp.in; d.out = tp.out; d.mode = tp.mode; d.bytes = tp.bytes; d.alg_bytes = tp.alg_bytes;
+        hp->t.push_back(d);
+    }
+    for (size_t i = 0; e == cudaSuccess && i < p.npasses.size(); ++i) {
+        const NPass& np = p.npasses[i];
+        e = put(o_ns[i], np.segs.data(), np.segs.size() * sizeof(NSeg));
+        if (e == cudaSuccess) e = put(o_nc[i], np.chunks.data(), np.chunks.size() * sizeof(NChunk));
+        DevNPass d;
+        d.segs = reinterpret_cast<const NSeg*>(hp->arena + o_ns[i]);
+        d.chunks = reinterpret_cast<const NChunk*>(hp->arena + o_nc[i]);
+        d.nsegs = int(np.segs.size());
+        d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
+        hp->n.push_back(d);
+    }
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(HLRC_ERR_CUDA, "upload copy failed: %s", cudaGetErrorString(e));
+    }
+    hp->store = reinterpret_cast<const double*>(hp->arena + o_store);
+    hp->ws_t = reinterpret_cast<double*>(hp->arena + o_t);
+    hp->ws_t2 = reinterpret_cast<double*>(hp->arena + o_t2);
+    hp->part = reinterpret_cast<double*>(hp->arena + o_part);
+    for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
+
+    fill_info(p, L, hp->info);
+    for (int op = 0; op < 3; ++op) {
+        int nl = 0;
+        for (const Stage& st : hp->stages[op])
+            nl += st.kind == 0 ? hp->t[size_t(st.idx)].launches() : hp->n[size_t(st.idx)].launches();
+        hp->info.launches[op] = nl;
+    }
+    *out = h.release();
+    return HLRC_OK;
+}
+
+double* bind(hlrc_hmat M, int name, const double* x, double* y) {
+    switch (name) {
+        case V_X: return const_cast<double*>(x);
+        case V_Y: return y;
+        case V_T: return M->ws_t;
+        default: return M->ws_t2;
+    }
+}
+
+void prof_begin(hlrc_hmat M, const char* name, int64_t alg_bytes, cudaStream_t s) {
+    if (!M->profiling) return;
+    if (M->nprof >= int(M->prof.size())) {
+        ProfileRec r{name, nullptr, nullptr, 0};
+        cudaEventCreate(&r.e0);
+        cudaEventCreate(&r.e1);
+        M->prof.push_back(r);
+    }
+    M->prof[size_t(M->nprof)].name = name;
+    M->prof[size_t(M->nprof)].alg_bytes = alg_bytes;
+    cudaEventRecord(M->prof[size_t(M->nprof)].e0, s);
+}
+void prof_end(hlrc_hmat M, cudaStream_t s) {
+    if (!M->profiling) return;
+    cudaEventRecord(M->prof[size_t(M->nprof)].e1, s);
+    ++M->nprof;
+}
+
+constexpr int NFORM_WARPS = 8;
+
+// one right-hand side: x, y are column vectors
+hlrc_status run_single(hlrc_hmat M, double alpha, int op, const double* x, double* y, cudaStream_t s) {
+    for (const Stage& st : M->stages[op]) {
+        if (st.kind == 0) {
+            const DevTPass& tp = M->t[size_t(st.idx)];
+            const double* vin = bind(M, tp.in, x, y);
+            double* vout = bind(M, tp.out, x, y);
+            const int add = tp.mode == OUT_ADD_ALPHA;
+            prof_begin(M, stage_name(M->kind, 0, st.idx), tp.alg_bytes, s);
+            for (int c = 0; c < 3; ++c) {
+                const int nu = tp.cls_begin[c + 1] - tp.cls_begin[c];
+                if (nu <= 0) continue;
+                const TUnit* u = tp.units + tp.cls_begin[c];
+                const int grid = (nu + 7) / 8;
+                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
+                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
+                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
+            }
+            if (tp.ngroups > 0)
+                k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->part, vout, alpha, add);
+            prof_end(M, s);
+        } else {
+            const DevNPass& np = M->n[size_t(st.idx)];
+            if (np.nsegs == 0) continue;
+            prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
+            k_nform_f64<NFORM_WARPS><<<np.nsegs, NFORM_WARPS * 32, 0, s>>>(
+                np.segs, np.chunks, M->store, bind(M, np.vx, x, y), bind(M, np.vt, x, y), bind(M, np.out, x, y),
+                alpha, np.mode == OUT_ADD_ALPHA);
+            prof_end(M, s);
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return HLRC_OK;
+}
+
+hlrc_status check_mvm_args(hlrc_hmat M, int op, const double* x, double* y, int nrhs, int64_t ldx, int64_t ldy) {
+    if (!M) return fail(HLRC_ERR_ARG, "matrix handle is NULL");
+    if (op < 0 || op > 2) return fail(HLRC_ERR_ARG, "op %d is not a valid hlrc_op", op);
+    if (M->stages[op].empty())
+        return fail(HLRC_ERR_UNSUPPORTED_OP, "op %d is not supported for this matrix (uniform-H: N and C only)", op);
+    if (nrhs < 0) return fail(HLRC_ERR_ARG, "nrhs < 0");
+    const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
+    const int64_t ny = op == HLRC_OP_N ? M->nrows : M->ncols;
+    if (nrhs > 1 && (ldx < nx || ldy < ny)) return fail(HLRC_ERR_SHAPE, "ldx/ldy smaller than the vector length");
+    if (nrhs > 0 && ((nx > 0 && !x) || (ny > 0 && !y))) return fail(HLRC_ERR_ARG, "x or y is NULL");
+    return HLRC_OK;
+}
+
+}  // namespace
+
+extern "C" hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options* opts, hlrc_hmat* out) {
+    clear_error();
+    if (!desc || !out) return fail(HLRC_ERR_ARG, "hlrc_upload_h: null argument");
+    *out = nullptr;
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_h(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    return upload_plan(p, o, out);
+}
+
+extern "C" hlrc_status hlrc_upload_uniform(const hlrc_uniform_desc* desc, const hlrc_options* opts, hlrc_hmat* out) {
+    clear_error();
+    if (!desc || !out) return fail(HLRC_ERR_ARG, "hlrc_upload_uniform: null argument");
+    *out = nullptr;
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_uniform(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    return upload_plan(p, o, out);
+}
+
+extern "C" hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_options* opts, hlrc_info* info) {
+    clear_error();
+    if (!desc || !info) return fail(HLRC_ERR_ARG, "hlrc_plan_info_h: null argument");
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_h(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    fill_info(p, arena_layout(p), *info);
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_plan_info_uniform(const hlrc_uniform_desc* desc, const hlrc_options* opts,
+                                              hlrc_info* info) {
+    clear_error();
+    if (!desc || !info) return fail(HLRC_ERR_ARG, "hlrc_plan_info_uniform: null argument");
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_uniform(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    fill_info(p, arena_layout(p), *info);
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double* x, double* y, int nrhs,
+                                int64_t ldx, int64_t ldy, void* stream) {
+    clear_error();
+    hlrc_status st = check_mvm_args(M, op, x, y, nrhs, ldx, ldy);
+    if (st != HLRC_OK) return st;
+    if (alpha == 0.0 || nrhs == 0) return HLRC_OK;
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (int r = 0; r < nrhs; ++r) {
+        st = run_single(M, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
+        if (st != HLRC_OK) return st;
+    }
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x, double* y, int nrhs,
+                                     int64_t ldx, int64_t ldy) {
+    clear_error();
+    hlrc_status st = check_mvm_args(M, op, x, y, nrhs, ldx, ldy);
+    if (st != HLRC_OK) return st;
+    if (alpha == 0.0 || nrhs == 0) return HLRC_OK;
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
+    const int64_t ny = op == HLRC_OP_N ? M->nrows : M->ncols;
+    const size_t ex = size_t(nx) * size_t(nrhs), ey = size_t(ny) * size_t(nrhs);
+    if (ex > M->hx_elems) {
+        cudaFree(M->hx);
+        M->hx = nullptr;
+        HLRC_CUDA(cudaMalloc(&M->hx, std::max<size_t>(ex, 1) * sizeof(double)));
+        M->hx_elems = ex;
+    }
+    if (ey > M->hy_elems) {
+        cudaFree(M->hy);
+        M->hy = nullptr;
+        HLRC_CUDA(cudaMalloc(&M->hy, std::max<size_t>(ey, 1) * sizeof(double)));
+        M->hy_elems = ey;
+    }
+    const int64_t lx = nrhs > 1 ? ldx : nx, ly = nrhs > 1 ? ldy : ny;
+    HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
+    HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
+    for (int r = 0; r < nrhs; ++r) {
+        st = run_single(M, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
+        if (st != HLRC_OK) return st;
+    }
+    HLRC_CUDA(cudaMemcpy2D(y, size_t(ly) * 8, M->hy, size_t(ny) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyDeviceToHost));
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info) {
+    if (!M || !info) return fail(HLRC_ERR_ARG, "hlrc_get_info: null argument");
+    *info = M->info;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_set_profiling(hlrc_hmat M, int enable) {
+    if (!M) return fail(HLRC_ERR_ARG, "hlrc_set_profiling: null handle");
+    M->profiling = enable != 0;
+    M->nprof = 0;
+    return HLRC_OK;
+}
+
+extern "C" int hlrc_last_profile(hlrc_hmat M, const char** names, int* count, double* ms, int64_t* bytes,
+                                 int cap) {
+    if (!M) return 0;
+    int n = 0;
+    for (int i = 0; i < M->nprof; ++i) {
+        const ProfileRec& r = M->prof[size_t(i)];
+        float t = 0.f;
+        cudaEventSynchronize(r.e1);
+        cudaEventElapsedTime(&t, r.e0, r.e1);
+        int k = 0;
+        while (k < n && names && std::strcmp(names[k], r.name) != 0) ++k;
+        if (k == n) {
+            if (n >= cap) continue;
+            if (names) names[n] = r.name;
+            if (count) count[n] = 0;
+            if (ms) ms[n] = 0.0;
+            if (bytes) bytes[n] = r.alg_bytes;
+            ++n;
+        }
+        if (count) count[k] += 1;
+        if (ms) ms[k] += double(t);
+    }
+    M->nprof = 0;
+    return n;
+}
+
+extern "C" hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code) {
+    if (!M || !code) return fail(HLRC_ERR_ARG, "hlrc_check_device_error: null argument");
+    *code = 0;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
+    if (!M) return HLRC_OK;
+    DeviceGuard g(M->device);
+    for (auto& r : M->prof) {
+        cudaEventDestroy(r.e0);
+        cudaEventDestroy(r.e1);
+    }
+    cudaFree(M->hx);
+    cudaFree(M->hy);
+    cudaFree(M->arena);
+    delete M;
+    return HLRC_OK;
+}

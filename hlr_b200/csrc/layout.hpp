@@ -1,0 +1,79 @@
+// Flattened device layout of an H-matrix / uniform-H matrix.
+//
+// Every matrix that takes part in the product (dense leaf D, low-rank factor
+// U or V, cluster basis V_t, coupling S) is cut into *slabs*: the rows that
+// fall into one output tile (a leaf cluster of <= 64 indices), stored
+// column-major and contiguous with a leading dimension padded to 16 bytes.
+//
+// Two generic batched GEMV forms cover all stages of the product:
+//
+//  N-form  y_tile (+)= alpha * sum_chunks  A_chunk * v_chunk
+//          one CTA per output tile ("segment"); the tile's column chunks
+//          (<= NCHUNK columns of one slab each) are spread over the CTA's
+//          warps; each lane owns two rows; warps are combined in a fixed
+//          order, so the result is deterministic (no atomics).
+//          Used for: U * t (per row tile), D * x, V_t * uy, S * ux.
+//
+//  T-form  out[0:nc] = sum_slabs  A_slab(:, c0:c0+nc)^T * x_slab
+//          one warp per work unit (a run of slabs of one block and <= 32
+//          columns); lanes own two rows; the per-lane column partials are
+//          combined by a butterfly transpose-reduction.  Units of one output
+//          are summed by a finish pass in fixed order (or written directly
+//          when an output has a single unit).
+//          Used for: V^T x (op N), U^T x (op T), D^T x (op T), V_s^T x.
+#pragma once
+
+#include <cstdint>
+
+namespace hlrc {
+
+constexpr int TILE = 64;          // max rows of an output tile / slab
+constexpr int NCHUNK = 8;         // columns per N-form chunk
+constexpr uint32_t VEC_T = 0x80000000u;  // v_off flag: vector lives in the t array
+
+struct NChunk {            // N-form work item: columns [0,nc) of one slab
+    uint64_t a_off;        // element offset of the chunk's first column
+    uint32_t v_off;        // offset of the vector entries (| VEC_T: in t)
+    uint16_t nc;           // columns (<= NCHUNK)
+    uint16_t sidx;         // scale index slot (reduced precision), unused for FP64
+};
+static_assert(sizeof(NChunk) == 16, "NChunk must be 16 bytes");
+
+struct NSeg {              // N-form output tile
+    uint32_t cb, ce;       // chunk range
+    uint32_t out;          // offset of the tile's first output entry
+    uint16_t rows;         // rows of the tile (<= 64)
+    uint16_t ld;           // leading dimension of all slabs of this tile
+};
+static_assert(sizeof(NSeg) == 16, "NSeg must be 16 bytes");
+
+struct TSlab {             // T-form input slab
+    uint64_t a_off;        // element offset of the slab's column 0
+    uint32_t v_off;        // offset of the slab's first row in the input vector
+    uint16_t rows;         // rows (<= 64)
+    uint16_t ld;           // leading dimension (rows padded)
+};
+static_assert(sizeof(TSlab) == 16, "TSlab must be 16 bytes");
+
+enum : uint8_t {
+    TU_DIRECT = 1,         // single unit of its output: write the result itself
+};
+
+struct TUnit {             // T-form work unit (one warp)
+    uint32_t sb, se;       // slab range
+    uint32_t out;          // DIRECT: output offset; else partial slot (x32)
+    uint16_t c0;           // first column of the unit within the slabs
+    uint8_t nc;            // columns (<= 32)
+    uint8_t flags;
+};
+static_assert(sizeof(TUnit) == 16, "TUnit must be 16 bytes");
+
+struct TGroup {            // output of several T-form units, summed in order
+    uint32_t slot0;        // partial slots [slot0, slot0+nslots), 32 doubles each
+    uint32_t nslots;
+    uint32_t out;          // output offset
+    uint32_t nc;           // columns
+};
+static_assert(sizeof(TGroup) == 16, "TGroup must be 16 bytes");
+
+}  // namespace hlrc

@@ -1,0 +1,75 @@
+// Host-side flattening of an H-matrix / uniform-H descriptor into the slab
+// layout and the work lists of the device passes (see layout.hpp).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "hlrc.h"
+#include "layout.hpp"
+
+namespace hlrc {
+
+// Where a pass reads its vectors from / writes its result to.  The device
+// code binds these names to pointers at launch time.
+enum VecName : int {
+    V_X = 0,      // the caller's x
+    V_Y = 1,      // the caller's y
+    V_T = 2,      // workspace coefficients t (H) / ux (uniform)
+    V_T2 = 3,     // workspace coefficients uy (uniform)
+};
+
+// How a pass writes its outputs.
+enum OutMode : int {
+    OUT_SET = 0,        // out = s            (coefficients)
+    OUT_ADD_ALPHA = 1,  // out += alpha * s   (y)
+};
+
+struct TPass {
+    std::vector<TSlab> slabs;
+    std::vector<TUnit> units;      // ordered by column class, then cost
+    int cls_begin[4] = {0, 0, 0, 0};  // units of class c: [cls_begin[c], cls_begin[c+1]); classes nc<=8,16,32
+    std::vector<TGroup> groups;    // outputs with several units
+    uint32_t nslots = 0;
+    int in = V_X, out = V_T, mode = OUT_SET;
+    int64_t bytes = 0;             // stored bytes streamed by the pass (with padding)
+    int64_t alg_bytes = 0;         // unpadded matrix bytes + vector reads/writes
+    bool empty() const { return units.empty(); }
+};
+
+struct NPass {
+    std::vector<NSeg> segs;        // ordered by cost (descending)
+    std::vector<NChunk> chunks;
+    int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
+    int64_t bytes = 0;
+    int64_t alg_bytes = 0;
+    bool empty() const { return segs.empty(); }
+};
+
+// One stage of a product: exactly one of the passes is used.
+struct Stage {
+    int kind;                      // 0 = T-form, 1 = N-form
+    int idx;                       // index into Plan::tpasses / npasses
+};
+
+struct Plan {
+    int kind = 0;                  // 0 = H, 1 = uniform-H
+    int precision = HLRC_PREC_F64;
+    int64_t nrows = 0, ncols = 0;
+    std::vector<double> store;     // FP64 slab storage
+    int64_t n_t = 0, n_t2 = 0;     // workspace vector lengths (per rhs)
+    std::vector<TPass> tpasses;
+    std::vector<NPass> npasses;
+    std::vector<Stage> stages[3];  // per op (N, T, C); empty = unsupported
+    // accounting (per product, one rhs)
+    int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
+    int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;
+    int32_t max_rank = 0;
+};
+
+// Returns HLRC_OK or an error (message recorded via fail()).
+hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p);
+hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan& p);
+
+}  // namespace hlrc

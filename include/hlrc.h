@@ -1,0 +1,291 @@
+/*
+ * hlrc.h — C ABI of the B200 H-matrix / uniform-H matrix-vector product.
+ *
+ * The product computes   y := y + alpha * op(M) * x   for an H-matrix M
+ * (dense leaves and low-rank leaves U*V^T) or a uniform-H matrix M (shared,
+ * non-nested row/column cluster bases with coupling matrices), exactly like
+ * HLR's CPU paths:
+ *
+ *   hlr::tbb::mul_vec(alpha, op_M, M, x, y)              include/hlr/tbb/arith.hh:312-340
+ *   hlr::seq::mul_vec / hlr::mul_vec                     include/hlr/arith/mulvec.hh:27-81
+ *   hlr::tbb::uniform::mul_vec(alpha, op_M, M, x, y,
+ *                              rowcb, colcb)             include/hlr/tbb/arith_uniform.hh:36-96
+ *
+ * Indices are in the matrix's internal (cluster-tree permuted) order, as in
+ * HLR, where the coefficient function is wrapped in TPermCoeffFn
+ * (programs/mvm/mvm.hh:66).
+ *
+ * Conventions
+ *  - Every entry point returns an hlrc_status; no C++ exception crosses the
+ *    ABI.  hlrc_last_error() returns a message for the calling thread.
+ *  - Matrices are column-major; low-rank leaves store M = U * V^T with
+ *    U (nrows x rank) and V (ncols x rank), as hlr::matrix::lrmatrix
+ *    (include/hlr/matrix/lrmatrix.hh:39-204).
+ *  - y is accumulated (y += ...), never overwritten; alpha == 0 is a no-op,
+ *    as in hlr::tbb::mul_vec (include/hlr/tbb/arith.hh:54-55).
+ *  - A device handle is immutable after upload.  Each handle owns one
+ *    scratch workspace, so two hlrc_mvm calls on the same handle must be
+ *    ordered on one stream (or use separate handles / hlrc_workspace).
+ *  - Device pointers (x, y) are plain CUDA device pointers; `stream` is a
+ *    cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Nothing here takes or returns a torch type.
+ */
+#ifndef HLRC_H
+#define HLRC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HLRC_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ status */
+typedef enum hlrc_status {
+    HLRC_OK                 = 0,
+    HLRC_ERR_ARG            = 1,  /* null pointer / bad argument            */
+    HLRC_ERR_SHAPE          = 2,  /* inconsistent sizes, bad block layout    */
+    HLRC_ERR_OOM            = 3,  /* device or host allocation failed        */
+    HLRC_ERR_CUDA           = 4,  /* a CUDA runtime call failed              */
+    HLRC_ERR_TIMEOUT        = 5,  /* a bounded device wait gave up           */
+    HLRC_ERR_UNSUPPORTED_OP = 6,  /* op not supported for this matrix kind   */
+    HLRC_ERR_NOT_CONVERGED  = 7,  /* iterative solver hit its iteration cap  */
+    HLRC_ERR_INTERNAL       = 8
+} hlrc_status;
+
+/* matop_t of HLIBpro (apply_normal/transposed/adjoint); for real data the
+ * transposed and adjoint products are identical. */
+typedef enum hlrc_op {
+    HLRC_OP_N = 0,   /* apply_normal     */
+    HLRC_OP_T = 1,   /* apply_transposed */
+    HLRC_OP_C = 2    /* apply_adjoint    */
+} hlrc_op;
+
+/* Storage precision of the device copy of the matrix data.
+ * Vectors x, y are always FP64; the per-row-tile accumulation of y is FP64. */
+typedef enum hlrc_precision {
+    HLRC_PREC_F64  = 0,  /* FP64 storage, FP64 arithmetic (drop-in path)        */
+    HLRC_PREC_F32  = 1,  /* FP32 storage, FP32 products, FP64 y accumulation     */
+    HLRC_PREC_BF16 = 2,  /* BF16 storage, per-column FP32 scale, FP32 products   */
+    HLRC_PREC_F16  = 3,  /* FP16 storage, per-column FP32 scale, FP32 products   */
+    HLRC_PREC_MIXED = 4  /* per-column choice FP32/FP16 from the singular values
+                            (HLR's VALR rule, include/hlr/compress/valr.hh:402-510);
+                            dense leaves FP32                                    */
+} hlrc_precision;
+
+/* ---------------------------------------------------------- host structures
+ * A caller describes its matrix by a flat list of leaf blocks.  The list
+ * order is the order in which the CPU reference visits leaves
+ * (hlr::mul_vec recursion, block row i then block column j).
+ */
+typedef enum hlrc_leaf_kind {
+    HLRC_LEAF_DENSE   = 0,   /* hlr::matrix::dense_matrix  (dense_matrix.hh:36)   */
+    HLRC_LEAF_LOWRANK = 1    /* hlr::matrix::lrmatrix      (lrmatrix.hh:39)       */
+} hlrc_leaf_kind;
+
+typedef struct hlrc_block {
+    int64_t       row0, nrows;   /* row index set [row0, row0+nrows)          */
+    int64_t       col0, ncols;   /* column index set [col0, col0+ncols)       */
+    int32_t       kind;          /* hlrc_leaf_kind                            */
+    int32_t       rank;          /* low-rank: k (may be 0)                    */
+    const double* D;             /* dense: nrows x ncols, column-major        */
+    int64_t       ldd;
+    const double* U;             /* low-rank: nrows x rank                     */
+    int64_t       ldu;
+    const double* V;             /* low-rank: ncols x rank;  M = U * V^T       */
+    int64_t       ldv;
+    const double* sv;            /* optional: rank singular values (descending)
+                                    of the block, used by HLRC_PREC_MIXED; NULL
+                                    = derive from ||U(:,i)||*||V(:,i)||        */
+} hlrc_block;
+
+typedef struct hlrc_h_desc {
+    int64_t            nrows, ncols;
+    int64_t            nblocks;
+    const hlrc_block*  blocks;
+} hlrc_h_desc;
+
+/* uniform-H: shared_cluster_basis (shared_cluster_basis.hh:39-356) per
+ * cluster, uniform_lrmatrix (uniform_lrmatrix.hh:59-154) per admissible leaf */
+typedef struct hlrc_basis {
+    int64_t       ofs, size;     /* cluster index set [ofs, ofs+size)          */
+    int32_t       rank;          /* k_t (0 allowed)                           */
+    int32_t       pad_;
+    const double* V;             /* size x rank, column-major                  */
+    int64_t       ldv;
+} hlrc_basis;
+
+typedef struct hlrc_uniform_block {
+    int64_t       row0, nrows, col0, ncols;
+    int32_t       kind;          /* HLRC_LEAF_DENSE or HLRC_LEAF_LOWRANK        */
+    int32_t       row_basis;     /* low-rank: index into row_bases            */
+    int32_t       col_basis;     /* low-rank: index into col_bases            */
+    int32_t       pad_;
+    const double* S;             /* low-rank: k_row x k_col coupling, col-major */
+    int64_t       lds;
+    const double* D;             /* dense: nrows x ncols                       */
+    int64_t       ldd;
+} hlrc_uniform_block;
+
+typedef struct hlrc_uniform_desc {
+    int64_t                    nrows, ncols;
+    int64_t                    nrow_bases;
+    const hlrc_basis*          row_bases;
+    int64_t                    ncol_bases;
+    const hlrc_basis*          col_bases;
+    int64_t                    nblocks;
+    const hlrc_uniform_block*  blocks;
+} hlrc_uniform_desc;
+
+typedef struct hlrc_options {
+    int32_t precision;     /* hlrc_precision (default HLRC_PREC_F64)            */
+    int32_t max_nrhs;      /* workspace sized for this many right-hand sides   */
+    double  mixed_eps;     /* HLRC_PREC_MIXED: target accuracy (e.g. 1e-6)      */
+    int32_t device;        /* CUDA device ordinal (-1 = current)                */
+    int32_t reserved[7];
+} hlrc_options;
+
+/* accounting of one product, following HLR's mul_vec_flops /
+ * mul_vec_datasize (arith/mulvec.hh:795-874, arith/uniform.hh:285-325) */
+typedef struct hlrc_info {
+    int64_t n_rows, n_cols;
+    int64_t n_dense, n_lowrank;        /* leaves                                */
+    int64_t n_row_tiles, n_col_tiles;  /* <=64-row output tiles of y            */
+    int64_t matrix_bytes;              /* stored matrix bytes on the device     */
+    int64_t algorithmic_bytes;         /* matrix bytes + vector bytes, 1 rhs    */
+    int64_t flops;                     /* per product, 1 rhs                    */
+    int64_t workspace_bytes;
+    int64_t device_bytes;              /* all device memory owned by the handle */
+    int32_t precision;
+    int32_t kind;                      /* 0 = H, 1 = uniform-H                  */
+    int32_t max_rank;
+    int32_t launches[3];               /* kernel launches per product, op N/T/C
+                                          (0 = op unsupported)                  */
+    int32_t reserved[2];
+} hlrc_info;
+
+typedef struct hlrc_hmat_s* hlrc_hmat;
+
+/* ------------------------------------------------------------ core entry points */
+
+/* Returns HLRC_ABI_VERSION. */
+int         hlrc_abi_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* hlrc_last_error(void);
+
+void        hlrc_default_options(hlrc_options* opts);
+
+/* Flatten an H-matrix into the device layout and upload it.
+ * Replaces building nothing on the HLR side: the caller's adapter walks its
+ * Hpro::TMatrix tree and fills hlrc_block entries.      */
+hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options* opts,
+                          hlrc_hmat* out);
+
+/* Same for a uniform-H matrix (row/column cluster bases + couplings).        */
+hlrc_status hlrc_upload_uniform(const hlrc_uniform_desc* desc,
+                                const hlrc_options* opts, hlrc_hmat* out);
+
+/* Dry run of hlrc_upload_h / hlrc_upload_uniform: validates the descriptor,
+ * flattens it on the host and reports the accounting and the device
+ * footprint that an upload would need, without touching a GPU.  Lets a
+ * caller size device memory before committing (no reference counterpart;
+ * the numbers follow mul_vec_flops / mul_vec_datasize).                     */
+hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_options* opts,
+                             hlrc_info* info);
+hlrc_status hlrc_plan_info_uniform(const hlrc_uniform_desc* desc,
+                                   const hlrc_options* opts, hlrc_info* info);
+
+/* y := y + alpha * op(M) * x on `stream`.
+ * x: ncols(op) x nrhs device array (leading dimension ldx),
+ * y: nrows(op) x nrhs device array (leading dimension ldy).
+ * Replaces hlr::tbb::mul_vec (tbb/arith.hh:312-340) for H-matrices and
+ * hlr::tbb::uniform::mul_vec (tbb/arith_uniform.hh:36-96) for uniform-H.
+ * Uniform-H supports op N and C only; op T returns HLRC_ERR_UNSUPPORTED_OP,
+ * as uniform_lrmatrix::uni_apply_add asserts (uniform_lrmatrix.hh:473-513). */
+hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double* x,
+                     double* y, int nrhs, int64_t ldx, int64_t ldy,
+                     void* stream);
+
+/* Same with x, y in host memory: copies x and y to the device, runs the
+ * product, copies y back, synchronises.  Matches the reference's call on
+ * host-resident scalar_vectors.                                              */
+hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x,
+                          double* y, int nrhs, int64_t ldx, int64_t ldy);
+
+hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info);
+
+/* Device timing of the passes of the products (for roofline reporting).
+ * While profiling is enabled every pass of every hlrc_mvm call is bracketed
+ * by CUDA events on the call's stream.  hlrc_last_profile synchronises on
+ * those events and returns, per pass *name* (static strings), the number of
+ * launches, the summed milliseconds and the algorithmic bytes of one launch
+ * (stored matrix bytes without padding, plus vector reads/writes), then
+ * clears the records.  Returns the number of names written.                 */
+hlrc_status hlrc_set_profiling(hlrc_hmat M, int enable);
+int         hlrc_last_profile(hlrc_hmat M, const char** names, int* count,
+                              double* ms, int64_t* bytes, int cap);
+
+hlrc_status hlrc_free(hlrc_hmat M);
+
+/* Debug-only: copies the device result of the most recent error word (set by
+ * bounded device waits / bounds checks) and clears it.                       */
+hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code);
+
+/* ----------------------------------------------------- host construction
+ * HLR builds its matrices with HLIBpro's clustering (TBSPCTBuilder,
+ * TCardBSPPartStrat), standard admissibility (TStdGeomAdmCond), ACA
+ * (approx/aca.hh:118-436) and SVD recompression (approx/svd.hh:94-197).
+ * HLIBpro is closed/absent, so these are restated here on the host in C++.  */
+
+typedef enum hlrc_problem_kind {
+    HLRC_PROBLEM_LOG1D       = 0,  /* A_ij = log|x_i-x_j|, A_ii = h(log h - 1), x_i ~ U[0,1]   */
+    HLRC_PROBLEM_EXP3D       = 1,  /* A_ij = exp(-|x_i-x_j|/ell) (+ nugget on diagonal), U[0,1]^3 */
+    HLRC_PROBLEM_LAPLACE_SPH = 2   /* collocation 1/(4 pi r) * area_j on a refined octahedron sphere */
+} hlrc_problem_kind;
+
+typedef struct hlrc_problem {
+    int32_t  kind;         /* hlrc_problem_kind                                   */
+    int32_t  leaf_size;    /* cluster tree leaf size (ntile), e.g. 64             */
+    int64_t  n;            /* number of points (ignored for LAPLACE_SPH)          */
+    int32_t  refine;       /* LAPLACE_SPH: octahedron refinement level            */
+    int32_t  uniform;      /* 1: build uniform-H (shared bases) instead of H      */
+    uint64_t seed;         /* point generator seed (std::mt19937_64)              */
+    double   eta;          /* admissibility parameter (2)                         */
+    double   eps;          /* relative ACA/SVD accuracy (1e-6)                    */
+    double   ell;          /* EXP3D correlation length                            */
+    double   nugget;       /* EXP3D diagonal nugget                               */
+    int32_t  nthreads;     /* host threads for the build (0 = all)                */
+    int32_t  reserved[5];
+} hlrc_problem;
+
+typedef struct hlrc_hbuild_s* hlrc_hbuild;
+
+hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out);
+/* descriptors pointing into the build's host storage (valid until free)     */
+hlrc_status hlrc_build_h_desc(hlrc_hbuild B, hlrc_h_desc* out);
+hlrc_status hlrc_build_uniform_desc(hlrc_hbuild B, hlrc_uniform_desc* out);
+/* coordinates in internal order: n x dim, row-major; dim returned           */
+hlrc_status hlrc_build_points(hlrc_hbuild B, const double** pts, int* dim,
+                              int64_t* n);
+/* per-point weights (LAPLACE_SPH: triangle areas), NULL otherwise           */
+hlrc_status hlrc_build_weights(hlrc_hbuild B, const double** w);
+/* internal -> external permutation (perm_i2e), length n                     */
+hlrc_status hlrc_build_perm(hlrc_hbuild B, const int64_t** perm_i2e);
+/* build statistics: seconds, number of leaves, max rank, stored bytes       */
+hlrc_status hlrc_build_stats(hlrc_hbuild B, double* seconds, int64_t* nleaves,
+                             int32_t* max_rank, int64_t* bytes);
+hlrc_status hlrc_build_free(hlrc_hbuild B);
+
+/* kernel entry (i,j) of the problem in internal order — used to form dense
+ * reference products and to assemble leaves                                 */
+double      hlrc_build_entry(hlrc_hbuild B, int64_t i, int64_t j);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HLRC_H */
