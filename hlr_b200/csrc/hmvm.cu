@@ -45,6 +45,16 @@ struct DevNPass {
     int launches() const { return nsegs > 0 ? 1 : 0; }
 };
 
+struct DevTTPass {
+    const TTSeg* segs = nullptr;
+    const TTChunk* chunks = nullptr;
+    const TGroup* groups = nullptr;
+    int nsegs = 0, ngroups = 0;
+    int in = V_X, out = V_T, mode = OUT_SET;
+    int64_t bytes = 0, alg_bytes = 0;
+    int launches() const { return (nsegs > 0 ? 1 : 0) + (ngroups > 0 ? 1 : 0); }
+};
+
 struct ProfileRec {
     const char* name;
     cudaEvent_t e0, e1;
@@ -69,6 +79,7 @@ struct hlrc_hmat_s {
     int64_t n_t = 0, n_t2 = 0;
     std::vector<DevTPass> t;
     std::vector<DevNPass> n;
+    std::vector<DevTTPass> tt;
     std::vector<Stage> stages[3];
     hlrc_info info{};
     // host-pointer entry point staging
@@ -105,19 +116,21 @@ struct DeviceGuard {
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 const char* stage_name(int kind, int nk, int idx) {
-    // names used in profiles: kind 0 = H, 1 = uniform
-    static const char* hn[] = {"tform_VtX", "tform_UtX", "tform_DtX"};
-    static const char* hnn[] = {"nform_Ut_Dx", "nform_Vt"};
-    static const char* un[] = {"tform_fwd_col", "tform_fwd_row", "tform_coupT", "tform_DtX"};
-    static const char* unn[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col"};
-    if (kind == 0) return nk == 0 ? hn[idx] : hnn[idx];
-    return nk == 0 ? un[idx] : unn[idx];
+    // names used in profiles: kind 0 = H, 1 = uniform; nk = stage kind (0 T, 1 N, 2 tile T)
+    static const char* ht[] = {"tform_DtX"};
+    static const char* hn[] = {"nform_Ut_Dx", "nform_Vt"};
+    static const char* htt[] = {"ttform_VtX", "ttform_UtX"};
+    static const char* ut[] = {"tform_unused0", "tform_unused1", "tform_coupT", "tform_DtX"};
+    static const char* un[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col"};
+    static const char* utt[] = {"ttform_fwd_col", "ttform_fwd_row"};
+    if (kind == 0) return nk == 0 ? ht[idx] : (nk == 1 ? hn[idx] : htt[idx]);
+    return nk == 0 ? ut[idx] : (nk == 1 ? un[idx] : utt[idx]);
 }
 
 // Offsets of every array inside the single device arena of a handle.
 struct ArenaLayout {
     size_t store = 0;
-    std::vector<size_t> tu, ts, tg, ns, nc;
+    std::vector<size_t> tu, ts, tg, ns, nc, tts, ttc, ttg;
     size_t t = 0, t2 = 0, part = 0, total = 0;
 };
 
@@ -137,9 +150,16 @@ ArenaLayout arena_layout(const Plan& p) {
         L.ns.push_back(take(np.segs.size() * sizeof(NSeg)));
         L.nc.push_back(take(np.chunks.size() * sizeof(NChunk)));
     }
+    size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
+    for (const TTPass& tp : p.ttpasses) {
+        L.tts.push_back(take(tp.segs.size() * sizeof(TTSeg)));
+        L.ttc.push_back(take(tp.chunks.size() * sizeof(TTChunk)));
+        L.ttg.push_back(take(tp.groups.size() * sizeof(TGroup)));
+        part_elems = std::max(part_elems, size_t(tp.npart));
+    }
     L.t = take(size_t(std::max<int64_t>(1, p.n_t)) * sizeof(double));
     L.t2 = take(size_t(std::max<int64_t>(1, p.n_t2)) * sizeof(double));
-    L.part = take(size_t(std::max<uint32_t>(1, max_slots)) * 32 * sizeof(double));
+    L.part = take(part_elems * sizeof(double));
     L.total = off;
     return L;
 }
@@ -214,6 +234,20 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
         hp->n.push_back(d);
     }
+    for (size_t i = 0; e == cudaSuccess && i < p.ttpasses.size(); ++i) {
+        const TTPass& tp = p.ttpasses[i];
+        e = put(L.tts[i], tp.segs.data(), tp.segs.size() * sizeof(TTSeg));
+        if (e == cudaSuccess) e = put(L.ttc[i], tp.chunks.data(), tp.chunks.size() * sizeof(TTChunk));
+        if (e == cudaSuccess) e = put(L.ttg[i], tp.groups.data(), tp.groups.size() * sizeof(TGroup));
+        DevTTPass d;
+        d.segs = reinterpret_cast<const TTSeg*>(hp->arena + L.tts[i]);
+        d.chunks = reinterpret_cast<const TTChunk*>(hp->arena + L.ttc[i]);
+        d.groups = reinterpret_cast<const TGroup*>(hp->arena + L.ttg[i]);
+        d.nsegs = int(tp.segs.size());
+        d.ngroups = int(tp.groups.size());
+        d.in = tp.in; d.out = tp.out; d.mode = tp.mode; d.bytes = tp.bytes; d.alg_bytes = tp.alg_bytes;
+        hp->tt.push_back(d);
+    }
     if (e != cudaSuccess) {
         cleanup();
         return fail(HLRC_ERR_CUDA, "upload copy failed: %s", cudaGetErrorString(e));
@@ -228,7 +262,8 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) {
         int nl = 0;
         for (const Stage& st : hp->stages[op])
-            nl += st.kind == 0 ? hp->t[size_t(st.idx)].launches() : hp->n[size_t(st.idx)].launches();
+            nl += st.kind == 0 ? hp->t[size_t(st.idx)].launches()
+                               : (st.kind == 1 ? hp->n[size_t(st.idx)].launches() : hp->tt[size_t(st.idx)].launches());
         hp->info.launches[op] = nl;
     }
     *out = h.release();
@@ -263,6 +298,7 @@ void prof_end(hlrc_hmat M, cudaStream_t s) {
 }
 
 constexpr int NFORM_WARPS = 8;
+constexpr int TTFORM_WARPS = 8;
 
 // one right-hand side: x, y are column vectors
 hlrc_status run_single(hlrc_hmat M, double alpha, int op, const double* x, double* y, cudaStream_t s) {
@@ -278,12 +314,26 @@ hlrc_status run_single(hlrc_hmat M, double alpha, int op, const double* x, doubl
                 if (nu <= 0) continue;
                 const TUnit* u = tp.units + tp.cls_begin[c];
                 const int grid = (nu + 7) / 8;
+                static_assert(TCOLS == 8, "T-form units are launched with the 8-column kernel");
                 if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
                 else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
                 else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
             }
             if (tp.ngroups > 0)
                 k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->part, vout, alpha, add);
+            prof_end(M, s);
+        } else if (st.kind == 2) {
+            const DevTTPass& tp = M->tt[size_t(st.idx)];
+            if (tp.nsegs == 0 && tp.ngroups == 0) continue;
+            const double* vin = bind(M, tp.in, x, y);
+            double* vout = bind(M, tp.out, x, y);
+            const int add = tp.mode == OUT_ADD_ALPHA;
+            prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
+            if (tp.nsegs > 0)
+                k_ttform_f64<TTFORM_WARPS><<<tp.nsegs, TTFORM_WARPS * 32, 0, s>>>(tp.segs, tp.chunks, M->store, vin, vout,
+                                                                            M->part, alpha, add);
+            if (tp.ngroups > 0)
+                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->part, vout, alpha, add);
             prof_end(M, s);
         } else {
             const DevNPass& np = M->n[size_t(st.idx)];

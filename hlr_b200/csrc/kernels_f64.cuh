@@ -109,19 +109,21 @@ k_tform_f64(const TUnit* __restrict__ units, int nunits, const TSlab* __restrict
 #pragma unroll
     for (int j = 0; j < NC; ++j) p[j] = 0.0;
     const int r = 2 * lane;
+    // the next slab's descriptor is fetched one iteration ahead so that its
+    // latency overlaps the current slab's loads
+    TSlab sl = u.sb < u.se ? slabs[u.sb] : TSlab{0, 0, 0, 0};
     for (uint32_t s = u.sb; s < u.se; ++s) {
-        const TSlab sl = slabs[s];
-        if (r < sl.ld) {
-            const double v0 = (r < sl.rows) ? __ldg(vin + sl.v_off + r) : 0.0;
-            const double v1 = (r + 1 < sl.rows) ? __ldg(vin + sl.v_off + r + 1) : 0.0;
-            const double* a = A + sl.a_off + size_t(u.c0) * sl.ld + r;
+        const TSlab cur = sl;
+        if (s + 1 < u.se) sl = slabs[s + 1];
+        if (r < cur.ld) {
+            const double v0 = (r < cur.rows) ? __ldg(vin + cur.v_off + r) : 0.0;
+            const double v1 = (r + 1 < cur.rows) ? __ldg(vin + cur.v_off + r + 1) : 0.0;
+            const double* a = A + cur.a_off + size_t(u.c0) * cur.ld + r;
+            double2 m[NC];
 #pragma unroll
-            for (int j = 0; j < NC; ++j) {
-                if (j < u.nc) {
-                    const double2 m = ld_stream(a + size_t(j) * sl.ld);
-                    p[j] = fma(m.y, v1, fma(m.x, v0, p[j]));
-                }
-            }
+            for (int j = 0; j < NC; ++j) m[j] = (j < u.nc) ? ld_stream(a + size_t(j) * cur.ld) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int j = 0; j < NC; ++j) p[j] = fma(m[j].y, v1, fma(m[j].x, v0, p[j]));
         }
     }
     TransposeReduce<NC, 16>::run(p, lane);
@@ -135,6 +137,65 @@ k_tform_f64(const TUnit* __restrict__ units, int nunits, const TSlab* __restrict
         } else {
             part[size_t(u.out) * 32 + c] = p[0];
         }
+    }
+}
+
+// Tile T-form: one CTA (W warps) per input tile; x restricted to the tile
+// stays in registers (lane l holds rows 2l, 2l+1); chunk c goes to warp
+// c % W and is reduced on its own (8 columns -> one transpose-reduction).
+template <int W>
+__global__ void __launch_bounds__(W * 32)
+k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks, const double* __restrict__ A,
+             const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
+             int add) {
+    const TTSeg sg = segs[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = 2 * lane;
+    const bool active = r < sg.ld;
+    const double v0 = (r < sg.rows) ? __ldg(vin + sg.v_off + r) : 0.0;
+    const double v1 = (r + 1 < sg.rows) ? __ldg(vin + sg.v_off + r + 1) : 0.0;
+    uint32_t c = sg.cb + warp;
+    TTChunk nxt = c < sg.ce ? chunks[c] : TTChunk{0, 0, 0, 0};
+    for (; c < sg.ce; c += W) {
+        const TTChunk ch = nxt;
+        if (c + W < sg.ce) nxt = chunks[c + W];
+        const double* a = A + ch.a_off + r;
+        double2 m[TCOLS];
+#pragma unroll
+        for (int j = 0; j < TCOLS; ++j)
+            m[j] = (active && j < ch.nc) ? ld_stream(a + size_t(j) * sg.ld) : make_double2(0.0, 0.0);
+        double p[TCOLS];
+#pragma unroll
+        for (int j = 0; j < TCOLS; ++j) p[j] = fma(m[j].y, v1, m[j].x * v0);
+        TransposeReduce<TCOLS, 16>::run(p, lane);
+        constexpr int SH = 5 - Log2<TCOLS>::v;
+        const int col = lane >> SH;
+        if ((lane & ((1 << SH) - 1)) == 0 && col < ch.nc) {
+            if (ch.flags & TT_DIRECT) {
+                double* o = out + ch.out + col;
+                if (add) *o += alpha * p[0];
+                else *o = p[0];
+            } else {
+                part[ch.out + col] = p[0];
+            }
+        }
+    }
+}
+
+// Sums the per-tile partials of multi-tile tile-T-form outputs in tile order.
+__global__ void __launch_bounds__(256)
+k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,
+               double* __restrict__ out, double alpha, int add) {
+    const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (gid >= ngroups) return;
+    const int lane = threadIdx.x & 31;
+    const TGroup g = groups[gid];
+    for (uint32_t j = lane; j < g.nc; j += 32) {
+        double s = 0.0;
+        for (uint32_t i = 0; i < g.nslots; ++i) s += part[size_t(g.slot0) + size_t(i) * g.nc + j];
+        double* o = out + g.out + j;
+        if (add) *o += alpha * s;
+        else *o = s;
     }
 }
 

@@ -29,6 +29,7 @@ namespace hlrc {
 
 constexpr int TILE = 64;          // max rows of an output tile / slab
 constexpr int NCHUNK = 8;         // columns per N-form chunk
+constexpr int TCOLS = 8;          // columns per T-form unit (register-light: 8 partials per lane)
 constexpr uint32_t VEC_T = 0x80000000u;  // v_off flag: vector lives in the t array
 
 struct NChunk {            // N-form work item: columns [0,nc) of one slab
@@ -69,11 +70,35 @@ struct TUnit {             // T-form work unit (one warp)
 static_assert(sizeof(TUnit) == 16, "TUnit must be 16 bytes");
 
 struct TGroup {            // output of several T-form units, summed in order
-    uint32_t slot0;        // partial slots [slot0, slot0+nslots), 32 doubles each
+    uint32_t slot0;        // unit passes: partial slots [slot0, slot0+nslots), 32 doubles each;
+                           // tile passes: partials at slot0 + i*nc + j, i < nslots
     uint32_t nslots;
     uint32_t out;          // output offset
     uint32_t nc;           // columns
 };
 static_assert(sizeof(TGroup) == 16, "TGroup must be 16 bytes");
+
+// Tile T-form ("TT"): one CTA per input tile (<= 64 rows of x); the tile's
+// slabs are contiguous in the store.  Every chunk (<= TCOLS columns of one
+// slab) is reduced on its own and written to its output or partial slot.
+enum : uint16_t {
+    TT_DIRECT = 1,         // chunk output is final (object has a single tile)
+};
+
+struct TTChunk {
+    uint64_t a_off;        // element offset of the chunk's first column
+    uint32_t out;          // DIRECT: output offset; else offset in the partial array
+    uint16_t nc;           // columns (<= TCOLS)
+    uint16_t flags;
+};
+static_assert(sizeof(TTChunk) == 16, "TTChunk must be 16 bytes");
+
+struct TTSeg {
+    uint32_t cb, ce;       // chunk range
+    uint32_t v_off;        // first row of the tile in the input vector
+    uint16_t rows;         // rows of the tile (<= 64)
+    uint16_t ld;           // leading dimension of all slabs of the tile
+};
+static_assert(sizeof(TTSeg) == 16, "TTSeg must be 16 bytes");
 
 }  // namespace hlrc

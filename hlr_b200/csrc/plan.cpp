@@ -16,7 +16,7 @@ namespace hlrc {
 
 namespace {
 
-constexpr int64_t TFORM_TARGET_ELEMS = 4096;  // elements per T-form unit (32 KB FP64)
+constexpr int64_t TFORM_TARGET_ELEMS = 8192;  // elements per T-form unit (64 KB FP64)
 
 inline int64_t pad_rows(int64_t r) { return (r + 1) & ~int64_t(1); }  // 16-byte FP64 columns
 
@@ -89,8 +89,8 @@ struct TBuilder {
     void add(uint32_t out, int64_t ncols, const std::vector<TSlab>& slabs) {
         for (const TSlab& s : slabs) P.alg_bytes += int64_t(sizeof(double)) * s.rows * (ncols + 1);
         P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
-        for (int64_t c0 = 0; c0 < ncols; c0 += 32) {
-            const int nc = int(std::min<int64_t>(32, ncols - c0));
+        for (int64_t c0 = 0; c0 < ncols; c0 += TCOLS) {
+            const int nc = int(std::min<int64_t>(TCOLS, ncols - c0));
             std::vector<std::pair<uint32_t, uint32_t>> runs;
             uint32_t sb = uint32_t(P.slabs.size());
             int64_t elems = 0;
@@ -160,6 +160,67 @@ struct NBuilder {
         NSeg s{cb, ce, out, uint16_t(rows_), uint16_t(pad_rows(rows_))};
         tmp.push_back({elems, s});
         P.alg_bytes += alg + int64_t(sizeof(double)) * rows_ * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
+    }
+    void finish() {
+        std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        P.segs.clear();
+        for (auto& e : tmp) {
+            P.segs.push_back(e.second);
+            P.bytes += e.first * int64_t(sizeof(double));
+        }
+    }
+};
+
+// Tile T-form pass: objects (low-rank blocks / cluster bases) own an output
+// of `ncols` coefficients and are cut into slabs by input tiles.  Objects on
+// one tile write their chunks' results directly; objects on several tiles
+// write per-tile partials that a finish pass sums in tile order.
+struct TTBuilder {
+    TTPass& P;
+    std::vector<std::pair<int64_t, TTSeg>> tmp;
+    std::vector<int64_t> pbase, ncol;
+    std::vector<uint32_t> oout;
+    uint32_t cb = 0, voff = 0;
+    int64_t elems = 0, rows = 0;
+    TTBuilder(TTPass& p, size_t nobj) : P(p), pbase(nobj, -2), ncol(nobj, 0), oout(nobj, 0) {}
+
+    void object(size_t id, uint32_t out, int64_t ncols, int64_t ntiles) {
+        ncol[id] = ncols;
+        oout[id] = out;
+        if (ntiles > 1) {
+            pbase[id] = P.npart;
+            P.groups.push_back({uint32_t(P.npart), uint32_t(ntiles), out, uint32_t(ncols)});
+            P.npart += ntiles * ncols;
+        } else {
+            pbase[id] = -1;
+        }
+        P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
+    }
+    void begin(int64_t v_off, int64_t tile_rows) {
+        cb = uint32_t(P.chunks.size());
+        voff = uint32_t(v_off);
+        rows = tile_rows;
+        elems = 0;
+    }
+    void slab(int64_t off, int64_t ld, size_t id, int64_t tile_idx) {
+        const int64_t k = ncol[id];
+        for (int64_t j0 = 0; j0 < k; j0 += TCOLS) {
+            const int nc = int(std::min<int64_t>(TCOLS, k - j0));
+            TTChunk c;
+            c.a_off = uint64_t(off + j0 * ld);
+            c.nc = uint16_t(nc);
+            if (pbase[id] < 0) { c.out = uint32_t(oout[id] + j0); c.flags = TT_DIRECT; }
+            else { c.out = uint32_t(pbase[id] + tile_idx * k + j0); c.flags = 0; }
+            P.chunks.push_back(c);
+            elems += ld * nc;
+        }
+        P.alg_bytes += int64_t(sizeof(double)) * rows * k;
+    }
+    void end() {
+        const uint32_t ce = uint32_t(P.chunks.size());
+        if (ce == cb) return;
+        tmp.push_back({elems, TTSeg{cb, ce, voff, uint16_t(rows), uint16_t(pad_rows(rows))}});
+        P.alg_bytes += int64_t(sizeof(double)) * rows;
     }
     void finish() {
         std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
@@ -247,32 +308,37 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
             else slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank));
         }
     }
-    for (int64_t i = 0; i < nb; ++i) {
-        const hlrc_block& b = d.blocks[i];
-        if (toff[size_t(i)] < 0) continue;
-        for (int64_t t = tc.first(b.col0); t < tc.first(b.col0 + b.ncols); ++t)
+    // V slabs ordered by column tile, so that stage A of op N streams one
+    // contiguous region per tile
+    for (int64_t t = 0; t < tc.n(); ++t)
+        for (int64_t i : collist[size_t(t)]) {
+            const hlrc_block& b = d.blocks[i];
+            if (b.kind != HLRC_LEAF_LOWRANK) continue;
             slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank));
-    }
+        }
     st.fill(p.store);
 
-    // op N: T-form V^T x -> t, then N-form per row tile: U t + D x -> y
-    p.tpasses.resize(3);
+    // op N: tile T-form V^T x -> t (per column tile), then N-form per row tile: U t + D x -> y
+    p.tpasses.resize(1);
     p.npasses.resize(2);
+    p.ttpasses.resize(2);
     {
-        TPass& tN = p.tpasses[0];
-        tN.in = V_X; tN.out = V_T; tN.mode = OUT_SET;
-        TBuilder tb(tN);
-        for (int64_t i = 0; i < nb; ++i) {
-            if (toff[size_t(i)] < 0) continue;
-            const hlrc_block& b = d.blocks[i];
-            std::vector<TSlab> sl;
-            int64_t t0 = tc.first(b.col0);
-            for (size_t s = 0; s < slabV[size_t(i)].size(); ++s) {
-                const int64_t t = t0 + int64_t(s);
-                sl.push_back({uint64_t(slabV[size_t(i)][s]), uint32_t(tc.lo(t)), uint16_t(tc.size(t)),
-                              uint16_t(pad_rows(tc.size(t)))});
+        TTPass& a = p.ttpasses[0];
+        a.in = V_X; a.out = V_T; a.mode = OUT_SET;
+        TTBuilder tb(a, size_t(nb));
+        for (int64_t i = 0; i < nb; ++i)
+            if (toff[size_t(i)] >= 0)
+                tb.object(size_t(i), uint32_t(toff[size_t(i)]), d.blocks[i].rank,
+                          tc.first(d.blocks[i].col0 + d.blocks[i].ncols) - tc.first(d.blocks[i].col0));
+        for (int64_t t = 0; t < tc.n(); ++t) {
+            tb.begin(tc.lo(t), tc.size(t));
+            const int64_t ld = pad_rows(tc.size(t));
+            for (int64_t i : collist[size_t(t)]) {
+                if (toff[size_t(i)] < 0) continue;
+                const int64_t ti = t - tc.first(d.blocks[i].col0);
+                tb.slab(slabV[size_t(i)][size_t(ti)], ld, size_t(i), ti);
             }
-            tb.add(uint32_t(toff[size_t(i)]), b.rank, sl);
+            tb.end();
         }
         tb.finish();
     }
@@ -294,22 +360,24 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
         }
         nbld.finish();
     }
-    // op T: T-form U^T x -> t; N-form per column tile V t -> y; T-form D^T x -> y
+    // op T: tile T-form U^T x -> t (per row tile); N-form per column tile V t -> y; T-form D^T x -> y
     {
-        TPass& tT = p.tpasses[1];
-        tT.in = V_X; tT.out = V_T; tT.mode = OUT_SET;
-        TBuilder tb(tT);
-        for (int64_t i = 0; i < nb; ++i) {
-            if (toff[size_t(i)] < 0) continue;
-            const hlrc_block& b = d.blocks[i];
-            std::vector<TSlab> sl;
-            const int64_t t0 = tr.first(b.row0);
-            for (size_t s = 0; s < slabA[size_t(i)].size(); ++s) {
-                const int64_t t = t0 + int64_t(s);
-                sl.push_back({uint64_t(slabA[size_t(i)][s]), uint32_t(tr.lo(t)), uint16_t(tr.size(t)),
-                              uint16_t(pad_rows(tr.size(t)))});
+        TTPass& a = p.ttpasses[1];
+        a.in = V_X; a.out = V_T; a.mode = OUT_SET;
+        TTBuilder tb(a, size_t(nb));
+        for (int64_t i = 0; i < nb; ++i)
+            if (toff[size_t(i)] >= 0)
+                tb.object(size_t(i), uint32_t(toff[size_t(i)]), d.blocks[i].rank,
+                          tr.first(d.blocks[i].row0 + d.blocks[i].nrows) - tr.first(d.blocks[i].row0));
+        for (int64_t t = 0; t < tr.n(); ++t) {
+            tb.begin(tr.lo(t), tr.size(t));
+            const int64_t ld = pad_rows(tr.size(t));
+            for (int64_t i : rowlist[size_t(t)]) {
+                if (toff[size_t(i)] < 0) continue;
+                const int64_t ti = t - tr.first(d.blocks[i].row0);
+                tb.slab(slabA[size_t(i)][size_t(ti)], ld, size_t(i), ti);
             }
-            tb.add(uint32_t(toff[size_t(i)]), b.rank, sl);
+            tb.end();
         }
         tb.finish();
     }
@@ -331,7 +399,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
         nbld.finish();
     }
     {
-        TPass& dT = p.tpasses[2];
+        TPass& dT = p.tpasses[0];
         dT.in = V_X; dT.out = V_Y; dT.mode = OUT_ADD_ALPHA;
         TBuilder tb(dT);
         for (int64_t t = 0; t < tc.n(); ++t) {
@@ -351,9 +419,11 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
         }
         tb.finish();
     }
-    p.stages[HLRC_OP_N] = {{0, 0}, {1, 0}};
-    p.stages[HLRC_OP_T] = {{0, 1}, {1, 1}, {0, 2}};
+    p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}};
+    p.stages[HLRC_OP_T] = {{2, 1}, {1, 1}, {0, 0}};
     p.stages[HLRC_OP_C] = p.stages[HLRC_OP_T];
+    for (const TTPass& tp : p.ttpasses)
+        if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
 
     // accounting (arith/mulvec.hh:795-874)
     double flops = 0, mbytes = 0;
@@ -481,12 +551,11 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
             sD[size_t(i)].push_back(st.alloc(b.D, b.ldd, tr.lo(t) - b.row0, tr.size(t), b.ncols));
         }
     }
-    for (int64_t i = 0; i < ncb; ++i) {
-        if (cboff[size_t(i)] < 0) continue;
-        const hlrc_basis& b = d.col_bases[i];
-        for (int64_t t = tc.first(b.ofs); t < tc.first(b.ofs + b.size); ++t)
+    for (int64_t t = 0; t < tc.n(); ++t)   // column bases by column tile
+        for (int64_t i : cbl[size_t(t)]) {
+            const hlrc_basis& b = d.col_bases[i];
             sCB[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.ofs, tc.size(t), b.rank));
-    }
+        }
     for (int64_t i = 0; i < nb; ++i) {
         const hlrc_uniform_block& b = d.blocks[i];
         if (b.kind != HLRC_LEAF_LOWRANK || b.nrows == 0 || b.ncols == 0) continue;
@@ -499,21 +568,24 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
 
     p.tpasses.resize(4);
     p.npasses.resize(3);
+    p.ttpasses.resize(2);
     // ---- op N
-    {   // forward: ux_s = V_s^T x
-        TPass& f = p.tpasses[0];
+    {   // forward: ux_s = V_s^T x, per column tile over all bases containing it
+        TTPass& f = p.ttpasses[0];
         f.in = V_X; f.out = V_T; f.mode = OUT_SET;
-        TBuilder tb(f);
-        for (int64_t i = 0; i < ncb; ++i) {
-            if (cboff[size_t(i)] < 0) continue;
-            const hlrc_basis& b = d.col_bases[i];
-            std::vector<TSlab> sl;
-            const int64_t t0 = tc.first(b.ofs);
-            for (size_t s = 0; s < sCB[size_t(i)].size(); ++s) {
-                const int64_t t = t0 + int64_t(s);
-                sl.push_back({uint64_t(sCB[size_t(i)][s]), uint32_t(tc.lo(t)), uint16_t(tc.size(t)), uint16_t(pad_rows(tc.size(t)))});
+        TTBuilder tb(f, size_t(ncb));
+        for (int64_t i = 0; i < ncb; ++i)
+            if (cboff[size_t(i)] >= 0)
+                tb.object(size_t(i), uint32_t(cboff[size_t(i)]), d.col_bases[i].rank,
+                          tc.first(d.col_bases[i].ofs + d.col_bases[i].size) - tc.first(d.col_bases[i].ofs));
+        for (int64_t t = 0; t < tc.n(); ++t) {
+            tb.begin(tc.lo(t), tc.size(t));
+            const int64_t ld = pad_rows(tc.size(t));
+            for (int64_t i : cbl[size_t(t)]) {
+                const int64_t ti = t - tc.first(d.col_bases[i].ofs);
+                tb.slab(sCB[size_t(i)][size_t(ti)], ld, size_t(i), ti);
             }
-            tb.add(uint32_t(cboff[size_t(i)]), b.rank, sl);
+            tb.end();
         }
         tb.finish();
     }
@@ -554,20 +626,22 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         nbld.finish();
     }
     // ---- op C (adjoint)
-    {   // forward with row bases: ux'_t = V_t^T x
-        TPass& f = p.tpasses[1];
+    {   // forward with row bases: ux'_t = V_t^T x, per row tile
+        TTPass& f = p.ttpasses[1];
         f.in = V_X; f.out = V_T; f.mode = OUT_SET;
-        TBuilder tb(f);
-        for (int64_t i = 0; i < nrb; ++i) {
-            if (rboff[size_t(i)] < 0) continue;
-            const hlrc_basis& b = d.row_bases[i];
-            std::vector<TSlab> sl;
-            const int64_t t0 = tr.first(b.ofs);
-            for (size_t s = 0; s < sRB[size_t(i)].size(); ++s) {
-                const int64_t t = t0 + int64_t(s);
-                sl.push_back({uint64_t(sRB[size_t(i)][s]), uint32_t(tr.lo(t)), uint16_t(tr.size(t)), uint16_t(pad_rows(tr.size(t)))});
+        TTBuilder tb(f, size_t(nrb));
+        for (int64_t i = 0; i < nrb; ++i)
+            if (rboff[size_t(i)] >= 0)
+                tb.object(size_t(i), uint32_t(rboff[size_t(i)]), d.row_bases[i].rank,
+                          tr.first(d.row_bases[i].ofs + d.row_bases[i].size) - tr.first(d.row_bases[i].ofs));
+        for (int64_t t = 0; t < tr.n(); ++t) {
+            tb.begin(tr.lo(t), tr.size(t));
+            const int64_t ld = pad_rows(tr.size(t));
+            for (int64_t i : rbl[size_t(t)]) {
+                const int64_t ti = t - tr.first(d.row_bases[i].ofs);
+                tb.slab(sRB[size_t(i)][size_t(ti)], ld, size_t(i), ti);
             }
-            tb.add(uint32_t(rboff[size_t(i)]), b.rank, sl);
+            tb.end();
         }
         tb.finish();
     }
@@ -625,9 +699,11 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         }
         tb.finish();
     }
-    p.stages[HLRC_OP_N] = {{0, 0}, {1, 0}, {1, 1}};
+    p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}, {1, 1}};
     p.stages[HLRC_OP_T].clear();  // uniform_lrmatrix::uni_apply_add asserts on apply_transposed
-    p.stages[HLRC_OP_C] = {{0, 1}, {0, 2}, {1, 2}, {0, 3}};
+    p.stages[HLRC_OP_C] = {{2, 1}, {0, 2}, {1, 2}, {0, 3}};
+    for (const TTPass& tp : p.ttpasses)
+        if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
 
     // accounting (arith/uniform.hh:285-325)
     double flops = 0, mbytes = 0, cbbytes = 0, rbbytes = 0;

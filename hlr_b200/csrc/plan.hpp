@@ -47,10 +47,20 @@ struct NPass {
     bool empty() const { return segs.empty(); }
 };
 
+struct TTPass {
+    std::vector<TTSeg> segs;       // ordered by cost (descending)
+    std::vector<TTChunk> chunks;
+    std::vector<TGroup> groups;    // multi-tile outputs: partials summed in tile order
+    int64_t npart = 0;             // partial array length (doubles)
+    int in = V_X, out = V_T, mode = OUT_SET;
+    int64_t bytes = 0, alg_bytes = 0;
+    bool empty() const { return segs.empty(); }
+};
+
 // One stage of a product: exactly one of the passes is used.
 struct Stage {
-    int kind;                      // 0 = T-form, 1 = N-form
-    int idx;                       // index into Plan::tpasses / npasses
+    int kind;                      // 0 = T-form (units), 1 = N-form, 2 = tile T-form
+    int idx;                       // index into Plan::tpasses / npasses / ttpasses
 };
 
 struct Plan {
@@ -61,6 +71,7 @@ struct Plan {
     int64_t n_t = 0, n_t2 = 0;     // workspace vector lengths (per rhs)
     std::vector<TPass> tpasses;
     std::vector<NPass> npasses;
+    std::vector<TTPass> ttpasses;
     std::vector<Stage> stages[3];  // per op (N, T, C); empty = unsupported
     // accounting (per product, one rhs)
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
