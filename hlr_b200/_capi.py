@@ -80,6 +80,7 @@ PROTOTYPES = {
                                          C.POINTER(hlrc_info)]),
     "hlrc_mvm": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64, C.c_void_p]),
     "hlrc_mvm_host": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64]),
+    "hlrc_mvm_noalloc": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hlrc_get_info": (C.c_int, [C.c_void_p, C.POINTER(hlrc_info)]),
     "hlrc_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "hlrc_last_profile": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_int), pdbl,

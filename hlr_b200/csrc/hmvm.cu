@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.hpp"
@@ -76,7 +77,7 @@ struct hlrc_hmat_s {
     double* ws_t = nullptr;
     double* ws_t2 = nullptr;
     double* part = nullptr;
-    int64_t n_t = 0, n_t2 = 0;
+    int64_t n_t = 0, n_t2 = 0, n_part = 0;
     std::vector<DevTPass> t;
     std::vector<DevNPass> n;
     std::vector<DevTTPass> tt;
@@ -132,6 +133,7 @@ struct ArenaLayout {
     size_t store = 0;
     std::vector<size_t> tu, ts, tg, ns, nc, tts, ttc, ttg;
     size_t t = 0, t2 = 0, part = 0, total = 0;
+    size_t part_elems = 0;
 };
 
 ArenaLayout arena_layout(const Plan& p) {
@@ -160,6 +162,7 @@ ArenaLayout arena_layout(const Plan& p) {
     L.t = take(size_t(std::max<int64_t>(1, p.n_t)) * sizeof(double));
     L.t2 = take(size_t(std::max<int64_t>(1, p.n_t2)) * sizeof(double));
     L.part = take(part_elems * sizeof(double));
+    L.part_elems = part_elems;
     L.total = off;
     return L;
 }
@@ -194,6 +197,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     h->n_t2 = p.n_t2;
 
     const ArenaLayout L = arena_layout(p);
+    h->n_part = int64_t(L.part_elems);
     const size_t o_store = L.store, o_t = L.t, o_t2 = L.t2, o_part = L.part;
     const std::vector<size_t>&o_tu = L.tu, &o_ts = L.ts, &o_tg = L.tg, &o_ns = L.ns, &o_nc = L.nc;
     h->arena_bytes = L.total;
@@ -270,12 +274,22 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     return HLRC_OK;
 }
 
-double* bind(hlrc_hmat M, int name, const double* x, double* y) {
+// Scratch used by one product: the coefficient vectors and the partial sums.
+struct Workspace {
+    double* t;
+    double* t2;
+    double* part;
+    bool profile;
+};
+
+Workspace handle_workspace(hlrc_hmat M) { return {M->ws_t, M->ws_t2, M->part, M->profiling}; }
+
+double* bind(const Workspace& ws, int name, const double* x, double* y) {
     switch (name) {
         case V_X: return const_cast<double*>(x);
         case V_Y: return y;
-        case V_T: return M->ws_t;
-        default: return M->ws_t2;
+        case V_T: return ws.t;
+        default: return ws.t2;
     }
 }
 
@@ -300,49 +314,50 @@ void prof_end(hlrc_hmat M, cudaStream_t s) {
 constexpr int NFORM_WARPS = 8;
 constexpr int TTFORM_WARPS = 8;
 
-// one right-hand side: x, y are column vectors
-hlrc_status run_single(hlrc_hmat M, double alpha, int op, const double* x, double* y, cudaStream_t s) {
+// one right-hand side: x, y are column vectors; scratch from `ws`
+hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, const double* x, double* y,
+                       cudaStream_t s) {
     for (const Stage& st : M->stages[op]) {
         if (st.kind == 0) {
             const DevTPass& tp = M->t[size_t(st.idx)];
-            const double* vin = bind(M, tp.in, x, y);
-            double* vout = bind(M, tp.out, x, y);
+            const double* vin = bind(ws, tp.in, x, y);
+            double* vout = bind(ws, tp.out, x, y);
             const int add = tp.mode == OUT_ADD_ALPHA;
-            prof_begin(M, stage_name(M->kind, 0, st.idx), tp.alg_bytes, s);
+            if (ws.profile) prof_begin(M, stage_name(M->kind, 0, st.idx), tp.alg_bytes, s);
             for (int c = 0; c < 3; ++c) {
                 const int nu = tp.cls_begin[c + 1] - tp.cls_begin[c];
                 if (nu <= 0) continue;
                 const TUnit* u = tp.units + tp.cls_begin[c];
                 const int grid = (nu + 7) / 8;
                 static_assert(TCOLS == 8, "T-form units are launched with the 8-column kernel");
-                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
-                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
-                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, M->part, alpha, add);
+                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
+                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
+                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
             }
             if (tp.ngroups > 0)
-                k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->part, vout, alpha, add);
-            prof_end(M, s);
+                k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+            if (ws.profile) prof_end(M, s);
         } else if (st.kind == 2) {
             const DevTTPass& tp = M->tt[size_t(st.idx)];
             if (tp.nsegs == 0 && tp.ngroups == 0) continue;
-            const double* vin = bind(M, tp.in, x, y);
-            double* vout = bind(M, tp.out, x, y);
+            const double* vin = bind(ws, tp.in, x, y);
+            double* vout = bind(ws, tp.out, x, y);
             const int add = tp.mode == OUT_ADD_ALPHA;
-            prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
+            if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
             if (tp.nsegs > 0)
                 k_ttform_f64<TTFORM_WARPS><<<tp.nsegs, TTFORM_WARPS * 32, 0, s>>>(tp.segs, tp.chunks, M->store, vin, vout,
-                                                                            M->part, alpha, add);
+                                                                            ws.part, alpha, add);
             if (tp.ngroups > 0)
-                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->part, vout, alpha, add);
-            prof_end(M, s);
+                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+            if (ws.profile) prof_end(M, s);
         } else {
             const DevNPass& np = M->n[size_t(st.idx)];
             if (np.nsegs == 0) continue;
-            prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
+            if (ws.profile) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
             k_nform_f64<NFORM_WARPS><<<np.nsegs, NFORM_WARPS * 32, 0, s>>>(
-                np.segs, np.chunks, M->store, bind(M, np.vx, x, y), bind(M, np.vt, x, y), bind(M, np.out, x, y),
+                np.segs, np.chunks, M->store, bind(ws, np.vx, x, y), bind(ws, np.vt, x, y), bind(ws, np.out, x, y),
                 alpha, np.mode == OUT_ADD_ALPHA);
-            prof_end(M, s);
+            if (ws.profile) prof_end(M, s);
         }
     }
     const cudaError_t e = cudaGetLastError();
@@ -423,8 +438,9 @@ extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double*
     DeviceGuard g(M->device);
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const Workspace ws = handle_workspace(M);
     for (int r = 0; r < nrhs; ++r) {
-        st = run_single(M, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
+        st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
         if (st != HLRC_OK) return st;
     }
     return HLRC_OK;
@@ -456,8 +472,9 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     const int64_t lx = nrhs > 1 ? ldx : nx, ly = nrhs > 1 ? ldy : ny;
     HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
+    const Workspace ws = handle_workspace(M);
     for (int r = 0; r < nrhs; ++r) {
-        st = run_single(M, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
+        st = run_single(M, ws, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
         if (st != HLRC_OK) return st;
     }
     HLRC_CUDA(cudaMemcpy2D(y, size_t(ly) * 8, M->hy, size_t(ny) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyDeviceToHost));
@@ -507,6 +524,68 @@ extern "C" hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code) {
     if (!M || !code) return fail(HLRC_ERR_ARG, "hlrc_check_device_error: null argument");
     *code = 0;
     return HLRC_OK;
+}
+
+// ------------------------------------------------------------------------
+// hlrc_mvm_noalloc: the product with its scratch in a static device array.
+//
+// The scratch of one product (low-rank coefficients t, the second
+// coefficient array of uniform-H, and the per-tile partial sums) lives in
+// this file-scope array instead of the handle's workspace.  Each device that
+// loads the library holds its own 8 MiB copy until the process exits.
+// Host code must not use `g_noalloc_scratch` as a pointer (on the host it
+// names a stand-in, not device memory): its device address is obtained once
+// per device with cudaGetSymbolAddress while that device is current.
+constexpr size_t NOALLOC_SCRATCH_DOUBLES = size_t(1) << 20;  // 8 MiB
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 128;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// device address of the scratch on `dev` (which must be current)
+hlrc_status noalloc_scratch(int dev, double** out) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(HLRC_ERR_ARG, "hlrc_mvm_noalloc: device ordinal %d outside 0..%d", dev, NOALLOC_MAX_DEVICES - 1);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(HLRC_ERR_CUDA, "hlrc_mvm_noalloc: cudaGetSymbolAddress on device %d failed: %s", dev,
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return HLRC_OK;
+}
+}  // namespace
+
+extern "C" hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op, const double* x, double* y,
+                                        void* stream) {
+    clear_error();
+    hlrc_status st = check_mvm_args(M, op, x, y, 1, 0, 0);
+    if (st != HLRC_OK) return st;
+    if (alpha == 0.0) return HLRC_OK;
+    const size_t need = size_t(std::max<int64_t>(1, M->n_t)) + size_t(std::max<int64_t>(1, M->n_t2)) +
+                        size_t(M->n_part);
+    if (need > NOALLOC_SCRATCH_DOUBLES)
+        return fail(HLRC_ERR_SHAPE,
+                    "hlrc_mvm_noalloc: this matrix needs %zu doubles (%.1f MiB) of scratch, the static scratch "
+                    "holds %zu doubles (8 MiB); use hlrc_mvm",
+                    need, double(need) * 8.0 / 1048576.0, NOALLOC_SCRATCH_DOUBLES);
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    double* base = nullptr;
+    st = noalloc_scratch(M->device, &base);
+    if (st != HLRC_OK) return st;
+    // every scratch entry a product reads is written earlier in the same
+    // product (coefficients with OUT_SET, each partial by its chunk), so the
+    // previous call's contents need no clearing
+    const Workspace ws{base, base + std::max<int64_t>(1, M->n_t),
+                       base + std::max<int64_t>(1, M->n_t) + std::max<int64_t>(1, M->n_t2), false};
+    return run_single(M, ws, alpha, op, x, y, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" hlrc_status hlrc_free(hlrc_hmat M) {

@@ -216,6 +216,33 @@ hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double* x,
 hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x,
                           double* y, int nrhs, int64_t ldx, int64_t ldy);
 
+/* y := y + alpha * op(M) * x for one right-hand side, without allocating.
+ * No counterpart in the reference: HLR's products allocate temporaries on
+ * every call.  Meant for callers that must not allocate device memory while
+ * they run: code that executes while a stream capture in global mode is open
+ * in the process (cudaMalloc/cudaFree are then illegal and break the
+ * capture), latency-critical loops that cannot afford the device-wide
+ * synchronisation cudaFree implies, and processes where another framework's
+ * caching allocator has already reserved the device memory so that a new
+ * cudaMalloc would fail.  The product runs the same kernels as hlrc_mvm, but
+ * its scratch (low-rank coefficients and per-tile partial sums) comes from
+ * one static 8 MiB device array in the library instead of the handle's
+ * workspace; the call itself never calls cudaMalloc, cudaFree or any
+ * allocating routine.
+ *  - Limit: a matrix whose scratch exceeds 8 MiB (about 1M doubles: the sum
+ *    of the low-rank ranks plus the partial sums of blocks spanning several
+ *    tiles) is rejected with HLRC_ERR_SHAPE; use hlrc_mvm for it.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress, with that device current); make that first call
+ *    before any stream capture.
+ *  - Every call on a device shares the one array, which keeps the last
+ *    call's contents (each call writes every entry before reading it).  Calls
+ *    that overlap on the GPU — on different streams, or with different
+ *    handles on the same device — race; order them on one stream.
+ *  - Uniform-H handles are accepted (op N and C).                          */
+hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op,
+                             const double* x, double* y, void* stream);
+
 hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info);
 
 /* Device timing of the passes of the products (for roofline reporting).
