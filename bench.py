@@ -210,6 +210,9 @@ def run_ours(args, rank, world, local_rank):
     ncpu = os.cpu_count() or 1
     nthreads = max(1, ncpu // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", world))))
     prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads)
+    if args.precision:
+        prec = args.precision
+        desc = desc.replace("FP64 ", f"{prec.upper()}-stored ") if prec != "f64" else desc
     tb = time.perf_counter()
     hm = hlr.build(prob)
     t_build = time.perf_counter() - tb
@@ -257,6 +260,31 @@ def run_ours(args, rank, world, local_rank):
     hlr.mul_vec(1.0, hlr.apply_normal, M, x, yc)
     torch.cuda.synchronize()
     ygpu = yc.cpu().numpy()
+
+    # reduced precision: the FP64 GPU product of the same matrix, timed the
+    # same way, is the error reference and the speed-up denominator
+    fp64 = None
+    if prec != "f64":
+        M64 = hlr.upload(hm, precision="f64", uniform=uniform)
+        y64 = torch.zeros(n, dtype=torch.float64, device=dev)
+        hlr.mul_vec(1.0, hlr.apply_normal, M64, x, y64)
+        yy = torch.zeros(n, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = f0.elapsed_time(f1)
+        y64h = y64.cpu().numpy()
+        fp64 = {"value": args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                "matrix_bytes": M64.info["matrix_bytes"],
+                "rel_err_vs_fp64": float(np.linalg.norm(ygpu - y64h) / np.linalg.norm(y64h))}
+        M64.free()
+        del yy, y64
 
     # end to end through the C ABI with pinned host buffers (copies inside)
     xp = torch.from_numpy(xh.copy()).pin_memory()
@@ -317,6 +345,9 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "clocks": clocks.summary(),
     }
+    if fp64 is not None:
+        fp64["speedup"] = (value / world) / fp64["value"]
+        line["fp64_gpu"] = fp64
     # CPU baseline (oracle port on the host cores, bounded sample) and error
     if not args.no_cpu_baseline and world == 1:
         d = hm.uniform_desc() if uniform else hm.h_desc()
@@ -341,17 +372,16 @@ def run_ours(args, rank, world, local_rank):
 
 
 def traffic_from_profiles(kernel: str, config: str):
-    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
-    p = ROOT / "profiles" / "traffic.md"
-    if not p.exists():
-        return None
-    for ln in p.read_text().splitlines():
-        parts = [s.strip() for s in ln.strip().strip("|").split("|")]
-        if len(parts) >= 3 and parts[0] == kernel and parts[1] == config:
-            try:
-                return float(parts[2])
-            except ValueError:
-                return None
+    """DRAM bytes per launch of `kernel` from a committed ncu summary table
+    row `| kernel | config | bytes |` in profiles/*.md, if any."""
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for ln in p.read_text().splitlines():
+            parts = [s.strip() for s in ln.strip().strip("|").split("|")]
+            if len(parts) == 3 and parts[0] == kernel and parts[1] == config:
+                try:
+                    return float(parts[2])
+                except ValueError:
+                    return None
     return None
 
 
@@ -363,6 +393,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed"],
+                    help="storage precision (default: the config's)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

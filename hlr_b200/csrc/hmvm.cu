@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -18,6 +19,7 @@
 #include "common.hpp"
 #include "hlrc.h"
 #include "kernels_f64.cuh"
+#include "kernels_q.cuh"
 #include "plan.hpp"
 
 namespace hlrc {
@@ -38,22 +40,32 @@ struct DevTPass {
 };
 
 struct DevNPass {
-    const NSeg* segs = nullptr;
-    const NChunk* chunks = nullptr;
-    int nsegs = 0;
+    const NSeg* segs[4] = {};         // per StoreFmt
+    int nsegs[4] = {0, 0, 0, 0};
+    const void* chunks = nullptr;     // NChunk (FP64 plan) or QNChunk (reduced precision)
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0, alg_bytes = 0;
-    int launches() const { return nsegs > 0 ? 1 : 0; }
+    int launches() const {
+        int n = 0;
+        for (int f = 0; f < 4; ++f) n += nsegs[f] > 0 ? 1 : 0;
+        return n;
+    }
 };
 
 struct DevTTPass {
-    const TTSeg* segs = nullptr;
-    const TTChunk* chunks = nullptr;
+    const TTSeg* segs[4] = {};
+    int nsegs[4] = {0, 0, 0, 0};
+    const void* chunks = nullptr;     // TTChunk (FP64 plan) or QTTChunk
     const TGroup* groups = nullptr;
-    int nsegs = 0, ngroups = 0;
+    int ngroups = 0;
+    int64_t npart = 0;
     int in = V_X, out = V_T, mode = OUT_SET;
     int64_t bytes = 0, alg_bytes = 0;
-    int launches() const { return (nsegs > 0 ? 1 : 0) + (ngroups > 0 ? 1 : 0); }
+    int launches() const {
+        int n = ngroups > 0 ? 1 : 0;
+        for (int f = 0; f < 4; ++f) n += nsegs[f] > 0 ? 1 : 0;
+        return n;
+    }
 };
 
 struct ProfileRec {
@@ -73,7 +85,7 @@ struct hlrc_hmat_s {
     int64_t nrows = 0, ncols = 0;
     char* arena = nullptr;
     size_t arena_bytes = 0;
-    const double* store = nullptr;
+    const uint8_t* store = nullptr;
     double* ws_t = nullptr;
     double* ws_t2 = nullptr;
     double* part = nullptr;
@@ -118,12 +130,12 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 const char* stage_name(int kind, int nk, int idx) {
     // names used in profiles: kind 0 = H, 1 = uniform; nk = stage kind (0 T, 1 N, 2 tile T)
-    static const char* ht[] = {"tform_DtX"};
+    static const char* ht[] = {"tform_unused"};
     static const char* hn[] = {"nform_Ut_Dx", "nform_Vt"};
-    static const char* htt[] = {"ttform_VtX", "ttform_UtX"};
-    static const char* ut[] = {"tform_unused0", "tform_unused1", "tform_coupT", "tform_DtX"};
+    static const char* htt[] = {"ttform_VtX", "ttform_UtX", "ttform_DtX"};
+    static const char* ut[] = {"tform_coupT"};
     static const char* un[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col"};
-    static const char* utt[] = {"ttform_fwd_col", "ttform_fwd_row"};
+    static const char* utt[] = {"ttform_fwd_col", "ttform_fwd_row", "ttform_DtX"};
     if (kind == 0) return nk == 0 ? ht[idx] : (nk == 1 ? hn[idx] : htt[idx]);
     return nk == 0 ? ut[idx] : (nk == 1 ? un[idx] : utt[idx]);
 }
@@ -131,7 +143,8 @@ const char* stage_name(int kind, int nk, int idx) {
 // Offsets of every array inside the single device arena of a handle.
 struct ArenaLayout {
     size_t store = 0;
-    std::vector<size_t> tu, ts, tg, ns, nc, tts, ttc, ttg;
+    std::vector<size_t> tu, ts, tg, nc, ttc, ttg;
+    std::vector<std::array<size_t, 4>> ns, tts;   // per pass, per StoreFmt
     size_t t = 0, t2 = 0, part = 0, total = 0;
     size_t part_elems = 0;
 };
@@ -140,7 +153,9 @@ ArenaLayout arena_layout(const Plan& p) {
     ArenaLayout L;
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o_ = off; off = align_up(off + bytes, 256); return o_; };
-    L.store = take(p.store.size() * sizeof(double));
+    static_assert(sizeof(NChunk) == sizeof(QNChunk) && sizeof(TTChunk) == sizeof(QTTChunk),
+                  "FP64 and reduced-precision chunk descriptors share one size");
+    L.store = take(p.store.size());
     uint32_t max_slots = 0;
     for (const TPass& tp : p.tpasses) {
         L.tu.push_back(take(tp.units.size() * sizeof(TUnit)));
@@ -149,13 +164,17 @@ ArenaLayout arena_layout(const Plan& p) {
         max_slots = std::max(max_slots, tp.nslots);
     }
     for (const NPass& np : p.npasses) {
-        L.ns.push_back(take(np.segs.size() * sizeof(NSeg)));
-        L.nc.push_back(take(np.chunks.size() * sizeof(NChunk)));
+        std::array<size_t, 4> o{};
+        for (int f = 0; f < 4; ++f) o[size_t(f)] = take(np.segs[f].size() * sizeof(NSeg));
+        L.ns.push_back(o);
+        L.nc.push_back(take(np.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(NChunk) : sizeof(QNPack))));
     }
     size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
     for (const TTPass& tp : p.ttpasses) {
-        L.tts.push_back(take(tp.segs.size() * sizeof(TTSeg)));
-        L.ttc.push_back(take(tp.chunks.size() * sizeof(TTChunk)));
+        std::array<size_t, 4> o{};
+        for (int f = 0; f < 4; ++f) o[size_t(f)] = take(tp.segs[f].size() * sizeof(TTSeg));
+        L.tts.push_back(o);
+        L.ttc.push_back(take(tp.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(TTChunk) : sizeof(QTTPack))));
         L.ttg.push_back(take(tp.groups.size() * sizeof(TGroup)));
         part_elems = std::max(part_elems, size_t(tp.npart));
     }
@@ -182,6 +201,62 @@ void fill_info(const Plan& p, const ArenaLayout& L, hlrc_info& in) {
     in.max_rank = p.max_rank;
 }
 
+// Device descriptors of the planner's chunks: FP64 plans address the store
+// in doubles (64-bit offsets), reduced-precision plans in 16-byte units and
+// carry each chunk's format and scale.
+// FP64 plans: one 16-byte descriptor per chunk.  Reduced-precision plans: one
+// 32-byte pack per chunk or pair of chunks (GC_PACK2 marks the second part);
+// pack_of[i] is the pack of chunk i, used to remap segment ranges.
+std::vector<uint8_t> encode_chunks(const std::vector<GChunk>& g, bool f64, bool tt, std::vector<uint32_t>& pack_of) {
+    std::vector<uint8_t> out;
+    pack_of.assign(g.size(), 0);
+    if (f64) {
+        out.resize(g.size() * 16);
+        for (size_t i = 0; i < g.size(); ++i) {
+            pack_of[i] = uint32_t(i);
+            if (tt) {
+                const TTChunk c{g[i].byte_off / 8, g[i].vo, g[i].nc, uint16_t(g[i].flags & ~GC_PACK2)};
+                std::memcpy(out.data() + 16 * i, &c, 16);
+            } else {
+                const NChunk c{g[i].byte_off / 8, g[i].vo, g[i].nc, 0};
+                std::memcpy(out.data() + 16 * i, &c, 16);
+            }
+        }
+        return out;
+    }
+    auto part = [&](size_t i, uint8_t* dst) {
+        if (tt) {
+            const QTTChunk c{uint32_t(g[i].byte_off / 16), g[i].vo, g[i].scale, g[i].nc, g[i].fmt,
+                             uint8_t(g[i].flags & ~GC_PACK2)};
+            std::memcpy(dst, &c, 16);
+        } else {
+            const QNChunk c{uint32_t(g[i].byte_off / 16), g[i].vo, g[i].scale, g[i].nc, g[i].fmt, 0};
+            std::memcpy(dst, &c, 16);
+        }
+    };
+    uint32_t np = 0;
+    for (size_t i = 0; i < g.size(); ++i) {
+        if (g[i].flags & GC_PACK2) { pack_of[i] = np - 1; continue; }
+        pack_of[i] = np++;
+    }
+    out.assign(size_t(np) * 32, 0);
+    for (size_t i = 0; i < g.size(); ++i) part(i, out.data() + 32 * pack_of[i] + ((g[i].flags & GC_PACK2) ? 16 : 0));
+    return out;
+}
+
+template <typename Seg>
+std::vector<Seg> remap_segs(const std::vector<Seg>& segs, const std::vector<uint32_t>& pack_of) {
+    std::vector<Seg> r = segs;
+    for (Seg& s : r) {
+        if (s.ce > s.cb) {
+            const uint32_t b = pack_of[s.cb], e = pack_of[s.ce - 1] + 1;
+            s.cb = b;
+            s.ce = e;
+        }
+    }
+    return r;
+}
+
 hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     auto h = std::make_unique<hlrc_hmat_s>();
     int dev = o.device;
@@ -199,7 +274,8 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     const ArenaLayout L = arena_layout(p);
     h->n_part = int64_t(L.part_elems);
     const size_t o_store = L.store, o_t = L.t, o_t2 = L.t2, o_part = L.part;
-    const std::vector<size_t>&o_tu = L.tu, &o_ts = L.ts, &o_tg = L.tg, &o_ns = L.ns, &o_nc = L.nc;
+    const std::vector<size_t>&o_tu = L.tu, &o_ts = L.ts, &o_tg = L.tg, &o_nc = L.nc;
+    const std::vector<std::array<size_t, 4>>& o_ns = L.ns;
     h->arena_bytes = L.total;
     cudaError_t e = cudaMalloc(&h->arena, h->arena_bytes);
     if (e != cudaSuccess) {
@@ -212,7 +288,8 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         if (bytes == 0) return cudaSuccess;
         return cudaMemcpy(hp->arena + o_, src, bytes, cudaMemcpyHostToDevice);
     };
-    e = put(o_store, p.store.data(), p.store.size() * sizeof(double));
+    const bool f64 = p.precision == HLRC_PREC_F64;
+    e = put(o_store, p.store.data(), p.store.size());
     for (size_t i = 0; e == cudaSuccess && i < p.tpasses.size(); ++i) {
         const TPass& tp = p.tpasses[i];
         e = put(o_tu[i], tp.units.data(), tp.units.size() * sizeof(TUnit));
@@ -229,26 +306,37 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     }
     for (size_t i = 0; e == cudaSuccess && i < p.npasses.size(); ++i) {
         const NPass& np = p.npasses[i];
-        e = put(o_ns[i], np.segs.data(), np.segs.size() * sizeof(NSeg));
-        if (e == cudaSuccess) e = put(o_nc[i], np.chunks.data(), np.chunks.size() * sizeof(NChunk));
         DevNPass d;
-        d.segs = reinterpret_cast<const NSeg*>(hp->arena + o_ns[i]);
-        d.chunks = reinterpret_cast<const NChunk*>(hp->arena + o_nc[i]);
-        d.nsegs = int(np.segs.size());
+        std::vector<uint32_t> pack_of;
+        const std::vector<uint8_t> enc = encode_chunks(np.chunks, f64, false, pack_of);
+        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+            const std::vector<NSeg> sg = remap_segs(np.segs[f], pack_of);
+            e = put(o_ns[i][size_t(f)], sg.data(), sg.size() * sizeof(NSeg));
+            d.segs[f] = reinterpret_cast<const NSeg*>(hp->arena + o_ns[i][size_t(f)]);
+            d.nsegs[f] = int(sg.size());
+        }
+        if (e == cudaSuccess) e = put(o_nc[i], enc.data(), enc.size());
+        d.chunks = hp->arena + o_nc[i];
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
         hp->n.push_back(d);
     }
     for (size_t i = 0; e == cudaSuccess && i < p.ttpasses.size(); ++i) {
         const TTPass& tp = p.ttpasses[i];
-        e = put(L.tts[i], tp.segs.data(), tp.segs.size() * sizeof(TTSeg));
-        if (e == cudaSuccess) e = put(L.ttc[i], tp.chunks.data(), tp.chunks.size() * sizeof(TTChunk));
-        if (e == cudaSuccess) e = put(L.ttg[i], tp.groups.data(), tp.groups.size() * sizeof(TGroup));
         DevTTPass d;
-        d.segs = reinterpret_cast<const TTSeg*>(hp->arena + L.tts[i]);
-        d.chunks = reinterpret_cast<const TTChunk*>(hp->arena + L.ttc[i]);
+        std::vector<uint32_t> pack_of;
+        const std::vector<uint8_t> enc = encode_chunks(tp.chunks, f64, true, pack_of);
+        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+            const std::vector<TTSeg> sg = remap_segs(tp.segs[f], pack_of);
+            e = put(L.tts[i][size_t(f)], sg.data(), sg.size() * sizeof(TTSeg));
+            d.segs[f] = reinterpret_cast<const TTSeg*>(hp->arena + L.tts[i][size_t(f)]);
+            d.nsegs[f] = int(sg.size());
+        }
+        if (e == cudaSuccess) e = put(L.ttc[i], enc.data(), enc.size());
+        if (e == cudaSuccess) e = put(L.ttg[i], tp.groups.data(), tp.groups.size() * sizeof(TGroup));
+        d.chunks = hp->arena + L.ttc[i];
         d.groups = reinterpret_cast<const TGroup*>(hp->arena + L.ttg[i]);
-        d.nsegs = int(tp.segs.size());
         d.ngroups = int(tp.groups.size());
+        d.npart = tp.npart;
         d.in = tp.in; d.out = tp.out; d.mode = tp.mode; d.bytes = tp.bytes; d.alg_bytes = tp.alg_bytes;
         hp->tt.push_back(d);
     }
@@ -256,7 +344,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         cleanup();
         return fail(HLRC_ERR_CUDA, "upload copy failed: %s", cudaGetErrorString(e));
     }
-    hp->store = reinterpret_cast<const double*>(hp->arena + o_store);
+    hp->store = reinterpret_cast<const uint8_t*>(hp->arena + o_store);
     hp->ws_t = reinterpret_cast<double*>(hp->arena + o_t);
     hp->ws_t2 = reinterpret_cast<double*>(hp->arena + o_t2);
     hp->part = reinterpret_cast<double*>(hp->arena + o_part);
@@ -330,33 +418,66 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 const TUnit* u = tp.units + tp.cls_begin[c];
                 const int grid = (nu + 7) / 8;
                 static_assert(TCOLS == 8, "T-form units are launched with the 8-column kernel");
-                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
-                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
-                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, M->store, vin, vout, ws.part, alpha, add);
+                const double* A = reinterpret_cast<const double*>(M->store);  // unit T-form: FP64 plans only
+                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
+                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
+                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
             }
             if (tp.ngroups > 0)
                 k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
             if (ws.profile) prof_end(M, s);
         } else if (st.kind == 2) {
             const DevTTPass& tp = M->tt[size_t(st.idx)];
-            if (tp.nsegs == 0 && tp.ngroups == 0) continue;
+            if (tp.launches() == 0) continue;
             const double* vin = bind(ws, tp.in, x, y);
             double* vout = bind(ws, tp.out, x, y);
             const int add = tp.mode == OUT_ADD_ALPHA;
             if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-            if (tp.nsegs > 0)
-                k_ttform_f64<TTFORM_WARPS><<<tp.nsegs, TTFORM_WARPS * 32, 0, s>>>(tp.segs, tp.chunks, M->store, vin, vout,
+            const QTTPack* qc = static_cast<const QTTPack*>(tp.chunks);
+            constexpr int TW = TTFORM_WARPS;
+            if (tp.nsegs[FMT_F64] > 0)
+                k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
+                    tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
+                    reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
+            if (tp.nsegs[FMT_F32] > 0)
+                k_ttform_q<TW, FMT_F32><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(tp.segs[FMT_F32], qc, M->store, vin, vout,
                                                                             ws.part, alpha, add);
-            if (tp.ngroups > 0)
-                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+            if (tp.nsegs[FMT_F16] > 0)
+                k_ttform_q<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(tp.segs[FMT_F16], qc, M->store, vin, vout,
+                                                                            ws.part, alpha, add);
+            if (tp.nsegs[FMT_BF16] > 0)
+                k_ttform_q<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(tp.segs[FMT_BF16], qc, M->store, vin,
+                                                                              vout, ws.part, alpha, add);
             if (ws.profile) prof_end(M, s);
+            if (tp.ngroups > 0) {
+                if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
+                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+                if (ws.profile) prof_end(M, s);
+            }
         } else {
             const DevNPass& np = M->n[size_t(st.idx)];
-            if (np.nsegs == 0) continue;
+            if (np.launches() == 0) continue;
             if (ws.profile) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
-            k_nform_f64<NFORM_WARPS><<<np.nsegs, NFORM_WARPS * 32, 0, s>>>(
-                np.segs, np.chunks, M->store, bind(ws, np.vx, x, y), bind(ws, np.vt, x, y), bind(ws, np.out, x, y),
-                alpha, np.mode == OUT_ADD_ALPHA);
+            const double* vx = bind(ws, np.vx, x, y);
+            const double* vt = bind(ws, np.vt, x, y);
+            double* vo = bind(ws, np.out, x, y);
+            const int add = np.mode == OUT_ADD_ALPHA;
+            const QNPack* qc = static_cast<const QNPack*>(np.chunks);
+            constexpr int NW = NFORM_WARPS;
+            // formats in fixed order: each launch adds its part of y
+            if (np.nsegs[FMT_F64] > 0)
+                k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
+                    np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
+                    reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
+            if (np.nsegs[FMT_F32] > 0)
+                k_nform_q<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(np.segs[FMT_F32], qc, M->store, vx, vt, vo,
+                                                                           alpha, add);
+            if (np.nsegs[FMT_F16] > 0)
+                k_nform_q<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(np.segs[FMT_F16], qc, M->store, vx, vt, vo,
+                                                                           alpha, add);
+            if (np.nsegs[FMT_BF16] > 0)
+                k_nform_q<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(np.segs[FMT_BF16], qc, M->store, vx, vt,
+                                                                             vo, alpha, add);
             if (ws.profile) prof_end(M, s);
         }
     }

@@ -19,22 +19,22 @@ __device__ __forceinline__ double2 ld_stream(const double* p) {
 // g <= 5): at each step a lane keeps one half of its values and trades the
 // other half with its partner, so 32 columns cost 31 shuffles instead of
 // 5 * 32.  Afterwards p[0] holds the warp total of column lane >> (5 - g).
-template <int N, int O>
+template <int N, int O, typename T = double>
 struct TransposeReduce {
-    static __device__ __forceinline__ void run(double* p, int lane) {
+    static __device__ __forceinline__ void run(T* p, int lane) {
         if constexpr (N > 1) {
             constexpr int H = N / 2;
             const bool up = (lane & O) != 0;
 #pragma unroll
             for (int j = 0; j < H; ++j) {
-                const double send = up ? p[j] : p[j + H];
-                const double keep = up ? p[j + H] : p[j];
+                const T send = up ? p[j] : p[j + H];
+                const T keep = up ? p[j + H] : p[j];
                 p[j] = keep + __shfl_xor_sync(0xffffffffu, send, O);
             }
-            if constexpr (O > 1) TransposeReduce<H, O / 2>::run(p, lane);
+            if constexpr (O > 1) TransposeReduce<H, O / 2, T>::run(p, lane);
         } else {
             p[0] += __shfl_xor_sync(0xffffffffu, p[0], O);
-            if constexpr (O > 1) TransposeReduce<1, O / 2>::run(p, lane);
+            if constexpr (O > 1) TransposeReduce<1, O / 2, T>::run(p, lane);
         }
     }
 };
@@ -191,8 +191,19 @@ k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __r
     const int lane = threadIdx.x & 31;
     const TGroup g = groups[gid];
     for (uint32_t j = lane; j < g.nc; j += 32) {
-        double s = 0.0;
-        for (uint32_t i = 0; i < g.nslots; ++i) s += part[size_t(g.slot0) + size_t(i) * g.nc + j];
+        // four interleaved partial sums keep four loads in flight; they are
+        // combined in a fixed order, so the result is deterministic
+        const double* p = part + size_t(g.slot0) + j;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        uint32_t i = 0;
+        for (; i + 4 <= g.nslots; i += 4) {
+            s0 += p[size_t(i) * g.nc];
+            s1 += p[size_t(i + 1) * g.nc];
+            s2 += p[size_t(i + 2) * g.nc];
+            s3 += p[size_t(i + 3) * g.nc];
+        }
+        for (; i < g.nslots; ++i) s0 += p[size_t(i) * g.nc];
+        const double s = (s0 + s1) + (s2 + s3);
         double* o = out + g.out + j;
         if (add) *o += alpha * s;
         else *o = s;

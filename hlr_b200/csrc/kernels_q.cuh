@@ -1,0 +1,238 @@
+// Reduced-precision (FP32 / scaled FP16 / scaled BF16 storage) versions of
+// the N-form and tile T-form kernels.
+//
+// Every load is 16 bytes per lane whatever the format: a lane owns R = 16/e
+// consecutive rows of a column (4 for FP32, 8 for 16-bit), G = 64/R lanes
+// cover a 64-row tile column, and one warp instruction reads C = 32/G
+// columns.  A work item is a pack of up to two chunks of one format with at
+// most 8*C columns together (4 KB at full tile height), so a warp iteration
+// moves as many bytes as the FP64 kernels'.  One launch handles one format.
+// Products and the sums inside a pack are FP32; pack results are added to
+// FP64 per-row accumulators, and y is accumulated in FP64 (HLR's compressed
+// BLAS likewise decodes entries inside the GEMV loop: compress/fp32.hh:210-312,
+// compress/bfp.hh:945-1100).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "kernels_f64.cuh"
+#include "layout.hpp"
+
+namespace hlrc {
+
+template <int FMT> struct QFmt;
+template <> struct QFmt<FMT_F32> { static constexpr int R = 4, G = 16, C = 2, LOG_G = 4; };
+template <> struct QFmt<FMT_F16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
+template <> struct QFmt<FMT_BF16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
+
+// 16 loaded bytes -> R floats
+template <int FMT>
+__device__ __forceinline__ void unpack16(const uint4& u, float* f) {
+    if constexpr (FMT == FMT_F32) {
+        f[0] = __uint_as_float(u.x); f[1] = __uint_as_float(u.y);
+        f[2] = __uint_as_float(u.z); f[3] = __uint_as_float(u.w);
+    } else if constexpr (FMT == FMT_F16) {
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            __half2 h;
+            memcpy(&h, &w[i], 4);
+            const float2 t = __half22float2(h);
+            f[2 * i] = t.x;
+            f[2 * i + 1] = t.y;
+        }
+    } else {
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            f[2 * i] = __uint_as_float(w[i] << 16);
+            f[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+        }
+    }
+}
+
+__device__ __forceinline__ QNPack ld_pack(const QNPack* p) {
+    QNPack r;
+    const uint4* s = reinterpret_cast<const uint4*>(p);
+    const uint4 a = __ldg(s), b = __ldg(s + 1);
+    memcpy(&r.p[0], &a, 16);
+    memcpy(&r.p[1], &b, 16);
+    return r;
+}
+__device__ __forceinline__ QTTPack ld_pack(const QTTPack* p) {
+    QTTPack r;
+    const uint4* s = reinterpret_cast<const uint4*>(p);
+    const uint4 a = __ldg(s), b = __ldg(s + 1);
+    memcpy(&r.p[0], &a, 16);
+    memcpy(&r.p[1], &b, 16);
+    return r;
+}
+
+// The lane's 8 loads of a pack: column j = g + C*i of the pack lies in part 0
+// for j < n0, else in part 1.
+template <int FMT>
+__device__ __forceinline__ void load_pack(const uint8_t* A, uint32_t a0, uint32_t a1, int n0, int ntot, int ld,
+                                          int lane, uint4* m) {
+    using F = QFmt<FMT>;
+    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
+    const bool active = l * F::R < ld;
+    const size_t colb = size_t(ld) * fmt_bytes(FMT);
+    const size_t b0 = size_t(a0) * 16 + size_t(l) * 16, b1 = size_t(a1) * 16 + size_t(l) * 16;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int j = g + F::C * i;
+        const size_t off = j < n0 ? b0 + size_t(j) * colb : b1 + size_t(j - n0) * colb;
+        m[i] = (active && j < ntot) ? __ldcs(reinterpret_cast<const uint4*>(A + off)) : make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+// ------------------------------------------------------------------ N-form
+// acc[R] (this lane's rows) += A_pack(:, own columns) * v(own columns)
+template <int FMT>
+__device__ __forceinline__ void npack_q(const QNPack& pk, const uint8_t* A, const double* vx, const double* vt,
+                                        int ld, int lane, double* acc) {
+    using F = QFmt<FMT>;
+    const int g = lane >> F::LOG_G;
+    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
+    // vector entries of the pack, one per lane, pre-multiplied by the part's scale
+    const bool second = lane >= n0;
+    const uint32_t vo = second ? pk.p[1].v_off : pk.p[0].v_off;
+    const float sc = second ? pk.p[1].scale : pk.p[0].scale;
+    const double* v = (vo & VEC_T) ? vt + (vo & ~VEC_T) : vx + vo;
+    const float vl = lane < ntot ? float(__ldg(v + (second ? lane - n0 : lane)) * double(sc)) : 0.f;
+    uint4 m[8];
+    load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m);
+    float s[F::R];
+#pragma unroll
+    for (int r = 0; r < F::R; ++r) s[r] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float vj = __shfl_sync(0xffffffffu, vl, (g + F::C * i) & 31);
+        float f[F::R];
+        unpack16<FMT>(m[i], f);
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) s[r] = fmaf(f[r], vj, s[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < F::R; ++r) acc[r] += double(s[r]);
+}
+
+// sum the C column groups of the accumulators and store rows to red[]
+template <int FMT>
+__device__ __forceinline__ void nflush_q(double* acc, int lane, double* red_row) {
+    using F = QFmt<FMT>;
+#pragma unroll
+    for (int o = F::G; o < 32; o <<= 1)
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+    if ((lane >> F::LOG_G) == 0)
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) red_row[(lane & (F::G - 1)) * F::R + r] = acc[r];
+}
+
+// one storage format per launch: a tile's packs of format FMT
+template <int W, int FMT>
+__global__ void __launch_bounds__(W * 32)
+k_nform_q(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
+          const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
+          int add) {
+    using F = QFmt<FMT>;
+    __shared__ double red[W][TILE];
+    const NSeg sg = segs[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc[F::R];
+#pragma unroll
+    for (int r = 0; r < F::R; ++r) acc[r] = 0.0;
+    uint32_t c = sg.cb + warp;
+    QNPack nxt{};
+    if (c < sg.ce) nxt = ld_pack(packs + c);
+    for (; c < sg.ce; c += W) {
+        const QNPack pk = nxt;
+        if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
+        npack_q<FMT>(pk, A, vx, vt, sg.ld, lane, acc);
+    }
+    nflush_q<FMT>(acc, lane, red[warp]);
+    __syncthreads();
+    if (threadIdx.x < sg.rows) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) s += red[w][threadIdx.x];
+        double* o = out + sg.out + threadIdx.x;
+        if (add) *o += alpha * s;
+        else *o = s;
+    }
+}
+
+// -------------------------------------------------------------- tile T-form
+// x of the lane's R rows
+template <int FMT>
+__device__ __forceinline__ void tx_q(const double* vin, const TTSeg& sg, int lane, float* xr) {
+    using F = QFmt<FMT>;
+    const int l = lane & (F::G - 1);
+#pragma unroll
+    for (int r = 0; r < F::R; ++r) {
+        const int row = l * F::R + r;
+        xr[r] = row < sg.rows ? float(__ldg(vin + sg.v_off + row)) : 0.f;
+    }
+}
+
+template <int FMT>
+__device__ __forceinline__ void ttpack_q(const QTTPack& pk, const uint8_t* A, int ld, int lane, const float* xr,
+                                         double* out, double* part, double alpha, int add) {
+    using F = QFmt<FMT>;
+    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
+    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
+    uint4 m[8];
+    load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m);
+    float p[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float f[F::R];
+        unpack16<FMT>(m[i], f);
+        float s = 0.f;
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) s = fmaf(f[r], xr[r], s);
+        p[i] = s;
+    }
+    // reduce the 8 column partials over the G lanes of the group; afterwards
+    // the lane holds pack column g + C * (l >> (LOG_G - 3))
+    TransposeReduce<8, F::G / 2, float>::run(p, lane);
+    constexpr int SH = F::LOG_G - 3;
+    const int j = g + F::C * (l >> SH);
+    if ((l & ((1 << SH) - 1)) == 0 && j < ntot) {
+        const QTTChunk& q = j < n0 ? pk.p[0] : pk.p[1];
+        const int jj = j < n0 ? j : j - n0;
+        const double val = double(q.scale) * double(p[0]);
+        if (q.flags & TT_DIRECT) {
+            double* o = out + q.out + jj;
+            if (add) *o += alpha * val;
+            else *o = val;
+        } else {
+            part[q.out + jj] = val;
+        }
+    }
+}
+
+template <int W, int FMT>
+__global__ void __launch_bounds__(W * 32)
+k_ttform_q(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, const uint8_t* __restrict__ A,
+           const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
+           int add) {
+    using F = QFmt<FMT>;
+    const TTSeg sg = segs[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float xr[F::R];
+    tx_q<FMT>(vin, sg, lane, xr);
+    uint32_t c = sg.cb + warp;
+    QTTPack nxt{};
+    if (c < sg.ce) nxt = ld_pack(packs + c);
+    for (; c < sg.ce; c += W) {
+        const QTTPack pk = nxt;
+        if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
+        ttpack_q<FMT>(pk, A, sg.ld, lane, xr, out, part, alpha, add);
+    }
+}
+
+}  // namespace hlrc

@@ -101,4 +101,46 @@ struct TTSeg {
 };
 static_assert(sizeof(TTSeg) == 16, "TTSeg must be 16 bytes");
 
+// ------------------------------------------------------ reduced precision
+// Storage formats of a chunk.  Scaled formats store value / scale; the
+// scale (one FP32 per chunk = per block, tile and <= 8 columns) is folded
+// into the chunk's partial sum.
+enum StoreFmt : uint8_t {
+    FMT_F64 = 0,
+    FMT_F32 = 1,
+    FMT_F16 = 2,     // IEEE binary16, scaled
+    FMT_BF16 = 3,    // bfloat16, scaled
+};
+
+inline constexpr int fmt_bytes(int f) { return f == FMT_F64 ? 8 : (f == FMT_F32 ? 4 : 2); }
+
+struct QNChunk {           // N-form chunk of a reduced-precision store
+    uint32_t a16;          // byte offset / 16 of the chunk's first column
+    uint32_t v_off;        // vector offset (| VEC_T)
+    float scale;
+    uint16_t nc;
+    uint8_t fmt;
+    uint8_t pad;
+};
+static_assert(sizeof(QNChunk) == 16, "QNChunk must be 16 bytes");
+
+struct QTTChunk {          // tile T-form chunk of a reduced-precision store
+    uint32_t a16;
+    uint32_t out;          // DIRECT: output offset; else partial offset
+    float scale;
+    uint16_t nc;
+    uint8_t fmt;
+    uint8_t flags;
+};
+static_assert(sizeof(QTTChunk) == 16, "QTTChunk must be 16 bytes");
+
+// Reduced-precision work items: two chunks of one tile and format whose
+// columns together fit the format's 4 KB capacity (16 FP32 / 32 16-bit
+// columns), processed as one (second part empty when nc == 0).  Low-rank
+// blocks split into FP32 and FP16 column runs would otherwise fill chunks
+// only about half.
+struct QNPack { QNChunk p[2]; };
+struct QTTPack { QTTChunk p[2]; };
+static_assert(sizeof(QNPack) == 32 && sizeof(QTTPack) == 32, "packs must be 32 bytes");
+
 }  // namespace hlrc

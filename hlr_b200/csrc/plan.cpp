@@ -1,6 +1,6 @@
 // Flattening of H-matrix / uniform-H descriptors into the slab layout and
-// the N-form / T-form work lists (layout.hpp).  Runs once per matrix on the
-// host; the result is uploaded as one device arena.
+// the N-form / tile-T-form work lists (layout.hpp).  Runs once per matrix on
+// the host; the result is uploaded as one device arena.
 #include "plan.hpp"
 
 #include <algorithm>
@@ -18,7 +18,8 @@ namespace {
 
 constexpr int64_t TFORM_TARGET_ELEMS = 8192;  // elements per T-form unit (64 KB FP64)
 
-inline int64_t pad_rows(int64_t r) { return (r + 1) & ~int64_t(1); }  // 16-byte FP64 columns
+inline int64_t pad_rows(int64_t r) { return (r + 1) & ~int64_t(1); }  // lanes own row pairs
+inline int64_t align16(int64_t b) { return (b + 15) & ~int64_t(15); }
 
 struct Tiles {
     std::vector<int64_t> b;  // boundaries, ntiles + 1 entries
@@ -51,34 +52,145 @@ Tiles make_tiles(int64_t n, std::vector<int64_t> cuts) {
     return t;
 }
 
-struct CopyJob {
-    int64_t dst;          // element offset in the store
-    const double* src;    // column-major source
-    int64_t lds, r0, rows, ncols, ld;
+// ---- number formats (round to nearest even), written from the IEEE 754
+// binary16 and bfloat16 definitions
+uint16_t to_bf16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return uint16_t((u >> 16) | ((u & 0xffffu) ? 0x40u : 0u));  // inf / nan
+    const uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7fffu + lsb;
+    return uint16_t(u >> 16);
+}
+
+uint16_t to_f16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    const uint32_t sign = (u >> 16) & 0x8000u;
+    const int32_t exp = int32_t((u >> 23) & 0xff);
+    uint32_t man = u & 0x7fffffu;
+    if (exp == 0xff) return uint16_t(sign | 0x7c00u | (man ? 0x200u : 0u));
+    int32_t e = exp - 127 + 15;
+    if (e >= 0x1f) return uint16_t(sign | 0x7c00u);  // overflow -> inf
+    if (e <= 0) {                                   // subnormal or zero
+        if (e < -10) return uint16_t(sign);
+        man |= 0x800000u;
+        const int shift = 14 - e;                   // 24-bit mantissa -> 10 - (1 - e) bits
+        const uint32_t half = 1u << (shift - 1);
+        uint32_t r = man >> shift;
+        const uint32_t rem = man & ((1u << shift) - 1u);
+        if (rem > half || (rem == half && (r & 1u))) ++r;
+        return uint16_t(sign | r);
+    }
+    uint32_t r = man >> 13;
+    const uint32_t rem = man & 0x1fffu;
+    if (rem > 0x1000u || (rem == 0x1000u && (r & 1u))) {
+        ++r;
+        if (r == 0x400u) { r = 0; ++e; if (e >= 0x1f) return uint16_t(sign | 0x7c00u); }
+    }
+    return uint16_t(sign | (uint32_t(e) << 10) | r);
+}
+
+// ---- store: slabs cut into chunks of one format.  A chunk holds at most
+// 4 KB at full tile height (FP64: 8 columns, FP32: 16, 16-bit: 32) and its
+// columns are padded so that every lane's 16-byte load is aligned: rows are
+// padded to 2 (FP64), 4 (FP32) or 8 (16-bit).
+inline int chunk_cols(int f) { return f == FMT_F64 ? 8 : (f == FMT_F32 ? 16 : 32); }
+inline int64_t pad_fmt(int64_t rows, int f) {
+    const int64_t m = f == FMT_F64 ? 2 : (f == FMT_F32 ? 4 : 8);
+    return (rows + m - 1) / m * m;
+}
+
+struct SChunk {
+    int64_t byte_off;
+    int32_t col0;
+    int16_t nc;
+    uint8_t fmt;
+    float scale;
+};
+
+struct SSlab {
+    const double* src;
+    int64_t lds, r0, rows, ld;   // ld: FP64 padding (FP64 stores); chunks use pad_fmt(rows, fmt)
+    int32_t c0, nch;             // chunks [c0, c0 + nch)
 };
 
 struct Store {
-    std::vector<CopyJob> jobs;
-    int64_t size = 0;
-    int64_t alloc(const double* src, int64_t lds, int64_t r0, int64_t rows, int64_t ncols) {
-        const int64_t ld = pad_rows(rows);
-        const int64_t off = size;
-        size += ld * ncols;
-        jobs.push_back({off, src, lds, r0, rows, ncols, ld});
-        return off;
+    std::vector<SSlab> slabs;
+    std::vector<SChunk> chunks;
+    int64_t bytes = 0;
+    int64_t unpadded[4] = {0, 0, 0, 0};
+
+    // rows [r0, r0+rows) x ncols of a column-major matrix; colfmt (per
+    // column, may be null -> deffmt); chunks do not straddle `cuts`
+    int alloc(const double* src, int64_t lds, int64_t r0, int64_t rows, int64_t ncols, const uint8_t* colfmt,
+              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr) {
+        SSlab s{src, lds, r0, rows, pad_rows(rows), int32_t(chunks.size()), 0};
+        int64_t j = 0;
+        size_t ci = 0;
+        while (j < ncols) {
+            const uint8_t f = colfmt ? colfmt[j] : deffmt;
+            int64_t e = std::min<int64_t>(j + chunk_cols(f), ncols);
+            if (cuts) {
+                while (ci < cuts->size() && (*cuts)[ci] <= j) ++ci;
+                if (ci < cuts->size()) e = std::min<int64_t>(e, (*cuts)[ci]);
+            }
+            for (int64_t c = j + 1; c < e; ++c)
+                if ((colfmt ? colfmt[c] : deffmt) != f) { e = c; break; }
+            SChunk ch{align16(bytes), int32_t(j), int16_t(e - j), f, 1.0f};
+            bytes = ch.byte_off + pad_fmt(rows, f) * (e - j) * fmt_bytes(f);
+            unpadded[f] += rows * (e - j) * fmt_bytes(f) + (f >= FMT_F16 ? 4 : 0);
+            chunks.push_back(ch);
+            ++s.nch;
+            j = e;
+        }
+        slabs.push_back(s);
+        return int(slabs.size()) - 1;
     }
-    void fill(std::vector<double>& st) const {
-        st.assign(size_t(size), 0.0);
+
+    void fill(std::vector<uint8_t>& st) {
+        st.assign(size_t(bytes), 0);
         #pragma omp parallel for schedule(dynamic, 64)
-        for (int64_t i = 0; i < int64_t(jobs.size()); ++i) {
-            const CopyJob& j = jobs[size_t(i)];
-            for (int64_t c = 0; c < j.ncols; ++c)
-                std::memcpy(st.data() + j.dst + c * j.ld, j.src + j.r0 + c * j.lds, size_t(j.rows) * sizeof(double));
+        for (int64_t si = 0; si < int64_t(slabs.size()); ++si) {
+            const SSlab& s = slabs[size_t(si)];
+            for (int32_t c = s.c0; c < s.c0 + s.nch; ++c) {
+                SChunk& ch = chunks[size_t(c)];
+                uint8_t* dst = st.data() + ch.byte_off;
+                const double* src = s.src + s.r0 + int64_t(ch.col0) * s.lds;
+                const int64_t ldc = pad_fmt(s.rows, ch.fmt);
+                if (ch.fmt == FMT_F64) {
+                    for (int j = 0; j < ch.nc; ++j)
+                        std::memcpy(dst + size_t(j * ldc) * 8, src + j * s.lds, size_t(s.rows) * 8);
+                } else if (ch.fmt == FMT_F32) {
+                    for (int j = 0; j < ch.nc; ++j) {
+                        float* d = reinterpret_cast<float*>(dst) + j * ldc;
+                        for (int64_t i = 0; i < s.rows; ++i) d[i] = float(src[i + j * s.lds]);
+                    }
+                } else {
+                    // power-of-two scale bringing the chunk's largest entry to [2^14, 2^15)
+                    double amax = 0;
+                    for (int j = 0; j < ch.nc; ++j)
+                        for (int64_t i = 0; i < s.rows; ++i) amax = std::max(amax, std::fabs(src[i + j * s.lds]));
+                    int ex = 0;
+                    if (amax > 0) std::frexp(amax, &ex);
+                    const double scale = amax > 0 ? std::ldexp(1.0, ex - 15) : 1.0;
+                    ch.scale = float(scale);
+                    const double inv = 1.0 / scale;
+                    for (int j = 0; j < ch.nc; ++j) {
+                        uint16_t* d = reinterpret_cast<uint16_t*>(dst) + j * ldc;
+                        for (int64_t i = 0; i < s.rows; ++i) {
+                            const float v = float(src[i + j * s.lds] * inv);
+                            d[i] = ch.fmt == FMT_F16 ? to_f16(v) : to_bf16(v);
+                        }
+                    }
+                }
+            }
         }
     }
+    int64_t slab_elem_off(int id) const {  // FP64 stores only: element offset of column 0
+        return chunks[size_t(slabs[size_t(id)].c0)].byte_off / 8;
+    }
 };
-
-inline int tclass(int nc) { return nc <= 8 ? 0 : (nc <= 16 ? 1 : 2); }
 
 struct TBuilder {
     TPass& P;
@@ -105,15 +217,14 @@ struct TBuilder {
             }
             if (sb != uint32_t(P.slabs.size()) || runs.empty()) runs.push_back({sb, uint32_t(P.slabs.size())});
             if (runs.size() == 1) {
-                TUnit u{runs[0].first, runs[0].second, uint32_t(out + c0), 0, uint8_t(nc), TU_DIRECT};
-                u.c0 = uint16_t(c0);
-                tmp[tclass(nc)].push_back({cost(u), u});
+                TUnit u{runs[0].first, runs[0].second, uint32_t(out + c0), uint16_t(c0), uint8_t(nc), TU_DIRECT};
+                tmp[0].push_back({cost(u), u});
             } else {
                 TGroup g{P.nslots, uint32_t(runs.size()), uint32_t(out + c0), uint32_t(nc)};
                 P.groups.push_back(g);
                 for (auto& r : runs) {
                     TUnit u{r.first, r.second, P.nslots++, uint16_t(c0), uint8_t(nc), 0};
-                    tmp[tclass(nc)].push_back({cost(u), u});
+                    tmp[0].push_back({cost(u), u});
                 }
             }
         }
@@ -138,59 +249,104 @@ struct TBuilder {
     }
 };
 
+// Reorders the reduced-precision chunks [s, e) of one tile and format into
+// packs: the widest chunk is paired with the narrowest one that fits next to
+// it in the format's capacity, repeatedly; the second part of a pair is
+// flagged GC_PACK2 and follows its first part.
+void pack_chunks(std::vector<GChunk>& ch, uint32_t s, uint32_t e) {
+    if (e - s < 2 || ch[s].fmt == FMT_F64) return;
+    const int cap = chunk_cols(ch[s].fmt);
+    std::vector<GChunk> g(ch.begin() + s, ch.begin() + e);
+    std::stable_sort(g.begin(), g.end(), [](const GChunk& a, const GChunk& b) { return a.nc > b.nc; });
+    std::vector<GChunk> out;
+    out.reserve(g.size());
+    size_t i = 0, k = g.size();
+    while (i < k) {
+        out.push_back(g[i]);
+        if (k - 1 > i && g[i].nc + g[k - 1].nc <= cap) {
+            GChunk second = g[k - 1];
+            second.flags |= GC_PACK2;
+            out.push_back(second);
+            --k;
+        }
+        ++i;
+    }
+    std::copy(out.begin(), out.end(), ch.begin() + s);
+}
+
+// N-form pass: one segment per output tile; the chunks of every slab that
+// covers the tile.
 struct NBuilder {
     NPass& P;
-    std::vector<std::pair<int64_t, NSeg>> tmp;
-    explicit NBuilder(NPass& p) : P(p) {}
+    const Store& S;
+    NBuilder(NPass& p, const Store& s) : P(p), S(s) {}
+    std::vector<std::pair<int64_t, NSeg>> tmp[4];
     uint32_t cb = 0;
-    int64_t elems = 0, rows = 0, alg = 0;
-    void begin(int64_t tile_rows) { cb = uint32_t(P.chunks.size()); elems = 0; rows = tile_rows; alg = 0; }
-    void slab(int64_t off, int64_t ld, int64_t ncols, uint32_t vbase) {
-        for (int64_t j0 = 0; j0 < ncols; j0 += NCHUNK) {
-            const int nc = int(std::min<int64_t>(NCHUNK, ncols - j0));
-            NChunk c{uint64_t(off + j0 * ld), uint32_t(vbase + uint32_t(j0)), uint16_t(nc), 0};
-            P.chunks.push_back(c);
-            elems += ld * nc;
+    int64_t bytes = 0, rows = 0, alg = 0;
+    void begin(int64_t tile_rows) { cb = uint32_t(P.chunks.size()); bytes = 0; rows = tile_rows; alg = 0; }
+    void slab(int id, uint32_t vbase) {
+        const SSlab& s = S.slabs[size_t(id)];
+        for (int32_t c = s.c0; c < s.c0 + s.nch; ++c) {
+            const SChunk& ch = S.chunks[size_t(c)];
+            P.chunks.push_back({uint64_t(ch.byte_off), uint32_t(vbase + uint32_t(ch.col0)), uint16_t(ch.nc), ch.fmt, 0,
+                                ch.scale});
+            bytes += pad_fmt(s.rows, ch.fmt) * ch.nc * fmt_bytes(ch.fmt);
+            alg += int64_t(ch.nc) * (rows * fmt_bytes(ch.fmt) + 8);
         }
-        alg += int64_t(sizeof(double)) * ncols * (rows + 1);
     }
+    // one segment per storage format present in the tile (OUT_SET passes,
+    // which overwrite, are single-format: uniform-H is FP64 only)
     void end(uint32_t out, int64_t rows_, bool keep_empty) {
         const uint32_t ce = uint32_t(P.chunks.size());
         if (ce == cb && !keep_empty) return;
-        NSeg s{cb, ce, out, uint16_t(rows_), uint16_t(pad_rows(rows_))};
-        tmp.push_back({elems, s});
+        std::stable_sort(P.chunks.begin() + cb, P.chunks.end(),
+                         [](const GChunk& a, const GChunk& b) { return a.fmt < b.fmt; });
+        if (ce == cb) tmp[FMT_F64].push_back({0, NSeg{cb, ce, out, uint16_t(rows_), uint16_t(pad_rows(rows_))}});
+        for (uint32_t s = cb; s < ce;) {
+            const uint8_t f = P.chunks[s].fmt;
+            uint32_t e = s;
+            int64_t by = 0;
+            for (; e < ce && P.chunks[e].fmt == f; ++e) by += pad_fmt(rows_, f) * P.chunks[e].nc * fmt_bytes(f);
+            pack_chunks(P.chunks, s, e);
+            tmp[f].push_back({by, NSeg{s, e, out, uint16_t(rows_), uint16_t(pad_fmt(rows_, f))}});
+            s = e;
+        }
         P.alg_bytes += alg + int64_t(sizeof(double)) * rows_ * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
     }
     void finish() {
-        std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-        P.segs.clear();
-        for (auto& e : tmp) {
-            P.segs.push_back(e.second);
-            P.bytes += e.first * int64_t(sizeof(double));
+        for (int f = 0; f < 4; ++f) {
+            std::stable_sort(tmp[f].begin(), tmp[f].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            P.segs[f].clear();
+            for (auto& e : tmp[f]) {
+                P.segs[f].push_back(e.second);
+                P.bytes += e.first;
+            }
         }
     }
 };
 
-// Tile T-form pass: objects (low-rank blocks / cluster bases) own an output
-// of `ncols` coefficients and are cut into slabs by input tiles.  Objects on
-// one tile write their chunks' results directly; objects on several tiles
-// write per-tile partials that a finish pass sums in tile order.
+// Tile T-form pass: objects (low-rank blocks / cluster bases / column tiles
+// of the near field) own an output of `ncols` values and receive one slab per
+// input tile.  Objects fed by one slab write their chunks' results directly;
+// objects fed by several write per-slab partials that a finish pass sums in
+// slab order.
 struct TTBuilder {
     TTPass& P;
-    std::vector<std::pair<int64_t, TTSeg>> tmp;
+    const Store& S;
+    std::vector<std::pair<int64_t, TTSeg>> tmp[4];
     std::vector<int64_t> pbase, ncol;
     std::vector<uint32_t> oout;
     uint32_t cb = 0, voff = 0;
-    int64_t elems = 0, rows = 0;
-    TTBuilder(TTPass& p, size_t nobj) : P(p), pbase(nobj, -2), ncol(nobj, 0), oout(nobj, 0) {}
+    int64_t bytes = 0, rows = 0;
+    TTBuilder(TTPass& p, const Store& s, size_t nobj) : P(p), S(s), pbase(nobj, -2), ncol(nobj, 0), oout(nobj, 0) {}
 
-    void object(size_t id, uint32_t out, int64_t ncols, int64_t ntiles) {
+    void object(size_t id, uint32_t out, int64_t ncols, int64_t nslabs) {
         ncol[id] = ncols;
         oout[id] = out;
-        if (ntiles > 1) {
+        if (nslabs > 1) {
             pbase[id] = P.npart;
-            P.groups.push_back({uint32_t(P.npart), uint32_t(ntiles), out, uint32_t(ncols)});
-            P.npart += ntiles * ncols;
+            P.groups.push_back({uint32_t(P.npart), uint32_t(nslabs), out, uint32_t(ncols)});
+            P.npart += nslabs * ncols;
         } else {
             pbase[id] = -1;
         }
@@ -200,39 +356,124 @@ struct TTBuilder {
         cb = uint32_t(P.chunks.size());
         voff = uint32_t(v_off);
         rows = tile_rows;
-        elems = 0;
+        bytes = 0;
     }
-    void slab(int64_t off, int64_t ld, size_t id, int64_t tile_idx) {
-        const int64_t k = ncol[id];
-        for (int64_t j0 = 0; j0 < k; j0 += TCOLS) {
-            const int nc = int(std::min<int64_t>(TCOLS, k - j0));
-            TTChunk c;
-            c.a_off = uint64_t(off + j0 * ld);
-            c.nc = uint16_t(nc);
-            if (pbase[id] < 0) { c.out = uint32_t(oout[id] + j0); c.flags = TT_DIRECT; }
-            else { c.out = uint32_t(pbase[id] + tile_idx * k + j0); c.flags = 0; }
-            P.chunks.push_back(c);
-            elems += ld * nc;
+    // columns [lo, lo + ncol[id]) of slab `sid` feed object `id` as its slab number `k`
+    void slab(int sid, size_t id, int64_t k, int64_t lo = 0) {
+        const SSlab& s = S.slabs[size_t(sid)];
+        const int64_t hi = lo + ncol[id];
+        for (int32_t c = s.c0; c < s.c0 + s.nch; ++c) {
+            const SChunk& ch = S.chunks[size_t(c)];
+            if (ch.col0 < lo || ch.col0 >= hi) continue;
+            const int64_t j = ch.col0 - lo;
+            GChunk g{uint64_t(ch.byte_off), 0, uint16_t(ch.nc), ch.fmt, 0, ch.scale};
+            if (pbase[id] < 0) { g.vo = uint32_t(oout[id] + j); g.flags = TT_DIRECT; }
+            else g.vo = uint32_t(pbase[id] + k * ncol[id] + j);
+            P.chunks.push_back(g);
+            bytes += pad_fmt(s.rows, ch.fmt) * ch.nc * fmt_bytes(ch.fmt);
+            P.alg_bytes += rows * ch.nc * fmt_bytes(ch.fmt);
         }
-        P.alg_bytes += int64_t(sizeof(double)) * rows * k;
     }
     void end() {
         const uint32_t ce = uint32_t(P.chunks.size());
         if (ce == cb) return;
-        tmp.push_back({elems, TTSeg{cb, ce, voff, uint16_t(rows), uint16_t(pad_rows(rows))}});
+        std::stable_sort(P.chunks.begin() + cb, P.chunks.end(),
+                         [](const GChunk& a, const GChunk& b) { return a.fmt < b.fmt; });
+        for (uint32_t s = cb; s < ce;) {
+            const uint8_t f = P.chunks[s].fmt;
+            uint32_t e = s;
+            int64_t by = 0;
+            for (; e < ce && P.chunks[e].fmt == f; ++e) by += pad_fmt(rows, f) * P.chunks[e].nc * fmt_bytes(f);
+            pack_chunks(P.chunks, s, e);
+            tmp[f].push_back({by, TTSeg{s, e, voff, uint16_t(rows), uint16_t(pad_fmt(rows, f))}});
+            s = e;
+        }
         P.alg_bytes += int64_t(sizeof(double)) * rows;
     }
     void finish() {
-        std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-        P.segs.clear();
-        for (auto& e : tmp) {
-            P.segs.push_back(e.second);
-            P.bytes += e.first * int64_t(sizeof(double));
+        for (int f = 0; f < 4; ++f) {
+            std::stable_sort(tmp[f].begin(), tmp[f].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            P.segs[f].clear();
+            for (auto& e : tmp[f]) {
+                P.segs[f].push_back(e.second);
+                P.bytes += e.first;
+            }
         }
     }
 };
 
 inline double flops_gemv(double m, double n) { return 2.0 * m * n + 2.0 * m; }
+
+// Transposed near field y_sigma += alpha sum D^T x as a tile T-form pass:
+// CTAs run over row tiles, objects are the column tiles, and every (dense
+// block, row tile) slab that covers a column tile is one of its inputs.
+template <typename DenseOf>
+void plan_dense_transposed(TTPass& P, const Store& st, const Tiles& tr, const Tiles& tc,
+                           const std::vector<std::vector<int64_t>>& dense_by_rowtile,
+                           const std::vector<std::vector<int>>& dslab, DenseOf dense) {
+    P.in = V_X; P.out = V_Y; P.mode = OUT_ADD_ALPHA;
+    TTBuilder tb(P, st, size_t(tc.n()));
+    std::vector<int64_t> cnt(size_t(tc.n()), 0);
+    for (int64_t t = 0; t < tr.n(); ++t)
+        for (int64_t i : dense_by_rowtile[size_t(t)]) {
+            int64_t col0, ncols;
+            dense(i, col0, ncols);
+            for (int64_t s = tc.first(col0); s < tc.first(col0 + ncols); ++s) ++cnt[size_t(s)];
+        }
+    for (int64_t s = 0; s < tc.n(); ++s)
+        if (cnt[size_t(s)] > 0) tb.object(size_t(s), uint32_t(tc.lo(s)), tc.size(s), cnt[size_t(s)]);
+    std::vector<int64_t> k(size_t(tc.n()), 0);
+    std::vector<size_t> pos(dslab.size(), 0);
+    for (int64_t t = 0; t < tr.n(); ++t) {
+        tb.begin(tr.lo(t), tr.size(t));
+        for (int64_t i : dense_by_rowtile[size_t(t)]) {
+            int64_t col0, ncols;
+            dense(i, col0, ncols);
+            const int sid = dslab[size_t(i)][pos[size_t(i)]++];
+            for (int64_t s = tc.first(col0); s < tc.first(col0 + ncols); ++s)
+                tb.slab(sid, size_t(s), k[size_t(s)]++, tc.lo(s) - col0);
+        }
+        tb.end();
+    }
+    tb.finish();
+}
+
+// column tile boundaries inside [col0, col0+ncols), relative to col0
+std::vector<int64_t> inner_cuts(const Tiles& tc, int64_t col0, int64_t ncols) {
+    std::vector<int64_t> c;
+    for (int64_t s = tc.first(col0) + 1; s < tc.first(col0 + ncols); ++s) c.push_back(tc.lo(s) - col0);
+    return c;
+}
+
+// VALR column precisions (compress/valr.hh:402-510): delta = eps sigma_0,
+// tol from  Sigma_l 1/sigma_l tol^2 - tol + delta = 0 (smaller root),
+// u_l = tol / sigma_l; a column may use the cheapest format whose unit
+// roundoff is <= u_l.
+void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt) {
+    if (k <= 0) return;
+    const double delta = eps * sv[0];
+    double sum = 0;
+    for (int64_t l = 0; l < k; ++l) sum += sv[l] > 0 ? 1.0 / sv[l] : 0.0;
+    double tol = delta;
+    if (sum > 0) {
+        const double p = 1.0 / sum, q = delta / sum;
+        const double t = std::max(0.0, p * p / 4 - q);
+        tol = std::min(std::fabs(p / 2 + std::sqrt(t)), std::fabs(p / 2 - std::sqrt(t)));
+    }
+    for (int64_t l = 0; l < k; ++l) {
+        const double u = sv[l] > 0 ? tol / sv[l] : 1.0;
+        fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : (u >= 0x1.0p-24 ? FMT_F32 : FMT_F64);
+    }
+}
+
+uint8_t default_format(int prec) {
+    switch (prec) {
+        case HLRC_PREC_F32: return FMT_F32;
+        case HLRC_PREC_BF16: return FMT_BF16;
+        case HLRC_PREC_F16: return FMT_F16;
+        default: return FMT_F64;
+    }
+}
 
 }  // namespace
 
@@ -242,8 +483,10 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
         return fail(HLRC_ERR_SHAPE, "matrix dimension exceeds 2^31-1");
-    if (o.precision != HLRC_PREC_F64)
-        return fail(HLRC_ERR_ARG, "precision %d not supported by this planner", o.precision);
+    if (o.precision < HLRC_PREC_F64 || o.precision > HLRC_PREC_MIXED)
+        return fail(HLRC_ERR_ARG, "unknown precision %d", o.precision);
+    if (o.precision == HLRC_PREC_MIXED && !(o.mixed_eps > 0))
+        return fail(HLRC_ERR_ARG, "HLRC_PREC_MIXED needs mixed_eps > 0");
     p = Plan();
     p.kind = 0;
     p.precision = o.precision;
@@ -282,166 +525,186 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
     p.n_col_tiles = tc.n();
 
     // coefficient offsets and per-tile block lists (block order preserved)
-    std::vector<int64_t> toff(size_t(nb), -1);
+    std::vector<int64_t> toff(static_cast<size_t>(nb), -1);
     int64_t nt = 0;
-    std::vector<std::vector<int64_t>> rowlist(size_t(tr.n())), collist(size_t(tc.n()));
+    std::vector<std::vector<int64_t>> rowlist(static_cast<size_t>(tr.n())), collist(static_cast<size_t>(tc.n())),
+        dense_rows(static_cast<size_t>(tr.n()));
     for (int64_t i = 0; i < nb; ++i) {
         const hlrc_block& b = d.blocks[i];
         if (b.nrows == 0 || b.ncols == 0) continue;
         const bool lr = b.kind == HLRC_LEAF_LOWRANK;
         if (lr && b.rank == 0) continue;
-        if (lr) { toff[i] = nt; nt += b.rank; }
-        for (int64_t t = tr.first(b.row0); t < tr.first(b.row0 + b.nrows); ++t) rowlist[size_t(t)].push_back(i);
+        if (lr) { toff[size_t(i)] = nt; nt += b.rank; }
+        for (int64_t t = tr.first(b.row0); t < tr.first(b.row0 + b.nrows); ++t) {
+            rowlist[size_t(t)].push_back(i);
+            if (!lr) dense_rows[size_t(t)].push_back(i);
+        }
         for (int64_t t = tc.first(b.col0); t < tc.first(b.col0 + b.ncols); ++t) collist[size_t(t)].push_back(i);
     }
     if (nt >= (int64_t(1) << 31)) return fail(HLRC_ERR_SHAPE, "sum of ranks exceeds 2^31-1");
     p.n_t = nt;
 
-    // storage: row region (per row tile: D and U slabs), then V region
+    // storage formats
+    const uint8_t deffmt = default_format(o.precision);
+    const uint8_t densefmt = o.precision == HLRC_PREC_MIXED ? uint8_t(FMT_F32) : deffmt;
+    std::vector<std::vector<uint8_t>> colfmt(static_cast<size_t>(nb));
+    if (o.precision == HLRC_PREC_MIXED) {
+        for (int64_t i = 0; i < nb; ++i) {
+            const hlrc_block& b = d.blocks[i];
+            if (toff[size_t(i)] < 0) continue;
+            std::vector<double> sv(static_cast<size_t>(b.rank));
+            for (int64_t l = 0; l < b.rank; ++l) {
+                if (b.sv) { sv[size_t(l)] = b.sv[l]; continue; }
+                double nu = 0, nv = 0;
+                for (int64_t r = 0; r < b.nrows; ++r) nu += b.U[r + l * b.ldu] * b.U[r + l * b.ldu];
+                for (int64_t r = 0; r < b.ncols; ++r) nv += b.V[r + l * b.ldv] * b.V[r + l * b.ldv];
+                sv[size_t(l)] = std::sqrt(nu * nv);
+            }
+            // VALR expects descending singular values; sort a copy for the
+            // tolerance and map formats back to the stored column order
+            std::vector<int64_t> ord(static_cast<size_t>(b.rank));
+            std::iota(ord.begin(), ord.end(), 0);
+            std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t c) { return sv[size_t(a)] > sv[size_t(c)]; });
+            std::vector<double> svs(static_cast<size_t>(b.rank));
+            for (int64_t l = 0; l < b.rank; ++l) svs[size_t(l)] = sv[size_t(ord[size_t(l)])];
+            std::vector<uint8_t> fs(static_cast<size_t>(b.rank));
+            valr_formats(svs.data(), b.rank, o.mixed_eps, fs.data());
+            colfmt[size_t(i)].assign(static_cast<size_t>(b.rank), FMT_F32);
+            for (int64_t l = 0; l < b.rank; ++l) colfmt[size_t(i)][size_t(ord[size_t(l)])] = fs[size_t(l)];
+        }
+    }
+    auto cf = [&](int64_t i) -> const uint8_t* { return colfmt[size_t(i)].empty() ? nullptr : colfmt[size_t(i)].data(); };
+
+    // storage: row region (per row tile: D and U slabs), then the V region
+    // ordered by column tile, so that each pass streams one contiguous
+    // range per tile
     Store st;
-    std::vector<std::vector<int64_t>> slabA(static_cast<size_t>(nb)), slabV(static_cast<size_t>(nb));  // A = D or U, by row tile
+    std::vector<std::vector<int>> slabA(static_cast<size_t>(nb)), slabV(static_cast<size_t>(nb));
     for (int64_t t = 0; t < tr.n(); ++t) {
         for (int64_t i : rowlist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
             const int64_t r0 = tr.lo(t) - b.row0, rows = tr.size(t);
-            if (b.kind == HLRC_LEAF_DENSE) slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols));
-            else slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank));
+            if (b.kind == HLRC_LEAF_DENSE) {
+                const std::vector<int64_t> cuts = inner_cuts(tc, b.col0, b.ncols);
+                slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols, nullptr, densefmt, &cuts));
+            } else {
+                slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank, cf(i), deffmt));
+            }
         }
     }
-    // V slabs ordered by column tile, so that stage A of op N streams one
-    // contiguous region per tile
     for (int64_t t = 0; t < tc.n(); ++t)
         for (int64_t i : collist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
             if (b.kind != HLRC_LEAF_LOWRANK) continue;
-            slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank));
+            slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank, cf(i), deffmt));
         }
+    if (st.bytes >= (int64_t(1) << 36) && o.precision != HLRC_PREC_F64)
+        return fail(HLRC_ERR_SHAPE, "reduced-precision store above 64 GiB");
     st.fill(p.store);
+    for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
-    // op N: tile T-form V^T x -> t (per column tile), then N-form per row tile: U t + D x -> y
-    p.tpasses.resize(1);
     p.npasses.resize(2);
-    p.ttpasses.resize(2);
+    p.ttpasses.resize(3);
+    // op N stage A: tile T-form V^T x -> t per column tile
     {
         TTPass& a = p.ttpasses[0];
         a.in = V_X; a.out = V_T; a.mode = OUT_SET;
-        TTBuilder tb(a, size_t(nb));
+        TTBuilder tb(a, st, size_t(nb));
         for (int64_t i = 0; i < nb; ++i)
             if (toff[size_t(i)] >= 0)
                 tb.object(size_t(i), uint32_t(toff[size_t(i)]), d.blocks[i].rank,
                           tc.first(d.blocks[i].col0 + d.blocks[i].ncols) - tc.first(d.blocks[i].col0));
         for (int64_t t = 0; t < tc.n(); ++t) {
             tb.begin(tc.lo(t), tc.size(t));
-            const int64_t ld = pad_rows(tc.size(t));
             for (int64_t i : collist[size_t(t)]) {
                 if (toff[size_t(i)] < 0) continue;
                 const int64_t ti = t - tc.first(d.blocks[i].col0);
-                tb.slab(slabV[size_t(i)][size_t(ti)], ld, size_t(i), ti);
+                tb.slab(slabV[size_t(i)][size_t(ti)], size_t(i), ti);
             }
             tb.end();
         }
         tb.finish();
     }
+    // op N stage B: N-form per row tile, y += alpha (U t + D x)
     {
         NPass& nN = p.npasses[0];
         nN.vx = V_X; nN.vt = V_T; nN.out = V_Y; nN.mode = OUT_ADD_ALPHA;
-        NBuilder nbld(nN);
-        std::vector<size_t> pos(size_t(nb), 0);
+        NBuilder nbld(nN, st);
+        std::vector<size_t> pos(static_cast<size_t>(nb), 0);
         for (int64_t t = 0; t < tr.n(); ++t) {
             nbld.begin(tr.size(t));
-            const int64_t ld = pad_rows(tr.size(t));
             for (int64_t i : rowlist[size_t(t)]) {
                 const hlrc_block& b = d.blocks[i];
-                const int64_t off = slabA[size_t(i)][pos[size_t(i)]++];
-                if (b.kind == HLRC_LEAF_DENSE) nbld.slab(off, ld, b.ncols, uint32_t(b.col0));
-                else nbld.slab(off, ld, b.rank, VEC_T | uint32_t(toff[size_t(i)]));
+                const int sid = slabA[size_t(i)][pos[size_t(i)]++];
+                if (b.kind == HLRC_LEAF_DENSE) nbld.slab(sid, uint32_t(b.col0));
+                else nbld.slab(sid, VEC_T | uint32_t(toff[size_t(i)]));
             }
             nbld.end(uint32_t(tr.lo(t)), tr.size(t), false);
         }
         nbld.finish();
     }
-    // op T: tile T-form U^T x -> t (per row tile); N-form per column tile V t -> y; T-form D^T x -> y
+    // op T stage A: tile T-form U^T x -> t per row tile
     {
         TTPass& a = p.ttpasses[1];
         a.in = V_X; a.out = V_T; a.mode = OUT_SET;
-        TTBuilder tb(a, size_t(nb));
+        TTBuilder tb(a, st, size_t(nb));
         for (int64_t i = 0; i < nb; ++i)
             if (toff[size_t(i)] >= 0)
                 tb.object(size_t(i), uint32_t(toff[size_t(i)]), d.blocks[i].rank,
                           tr.first(d.blocks[i].row0 + d.blocks[i].nrows) - tr.first(d.blocks[i].row0));
         for (int64_t t = 0; t < tr.n(); ++t) {
             tb.begin(tr.lo(t), tr.size(t));
-            const int64_t ld = pad_rows(tr.size(t));
             for (int64_t i : rowlist[size_t(t)]) {
                 if (toff[size_t(i)] < 0) continue;
                 const int64_t ti = t - tr.first(d.blocks[i].row0);
-                tb.slab(slabA[size_t(i)][size_t(ti)], ld, size_t(i), ti);
+                tb.slab(slabA[size_t(i)][size_t(ti)], size_t(i), ti);
             }
             tb.end();
         }
         tb.finish();
     }
+    // op T stage B: N-form per column tile, y += alpha V t
     {
         NPass& nT = p.npasses[1];
         nT.vx = V_X; nT.vt = V_T; nT.out = V_Y; nT.mode = OUT_ADD_ALPHA;
-        NBuilder nbld(nT);
+        NBuilder nbld(nT, st);
         for (int64_t t = 0; t < tc.n(); ++t) {
             nbld.begin(tc.size(t));
-            const int64_t ld = pad_rows(tc.size(t));
             for (int64_t i : collist[size_t(t)]) {
                 const hlrc_block& b = d.blocks[i];
-                if (b.kind != HLRC_LEAF_LOWRANK) continue;
-                const int64_t off = slabV[size_t(i)][size_t(t - tc.first(b.col0))];
-                nbld.slab(off, ld, b.rank, VEC_T | uint32_t(toff[size_t(i)]));
+                if (b.kind != HLRC_LEAF_LOWRANK || toff[size_t(i)] < 0) continue;
+                nbld.slab(slabV[size_t(i)][size_t(t - tc.first(b.col0))], VEC_T | uint32_t(toff[size_t(i)]));
             }
             nbld.end(uint32_t(tc.lo(t)), tc.size(t), false);
         }
         nbld.finish();
     }
-    {
-        TPass& dT = p.tpasses[0];
-        dT.in = V_X; dT.out = V_Y; dT.mode = OUT_ADD_ALPHA;
-        TBuilder tb(dT);
-        for (int64_t t = 0; t < tc.n(); ++t) {
-            std::vector<TSlab> sl;
-            for (int64_t i : collist[size_t(t)]) {
-                const hlrc_block& b = d.blocks[i];
-                if (b.kind != HLRC_LEAF_DENSE) continue;
-                const int64_t r0 = tr.first(b.row0);
-                for (size_t s = 0; s < slabA[size_t(i)].size(); ++s) {
-                    const int64_t rt = r0 + int64_t(s);
-                    const int64_t ld = pad_rows(tr.size(rt));
-                    sl.push_back({uint64_t(slabA[size_t(i)][s] + (tc.lo(t) - b.col0) * ld), uint32_t(tr.lo(rt)),
-                                  uint16_t(tr.size(rt)), uint16_t(ld)});
-                }
-            }
-            if (!sl.empty()) tb.add(uint32_t(tc.lo(t)), tc.size(t), sl);
-        }
-        tb.finish();
-    }
+    // op T near field: y += alpha D^T x
+    plan_dense_transposed(p.ttpasses[2], st, tr, tc, dense_rows, slabA, [&](int64_t i, int64_t& c0, int64_t& nc) {
+        c0 = d.blocks[i].col0;
+        nc = d.blocks[i].ncols;
+    });
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}};
-    p.stages[HLRC_OP_T] = {{2, 1}, {1, 1}, {0, 0}};
+    p.stages[HLRC_OP_T] = {{2, 1}, {1, 1}, {2, 2}};
     p.stages[HLRC_OP_C] = p.stages[HLRC_OP_T];
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
 
     // accounting (arith/mulvec.hh:795-874)
-    double flops = 0, mbytes = 0;
+    double flops = 0;
     for (int64_t i = 0; i < nb; ++i) {
         const hlrc_block& b = d.blocks[i];
         if (b.kind == HLRC_LEAF_DENSE) {
             ++p.n_dense;
             flops += flops_gemv(double(b.nrows), double(b.ncols));
-            mbytes += 8.0 * double(b.nrows) * double(b.ncols);
         } else {
             ++p.n_lowrank;
             flops += flops_gemv(double(b.ncols), b.rank) + flops_gemv(double(b.nrows), b.rank);
-            mbytes += 8.0 * double(b.rank) * double(b.nrows + b.ncols);
             p.max_rank = std::max(p.max_rank, b.rank);
         }
     }
-    p.matrix_bytes = int64_t(mbytes);
-    p.algorithmic_bytes = int64_t(mbytes) + 2 * 8 * (d.nrows + d.ncols);
+    p.matrix_bytes = st.unpadded[0] + st.unpadded[1] + st.unpadded[2] + st.unpadded[3];
+    p.algorithmic_bytes = p.matrix_bytes + 2 * 8 * (d.nrows + d.ncols);
     p.flops = int64_t(flops);
     return HLRC_OK;
 }
@@ -455,7 +718,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
         return fail(HLRC_ERR_SHAPE, "matrix dimension exceeds 2^31-1");
     if (o.precision != HLRC_PREC_F64)
-        return fail(HLRC_ERR_ARG, "precision %d not supported for uniform-H", o.precision);
+        return fail(HLRC_ERR_ARG, "precision %d not supported for uniform-H (FP64 only)", o.precision);
     p = Plan();
     p.kind = 1;
     p.precision = o.precision;
@@ -505,7 +768,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     p.n_row_tiles = tr.n();
     p.n_col_tiles = tc.n();
 
-    std::vector<int64_t> rboff(size_t(nrb), -1), cboff(size_t(ncb), -1);
+    std::vector<int64_t> rboff(static_cast<size_t>(nrb), -1), cboff(static_cast<size_t>(ncb), -1);
     int64_t nkr = 0, nkc = 0;
     for (int64_t i = 0; i < nrb; ++i)
         if (d.row_bases[i].rank > 0 && d.row_bases[i].size > 0) { rboff[size_t(i)] = nkr; nkr += d.row_bases[i].rank; }
@@ -516,7 +779,8 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     p.n_t2 = std::max(nkr, nkc);
 
     // tile -> bases / dense blocks covering it
-    std::vector<std::vector<int64_t>> rbl(size_t(tr.n())), cbl(size_t(tc.n())), rdl(size_t(tr.n())), cdl(size_t(tc.n()));
+    std::vector<std::vector<int64_t>> rbl(static_cast<size_t>(tr.n())), cbl(static_cast<size_t>(tc.n())),
+        rdl(static_cast<size_t>(tr.n()));
     for (int64_t i = 0; i < nrb; ++i)
         if (rboff[size_t(i)] >= 0)
             for (int64_t t = tr.first(d.row_bases[i].ofs); t < tr.first(d.row_bases[i].ofs + d.row_bases[i].size); ++t)
@@ -531,7 +795,6 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         if (b.nrows == 0 || b.ncols == 0) continue;
         if (b.kind == HLRC_LEAF_DENSE) {
             for (int64_t t = tr.first(b.row0); t < tr.first(b.row0 + b.nrows); ++t) rdl[size_t(t)].push_back(i);
-            for (int64_t t = tc.first(b.col0); t < tc.first(b.col0 + b.ncols); ++t) cdl[size_t(t)].push_back(i);
         } else {
             if (rboff[size_t(b.row_basis)] < 0 || cboff[size_t(b.col_basis)] < 0) continue;
             lr_by_row[size_t(b.row_basis)].push_back(i);
@@ -540,21 +803,23 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     }
 
     Store st;
-    std::vector<std::vector<int64_t>> sRB(static_cast<size_t>(nrb)), sCB(static_cast<size_t>(ncb)), sD(static_cast<size_t>(nb)), sS(static_cast<size_t>(nb));
+    std::vector<std::vector<int>> sRB(static_cast<size_t>(nrb)), sCB(static_cast<size_t>(ncb)), sD(static_cast<size_t>(nb)),
+        sS(static_cast<size_t>(nb));
     for (int64_t t = 0; t < tr.n(); ++t) {
         for (int64_t i : rbl[size_t(t)]) {
             const hlrc_basis& b = d.row_bases[i];
-            sRB[size_t(i)].push_back(st.alloc(b.V, b.ldv, tr.lo(t) - b.ofs, tr.size(t), b.rank));
+            sRB[size_t(i)].push_back(st.alloc(b.V, b.ldv, tr.lo(t) - b.ofs, tr.size(t), b.rank, nullptr, FMT_F64));
         }
         for (int64_t i : rdl[size_t(t)]) {
             const hlrc_uniform_block& b = d.blocks[i];
-            sD[size_t(i)].push_back(st.alloc(b.D, b.ldd, tr.lo(t) - b.row0, tr.size(t), b.ncols));
+            const std::vector<int64_t> cuts = inner_cuts(tc, b.col0, b.ncols);
+            sD[size_t(i)].push_back(st.alloc(b.D, b.ldd, tr.lo(t) - b.row0, tr.size(t), b.ncols, nullptr, FMT_F64, &cuts));
         }
     }
-    for (int64_t t = 0; t < tc.n(); ++t)   // column bases by column tile
+    for (int64_t t = 0; t < tc.n(); ++t)  // column bases by column tile
         for (int64_t i : cbl[size_t(t)]) {
             const hlrc_basis& b = d.col_bases[i];
-            sCB[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.ofs, tc.size(t), b.rank));
+            sCB[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.ofs, tc.size(t), b.rank, nullptr, FMT_F64));
         }
     for (int64_t i = 0; i < nb; ++i) {
         const hlrc_uniform_block& b = d.blocks[i];
@@ -562,28 +827,28 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         if (rboff[size_t(b.row_basis)] < 0 || cboff[size_t(b.col_basis)] < 0) continue;
         const int64_t kr = d.row_bases[b.row_basis].rank, kc = d.col_bases[b.col_basis].rank;
         for (int64_t r0 = 0; r0 < kr; r0 += TILE)
-            sS[size_t(i)].push_back(st.alloc(b.S, b.lds, r0, std::min<int64_t>(TILE, kr - r0), kc));
+            sS[size_t(i)].push_back(st.alloc(b.S, b.lds, r0, std::min<int64_t>(TILE, kr - r0), kc, nullptr, FMT_F64));
     }
     st.fill(p.store);
+    for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
-    p.tpasses.resize(4);
+    p.tpasses.resize(1);
     p.npasses.resize(3);
-    p.ttpasses.resize(2);
+    p.ttpasses.resize(3);
     // ---- op N
     {   // forward: ux_s = V_s^T x, per column tile over all bases containing it
         TTPass& f = p.ttpasses[0];
         f.in = V_X; f.out = V_T; f.mode = OUT_SET;
-        TTBuilder tb(f, size_t(ncb));
+        TTBuilder tb(f, st, size_t(ncb));
         for (int64_t i = 0; i < ncb; ++i)
             if (cboff[size_t(i)] >= 0)
                 tb.object(size_t(i), uint32_t(cboff[size_t(i)]), d.col_bases[i].rank,
                           tc.first(d.col_bases[i].ofs + d.col_bases[i].size) - tc.first(d.col_bases[i].ofs));
         for (int64_t t = 0; t < tc.n(); ++t) {
             tb.begin(tc.lo(t), tc.size(t));
-            const int64_t ld = pad_rows(tc.size(t));
             for (int64_t i : cbl[size_t(t)]) {
                 const int64_t ti = t - tc.first(d.col_bases[i].ofs);
-                tb.slab(sCB[size_t(i)][size_t(ti)], ld, size_t(i), ti);
+                tb.slab(sCB[size_t(i)][size_t(ti)], size_t(i), ti);
             }
             tb.end();
         }
@@ -592,17 +857,16 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     {   // coupling: uy_t = sum_s S_ts ux_s
         NPass& c = p.npasses[0];
         c.vx = V_X; c.vt = V_T; c.out = V_T2; c.mode = OUT_SET;
-        NBuilder nbld(c);
+        NBuilder nbld(c, st);
         for (int64_t t = 0; t < nrb; ++t) {
             if (rboff[size_t(t)] < 0) continue;
             const int64_t kr = d.row_bases[t].rank;
             for (int64_t r0 = 0, piece = 0; r0 < kr; r0 += TILE, ++piece) {
-                nbld.begin(std::min<int64_t>(TILE, kr - r0));
                 const int64_t rows = std::min<int64_t>(TILE, kr - r0);
+                nbld.begin(rows);
                 for (int64_t i : lr_by_row[size_t(t)]) {
                     const hlrc_uniform_block& b = d.blocks[i];
-                    nbld.slab(sS[size_t(i)][size_t(piece)], pad_rows(rows), d.col_bases[b.col_basis].rank,
-                              VEC_T | uint32_t(cboff[size_t(b.col_basis)]));
+                    nbld.slab(sS[size_t(i)][size_t(piece)], VEC_T | uint32_t(cboff[size_t(b.col_basis)]));
                 }
                 nbld.end(uint32_t(rboff[size_t(t)] + r0), rows, true);
             }
@@ -612,15 +876,12 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     {   // backward + near field: y_tau += alpha (sum_t V_t[tau] uy_t + sum D x)
         NPass& bw = p.npasses[1];
         bw.vx = V_X; bw.vt = V_T2; bw.out = V_Y; bw.mode = OUT_ADD_ALPHA;
-        NBuilder nbld(bw);
-        std::vector<size_t> posRB(size_t(nrb), 0), posD(size_t(nb), 0);
+        NBuilder nbld(bw, st);
+        std::vector<size_t> posRB(static_cast<size_t>(nrb), 0), posD(static_cast<size_t>(nb), 0);
         for (int64_t t = 0; t < tr.n(); ++t) {
             nbld.begin(tr.size(t));
-            const int64_t ld = pad_rows(tr.size(t));
-            for (int64_t i : rbl[size_t(t)])
-                nbld.slab(sRB[size_t(i)][posRB[size_t(i)]++], ld, d.row_bases[i].rank, VEC_T | uint32_t(rboff[size_t(i)]));
-            for (int64_t i : rdl[size_t(t)])
-                nbld.slab(sD[size_t(i)][posD[size_t(i)]++], ld, d.blocks[i].ncols, uint32_t(d.blocks[i].col0));
+            for (int64_t i : rbl[size_t(t)]) nbld.slab(sRB[size_t(i)][posRB[size_t(i)]++], VEC_T | uint32_t(rboff[size_t(i)]));
+            for (int64_t i : rdl[size_t(t)]) nbld.slab(sD[size_t(i)][posD[size_t(i)]++], uint32_t(d.blocks[i].col0));
             nbld.end(uint32_t(tr.lo(t)), tr.size(t), false);
         }
         nbld.finish();
@@ -629,24 +890,23 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     {   // forward with row bases: ux'_t = V_t^T x, per row tile
         TTPass& f = p.ttpasses[1];
         f.in = V_X; f.out = V_T; f.mode = OUT_SET;
-        TTBuilder tb(f, size_t(nrb));
+        TTBuilder tb(f, st, size_t(nrb));
         for (int64_t i = 0; i < nrb; ++i)
             if (rboff[size_t(i)] >= 0)
                 tb.object(size_t(i), uint32_t(rboff[size_t(i)]), d.row_bases[i].rank,
                           tr.first(d.row_bases[i].ofs + d.row_bases[i].size) - tr.first(d.row_bases[i].ofs));
         for (int64_t t = 0; t < tr.n(); ++t) {
             tb.begin(tr.lo(t), tr.size(t));
-            const int64_t ld = pad_rows(tr.size(t));
             for (int64_t i : rbl[size_t(t)]) {
                 const int64_t ti = t - tr.first(d.row_bases[i].ofs);
-                tb.slab(sRB[size_t(i)][size_t(ti)], ld, size_t(i), ti);
+                tb.slab(sRB[size_t(i)][size_t(ti)], size_t(i), ti);
             }
             tb.end();
         }
         tb.finish();
     }
-    {   // coupling^T: uy'_s = sum_t S_ts^T ux'_t
-        TPass& c = p.tpasses[2];
+    {   // coupling^T: uy'_s = sum_t S_ts^T ux'_t (coefficient vectors are small: unit T-form)
+        TPass& c = p.tpasses[0];
         c.in = V_T; c.out = V_T2; c.mode = OUT_SET;
         TBuilder tb(c);
         for (int64_t s = 0; s < ncb; ++s) {
@@ -657,8 +917,8 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
                 const int64_t kr = d.row_bases[b.row_basis].rank;
                 for (int64_t r0 = 0, piece = 0; r0 < kr; r0 += TILE, ++piece) {
                     const int64_t rows = std::min<int64_t>(TILE, kr - r0);
-                    sl.push_back({uint64_t(sS[size_t(i)][size_t(piece)]), uint32_t(rboff[size_t(b.row_basis)] + r0),
-                                  uint16_t(rows), uint16_t(pad_rows(rows))});
+                    sl.push_back({uint64_t(st.slab_elem_off(sS[size_t(i)][size_t(piece)])),
+                                  uint32_t(rboff[size_t(b.row_basis)] + r0), uint16_t(rows), uint16_t(pad_rows(rows))});
                 }
             }
             tb.add(uint32_t(cboff[size_t(s)]), d.col_bases[s].rank, sl);
@@ -668,40 +928,23 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     {   // backward with column bases: y_sigma += alpha sum_s V_s[sigma] uy'_s
         NPass& bw = p.npasses[2];
         bw.vx = V_X; bw.vt = V_T2; bw.out = V_Y; bw.mode = OUT_ADD_ALPHA;
-        NBuilder nbld(bw);
+        NBuilder nbld(bw, st);
         for (int64_t t = 0; t < tc.n(); ++t) {
             nbld.begin(tc.size(t));
-            const int64_t ld = pad_rows(tc.size(t));
             for (int64_t i : cbl[size_t(t)])
-                nbld.slab(sCB[size_t(i)][size_t(t - tc.first(d.col_bases[i].ofs))], ld, d.col_bases[i].rank,
-                          VEC_T | uint32_t(cboff[size_t(i)]));
+                nbld.slab(sCB[size_t(i)][size_t(t - tc.first(d.col_bases[i].ofs))], VEC_T | uint32_t(cboff[size_t(i)]));
             nbld.end(uint32_t(tc.lo(t)), tc.size(t), false);
         }
         nbld.finish();
     }
-    {   // near field transposed: y_sigma += alpha sum D^T x
-        TPass& dT = p.tpasses[3];
-        dT.in = V_X; dT.out = V_Y; dT.mode = OUT_ADD_ALPHA;
-        TBuilder tb(dT);
-        for (int64_t t = 0; t < tc.n(); ++t) {
-            std::vector<TSlab> sl;
-            for (int64_t i : cdl[size_t(t)]) {
-                const hlrc_uniform_block& b = d.blocks[i];
-                const int64_t r0 = tr.first(b.row0);
-                for (size_t s = 0; s < sD[size_t(i)].size(); ++s) {
-                    const int64_t rt = r0 + int64_t(s);
-                    const int64_t ld = pad_rows(tr.size(rt));
-                    sl.push_back({uint64_t(sD[size_t(i)][s] + (tc.lo(t) - b.col0) * ld), uint32_t(tr.lo(rt)),
-                                  uint16_t(tr.size(rt)), uint16_t(ld)});
-                }
-            }
-            if (!sl.empty()) tb.add(uint32_t(tc.lo(t)), tc.size(t), sl);
-        }
-        tb.finish();
-    }
+    // near field transposed: y_sigma += alpha sum D^T x
+    plan_dense_transposed(p.ttpasses[2], st, tr, tc, rdl, sD, [&](int64_t i, int64_t& c0, int64_t& nc) {
+        c0 = d.blocks[i].col0;
+        nc = d.blocks[i].ncols;
+    });
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}, {1, 1}};
     p.stages[HLRC_OP_T].clear();  // uniform_lrmatrix::uni_apply_add asserts on apply_transposed
-    p.stages[HLRC_OP_C] = {{2, 1}, {0, 2}, {1, 2}, {0, 3}};
+    p.stages[HLRC_OP_C] = {{2, 1}, {0, 0}, {1, 2}, {2, 2}};
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
 

@@ -26,6 +26,20 @@ enum OutMode : int {
     OUT_ADD_ALPHA = 1,  // out += alpha * s   (y)
 };
 
+// A chunk of stored matrix data as the planner sees it, before it is
+// encoded into the device descriptor of the plan's precision: <= 8 columns
+// of one slab, all in one storage format.
+struct GChunk {
+    uint64_t byte_off;     // offset of the chunk's first column in the store
+    uint32_t vo;           // N-form: vector offset (| VEC_T); TT-form: output / partial offset
+    uint16_t nc;           // columns
+    uint8_t fmt;           // StoreFmt
+    uint8_t flags;         // TT_DIRECT for tile T-form chunks; GC_PACK2 (planner only)
+    float scale;           // value = stored * scale (1 for unscaled formats)
+};
+// planner flag: this chunk is the second part of a pack with the chunk before it
+constexpr uint8_t GC_PACK2 = 0x80;
+
 struct TPass {
     std::vector<TSlab> slabs;
     std::vector<TUnit> units;      // ordered by column class, then cost
@@ -38,23 +52,24 @@ struct TPass {
     bool empty() const { return units.empty(); }
 };
 
+// N-form and tile-T-form passes keep one segment list per storage format:
+// a tile's chunks are grouped by format, and each format runs as its own
+// launch (FP64, FP32, FP16, BF16 in that fixed order).
 struct NPass {
-    std::vector<NSeg> segs;        // ordered by cost (descending)
-    std::vector<NChunk> chunks;
+    std::vector<NSeg> segs[4];     // per StoreFmt, ordered by cost (descending)
+    std::vector<GChunk> chunks;
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0;
     int64_t alg_bytes = 0;
-    bool empty() const { return segs.empty(); }
 };
 
 struct TTPass {
-    std::vector<TTSeg> segs;       // ordered by cost (descending)
-    std::vector<TTChunk> chunks;
+    std::vector<TTSeg> segs[4];    // per StoreFmt, ordered by cost (descending)
+    std::vector<GChunk> chunks;
     std::vector<TGroup> groups;    // multi-tile outputs: partials summed in tile order
     int64_t npart = 0;             // partial array length (doubles)
     int in = V_X, out = V_T, mode = OUT_SET;
     int64_t bytes = 0, alg_bytes = 0;
-    bool empty() const { return segs.empty(); }
 };
 
 // One stage of a product: exactly one of the passes is used.
@@ -67,7 +82,7 @@ struct Plan {
     int kind = 0;                  // 0 = H, 1 = uniform-H
     int precision = HLRC_PREC_F64;
     int64_t nrows = 0, ncols = 0;
-    std::vector<double> store;     // FP64 slab storage
+    std::vector<uint8_t> store;    // slab storage (FP64, or per-chunk formats)
     int64_t n_t = 0, n_t2 = 0;     // workspace vector lengths (per rhs)
     std::vector<TPass> tpasses;
     std::vector<NPass> npasses;
@@ -77,6 +92,7 @@ struct Plan {
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;
     int32_t max_rank = 0;
+    int64_t fmt_bytes[4] = {0, 0, 0, 0};  // stored bytes per StoreFmt (accounting of mixed precision)
 };
 
 // Returns HLRC_OK or an error (message recorded via fail()).

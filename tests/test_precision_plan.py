@@ -1,0 +1,40 @@
+"""Host-side planning of the reduced-precision stores (no GPU)."""
+import numpy as np
+import pytest
+
+import hlr_b200 as hlr
+
+
+@pytest.mark.parametrize("fixture", ["c1_small", "c2_small"])
+def test_store_bytes_by_precision(request, fixture):
+    hm = request.getfixturevalue(fixture)
+    b64 = hlr.plan_info(hm, precision="f64")["matrix_bytes"]
+    b32 = hlr.plan_info(hm, precision="f32")["matrix_bytes"]
+    b16 = hlr.plan_info(hm, precision="f16")["matrix_bytes"]
+    bbf = hlr.plan_info(hm, precision="bf16")["matrix_bytes"]
+    bmx = hlr.plan_info(hm, precision="mixed")["matrix_bytes"]
+    assert b32 * 2 == b64
+    assert b16 == bbf and b64 / 4 < b16 < b64 / 4 * 1.2  # 16-bit data + one FP32 scale per chunk
+    assert b16 < bmx < b32  # dense FP32, low-rank columns FP32 or FP16
+
+
+def test_mixed_eps_controls_the_mix(c2_small):
+    loose = hlr.plan_info(c2_small, precision="mixed", mixed_eps=1e-4)["matrix_bytes"]
+    tight = hlr.plan_info(c2_small, precision="mixed", mixed_eps=1e-8)["matrix_bytes"]
+    assert loose < tight
+    with pytest.raises(hlr.HLRCError):
+        hlr.plan_info(c2_small, precision="mixed", mixed_eps=0.0)
+
+
+def test_uniform_is_fp64_only(c3_small):
+    with pytest.raises(hlr.HLRCError) as e:
+        hlr.plan_info(c3_small, uniform=True, precision="f32")
+    assert e.value.status == 1
+
+
+def test_fp16_conversion_is_round_to_nearest_even():
+    # exactly representable values survive; the planner's scale is a power of two
+    ll = hlr.LeafList(2, 2)
+    ll.add_dense(0, 0, np.array([[1.0, -2.5], [0.125, 1024.0]]))
+    info = hlr.plan_info(ll, precision="f16")
+    assert info["matrix_bytes"] == 2 * 4 + 4
