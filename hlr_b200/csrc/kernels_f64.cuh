@@ -154,19 +154,30 @@ k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks,
     const bool active = r < sg.ld;
     const double v0 = (r < sg.rows) ? __ldg(vin + sg.v_off + r) : 0.0;
     const double v1 = (r + 1 < sg.rows) ? __ldg(vin + sg.v_off + r + 1) : 0.0;
+    // software pipeline: the loads of chunk c + W are issued before chunk c
+    // is reduced and written; descriptors are fetched two iterations ahead
     uint32_t c = sg.cb + warp;
-    TTChunk nxt = c < sg.ce ? chunks[c] : TTChunk{0, 0, 0, 0};
-    for (; c < sg.ce; c += W) {
-        const TTChunk ch = nxt;
-        if (c + W < sg.ce) nxt = chunks[c + W];
-        const double* a = A + ch.a_off + r;
-        double2 m[TCOLS];
+    if (c >= sg.ce) return;
+    TTChunk cur = chunks[c], nxt{0, 0, 0, 0};
+    if (c + W < sg.ce) nxt = chunks[c + W];
+    double2 m[TCOLS];
+    auto issue = [&](const TTChunk& q) {
+        const double* a = A + q.a_off + r;
 #pragma unroll
         for (int j = 0; j < TCOLS; ++j)
-            m[j] = (active && j < ch.nc) ? ld_stream(a + size_t(j) * sg.ld) : make_double2(0.0, 0.0);
+            m[j] = (active && j < q.nc) ? ld_stream(a + size_t(j) * sg.ld) : make_double2(0.0, 0.0);
+    };
+    issue(cur);
+    for (; c < sg.ce; c += W) {
         double p[TCOLS];
 #pragma unroll
         for (int j = 0; j < TCOLS; ++j) p[j] = fma(m[j].y, v1, m[j].x * v0);
+        const TTChunk ch = cur;
+        if (c + W < sg.ce) {
+            cur = nxt;
+            issue(cur);
+            if (c + 2 * W < sg.ce) nxt = chunks[c + 2 * W];
+        }
         TransposeReduce<TCOLS, 16>::run(p, lane);
         constexpr int SH = 5 - Log2<TCOLS>::v;
         const int col = lane >> SH;

@@ -178,15 +178,10 @@ __device__ __forceinline__ void tx_q(const double* vin, const TTSeg& sg, int lan
     }
 }
 
+// per-lane dot products of the 8 loaded column pieces with x
 template <int FMT>
-__device__ __forceinline__ void ttpack_q(const QTTPack& pk, const uint8_t* A, int ld, int lane, const float* xr,
-                                         double* out, double* part, double alpha, int add) {
+__device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float* p) {
     using F = QFmt<FMT>;
-    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
-    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
-    uint4 m[8];
-    load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m);
-    float p[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         float f[F::R];
@@ -196,6 +191,15 @@ __device__ __forceinline__ void ttpack_q(const QTTPack& pk, const uint8_t* A, in
         for (int r = 0; r < F::R; ++r) s = fmaf(f[r], xr[r], s);
         p[i] = s;
     }
+}
+
+// reduce the pack's column partials and write them
+template <int FMT>
+__device__ __forceinline__ void ttreduce_q(const QTTPack& pk, int lane, float* p, double* out, double* part,
+                                           double alpha, int add) {
+    using F = QFmt<FMT>;
+    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
+    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
     // reduce the 8 column partials over the G lanes of the group; afterwards
     // the lane holds pack column g + C * (l >> (LOG_G - 3))
     TransposeReduce<8, F::G / 2, float>::run(p, lane);
@@ -225,13 +229,24 @@ k_ttform_q(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, co
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float xr[F::R];
     tx_q<FMT>(vin, sg, lane, xr);
+    // software pipeline: the loads of pack c + W are issued before pack c is
+    // reduced and written, and descriptors are fetched two iterations ahead
     uint32_t c = sg.cb + warp;
-    QTTPack nxt{};
-    if (c < sg.ce) nxt = ld_pack(packs + c);
+    if (c >= sg.ce) return;
+    QTTPack cur = ld_pack(packs + c), nxt{};
+    if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
+    uint4 m[8];
+    load_pack<FMT>(A, cur.p[0].a16, cur.p[1].a16, cur.p[0].nc, cur.p[0].nc + cur.p[1].nc, sg.ld, lane, m);
     for (; c < sg.ce; c += W) {
-        const QTTPack pk = nxt;
-        if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
-        ttpack_q<FMT>(pk, A, sg.ld, lane, xr, out, part, alpha, add);
+        float p[8];
+        ttdots_q<FMT>(m, xr, p);
+        const QTTPack done = cur;
+        if (c + W < sg.ce) {
+            cur = nxt;
+            load_pack<FMT>(A, cur.p[0].a16, cur.p[1].a16, cur.p[0].nc, cur.p[0].nc + cur.p[1].nc, sg.ld, lane, m);
+            if (c + 2 * W < sg.ce) nxt = ld_pack(packs + c + 2 * W);
+        }
+        ttreduce_q<FMT>(done, lane, p, out, part, alpha, add);
     }
 }
 
