@@ -213,17 +213,25 @@ def run_ours(args, rank, world, local_rank):
     if args.precision:
         prec = args.precision
         desc = desc.replace("FP64 ", f"{prec.upper()}-stored ") if prec != "f64" else desc
+    if args.nrhs:
+        nrhs = args.nrhs
     tb = time.perf_counter()
     hm = hlr.build(prob)
     t_build = time.perf_counter() - tb
     tu = time.perf_counter()
-    M = hlr.upload(hm, precision=prec, uniform=uniform)
+    M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs)
     t_upload = time.perf_counter() - tu
     info = M.info
     n = hm.n
-    xh = np.random.default_rng(2).standard_normal(n)
-    x = torch.from_numpy(xh).to(dev)
-    y = torch.zeros(n, dtype=torch.float64, device=dev)
+    # x ~ N(0,1), one column per right-hand side (column-major (n, nrhs))
+    xh = np.random.default_rng(2).standard_normal((nrhs, n))
+
+    def dev_vec(a):
+        t_ = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        return t_[0] if nrhs == 1 else t_.T
+
+    x = dev_vec(xh)
+    y = dev_vec(np.zeros((nrhs, n)))
     alpha = 2.0
     stream = torch.cuda.current_stream(dev)
 
@@ -239,12 +247,14 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = M.launch_count()
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
+    timed_launches = M.launch_count() - launches0
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
@@ -255,20 +265,22 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
 
-    # correctness of the timed path: one product from zero, against the oracle
-    yc = torch.zeros(n, dtype=torch.float64, device=dev)
+    # correctness of the timed path: one product from zero; column 0 is
+    # compared with the oracle below
+    yc = dev_vec(np.zeros((nrhs, n)))
     hlr.mul_vec(1.0, hlr.apply_normal, M, x, yc)
     torch.cuda.synchronize()
-    ygpu = yc.cpu().numpy()
+    ygpu_all = (yc if nrhs > 1 else yc[:, None]).cpu().numpy()
+    ygpu = ygpu_all[:, 0].copy()
 
     # reduced precision: the FP64 GPU product of the same matrix, timed the
     # same way, is the error reference and the speed-up denominator
     fp64 = None
     if prec != "f64":
-        M64 = hlr.upload(hm, precision="f64", uniform=uniform)
-        y64 = torch.zeros(n, dtype=torch.float64, device=dev)
+        M64 = hlr.upload(hm, precision="f64", uniform=uniform, max_nrhs=nrhs)
+        y64 = dev_vec(np.zeros((nrhs, n)))
         hlr.mul_vec(1.0, hlr.apply_normal, M64, x, y64)
-        yy = torch.zeros(n, dtype=torch.float64, device=dev)
+        yy = dev_vec(np.zeros((nrhs, n)))
         for _ in range(args.warmup):
             hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy)
         torch.cuda.synchronize()
@@ -279,17 +291,21 @@ def run_ours(args, rank, world, local_rank):
         f1.record(stream)
         torch.cuda.synchronize()
         ms64 = f0.elapsed_time(f1)
-        y64h = y64.cpu().numpy()
-        fp64 = {"value": args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+        y64h = (y64 if nrhs > 1 else y64[:, None]).cpu().numpy()
+        fp64 = {"value": nrhs * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
                 "matrix_bytes": M64.info["matrix_bytes"],
-                "rel_err_vs_fp64": float(np.linalg.norm(ygpu - y64h) / np.linalg.norm(y64h))}
+                "rel_err_vs_fp64": float(np.linalg.norm(ygpu_all - y64h) / np.linalg.norm(y64h))}
         M64.free()
         del yy, y64
 
     # end to end through the C ABI with pinned host buffers (copies inside)
     xp = torch.from_numpy(xh.copy()).pin_memory()
-    yp = torch.zeros(n, dtype=torch.float64).pin_memory()
+    yp = torch.zeros((nrhs, n), dtype=torch.float64).pin_memory()
     xpn, ypn = xp.numpy(), yp.numpy()
+    if nrhs == 1:
+        xpn, ypn = xpn[0], ypn[0]
+    else:  # (n, nrhs) Fortran-ordered views of the pinned (nrhs, n) buffers
+        xpn, ypn = xpn.T, ypn.T
     for _ in range(max(1, args.warmup // 2)):
         hlr.mul_vec(alpha, hlr.apply_normal, M, xpn, ypn)
     torch.cuda.synchronize()
@@ -312,9 +328,10 @@ def run_ours(args, rank, world, local_rank):
         return
 
     hbm_peak, peak_kind = peaks()
-    value = world * args.steps / (ms_max / 1e3)
+    # every right-hand side counts as one matrix-vector product
+    value = world * args.steps * nrhs / (ms_max / 1e3)
     alg = info["algorithmic_bytes"]
-    gbs = alg / (ms_max / 1e3 / args.steps) / 1e9
+    gbs = alg / (ms_max / 1e3 / args.steps) / 1e9   # matrix bytes streamed per step (one pass per step at nrhs=1)
     # dominant kernel = pass with the largest device time
     dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
     roof = None
@@ -340,9 +357,9 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
                    for k, v in prof.items()},
-        "gpu_launches": info["launches"][0] * args.steps,
-        "e2e": {"value": world * ksteps / (e2e_ms / 1e3), "unit": "MVM/s",
-                "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": timed_launches,
+        "e2e": {"value": world * ksteps * nrhs / (e2e_ms / 1e3), "unit": "MVM/s",
+                "h2d_bytes_per_step": 2 * 8 * n * nrhs, "d2h_bytes_per_step": 8 * n * nrhs},
         "clocks": clocks.summary(),
     }
     if fp64 is not None:
@@ -354,7 +371,7 @@ def run_ours(args, rank, world, local_rank):
         ncores = os.cpu_count() or 1
         yo = np.zeros(n)
         t0 = time.perf_counter()
-        cpu_mvm(hm, uniform, d, xh, yo, ncores)
+        cpu_mvm(hm, uniform, d, np.ascontiguousarray(xh[0]), yo, ncores)
         t1 = time.perf_counter() - t0
         line["rel_err_vs_oracle"] = float(np.linalg.norm(ygpu - yo) / np.linalg.norm(yo))
         reps, el = 0, 0.0
@@ -362,7 +379,7 @@ def run_ours(args, rank, world, local_rank):
         while el < budget and reps < 50:
             yy = np.zeros(n)
             t0 = time.perf_counter()
-            cpu_mvm(hm, uniform, d, xh, yy, ncores)
+            cpu_mvm(hm, uniform, d, np.ascontiguousarray(xh[0]), yy, ncores)
             el += time.perf_counter() - t0
             reps += 1
         line["cpu_baseline"] = {"value": reps / el, "unit": "MVM/s", "cores": ncores, "kind": "port",
@@ -395,6 +412,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed"],
                     help="storage precision (default: the config's)")
+    ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -216,6 +216,10 @@ class DeviceMatrix:
         k = lib().hlrc_last_profile(self._h, names, cnt, ms, by, 64)
         return {names[i].decode(): (cnt[i], ms[i], by[i]) for i in range(k)}
 
+    def launch_count(self) -> int:
+        """Kernels launched by this handle so far (hlrc_launch_count)."""
+        return int(lib().hlrc_launch_count(self._h))
+
     def free(self) -> None:
         if self._h:
             lib().hlrc_free(self._h)

@@ -86,6 +86,7 @@ PROTOTYPES = {
     "hlrc_last_profile": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_int), pdbl,
                                     C.POINTER(i64), C.c_int]),
     "hlrc_free": (C.c_int, [C.c_void_p]),
+    "hlrc_launch_count": (i64, [C.c_void_p]),
     "hlrc_check_device_error": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "hlrc_build": (C.c_int, [C.POINTER(hlrc_problem), C.POINTER(C.c_void_p)]),
     "hlrc_build_h_desc": (C.c_int, [C.c_void_p, C.POINTER(hlrc_h_desc)]),

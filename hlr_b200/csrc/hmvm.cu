@@ -19,6 +19,7 @@
 #include "common.hpp"
 #include "hlrc.h"
 #include "kernels_f64.cuh"
+#include "kernels_mr.cuh"
 #include "kernels_q.cuh"
 #include "plan.hpp"
 
@@ -95,10 +96,15 @@ struct hlrc_hmat_s {
     std::vector<DevTTPass> tt;
     std::vector<Stage> stages[3];
     hlrc_info info{};
+    // multi-RHS workspace (FP64 plans, allocated at upload when max_nrhs > 1):
+    // row-major blocks of MR_RB vectors
+    char* mr_arena = nullptr;
+    double *mr_x = nullptr, *mr_t = nullptr, *mr_t2 = nullptr, *mr_part = nullptr;
     // host-pointer entry point staging
     double* hx = nullptr;
     double* hy = nullptr;
     size_t hx_elems = 0, hy_elems = 0;
+    int64_t launches = 0;     // kernels launched by this handle
     // profiling
     bool profiling = false;
     std::vector<ProfileRec> prof;
@@ -351,6 +357,30 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
 
     fill_info(p, L, hp->info);
+    if (o.max_nrhs > 1 && p.precision == HLRC_PREC_F64) {
+        const size_t nx = size_t(std::max(p.nrows, p.ncols)) * MR_RB;
+        const size_t nt = size_t(std::max<int64_t>(1, p.n_t)) * MR_RB, nt2 = size_t(std::max<int64_t>(1, p.n_t2)) * MR_RB;
+        const size_t np = size_t(std::max<int64_t>(1, hp->n_part)) * MR_RB;
+        const size_t bytes = (nx + nt + nt2 + np) * sizeof(double) + 4 * 256;
+        e = cudaMalloc(&hp->mr_arena, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cleanup();
+            return fail(HLRC_ERR_OOM, "multi-RHS workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
+        }
+        size_t off = 0;
+        auto carve = [&](size_t elems) {
+            double* q = reinterpret_cast<double*>(hp->mr_arena + off);
+            off = align_up(off + elems * sizeof(double), 256);
+            return q;
+        };
+        hp->mr_x = carve(nx);
+        hp->mr_t = carve(nt);
+        hp->mr_t2 = carve(nt2);
+        hp->mr_part = carve(np);
+        hp->info.workspace_bytes += int64_t(bytes);
+        hp->info.device_bytes += int64_t(bytes);
+    }
     for (int op = 0; op < 3; ++op) {
         int nl = 0;
         for (const Stage& st : hp->stages[op])
@@ -371,6 +401,7 @@ struct Workspace {
 };
 
 Workspace handle_workspace(hlrc_hmat M) { return {M->ws_t, M->ws_t2, M->part, M->profiling}; }
+bool ws_profile(hlrc_hmat M) { return M->profiling; }
 
 double* bind(const Workspace& ws, int name, const double* x, double* y) {
     switch (name) {
@@ -406,6 +437,8 @@ constexpr int TTFORM_WARPS = 8;
 hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, const double* x, double* y,
                        cudaStream_t s) {
     for (const Stage& st : M->stages[op]) {
+        M->launches += st.kind == 0 ? M->t[size_t(st.idx)].launches()
+                                    : (st.kind == 1 ? M->n[size_t(st.idx)].launches() : M->tt[size_t(st.idx)].launches());
         if (st.kind == 0) {
             const DevTPass& tp = M->t[size_t(st.idx)];
             const double* vin = bind(ws, tp.in, x, y);
@@ -486,6 +519,73 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
     return HLRC_OK;
 }
 
+// Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
+// the multi-RHS workspace, an FP64 store, and no unit T-form stage (the
+// uniform-H adjoint coupling runs per vector).
+bool multi_rhs_ok(hlrc_hmat M, int op) {
+    if (!M->mr_arena || M->precision != HLRC_PREC_F64) return false;
+    for (const Stage& st : M->stages[op])
+        if (st.kind == 0) return false;
+    return true;
+}
+
+// y := y + alpha op(M) X for nrhs column vectors, MR_RB at a time: the matrix
+// is streamed once per block instead of once per vector.
+hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                      int nrhs, cudaStream_t s) {
+    const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
+    for (int r0 = 0; r0 < nrhs; r0 += MR_RB) {
+        const int nr = std::min(MR_RB, nrhs - r0);
+        const int64_t tot = nx * MR_RB;
+        k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, M->mr_x);
+        M->launches += 1;
+        for (const Stage& st : M->stages[op]) {
+            if (st.kind == 2) {
+                const DevTTPass& tp = M->tt[size_t(st.idx)];
+                M->launches += (tp.nsegs[FMT_F64] > 0 ? MR_RB / MR_TB : 0) + (tp.ngroups > 0 ? 1 : 0);
+            } else if (st.kind == 1) {
+                M->launches += M->n[size_t(st.idx)].nsegs[FMT_F64] > 0 ? 1 : 0;
+            }
+        }
+        auto vec = [&](int name) -> double* {
+            return name == V_X ? M->mr_x : (name == V_T ? M->mr_t : M->mr_t2);
+        };
+        auto omap = [&](int name) -> OutMap {
+            if (name == V_Y) return OutMap{Y + int64_t(r0) * ldy, 1, ldy, nr};
+            return OutMap{vec(name), MR_RB, 1, MR_RB};
+        };
+        const double* A = reinterpret_cast<const double*>(M->store);
+        for (const Stage& st : M->stages[op]) {
+            if (st.kind == 2) {
+                const DevTTPass& tp = M->tt[size_t(st.idx)];
+                const int add = tp.mode == OUT_ADD_ALPHA;
+                const OutMap om = omap(tp.out);
+                if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
+                if (tp.nsegs[FMT_F64] > 0)
+                    for (int rt = 0; rt < MR_RB; rt += MR_TB)
+                        k_ttform_f64_mr<TTFORM_WARPS><<<tp.nsegs[FMT_F64], TTFORM_WARPS * 32, 0, s>>>(
+                            tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), rt, om, M->mr_part,
+                            alpha, add);
+                if (tp.ngroups > 0)
+                    k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om, alpha,
+                                                                          add);
+                if (ws_profile(M)) prof_end(M, s);
+            } else if (st.kind == 1) {
+                const DevNPass& np = M->n[size_t(st.idx)];
+                if (np.nsegs[FMT_F64] == 0) continue;
+                if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
+                k_nform_f64_mr<NFORM_WARPS><<<np.nsegs[FMT_F64], NFORM_WARPS * 32, 0, s>>>(
+                    np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), omap(np.out),
+                    alpha, np.mode == OUT_ADD_ALPHA);
+                if (ws_profile(M)) prof_end(M, s);
+            }
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return HLRC_OK;
+}
+
 hlrc_status check_mvm_args(hlrc_hmat M, int op, const double* x, double* y, int nrhs, int64_t ldx, int64_t ldy) {
     if (!M) return fail(HLRC_ERR_ARG, "matrix handle is NULL");
     if (op < 0 || op > 2) return fail(HLRC_ERR_ARG, "op %d is not a valid hlrc_op", op);
@@ -559,6 +659,7 @@ extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double*
     DeviceGuard g(M->device);
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (nrhs > 1 && multi_rhs_ok(M, op)) return run_multi(M, alpha, op, x, ldx, y, ldy, nrhs, s);
     const Workspace ws = handle_workspace(M);
     for (int r = 0; r < nrhs; ++r) {
         st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
@@ -593,10 +694,15 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     const int64_t lx = nrhs > 1 ? ldx : nx, ly = nrhs > 1 ? ldy : ny;
     HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
-    const Workspace ws = handle_workspace(M);
-    for (int r = 0; r < nrhs; ++r) {
-        st = run_single(M, ws, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
+    if (nrhs > 1 && multi_rhs_ok(M, op)) {
+        st = run_multi(M, alpha, op, M->hx, nx, M->hy, ny, nrhs, nullptr);
         if (st != HLRC_OK) return st;
+    } else {
+        const Workspace ws = handle_workspace(M);
+        for (int r = 0; r < nrhs; ++r) {
+            st = run_single(M, ws, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
+            if (st != HLRC_OK) return st;
+        }
     }
     HLRC_CUDA(cudaMemcpy2D(y, size_t(ly) * 8, M->hy, size_t(ny) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyDeviceToHost));
     return HLRC_OK;
@@ -709,6 +815,8 @@ extern "C" hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op, const
     return run_single(M, ws, alpha, op, x, y, static_cast<cudaStream_t>(stream));
 }
 
+extern "C" int64_t hlrc_launch_count(hlrc_hmat M) { return M ? M->launches : 0; }
+
 extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     if (!M) return HLRC_OK;
     DeviceGuard g(M->device);
@@ -718,6 +826,7 @@ extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     }
     cudaFree(M->hx);
     cudaFree(M->hy);
+    cudaFree(M->mr_arena);
     cudaFree(M->arena);
     delete M;
     return HLRC_OK;

@@ -256,6 +256,10 @@ hlrc_status hlrc_set_profiling(hlrc_hmat M, int enable);
 int         hlrc_last_profile(hlrc_hmat M, const char** names, int* count,
                               double* ms, int64_t* bytes, int cap);
 
+/* Number of kernels this handle has launched since upload (all entry
+ * points); lets a caller count the launches inside a timed region.         */
+int64_t     hlrc_launch_count(hlrc_hmat M);
+
 hlrc_status hlrc_free(hlrc_hmat M);
 
 /* Debug-only: copies the device result of the most recent error word (set by
