@@ -388,6 +388,107 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def c5_problems(count=32, seed=5, nthreads=0):
+    """The batched workload: count 3D exponential-covariance matrices with
+    ell ~ U[0.05, 0.2], n log-uniform in [4096, 65536] (numpy default_rng(seed),
+    ell drawn before n for each member), U[0,1]^3 points with seed 1000 + i,
+    nugget 1e-4, leaf 64, eta 2, eps 1e-6."""
+    import hlr_b200 as hlr
+    rng = np.random.default_rng(seed)
+    probs = []
+    for i in range(count):
+        ell = float(rng.uniform(0.05, 0.2))
+        n = int(round(np.exp(rng.uniform(np.log(4096), np.log(65536)))))
+        probs.append(hlr.Problem.exp3d(n, ell=ell, nugget=1e-4, seed=1000 + i, nthreads=nthreads))
+    return probs
+
+
+def run_batch(args, rank, world, local_rank):
+    """C5: all members in one batched handle; K timed batched products with
+    8 right-hand sides in the inner precision, then one CG solve with FP64
+    iterative refinement to 1e-10."""
+    import torch
+
+    import hlr_b200 as hlr
+    from hlr_b200.solve import cg_refine
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nrhs = args.nrhs or 8
+    inner = args.precision or "mixed"
+    count = 32
+    tb = time.perf_counter()
+    hms = [hlr.build(p) for p in c5_problems(count, nthreads=os.cpu_count() or 0)]
+    t_build = time.perf_counter() - tb
+    pad = (max(h.n for h in hms) + 63) // 64 * 64
+    A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
+    Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
+    N = count * pad
+    rng = np.random.default_rng(9)
+    b = np.zeros((nrhs, N))
+    for i, h in enumerate(hms):
+        b[:, i * pad:i * pad + h.n] = rng.standard_normal((nrhs, h.n))
+    bt = torch.from_numpy(b).to(dev)
+    y = torch.zeros_like(bt)
+    for _ in range(args.warmup):
+        hlr.mul_vec(1.0, hlr.apply_normal, Alow, bt.T, y.T)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = Alow.launch_count()
+    with ClockSampler(gpu_uuid(local_rank)) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            hlr.mul_vec(1.0, hlr.apply_normal, Alow, bt.T, y.T)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = Alow.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    # FP64 batched product, same protocol, for the speed-up statement
+    y64 = torch.zeros_like(bt)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        hlr.mul_vec(1.0, hlr.apply_normal, A64, bt.T, y64.T)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms64 = f0.elapsed_time(f1)
+    # one full solve
+    torch.cuda.synchronize()
+    ts = time.perf_counter()
+    res = cg_refine(A64, Alow, bt, count, pad, tol=1e-10, inner_rtol=1e-7 if inner != "f64" else 1e-11,
+                    max_outer=12, max_inner=20000, check_every=25)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - ts
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = peaks()
+    value = world * args.steps * nrhs * count / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": inner, "data": "synthetic",
+        "config": {"workload": f"{count} x 3D exp-covariance (ell~U[0.05,0.2], n log-uniform [4096,65536], "
+                               f"nugget 1e-4, eps 1e-6) batched in one handle, {nrhs} RHS each, inner storage "
+                               f"{inner}, CG + FP64 refinement to 1e-10",
+                   "members": count, "n_total": sum(h.n for h in hms), "pad": pad, "nrhs": nrhs,
+                   "matrix_bytes_inner": Alow.info["matrix_bytes"], "matrix_bytes_f64": A64.info["matrix_bytes"],
+                   "build_s": round(t_build, 1),
+                   "l2": "inputs larger than L2"},
+        "hbm_gbs": Alow.info["matrix_bytes"] / (ms / 1e3 / args.steps) / 1e9,
+        "fp64_gpu": {"value": args.steps * nrhs * count / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                     "speedup": ms64 / ms},
+        "solve": {"seconds": t_solve, "outer_iterations": res.outer_iterations,
+                  "inner_iterations": res.inner_iterations, "history": res.history,
+                  "systems": int(res.converged.numel()), "converged": int(res.converged.sum()),
+                  "max_rel_residual": float(res.rel_residual.max())},
+        "gpu_launches": launches,
+        "e2e": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def traffic_from_profiles(kernel: str, config: str):
     """DRAM bytes per launch of `kernel` from a committed ncu summary table
     row `| kernel | config | bytes |` in profiles/*.md, if any."""
@@ -408,7 +509,7 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed"],
                     help="storage precision (default: the config's)")
@@ -430,7 +531,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.config == "c5":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

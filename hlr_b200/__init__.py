@@ -248,6 +248,36 @@ def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int =
     return DeviceMatrix(h, uniform)
 
 
+def upload_batch(members, precision="f64", max_nrhs: int = 1, pad_to: Optional[int] = None,
+                 mixed_eps: float = 1e-6, device: int = -1) -> DeviceMatrix:
+    """Upload many H-matrices as one block-diagonal handle.
+
+    Member i occupies rows/columns [offsets[i], offsets[i] + n_i); with
+    ``pad_to`` every member starts at i * pad_to (zero padding between), so
+    batched vectors can be viewed as (count, pad_to, nrhs) tensors.  Every
+    pass of a product then runs as one launch over all members.
+    """
+    descs = [m.h_desc() if hasattr(m, "h_desc") else m for m in members]
+    sizes = [int(d.nrows) for d in descs]
+    if pad_to is not None:
+        if max(sizes) > pad_to:
+            raise ValueError("pad_to is smaller than the largest member")
+        offsets = [i * pad_to for i in range(len(descs) + 1)]
+    else:
+        offsets = [0]
+        for s in sizes:
+            offsets.append(offsets[-1] + s)
+    arr = (_capi.hlrc_h_desc * len(descs))(*descs)
+    offs = (C.c_int64 * len(offsets))(*offsets)
+    o = _options(precision, max_nrhs, mixed_eps, device)
+    h = C.c_void_p()
+    check(lib().hlrc_upload_h_batch(arr, len(descs), offs, C.byref(o), C.byref(h)), "hlrc_upload_h_batch")
+    M = DeviceMatrix(h, False)
+    M.offsets = offsets
+    M.sizes = sizes
+    return M
+
+
 def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
               mixed_eps: float = 1e-6) -> dict:
     """Dry run of :func:`upload`: validates and flattens on the host only."""

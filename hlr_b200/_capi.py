@@ -75,6 +75,8 @@ PROTOTYPES = {
     "hlrc_default_options": (None, [C.POINTER(hlrc_options)]),
     "hlrc_upload_h": (C.c_int, [C.POINTER(hlrc_h_desc), C.POINTER(hlrc_options), C.POINTER(C.c_void_p)]),
     "hlrc_upload_uniform": (C.c_int, [C.POINTER(hlrc_uniform_desc), C.POINTER(hlrc_options), C.POINTER(C.c_void_p)]),
+    "hlrc_upload_h_batch": (C.c_int, [C.POINTER(hlrc_h_desc), C.c_int, C.POINTER(i64), C.POINTER(hlrc_options),
+                                      C.POINTER(C.c_void_p)]),
     "hlrc_plan_info_h": (C.c_int, [C.POINTER(hlrc_h_desc), C.POINTER(hlrc_options), C.POINTER(hlrc_info)]),
     "hlrc_plan_info_uniform": (C.c_int, [C.POINTER(hlrc_uniform_desc), C.POINTER(hlrc_options),
                                          C.POINTER(hlrc_info)]),

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <array>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -350,6 +351,14 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         cleanup();
         return fail(HLRC_ERR_CUDA, "upload copy failed: %s", cudaGetErrorString(e));
     }
+    // FP64 plans carry FP64 descriptors only, reduced-precision plans packs
+    // only; a mix would hand one kind of kernel the other's descriptors
+    for (const DevNPass& d : hp->n)
+        for (int f = 0; f < 4; ++f)
+            if (d.nsegs[f] > 0 && ((f == FMT_F64) != f64)) { cleanup(); return fail(HLRC_ERR_INTERNAL, "format mix in plan"); }
+    for (const DevTTPass& d : hp->tt)
+        for (int f = 0; f < 4; ++f)
+            if (d.nsegs[f] > 0 && ((f == FMT_F64) != f64)) { cleanup(); return fail(HLRC_ERR_INTERNAL, "format mix in plan"); }
     hp->store = reinterpret_cast<const uint8_t*>(hp->arena + o_store);
     hp->ws_t = reinterpret_cast<double*>(hp->arena + o_t);
     hp->ws_t2 = reinterpret_cast<double*>(hp->arena + o_t2);
@@ -357,7 +366,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
 
     fill_info(p, L, hp->info);
-    if (o.max_nrhs > 1 && p.precision == HLRC_PREC_F64) {
+    if (o.max_nrhs > 1) {
         const size_t nx = size_t(std::max(p.nrows, p.ncols)) * MR_RB;
         const size_t nt = size_t(std::max<int64_t>(1, p.n_t)) * MR_RB, nt2 = size_t(std::max<int64_t>(1, p.n_t2)) * MR_RB;
         const size_t np = size_t(std::max<int64_t>(1, hp->n_part)) * MR_RB;
@@ -433,9 +442,31 @@ void prof_end(hlrc_hmat M, cudaStream_t s) {
 constexpr int NFORM_WARPS = 8;
 constexpr int TTFORM_WARPS = 8;
 
+// Diagnostics: with HLRC_DEBUG_SYNC=1 in the environment every pass is
+// followed by a stream synchronisation, and an asynchronous kernel error is
+// reported with the name of the pass that raised it.
+bool debug_sync() {
+    static const bool on = [] {
+        const char* e = std::getenv("HLRC_DEBUG_SYNC");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+#define HLRC_AFTER_LAUNCH(name)                                                                        \
+    do {                                                                                               \
+        if (debug_sync()) {                                                                            \
+            const cudaError_t e_ = cudaStreamSynchronize(s);                                           \
+            if (e_ != cudaSuccess) return fail(HLRC_ERR_CUDA, "%s: %s", name, cudaGetErrorString(e_)); \
+        }                                                                                              \
+    } while (0)
+
 // one right-hand side: x, y are column vectors; scratch from `ws`
 hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, const double* x, double* y,
                        cudaStream_t s) {
+    // FP64 plans carry 16-byte FP64 descriptors, reduced-precision plans
+    // 32-byte packs: each kind of kernel only ever sees its own kind
+    const bool f64plan = M->precision == HLRC_PREC_F64;
     for (const Stage& st : M->stages[op]) {
         M->launches += st.kind == 0 ? M->t[size_t(st.idx)].launches()
                                     : (st.kind == 1 ? M->n[size_t(st.idx)].launches() : M->tt[size_t(st.idx)].launches());
@@ -459,6 +490,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             if (tp.ngroups > 0)
                 k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
             if (ws.profile) prof_end(M, s);
+            HLRC_AFTER_LAUNCH(stage_name(M->kind, 0, st.idx));
         } else if (st.kind == 2) {
             const DevTTPass& tp = M->tt[size_t(st.idx)];
             if (tp.launches() == 0) continue;
@@ -468,17 +500,17 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
             const QTTPack* qc = static_cast<const QTTPack*>(tp.chunks);
             constexpr int TW = TTFORM_WARPS;
-            if (tp.nsegs[FMT_F64] > 0)
+            if (f64plan && tp.nsegs[FMT_F64] > 0)
                 k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
                     tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
                     reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
-            if (tp.nsegs[FMT_F32] > 0)
+            if (!f64plan && tp.nsegs[FMT_F32] > 0)
                 k_ttform_q<TW, FMT_F32><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(tp.segs[FMT_F32], qc, M->store, vin, vout,
                                                                             ws.part, alpha, add);
-            if (tp.nsegs[FMT_F16] > 0)
+            if (!f64plan && tp.nsegs[FMT_F16] > 0)
                 k_ttform_q<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(tp.segs[FMT_F16], qc, M->store, vin, vout,
                                                                             ws.part, alpha, add);
-            if (tp.nsegs[FMT_BF16] > 0)
+            if (!f64plan && tp.nsegs[FMT_BF16] > 0)
                 k_ttform_q<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(tp.segs[FMT_BF16], qc, M->store, vin,
                                                                               vout, ws.part, alpha, add);
             if (ws.profile) prof_end(M, s);
@@ -487,6 +519,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
                 if (ws.profile) prof_end(M, s);
             }
+            HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));
         } else {
             const DevNPass& np = M->n[size_t(st.idx)];
             if (np.launches() == 0) continue;
@@ -498,20 +531,21 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             const QNPack* qc = static_cast<const QNPack*>(np.chunks);
             constexpr int NW = NFORM_WARPS;
             // formats in fixed order: each launch adds its part of y
-            if (np.nsegs[FMT_F64] > 0)
+            if (f64plan && np.nsegs[FMT_F64] > 0)
                 k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                     np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
                     reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
-            if (np.nsegs[FMT_F32] > 0)
+            if (!f64plan && np.nsegs[FMT_F32] > 0)
                 k_nform_q<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(np.segs[FMT_F32], qc, M->store, vx, vt, vo,
                                                                            alpha, add);
-            if (np.nsegs[FMT_F16] > 0)
+            if (!f64plan && np.nsegs[FMT_F16] > 0)
                 k_nform_q<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(np.segs[FMT_F16], qc, M->store, vx, vt, vo,
                                                                            alpha, add);
-            if (np.nsegs[FMT_BF16] > 0)
+            if (!f64plan && np.nsegs[FMT_BF16] > 0)
                 k_nform_q<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(np.segs[FMT_BF16], qc, M->store, vx, vt,
                                                                              vo, alpha, add);
             if (ws.profile) prof_end(M, s);
+            HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
         }
     }
     const cudaError_t e = cudaGetLastError();
@@ -520,10 +554,10 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
 }
 
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
-// the multi-RHS workspace, an FP64 store, and no unit T-form stage (the
-// uniform-H adjoint coupling runs per vector).
+// the multi-RHS workspace and no unit T-form stage (the uniform-H adjoint
+// coupling runs per vector).
 bool multi_rhs_ok(hlrc_hmat M, int op) {
-    if (!M->mr_arena || M->precision != HLRC_PREC_F64) return false;
+    if (!M->mr_arena) return false;
     for (const Stage& st : M->stages[op])
         if (st.kind == 0) return false;
     return true;
@@ -539,12 +573,15 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
         const int64_t tot = nx * MR_RB;
         k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, M->mr_x);
         M->launches += 1;
+        HLRC_AFTER_LAUNCH("rows_from_cols");
         for (const Stage& st : M->stages[op]) {
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
-                M->launches += (tp.nsegs[FMT_F64] > 0 ? MR_RB / MR_TB : 0) + (tp.ngroups > 0 ? 1 : 0);
+                int nf = 0;
+                for (int f = 0; f < 4; ++f) nf += tp.nsegs[f] > 0 ? 1 : 0;
+                M->launches += nf * (MR_RB / MR_TB) + (tp.ngroups > 0 ? 1 : 0);
             } else if (st.kind == 1) {
-                M->launches += M->n[size_t(st.idx)].nsegs[FMT_F64] > 0 ? 1 : 0;
+                M->launches += M->n[size_t(st.idx)].launches();
             }
         }
         auto vec = [&](int name) -> double* {
@@ -561,23 +598,55 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 const int add = tp.mode == OUT_ADD_ALPHA;
                 const OutMap om = omap(tp.out);
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-                if (tp.nsegs[FMT_F64] > 0)
-                    for (int rt = 0; rt < MR_RB; rt += MR_TB)
-                        k_ttform_f64_mr<TTFORM_WARPS><<<tp.nsegs[FMT_F64], TTFORM_WARPS * 32, 0, s>>>(
-                            tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), rt, om, M->mr_part,
-                            alpha, add);
+                const QTTPack* qp = static_cast<const QTTPack*>(tp.chunks);
+                constexpr int TW = TTFORM_WARPS;
+                for (int rt = 0; rt < MR_RB; rt += MR_TB) {
+                    if (M->precision == HLRC_PREC_F64) {
+                        if (tp.nsegs[FMT_F64] > 0)
+                            k_ttform_f64_mr<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
+                                tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), rt, om,
+                                M->mr_part, alpha, add);
+                        continue;
+                    }
+                    if (tp.nsegs[FMT_F32] > 0)
+                        k_ttform_q_mr<TW, FMT_F32><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(
+                            tp.segs[FMT_F32], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                    if (tp.nsegs[FMT_F16] > 0)
+                        k_ttform_q_mr<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(
+                            tp.segs[FMT_F16], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                    if (tp.nsegs[FMT_BF16] > 0)
+                        k_ttform_q_mr<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(
+                            tp.segs[FMT_BF16], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                }
                 if (tp.ngroups > 0)
                     k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om, alpha,
                                                                           add);
                 if (ws_profile(M)) prof_end(M, s);
+                HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));
             } else if (st.kind == 1) {
                 const DevNPass& np = M->n[size_t(st.idx)];
-                if (np.nsegs[FMT_F64] == 0) continue;
+                if (np.launches() == 0) continue;
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
-                k_nform_f64_mr<NFORM_WARPS><<<np.nsegs[FMT_F64], NFORM_WARPS * 32, 0, s>>>(
-                    np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), omap(np.out),
-                    alpha, np.mode == OUT_ADD_ALPHA);
+                const int add = np.mode == OUT_ADD_ALPHA;
+                const OutMap om = omap(np.out);
+                const QNPack* qp = static_cast<const QNPack*>(np.chunks);
+                constexpr int NW = NFORM_WARPS;
+                const bool f64plan = M->precision == HLRC_PREC_F64;
+                if (f64plan && np.nsegs[FMT_F64] > 0)
+                    k_nform_f64_mr<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
+                        np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
+                        add);
+                if (!f64plan && np.nsegs[FMT_F32] > 0)
+                    k_nform_q_mr<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(
+                        np.segs[FMT_F32], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                if (!f64plan && np.nsegs[FMT_F16] > 0)
+                    k_nform_q_mr<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(
+                        np.segs[FMT_F16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                if (!f64plan && np.nsegs[FMT_BF16] > 0)
+                    k_nform_q_mr<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(
+                        np.segs[FMT_BF16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (ws_profile(M)) prof_end(M, s);
+                HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
             }
         }
     }
@@ -609,6 +678,46 @@ extern "C" hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options
     if (opts) o = *opts; else hlrc_default_options(&o);
     Plan p;
     hlrc_status st = plan_h(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    return upload_plan(p, o, out);
+}
+
+extern "C" hlrc_status hlrc_upload_h_batch(const hlrc_h_desc* descs, int count, const int64_t* offsets,
+                                           const hlrc_options* opts, hlrc_hmat* out) {
+    clear_error();
+    if (!descs || !offsets || !out || count < 1) return fail(HLRC_ERR_ARG, "hlrc_upload_h_batch: bad argument");
+    *out = nullptr;
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    std::vector<hlrc_block> all;
+    double area = 0;
+    for (int i = 0; i < count; ++i) {
+        const hlrc_h_desc& d = descs[i];
+        if (d.nrows != d.ncols) return fail(HLRC_ERR_SHAPE, "batch member %d is not square", i);
+        if (offsets[i] < 0 || offsets[i] + d.nrows > offsets[i + 1])
+            return fail(HLRC_ERR_SHAPE, "batch member %d does not fit between offsets %lld and %lld", i,
+                        (long long)offsets[i], (long long)offsets[i + 1]);
+        if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "batch member %d: blocks == NULL", i);
+        double a = 0;
+        for (int64_t b = 0; b < d.nblocks; ++b) {
+            hlrc_block blk = d.blocks[b];
+            if (blk.row0 < 0 || blk.col0 < 0 || blk.nrows < 0 || blk.ncols < 0 || blk.row0 + blk.nrows > d.nrows ||
+                blk.col0 + blk.ncols > d.ncols)
+                return fail(HLRC_ERR_SHAPE, "batch member %d, block %lld: index set outside the member", i,
+                            (long long)b);
+            a += double(blk.nrows) * double(blk.ncols);
+            blk.row0 += offsets[i];
+            blk.col0 += offsets[i];
+            all.push_back(blk);
+        }
+        if (a != double(d.nrows) * double(d.ncols))
+            return fail(HLRC_ERR_SHAPE, "batch member %d: leaves cover %.0f of %.0f entries", i, a,
+                        double(d.nrows) * double(d.ncols));
+        area += a;
+    }
+    const hlrc_h_desc cd{offsets[count], offsets[count], int64_t(all.size()), all.data()};
+    Plan p;
+    hlrc_status st = plan_h(cd, o, p, area);
     if (st != HLRC_OK) return st;
     return upload_plan(p, o, out);
 }

@@ -448,7 +448,10 @@ std::vector<int64_t> inner_cuts(const Tiles& tc, int64_t col0, int64_t ncols) {
 // VALR column precisions (compress/valr.hh:402-510): delta = eps sigma_0,
 // tol from  Sigma_l 1/sigma_l tol^2 - tol + delta = 0 (smaller root),
 // u_l = tol / sigma_l; a column may use the cheapest format whose unit
-// roundoff is <= u_l.
+// roundoff is <= u_l.  Reduced-precision stores hold FP32 and FP16 only:
+// columns whose u_l asks for more than FP32 (possible when the block's
+// singular values span many orders of magnitude and the quadratic's root is
+// clamped) are stored in FP32.
 void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt) {
     if (k <= 0) return;
     const double delta = eps * sv[0];
@@ -462,8 +465,71 @@ void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt) {
     }
     for (int64_t l = 0; l < k; ++l) {
         const double u = sv[l] > 0 ? tol / sv[l] : 1.0;
-        fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : (u >= 0x1.0p-24 ? FMT_F32 : FMT_F64);
+        fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : FMT_F32;
     }
+}
+
+// Checks every descriptor of the N-form and tile-T-form passes against the
+// store, the vector lengths and the alignment the kernels rely on (16-byte
+// chunk starts; columns of pad_fmt(rows, fmt) elements; lane pairs inside
+// the padded column).  A violation is a planner bug: the upload is refused
+// instead of handing the GPU an out-of-bounds address.
+hlrc_status validate_plan(const Plan& p) {
+    const int64_t store = int64_t(p.store.size());
+    auto vec_len = [&](int name) -> int64_t {
+        switch (name) {
+            case V_X: return std::max(p.nrows, p.ncols);
+            case V_Y: return std::max(p.nrows, p.ncols);
+            case V_T: return p.n_t;
+            default: return p.n_t2;
+        }
+    };
+    auto chunk_ok = [&](const GChunk& c, int64_t rows) -> bool {
+        if (c.nc == 0 || rows <= 0 || rows > TILE) return false;
+        if (c.byte_off % 16 != 0) return false;
+        const int64_t ld = pad_fmt(rows, c.fmt);
+        return int64_t(c.byte_off) + ld * c.nc * fmt_bytes(c.fmt) <= store;
+    };
+    for (size_t pi = 0; pi < p.npasses.size(); ++pi) {
+        const NPass& np = p.npasses[pi];
+        for (int f = 0; f < 4; ++f)
+            for (const NSeg& s : np.segs[f]) {
+                if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > np.chunks.size())
+                    return fail(HLRC_ERR_INTERNAL, "N-pass %zu: bad segment", pi);
+                if (int64_t(s.out) + s.rows > vec_len(np.out))
+                    return fail(HLRC_ERR_INTERNAL, "N-pass %zu: output tile outside the vector", pi);
+                for (uint32_t c = s.cb; c < s.ce; ++c) {
+                    const GChunk& g = np.chunks[c];
+                    if (g.fmt != f || !chunk_ok(g, s.rows))
+                        return fail(HLRC_ERR_INTERNAL, "N-pass %zu: chunk %u outside the store or misaligned", pi, c);
+                    const bool t = (g.vo & VEC_T) != 0;
+                    if (int64_t(g.vo & ~VEC_T) + g.nc > vec_len(t ? np.vt : np.vx))
+                        return fail(HLRC_ERR_INTERNAL, "N-pass %zu: chunk %u vector outside its array", pi, c);
+                }
+            }
+    }
+    for (size_t pi = 0; pi < p.ttpasses.size(); ++pi) {
+        const TTPass& tp = p.ttpasses[pi];
+        for (int f = 0; f < 4; ++f)
+            for (const TTSeg& s : tp.segs[f]) {
+                if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > tp.chunks.size())
+                    return fail(HLRC_ERR_INTERNAL, "T-pass %zu: bad segment", pi);
+                if (int64_t(s.v_off) + s.rows > vec_len(tp.in))
+                    return fail(HLRC_ERR_INTERNAL, "T-pass %zu: input tile outside the vector", pi);
+                for (uint32_t c = s.cb; c < s.ce; ++c) {
+                    const GChunk& g = tp.chunks[c];
+                    if (g.fmt != f || !chunk_ok(g, s.rows))
+                        return fail(HLRC_ERR_INTERNAL, "T-pass %zu: chunk %u outside the store or misaligned", pi, c);
+                    const int64_t lim = (g.flags & TT_DIRECT) ? vec_len(tp.out) : tp.npart;
+                    if (int64_t(g.vo) + g.nc > lim)
+                        return fail(HLRC_ERR_INTERNAL, "T-pass %zu: chunk %u output outside its array", pi, c);
+                }
+            }
+        for (const TGroup& g : tp.groups)
+            if (int64_t(g.slot0) + int64_t(g.nslots) * g.nc > tp.npart || int64_t(g.out) + g.nc > vec_len(tp.out))
+                return fail(HLRC_ERR_INTERNAL, "T-pass %zu: finish group outside its arrays", pi);
+    }
+    return HLRC_OK;
 }
 
 uint8_t default_format(int prec) {
@@ -478,7 +544,7 @@ uint8_t default_format(int prec) {
 }  // namespace
 
 // --------------------------------------------------------------------- H
-hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
+hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area) {
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0) return fail(HLRC_ERR_SHAPE, "negative matrix size");
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
@@ -517,9 +583,9 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
         ccuts.push_back(b.col0);
         ccuts.push_back(b.col0 + b.ncols);
     }
-    if (area != double(d.nrows) * double(d.ncols))
-        return fail(HLRC_ERR_SHAPE, "leaf blocks cover %.0f entries, matrix has %.0f (gap or overlap)", area,
-                    double(d.nrows) * double(d.ncols));
+    const double want = expected_area >= 0 ? expected_area : double(d.nrows) * double(d.ncols);
+    if (area != want)
+        return fail(HLRC_ERR_SHAPE, "leaf blocks cover %.0f entries, matrix has %.0f (gap or overlap)", area, want);
     const Tiles tr = make_tiles(d.nrows, rcuts), tc = make_tiles(d.ncols, ccuts);
     p.n_row_tiles = tr.n();
     p.n_col_tiles = tc.n();
@@ -600,6 +666,11 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
         }
     if (st.bytes >= (int64_t(1) << 36) && o.precision != HLRC_PREC_F64)
         return fail(HLRC_ERR_SHAPE, "reduced-precision store above 64 GiB");
+    // FP64 plans hold FP64 chunks only, reduced-precision plans none: the two
+    // kinds use different device descriptors
+    for (const SChunk& ch : st.chunks)
+        if ((ch.fmt == FMT_F64) != (o.precision == HLRC_PREC_F64))
+            return fail(HLRC_ERR_INTERNAL, "chunk format %d in a plan of precision %d", ch.fmt, o.precision);
     st.fill(p.store);
     for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
@@ -689,6 +760,8 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p) {
     p.stages[HLRC_OP_C] = p.stages[HLRC_OP_T];
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
+
+    if (hlrc_status vs = validate_plan(p); vs != HLRC_OK) return vs;
 
     // accounting (arith/mulvec.hh:795-874)
     double flops = 0;
@@ -947,6 +1020,8 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     p.stages[HLRC_OP_C] = {{2, 1}, {0, 0}, {1, 2}, {2, 2}};
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
+
+    if (hlrc_status vs = validate_plan(p); vs != HLRC_OK) return vs;
 
     // accounting (arith/uniform.hh:285-325)
     double flops = 0, mbytes = 0, cbbytes = 0, rbbytes = 0;

@@ -95,8 +95,10 @@ struct Plan {
     int64_t fmt_bytes[4] = {0, 0, 0, 0};  // stored bytes per StoreFmt (accounting of mixed precision)
 };
 
-// Returns HLRC_OK or an error (message recorded via fail()).
-hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p);
+// Returns HLRC_OK or an error (message recorded via fail()).  expected_area
+// is the number of entries the leaves must cover (< 0: nrows * ncols; a
+// batch passes the sum over its members).
+hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area = -1.0);
 hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan& p);
 
 }  // namespace hlrc

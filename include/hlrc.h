@@ -185,6 +185,17 @@ void        hlrc_default_options(hlrc_options* opts);
 hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options* opts,
                           hlrc_hmat* out);
 
+/* Batch of `count` H-matrices as one handle: member i occupies rows and
+ * columns [offsets[i], offsets[i] + n_i) of a block-diagonal matrix of size
+ * offsets[count] (offsets may leave gaps, e.g. to pad every member to the
+ * same length).  Every pass of the product then runs as one launch over the
+ * blocks of all members, so x and y are the concatenations of the members'
+ * vectors.  No counterpart in the reference (which multiplies one matrix
+ * per call); each member is checked like hlrc_upload_h.                     */
+hlrc_status hlrc_upload_h_batch(const hlrc_h_desc* descs, int count,
+                                const int64_t* offsets,
+                                const hlrc_options* opts, hlrc_hmat* out);
+
 /* Same for a uniform-H matrix (row/column cluster bases + couplings).        */
 hlrc_status hlrc_upload_uniform(const hlrc_uniform_desc* desc,
                                 const hlrc_options* opts, hlrc_hmat* out);

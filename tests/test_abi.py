@@ -112,6 +112,24 @@ def test_rejects_out_of_range_and_bad_args():
     assert L.hlrc_free(None) == 0
 
 
+def test_batch_upload_validates_members_before_any_device_work():
+    L = _capi.lib()
+    a, b = _ll_desc(8), _ll_desc(8)
+    da, db = a.h_desc(), b.h_desc()
+    arr = (_capi.hlrc_h_desc * 2)(da, db)
+    out = C.c_void_p()
+    overlap = (C.c_int64 * 3)(0, 4, 12)   # member 0 (n = 8) does not fit in [0, 4)
+    assert L.hlrc_upload_h_batch(arr, 2, overlap, None, C.byref(out)) == 2
+    assert b"does not fit" in L.hlrc_last_error()
+    ll = hlr.LeafList(8, 8)
+    ll.add_dense(0, 0, np.ones((8, 4)))  # member with a gap
+    arr2 = (_capi.hlrc_h_desc * 2)(da, ll.h_desc())
+    offs = (C.c_int64 * 3)(0, 8, 16)
+    assert L.hlrc_upload_h_batch(arr2, 2, offs, None, C.byref(out)) == 2
+    assert b"cover" in L.hlrc_last_error()
+    assert L.hlrc_upload_h_batch(arr, 0, offs, None, C.byref(out)) == 1
+
+
 def test_uniform_basis_mismatch_is_rejected(c3_small):
     u = c3_small.uniform_desc()
     # find an admissible block and corrupt its basis index

@@ -26,6 +26,14 @@ def test_mixed_eps_controls_the_mix(c2_small):
         hlr.plan_info(c2_small, precision="mixed", mixed_eps=0.0)
 
 
+def test_mixed_store_never_holds_fp64_columns(c2_small):
+    """A tolerance so tight that some columns would want more than FP32
+    still gives an all-FP32 store: reduced-precision plans carry packed
+    descriptors only, which FP64 kernels must never see."""
+    tight = hlr.plan_info(c2_small, precision="mixed", mixed_eps=1e-14)["matrix_bytes"]
+    assert tight == hlr.plan_info(c2_small, precision="f32")["matrix_bytes"]
+
+
 def test_uniform_is_fp64_only(c3_small):
     with pytest.raises(hlr.HLRCError) as e:
         hlr.plan_info(c3_small, uniform=True, precision="f32")
