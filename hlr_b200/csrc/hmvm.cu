@@ -22,6 +22,7 @@
 #include "kernels_f64.cuh"
 #include "kernels_mr.cuh"
 #include "kernels_q.cuh"
+#include "kernels_tc.cuh"
 #include "plan.hpp"
 
 namespace hlrc {
@@ -577,9 +578,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
         for (const Stage& st : M->stages[op]) {
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
-                int nf = 0;
-                for (int f = 0; f < 4; ++f) nf += tp.nsegs[f] > 0 ? 1 : 0;
-                M->launches += nf * (MR_RB / MR_TB) + (tp.ngroups > 0 ? 1 : 0);
+                M->launches += M->tt[size_t(st.idx)].launches();
             } else if (st.kind == 1) {
                 M->launches += M->n[size_t(st.idx)].launches();
             }
@@ -600,23 +599,21 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
                 const QTTPack* qp = static_cast<const QTTPack*>(tp.chunks);
                 constexpr int TW = TTFORM_WARPS;
-                for (int rt = 0; rt < MR_RB; rt += MR_TB) {
-                    if (M->precision == HLRC_PREC_F64) {
-                        if (tp.nsegs[FMT_F64] > 0)
-                            k_ttform_f64_mr<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
-                                tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), rt, om,
-                                M->mr_part, alpha, add);
-                        continue;
-                    }
+                if (M->precision == HLRC_PREC_F64) {
+                    if (tp.nsegs[FMT_F64] > 0)
+                        k_ttform_dmma<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
+                            tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, M->mr_part,
+                            alpha, add);
+                } else {
                     if (tp.nsegs[FMT_F32] > 0)
-                        k_ttform_q_mr<TW, FMT_F32><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(
-                            tp.segs[FMT_F32], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                        k_ttform_tc32<TW><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(
+                            tp.segs[FMT_F32], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                     if (tp.nsegs[FMT_F16] > 0)
-                        k_ttform_q_mr<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(
-                            tp.segs[FMT_F16], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                        k_ttform_tc<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(
+                            tp.segs[FMT_F16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                     if (tp.nsegs[FMT_BF16] > 0)
-                        k_ttform_q_mr<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(
-                            tp.segs[FMT_BF16], qp, M->store, vec(tp.in), rt, om, M->mr_part, alpha, add);
+                        k_ttform_tc<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(
+                            tp.segs[FMT_BF16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                 }
                 if (tp.ngroups > 0)
                     k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om, alpha,
@@ -633,17 +630,17 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 constexpr int NW = NFORM_WARPS;
                 const bool f64plan = M->precision == HLRC_PREC_F64;
                 if (f64plan && np.nsegs[FMT_F64] > 0)
-                    k_nform_f64_mr<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
+                    k_nform_dmma<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
                 if (!f64plan && np.nsegs[FMT_F32] > 0)
-                    k_nform_q_mr<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(
+                    k_nform_tc32<NW><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(
                         np.segs[FMT_F32], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nsegs[FMT_F16] > 0)
-                    k_nform_q_mr<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(
+                    k_nform_tc<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(
                         np.segs[FMT_F16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nsegs[FMT_BF16] > 0)
-                    k_nform_q_mr<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(
+                    k_nform_tc<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(
                         np.segs[FMT_BF16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (ws_profile(M)) prof_end(M, s);
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));

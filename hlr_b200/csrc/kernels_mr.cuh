@@ -1,5 +1,7 @@
-// Multi-right-hand-side FP64 kernels: the matrix is streamed once per block
-// of RB right-hand sides instead of once per vector.
+// Multi-right-hand-side products: the matrix is streamed once per block of
+// MR_RB right-hand sides instead of once per vector.  This file holds the
+// block layout helpers, the partial-sum finish and the FP64 kernels (FP64
+// tensor cores); the reduced-precision kernels are in kernels_tc.cuh.
 //
 // Vector operands are row-major blocks (entry (i, r) at i * RB + r), so the
 // RB values that multiply one matrix column are contiguous: the caller's
@@ -9,8 +11,6 @@
 // coefficients or the caller's column-major Y.
 #pragma once
 
-#include <cuda_bf16.h>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "kernels_f64.cuh"
@@ -18,8 +18,7 @@
 
 namespace hlrc {
 
-constexpr int MR_RB = 8;   // right-hand sides per block (N-form, finish, workspaces)
-constexpr int MR_TB = 4;   // right-hand sides per tile T-form launch
+constexpr int MR_RB = 8;   // right-hand sides per block (kernels, finish, workspaces)
 
 // xr[i * RB + r] = X[i + (r0 + r) * ldx] for r < nr, 0 for nr <= r < RB
 __global__ void k_rows_from_cols(const double* __restrict__ X, int64_t ldx, int64_t n, int r0, int nr,
@@ -36,106 +35,6 @@ struct OutMap {            // output element (i, r) lives at base[i * rs + r * c
     int64_t rs, cs;
     int nr;                // valid right-hand sides
 };
-
-// N-form, RB right-hand sides: one CTA per output tile, lane owns rows
-// 2l, 2l+1 for all RB vectors; fixed-order cross-warp sum in shared memory.
-template <int W>
-__global__ void __launch_bounds__(W * 32)
-k_nform_f64_mr(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, const double* __restrict__ A,
-               const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
-    constexpr int RB = MR_RB;
-    __shared__ double red[W][TILE][RB];
-    const NSeg sg = segs[blockIdx.x];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = 2 * lane;
-    const bool active = r < sg.ld;
-    double acc0[RB], acc1[RB];
-#pragma unroll
-    for (int k = 0; k < RB; ++k) acc0[k] = acc1[k] = 0.0;
-    for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const NChunk ch = chunks[c];
-        const double* v = (ch.v_off & VEC_T) ? vt + size_t(ch.v_off & ~VEC_T) * RB : vx + size_t(ch.v_off) * RB;
-        const double* a = A + ch.a_off + r;
-        double2 m[NCHUNK];
-#pragma unroll
-        for (int j = 0; j < NCHUNK; ++j)
-            m[j] = (active && j < ch.nc) ? ld_stream(a + size_t(j) * sg.ld) : make_double2(0.0, 0.0);
-#pragma unroll
-        for (int j = 0; j < NCHUNK; ++j) {
-            if (j >= ch.nc) break;
-            const double2* vj = reinterpret_cast<const double2*>(v + size_t(j) * RB);
-#pragma unroll
-            for (int k = 0; k < RB / 2; ++k) {
-                const double2 w = __ldg(vj + k);
-                acc0[2 * k] = fma(m[j].x, w.x, acc0[2 * k]);
-                acc0[2 * k + 1] = fma(m[j].x, w.y, acc0[2 * k + 1]);
-                acc1[2 * k] = fma(m[j].y, w.x, acc1[2 * k]);
-                acc1[2 * k + 1] = fma(m[j].y, w.y, acc1[2 * k + 1]);
-            }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < RB; ++k) {
-        red[warp][r][k] = acc0[k];
-        red[warp][r + 1][k] = acc1[k];
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < TILE * RB; t += W * 32) {
-        const int row = t % TILE, k = t / TILE;
-        if (row >= sg.rows || k >= om.nr) continue;
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) s += red[w][row][k];
-        double* o = om.base + int64_t(sg.out + row) * om.rs + int64_t(k) * om.cs;
-        if (add) *o += alpha * s;
-        else *o = s;
-    }
-}
-
-// Tile T-form for MR_TB right-hand sides r0 .. r0+3 of the row-major input
-// (stride MR_RB): 8 columns x 4 vectors = 32 partials per lane, one
-// transpose-reduction, lane l then holds (column l / 4, vector l % 4).
-template <int W>
-__global__ void __launch_bounds__(W * 32)
-k_ttform_f64_mr(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks, const double* __restrict__ A,
-                const double* __restrict__ vin, int r0, OutMap om, double* __restrict__ part, double alpha,
-                int add) {
-    constexpr int TB = MR_TB;
-    const TTSeg sg = segs[blockIdx.x];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = 2 * lane;
-    const bool active = r < sg.ld;
-    double x0[TB], x1[TB];
-#pragma unroll
-    for (int k = 0; k < TB; ++k) {
-        x0[k] = r < sg.rows ? __ldg(vin + size_t(sg.v_off + r) * MR_RB + r0 + k) : 0.0;
-        x1[k] = r + 1 < sg.rows ? __ldg(vin + size_t(sg.v_off + r + 1) * MR_RB + r0 + k) : 0.0;
-    }
-    for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const TTChunk ch = chunks[c];
-        const double* a = A + ch.a_off + r;
-        double2 m[TCOLS];
-#pragma unroll
-        for (int j = 0; j < TCOLS; ++j)
-            m[j] = (active && j < ch.nc) ? ld_stream(a + size_t(j) * sg.ld) : make_double2(0.0, 0.0);
-        double p[TCOLS * TB];
-#pragma unroll
-        for (int j = 0; j < TCOLS; ++j)
-#pragma unroll
-            for (int k = 0; k < TB; ++k) p[j * TB + k] = fma(m[j].y, x1[k], m[j].x * x0[k]);
-        TransposeReduce<TCOLS * TB, 16>::run(p, lane);
-        const int j = lane / TB, k = lane % TB;
-        if (j < ch.nc && r0 + k < om.nr) {
-            if (ch.flags & TT_DIRECT) {
-                double* o = om.base + int64_t(ch.out + j) * om.rs + int64_t(r0 + k) * om.cs;
-                if (add) *o += alpha * p[0];
-                else *o = p[0];
-            } else {
-                part[size_t(ch.out + j) * MR_RB + r0 + k] = p[0];
-            }
-        }
-    }
-}
 
 // Sums per-tile partials (row-major, MR_RB vectors) of multi-tile outputs.
 __global__ void __launch_bounds__(256)
@@ -164,83 +63,65 @@ k_ttfinish_f64_mr(const TGroup* __restrict__ groups, int ngroups, const double* 
     }
 }
 
-// ------------------------------------------------- reduced-precision stores
-// Multi-RHS kernels for FP32 / scaled 16-bit stores: lane owns rows 2l, 2l+1
-// (a pair load of 8 or 4 bytes), products and sums inside a chunk in FP32,
-// chunk results accumulated in FP64.  Work items are the stores' packs (up
-// to two chunks each).
+// ------------------------------------------------------ FP64 tensor cores
+// The same two forms on FP64 tensor cores (mma.sync m8n8k4, FP64 products
+// and sums), all MR_RB vectors in one launch.  A lane's 16-byte load is two
+// consecutive rows of one column; the contraction / output rows of the MMA
+// are mapped onto them as follows.
+//   N-form: contraction = chunk columns 4kt + t; m-tile i = 2p + b takes
+//     tile row 16p + 2g + b as its fragment row g.
+//   tile T-form: contraction = tile rows, k-step s = 2j + b maps fragment
+//     k = t to row 8j + 2t + b; the output rows are the chunk's 8 columns.
 
-// rows r, r+1 of a column (r even: the pair is aligned to two elements)
-template <int FMT>
-__device__ __forceinline__ float2 ld_pair(const uint8_t* col, int r) {
-    if constexpr (FMT == FMT_F32) {
-        return __ldcs(reinterpret_cast<const float2*>(col) + (r >> 1));
-    } else if constexpr (FMT == FMT_F16) {
-        const unsigned u = __ldcs(reinterpret_cast<const unsigned*>(col) + (r >> 1));
-        __half2 h;
-        memcpy(&h, &u, 4);
-        return __half22float2(h);
-    } else {
-        const unsigned u = __ldcs(reinterpret_cast<const unsigned*>(col) + (r >> 1));
-        return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
-    }
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
 }
 
-template <int W, int FMT>
+template <int W>
 __global__ void __launch_bounds__(W * 32)
-k_nform_q_mr(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
+k_nform_dmma(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, const double* __restrict__ A,
              const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
-    constexpr int RB = MR_RB;
-    __shared__ double red[W][TILE][RB];
+    __shared__ double red[W][TILE][MR_RB];
     const NSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = 2 * lane;
-    const bool active = r < sg.ld;
-    const size_t colb = size_t(sg.ld) * fmt_bytes(FMT);
-    double acc0[RB], acc1[RB];
+    const int g = lane >> 2, t = lane & 3;
+    // acc[2p + b]: tile row 16p + 2g + b, right-hand sides 2t, 2t+1
+    double acc[8][2];
 #pragma unroll
-    for (int k = 0; k < RB; ++k) acc0[k] = acc1[k] = 0.0;
+    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
     for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const QNPack pk = packs[c];
+        const NChunk ch = chunks[c];
+        const double* v = (ch.v_off & VEC_T) ? vt + size_t(ch.v_off & ~VEC_T) * MR_RB : vx + size_t(ch.v_off) * MR_RB;
+        const double* a = A + ch.a_off;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const QNChunk& part = pk.p[q];
-            if (part.nc == 0) continue;
-            const uint8_t* a = A + size_t(part.a16) * 16;
-            const double* v = (part.v_off & VEC_T) ? vt + size_t(part.v_off & ~VEC_T) * RB
-                                                   : vx + size_t(part.v_off) * RB;
-            float s0[RB], s1[RB];
+        for (int kt = 0; kt < 2; ++kt) {
+            const int col = 4 * kt + t;
+            const bool okc = col < ch.nc;
+            const double b = okc ? __ldg(v + size_t(col) * MR_RB + g) : 0.0;
+            double2 m[4];
 #pragma unroll
-            for (int k = 0; k < RB; ++k) s0[k] = s1[k] = 0.f;
-            for (int j = 0; j < part.nc; ++j) {
-                const float2 m = active ? ld_pair<FMT>(a + size_t(j) * colb, r) : make_float2(0.f, 0.f);
-                const double2* vj = reinterpret_cast<const double2*>(v + size_t(j) * RB);
-#pragma unroll
-                for (int k = 0; k < RB / 2; ++k) {
-                    const double2 w = __ldg(vj + k);
-                    const float w0 = float(w.x), w1 = float(w.y);
-                    s0[2 * k] = fmaf(m.x, w0, s0[2 * k]);
-                    s0[2 * k + 1] = fmaf(m.x, w1, s0[2 * k + 1]);
-                    s1[2 * k] = fmaf(m.y, w0, s1[2 * k]);
-                    s1[2 * k + 1] = fmaf(m.y, w1, s1[2 * k + 1]);
-                }
+            for (int p = 0; p < 4; ++p) {
+                const int row = 16 * p + 2 * g;
+                m[p] = (okc && row < sg.ld) ? ld_stream(a + size_t(col) * sg.ld + row) : make_double2(0.0, 0.0);
             }
-            const double sc = part.scale;
 #pragma unroll
-            for (int k = 0; k < RB; ++k) {
-                acc0[k] = fma(sc, double(s0[k]), acc0[k]);
-                acc1[k] = fma(sc, double(s1[k]), acc1[k]);
+            for (int p = 0; p < 4; ++p) {
+                dmma(acc[2 * p], m[p].x, b);
+                dmma(acc[2 * p + 1], m[p].y, b);
             }
         }
     }
 #pragma unroll
-    for (int k = 0; k < RB; ++k) {
-        red[warp][r][k] = acc0[k];
-        red[warp][r + 1][k] = acc1[k];
+    for (int i = 0; i < 8; ++i) {
+        const int row = 16 * (i >> 1) + 2 * g + (i & 1);
+        red[warp][row][2 * t] = acc[i][0];
+        red[warp][row][2 * t + 1] = acc[i][1];
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < TILE * RB; t += W * 32) {
-        const int row = t % TILE, k = t / TILE;
+    for (int i = threadIdx.x; i < TILE * MR_RB; i += W * 32) {
+        const int row = i % TILE, k = i / TILE;
         if (row >= sg.rows || k >= om.nr) continue;
         double s = 0.0;
 #pragma unroll
@@ -251,50 +132,49 @@ k_nform_q_mr(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, co
     }
 }
 
-template <int W, int FMT>
+template <int W>
 __global__ void __launch_bounds__(W * 32)
-k_ttform_q_mr(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, const uint8_t* __restrict__ A,
-              const double* __restrict__ vin, int r0, OutMap om, double* __restrict__ part, double alpha, int add) {
-    constexpr int TB = MR_TB;
+k_ttform_dmma(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks, const double* __restrict__ A,
+              const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
     const TTSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = 2 * lane;
-    const bool active = r < sg.ld;
-    const size_t colb = size_t(sg.ld) * fmt_bytes(FMT);
-    float x0[TB], x1[TB];
+    const int g = lane >> 2, t = lane & 3;
+    // x of the lane: rows 8j + 2t + b (j < 8, b < 2), right-hand side g
+    double xv[16];
 #pragma unroll
-    for (int k = 0; k < TB; ++k) {
-        x0[k] = r < sg.rows ? float(__ldg(vin + size_t(sg.v_off + r) * MR_RB + r0 + k)) : 0.f;
-        x1[k] = r + 1 < sg.rows ? float(__ldg(vin + size_t(sg.v_off + r + 1) * MR_RB + r0 + k)) : 0.f;
-    }
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int row = 8 * j + 2 * t + b;
+            xv[2 * j + b] = row < sg.rows ? __ldg(vin + size_t(sg.v_off + row) * MR_RB + g) : 0.0;
+        }
     for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const QTTPack pk = packs[c];
+        const TTChunk ch = chunks[c];
+        const bool okc = g < ch.nc;
+        const double* a = A + ch.a_off + size_t(g) * sg.ld;
+        double2 m[8];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const QTTChunk& ch = pk.p[q];
-            for (int j0 = 0; j0 < ch.nc; j0 += TCOLS) {
-                const uint8_t* a = A + size_t(ch.a16) * 16 + size_t(j0) * colb;
-                float2 m[TCOLS];
+        for (int j = 0; j < 8; ++j) {
+            const int row = 8 * j + 2 * t;
+            m[j] = (okc && row < sg.ld) ? ld_stream(a + row) : make_double2(0.0, 0.0);
+        }
+        double d[2] = {0.0, 0.0};
 #pragma unroll
-                for (int j = 0; j < TCOLS; ++j)
-                    m[j] = (active && j0 + j < ch.nc) ? ld_pair<FMT>(a + size_t(j) * colb, r) : make_float2(0.f, 0.f);
-                float p[TCOLS * TB];
+        for (int j = 0; j < 8; ++j) {
+            dmma(d, m[j].x, xv[2 * j]);
+            dmma(d, m[j].y, xv[2 * j + 1]);
+        }
+        // d[e]: chunk column g, right-hand side 2t + e
 #pragma unroll
-                for (int j = 0; j < TCOLS; ++j)
-#pragma unroll
-                    for (int k = 0; k < TB; ++k) p[j * TB + k] = fmaf(m[j].y, x1[k], m[j].x * x0[k]);
-                TransposeReduce<TCOLS * TB, 16, float>::run(p, lane);
-                const int j = j0 + lane / TB, k = lane % TB;
-                if (j < ch.nc && r0 + k < om.nr) {
-                    const double val = double(ch.scale) * double(p[0]);
-                    if (ch.flags & TT_DIRECT) {
-                        double* o = om.base + int64_t(ch.out + j) * om.rs + int64_t(r0 + k) * om.cs;
-                        if (add) *o += alpha * val;
-                        else *o = val;
-                    } else {
-                        part[size_t(ch.out + j) * MR_RB + r0 + k] = val;
-                    }
-                }
+        for (int e = 0; e < 2; ++e) {
+            const int n = 2 * t + e;
+            if (!okc || n >= om.nr) continue;
+            if (ch.flags & TT_DIRECT) {
+                double* o = om.base + int64_t(ch.out + g) * om.rs + int64_t(n) * om.cs;
+                if (add) *o += alpha * d[e];
+                else *o = d[e];
+            } else {
+                part[size_t(ch.out + g) * MR_RB + n] = d[e];
             }
         }
     }
