@@ -265,12 +265,40 @@ std::vector<Seg> remap_segs(const std::vector<Seg>& segs, const std::vector<uint
     return r;
 }
 
+// The tensor-core kernels use more than 48 KB of dynamic shared memory;
+// the limit is raised once per device (the attribute belongs to the device
+// context that is current when it is set).
+hlrc_status enable_tc_smem(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_T16)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_T16)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_N16)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_N16)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_T32)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_N32)));
+    done.push_back(dev);
+    return HLRC_OK;
+}
+
 hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     auto h = std::make_unique<hlrc_hmat_s>();
     int dev = o.device;
     if (dev < 0) HLRC_CUDA(cudaGetDevice(&dev));
     DeviceGuard g(dev);
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", dev);
+    if (o.max_nrhs > 1 && p.precision != HLRC_PREC_F64) {
+        const hlrc_status st = enable_tc_smem(dev);
+        if (st != HLRC_OK) return st;
+    }
     h->device = dev;
     h->kind = p.kind;
     h->precision = p.precision;
@@ -606,19 +634,22 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                             alpha, add);
                 } else {
                     if (tp.nsegs[FMT_F32] > 0)
-                        k_ttform_tc32<TW><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(
+                        k_ttform_tc32<<<tp.nsegs[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
                             tp.segs[FMT_F32], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                     if (tp.nsegs[FMT_F16] > 0)
-                        k_ttform_tc<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(
+                        k_ttform_tc<FMT_F16><<<tp.nsegs[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
                             tp.segs[FMT_F16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                     if (tp.nsegs[FMT_BF16] > 0)
-                        k_ttform_tc<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(
+                        k_ttform_tc<FMT_BF16><<<tp.nsegs[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
                             tp.segs[FMT_BF16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                 }
-                if (tp.ngroups > 0)
-                    k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om, alpha,
-                                                                          add);
                 if (ws_profile(M)) prof_end(M, s);
+                if (tp.ngroups > 0) {
+                    if (ws_profile(M)) prof_begin(M, "ttfinish", tp.npart * 8 * MR_RB, s);
+                    k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om,
+                                                                          alpha, add);
+                    if (ws_profile(M)) prof_end(M, s);
+                }
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));
             } else if (st.kind == 1) {
                 const DevNPass& np = M->n[size_t(st.idx)];
@@ -634,13 +665,13 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
                 if (!f64plan && np.nsegs[FMT_F32] > 0)
-                    k_nform_tc32<NW><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(
+                    k_nform_tc32<<<np.nsegs[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
                         np.segs[FMT_F32], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nsegs[FMT_F16] > 0)
-                    k_nform_tc<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(
+                    k_nform_tc<FMT_F16><<<np.nsegs[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.segs[FMT_F16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nsegs[FMT_BF16] > 0)
-                    k_nform_tc<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(
+                    k_nform_tc<FMT_BF16><<<np.nsegs[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.segs[FMT_BF16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (ws_profile(M)) prof_end(M, s);
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));

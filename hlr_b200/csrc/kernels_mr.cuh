@@ -36,7 +36,10 @@ struct OutMap {            // output element (i, r) lives at base[i * rs + r * c
     int nr;                // valid right-hand sides
 };
 
-// Sums per-tile partials (row-major, MR_RB vectors) of multi-tile outputs.
+// Sums per-tile partials (row-major, MR_RB vectors) of multi-tile outputs:
+// slot i, column j, vector k of a group is part[(slot0 + i*nc + j)*MR_RB + k].
+// A lane owns a pair of vectors of one column and keeps four interleaved
+// sums (four 16-byte loads in flight), combined in a fixed order.
 __global__ void __launch_bounds__(256)
 k_ttfinish_f64_mr(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part, OutMap om,
                   double alpha, int add) {
@@ -44,22 +47,36 @@ k_ttfinish_f64_mr(const TGroup* __restrict__ groups, int ngroups, const double* 
     if (gid >= ngroups) return;
     const int lane = threadIdx.x & 31;
     const TGroup g = groups[gid];
-    const uint32_t n = g.nc * MR_RB;
-    for (uint32_t q = lane; q < n; q += 32) {
-        const uint32_t j = q / MR_RB, k = q % MR_RB;
-        if (int(k) >= om.nr) continue;
-        const double* p = part + size_t(g.slot0) * MR_RB + q;
-        double s0 = 0.0, s1 = 0.0;
+    constexpr uint32_t PAIRS = MR_RB / 2;
+    const uint32_t n2 = g.nc * PAIRS;
+    const double2* p0 = reinterpret_cast<const double2*>(part + size_t(g.slot0) * MR_RB);
+    for (uint32_t q = lane; q < n2; q += 32) {
+        const uint32_t j = q / PAIRS;
+        const int k = int(2 * (q % PAIRS));
+        if (k >= om.nr) continue;
+        const double2* p = p0 + q;
+        double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
         uint32_t i = 0;
-        for (; i + 2 <= g.nslots; i += 2) {
-            s0 += p[size_t(i) * n];
-            s1 += p[size_t(i + 1) * n];
+        for (; i + 4 <= g.nslots; i += 4) {
+            const double2 a = __ldcs(p + size_t(i) * n2), b = __ldcs(p + size_t(i + 1) * n2);
+            const double2 c = __ldcs(p + size_t(i + 2) * n2), d = __ldcs(p + size_t(i + 3) * n2);
+            s0.x += a.x; s0.y += a.y;
+            s1.x += b.x; s1.y += b.y;
+            s2.x += c.x; s2.y += c.y;
+            s3.x += d.x; s3.y += d.y;
         }
-        for (; i < g.nslots; ++i) s0 += p[size_t(i) * n];
-        const double s = s0 + s1;
+        for (; i < g.nslots; ++i) {
+            const double2 a = __ldcs(p + size_t(i) * n2);
+            s0.x += a.x; s0.y += a.y;
+        }
+        const double r0 = (s0.x + s1.x) + (s2.x + s3.x), r1 = (s0.y + s1.y) + (s2.y + s3.y);
         double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
-        if (add) *o += alpha * s;
-        else *o = s;
+        if (add) *o += alpha * r0;
+        else *o = r0;
+        if (k + 1 < om.nr) {
+            if (add) o[om.cs] += alpha * r1;
+            else o[om.cs] = r1;
+        }
     }
 }
 
@@ -79,8 +96,11 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
         : "d"(a), "d"(b));
 }
 
+// Both kernels keep two operand sets in registers: the loads of chunk
+// c + W are in flight while chunk c is multiplied, and chunk descriptors are
+// read two chunks ahead.
 template <int W>
-__global__ void __launch_bounds__(W * 32)
+__global__ void __launch_bounds__(W * 32, 2)
 k_nform_dmma(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, const double* __restrict__ A,
              const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     __shared__ double red[W][TILE][MR_RB];
@@ -91,26 +111,53 @@ k_nform_dmma(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, c
     double acc[8][2];
 #pragma unroll
     for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
-    for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const NChunk ch = chunks[c];
-        const double* v = (ch.v_off & VEC_T) ? vt + size_t(ch.v_off & ~VEC_T) * MR_RB : vx + size_t(ch.v_off) * MR_RB;
-        const double* a = A + ch.a_off;
+    // operands of one chunk: k-step kt = column 4kt + t; m[kt][p] = rows
+    // 16p + 2g, +1; b[kt] = vector entry of that column, right-hand side g
+    auto issue = [&](const NChunk& q, double2 (&m)[2][4], double (&b)[2]) {
+        const double* v = (q.v_off & VEC_T) ? vt + size_t(q.v_off & ~VEC_T) * MR_RB : vx + size_t(q.v_off) * MR_RB;
+        const double* a = A + q.a_off;
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
             const int col = 4 * kt + t;
-            const bool okc = col < ch.nc;
-            const double b = okc ? __ldg(v + size_t(col) * MR_RB + g) : 0.0;
-            double2 m[4];
+            const bool okc = col < q.nc;
+            b[kt] = okc ? __ldg(v + size_t(col) * MR_RB + g) : 0.0;
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
                 const int row = 16 * p + 2 * g;
-                m[p] = (okc && row < sg.ld) ? ld_stream(a + size_t(col) * sg.ld + row) : make_double2(0.0, 0.0);
+                m[kt][p] = (okc && row < sg.ld) ? ld_stream(a + size_t(col) * sg.ld + row) : make_double2(0.0, 0.0);
             }
+        }
+    };
+    auto compute = [&](const double2 (&m)[2][4], const double (&b)[2]) {
+#pragma unroll
+        for (int kt = 0; kt < 2; ++kt)
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
-                dmma(acc[2 * p], m[p].x, b);
-                dmma(acc[2 * p + 1], m[p].y, b);
+                dmma(acc[2 * p], m[kt][p].x, b[kt]);
+                dmma(acc[2 * p + 1], m[kt][p].y, b[kt]);
             }
+    };
+    uint32_t c = sg.cb + warp;
+    if (c < sg.ce) {
+        const NChunk none{0, 0, 0, 0};
+        double2 mA[2][4], mB[2][4];
+        double bA[2], bB[2];
+        issue(chunks[c], mA, bA);
+        NChunk qn = c + W < sg.ce ? chunks[c + W] : none;
+        for (;;) {
+            const bool hasB = c + W < sg.ce;
+            const NChunk qnn = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
+            if (hasB) issue(qn, mB, bB);
+            compute(mA, bA);
+            if (!hasB) break;
+            c += W;
+            const bool hasA = c + W < sg.ce;
+            const NChunk q3 = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
+            if (hasA) issue(qnn, mA, bA);
+            compute(mB, bB);
+            if (!hasA) break;
+            c += W;
+            qn = q3;
         }
     }
 #pragma unroll
@@ -133,7 +180,7 @@ k_nform_dmma(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, c
 }
 
 template <int W>
-__global__ void __launch_bounds__(W * 32)
+__global__ void __launch_bounds__(W * 32, 2)
 k_ttform_dmma(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks, const double* __restrict__ A,
               const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
     const TTSeg sg = segs[blockIdx.x];
@@ -148,16 +195,17 @@ k_ttform_dmma(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks
             const int row = 8 * j + 2 * t + b;
             xv[2 * j + b] = row < sg.rows ? __ldg(vin + size_t(sg.v_off + row) * MR_RB + g) : 0.0;
         }
-    for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
-        const TTChunk ch = chunks[c];
-        const bool okc = g < ch.nc;
-        const double* a = A + ch.a_off + size_t(g) * sg.ld;
-        double2 m[8];
+    // operands of one chunk: column g, rows 8j + 2t, +1
+    auto issue = [&](const TTChunk& q, double2 (&m)[8]) {
+        const bool okc = g < q.nc;
+        const double* a = A + q.a_off + size_t(g) * sg.ld;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int row = 8 * j + 2 * t;
             m[j] = (okc && row < sg.ld) ? ld_stream(a + row) : make_double2(0.0, 0.0);
         }
+    };
+    auto finish = [&](const TTChunk& q, const double2 (&m)[8]) {
         double d[2] = {0.0, 0.0};
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -168,15 +216,38 @@ k_ttform_dmma(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int n = 2 * t + e;
-            if (!okc || n >= om.nr) continue;
-            if (ch.flags & TT_DIRECT) {
-                double* o = om.base + int64_t(ch.out + g) * om.rs + int64_t(n) * om.cs;
+            if (g >= q.nc || n >= om.nr) continue;
+            if (q.flags & TT_DIRECT) {
+                double* o = om.base + int64_t(q.out + g) * om.rs + int64_t(n) * om.cs;
                 if (add) *o += alpha * d[e];
                 else *o = d[e];
             } else {
-                part[size_t(ch.out + g) * MR_RB + n] = d[e];
+                part[size_t(q.out + g) * MR_RB + n] = d[e];
             }
         }
+    };
+    uint32_t c = sg.cb + warp;
+    if (c >= sg.ce) return;
+    const TTChunk none{0, 0, 0, 0};
+    double2 mA[8], mB[8];
+    TTChunk qA = chunks[c];
+    issue(qA, mA);
+    TTChunk qB = c + W < sg.ce ? chunks[c + W] : none;
+    for (;;) {
+        const bool hasB = c + W < sg.ce;
+        const TTChunk qnn = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
+        if (hasB) issue(qB, mB);
+        finish(qA, mA);
+        if (!hasB) break;
+        c += W;
+        const bool hasA = c + W < sg.ce;
+        const TTChunk q3 = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
+        qA = qnn;
+        if (hasA) issue(qA, mA);
+        finish(qB, mB);
+        if (!hasA) break;
+        c += W;
+        qB = q3;
     }
 }
 
