@@ -220,6 +220,13 @@ class DeviceMatrix:
         """Kernels launched by this handle so far (hlrc_launch_count)."""
         return int(lib().hlrc_launch_count(self._h))
 
+    def device_error(self) -> int:
+        """Reads and clears the device error word (hlrc_check_device_error):
+        0, or the code of a bounded device wait that ran out."""
+        code = C.c_int(0)
+        check(lib().hlrc_check_device_error(self._h, C.byref(code)), "hlrc_check_device_error")
+        return int(code.value)
+
     def free(self) -> None:
         if self._h:
             lib().hlrc_free(self._h)

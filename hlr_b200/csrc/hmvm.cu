@@ -106,6 +106,7 @@ struct hlrc_hmat_s {
     double* hx = nullptr;
     double* hy = nullptr;
     size_t hx_elems = 0, hy_elems = 0;
+    int* dev_err = nullptr;   // device error word (bounded waits that ran out)
     int64_t launches = 0;     // kernels launched by this handle
     // profiling
     bool profiling = false;
@@ -153,7 +154,7 @@ struct ArenaLayout {
     size_t store = 0;
     std::vector<size_t> tu, ts, tg, nc, ttc, ttg;
     std::vector<std::array<size_t, 4>> ns, tts;   // per pass, per StoreFmt
-    size_t t = 0, t2 = 0, part = 0, total = 0;
+    size_t t = 0, t2 = 0, part = 0, err = 0, total = 0;
     size_t part_elems = 0;
 };
 
@@ -189,6 +190,7 @@ ArenaLayout arena_layout(const Plan& p) {
     L.t = take(size_t(std::max<int64_t>(1, p.n_t)) * sizeof(double));
     L.t2 = take(size_t(std::max<int64_t>(1, p.n_t2)) * sizeof(double));
     L.part = take(part_elems * sizeof(double));
+    L.err = take(sizeof(int));
     L.part_elems = part_elems;
     L.total = off;
     return L;
@@ -376,6 +378,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         d.in = tp.in; d.out = tp.out; d.mode = tp.mode; d.bytes = tp.bytes; d.alg_bytes = tp.alg_bytes;
         hp->tt.push_back(d);
     }
+    if (e == cudaSuccess) e = cudaMemset(hp->arena + L.err, 0, sizeof(int));
     if (e != cudaSuccess) {
         cleanup();
         return fail(HLRC_ERR_CUDA, "upload copy failed: %s", cudaGetErrorString(e));
@@ -392,6 +395,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     hp->ws_t = reinterpret_cast<double*>(hp->arena + o_t);
     hp->ws_t2 = reinterpret_cast<double*>(hp->arena + o_t2);
     hp->part = reinterpret_cast<double*>(hp->arena + o_part);
+    hp->dev_err = reinterpret_cast<int*>(hp->arena + L.err);
     for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
 
     fill_info(p, L, hp->info);
@@ -885,8 +889,13 @@ extern "C" int hlrc_last_profile(hlrc_hmat M, const char** names, int* count, do
 }
 
 extern "C" hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code) {
+    clear_error();
     if (!M || !code) return fail(HLRC_ERR_ARG, "hlrc_check_device_error: null argument");
     *code = 0;
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    HLRC_CUDA(cudaMemcpy(code, M->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+    HLRC_CUDA(cudaMemset(M->dev_err, 0, sizeof(int)));
     return HLRC_OK;
 }
 

@@ -214,20 +214,23 @@ __device__ __forceinline__ void warp_ring(const Pack* __restrict__ packs, uint32
 // 0, [nc0, nc0 + nc1) from part 1, zero-filled up to COLS.  A column holds
 // `units` 16-byte units (ld * element bytes / 16) at global stride `units`
 // and shared stride `stride`; UPL units make a full 64-row column, and lane
-// l copies unit l % UPL of columns l / UPL + (32 / UPL) i.
+// l copies unit l % UPL of columns l / UPL + (32 / UPL) i.  The parts are
+// selected through two base pointers (no indexing into the descriptor).
 template <int UPL, int COLS, typename Pack>
 __device__ __forceinline__ void stage_columns(uint8_t* dst, int stride, const uint8_t* A, const Pack& pk, int units,
                                               int lane) {
     const int u = lane % UPL;
     const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
+    const size_t cb = size_t(units) * 16;
+    const uint8_t* b0 = A + size_t(pk.p[0].a16) * 16 + u * 16;
+    const uint8_t* b1 = A + size_t(pk.p[1].a16) * 16 + u * 16 - size_t(n0) * cb;
+    uint8_t* d = dst + (lane / UPL) * stride + u * 16;
 #pragma unroll
     for (int i = 0; i < COLS * UPL / 32; ++i) {
         const int j = lane / UPL + (32 / UPL) * i;
-        const int q = j < n0 ? 0 : 1;
-        const int jc = j - (q ? n0 : 0);
         const bool ok = j < ntot && u < units;
-        const uint8_t* src = A + size_t(pk.p[q].a16) * 16 + (size_t(jc) * units + u) * 16;
-        cp16(dst + j * stride + u * 16, ok ? src : A, ok);
+        const uint8_t* src = (j < n0 ? b0 : b1) + size_t(j) * cb;
+        cp16(d + (32 / UPL) * i * stride, ok ? src : A, ok);
     }
 }
 
@@ -238,15 +241,17 @@ __device__ __forceinline__ void stage_vector(uint8_t* dst, const double* vx, con
                                              int lane) {
     const int u = lane & 3;
     const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
+    const uint32_t o0 = pk.p[0].v_off, o1 = pk.p[1].v_off;
+    const double* v0 = ((o0 & VEC_T) ? vt + size_t(o0 & ~VEC_T) * MR_RB : vx + size_t(o0) * MR_RB) + 2 * u;
+    const double* v1 = ((o1 & VEC_T) ? vt + size_t(o1 & ~VEC_T) * MR_RB : vx + size_t(o1) * MR_RB) + 2 * u -
+                       size_t(n0) * MR_RB;
+    uint8_t* d = dst + (lane >> 2) * TC_V_STRIDE + u * 16;
 #pragma unroll
     for (int i = 0; i < COLS / 8; ++i) {
         const int j = (lane >> 2) + 8 * i;
-        const int q = j < n0 ? 0 : 1;
-        const int jc = j - (q ? n0 : 0);
-        const uint32_t vo = pk.p[q].v_off;
-        const double* v = (vo & VEC_T) ? vt + size_t(vo & ~VEC_T) * MR_RB : vx + size_t(vo) * MR_RB;
         const bool ok = j < ntot;
-        cp16(dst + j * TC_V_STRIDE + u * 16, ok ? static_cast<const void*>(v + size_t(jc) * MR_RB + 2 * u) : vx, ok);
+        const double* src = (j < n0 ? v0 : v1) + size_t(j) * MR_RB;
+        cp16(d + 8 * i * TC_V_STRIDE, ok ? static_cast<const void*>(src) : vx, ok);
     }
 }
 

@@ -273,8 +273,9 @@ int64_t     hlrc_launch_count(hlrc_hmat M);
 
 hlrc_status hlrc_free(hlrc_hmat M);
 
-/* Debug-only: copies the device result of the most recent error word (set by
- * bounded device waits / bounds checks) and clears it.                       */
+/* Reads and clears the handle's device error word (synchronous).  Kernels
+ * that wait with a bound set it when a wait runs out; the products launched
+ * since then are incomplete.  0 means no error.                              */
 hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code);
 
 /* ----------------------------------------------------- host construction

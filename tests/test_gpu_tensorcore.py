@@ -54,6 +54,7 @@ def test_multi_rhs_reduced_precision(name, prec, op):
         hlr.mul_vec(1.0, op, M, torch.from_numpy(X[:, j].copy()).cuda(), ys)
         torch.cuda.synchronize()
         assert relerr(Y[:, j], ys.cpu().numpy()) <= SAME_STORE[prec], (prec, op, j)
+    assert M.device_error() == 0
     M.free()
 
 
