@@ -45,6 +45,9 @@ struct DevTPass {
 struct DevNPass {
     const NSeg* segs[4] = {};         // per StoreFmt
     int nsegs[4] = {0, 0, 0, 0};
+    const MSeg* mseg[4] = {};         // multi-RHS column streams (reduced precision)
+    int nmseg[4] = {0, 0, 0, 0};
+    const MCol* mcol = nullptr;
     const void* chunks = nullptr;     // NChunk (FP64 plan) or QNChunk (reduced precision)
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0, alg_bytes = 0;
@@ -58,6 +61,9 @@ struct DevNPass {
 struct DevTTPass {
     const TTSeg* segs[4] = {};
     int nsegs[4] = {0, 0, 0, 0};
+    const MSeg* mseg[4] = {};
+    int nmseg[4] = {0, 0, 0, 0};
+    const MCol* mcol = nullptr;
     const void* chunks = nullptr;     // TTChunk (FP64 plan) or QTTChunk
     const TGroup* groups = nullptr;
     int ngroups = 0;
@@ -102,6 +108,7 @@ struct hlrc_hmat_s {
     // row-major blocks of MR_RB vectors
     char* mr_arena = nullptr;
     double *mr_x = nullptr, *mr_t = nullptr, *mr_t2 = nullptr, *mr_part = nullptr;
+    char* mr_tables = nullptr;   // column streams of the reduced-precision multi-RHS kernels
     // host-pointer entry point staging
     double* hx = nullptr;
     double* hy = nullptr;
@@ -267,6 +274,105 @@ std::vector<Seg> remap_segs(const std::vector<Seg>& segs, const std::vector<uint
     return r;
 }
 
+// Column streams of one pass (MSeg): the chunks of each reduced-precision
+// segment, in store order, must form one contiguous run of columns; their
+// columns get one MCol entry each.
+struct StreamTables {
+    std::vector<MSeg> seg[4];
+    std::vector<MCol> col;
+};
+
+template <typename Seg, typename VoOf>
+hlrc_status build_streams(const std::vector<Seg> (&segs)[4], const std::vector<GChunk>& chunks, bool tt, VoOf vo_of,
+                          StreamTables& out) {
+    for (int f = FMT_F32; f <= FMT_BF16; ++f) {
+        for (const Seg& s : segs[f]) {
+            if (s.ce <= s.cb) continue;
+            std::vector<uint32_t> idx(s.ce - s.cb);
+            for (uint32_t k = 0; k < idx.size(); ++k) idx[k] = s.cb + k;
+            std::sort(idx.begin(), idx.end(),
+                      [&](uint32_t a, uint32_t b) { return chunks[a].byte_off < chunks[b].byte_off; });
+            const uint64_t colb = uint64_t(s.ld) * uint64_t(fmt_bytes(f));
+            uint64_t expect = chunks[idx[0]].byte_off;
+            if (expect % 16 != 0) return fail(HLRC_ERR_INTERNAL, "column stream not 16-byte aligned");
+            MSeg m{uint32_t(expect / 16), 0, uint32_t(out.col.size()), vo_of(s), s.rows, s.ld, 0};
+            for (uint32_t c : idx) {
+                const GChunk& g = chunks[c];
+                if (g.byte_off != expect || g.fmt != f)
+                    return fail(HLRC_ERR_INTERNAL, "segment chunks are not one contiguous column run");
+                expect += colb * g.nc;
+                for (uint32_t j = 0; j < g.nc; ++j) {
+                    uint32_t e;
+                    if (tt) {
+                        const uint64_t o = uint64_t(g.vo) + j;
+                        if (o >= MC_DIRECT) return fail(HLRC_ERR_SHAPE, "output index beyond 2^31");
+                        e = uint32_t(o) | ((g.flags & TT_DIRECT) ? MC_DIRECT : 0u);
+                    } else {
+                        e = ((g.vo & ~VEC_T) + j) | (g.vo & VEC_T);
+                    }
+                    out.col.push_back(MCol{e, g.scale});
+                }
+                m.ncols += g.nc;
+            }
+            out.seg[f].push_back(m);
+        }
+    }
+    if (out.col.size() >= (size_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "column table beyond 2^32 entries");
+    return HLRC_OK;
+}
+
+// Builds and uploads the column streams of every N-form and tile T-form pass.
+hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
+    std::vector<StreamTables> nt(p.npasses.size()), tt(p.ttpasses.size());
+    size_t bytes = 0;
+    auto take = [&](size_t b) { const size_t o = bytes; bytes = align_up(bytes + b, 256); return o; };
+    std::vector<std::array<size_t, 4>> n_seg_off(nt.size()), t_seg_off(tt.size());
+    std::vector<size_t> n_col_off(nt.size()), t_col_off(tt.size());
+    for (size_t i = 0; i < nt.size(); ++i) {
+        const hlrc_status st = build_streams(p.npasses[i].segs, p.npasses[i].chunks, false,
+                                             [](const NSeg& s) { return s.out; }, nt[i]);
+        if (st != HLRC_OK) return st;
+        for (int f = 0; f < 4; ++f) n_seg_off[i][size_t(f)] = take(nt[i].seg[f].size() * sizeof(MSeg));
+        n_col_off[i] = take(nt[i].col.size() * sizeof(MCol));
+    }
+    for (size_t i = 0; i < tt.size(); ++i) {
+        const hlrc_status st = build_streams(p.ttpasses[i].segs, p.ttpasses[i].chunks, true,
+                                             [](const TTSeg& s) { return s.v_off; }, tt[i]);
+        if (st != HLRC_OK) return st;
+        for (int f = 0; f < 4; ++f) t_seg_off[i][size_t(f)] = take(tt[i].seg[f].size() * sizeof(MSeg));
+        t_col_off[i] = take(tt[i].col.size() * sizeof(MCol));
+    }
+    cudaError_t e = cudaMalloc(&h->mr_tables, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HLRC_ERR_OOM, "multi-RHS column tables of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    auto put = [&](size_t off, const void* src, size_t b) -> cudaError_t {
+        return b ? cudaMemcpy(h->mr_tables + off, src, b, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    for (size_t i = 0; i < nt.size() && e == cudaSuccess; ++i) {
+        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+            e = put(n_seg_off[i][size_t(f)], nt[i].seg[f].data(), nt[i].seg[f].size() * sizeof(MSeg));
+            h->n[i].mseg[f] = reinterpret_cast<const MSeg*>(h->mr_tables + n_seg_off[i][size_t(f)]);
+            h->n[i].nmseg[f] = int(nt[i].seg[f].size());
+        }
+        if (e == cudaSuccess) e = put(n_col_off[i], nt[i].col.data(), nt[i].col.size() * sizeof(MCol));
+        h->n[i].mcol = reinterpret_cast<const MCol*>(h->mr_tables + n_col_off[i]);
+    }
+    for (size_t i = 0; i < tt.size() && e == cudaSuccess; ++i) {
+        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+            e = put(t_seg_off[i][size_t(f)], tt[i].seg[f].data(), tt[i].seg[f].size() * sizeof(MSeg));
+            h->tt[i].mseg[f] = reinterpret_cast<const MSeg*>(h->mr_tables + t_seg_off[i][size_t(f)]);
+            h->tt[i].nmseg[f] = int(tt[i].seg[f].size());
+        }
+        if (e == cudaSuccess) e = put(t_col_off[i], tt[i].col.data(), tt[i].col.size() * sizeof(MCol));
+        h->tt[i].mcol = reinterpret_cast<const MCol*>(h->mr_tables + t_col_off[i]);
+    }
+    if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "column table upload failed: %s", cudaGetErrorString(e));
+    h->info.device_bytes += int64_t(bytes);
+    return HLRC_OK;
+}
+
 // The tensor-core kernels use more than 48 KB of dynamic shared memory;
 // the limit is raised once per device (the attribute belongs to the device
 // context that is current when it is set).
@@ -422,6 +528,15 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         hp->mr_part = carve(np);
         hp->info.workspace_bytes += int64_t(bytes);
         hp->info.device_bytes += int64_t(bytes);
+        if (p.precision != HLRC_PREC_F64) {
+            const hlrc_status st = upload_streams(p, hp);
+            if (st != HLRC_OK) {
+                cudaFree(hp->mr_tables);
+                cudaFree(hp->mr_arena);
+                cleanup();
+                return st;
+            }
+        }
     }
     for (int op = 0; op < 3; ++op) {
         int nl = 0;
@@ -637,15 +752,15 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                             tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, M->mr_part,
                             alpha, add);
                 } else {
-                    if (tp.nsegs[FMT_F32] > 0)
-                        k_ttform_tc32<<<tp.nsegs[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
-                            tp.segs[FMT_F32], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
-                    if (tp.nsegs[FMT_F16] > 0)
-                        k_ttform_tc<FMT_F16><<<tp.nsegs[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.segs[FMT_F16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
-                    if (tp.nsegs[FMT_BF16] > 0)
-                        k_ttform_tc<FMT_BF16><<<tp.nsegs[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.segs[FMT_BF16], qp, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                    if (tp.nmseg[FMT_F32] > 0)
+                        k_ttform_tc32<<<tp.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
+                            tp.mseg[FMT_F32], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                    if (tp.nmseg[FMT_F16] > 0)
+                        k_ttform_tc<FMT_F16><<<tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
+                            tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                    if (tp.nmseg[FMT_BF16] > 0)
+                        k_ttform_tc<FMT_BF16><<<tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
+                            tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
                 }
                 if (ws_profile(M)) prof_end(M, s);
                 if (tp.ngroups > 0) {
@@ -668,15 +783,15 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                     k_nform_dmma<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
-                if (!f64plan && np.nsegs[FMT_F32] > 0)
-                    k_nform_tc32<<<np.nsegs[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
-                        np.segs[FMT_F32], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
-                if (!f64plan && np.nsegs[FMT_F16] > 0)
-                    k_nform_tc<FMT_F16><<<np.nsegs[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
-                        np.segs[FMT_F16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
-                if (!f64plan && np.nsegs[FMT_BF16] > 0)
-                    k_nform_tc<FMT_BF16><<<np.nsegs[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
-                        np.segs[FMT_BF16], qp, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                if (!f64plan && np.nmseg[FMT_F32] > 0)
+                    k_nform_tc32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
+                        np.mseg[FMT_F32], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                if (!f64plan && np.nmseg[FMT_F16] > 0)
+                    k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
+                        np.mseg[FMT_F16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                if (!f64plan && np.nmseg[FMT_BF16] > 0)
+                    k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
+                        np.mseg[FMT_BF16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (ws_profile(M)) prof_end(M, s);
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
             }
@@ -973,6 +1088,7 @@ extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     cudaFree(M->hx);
     cudaFree(M->hy);
     cudaFree(M->mr_arena);
+    cudaFree(M->mr_tables);
     cudaFree(M->arena);
     delete M;
     return HLRC_OK;

@@ -45,14 +45,13 @@ constexpr int TC_A16_STRIDE = 144;    // 16-bit chunk column (64 rows = 128 B) +
 constexpr int TC_A32N_STRIDE = 288;   // FP32 column (256 B) + 32 B pad, N-form (16-byte reads)
 constexpr int TC_A32T_STRIDE = 272;   // FP32 column + 16 B pad, tile T-form (ldmatrix reads)
 constexpr int TC_V_STRIDE = 80;       // MR_RB doubles of one vector column + 16 B pad
-constexpr int TC_STAGE_N16 = 32 * TC_A16_STRIDE + 32 * TC_V_STRIDE;
-constexpr int TC_STAGE_T16 = 32 * TC_A16_STRIDE;
-constexpr int TC_STAGE_N32 = 16 * TC_A32N_STRIDE + 16 * TC_V_STRIDE;
-constexpr int TC_STAGE_T32 = 16 * TC_A32T_STRIDE;
+constexpr int TC_STAGE_N16 = 32 * TC_A16_STRIDE + 32 * TC_V_STRIDE + 32 * 4;   // columns, vector, column scales
+constexpr int TC_STAGE_T16 = 32 * TC_A16_STRIDE + 32 * 8;                        // columns, column table
+constexpr int TC_STAGE_N32 = 16 * TC_A32N_STRIDE + 16 * TC_V_STRIDE + 16 * 4;
+constexpr int TC_STAGE_T32 = 16 * TC_A32T_STRIDE + 16 * 8;
 
-// dynamic shared memory of a launch: the warps' rings, then per warp one
-// 32-byte pack descriptor per stage
-constexpr int tc_smem_bytes(int stage) { return TC_WARPS * TC_STAGES * (stage + 32); }
+// dynamic shared memory of a launch: one ring of TC_STAGES stages per warp
+constexpr int tc_smem_bytes(int stage) { return TC_WARPS * TC_STAGES * stage; }
 
 template <int FMT> struct TcOp;
 
@@ -176,24 +175,17 @@ __device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* row) {
                  : "r"(smem_addr(row)));
 }
 
-// One warp's pass over packs c0, c0 + step, ... < ce through its ring of
-// TC_STAGES stages: issue(stage, pack) starts the copies of a pack, and
-// compute(stage, pack) consumes a stage once its copies have landed.  Pack
-// descriptors are read one pack ahead and kept beside their stage.
-template <typename Pack, typename Issue, typename Compute>
-__device__ __forceinline__ void warp_ring(const Pack* __restrict__ packs, uint32_t c0, uint32_t ce, uint32_t step,
-                                          Pack* sdesc, int lane, Issue&& issue, Compute&& compute) {
-    const int n = c0 < ce ? int((ce - c0 + step - 1) / step) : 0;
-    Pack nxt;
-    if (n > 0) nxt = ld_pack(packs + c0);
+// One warp's pass over the stages s = warp, warp + W, ... < nst of a column
+// stream through its ring: issue(slot, s) starts the copies of stage s into
+// ring slot `slot`, and compute(slot, s) consumes the slot once its copies
+// have landed.
+template <typename Issue, typename Compute>
+__device__ __forceinline__ void warp_stream(int nst, int warp, Issue&& issue, Compute&& compute) {
+    const int n = nst > warp ? (nst - warp + TC_WARPS - 1) / TC_WARPS : 0;
     int issued = 0;
     auto issue_next = [&]() {
         if (issued < n) {
-            const Pack cur = nxt;
-            if (issued + 1 < n) nxt = ld_pack(packs + c0 + uint32_t(issued + 1) * step);
-            const int st = issued % TC_STAGES;
-            if (lane == 0) sdesc[st] = cur;
-            issue(st, cur);
+            issue(issued % TC_STAGES, warp + issued * TC_WARPS);
             ++issued;
         }
         cp_commit();
@@ -204,104 +196,98 @@ __device__ __forceinline__ void warp_ring(const Pack* __restrict__ packs, uint32
         issue_next();
         cp_wait<TC_STAGES - 1>();
         __syncwarp();
-        const int st = k % TC_STAGES;
-        compute(st, sdesc[st]);
+        compute(k % TC_STAGES, warp + k * TC_WARPS);
         __syncwarp();
     }
 }
 
-// Copies of the columns of a pack into a stage: columns [0, nc0) from part
-// 0, [nc0, nc0 + nc1) from part 1, zero-filled up to COLS.  A column holds
-// `units` 16-byte units (ld * element bytes / 16) at global stride `units`
-// and shared stride `stride`; UPL units make a full 64-row column, and lane
-// l copies unit l % UPL of columns l / UPL + (32 / UPL) i.  The parts are
-// selected through two base pointers (no indexing into the descriptor).
-template <int UPL, int COLS, typename Pack>
-__device__ __forceinline__ void stage_columns(uint8_t* dst, int stride, const uint8_t* A, const Pack& pk, int units,
-                                              int lane) {
-    const int u = lane % UPL;
-    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
-    const size_t cb = size_t(units) * 16;
-    const uint8_t* b0 = A + size_t(pk.p[0].a16) * 16 + u * 16;
-    const uint8_t* b1 = A + size_t(pk.p[1].a16) * 16 + u * 16 - size_t(n0) * cb;
+// Copies columns [c0, c0 + COLS) of a column stream (column j at
+// base + j * colb, colb = ld * element bytes) into a stage at shared stride
+// `stride`.  UPL 16-byte units make a 64-row column; lane l copies unit
+// l % UPL of columns l / UPL + (32 / UPL) i.  Units below the column height
+// of columns past ncols, and units past the column height, are zero-filled.
+template <int UPL, int COLS>
+__device__ __forceinline__ void stage_run(uint8_t* dst, int stride, const uint8_t* base, int c0, int ncols, int colb,
+                                          int lane) {
+    const int u = lane % UPL, units = colb / 16;
+    const uint8_t* src = base + size_t(c0 + lane / UPL) * colb + u * 16;
     uint8_t* d = dst + (lane / UPL) * stride + u * 16;
 #pragma unroll
     for (int i = 0; i < COLS * UPL / 32; ++i) {
-        const int j = lane / UPL + (32 / UPL) * i;
-        const bool ok = j < ntot && u < units;
-        const uint8_t* src = (j < n0 ? b0 : b1) + size_t(j) * cb;
-        cp16(d + (32 / UPL) * i * stride, ok ? src : A, ok);
+        const bool ok = c0 + lane / UPL + (32 / UPL) * i < ncols && u < units;
+        cp16(d + (32 / UPL) * i * stride, ok ? src + size_t((32 / UPL) * i) * colb : base, ok);
     }
 }
 
-// Copies of the vector entries (MR_RB doubles = 4 units per column) of the
-// columns of an N-form pack into a stage, at shared stride TC_V_STRIDE.
-template <int COLS, typename Pack>
-__device__ __forceinline__ void stage_vector(uint8_t* dst, const double* vx, const double* vt, const Pack& pk,
-                                             int lane) {
+// Copies the vector entries (MR_RB doubles = 4 units) of the COLS columns
+// of an N-form stage, at shared stride TC_V_STRIDE.  Lane j holds the table
+// entry of column j of the stage in `idx`.
+template <int COLS>
+__device__ __forceinline__ void stage_vector(uint8_t* dst, uint32_t idx, int c0, int ncols, const double* vx,
+                                             const double* vt, int lane) {
     const int u = lane & 3;
-    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
-    const uint32_t o0 = pk.p[0].v_off, o1 = pk.p[1].v_off;
-    const double* v0 = ((o0 & VEC_T) ? vt + size_t(o0 & ~VEC_T) * MR_RB : vx + size_t(o0) * MR_RB) + 2 * u;
-    const double* v1 = ((o1 & VEC_T) ? vt + size_t(o1 & ~VEC_T) * MR_RB : vx + size_t(o1) * MR_RB) + 2 * u -
-                       size_t(n0) * MR_RB;
-    uint8_t* d = dst + (lane >> 2) * TC_V_STRIDE + u * 16;
 #pragma unroll
     for (int i = 0; i < COLS / 8; ++i) {
         const int j = (lane >> 2) + 8 * i;
-        const bool ok = j < ntot;
-        const double* src = (j < n0 ? v0 : v1) + size_t(j) * MR_RB;
-        cp16(d + 8 * i * TC_V_STRIDE, ok ? static_cast<const void*>(src) : vx, ok);
+        const uint32_t e = __shfl_sync(0xffffffffu, idx, j);
+        const bool ok = c0 + j < ncols;
+        const double* v = ((e & VEC_T) ? vt : vx) + size_t(e & ~VEC_T) * MR_RB + 2 * u;
+        cp16(dst + j * TC_V_STRIDE + u * 16, ok ? static_cast<const void*>(v) : vx, ok);
     }
 }
 
-// Shared epilogue of the tile T-forms: value val of chunk column col,
-// right-hand side n goes to its output or to its partial slot.
-template <typename Chunk>
-__device__ __forceinline__ void tt_store(const Chunk& ch, int col, int n, double val, const OutMap& om,
-                                         double* __restrict__ part, double alpha, int add) {
-    if (col >= ch.nc || n >= om.nr) return;
-    if (ch.flags & TT_DIRECT) {
-        double* o = om.base + int64_t(ch.out + col) * om.rs + int64_t(n) * om.cs;
+__device__ __forceinline__ MCol ld_mcol(const MCol* p) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+    return MCol{u.x, __uint_as_float(u.y)};
+}
+
+// Epilogue of the tile T-forms: value val (already unscaled) of stream
+// column entry m, right-hand side n, to its output or partial slot.
+__device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const OutMap& om, double* __restrict__ part,
+                                       double alpha, int add) {
+    if (n >= om.nr) return;
+    if (m.idx & MC_DIRECT) {
+        double* o = om.base + int64_t(m.idx & ~MC_DIRECT) * om.rs + int64_t(n) * om.cs;
         if (add) *o += alpha * val;
         else *o = val;
     } else {
-        part[size_t(ch.out + col) * MR_RB + n] = val;
+        part[size_t(m.idx) * MR_RB + n] = val;
     }
 }
 
 // Fixed-order sum of the per-warp accumulators of an N-form tile
 // (red[(w * TILE + row) * MR_RB + k]) and the update of the output rows.
-__device__ __forceinline__ void nform_store(const double* red, const NSeg& sg, const OutMap& om, double alpha,
+__device__ __forceinline__ void nform_store(const double* red, int out, int rows, const OutMap& om, double alpha,
                                             int add) {
     for (int i = threadIdx.x; i < TILE * MR_RB; i += TC_WARPS * 32) {
         const int row = i % TILE, k = i / TILE;
-        if (row >= sg.rows || k >= om.nr) continue;
+        if (row >= rows || k >= om.nr) continue;
         double sum = 0.0;
 #pragma unroll
         for (int w = 0; w < TC_WARPS; ++w) sum += red[(w * TILE + row) * MR_RB + k];
-        double* o = om.base + int64_t(sg.out + row) * om.rs + int64_t(k) * om.cs;
+        double* o = om.base + int64_t(out + row) * om.rs + int64_t(k) * om.cs;
         if (add) *o += alpha * sum;
         else *o = sum;
     }
 }
 
 // ------------------------------------------------------- 16-bit chunks
-// Tile T-form: one CTA per input tile; each chunk result is complete (the
-// contraction covers the whole tile) and goes to its output or partial slot.
-// Fragments (natural placement): A[m][k] = chunk column m, tile row k, read
-// with ldmatrix from the staged columns; B[k][n] = x row k, right-hand side n.
+// Tile T-form: one CTA per input tile (stream segment); the warps take the
+// segment's 32-column stages round-robin.  Each column result is complete
+// (the contraction covers the whole tile) and goes to its output or partial
+// slot through the column table.  Fragments (natural placement): A[m][k] =
+// stream column m, tile row k, read with ldmatrix from the staged columns;
+// B[k][n] = x row k, right-hand side n.
 template <int FMT>
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_tc(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, const uint8_t* __restrict__ A,
+k_ttform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
             const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
     using O = TcOp<FMT>;
     extern __shared__ __align__(16) uint8_t smem[];
-    const TTSeg sg = segs[blockIdx.x];
+    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T16);
-    QTTPack* sdesc = reinterpret_cast<QTTPack*>(smem + TC_WARPS * TC_STAGES * TC_STAGE_T16) + warp * TC_STAGES;
     // x entries of the lane: rows 16kt + 2t + {0, 1, 8, 9} (kt < 4), right-hand side g
     double xv[4][4];
     int E = 0;
@@ -310,7 +296,7 @@ k_ttform_tc(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, c
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int row = 16 * kt + 2 * t + (j & 1) + 8 * (j >> 1);
-            const double v = row < sg.rows ? __ldg(vin + size_t(sg.v_off + row) * MR_RB + g) : 0.0;
+            const double v = row < sg.rows ? __ldg(vin + size_t(sg.vo + row) * MR_RB + g) : 0.0;
             xv[kt][j] = v;
             E = max(E, dexp(v));
         }
@@ -326,126 +312,138 @@ k_ttform_tc(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, c
         tc_split<FMT>(xv[kt][0], xv[kt][1], s, bh[kt][0], bl[kt][0]);
         tc_split<FMT>(xv[kt][2], xv[kt][3], s, bh[kt][1], bl[kt][1]);
     }
-    const int units = sg.ld / 8;
+    const int colb = sg.ld * 2, ncols = int(sg.ncols);
+    const uint8_t* base = A + size_t(sg.a16) * 16;
+    const MCol* ctab = cols + sg.col0;
     const int nkt = (sg.rows + 15) / 16;
     // ldmatrix row of this lane: column + 8 for lanes 8-15 and 24-31, rows + 8 for lanes 16-31
     const int lcol = (lane & 7) + ((lane >> 3) & 1) * 8, lrow = ((lane >> 4) & 1) * 8;
-    warp_ring(
-        packs, sg.cb + warp, sg.ce, TC_WARPS, sdesc, lane,
-        [&](int st, const QTTPack& pk) {
-            stage_columns<8, 32>(ring + st * TC_STAGE_T16, TC_A16_STRIDE, A, pk, units, lane);
+    MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
+    warp_stream(
+        (ncols + 31) / 32, warp,
+        [&](int slot, int st) {
+            uint8_t* sa = ring + slot * TC_STAGE_T16;
+            const int c0 = 32 * st;
+            stage_run<8, 32>(sa, TC_A16_STRIDE, base, c0, ncols, colb, lane);
+            reinterpret_cast<MCol*>(sa + 32 * TC_A16_STRIDE)[lane] = mc;
+            const int cn = c0 + 32 * TC_WARPS + lane;
+            mc = cn < ncols ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
-        [&](int st, const QTTPack& pk) {
-            const uint8_t* sa = ring + st * TC_STAGE_T16;
-            int col0 = 0;
+        [&](int slot, int st) {
+            const uint8_t* sa = ring + slot * TC_STAGE_T16;
+            const MCol* tab = reinterpret_cast<const MCol*>(sa + 32 * TC_A16_STRIDE);
+            const int cnt = min(32, ncols - 32 * st);
+            for (int mt = 0; 16 * mt < cnt; ++mt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+                const uint8_t* row0 = sa + (16 * mt + lcol) * TC_A16_STRIDE + 2 * lrow;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const QTTChunk& ch = pk.p[q];
-                const double f0 = double(ch.scale) * inv0, f1 = double(ch.scale) * inv1;
-                for (int mt = 0; 16 * mt < ch.nc; ++mt) {
-                    float d[4] = {0.f, 0.f, 0.f, 0.f};
-                    const uint8_t* base = sa + min(col0 + 16 * mt + lcol, 31) * TC_A16_STRIDE + 2 * lrow;
-#pragma unroll
-                    for (int kt = 0; kt < 4; ++kt) {
-                        if (kt >= nkt) break;
-                        uint32_t a[4];
-                        ldsm_x4(a, base + 32 * kt);
-                        O::mma(d, a, bh[kt][0], bh[kt][1]);
-                        O::mma(d, a, bl[kt][0], bl[kt][1]);
-                    }
-                    const int c = 16 * mt + g;
-                    tt_store(ch, c, 2 * t, double(d[0]) * f0, om, part, alpha, add);
-                    tt_store(ch, c, 2 * t + 1, double(d[1]) * f1, om, part, alpha, add);
-                    tt_store(ch, c + 8, 2 * t, double(d[2]) * f0, om, part, alpha, add);
-                    tt_store(ch, c + 8, 2 * t + 1, double(d[3]) * f1, om, part, alpha, add);
+                for (int kt = 0; kt < 4; ++kt) {
+                    if (kt >= nkt) break;
+                    uint32_t a[4];
+                    ldsm_x4(a, row0 + 32 * kt);
+                    O::mma(d, a, bh[kt][0], bh[kt][1]);
+                    O::mma(d, a, bl[kt][0], bl[kt][1]);
                 }
-                col0 += ch.nc;
+                const int c = 16 * mt + g;
+                if (c < cnt) {
+                    const MCol m = tab[c];
+                    tt_out(m, 2 * t, double(d[0]) * (double(m.scale) * inv0), om, part, alpha, add);
+                    tt_out(m, 2 * t + 1, double(d[1]) * (double(m.scale) * inv1), om, part, alpha, add);
+                }
+                if (c + 8 < cnt) {
+                    const MCol m = tab[c + 8];
+                    tt_out(m, 2 * t, double(d[2]) * (double(m.scale) * inv0), om, part, alpha, add);
+                    tt_out(m, 2 * t + 1, double(d[3]) * (double(m.scale) * inv1), om, part, alpha, add);
+                }
             }
         });
 }
 
-// N-form: one CTA per output tile.  Fragments (natural placement): A[m][k] =
-// tile row m, chunk column k, read with ldmatrix.trans from the staged
-// columns; B[k][n] = vector entry of column k, right-hand side n, from the
-// staged vector.  Lane (g, t) accumulates rows 16i + g, 16i + g + 8 (i < 4)
-// for right-hand sides 2t, 2t+1 in FP64; fixed-order cross-warp sum.
+// N-form: one CTA per output tile (stream segment); the warps take the
+// segment's 32-column stages round-robin.  The column scales are folded into
+// the vector operand (B = scale * v, then one power-of-two scale per stage
+// and right-hand side), so a whole stage accumulates in one set of MMA
+// results and is added to FP64 once.  Fragments (natural placement):
+// A[m][k] = tile row m, stream column k, read with ldmatrix.trans; lane
+// (g, t) accumulates rows 16i + g, 16i + g + 8 (i < 4) for right-hand sides
+// 2t, 2t+1; fixed-order cross-warp sum at the end.
 template <int FMT>
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_nform_tc(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
+k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
            const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     using O = TcOp<FMT>;
     extern __shared__ __align__(16) uint8_t smem[];
-    const NSeg sg = segs[blockIdx.x];
+    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_N16);
-    QNPack* sdesc = reinterpret_cast<QNPack*>(smem + TC_WARPS * TC_STAGES * TC_STAGE_N16) + warp * TC_STAGES;
-    const int units = sg.ld / 8;
+    const int colb = sg.ld * 2, ncols = int(sg.ncols);
+    const uint8_t* base = A + size_t(sg.a16) * 16;
+    const MCol* ctab = cols + sg.col0;
     const int nmt = (sg.rows + 15) / 16;
     // ldmatrix.trans row of this lane: column + 8 for lanes 16-31, rows + 8 for lanes 8-15 and 24-31
     const int lcol = (lane & 7) + ((lane >> 4) & 1) * 8, lrow = ((lane >> 3) & 1) * 8;
     double acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
-    warp_ring(
-        packs, sg.cb + warp, sg.ce, TC_WARPS, sdesc, lane,
-        [&](int st, const QNPack& pk) {
-            uint8_t* sa = ring + st * TC_STAGE_N16;
-            stage_columns<8, 32>(sa, TC_A16_STRIDE, A, pk, units, lane);
-            stage_vector<32>(sa + 32 * TC_A16_STRIDE, vx, vt, pk, lane);
+    MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
+    warp_stream(
+        (ncols + 31) / 32, warp,
+        [&](int slot, int st) {
+            uint8_t* sa = ring + slot * TC_STAGE_N16;
+            const int c0 = 32 * st;
+            stage_run<8, 32>(sa, TC_A16_STRIDE, base, c0, ncols, colb, lane);
+            stage_vector<32>(sa + 32 * TC_A16_STRIDE, mc.idx, c0, ncols, vx, vt, lane);
+            reinterpret_cast<float*>(sa + 32 * (TC_A16_STRIDE + TC_V_STRIDE))[lane] = mc.scale;
+            const int cn = c0 + 32 * TC_WARPS + lane;
+            mc = cn < ncols ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
-        [&](int st, const QNPack& pk) {
-            const uint8_t* sa = ring + st * TC_STAGE_N16;
+        [&](int slot, int st) {
+            const uint8_t* sa = ring + slot * TC_STAGE_N16;
             const double* sv = reinterpret_cast<const double*>(sa + 32 * TC_A16_STRIDE);
-            int col0 = 0;
+            const float* ssc = reinterpret_cast<const float*>(sa + 32 * (TC_A16_STRIDE + TC_V_STRIDE));
+            const int nkt = ncols - 32 * st > 16 ? 2 : 1;
+            // vector operand: columns 16kt + 2t + {0, 1, 8, 9}, right-hand side g, times the column scale
+            double bv[2][4];
+            int E = 0;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const QNChunk& ch = pk.p[q];
-                if (ch.nc == 0) continue;
-                const int nkt = ch.nc > 16 ? 2 : 1;
-                // vector operand: columns 16kt + 2t + {0, 1, 8, 9}, right-hand side g
-                double bv[2][4];
-                int E = 0;
+            for (int kt = 0; kt < 2; ++kt)
 #pragma unroll
-                for (int kt = 0; kt < 2; ++kt)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int col = 16 * kt + 2 * t + (j & 1) + 8 * (j >> 1);
-                        const double x = col < ch.nc ? sv[(col0 + col) * (TC_V_STRIDE / 8) + g] : 0.0;
-                        bv[kt][j] = x;
-                        E = max(E, dexp(x));
-                    }
-                E = quad_max(E);
-                const double s = exp_scale(E);
-                const double f0 = double(ch.scale) * exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
-                const double f1 = double(ch.scale) * exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
-                float d[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
-#pragma unroll
-                for (int kt = 0; kt < 2; ++kt) {
-                    if (kt >= nkt) break;
-                    uint32_t bh0, bl0, bh1, bl1;
-                    tc_split<FMT>(bv[kt][0], bv[kt][1], s, bh0, bl0);
-                    tc_split<FMT>(bv[kt][2], bv[kt][3], s, bh1, bl1);
-                    const uint8_t* base = sa + min(col0 + 16 * kt + lcol, 31) * TC_A16_STRIDE + 2 * lrow;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        if (i >= nmt) break;
-                        uint32_t a[4];
-                        ldsm_x4_t(a, base + 32 * i);
-                        O::mma(d[i], a, bh0, bh1);
-                        O::mma(d[i], a, bl0, bl1);
-                    }
+                for (int j = 0; j < 4; ++j) {
+                    const int col = 16 * kt + 2 * t + (j & 1) + 8 * (j >> 1);
+                    const double x = sv[col * (TC_V_STRIDE / 8) + g] * double(ssc[col]);
+                    bv[kt][j] = x;
+                    E = max(E, dexp(x));
                 }
+            E = quad_max(E);
+            const double s = exp_scale(E);
+            const double f0 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
+            const double f1 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
+            float d[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
+#pragma unroll
+            for (int kt = 0; kt < 2; ++kt) {
+                if (kt >= nkt) break;
+                uint32_t bh0, bl0, bh1, bl1;
+                tc_split<FMT>(bv[kt][0], bv[kt][1], s, bh0, bl0);
+                tc_split<FMT>(bv[kt][2], bv[kt][3], s, bh1, bl1);
+                const uint8_t* row0 = sa + (16 * kt + lcol) * TC_A16_STRIDE + 2 * lrow;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    acc[i][0] = fma(double(d[i][0]), f0, acc[i][0]);
-                    acc[i][1] = fma(double(d[i][1]), f1, acc[i][1]);
-                    acc[i][2] = fma(double(d[i][2]), f0, acc[i][2]);
-                    acc[i][3] = fma(double(d[i][3]), f1, acc[i][3]);
+                    if (i >= nmt) break;
+                    uint32_t a[4];
+                    ldsm_x4_t(a, row0 + 32 * i);
+                    O::mma(d[i], a, bh0, bh1);
+                    O::mma(d[i], a, bl0, bl1);
                 }
-                col0 += ch.nc;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                acc[i][0] = fma(double(d[i][0]), f0, acc[i][0]);
+                acc[i][1] = fma(double(d[i][1]), f1, acc[i][1]);
+                acc[i][2] = fma(double(d[i][2]), f0, acc[i][2]);
+                acc[i][3] = fma(double(d[i][3]), f1, acc[i][3]);
             }
         });
     // all warps are done with their rings: reuse the start of shared memory
@@ -461,23 +459,22 @@ k_nform_tc(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, cons
         r1[1] = acc[i][3];
     }
     __syncthreads();
-    nform_store(red, sg, om, alpha, add);
+    nform_store(red, int(sg.vo), sg.rows, om, alpha, add);
 }
 
 // --------------------------------------------------------- FP32 chunks
-// Tile T-form on TF32 tiles.  ldmatrix (b16 granules) reads 32-bit A
-// fragments directly: a 16-byte row of a staged column is 4 tile rows, and
-// lane (g, t) receives granule pair (g, t) = chunk column g, tile row t of an
-// 8 x 4 block, which is the m16n8k8 TF32 A layout.
+// Tile T-form on TF32 tiles, 16-column stages.  ldmatrix (b16 granules)
+// reads 32-bit A fragments directly: a 16-byte row of a staged column is 4
+// tile rows, and lane (g, t) receives granule pair (g, t) = column g, tile
+// row t of an 8 x 4 block, which is the m16n8k8 TF32 A layout.
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_tc32(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, const uint8_t* __restrict__ A,
+k_ttform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
               const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const TTSeg sg = segs[blockIdx.x];
+    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T32);
-    QTTPack* sdesc = reinterpret_cast<QTTPack*>(smem + TC_WARPS * TC_STAGES * TC_STAGE_T32) + warp * TC_STAGES;
     // x entries of the lane: rows 8ks + t and 8ks + t + 4 (ks < 8), right-hand side g
     double xv[8][2];
     int E = 0;
@@ -486,7 +483,7 @@ k_ttform_tc32(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs,
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int row = 8 * ks + t + 4 * j;
-            const double v = row < sg.rows ? __ldg(vin + size_t(sg.v_off + row) * MR_RB + g) : 0.0;
+            const double v = row < sg.rows ? __ldg(vin + size_t(sg.vo + row) * MR_RB + g) : 0.0;
             xv[ks][j] = v;
             E = max(E, dexp(v));
         }
@@ -499,129 +496,137 @@ k_ttform_tc32(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs,
     for (int ks = 0; ks < 8; ++ks)
 #pragma unroll
         for (int j = 0; j < 2; ++j) tf32_split(float(xv[ks][j] * s), bb[ks][j], bs[ks][j]);
-    const int units = sg.ld / 4;
+    const int colb = sg.ld * 4, ncols = int(sg.ncols);
+    const uint8_t* base = A + size_t(sg.a16) * 16;
+    const MCol* ctab = cols + sg.col0;
     const int nks = (sg.rows + 7) / 8;
     // ldmatrix row of this lane: column + 8 for lanes 8-15 and 24-31, rows + 4 for lanes 16-31
     const int lcol = (lane & 7) + ((lane >> 3) & 1) * 8, lrow = ((lane >> 4) & 1) * 4;
-    warp_ring(
-        packs, sg.cb + warp, sg.ce, TC_WARPS, sdesc, lane,
-        [&](int st, const QTTPack& pk) {
-            stage_columns<16, 16>(ring + st * TC_STAGE_T32, TC_A32T_STRIDE, A, pk, units, lane);
+    MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
+    warp_stream(
+        (ncols + 15) / 16, warp,
+        [&](int slot, int st) {
+            uint8_t* sa = ring + slot * TC_STAGE_T32;
+            const int c0 = 16 * st;
+            stage_run<16, 16>(sa, TC_A32T_STRIDE, base, c0, ncols, colb, lane);
+            if (lane < 16) reinterpret_cast<MCol*>(sa + 16 * TC_A32T_STRIDE)[lane] = mc;
+            const int cn = c0 + 16 * TC_WARPS + lane;
+            mc = (lane < 16 && cn < ncols) ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
-        [&](int st, const QTTPack& pk) {
-            const uint8_t* sa = ring + st * TC_STAGE_T32;
-            int col0 = 0;
+        [&](int slot, int st) {
+            const uint8_t* sa = ring + slot * TC_STAGE_T32;
+            const MCol* tab = reinterpret_cast<const MCol*>(sa + 16 * TC_A32T_STRIDE);
+            const int cnt = min(16, ncols - 16 * st);
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            const uint8_t* row0 = sa + lcol * TC_A32T_STRIDE + 4 * lrow;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const QTTChunk& ch = pk.p[q];
-                if (ch.nc == 0) continue;
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-                const uint8_t* base = sa + min(col0 + lcol, 15) * TC_A32T_STRIDE + 4 * lrow;
-#pragma unroll
-                for (int ks = 0; ks < 8; ++ks) {
-                    if (ks >= nks) break;
-                    uint32_t a[4];
-                    ldsm_x4(a, base + 32 * ks);
-                    mma_tf32x3(d, a, bb[ks], bs[ks]);
-                }
-                const double f0 = double(ch.scale) * inv0, f1 = double(ch.scale) * inv1;
-                tt_store(ch, g, 2 * t, double(d[0]) * f0, om, part, alpha, add);
-                tt_store(ch, g, 2 * t + 1, double(d[1]) * f1, om, part, alpha, add);
-                tt_store(ch, g + 8, 2 * t, double(d[2]) * f0, om, part, alpha, add);
-                tt_store(ch, g + 8, 2 * t + 1, double(d[3]) * f1, om, part, alpha, add);
-                col0 += ch.nc;
+            for (int ks = 0; ks < 8; ++ks) {
+                if (ks >= nks) break;
+                uint32_t a[4];
+                ldsm_x4(a, row0 + 32 * ks);
+                mma_tf32x3(d, a, bb[ks], bs[ks]);
+            }
+            if (g < cnt) {
+                const MCol m = tab[g];
+                tt_out(m, 2 * t, double(d[0]) * (double(m.scale) * inv0), om, part, alpha, add);
+                tt_out(m, 2 * t + 1, double(d[1]) * (double(m.scale) * inv1), om, part, alpha, add);
+            }
+            if (g + 8 < cnt) {
+                const MCol m = tab[g + 8];
+                tt_out(m, 2 * t, double(d[2]) * (double(m.scale) * inv0), om, part, alpha, add);
+                tt_out(m, 2 * t + 1, double(d[3]) * (double(m.scale) * inv1), om, part, alpha, add);
             }
         });
 }
 
-// N-form on TF32 tiles.  A 32-bit fragment cannot be transposed by
-// ldmatrix, so a lane reads 16-byte runs of 4 rows: lane (g, t) takes rows
-// 4g .. 4g+3 and 32+4g .. 32+4g+3 of chunk columns 8kt + t and 8kt + t + 4,
-// and m-tile i uses rows 4g + 2i, 4g + 2i + 1 (i < 2), or 32 + 4g + 2(i-2)
-// + {0, 1}, as its fragment rows g and g + 8.  The shared stride of 288 bytes
-// keeps these reads free of bank conflicts.
+// N-form on TF32 tiles, 16-column stages.  A 32-bit fragment cannot be
+// transposed by ldmatrix, so a lane reads 16-byte runs of 4 rows: lane
+// (g, t) takes rows 4g .. 4g+3 and 32+4g .. 32+4g+3 of stage columns
+// 8kt + t and 8kt + t + 4, and m-tile i uses rows 4g + 2i, 4g + 2i + 1
+// (i < 2), or 32 + 4g + 2(i-2) + {0, 1}, as its fragment rows g and g + 8.
+// The shared stride of 288 bytes keeps these reads free of bank conflicts.
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_nform_tc32(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
+k_nform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
              const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const NSeg sg = segs[blockIdx.x];
+    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_N32);
-    QNPack* sdesc = reinterpret_cast<QNPack*>(smem + TC_WARPS * TC_STAGES * TC_STAGE_N32) + warp * TC_STAGES;
-    const int units = sg.ld / 4;
+    const int colb = sg.ld * 4, ncols = int(sg.ncols);
+    const uint8_t* base = A + size_t(sg.a16) * 16;
+    const MCol* ctab = cols + sg.col0;
     const bool hi_rows = 32 < sg.ld;
     // accumulators: rows 4g + r and 32 + 4g + r (r < 4) -> acc[r] / acc[4 + r]
     double acc[8][2];
 #pragma unroll
     for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
-    warp_ring(
-        packs, sg.cb + warp, sg.ce, TC_WARPS, sdesc, lane,
-        [&](int st, const QNPack& pk) {
-            uint8_t* sa = ring + st * TC_STAGE_N32;
-            stage_columns<16, 16>(sa, TC_A32N_STRIDE, A, pk, units, lane);
-            stage_vector<16>(sa + 16 * TC_A32N_STRIDE, vx, vt, pk, lane);
+    MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
+    warp_stream(
+        (ncols + 15) / 16, warp,
+        [&](int slot, int st) {
+            uint8_t* sa = ring + slot * TC_STAGE_N32;
+            const int c0 = 16 * st;
+            stage_run<16, 16>(sa, TC_A32N_STRIDE, base, c0, ncols, colb, lane);
+            stage_vector<16>(sa + 16 * TC_A32N_STRIDE, mc.idx, c0, ncols, vx, vt, lane);
+            if (lane < 16) reinterpret_cast<float*>(sa + 16 * (TC_A32N_STRIDE + TC_V_STRIDE))[lane] = mc.scale;
+            const int cn = c0 + 16 * TC_WARPS + lane;
+            mc = (lane < 16 && cn < ncols) ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
-        [&](int st, const QNPack& pk) {
-            const uint8_t* sa = ring + st * TC_STAGE_N32;
+        [&](int slot, int st) {
+            const uint8_t* sa = ring + slot * TC_STAGE_N32;
             const double* sv = reinterpret_cast<const double*>(sa + 16 * TC_A32N_STRIDE);
-            int col0 = 0;
+            const float* ssc = reinterpret_cast<const float*>(sa + 16 * (TC_A32N_STRIDE + TC_V_STRIDE));
+            const int nkt = ncols - 16 * st > 8 ? 2 : 1;
+            // vector operand: columns 8kt + t and 8kt + t + 4, right-hand side g, times the column scale
+            double bv[2][2];
+            int E = 0;
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const QNChunk& ch = pk.p[q];
-                if (ch.nc == 0) continue;
-                const int nkt = ch.nc > 8 ? 2 : 1;
-                // vector operand: columns 8kt + t and 8kt + t + 4, right-hand side g
-                double bv[2][2];
-                int E = 0;
+            for (int kt = 0; kt < 2; ++kt)
 #pragma unroll
-                for (int kt = 0; kt < 2; ++kt)
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                        const int col = 8 * kt + t + 4 * j;
-                        const double x = col < ch.nc ? sv[(col0 + col) * (TC_V_STRIDE / 8) + g] : 0.0;
-                        bv[kt][j] = x;
-                        E = max(E, dexp(x));
-                    }
-                E = quad_max(E);
-                const double s = exp_scale(E);
-                const double f0 = double(ch.scale) * exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
-                const double f1 = double(ch.scale) * exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
-                float d[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
-#pragma unroll
-                for (int kt = 0; kt < 2; ++kt) {
-                    if (kt >= nkt) break;
-                    uint32_t bb[2], bs[2];
-                    tf32_split(float(bv[kt][0] * s), bb[0], bs[0]);
-                    tf32_split(float(bv[kt][1] * s), bb[1], bs[1]);
-                    const uint8_t* ca = sa + min(col0 + 8 * kt + t, 15) * TC_A32N_STRIDE + 16 * g;
-                    const uint8_t* cb = sa + min(col0 + 8 * kt + t + 4, 15) * TC_A32N_STRIDE + 16 * g;
-                    const uint4 La0 = *reinterpret_cast<const uint4*>(ca);
-                    const uint4 Lb0 = *reinterpret_cast<const uint4*>(cb);
-                    const uint32_t a0[4] = {La0.x, La0.y, Lb0.x, Lb0.y};
-                    const uint32_t a1[4] = {La0.z, La0.w, Lb0.z, Lb0.w};
-                    mma_tf32x3(d[0], a0, bb, bs);
-                    mma_tf32x3(d[1], a1, bb, bs);
-                    if (hi_rows) {
-                        const uint4 La1 = *reinterpret_cast<const uint4*>(ca + 128);
-                        const uint4 Lb1 = *reinterpret_cast<const uint4*>(cb + 128);
-                        const uint32_t a2[4] = {La1.x, La1.y, Lb1.x, Lb1.y};
-                        const uint32_t a3[4] = {La1.z, La1.w, Lb1.z, Lb1.w};
-                        mma_tf32x3(d[2], a2, bb, bs);
-                        mma_tf32x3(d[3], a3, bb, bs);
-                    }
+                for (int j = 0; j < 2; ++j) {
+                    const int col = 8 * kt + t + 4 * j;
+                    const double x = sv[col * (TC_V_STRIDE / 8) + g] * double(ssc[col]);
+                    bv[kt][j] = x;
+                    E = max(E, dexp(x));
                 }
-                // m-tile i: fragment row g -> local row 2i, row g + 8 -> 2i + 1
+            E = quad_max(E);
+            const double s = exp_scale(E);
+            const double f0 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
+            const double f1 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
+            float d[4][4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    acc[2 * i][0] = fma(double(d[i][0]), f0, acc[2 * i][0]);
-                    acc[2 * i][1] = fma(double(d[i][1]), f1, acc[2 * i][1]);
-                    acc[2 * i + 1][0] = fma(double(d[i][2]), f0, acc[2 * i + 1][0]);
-                    acc[2 * i + 1][1] = fma(double(d[i][3]), f1, acc[2 * i + 1][1]);
+            for (int i = 0; i < 4; ++i) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
+#pragma unroll
+            for (int kt = 0; kt < 2; ++kt) {
+                if (kt >= nkt) break;
+                uint32_t bb[2], bs[2];
+                tf32_split(float(bv[kt][0] * s), bb[0], bs[0]);
+                tf32_split(float(bv[kt][1] * s), bb[1], bs[1]);
+                const uint8_t* ca = sa + (8 * kt + t) * TC_A32N_STRIDE + 16 * g;
+                const uint8_t* cb = ca + 4 * TC_A32N_STRIDE;
+                const uint4 La0 = *reinterpret_cast<const uint4*>(ca);
+                const uint4 Lb0 = *reinterpret_cast<const uint4*>(cb);
+                const uint32_t a0[4] = {La0.x, La0.y, Lb0.x, Lb0.y};
+                const uint32_t a1[4] = {La0.z, La0.w, Lb0.z, Lb0.w};
+                mma_tf32x3(d[0], a0, bb, bs);
+                mma_tf32x3(d[1], a1, bb, bs);
+                if (hi_rows) {
+                    const uint4 La1 = *reinterpret_cast<const uint4*>(ca + 128);
+                    const uint4 Lb1 = *reinterpret_cast<const uint4*>(cb + 128);
+                    const uint32_t a2[4] = {La1.x, La1.y, Lb1.x, Lb1.y};
+                    const uint32_t a3[4] = {La1.z, La1.w, Lb1.z, Lb1.w};
+                    mma_tf32x3(d[2], a2, bb, bs);
+                    mma_tf32x3(d[3], a3, bb, bs);
                 }
-                col0 += ch.nc;
+            }
+            // m-tile i: fragment row g -> local row 2i, row g + 8 -> 2i + 1
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                acc[2 * i][0] = fma(double(d[i][0]), f0, acc[2 * i][0]);
+                acc[2 * i][1] = fma(double(d[i][1]), f1, acc[2 * i][1]);
+                acc[2 * i + 1][0] = fma(double(d[i][2]), f0, acc[2 * i + 1][0]);
+                acc[2 * i + 1][1] = fma(double(d[i][3]), f1, acc[2 * i + 1][1]);
             }
         });
     __syncthreads();
@@ -634,7 +639,7 @@ k_nform_tc32(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, co
         red[(warp * TILE + row) * MR_RB + 2 * t + 1] = acc[l][1];
     }
     __syncthreads();
-    nform_store(red, sg, om, alpha, add);
+    nform_store(red, int(sg.vo), sg.rows, om, alpha, add);
 }
 
 }  // namespace hlrc

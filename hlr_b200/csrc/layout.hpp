@@ -143,4 +143,27 @@ struct QNPack { QNChunk p[2]; };
 struct QTTPack { QTTChunk p[2]; };
 static_assert(sizeof(QNPack) == 32 && sizeof(QTTPack) == 32, "packs must be 32 bytes");
 
+// ------------------------------------------------ multi-RHS column streams
+// The reduced-precision stores are laid out so that the chunks of one format
+// that one pass segment (tile) visits are contiguous: the multi-RHS kernels
+// stream a segment as one run of columns (column j at a16*16 + j*ld*element
+// bytes) with one table entry per column.
+struct MSeg {
+    uint32_t a16;          // byte offset / 16 of the segment's first column
+    uint32_t ncols;        // columns in the run
+    uint32_t col0;         // first entry of the column table
+    uint32_t vo;           // N-form: first output row; tile T-form: first input row
+    uint16_t rows;         // rows of the tile (<= 64)
+    uint16_t ld;           // leading dimension of every column
+    uint32_t pad;
+};
+static_assert(sizeof(MSeg) == 24, "MSeg is 24 bytes");
+
+constexpr uint32_t MC_DIRECT = 0x80000000u;   // tile T-form column table: output, not partial slot
+struct MCol {
+    uint32_t idx;          // N-form: vector entry (| VEC_T: in t); T-form: output (| MC_DIRECT) or partial
+    float scale;           // the chunk's scale (1 for FP32)
+};
+static_assert(sizeof(MCol) == 8, "MCol is 8 bytes");
+
 }  // namespace hlrc

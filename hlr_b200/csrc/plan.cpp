@@ -115,16 +115,29 @@ struct SSlab {
     int32_t c0, nch;             // chunks [c0, c0 + nch)
 };
 
+// Layout order of the chunks of one tile region: dense (D) or factor (U, V,
+// bases) slabs, by format.  With it, every pass segment of one format is a
+// contiguous run of columns in every store this planner produces: FP64 D,U;
+// FP32 D,U; mixed D(FP32),U(FP32),U(FP16); FP16 / BF16 U,D.
+inline int layout_rank(int group, int fmt) {
+    static const int rank[4][2] = {{0, 1}, {2, 3}, {5, 4}, {7, 6}};   // [fmt][group]: D = 0, factor = 1
+    return rank[fmt][group];
+}
+
 struct Store {
     std::vector<SSlab> slabs;
     std::vector<SChunk> chunks;
+    std::vector<uint8_t> group;        // per chunk: 0 = dense slab, 1 = factor slab
+    std::vector<int32_t> crows;        // per chunk: rows of its slab
+    size_t region_begin = 0;           // first chunk without a byte offset
     int64_t bytes = 0;
     int64_t unpadded[4] = {0, 0, 0, 0};
 
     // rows [r0, r0+rows) x ncols of a column-major matrix; colfmt (per
-    // column, may be null -> deffmt); chunks do not straddle `cuts`
+    // column, may be null -> deffmt); chunks do not straddle `cuts`.  Byte
+    // offsets are assigned by close_region().
     int alloc(const double* src, int64_t lds, int64_t r0, int64_t rows, int64_t ncols, const uint8_t* colfmt,
-              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr) {
+              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr, int grp = 1) {
         SSlab s{src, lds, r0, rows, pad_rows(rows), int32_t(chunks.size()), 0};
         int64_t j = 0;
         size_t ci = 0;
@@ -137,15 +150,29 @@ struct Store {
             }
             for (int64_t c = j + 1; c < e; ++c)
                 if ((colfmt ? colfmt[c] : deffmt) != f) { e = c; break; }
-            SChunk ch{align16(bytes), int32_t(j), int16_t(e - j), f, 1.0f};
-            bytes = ch.byte_off + pad_fmt(rows, f) * (e - j) * fmt_bytes(f);
+            SChunk ch{-1, int32_t(j), int16_t(e - j), f, 1.0f};
             unpadded[f] += rows * (e - j) * fmt_bytes(f) + (f >= FMT_F16 ? 4 : 0);
             chunks.push_back(ch);
+            group.push_back(uint8_t(grp));
+            crows.push_back(int32_t(rows));
             ++s.nch;
             j = e;
         }
         slabs.push_back(s);
         return int(slabs.size()) - 1;
+    }
+
+    // Places the chunks allocated since the last call: by layout_rank, then
+    // in allocation order, each on a 16-byte boundary.
+    void close_region() {
+        for (int r = 0; r < 8; ++r)
+            for (size_t c = region_begin; c < chunks.size(); ++c) {
+                SChunk& ch = chunks[c];
+                if (layout_rank(group[c], ch.fmt) != r) continue;
+                ch.byte_off = align16(bytes);
+                bytes = ch.byte_off + pad_fmt(crows[c], ch.fmt) * ch.nc * fmt_bytes(ch.fmt);
+            }
+        region_begin = chunks.size();
     }
 
     void fill(std::vector<uint8_t>& st) {
@@ -484,6 +511,23 @@ hlrc_status validate_plan(const Plan& p) {
             default: return p.n_t2;
         }
     };
+    // reduced-precision segments must be one contiguous run of columns in
+    // the store (the multi-RHS kernels stream them as such)
+    auto contiguous = [&](const std::vector<GChunk>& ch, uint32_t cb, uint32_t ce, int f, int64_t ld) -> bool {
+        if (f == FMT_F64 || ce <= cb) return true;
+        std::vector<uint64_t> offs;
+        offs.reserve(ce - cb);
+        for (uint32_t c = cb; c < ce; ++c) offs.push_back(ch[c].byte_off);
+        std::vector<uint32_t> idx(ce - cb);
+        for (uint32_t k = 0; k < idx.size(); ++k) idx[k] = k;
+        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return offs[a] < offs[b]; });
+        uint64_t expect = offs[idx[0]];
+        for (uint32_t k : idx) {
+            if (offs[k] != expect) return false;
+            expect += uint64_t(ld) * fmt_bytes(f) * ch[cb + k].nc;
+        }
+        return true;
+    };
     auto chunk_ok = [&](const GChunk& c, int64_t rows) -> bool {
         if (c.nc == 0 || rows <= 0 || rows > TILE) return false;
         if (c.byte_off % 16 != 0) return false;
@@ -496,6 +540,8 @@ hlrc_status validate_plan(const Plan& p) {
             for (const NSeg& s : np.segs[f]) {
                 if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > np.chunks.size())
                     return fail(HLRC_ERR_INTERNAL, "N-pass %zu: bad segment", pi);
+                if (!contiguous(np.chunks, s.cb, s.ce, f, s.ld))
+                    return fail(HLRC_ERR_INTERNAL, "N-pass %zu: segment is not one column run", pi);
                 if (int64_t(s.out) + s.rows > vec_len(np.out))
                     return fail(HLRC_ERR_INTERNAL, "N-pass %zu: output tile outside the vector", pi);
                 for (uint32_t c = s.cb; c < s.ce; ++c) {
@@ -514,6 +560,8 @@ hlrc_status validate_plan(const Plan& p) {
             for (const TTSeg& s : tp.segs[f]) {
                 if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > tp.chunks.size())
                     return fail(HLRC_ERR_INTERNAL, "T-pass %zu: bad segment", pi);
+                if (!contiguous(tp.chunks, s.cb, s.ce, f, s.ld))
+                    return fail(HLRC_ERR_INTERNAL, "T-pass %zu: segment is not one column run", pi);
                 if (int64_t(s.v_off) + s.rows > vec_len(tp.in))
                     return fail(HLRC_ERR_INTERNAL, "T-pass %zu: input tile outside the vector", pi);
                 for (uint32_t c = s.cb; c < s.ce; ++c) {
@@ -652,18 +700,21 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
             const int64_t r0 = tr.lo(t) - b.row0, rows = tr.size(t);
             if (b.kind == HLRC_LEAF_DENSE) {
                 const std::vector<int64_t> cuts = inner_cuts(tc, b.col0, b.ncols);
-                slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols, nullptr, densefmt, &cuts));
+                slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols, nullptr, densefmt, &cuts, 0));
             } else {
                 slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank, cf(i), deffmt));
             }
         }
+        st.close_region();
     }
-    for (int64_t t = 0; t < tc.n(); ++t)
+    for (int64_t t = 0; t < tc.n(); ++t) {
         for (int64_t i : collist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
             if (b.kind != HLRC_LEAF_LOWRANK) continue;
             slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank, cf(i), deffmt));
         }
+        st.close_region();
+    }
     if (st.bytes >= (int64_t(1) << 36) && o.precision != HLRC_PREC_F64)
         return fail(HLRC_ERR_SHAPE, "reduced-precision store above 64 GiB");
     // FP64 plans hold FP64 chunks only, reduced-precision plans none: the two
@@ -902,6 +953,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         for (int64_t r0 = 0; r0 < kr; r0 += TILE)
             sS[size_t(i)].push_back(st.alloc(b.S, b.lds, r0, std::min<int64_t>(TILE, kr - r0), kc, nullptr, FMT_F64));
     }
+    st.close_region();   // one region: allocation order (FP64 only)
     st.fill(p.store);
     for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
