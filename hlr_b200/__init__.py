@@ -311,9 +311,11 @@ def _vec_args(v, n: int):
             if v.stride(0) != 1 and v.numel() > 1:
                 raise ValueError("vector must be contiguous")
             return v.data_ptr(), 1, max(1, v.shape[0]), v.is_cuda
-        if v.stride(0) != 1:
+        # the stride of a dimension of size 1 is arbitrary in torch
+        if v.stride(0) != 1 and v.shape[0] > 1:
             raise ValueError("multi-RHS arrays must be column-major (n, nrhs) with stride(0) == 1")
-        return v.data_ptr(), v.shape[1], v.stride(1), v.is_cuda
+        ld = v.stride(1) if v.shape[1] > 1 else max(1, v.shape[0])
+        return v.data_ptr(), v.shape[1], ld, v.is_cuda
     a = v
     if not isinstance(a, np.ndarray) or a.dtype != np.float64:
         raise TypeError("vectors must be float64 numpy arrays or torch tensors")

@@ -754,19 +754,24 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 } else {
                     if (tp.nmseg[FMT_F32] > 0)
                         k_ttform_tc32<<<tp.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
-                            tp.mseg[FMT_F32], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                            tp.mseg[FMT_F32], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
                     if (tp.nmseg[FMT_F16] > 0)
                         k_ttform_tc<FMT_F16><<<tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                            tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
                     if (tp.nmseg[FMT_BF16] > 0)
                         k_ttform_tc<FMT_BF16><<<tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, M->mr_part, alpha, add);
+                            tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
                 }
                 if (ws_profile(M)) prof_end(M, s);
                 if (tp.ngroups > 0) {
-                    if (ws_profile(M)) prof_begin(M, "ttfinish", tp.npart * 8 * MR_RB, s);
-                    k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om,
-                                                                          alpha, add);
+                    if (ws_profile(M))
+                        prof_begin(M, "ttfinish", tp.npart * MR_RB * (M->precision == HLRC_PREC_F64 ? 8 : 4), s);
+                    if (M->precision == HLRC_PREC_F64)
+                        k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om,
+                                                                              alpha, add);
+                    else
+                        k_ttfinish_f32_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(
+                            tp.groups, tp.ngroups, reinterpret_cast<const float*>(M->mr_part), om, alpha, add);
                     if (ws_profile(M)) prof_end(M, s);
                 }
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));

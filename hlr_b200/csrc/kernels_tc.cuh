@@ -242,8 +242,10 @@ __device__ __forceinline__ MCol ld_mcol(const MCol* p) {
 }
 
 // Epilogue of the tile T-forms: value val (already unscaled) of stream
-// column entry m, right-hand side n, to its output or partial slot.
-__device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const OutMap& om, double* __restrict__ part,
+// column entry m, right-hand side n, to its output (FP64) or to its partial
+// slot.  Partials are stored in FP32: they are sums of FP32 MMA results of
+// one tile, so nothing is lost, and the finish adds them up in FP64.
+__device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const OutMap& om, float* __restrict__ part,
                                        double alpha, int add) {
     if (n >= om.nr) return;
     if (m.idx & MC_DIRECT) {
@@ -251,7 +253,50 @@ __device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const O
         if (add) *o += alpha * val;
         else *o = val;
     } else {
-        part[size_t(m.idx) * MR_RB + n] = val;
+        part[size_t(m.idx) * MR_RB + n] = float(val);
+    }
+}
+
+// Sums FP32 per-tile partials (row-major, MR_RB vectors) of multi-tile
+// outputs in FP64: slot i, column j, vector k of a group is
+// part[(slot0 + i*nc + j)*MR_RB + k].  A lane owns four vectors of one
+// column and keeps four interleaved sums; fixed order.
+__global__ void __launch_bounds__(256)
+k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* __restrict__ part, OutMap om,
+                  double alpha, int add) {
+    const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (gid >= ngroups) return;
+    const int lane = threadIdx.x & 31;
+    const TGroup g = groups[gid];
+    constexpr uint32_t QUADS = MR_RB / 4;
+    const uint32_t n4 = g.nc * QUADS;
+    const float4* p0 = reinterpret_cast<const float4*>(part + size_t(g.slot0) * MR_RB);
+    for (uint32_t q = lane; q < n4; q += 32) {
+        const uint32_t j = q / QUADS;
+        const int k = int(4 * (q % QUADS));
+        if (k >= om.nr) continue;
+        const float4* p = p0 + q;
+        double s[4][4] = {};
+        uint32_t i = 0;
+        for (; i + 4 <= g.nslots; i += 4) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const float4 v = __ldcs(p + size_t(i + a) * n4);
+                s[a][0] += v.x; s[a][1] += v.y; s[a][2] += v.z; s[a][3] += v.w;
+            }
+        }
+        for (; i < g.nslots; ++i) {
+            const float4 v = __ldcs(p + size_t(i) * n4);
+            s[0][0] += v.x; s[0][1] += v.y; s[0][2] += v.z; s[0][3] += v.w;
+        }
+        double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (k + e >= om.nr) break;
+            const double r = (s[0][e] + s[1][e]) + (s[2][e] + s[3][e]);
+            if (add) o[e * om.cs] += alpha * r;
+            else o[e * om.cs] = r;
+        }
     }
 }
 
@@ -281,7 +326,7 @@ __device__ __forceinline__ void nform_store(const double* red, int out, int rows
 template <int FMT>
 __global__ void __launch_bounds__(TC_WARPS * 32)
 k_ttform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-            const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
+            const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
     using O = TcOp<FMT>;
     extern __shared__ __align__(16) uint8_t smem[];
     const MSeg sg = segs[blockIdx.x];
@@ -469,7 +514,7 @@ k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const u
 // row t of an 8 x 4 block, which is the m16n8k8 TF32 A layout.
 __global__ void __launch_bounds__(TC_WARPS * 32)
 k_ttform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-              const double* __restrict__ vin, OutMap om, double* __restrict__ part, double alpha, int add) {
+              const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
