@@ -389,9 +389,9 @@ hlrc_status enable_tc_smem(int dev) {
                                    tc_smem_bytes(TC_STAGE_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N16)));
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_T32)));
-    HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N32)));
     done.push_back(dev);
     return HLRC_OK;
@@ -753,7 +753,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                             alpha, add);
                 } else {
                     if (tp.nmseg[FMT_F32] > 0)
-                        k_ttform_tc32<<<tp.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
+                        k_ttform_d32<<<tp.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
                             tp.mseg[FMT_F32], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
                     if (tp.nmseg[FMT_F16] > 0)
                         k_ttform_tc<FMT_F16><<<tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
@@ -789,7 +789,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
                 if (!f64plan && np.nmseg[FMT_F32] > 0)
-                    k_nform_tc32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
+                    k_nform_d32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
                         np.mseg[FMT_F32], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nmseg[FMT_F16] > 0)
                     k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(

@@ -1,30 +1,28 @@
 // Tensor-core multi-right-hand-side kernels for reduced-precision stores,
 // MR_RB = 8 right-hand sides per launch.
 //
-// With 8 right-hand sides a chunk product is a small dense contraction:
-// 16-bit chunks (scaled FP16 / BF16) run as mma.sync m16n8k16 tiles, FP32
-// chunks as m16n8k8 TF32 tiles with the three-term split, all with FP32
-// accumulation inside a chunk and FP64 accumulation across chunks.  The
-// vector operand is split into two 16-bit terms, hi = round(s*v) and
-// lo = round(s*v - hi), with a power-of-two scale s per chunk (N-form) or
-// input tile (tile T-form) and right-hand side, so the product keeps about
-// 22 significant bits of v (FP16) or 16 (BF16) and the storage rounding of
-// the matrix stays the dominant error.
+// With 8 right-hand sides a chunk product is a small dense contraction.
+// 16-bit columns (scaled FP16 / BF16) run as mma.sync m16n8k16 tiles with
+// FP32 accumulation; the vector operand is split into two 16-bit terms,
+// hi = round(s*v) and lo = round(s*v - hi), with a power-of-two scale per
+// stage (N-form) or input tile (tile T-form) and right-hand side, so the
+// product keeps about 22 significant bits of v (FP16) or 16 (BF16) and the
+// storage rounding of the matrix stays the dominant error.  FP32 columns run
+// on the FP64 tensor cores (m8n8k4): their values convert to FP64 exactly.
+// Results are accumulated in FP64.
 //
-// Data movement.  Each warp streams its packs (work items of up to two
-// chunks) through a ring of TC_STAGES shared-memory stages filled with
-// cp.async 16-byte copies, so several chunks per warp are in flight without
-// holding registers.  A stage holds the chunk columns at a padded stride
-// (no bank conflicts for the fragment loads) and, for the N-form, the vector
-// entries of those columns; units outside the chunk are zero-filled by the
-// copies themselves, so no stage ever holds stale data.  Fragments come from
-// ldmatrix: plain for the tile T-form (A = chunk^T, rows contiguous), .trans
-// for the N-form (A = chunk, columns contiguous).  Fragment rows or columns
-// that fall past the pack's columns read the stage's last column instead:
-// their products either meet a zero vector entry or land in accumulator
-// rows that are never stored.  FP32 N-form fragments are
-// read as 16-byte runs of 4 rows with the row placement described at
-// k_nform_tc32.
+// Data movement.  The store is laid out so that the columns one segment
+// (tile, format) visits form one contiguous run; a CTA owns a segment and its
+// warps take 32-column stages (16 for FP32) of the run round-robin.  Each
+// warp streams its stages through a ring of TC_STAGES shared-memory slots
+// filled with cp.async 16-byte copies.  Columns land at a padded stride, so
+// the fragment loads are free of bank conflicts, and the copies zero-fill
+// everything past the run, so no slot ever holds stale data.  16-bit
+// fragments come from ldmatrix: plain for the tile T-form (A = run^T, rows
+// contiguous), .trans for the N-form (A = run, columns contiguous).  A
+// per-column table gives each column's vector entry (N-form) or output
+// (tile T-form) and its chunk scale; in the N-form the scale is folded into
+// the vector operand, so a whole stage accumulates in one set of MMA results.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -42,13 +40,12 @@ constexpr int TC_STAGES = 2;   // shared-memory stages per warp
 
 // stage geometry: column strides in bytes
 constexpr int TC_A16_STRIDE = 144;    // 16-bit chunk column (64 rows = 128 B) + 16 B pad
-constexpr int TC_A32N_STRIDE = 288;   // FP32 column (256 B) + 32 B pad, N-form (16-byte reads)
-constexpr int TC_A32T_STRIDE = 272;   // FP32 column + 16 B pad, tile T-form (ldmatrix reads)
+constexpr int TC_A32_STRIDE = 288;    // FP32 column (256 B) + 32 B pad (8-byte reads of row pairs)
 constexpr int TC_V_STRIDE = 80;       // MR_RB doubles of one vector column + 16 B pad
 constexpr int TC_STAGE_N16 = 32 * TC_A16_STRIDE + 32 * TC_V_STRIDE + 32 * 4;   // columns, vector, column scales
 constexpr int TC_STAGE_T16 = 32 * TC_A16_STRIDE + 32 * 8;                        // columns, column table
-constexpr int TC_STAGE_N32 = 16 * TC_A32N_STRIDE + 16 * TC_V_STRIDE + 16 * 4;
-constexpr int TC_STAGE_T32 = 16 * TC_A32T_STRIDE + 16 * 8;
+constexpr int TC_STAGE_N32 = 16 * TC_A32_STRIDE + 16 * TC_V_STRIDE + 16 * 4;
+constexpr int TC_STAGE_T32 = 16 * TC_A32_STRIDE + 16 * 8;
 
 // dynamic shared memory of a launch: one ring of TC_STAGES stages per warp
 constexpr int tc_smem_bytes(int stage) { return TC_WARPS * TC_STAGES * stage; }
@@ -115,36 +112,6 @@ __device__ __forceinline__ void tc_split(double v0, double v1, double s, uint32_
     hi = O::cvt2(f0, f1);
     const float2 h = O::unpack(hi);
     lo = O::cvt2(f0 - h.x, f1 - h.y);
-}
-
-__device__ __forceinline__ uint32_t to_tf32(float v) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(v));
-    return r;
-}
-
-// big / small TF32 terms of a float
-__device__ __forceinline__ void tf32_split(float v, uint32_t& big, uint32_t& small) {
-    big = to_tf32(v);
-    small = to_tf32(v - __uint_as_float(big));
-}
-
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// d += A B for the three-term split of A (four FP32 values, as bits) and
-// B = (bb, bs); the small products first
-__device__ __forceinline__ void mma_tf32x3(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&bb)[2],
-                                           const uint32_t (&bs)[2]) {
-    uint32_t ab[4], as[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) tf32_split(__uint_as_float(a[i]), ab[i], as[i]);
-    mma_tf32(d, as, bb[0], bb[1]);
-    mma_tf32(d, ab, bs[0], bs[1]);
-    mma_tf32(d, ab, bb[0], bb[1]);
 }
 
 // ------------------------------------------------ shared-memory staging
@@ -508,91 +475,80 @@ k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const u
 }
 
 // --------------------------------------------------------- FP32 chunks
-// Tile T-form on TF32 tiles, 16-column stages.  ldmatrix (b16 granules)
-// reads 32-bit A fragments directly: a 16-byte row of a staged column is 4
-// tile rows, and lane (g, t) receives granule pair (g, t) = column g, tile
-// row t of an 8 x 4 block, which is the m16n8k8 TF32 A layout.
+// FP32 columns run on the FP64 tensor cores (mma.sync m8n8k4 f64): FP32
+// values convert to FP64 exactly, so the products are exact and the sums
+// FP64, and no operand needs splitting.  Both forms read 8-byte pairs of
+// rows from staged columns at a 288-byte stride (free of bank conflicts).
+//   N-form: contraction = stream columns 4ks + t; m-tile 2p + b takes tile
+//     row 16p + 2g + b as its fragment row g; the accumulators are the MMA
+//     results themselves (FP64).
+//   tile T-form: contraction = tile rows, k-step 2j + b maps fragment k = t to
+//     row 8j + 2t + b; m-tiles are 8 stream columns.
+
+// Tile T-form: one CTA per input tile; x in FP64 registers; 16-column stages.
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-              const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
+k_ttform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
+             const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T32);
-    // x entries of the lane: rows 8ks + t and 8ks + t + 4 (ks < 8), right-hand side g
-    double xv[8][2];
-    int E = 0;
+    // x of the lane: rows 8j + 2t + b (j < 8, b < 2), right-hand side g
+    double xv[16];
 #pragma unroll
-    for (int ks = 0; ks < 8; ++ks)
+    for (int jj = 0; jj < 8; ++jj)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int row = 8 * ks + t + 4 * j;
-            const double v = row < sg.rows ? __ldg(vin + size_t(sg.vo + row) * MR_RB + g) : 0.0;
-            xv[ks][j] = v;
-            E = max(E, dexp(v));
+        for (int b = 0; b < 2; ++b) {
+            const int row = 8 * jj + 2 * t + b;
+            xv[2 * jj + b] = row < sg.rows ? __ldg(vin + size_t(sg.vo + row) * MR_RB + g) : 0.0;
         }
-    E = quad_max(E);
-    const double s = exp_scale(E);
-    const double inv0 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
-    const double inv1 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
-    uint32_t bb[8][2], bs[8][2];
-#pragma unroll
-    for (int ks = 0; ks < 8; ++ks)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) tf32_split(float(xv[ks][j] * s), bb[ks][j], bs[ks][j]);
     const int colb = sg.ld * 4, ncols = int(sg.ncols);
     const uint8_t* base = A + size_t(sg.a16) * 16;
     const MCol* ctab = cols + sg.col0;
-    const int nks = (sg.rows + 7) / 8;
-    // ldmatrix row of this lane: column + 8 for lanes 8-15 and 24-31, rows + 4 for lanes 16-31
-    const int lcol = (lane & 7) + ((lane >> 3) & 1) * 8, lrow = ((lane >> 4) & 1) * 4;
+    const int nj = (sg.rows + 7) / 8;
     MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
     warp_stream(
         (ncols + 15) / 16, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_T32;
             const int c0 = 16 * st;
-            stage_run<16, 16>(sa, TC_A32T_STRIDE, base, c0, ncols, colb, lane);
-            if (lane < 16) reinterpret_cast<MCol*>(sa + 16 * TC_A32T_STRIDE)[lane] = mc;
+            stage_run<16, 16>(sa, TC_A32_STRIDE, base, c0, ncols, colb, lane);
+            if (lane < 16) reinterpret_cast<MCol*>(sa + 16 * TC_A32_STRIDE)[lane] = mc;
             const int cn = c0 + 16 * TC_WARPS + lane;
             mc = (lane < 16 && cn < ncols) ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
         [&](int slot, int st) {
             const uint8_t* sa = ring + slot * TC_STAGE_T32;
-            const MCol* tab = reinterpret_cast<const MCol*>(sa + 16 * TC_A32T_STRIDE);
+            const MCol* tab = reinterpret_cast<const MCol*>(sa + 16 * TC_A32_STRIDE);
             const int cnt = min(16, ncols - 16 * st);
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            const uint8_t* row0 = sa + lcol * TC_A32T_STRIDE + 4 * lrow;
 #pragma unroll
-            for (int ks = 0; ks < 8; ++ks) {
-                if (ks >= nks) break;
-                uint32_t a[4];
-                ldsm_x4(a, row0 + 32 * ks);
-                mma_tf32x3(d, a, bb[ks], bs[ks]);
-            }
-            if (g < cnt) {
-                const MCol m = tab[g];
-                tt_out(m, 2 * t, double(d[0]) * (double(m.scale) * inv0), om, part, alpha, add);
-                tt_out(m, 2 * t + 1, double(d[1]) * (double(m.scale) * inv1), om, part, alpha, add);
-            }
-            if (g + 8 < cnt) {
-                const MCol m = tab[g + 8];
-                tt_out(m, 2 * t, double(d[2]) * (double(m.scale) * inv0), om, part, alpha, add);
-                tt_out(m, 2 * t + 1, double(d[3]) * (double(m.scale) * inv1), om, part, alpha, add);
+            for (int mt = 0; mt < 2; ++mt) {
+                if (8 * mt >= cnt) break;
+                const uint8_t* ca = sa + (8 * mt + g) * TC_A32_STRIDE + 8 * t;
+                double d[2] = {0.0, 0.0};
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    if (jj >= nj) break;
+                    const float2 a = *reinterpret_cast<const float2*>(ca + 32 * jj);
+                    dmma(d, double(a.x), xv[2 * jj]);
+                    dmma(d, double(a.y), xv[2 * jj + 1]);
+                }
+                const int c = 8 * mt + g;
+                if (c < cnt) {
+                    const MCol m = tab[c];
+                    tt_out(m, 2 * t, d[0] * double(m.scale), om, part, alpha, add);
+                    tt_out(m, 2 * t + 1, d[1] * double(m.scale), om, part, alpha, add);
+                }
             }
         });
 }
 
-// N-form on TF32 tiles, 16-column stages.  A 32-bit fragment cannot be
-// transposed by ldmatrix, so a lane reads 16-byte runs of 4 rows: lane
-// (g, t) takes rows 4g .. 4g+3 and 32+4g .. 32+4g+3 of stage columns
-// 8kt + t and 8kt + t + 4, and m-tile i uses rows 4g + 2i, 4g + 2i + 1
-// (i < 2), or 32 + 4g + 2(i-2) + {0, 1}, as its fragment rows g and g + 8.
-// The shared stride of 288 bytes keeps these reads free of bank conflicts.
+// N-form: one CTA per output tile; 16-column stages; the vector entries (times
+// the column scale) are the B operand, and the MMA accumulates in FP64.
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_nform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-             const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
+k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
+            const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -601,87 +557,50 @@ k_nform_tc32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
     const int colb = sg.ld * 4, ncols = int(sg.ncols);
     const uint8_t* base = A + size_t(sg.a16) * 16;
     const MCol* ctab = cols + sg.col0;
-    const bool hi_rows = 32 < sg.ld;
-    // accumulators: rows 4g + r and 32 + 4g + r (r < 4) -> acc[r] / acc[4 + r]
+    const int np = (sg.rows + 15) / 16;
+    // acc[2p + b]: tile row 16p + 2g + b, right-hand sides 2t, 2t+1
     double acc[8][2];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
+    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
     MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
     warp_stream(
         (ncols + 15) / 16, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_N32;
             const int c0 = 16 * st;
-            stage_run<16, 16>(sa, TC_A32N_STRIDE, base, c0, ncols, colb, lane);
-            stage_vector<16>(sa + 16 * TC_A32N_STRIDE, mc.idx, c0, ncols, vx, vt, lane);
-            if (lane < 16) reinterpret_cast<float*>(sa + 16 * (TC_A32N_STRIDE + TC_V_STRIDE))[lane] = mc.scale;
+            stage_run<16, 16>(sa, TC_A32_STRIDE, base, c0, ncols, colb, lane);
+            stage_vector<16>(sa + 16 * TC_A32_STRIDE, mc.idx, c0, ncols, vx, vt, lane);
+            if (lane < 16) reinterpret_cast<float*>(sa + 16 * (TC_A32_STRIDE + TC_V_STRIDE))[lane] = mc.scale;
             const int cn = c0 + 16 * TC_WARPS + lane;
             mc = (lane < 16 && cn < ncols) ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
         [&](int slot, int st) {
             const uint8_t* sa = ring + slot * TC_STAGE_N32;
-            const double* sv = reinterpret_cast<const double*>(sa + 16 * TC_A32N_STRIDE);
-            const float* ssc = reinterpret_cast<const float*>(sa + 16 * (TC_A32N_STRIDE + TC_V_STRIDE));
-            const int nkt = ncols - 16 * st > 8 ? 2 : 1;
-            // vector operand: columns 8kt + t and 8kt + t + 4, right-hand side g, times the column scale
-            double bv[2][2];
-            int E = 0;
+            const double* sv = reinterpret_cast<const double*>(sa + 16 * TC_A32_STRIDE);
+            const float* ssc = reinterpret_cast<const float*>(sa + 16 * (TC_A32_STRIDE + TC_V_STRIDE));
+            const int nks = (min(16, ncols - 16 * st) + 3) / 4;
 #pragma unroll
-            for (int kt = 0; kt < 2; ++kt)
+            for (int ks = 0; ks < 4; ++ks) {
+                if (ks >= nks) break;
+                const int col = 4 * ks + t;
+                const double b = sv[col * (TC_V_STRIDE / 8) + g] * double(ssc[col]);
+                const uint8_t* ca = sa + col * TC_A32_STRIDE + 8 * g;
 #pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int col = 8 * kt + t + 4 * j;
-                    const double x = sv[col * (TC_V_STRIDE / 8) + g] * double(ssc[col]);
-                    bv[kt][j] = x;
-                    E = max(E, dexp(x));
+                for (int p = 0; p < 4; ++p) {
+                    if (p >= np) break;
+                    const float2 a = *reinterpret_cast<const float2*>(ca + 64 * p);
+                    dmma(acc[2 * p], double(a.x), b);
+                    dmma(acc[2 * p + 1], double(a.y), b);
                 }
-            E = quad_max(E);
-            const double s = exp_scale(E);
-            const double f0 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t));
-            const double f1 = exp_unscale(__shfl_sync(0xffffffffu, E, 8 * t + 4));
-            float d[4][4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) d[i][0] = d[i][1] = d[i][2] = d[i][3] = 0.f;
-#pragma unroll
-            for (int kt = 0; kt < 2; ++kt) {
-                if (kt >= nkt) break;
-                uint32_t bb[2], bs[2];
-                tf32_split(float(bv[kt][0] * s), bb[0], bs[0]);
-                tf32_split(float(bv[kt][1] * s), bb[1], bs[1]);
-                const uint8_t* ca = sa + (8 * kt + t) * TC_A32N_STRIDE + 16 * g;
-                const uint8_t* cb = ca + 4 * TC_A32N_STRIDE;
-                const uint4 La0 = *reinterpret_cast<const uint4*>(ca);
-                const uint4 Lb0 = *reinterpret_cast<const uint4*>(cb);
-                const uint32_t a0[4] = {La0.x, La0.y, Lb0.x, Lb0.y};
-                const uint32_t a1[4] = {La0.z, La0.w, Lb0.z, Lb0.w};
-                mma_tf32x3(d[0], a0, bb, bs);
-                mma_tf32x3(d[1], a1, bb, bs);
-                if (hi_rows) {
-                    const uint4 La1 = *reinterpret_cast<const uint4*>(ca + 128);
-                    const uint4 Lb1 = *reinterpret_cast<const uint4*>(cb + 128);
-                    const uint32_t a2[4] = {La1.x, La1.y, Lb1.x, Lb1.y};
-                    const uint32_t a3[4] = {La1.z, La1.w, Lb1.z, Lb1.w};
-                    mma_tf32x3(d[2], a2, bb, bs);
-                    mma_tf32x3(d[3], a3, bb, bs);
-                }
-            }
-            // m-tile i: fragment row g -> local row 2i, row g + 8 -> 2i + 1
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                acc[2 * i][0] = fma(double(d[i][0]), f0, acc[2 * i][0]);
-                acc[2 * i][1] = fma(double(d[i][1]), f1, acc[2 * i][1]);
-                acc[2 * i + 1][0] = fma(double(d[i][2]), f0, acc[2 * i + 1][0]);
-                acc[2 * i + 1][1] = fma(double(d[i][3]), f1, acc[2 * i + 1][1]);
             }
         });
     __syncthreads();
     double* red = reinterpret_cast<double*>(smem);
-    // local row l < 4 is tile row 4g + l, l >= 4 is 32 + 4g + (l - 4)
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        const int row = (l < 4 ? 0 : 32) + 4 * g + (l & 3);
-        red[(warp * TILE + row) * MR_RB + 2 * t] = acc[l][0];
-        red[(warp * TILE + row) * MR_RB + 2 * t + 1] = acc[l][1];
+    for (int i = 0; i < 8; ++i) {
+        const int row = 16 * (i >> 1) + 2 * g + (i & 1);
+        red[(warp * TILE + row) * MR_RB + 2 * t] = acc[i][0];
+        red[(warp * TILE + row) * MR_RB + 2 * t + 1] = acc[i][1];
     }
     __syncthreads();
     nform_store(red, int(sg.vo), sg.rows, om, alpha, add);
