@@ -108,7 +108,7 @@ struct hlrc_hmat_s {
     // row-major blocks of MR_RB vectors
     char* mr_arena = nullptr;
     double *mr_x = nullptr, *mr_t = nullptr, *mr_t2 = nullptr, *mr_part = nullptr;
-    char* mr_tables = nullptr;   // column streams of the reduced-precision multi-RHS kernels
+    char* mr_tables = nullptr;   // column streams of reduced-precision stores (MSeg / MCol)
     // host-pointer entry point staging
     double* hx = nullptr;
     double* hy = nullptr;
@@ -528,14 +528,14 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         hp->mr_part = carve(np);
         hp->info.workspace_bytes += int64_t(bytes);
         hp->info.device_bytes += int64_t(bytes);
-        if (p.precision != HLRC_PREC_F64) {
-            const hlrc_status st = upload_streams(p, hp);
-            if (st != HLRC_OK) {
-                cudaFree(hp->mr_tables);
-                cudaFree(hp->mr_arena);
-                cleanup();
-                return st;
-            }
+    }
+    if (p.precision != HLRC_PREC_F64) {
+        const hlrc_status st = upload_streams(p, hp);
+        if (st != HLRC_OK) {
+            cudaFree(hp->mr_tables);
+            cudaFree(hp->mr_arena);
+            cleanup();
+            return st;
         }
     }
     for (int op = 0; op < 3; ++op) {
@@ -646,21 +646,21 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             double* vout = bind(ws, tp.out, x, y);
             const int add = tp.mode == OUT_ADD_ALPHA;
             if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-            const QTTPack* qc = static_cast<const QTTPack*>(tp.chunks);
             constexpr int TW = TTFORM_WARPS;
             if (f64plan && tp.nsegs[FMT_F64] > 0)
                 k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
                     tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
                     reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
-            if (!f64plan && tp.nsegs[FMT_F32] > 0)
-                k_ttform_q<TW, FMT_F32><<<tp.nsegs[FMT_F32], TW * 32, 0, s>>>(tp.segs[FMT_F32], qc, M->store, vin, vout,
-                                                                            ws.part, alpha, add);
-            if (!f64plan && tp.nsegs[FMT_F16] > 0)
-                k_ttform_q<TW, FMT_F16><<<tp.nsegs[FMT_F16], TW * 32, 0, s>>>(tp.segs[FMT_F16], qc, M->store, vin, vout,
-                                                                            ws.part, alpha, add);
-            if (!f64plan && tp.nsegs[FMT_BF16] > 0)
-                k_ttform_q<TW, FMT_BF16><<<tp.nsegs[FMT_BF16], TW * 32, 0, s>>>(tp.segs[FMT_BF16], qc, M->store, vin,
-                                                                              vout, ws.part, alpha, add);
+            // reduced precision: each tile's run of columns, streamed in full 4 KB iterations
+            if (!f64plan && tp.nmseg[FMT_F32] > 0)
+                k_ttform_qs<TW, FMT_F32><<<tp.nmseg[FMT_F32], TW * 32, 0, s>>>(tp.mseg[FMT_F32], tp.mcol, M->store, vin,
+                                                                             vout, ws.part, alpha, add);
+            if (!f64plan && tp.nmseg[FMT_F16] > 0)
+                k_ttform_qs<TW, FMT_F16><<<tp.nmseg[FMT_F16], TW * 32, 0, s>>>(tp.mseg[FMT_F16], tp.mcol, M->store, vin,
+                                                                             vout, ws.part, alpha, add);
+            if (!f64plan && tp.nmseg[FMT_BF16] > 0)
+                k_ttform_qs<TW, FMT_BF16><<<tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(tp.mseg[FMT_BF16], tp.mcol, M->store,
+                                                                               vin, vout, ws.part, alpha, add);
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
@@ -676,13 +676,13 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             const double* vt = bind(ws, np.vt, x, y);
             double* vo = bind(ws, np.out, x, y);
             const int add = np.mode == OUT_ADD_ALPHA;
-            const QNPack* qc = static_cast<const QNPack*>(np.chunks);
             constexpr int NW = NFORM_WARPS;
             // formats in fixed order: each launch adds its part of y
             if (f64plan && np.nsegs[FMT_F64] > 0)
                 k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                     np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
                     reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
+            const QNPack* qc = static_cast<const QNPack*>(np.chunks);
             if (!f64plan && np.nsegs[FMT_F32] > 0)
                 k_nform_q<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(np.segs[FMT_F32], qc, M->store, vx, vt, vo,
                                                                            alpha, add);

@@ -167,17 +167,6 @@ k_nform_q(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const
 
 // -------------------------------------------------------------- tile T-form
 // x of the lane's R rows
-template <int FMT>
-__device__ __forceinline__ void tx_q(const double* vin, const TTSeg& sg, int lane, float* xr) {
-    using F = QFmt<FMT>;
-    const int l = lane & (F::G - 1);
-#pragma unroll
-    for (int r = 0; r < F::R; ++r) {
-        const int row = l * F::R + r;
-        xr[r] = row < sg.rows ? float(__ldg(vin + sg.v_off + row)) : 0.f;
-    }
-}
-
 // per-lane dot products of the 8 loaded column pieces with x
 template <int FMT>
 __device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float* p) {
@@ -193,60 +182,76 @@ __device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float*
     }
 }
 
-// reduce the pack's column partials and write them
-template <int FMT>
-__device__ __forceinline__ void ttreduce_q(const QTTPack& pk, int lane, float* p, double* out, double* part,
-                                           double alpha, int add) {
-    using F = QFmt<FMT>;
-    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
-    const int n0 = pk.p[0].nc, ntot = n0 + pk.p[1].nc;
-    // reduce the 8 column partials over the G lanes of the group; afterwards
-    // the lane holds pack column g + C * (l >> (LOG_G - 3))
-    TransposeReduce<8, F::G / 2, float>::run(p, lane);
-    constexpr int SH = F::LOG_G - 3;
-    const int j = g + F::C * (l >> SH);
-    if ((l & ((1 << SH) - 1)) == 0 && j < ntot) {
-        const QTTChunk& q = j < n0 ? pk.p[0] : pk.p[1];
-        const int jj = j < n0 ? j : j - n0;
-        const double val = double(q.scale) * double(p[0]);
-        if (q.flags & TT_DIRECT) {
-            double* o = out + q.out + jj;
-            if (add) *o += alpha * val;
-            else *o = val;
-        } else {
-            part[q.out + jj] = val;
-        }
-    }
+// ------------------------------------------------------- column streams
+__device__ __forceinline__ MCol ld_mcol(const MCol* p) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+    return MCol{u.x, __uint_as_float(u.y)};
 }
 
+// Tile T-form on the tile's column stream (the chunks of one format that the
+// tile visits, contiguous in the store; see MSeg).  Like k_ttform_q, but a
+// warp iteration takes the next 8*C columns of the run whatever the chunk
+// boundaries, so every iteration moves a full 4 KB even where the chunks
+// are narrow; the output slot and scale of each column come from the
+// per-column table.
 template <int W, int FMT>
 __global__ void __launch_bounds__(W * 32)
-k_ttform_q(const TTSeg* __restrict__ segs, const QTTPack* __restrict__ packs, const uint8_t* __restrict__ A,
-           const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
-           int add) {
+k_ttform_qs(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
+            const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
+            int add) {
     using F = QFmt<FMT>;
-    const TTSeg sg = segs[blockIdx.x];
+    constexpr int BC = 8 * F::C;   // columns per warp iteration
+    constexpr int SH = F::LOG_G - 3;
+    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
     float xr[F::R];
-    tx_q<FMT>(vin, sg, lane, xr);
-    // software pipeline: the loads of pack c + W are issued before pack c is
-    // reduced and written, and descriptors are fetched two iterations ahead
-    uint32_t c = sg.cb + warp;
-    if (c >= sg.ce) return;
-    QTTPack cur = ld_pack(packs + c), nxt{};
-    if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
+#pragma unroll
+    for (int r = 0; r < F::R; ++r) {
+        const int row = l * F::R + r;
+        xr[r] = row < sg.rows ? float(__ldg(vin + sg.vo + row)) : 0.f;
+    }
+    const int ncols = int(sg.ncols);
+    const size_t colb = size_t(sg.ld) * fmt_bytes(FMT);
+    const uint8_t* base = A + size_t(sg.a16) * 16 + size_t(l) * 16;
+    const bool active = l * F::R < sg.ld;
+    const MCol* ctab = cols + sg.col0;
+    // after the reduction the lane holds column jown of the iteration
+    const int jown = g + F::C * (l >> SH);
+    const bool writer = (l & ((1 << SH) - 1)) == 0;
+    auto load = [&](int c0, uint4 (&m)[8]) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int j = c0 + g + F::C * i;
+            m[i] = (active && j < ncols) ? __ldcs(reinterpret_cast<const uint4*>(base + size_t(j) * colb))
+                                         : make_uint4(0u, 0u, 0u, 0u);
+        }
+    };
+    int c0 = warp * BC;
+    if (c0 >= ncols) return;
     uint4 m[8];
-    load_pack<FMT>(A, cur.p[0].a16, cur.p[1].a16, cur.p[0].nc, cur.p[0].nc + cur.p[1].nc, sg.ld, lane, m);
-    for (; c < sg.ce; c += W) {
+    load(c0, m);
+    MCol mc = (writer && c0 + jown < ncols) ? ld_mcol(ctab + c0 + jown) : MCol{0u, 0.f};
+    for (; c0 < ncols; c0 += W * BC) {
         float p[8];
         ttdots_q<FMT>(m, xr, p);
-        const QTTPack done = cur;
-        if (c + W < sg.ce) {
-            cur = nxt;
-            load_pack<FMT>(A, cur.p[0].a16, cur.p[1].a16, cur.p[0].nc, cur.p[0].nc + cur.p[1].nc, sg.ld, lane, m);
-            if (c + 2 * W < sg.ce) nxt = ld_pack(packs + c + 2 * W);
+        const MCol done = mc;
+        const int cd = c0;
+        if (c0 + W * BC < ncols) {
+            load(c0 + W * BC, m);
+            mc = (writer && c0 + W * BC + jown < ncols) ? ld_mcol(ctab + c0 + W * BC + jown) : MCol{0u, 0.f};
         }
-        ttreduce_q<FMT>(done, lane, p, out, part, alpha, add);
+        TransposeReduce<8, F::G / 2, float>::run(p, lane);
+        if (writer && cd + jown < ncols) {
+            const double val = double(done.scale) * double(p[0]);
+            if (done.idx & MC_DIRECT) {
+                double* o = out + (done.idx & ~MC_DIRECT);
+                if (add) *o += alpha * val;
+                else *o = val;
+            } else {
+                part[done.idx] = val;
+            }
+        }
     }
 }
 

@@ -203,11 +203,6 @@ __device__ __forceinline__ void stage_vector(uint8_t* dst, uint32_t idx, int c0,
     }
 }
 
-__device__ __forceinline__ MCol ld_mcol(const MCol* p) {
-    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
-    return MCol{u.x, __uint_as_float(u.y)};
-}
-
 // Epilogue of the tile T-forms: value val (already unscaled) of stream
 // column entry m, right-hand side n, to its output (FP64) or to its partial
 // slot.  Partials are stored in FP32: they are sums of FP32 MMA results of
