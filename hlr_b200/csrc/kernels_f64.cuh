@@ -193,12 +193,7 @@ k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks,
     }
 }
 
-// Sums the per-tile partials of multi-tile tile-T-form outputs.  A group of
-// nc columns with fewer than 32 columns spreads its slots over L lanes per
-// column (slot i goes to lane phase i % L, L a power of two with L * nc <=
-// 32); every lane keeps four interleaved sums, and the L phases are combined
-// by a butterfly.  The order of all sums depends on the group's shape only,
-// so results are reproducible.
+// Sums the per-tile partials of multi-tile tile-T-form outputs in tile order.
 __global__ void __launch_bounds__(256)
 k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,
                double* __restrict__ out, double alpha, int add) {
@@ -206,30 +201,23 @@ k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __r
     if (gid >= ngroups) return;
     const int lane = threadIdx.x & 31;
     const TGroup g = groups[gid];
-    uint32_t L = 1;
-    while (L < 32 && 2 * L * g.nc <= 32) L *= 2;
-    const uint32_t phase = uint32_t(lane) & (L - 1), qstep = 32 / L;
-    const uint32_t qend = (g.nc + qstep - 1) / qstep * qstep;   // same trip count for every lane
-    for (uint32_t j = uint32_t(lane) / L; j < qend; j += qstep) {
+    for (uint32_t j = lane; j < g.nc; j += 32) {
+        // four interleaved partial sums keep four loads in flight; they are
+        // combined in a fixed order, so the result is deterministic
+        const double* p = part + size_t(g.slot0) + j;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        if (j < g.nc) {
-            const double* p = part + size_t(g.slot0) + j;
-            uint32_t i = phase;
-            for (; i + 3 * L < g.nslots; i += 4 * L) {
-                s0 += p[size_t(i) * g.nc];
-                s1 += p[size_t(i + L) * g.nc];
-                s2 += p[size_t(i + 2 * L) * g.nc];
-                s3 += p[size_t(i + 3 * L) * g.nc];
-            }
-            for (; i < g.nslots; i += L) s0 += p[size_t(i) * g.nc];
+        uint32_t i = 0;
+        for (; i + 4 <= g.nslots; i += 4) {
+            s0 += p[size_t(i) * g.nc];
+            s1 += p[size_t(i + 1) * g.nc];
+            s2 += p[size_t(i + 2) * g.nc];
+            s3 += p[size_t(i + 3) * g.nc];
         }
-        double s = (s0 + s1) + (s2 + s3);
-        for (uint32_t m = 1; m < L; m *= 2) s += __shfl_xor_sync(0xffffffffu, s, int(m));
-        if (phase == 0 && j < g.nc) {
-            double* o = out + g.out + j;
-            if (add) *o += alpha * s;
-            else *o = s;
-        }
+        for (; i < g.nslots; ++i) s0 += p[size_t(i) * g.nc];
+        const double s = (s0 + s1) + (s2 + s3);
+        double* o = out + g.out + j;
+        if (add) *o += alpha * s;
+        else *o = s;
     }
 }
 
