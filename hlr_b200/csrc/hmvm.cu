@@ -71,9 +71,12 @@ struct DevTTPass {
     int in = V_X, out = V_T, mode = OUT_SET;
     int64_t bytes = 0, alg_bytes = 0;
     int launches() const {
-        int n = ngroups > 0 ? 1 : 0;
-        for (int f = 0; f < 4; ++f) n += nsegs[f] > 0 ? 1 : 0;
-        return n;
+        const int n = ngroups > 0 ? 1 : 0;
+        // reduced-precision stores: one grid for the runs of all formats
+        if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] > 0) return n + 1;
+        int k = n;
+        for (int f = 0; f < 4; ++f) k += nsegs[f] > 0 ? 1 : 0;
+        return k;
     }
 };
 
@@ -381,16 +384,14 @@ hlrc_status enable_tc_smem(int dev) {
     static std::vector<int> done;
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_T16)));
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_T16)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_mr<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_TT)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_mr<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tc_smem_bytes(TC_STAGE_TT)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N16)));
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_T32)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N32)));
     done.push_back(dev);
@@ -651,16 +652,17 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
                     tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
                     reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
-            // reduced precision: each tile's run of columns, streamed in full 4 KB iterations
-            if (!f64plan && tp.nmseg[FMT_F32] > 0)
-                k_ttform_qs<TW, FMT_F32><<<tp.nmseg[FMT_F32], TW * 32, 0, s>>>(tp.mseg[FMT_F32], tp.mcol, M->store, vin,
-                                                                             vout, ws.part, alpha, add);
-            if (!f64plan && tp.nmseg[FMT_F16] > 0)
-                k_ttform_qs<TW, FMT_F16><<<tp.nmseg[FMT_F16], TW * 32, 0, s>>>(tp.mseg[FMT_F16], tp.mcol, M->store, vin,
-                                                                             vout, ws.part, alpha, add);
-            if (!f64plan && tp.nmseg[FMT_BF16] > 0)
-                k_ttform_qs<TW, FMT_BF16><<<tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(tp.mseg[FMT_BF16], tp.mcol, M->store,
-                                                                               vin, vout, ws.part, alpha, add);
+            // reduced precision: each tile's run of columns, streamed in full 4 KB
+            // iterations; FP32 and 16-bit runs in one grid
+            if (!f64plan) {
+                const int n32 = tp.nmseg[FMT_F32];
+                if (tp.nmseg[FMT_BF16] > 0)
+                    k_ttform_qs<TW, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
+                        tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part, alpha, add);
+                else if (n32 + tp.nmseg[FMT_F16] > 0)
+                    k_ttform_qs<TW, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
+                        tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part, alpha, add);
+            }
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
@@ -752,15 +754,14 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                             tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, M->mr_part,
                             alpha, add);
                 } else {
-                    if (tp.nmseg[FMT_F32] > 0)
-                        k_ttform_d32<<<tp.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T32), s>>>(
-                            tp.mseg[FMT_F32], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
-                    if (tp.nmseg[FMT_F16] > 0)
-                        k_ttform_tc<FMT_F16><<<tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
+                    const int n32 = tp.nmseg[FMT_F32];
+                    float* fpart = reinterpret_cast<float*>(M->mr_part);
                     if (tp.nmseg[FMT_BF16] > 0)
-                        k_ttform_tc<FMT_BF16><<<tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_T16), s>>>(
-                            tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, reinterpret_cast<float*>(M->mr_part), alpha, add);
+                        k_ttform_mr<FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
+                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
+                    else if (n32 + tp.nmseg[FMT_F16] > 0)
+                        k_ttform_mr<FMT_F16><<<n32 + tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
+                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
                 }
                 if (ws_profile(M)) prof_end(M, s);
                 if (tp.ngroups > 0) {

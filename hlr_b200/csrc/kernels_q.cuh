@@ -195,14 +195,12 @@ __device__ __forceinline__ MCol ld_mcol(const MCol* p) {
 // are narrow; the output slot and scale of each column come from the
 // per-column table.
 template <int W, int FMT>
-__global__ void __launch_bounds__(W * 32)
-k_ttform_qs(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-            const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
-            int add) {
+__device__ __forceinline__ void ttform_qs(const MSeg& sg, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
+                                          const double* __restrict__ vin, double* __restrict__ out,
+                                          double* __restrict__ part, double alpha, int add) {
     using F = QFmt<FMT>;
     constexpr int BC = 8 * F::C;   // columns per warp iteration
     constexpr int SH = F::LOG_G - 3;
-    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
     float xr[F::R];
@@ -253,6 +251,19 @@ k_ttform_qs(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
             }
         }
     }
+}
+
+// All stream segments of one tile T-form pass in one grid: the first n32
+// CTAs take the FP32 runs, the others the runs of the 16-bit format F16.
+// The outputs of the two formats are disjoint, so their CTAs may run side
+// by side, and the pass has a single tail.
+template <int W, int F16>
+__global__ void __launch_bounds__(W * 32)
+k_ttform_qs(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
+            const uint8_t* __restrict__ A, const double* __restrict__ vin, double* __restrict__ out,
+            double* __restrict__ part, double alpha, int add) {
+    if (int(blockIdx.x) < n32) ttform_qs<W, FMT_F32>(segs32[blockIdx.x], cols, A, vin, out, part, alpha, add);
+    else ttform_qs<W, F16>(segs16[blockIdx.x - n32], cols, A, vin, out, part, alpha, add);
 }
 
 }  // namespace hlrc

@@ -286,12 +286,10 @@ __device__ __forceinline__ void nform_store(const double* red, int out, int rows
 // stream column m, tile row k, read with ldmatrix from the staged columns;
 // B[k][n] = x row k, right-hand side n.
 template <int FMT>
-__global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-            const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
+__device__ __forceinline__ void ttform_tc(const MSeg& sg, uint8_t* smem, const MCol* __restrict__ cols,
+                                          const uint8_t* __restrict__ A, const double* __restrict__ vin,
+                                          const OutMap& om, float* __restrict__ part, double alpha, int add) {
     using O = TcOp<FMT>;
-    extern __shared__ __align__(16) uint8_t smem[];
-    const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T16);
@@ -481,11 +479,9 @@ k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const u
 //     row 8j + 2t + b; m-tiles are 8 stream columns.
 
 // Tile T-form: one CTA per input tile; x in FP64 registers; 16-column stages.
-__global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-             const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const MSeg sg = segs[blockIdx.x];
+__device__ __forceinline__ void ttform_d32(const MSeg& sg, uint8_t* smem, const MCol* __restrict__ cols,
+                                           const uint8_t* __restrict__ A, const double* __restrict__ vin,
+                                           const OutMap& om, float* __restrict__ part, double alpha, int add) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T32);
@@ -599,6 +595,21 @@ k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
     }
     __syncthreads();
     nform_store(red, int(sg.vo), sg.rows, om, alpha, add);
+}
+
+// One tile T-form pass of a reduced-precision store in one grid: the first
+// n32 CTAs take the FP32 runs (FP64 tensor cores), the others the runs of the
+// 16-bit format F16.  The outputs of the two formats are disjoint.  Dynamic
+// shared memory: tc_smem_bytes(TC_STAGE_TT).
+constexpr int TC_STAGE_TT = TC_STAGE_T16 > TC_STAGE_T32 ? TC_STAGE_T16 : TC_STAGE_T32;
+template <int F16>
+__global__ void __launch_bounds__(TC_WARPS * 32)
+k_ttform_mr(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
+            const uint8_t* __restrict__ A, const double* __restrict__ vin, OutMap om, float* __restrict__ part,
+            double alpha, int add) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    if (int(blockIdx.x) < n32) ttform_d32(segs32[blockIdx.x], smem, cols, A, vin, om, part, alpha, add);
+    else ttform_tc<F16>(segs16[blockIdx.x - n32], smem, cols, A, vin, om, part, alpha, add);
 }
 
 }  // namespace hlrc
