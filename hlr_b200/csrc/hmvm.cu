@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "common.hpp"
@@ -48,10 +49,14 @@ struct DevNPass {
     const MSeg* mseg[4] = {};         // multi-RHS column streams (reduced precision)
     int nmseg[4] = {0, 0, 0, 0};
     const MCol* mcol = nullptr;
+    const NSeg2* seg2 = nullptr;      // reduced precision: both formats of a tile in one CTA
+    int nseg2 = 0;
+    int f16 = FMT_F16;                // the store's 16-bit format
     const void* chunks = nullptr;     // NChunk (FP64 plan) or QNChunk (reduced precision)
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0, alg_bytes = 0;
     int launches() const {
+        if (nseg2 > 0) return 1;
         int n = 0;
         for (int f = 0; f < 4; ++f) n += nsegs[f] > 0 ? 1 : 0;
         return n;
@@ -162,7 +167,7 @@ const char* stage_name(int kind, int nk, int idx) {
 // Offsets of every array inside the single device arena of a handle.
 struct ArenaLayout {
     size_t store = 0;
-    std::vector<size_t> tu, ts, tg, nc, ttc, ttg;
+    std::vector<size_t> tu, ts, tg, nc, ttc, ttg, n2;
     std::vector<std::array<size_t, 4>> ns, tts;   // per pass, per StoreFmt
     size_t t = 0, t2 = 0, part = 0, err = 0, total = 0;
     size_t part_elems = 0;
@@ -187,6 +192,10 @@ ArenaLayout arena_layout(const Plan& p) {
         for (int f = 0; f < 4; ++f) o[size_t(f)] = take(np.segs[f].size() * sizeof(NSeg));
         L.ns.push_back(o);
         L.nc.push_back(take(np.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(NChunk) : sizeof(QNPack))));
+        L.n2.push_back(take(p.precision == HLRC_PREC_F64
+                                ? 0
+                                : (np.segs[FMT_F32].size() + np.segs[FMT_F16].size() + np.segs[FMT_BF16].size()) *
+                                      sizeof(NSeg2)));
     }
     size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
     for (const TTPass& tp : p.ttpasses) {
@@ -463,6 +472,35 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         if (e == cudaSuccess) e = put(o_nc[i], enc.data(), enc.size());
         d.chunks = hp->arena + o_nc[i];
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
+        if (!f64 && e == cudaSuccess) {
+            // pair the FP32 and 16-bit segments of every output tile
+            d.f16 = np.segs[FMT_BF16].empty() ? FMT_F16 : FMT_BF16;
+            const std::vector<NSeg> s32 = remap_segs(np.segs[FMT_F32], pack_of);
+            const std::vector<NSeg> s16 = remap_segs(np.segs[d.f16], pack_of);
+            std::vector<NSeg2> pairs;
+            std::vector<int64_t> weight;
+            std::unordered_map<uint32_t, size_t> by_out;
+            for (const NSeg& g : s32) {
+                by_out[g.out] = pairs.size();
+                pairs.push_back(NSeg2{g.cb, g.ce, 0, 0, g.out, g.rows, g.ld, 0, 0, 0});
+            }
+            for (const NSeg& g : s16) {
+                auto it = by_out.find(g.out);
+                if (it == by_out.end()) {
+                    pairs.push_back(NSeg2{0, 0, g.cb, g.ce, g.out, g.rows, 0, g.ld, 0, 0});
+                } else {
+                    NSeg2& q = pairs[it->second];
+                    q.cb16 = g.cb; q.ce16 = g.ce; q.ld16 = g.ld;
+                }
+            }
+            // heaviest tiles first (packs are at most 4 KB each)
+            std::stable_sort(pairs.begin(), pairs.end(), [](const NSeg2& a, const NSeg2& b) {
+                return (a.ce32 - a.cb32) + (a.ce16 - a.cb16) > (b.ce32 - b.cb32) + (b.ce16 - b.cb16);
+            });
+            e = put(L.n2[i], pairs.data(), pairs.size() * sizeof(NSeg2));
+            d.seg2 = reinterpret_cast<const NSeg2*>(hp->arena + L.n2[i]);
+            d.nseg2 = int(pairs.size());
+        }
         hp->n.push_back(d);
     }
     for (size_t i = 0; e == cudaSuccess && i < p.ttpasses.size(); ++i) {
@@ -684,16 +722,14 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                     np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
                     reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
+            // reduced precision: one CTA per tile takes the packs of both formats
             const QNPack* qc = static_cast<const QNPack*>(np.chunks);
-            if (!f64plan && np.nsegs[FMT_F32] > 0)
-                k_nform_q<NW, FMT_F32><<<np.nsegs[FMT_F32], NW * 32, 0, s>>>(np.segs[FMT_F32], qc, M->store, vx, vt, vo,
-                                                                           alpha, add);
-            if (!f64plan && np.nsegs[FMT_F16] > 0)
-                k_nform_q<NW, FMT_F16><<<np.nsegs[FMT_F16], NW * 32, 0, s>>>(np.segs[FMT_F16], qc, M->store, vx, vt, vo,
-                                                                           alpha, add);
-            if (!f64plan && np.nsegs[FMT_BF16] > 0)
-                k_nform_q<NW, FMT_BF16><<<np.nsegs[FMT_BF16], NW * 32, 0, s>>>(np.segs[FMT_BF16], qc, M->store, vx, vt,
-                                                                             vo, alpha, add);
+            if (!f64plan && np.nseg2 > 0) {
+                if (np.f16 == FMT_BF16)
+                    k_nform_q<NW, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha, add);
+                else
+                    k_nform_q<NW, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha, add);
+            }
             if (ws.profile) prof_end(M, s);
             HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
         }

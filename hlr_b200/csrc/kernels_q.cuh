@@ -132,28 +132,56 @@ __device__ __forceinline__ void nflush_q(double* acc, int lane, double* red_row)
         for (int r = 0; r < F::R; ++r) red_row[(lane & (F::G - 1)) * F::R + r] = acc[r];
 }
 
-// one storage format per launch: a tile's packs of format FMT
+// sum the C column groups of the accumulators and add rows to red[]
+template <int FMT>
+__device__ __forceinline__ void nflush_add_q(double* acc, int lane, double* red_row) {
+    using F = QFmt<FMT>;
+#pragma unroll
+    for (int o = F::G; o < 32; o <<= 1)
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+    if ((lane >> F::LOG_G) == 0)
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) red_row[(lane & (F::G - 1)) * F::R + r] += acc[r];
+}
+
+// a warp's share (packs cb + warp, cb + warp + W, ...) of one format's packs
+// of a tile, with the next descriptor read ahead
 template <int W, int FMT>
-__global__ void __launch_bounds__(W * 32)
-k_nform_q(const NSeg* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
+__device__ __forceinline__ void npacks_q(uint32_t cb, uint32_t ce, int ld, const QNPack* __restrict__ packs,
+                                         const uint8_t* __restrict__ A, const double* __restrict__ vx,
+                                         const double* __restrict__ vt, int warp, int lane, double* acc) {
+    uint32_t c = cb + warp;
+    QNPack nxt{};
+    if (c < ce) nxt = ld_pack(packs + c);
+    for (; c < ce; c += W) {
+        const QNPack pk = nxt;
+        if (c + W < ce) nxt = ld_pack(packs + c + W);
+        npack_q<FMT>(pk, A, vx, vt, ld, lane, acc);
+    }
+}
+
+// N-form of a reduced-precision store: a CTA takes one output tile, both its
+// FP32 packs and its packs of the 16-bit format F16 (either may be empty),
+// sums them in FP64 and updates y once.
+template <int W, int F16>
+__global__ void __launch_bounds__(W * 32, 3)
+k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
           const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
           int add) {
-    using F = QFmt<FMT>;
     __shared__ double red[W][TILE];
-    const NSeg sg = segs[blockIdx.x];
+    const NSeg2 sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double acc[F::R];
+    double a32[QFmt<FMT_F32>::R], a16[QFmt<F16>::R];
 #pragma unroll
-    for (int r = 0; r < F::R; ++r) acc[r] = 0.0;
-    uint32_t c = sg.cb + warp;
-    QNPack nxt{};
-    if (c < sg.ce) nxt = ld_pack(packs + c);
-    for (; c < sg.ce; c += W) {
-        const QNPack pk = nxt;
-        if (c + W < sg.ce) nxt = ld_pack(packs + c + W);
-        npack_q<FMT>(pk, A, vx, vt, sg.ld, lane, acc);
-    }
-    nflush_q<FMT>(acc, lane, red[warp]);
+    for (int r = 0; r < QFmt<FMT_F32>::R; ++r) a32[r] = 0.0;
+#pragma unroll
+    for (int r = 0; r < QFmt<F16>::R; ++r) a16[r] = 0.0;
+    npacks_q<W, FMT_F32>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
+    npacks_q<W, F16>(sg.cb16, sg.ce16, sg.ld16, packs, A, vx, vt, warp, lane, a16);
+    nflush_q<FMT_F32>(a32, lane, red[warp]);
+    __syncwarp();
+    nflush_add_q<F16>(a16, lane, red[warp]);
     __syncthreads();
     if (threadIdx.x < sg.rows) {
         double s = 0.0;

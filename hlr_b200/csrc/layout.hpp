@@ -143,6 +143,19 @@ struct QNPack { QNChunk p[2]; };
 struct QTTPack { QTTChunk p[2]; };
 static_assert(sizeof(QNPack) == 32 && sizeof(QTTPack) == 32, "packs must be 32 bytes");
 
+// One output tile of a reduced-precision N-form pass with the packs of both
+// of its formats: FP32 packs [cb32, ce32) and packs of the store's 16-bit
+// format [cb16, ce16), each range possibly empty.
+struct NSeg2 {
+    uint32_t cb32, ce32, cb16, ce16;
+    uint32_t out;          // offset of the tile's first output entry
+    uint16_t rows;         // rows of the tile (<= 64)
+    uint16_t ld32, ld16;   // leading dimensions of the two formats
+    uint16_t pad0;
+    uint32_t pad1;
+};
+static_assert(sizeof(NSeg2) == 32, "NSeg2 is 32 bytes");
+
 // ------------------------------------------------ multi-RHS column streams
 // The reduced-precision stores are laid out so that the chunks of one format
 // that one pass segment (tile) visits are contiguous: the multi-RHS kernels
