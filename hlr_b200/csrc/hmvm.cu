@@ -72,11 +72,13 @@ struct DevTTPass {
     const void* chunks = nullptr;     // TTChunk (FP64 plan) or QTTChunk
     const TGroup* groups = nullptr;
     int ngroups = 0;
+    const TGroup* groups1 = nullptr;  // first finish level (long outputs), into the partial array
+    int ngroups1 = 0;
     int64_t npart = 0;
     int in = V_X, out = V_T, mode = OUT_SET;
     int64_t bytes = 0, alg_bytes = 0;
     int launches() const {
-        const int n = ngroups > 0 ? 1 : 0;
+        const int n = (ngroups > 0 ? 1 : 0) + (ngroups1 > 0 ? 1 : 0);
         // reduced-precision stores: one grid for the runs of all formats
         if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] > 0) return n + 1;
         int k = n;
@@ -167,7 +169,7 @@ const char* stage_name(int kind, int nk, int idx) {
 // Offsets of every array inside the single device arena of a handle.
 struct ArenaLayout {
     size_t store = 0;
-    std::vector<size_t> tu, ts, tg, nc, ttc, ttg, n2;
+    std::vector<size_t> tu, ts, tg, nc, ttc, ttg, ttg1, n2;
     std::vector<std::array<size_t, 4>> ns, tts;   // per pass, per StoreFmt
     size_t t = 0, t2 = 0, part = 0, err = 0, total = 0;
     size_t part_elems = 0;
@@ -204,6 +206,7 @@ ArenaLayout arena_layout(const Plan& p) {
         L.tts.push_back(o);
         L.ttc.push_back(take(tp.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(TTChunk) : sizeof(QTTPack))));
         L.ttg.push_back(take(tp.groups.size() * sizeof(TGroup)));
+        L.ttg1.push_back(take(tp.groups1.size() * sizeof(TGroup)));
         part_elems = std::max(part_elems, size_t(tp.npart));
     }
     L.t = take(size_t(std::max<int64_t>(1, p.n_t)) * sizeof(double));
@@ -516,9 +519,12 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         }
         if (e == cudaSuccess) e = put(L.ttc[i], enc.data(), enc.size());
         if (e == cudaSuccess) e = put(L.ttg[i], tp.groups.data(), tp.groups.size() * sizeof(TGroup));
+        if (e == cudaSuccess) e = put(L.ttg1[i], tp.groups1.data(), tp.groups1.size() * sizeof(TGroup));
         d.chunks = hp->arena + L.ttc[i];
         d.groups = reinterpret_cast<const TGroup*>(hp->arena + L.ttg[i]);
         d.ngroups = int(tp.groups.size());
+        d.groups1 = reinterpret_cast<const TGroup*>(hp->arena + L.ttg1[i]);
+        d.ngroups1 = int(tp.groups1.size());
         d.npart = tp.npart;
         d.in = tp.in; d.out = tp.out; d.mode = tp.mode; d.bytes = tp.bytes; d.alg_bytes = tp.alg_bytes;
         hp->tt.push_back(d);
@@ -704,6 +710,9 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
+                if (tp.ngroups1 > 0)   // first level: runs of slots into the scratch part of the partials
+                    k_ttfinish_f64<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, ws.part, ws.part, 1.0,
+                                                                         0);
                 k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
                 if (ws.profile) prof_end(M, s);
             }
@@ -803,12 +812,22 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 if (tp.ngroups > 0) {
                     if (ws_profile(M))
                         prof_begin(M, "ttfinish", tp.npart * MR_RB * (M->precision == HLRC_PREC_F64 ? 8 : 4), s);
-                    if (M->precision == HLRC_PREC_F64)
+                    // first level: runs of slots into the scratch part of the partials
+                    const OutMap pm{M->mr_part, MR_RB, 1, MR_RB};
+                    float* fpart = reinterpret_cast<float*>(M->mr_part);
+                    if (M->precision == HLRC_PREC_F64) {
+                        if (tp.ngroups1 > 0)
+                            k_ttfinish_f64_mr<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, M->mr_part,
+                                                                                   pm, 1.0, 0);
                         k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om,
                                                                               alpha, add);
-                    else
-                        k_ttfinish_f32_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(
-                            tp.groups, tp.ngroups, reinterpret_cast<const float*>(M->mr_part), om, alpha, add);
+                    } else {
+                        if (tp.ngroups1 > 0)
+                            k_ttfinish_f32_mr<true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, fpart,
+                                                                                         pm, fpart, 1.0, 0);
+                        k_ttfinish_f32_mr<false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, fpart, om,
+                                                                                     nullptr, alpha, add);
+                    }
                     if (ws_profile(M)) prof_end(M, s);
                 }
                 HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));

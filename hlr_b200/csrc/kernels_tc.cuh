@@ -223,8 +223,11 @@ __device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const O
 // outputs in FP64: slot i, column j, vector k of a group is
 // part[(slot0 + i*nc + j)*MR_RB + k].  A lane owns four vectors of one
 // column and keeps four interleaved sums; fixed order.
+// With TO_PART the sums are written as FP32 partials (the first level of a
+// two-level finish) to part_out[(g.out + j)*MR_RB + k] instead of to om.
+template <bool TO_PART>
 __global__ void __launch_bounds__(256)
-k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* __restrict__ part, OutMap om,
+k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* part, OutMap om, float* part_out,
                   double alpha, int add) {
     const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (gid >= ngroups) return;
@@ -251,13 +254,19 @@ k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* _
             const float4 v = __ldcs(p + size_t(i) * n4);
             s[0][0] += v.x; s[0][1] += v.y; s[0][2] += v.z; s[0][3] += v.w;
         }
-        double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
+        if constexpr (TO_PART) {
+            float* o = part_out + size_t(g.out + j) * MR_RB + k;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            if (k + e >= om.nr) break;
-            const double r = (s[0][e] + s[1][e]) + (s[2][e] + s[3][e]);
-            if (add) o[e * om.cs] += alpha * r;
-            else o[e * om.cs] = r;
+            for (int e = 0; e < 4; ++e) o[e] = float((s[0][e] + s[1][e]) + (s[2][e] + s[3][e]));
+        } else {
+            double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                if (k + e >= om.nr) break;
+                const double r = (s[0][e] + s[1][e]) + (s[2][e] + s[3][e]);
+                if (add) o[e * om.cs] += alpha * r;
+                else o[e * om.cs] = r;
+            }
         }
     }
 }

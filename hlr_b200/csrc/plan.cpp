@@ -426,6 +426,24 @@ struct TTBuilder {
                 P.bytes += e.first;
             }
         }
+        // Outputs with more than FINISH_SLOTS tiles are summed in two levels,
+        // so that no warp adds more than FINISH_SLOTS slots in a row: the
+        // slots are cut into runs whose sums go to a scratch region appended
+        // to the partial array (layout [run][column], like the slots), and
+        // the output's group then sums the runs.  The order of all additions
+        // depends on the shapes only.
+        for (TGroup& g : P.groups) {
+            if (g.nslots <= FINISH_SLOTS) continue;
+            const uint32_t nrun = (g.nslots + FINISH_SLOTS - 1) / FINISH_SLOTS;
+            const uint32_t scratch = uint32_t(P.npart);
+            for (uint32_t r = 0; r < nrun; ++r) {
+                const uint32_t s0 = r * FINISH_SLOTS;
+                P.groups1.push_back({g.slot0 + s0 * g.nc, std::min(FINISH_SLOTS, g.nslots - s0), scratch + r * g.nc, g.nc});
+            }
+            P.npart += int64_t(nrun) * g.nc;
+            g.slot0 = scratch;
+            g.nslots = nrun;
+        }
     }
 };
 
@@ -576,6 +594,9 @@ hlrc_status validate_plan(const Plan& p) {
         for (const TGroup& g : tp.groups)
             if (int64_t(g.slot0) + int64_t(g.nslots) * g.nc > tp.npart || int64_t(g.out) + g.nc > vec_len(tp.out))
                 return fail(HLRC_ERR_INTERNAL, "T-pass %zu: finish group outside its arrays", pi);
+        for (const TGroup& g : tp.groups1)
+            if (int64_t(g.slot0) + int64_t(g.nslots) * g.nc > tp.npart || int64_t(g.out) + g.nc > tp.npart)
+                return fail(HLRC_ERR_INTERNAL, "T-pass %zu: first-level finish group outside the partials", pi);
     }
     return HLRC_OK;
 }

@@ -67,10 +67,16 @@ struct TTPass {
     std::vector<TTSeg> segs[4];    // per StoreFmt, ordered by cost (descending)
     std::vector<GChunk> chunks;
     std::vector<TGroup> groups;    // multi-tile outputs: partials summed in tile order
-    int64_t npart = 0;             // partial array length (doubles)
+    // first level of the finish for outputs with many tiles: each entry sums
+    // at most FINISH_SLOTS slots into the scratch region at the end of the
+    // partial array, which the entry's final group in `groups` then reads
+    std::vector<TGroup> groups1;
+    int64_t npart = 0;             // partial array length (doubles), scratch region included
     int in = V_X, out = V_T, mode = OUT_SET;
     int64_t bytes = 0, alg_bytes = 0;
 };
+
+constexpr uint32_t FINISH_SLOTS = 16;   // slots one finish warp sums serially
 
 // One stage of a product: exactly one of the passes is used.
 struct Stage {
