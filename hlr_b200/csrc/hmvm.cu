@@ -405,7 +405,7 @@ hlrc_status enable_tc_smem(int dev) {
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_N32)));
+                                   tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32)));
     done.push_back(dev);
     return HLRC_OK;
 }
@@ -791,7 +791,6 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 const int add = tp.mode == OUT_ADD_ALPHA;
                 const OutMap om = omap(tp.out);
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-                const QTTPack* qp = static_cast<const QTTPack*>(tp.chunks);
                 constexpr int TW = TTFORM_WARPS;
                 if (M->precision == HLRC_PREC_F64) {
                     if (tp.nsegs[FMT_F64] > 0)
@@ -837,7 +836,6 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
                 const int add = np.mode == OUT_ADD_ALPHA;
                 const OutMap om = omap(np.out);
-                const QNPack* qp = static_cast<const QNPack*>(np.chunks);
                 constexpr int NW = NFORM_WARPS;
                 const bool f64plan = M->precision == HLRC_PREC_F64;
                 if (f64plan && np.nsegs[FMT_F64] > 0)
@@ -845,7 +843,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
                 if (!f64plan && np.nmseg[FMT_F32] > 0)
-                    k_nform_d32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32), s>>>(
+                    k_nform_d32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32), s>>>(
                         np.mseg[FMT_F32], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (!f64plan && np.nmseg[FMT_F16] > 0)
                     k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(

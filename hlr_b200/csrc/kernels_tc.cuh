@@ -47,8 +47,13 @@ constexpr int TC_STAGE_T16 = 32 * TC_A16_STRIDE + 32 * 8;                       
 constexpr int TC_STAGE_N32 = 16 * TC_A32_STRIDE + 16 * TC_V_STRIDE + 16 * 4;
 constexpr int TC_STAGE_T32 = 16 * TC_A32_STRIDE + 16 * 8;
 
-// dynamic shared memory of a launch: one ring of TC_STAGES stages per warp
-constexpr int tc_smem_bytes(int stage) { return TC_WARPS * TC_STAGES * stage; }
+#ifndef HLRC_D32_STAGES
+#define HLRC_D32_STAGES 2
+#endif
+constexpr int TC_STAGES_D32 = HLRC_D32_STAGES;   // ring depth of the FP32 N-form
+
+// dynamic shared memory of a launch: one ring of `nst` stages per warp
+constexpr int tc_smem_bytes(int stage, int nst = TC_STAGES) { return TC_WARPS * nst * stage; }
 
 template <int FMT> struct TcOp;
 
@@ -146,24 +151,24 @@ __device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* row) {
 // stream through its ring: issue(slot, s) starts the copies of stage s into
 // ring slot `slot`, and compute(slot, s) consumes the slot once its copies
 // have landed.
-template <typename Issue, typename Compute>
+template <int RING = TC_STAGES, typename Issue, typename Compute>
 __device__ __forceinline__ void warp_stream(int nst, int warp, Issue&& issue, Compute&& compute) {
     const int n = nst > warp ? (nst - warp + TC_WARPS - 1) / TC_WARPS : 0;
     int issued = 0;
     auto issue_next = [&]() {
         if (issued < n) {
-            issue(issued % TC_STAGES, warp + issued * TC_WARPS);
+            issue(issued % RING, warp + issued * TC_WARPS);
             ++issued;
         }
         cp_commit();
     };
 #pragma unroll
-    for (int k = 0; k < TC_STAGES - 1; ++k) issue_next();
+    for (int k = 0; k < RING - 1; ++k) issue_next();
     for (int k = 0; k < n; ++k) {
         issue_next();
-        cp_wait<TC_STAGES - 1>();
+        cp_wait<RING - 1>();
         __syncwarp();
-        compute(k % TC_STAGES, warp + k * TC_WARPS);
+        compute(k % RING, warp + k * TC_WARPS);
         __syncwarp();
     }
 }
@@ -527,9 +532,11 @@ __device__ __forceinline__ void ttform_d32(const MSeg& sg, uint8_t* smem, const 
                 if (8 * mt >= cnt) break;
                 const uint8_t* ca = sa + (8 * mt + g) * TC_A32_STRIDE + 8 * t;
                 double d[2] = {0.0, 0.0};
+                // all 8 row steps: rows past the tile hold zero-filled
+                // columns and zero x entries
+                (void)nj;
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
-                    if (jj >= nj) break;
                     const float2 a = *reinterpret_cast<const float2*>(ca + 32 * jj);
                     dmma(d, double(a.x), xv[2 * jj]);
                     dmma(d, double(a.y), xv[2 * jj + 1]);
@@ -553,7 +560,7 @@ k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_N32);
+    uint8_t* ring = smem + warp * (TC_STAGES_D32 * TC_STAGE_N32);
     const int colb = sg.ld * 4, ncols = int(sg.ncols);
     const uint8_t* base = A + size_t(sg.a16) * 16;
     const MCol* ctab = cols + sg.col0;
@@ -563,7 +570,7 @@ k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
 #pragma unroll
     for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
     MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<TC_STAGES_D32>(
         (ncols + 15) / 16, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_N32;
@@ -578,16 +585,18 @@ k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
             const uint8_t* sa = ring + slot * TC_STAGE_N32;
             const double* sv = reinterpret_cast<const double*>(sa + 16 * TC_A32_STRIDE);
             const float* ssc = reinterpret_cast<const float*>(sa + 16 * (TC_A32_STRIDE + TC_V_STRIDE));
-            const int nks = (min(16, ncols - 16 * st) + 3) / 4;
+            // every stage runs in full: the copies zero-fill the columns past
+            // the run (and their vector entries and scales) and the rows past
+            // the column height, so the extra products add zeros, and the
+            // loads and conversions of a stage can all be issued up front
+            (void)np;
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
-                if (ks >= nks) break;
                 const int col = 4 * ks + t;
                 const double b = sv[col * (TC_V_STRIDE / 8) + g] * double(ssc[col]);
                 const uint8_t* ca = sa + col * TC_A32_STRIDE + 8 * g;
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
-                    if (p >= np) break;
                     const float2 a = *reinterpret_cast<const float2*>(ca + 64 * p);
                     dmma(acc[2 * p], double(a.x), b);
                     dmma(acc[2 * p + 1], double(a.y), b);

@@ -173,6 +173,9 @@ struct MSeg {
 static_assert(sizeof(MSeg) == 24, "MSeg is 24 bytes");
 
 constexpr uint32_t MC_DIRECT = 0x80000000u;   // tile T-form column table: output, not partial slot
+// Longest run of partial slots one finish lane sums: longer outputs are
+// summed in two levels (runs of at most FINISH_SLOTS slots first).
+constexpr uint32_t FINISH_SLOTS = 16;
 struct MCol {
     uint32_t idx;          // N-form: vector entry (| VEC_T: in t); T-form: output (| MC_DIRECT) or partial
     float scale;           // the chunk's scale (1 for FP32)

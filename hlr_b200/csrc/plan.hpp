@@ -76,8 +76,6 @@ struct TTPass {
     int64_t bytes = 0, alg_bytes = 0;
 };
 
-constexpr uint32_t FINISH_SLOTS = 16;   // slots one finish warp sums serially
-
 // One stage of a product: exactly one of the passes is used.
 struct Stage {
     int kind;                      // 0 = T-form (units), 1 = N-form, 2 = tile T-form
