@@ -393,7 +393,9 @@ def run_ours(args, rank, world, local_rank):
         name, (cnt, tot_ms, by) = dom
         avg_ms = tot_ms / max(1, cnt)
         achieved = by / (avg_ms / 1e3) / 1e9
-        traffic = traffic_from_profiles(name, args.config)
+        # the summaries key a workload as config[/precision][/nrhs]
+        wl = args.config + ("" if prec == "f64" else "/" + prec) + ("" if nrhs == 1 else f"/{nrhs}")
+        traffic = traffic_from_profiles(name, wl)
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                 "bytes_per_launch": by, "avg_ms": avg_ms,
@@ -583,7 +585,9 @@ def run_batch(args, rank, world, local_rank):
 
 def traffic_from_profiles(kernel: str, config: str):
     """DRAM bytes per launch of `kernel` from a committed ncu summary table
-    row `| kernel | config | bytes |` in profiles/*.md, if any."""
+    row `| kernel | workload | bytes |` in profiles/*.md, if any; the
+    workload is the config, then /precision unless FP64, then /nrhs unless 1
+    (e.g. c2, c2/mixed, c2/mixed/8)."""
     for p in sorted((ROOT / "profiles").glob("*.md")):
         for ln in p.read_text().splitlines():
             parts = [s.strip() for s in ln.strip().strip("|").split("|")]
