@@ -7,7 +7,8 @@ eps = 1e-6, one right-hand side x ~ N(0,1).  Synthetic inputs, built on the
 host by the library's own construction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c2|c1|c3|c2s|c4] [--no-cpu-baseline]
+                    [--config c2|c1|c3|c2s|c4|c5] [--precision P] [--nrhs K]
+                    [--no-cpu-baseline] [--no-autotune]
 
 Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
 independent replica of the product on its own GPU (the MVM has no exchange
@@ -280,6 +281,7 @@ def run_ours(args, rank, world, local_rank):
     tu = time.perf_counter()
     M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs)
     t_upload = time.perf_counter() - tu
+    tuned = tune_handle(M, nrhs, args)
     info = M.info
     n = hm.n
     # x ~ N(0,1), one column per right-hand side (column-major (n, nrhs))
@@ -334,6 +336,7 @@ def run_ours(args, rank, world, local_rank):
     fp64 = None
     if prec != "f64":
         M64 = hlr.upload(hm, precision="f64", uniform=uniform, max_nrhs=nrhs)
+        tune_handle(M64, nrhs, args)
         y64 = dev_vec(np.zeros((nrhs, n)))
         hlr.mul_vec(1.0, hlr.apply_normal, M64, x, y64)
         yy = dev_vec(np.zeros((nrhs, n)))
@@ -408,7 +411,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": f"inputs larger than L2 ({info['matrix_bytes'] / 1e9:.2f} GB matrix streamed per step)",
                    "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": alg, "flops": info["flops"],
                    "leaves": info["n_dense"] + info["n_lowrank"], "max_rank": info["max_rank"],
-                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2)},
+                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2), "tuning": tuned},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "roofline": roof,
         "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
@@ -481,6 +484,8 @@ def run_batch(args, rank, world, local_rank):
     pad = (max(h.n for h in hms) + 63) // 64 * 64
     A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
     Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
+    tuned64 = tune_handle(A64, nrhs, args)
+    tuned = tune_handle(Alow, nrhs, args) if Alow is not A64 else tuned64
     N = count * pad
     rng = np.random.default_rng(9)
     b = np.zeros((nrhs, N))
@@ -564,7 +569,8 @@ def run_batch(args, rank, world, local_rank):
                                f"{inner}, CG + FP64 refinement to 1e-10",
                    "members": count, "n_total": sum(h.n for h in hms), "pad": pad, "nrhs": nrhs,
                    "matrix_bytes_inner": Alow.info["matrix_bytes"], "matrix_bytes_f64": A64.info["matrix_bytes"],
-                   "build_s": round(t_build, 1), "l2": "inputs larger than L2"},
+                   "build_s": round(t_build, 1), "l2": "inputs larger than L2",
+                   "tuning": tuned, "tuning_f64": tuned64},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "rel_err_vs_fp64": rel_err,
         "fp64_gpu": {"value": v64, "ms_per_step": ms64 / args.steps, "speedup": value / world / v64,
@@ -581,6 +587,19 @@ def run_batch(args, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def tune_handle(M, nrhs: int, args):
+    """Launch shapes from the autotuner, before any timed region: warps per
+    CTA for one vector, then (nrhs > 1) the 8-vector kernels against a loop
+    of one-vector products.  No cache file: each run times its own device."""
+    if args.no_autotune:
+        return None
+    from hlr_b200.tune import autotune
+    autotune(M, nrhs=1, cache=None)
+    if nrhs > 1:
+        autotune(M, nrhs=nrhs, cache=None)
+    return M.tuning
 
 
 def traffic_from_profiles(kernel: str, config: str):
@@ -607,6 +626,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed"],
                     help="storage precision (default: the config's)")
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")

@@ -216,6 +216,25 @@ class DeviceMatrix:
         k = lib().hlrc_last_profile(self._h, names, cnt, ms, by, 64)
         return {names[i].decode(): (cnt[i], ms[i], by[i]) for i in range(k)}
 
+    @property
+    def tuning(self) -> dict:
+        """Launch shapes of this handle's products (hlrc_get_tuning):
+        nform_warps, ttform_warps (4 or 8) and mr_min_nrhs."""
+        t = _capi.hlrc_tuning()
+        check(lib().hlrc_get_tuning(self._h, C.byref(t)), "hlrc_get_tuning")
+        return {"nform_warps": t.nform_warps, "ttform_warps": t.ttform_warps, "mr_min_nrhs": t.mr_min_nrhs}
+
+    def set_tuning(self, **kw) -> None:
+        """Changes some launch shapes (hlrc_set_tuning); the others keep their
+        values.  Invalid values raise HLRCError (HLRC_ERR_ARG)."""
+        cur = self.tuning
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning keys {sorted(unknown)}")
+        cur.update(kw)
+        t = _capi.hlrc_tuning(int(cur["nform_warps"]), int(cur["ttform_warps"]), int(cur["mr_min_nrhs"]))
+        check(lib().hlrc_set_tuning(self._h, C.byref(t)), "hlrc_set_tuning")
+
     def launch_count(self) -> int:
         """Kernels launched by this handle so far (hlrc_launch_count)."""
         return int(lib().hlrc_launch_count(self._h))

@@ -62,6 +62,13 @@ class hlrc_info(C.Structure):
                 ("launches", i32 * 3), ("reserved", i32 * 2)]
 
 
+class hlrc_tuning(C.Structure):
+    _fields_ = [("nform_warps", i32), ("ttform_warps", i32), ("mr_min_nrhs", i32), ("reserved", i32 * 5)]
+
+
+HLRC_MR_NEVER = 1000000
+
+
 class hlrc_problem(C.Structure):
     _fields_ = [("kind", i32), ("leaf_size", i32), ("n", i64), ("refine", i32), ("uniform", i32),
                 ("seed", u64), ("eta", f64), ("eps", f64), ("ell", f64), ("nugget", f64),
@@ -84,6 +91,8 @@ PROTOTYPES = {
     "hlrc_mvm_host": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64]),
     "hlrc_mvm_noalloc": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hlrc_get_info": (C.c_int, [C.c_void_p, C.POINTER(hlrc_info)]),
+    "hlrc_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
+    "hlrc_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
     "hlrc_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "hlrc_last_profile": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_int), pdbl,
                                     C.POINTER(i64), C.c_int]),

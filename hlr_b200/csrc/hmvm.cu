@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -125,6 +126,10 @@ struct hlrc_hmat_s {
     size_t hx_elems = 0, hy_elems = 0;
     int* dev_err = nullptr;   // device error word (bounded waits that ran out)
     int64_t launches = 0;     // kernels launched by this handle
+    // launch shapes picked by the autotuner (hlrc_set_tuning)
+    int nform_warps = 8;      // warps per CTA, single-vector N-form
+    int ttform_warps = 8;     // warps per CTA, single-vector tile T-form
+    int mr_min_nrhs = 2;      // fewest vectors that take the 8-vector kernels
     // profiling
     bool profiling = false;
     std::vector<ProfileRec> prof;
@@ -632,8 +637,10 @@ void prof_end(hlrc_hmat M, cudaStream_t s) {
     ++M->nprof;
 }
 
-constexpr int NFORM_WARPS = 8;
-constexpr int TTFORM_WARPS = 8;
+// warps per CTA of the single-vector kernels: the handle picks one of these
+// (hlrc_tuning); each kernel is compiled for both
+template <int W> using Warps = std::integral_constant<int, W>;
+constexpr int DMMA_WARPS = 8;   // warps per CTA of the FP64 8-vector kernels
 
 // Diagnostics: with HLRC_DEBUG_SYNC=1 in the environment every pass is
 // followed by a stream synchronisation, and an asynchronous kernel error is
@@ -691,22 +698,28 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             double* vout = bind(ws, tp.out, x, y);
             const int add = tp.mode == OUT_ADD_ALPHA;
             if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-            constexpr int TW = TTFORM_WARPS;
-            if (f64plan && tp.nsegs[FMT_F64] > 0)
-                k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
-                    tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
-                    reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
-            // reduced precision: each tile's run of columns, streamed in full 4 KB
-            // iterations; FP32 and 16-bit runs in one grid
-            if (!f64plan) {
-                const int n32 = tp.nmseg[FMT_F32];
-                if (tp.nmseg[FMT_BF16] > 0)
-                    k_ttform_qs<TW, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
-                        tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part, alpha, add);
-                else if (n32 + tp.nmseg[FMT_F16] > 0)
-                    k_ttform_qs<TW, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
-                        tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part, alpha, add);
-            }
+            auto ttform = [&](auto wc) {
+                constexpr int TW = decltype(wc)::value;
+                if (f64plan && tp.nsegs[FMT_F64] > 0)
+                    k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
+                        tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
+                        reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
+                // reduced precision: each tile's run of columns, streamed in full
+                // 4 KB iterations; FP32 and 16-bit runs in one grid
+                if (!f64plan) {
+                    const int n32 = tp.nmseg[FMT_F32];
+                    if (tp.nmseg[FMT_BF16] > 0)
+                        k_ttform_qs<TW, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
+                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part, alpha,
+                            add);
+                    else if (n32 + tp.nmseg[FMT_F16] > 0)
+                        k_ttform_qs<TW, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
+                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part, alpha,
+                            add);
+                }
+            };
+            if (M->ttform_warps == 4) ttform(Warps<4>{});
+            else ttform(Warps<8>{});
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
@@ -725,20 +738,25 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             const double* vt = bind(ws, np.vt, x, y);
             double* vo = bind(ws, np.out, x, y);
             const int add = np.mode == OUT_ADD_ALPHA;
-            constexpr int NW = NFORM_WARPS;
-            // formats in fixed order: each launch adds its part of y
-            if (f64plan && np.nsegs[FMT_F64] > 0)
-                k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
-                    np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
-                    reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
-            // reduced precision: one CTA per tile takes the packs of both formats
-            const QNPack* qc = static_cast<const QNPack*>(np.chunks);
-            if (!f64plan && np.nseg2 > 0) {
-                if (np.f16 == FMT_BF16)
-                    k_nform_q<NW, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha, add);
-                else
-                    k_nform_q<NW, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha, add);
-            }
+            auto nform = [&](auto wc) {
+                constexpr int NW = decltype(wc)::value;
+                if (f64plan && np.nsegs[FMT_F64] > 0)
+                    k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
+                        np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
+                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
+                // reduced precision: one CTA per tile takes the packs of both formats
+                const QNPack* qc = static_cast<const QNPack*>(np.chunks);
+                if (!f64plan && np.nseg2 > 0) {
+                    if (np.f16 == FMT_BF16)
+                        k_nform_q<NW, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
+                                                                             add);
+                    else
+                        k_nform_q<NW, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
+                                                                            add);
+                }
+            };
+            if (M->nform_warps == 4) nform(Warps<4>{});
+            else nform(Warps<8>{});
             if (ws.profile) prof_end(M, s);
             HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
         }
@@ -751,8 +769,8 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
 // the multi-RHS workspace and no unit T-form stage (the uniform-H adjoint
 // coupling runs per vector).
-bool multi_rhs_ok(hlrc_hmat M, int op) {
-    if (!M->mr_arena) return false;
+bool multi_rhs_ok(hlrc_hmat M, int op, int nrhs) {
+    if (nrhs < 2 || nrhs < M->mr_min_nrhs || !M->mr_arena) return false;
     for (const Stage& st : M->stages[op])
         if (st.kind == 0) return false;
     return true;
@@ -791,7 +809,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 const int add = tp.mode == OUT_ADD_ALPHA;
                 const OutMap om = omap(tp.out);
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
-                constexpr int TW = TTFORM_WARPS;
+                constexpr int TW = DMMA_WARPS;
                 if (M->precision == HLRC_PREC_F64) {
                     if (tp.nsegs[FMT_F64] > 0)
                         k_ttform_dmma<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
@@ -836,7 +854,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                 if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
                 const int add = np.mode == OUT_ADD_ALPHA;
                 const OutMap om = omap(np.out);
-                constexpr int NW = NFORM_WARPS;
+                constexpr int NW = DMMA_WARPS;
                 const bool f64plan = M->precision == HLRC_PREC_F64;
                 if (f64plan && np.nsegs[FMT_F64] > 0)
                     k_nform_dmma<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
@@ -974,7 +992,7 @@ extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double*
     DeviceGuard g(M->device);
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (nrhs > 1 && multi_rhs_ok(M, op)) return run_multi(M, alpha, op, x, ldx, y, ldy, nrhs, s);
+    if (multi_rhs_ok(M, op, nrhs)) return run_multi(M, alpha, op, x, ldx, y, ldy, nrhs, s);
     const Workspace ws = handle_workspace(M);
     for (int r = 0; r < nrhs; ++r) {
         st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
@@ -1009,7 +1027,7 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     const int64_t lx = nrhs > 1 ? ldx : nx, ly = nrhs > 1 ? ldy : ny;
     HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
-    if (nrhs > 1 && multi_rhs_ok(M, op)) {
+    if (multi_rhs_ok(M, op, nrhs)) {
         st = run_multi(M, alpha, op, M->hx, nx, M->hy, ny, nrhs, nullptr);
         if (st != HLRC_OK) return st;
     } else {
@@ -1026,6 +1044,30 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
 extern "C" hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info) {
     if (!M || !info) return fail(HLRC_ERR_ARG, "hlrc_get_info: null argument");
     *info = M->info;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t) {
+    if (!M || !t) return fail(HLRC_ERR_ARG, "hlrc_get_tuning: null argument");
+    std::memset(t, 0, sizeof(*t));
+    t->nform_warps = M->nform_warps;
+    t->ttform_warps = M->ttform_warps;
+    t->mr_min_nrhs = M->mr_min_nrhs;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t) {
+    if (!M || !t) return fail(HLRC_ERR_ARG, "hlrc_set_tuning: null argument");
+    auto warps_ok = [](int w) { return w == 4 || w == 8; };
+    if (!warps_ok(t->nform_warps) || !warps_ok(t->ttform_warps))
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: warps per CTA must be 4 or 8 (got %d, %d)", t->nform_warps,
+                    t->ttform_warps);
+    if (t->mr_min_nrhs < 2 || t->mr_min_nrhs > HLRC_MR_NEVER)
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: mr_min_nrhs must be in [2, %d] (got %d)", HLRC_MR_NEVER,
+                    t->mr_min_nrhs);
+    M->nform_warps = t->nform_warps;
+    M->ttform_warps = t->ttform_warps;
+    M->mr_min_nrhs = t->mr_min_nrhs;
     return HLRC_OK;
 }
 

@@ -1,0 +1,149 @@
+"""Autotuner for the launch shapes of a device matrix's products.
+
+For one matrix, right-hand-side count and operation, ``autotune`` times the
+candidate settings of ``hlrc_tuning`` on the current device and keeps the
+fastest:
+
+* one vector: warps per CTA (4 or 8) of the N-form and of the tile T-form
+  kernels, four combinations;
+* several vectors: the 8-vector tensor-core kernels against a loop of
+  one-vector products (``mr_min_nrhs`` 2 or ``HLRC_MR_NEVER``).
+
+Each candidate runs ``warmup`` untimed products and then ``reps`` products
+timed with CUDA events on the launching stream, on private random vectors
+(the caller's vectors are not touched).  The default setting is kept unless
+another one is faster by more than ``keep_default_within`` (2 %), so timing
+noise does not flip the choice.  Winners are cached in a JSON file keyed by
+the device name and the matrix's signature (kind, precision, shape, stored
+bytes, leaf counts, vector count, operation); a later call for the same
+signature takes the cached setting without timing anything.
+
+The reference has no counterpart: its TBB products have no launch shapes.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Callable, Optional
+
+from ._capi import HLRC_MR_NEVER
+
+DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2}
+
+
+def default_cache_path() -> Path:
+    """``$HLRC_TUNING_CACHE``, else ``~/.cache/hlr_b200/tuning.json``."""
+    env = os.environ.get("HLRC_TUNING_CACHE")
+    return Path(env) if env else Path.home() / ".cache" / "hlr_b200" / "tuning.json"
+
+
+def signature(M, nrhs: int, op: int, device_name: str) -> str:
+    i = M.info
+    return "|".join(str(v) for v in (device_name, "uniform" if M.uniform else "h", i["precision"], i["n_rows"],
+                                      i["n_cols"], i["matrix_bytes"], i["n_dense"], i["n_lowrank"], nrhs, op))
+
+
+def candidates(current: dict, nrhs: int) -> list:
+    """Settings to time; the first is the default for this vector count."""
+    if nrhs <= 1:
+        return [dict(current, nform_warps=a, ttform_warps=b) for a in (8, 4) for b in (8, 4)]
+    return [dict(current, mr_min_nrhs=2), dict(current, mr_min_nrhs=HLRC_MR_NEVER)]
+
+
+def _load(path: Path) -> dict:
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d if isinstance(d, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path: Path, key: str, entry: dict) -> None:
+    d = _load(path)
+    d[key] = entry
+    path.parent.mkdir(parents=True, exist_ok=True)
+    tmp = path.with_name(path.name + f".tmp{os.getpid()}")
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2) -> Callable[[], float]:
+    """Returns a function timing one product of M (ms, mean of ``reps``) with
+    the handle's current setting, on private random device vectors."""
+    import torch
+
+    from . import apply_normal, mul_vec
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    nx = M.ncols if op == apply_normal else M.nrows
+    ny = M.nrows if op == apply_normal else M.ncols
+    g = torch.Generator(device=dev).manual_seed(12345)
+    if nrhs == 1:
+        x = torch.randn(nx, dtype=torch.float64, device=dev, generator=g)
+        y = torch.zeros(ny, dtype=torch.float64, device=dev)
+    else:  # column-major (n, nrhs) views
+        x = torch.randn((nrhs, nx), dtype=torch.float64, device=dev, generator=g).T
+        y = torch.zeros((nrhs, ny), dtype=torch.float64, device=dev).T
+    stream = torch.cuda.current_stream(dev)
+
+    def run() -> float:
+        for _ in range(warmup):
+            mul_vec(1.0, op, M, x, y)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            mul_vec(1.0, op, M, x, y)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    return run
+
+
+def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "default", reps: int = 5,
+             warmup: int = 2, keep_default_within: float = 0.02, timer: Optional[Callable[[], float]] = None,
+             device_name: Optional[str] = None) -> dict:
+    """Picks and sets the fastest launch shapes of M for ``nrhs`` vectors and
+    operation ``op``.  ``cache`` is a JSON path, "default" for
+    ``default_cache_path()``, or None for no cache.  ``timer`` (tests) times
+    one product with the handle's current setting; by default CUDA events.
+
+    Returns {"tuning": chosen setting, "times_ms": [(setting, ms), ...],
+    "cached": whether the setting came from the cache, "key": cache key}."""
+    if device_name is None:
+        import torch
+        device_name = torch.cuda.get_device_name(torch.cuda.current_device())
+    path = default_cache_path() if cache == "default" else (Path(cache) if cache is not None else None)
+    key = signature(M, nrhs, op, device_name)
+    if path is not None:
+        hit = _load(path).get(key)
+        if isinstance(hit, dict) and isinstance(hit.get("tuning"), dict):
+            try:
+                M.set_tuning(**hit["tuning"])
+                return {"tuning": M.tuning, "times_ms": hit.get("times_ms", []), "cached": True, "key": key}
+            except Exception:
+                pass  # stale or foreign entry: tune afresh
+    if timer is None:
+        timer = event_timer(M, nrhs, op, reps=reps, warmup=warmup)
+    start = M.tuning
+    cands = candidates(start, nrhs)
+    times = []
+    try:
+        for c in cands:
+            M.set_tuning(**c)
+            times.append((dict(c), float(timer())))
+    except BaseException:
+        M.set_tuning(**start)
+        raise
+    best_c, best_t = min(times, key=lambda ct: ct[1])
+    first_c, first_t = times[0]
+    if first_t <= best_t * (1.0 + keep_default_within):
+        best_c = first_c
+    M.set_tuning(**best_c)
+    out = {"tuning": M.tuning, "times_ms": times, "cached": False, "key": key}
+    if path is not None:
+        _store(path, key, {"tuning": out["tuning"], "times_ms": times})
+    return out

@@ -256,6 +256,29 @@ hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op,
 
 hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info);
 
+/* Launch shapes of a handle's products, chosen per matrix and device by the
+ * autotuner (hlr_b200.tune.autotune times the candidates and caches the
+ * winner).  No counterpart in the reference, whose TBB products have no
+ * launch shapes; every setting computes the same product (the order of the
+ * per-warp partial sums differs, so results agree to rounding).
+ *   nform_warps, ttform_warps: warps per CTA (4 or 8) of the one-vector
+ *     N-form and tile T-form kernels;
+ *   mr_min_nrhs: products with at least this many vectors use the
+ *     8-vector tensor-core kernels, smaller ones loop the one-vector kernels
+ *     (2..HLRC_MR_NEVER; HLRC_MR_NEVER always loops).
+ * Defaults: 8, 8, 2.  hlrc_set_tuning rejects other values (HLRC_ERR_ARG)
+ * and must not race with products of the same handle.                     */
+#define HLRC_MR_NEVER 1000000
+typedef struct hlrc_tuning {
+    int32_t nform_warps;
+    int32_t ttform_warps;
+    int32_t mr_min_nrhs;
+    int32_t reserved[5];
+} hlrc_tuning;
+
+hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t);
+hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t);
+
 /* Device timing of the passes of the products (for roofline reporting).
  * While profiling is enabled every pass of every hlrc_mvm call is bracketed
  * by CUDA events on the call's stream.  hlrc_last_profile synchronises on

@@ -1,0 +1,118 @@
+"""Autotuner host logic (no GPU): candidate sets, choice of the fastest
+setting with the default kept inside the noise band, the JSON cache and its
+reuse, and rejection of unknown settings.  A fake handle stands in for an
+uploaded matrix and a fake timer for the CUDA-event timing."""
+import json
+
+import pytest
+
+from hlr_b200 import tune
+from hlr_b200._capi import HLRC_MR_NEVER
+
+
+class FakeMatrix:
+    uniform = False
+    info = {"precision": 0, "n_rows": 4096, "n_cols": 4096, "matrix_bytes": 123456, "n_dense": 10,
+            "n_lowrank": 20}
+
+    def __init__(self):
+        self._t = dict(tune.DEFAULT)
+        self.sets = 0
+
+    @property
+    def tuning(self):
+        return dict(self._t)
+
+    def set_tuning(self, **kw):
+        if set(kw) - set(self._t):
+            raise ValueError("unknown key")
+        if kw.get("nform_warps", 8) not in (4, 8) or kw.get("ttform_warps", 8) not in (4, 8):
+            raise ValueError("bad warps")
+        self._t.update(kw)
+        self.sets += 1
+
+
+def timer_for(M, table):
+    """Time of the handle's current setting, looked up in `table`."""
+    calls = []
+
+    def t():
+        s = M.tuning
+        calls.append(s)
+        return table(s)
+    return t, calls
+
+
+def test_candidates():
+    one = tune.candidates(dict(tune.DEFAULT), 1)
+    assert one[0] == tune.DEFAULT and len(one) == 4
+    assert {(c["nform_warps"], c["ttform_warps"]) for c in one} == {(8, 8), (8, 4), (4, 8), (4, 4)}
+    many = tune.candidates(dict(tune.DEFAULT), 8)
+    assert [c["mr_min_nrhs"] for c in many] == [2, HLRC_MR_NEVER]
+
+
+def test_picks_fastest_and_caches(tmp_path):
+    M = FakeMatrix()
+    t, calls = timer_for(M, lambda s: 1.0 if s["nform_warps"] == 4 and s["ttform_warps"] == 8 else 2.0)
+    path = tmp_path / "tuning.json"
+    r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
+    assert not r["cached"] and len(calls) == 4
+    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2}
+    d = json.loads(path.read_text())
+    assert d[r["key"]]["tuning"] == M.tuning
+    # a fresh handle of the same signature takes the cached setting untimed
+    M2 = FakeMatrix()
+    t2, calls2 = timer_for(M2, lambda s: 1.0)
+    r2 = tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="GPU-X")
+    assert r2["cached"] and calls2 == [] and M2.tuning == M.tuning
+    # another device or vector count is another key
+    M3 = FakeMatrix()
+    t3, calls3 = timer_for(M3, lambda s: 1.0)
+    assert not tune.autotune(M3, nrhs=1, cache=path, timer=t3, device_name="GPU-Y")["cached"]
+    assert not tune.autotune(M3, nrhs=8, cache=path, timer=t3, device_name="GPU-X")["cached"]
+    assert len(json.loads(path.read_text())) == 3
+
+
+def test_default_kept_within_noise():
+    M = FakeMatrix()
+    t, _ = timer_for(M, lambda s: 1.00 if s == tune.DEFAULT else 0.99)
+    assert tune.autotune(M, nrhs=1, cache=None, timer=t, device_name="G")["tuning"] == tune.DEFAULT
+    M = FakeMatrix()
+    t, _ = timer_for(M, lambda s: 1.00 if s == tune.DEFAULT else 0.90)
+    assert tune.autotune(M, nrhs=1, cache=None, timer=t, device_name="G")["tuning"] != tune.DEFAULT
+
+
+def test_multi_vector_choice():
+    M = FakeMatrix()
+    t, calls = timer_for(M, lambda s: 5.0 if s["mr_min_nrhs"] == 2 else 9.0)
+    r = tune.autotune(M, nrhs=8, cache=None, timer=t, device_name="G")
+    assert r["tuning"]["mr_min_nrhs"] == 2 and len(calls) == 2
+    M = FakeMatrix()
+    t, _ = timer_for(M, lambda s: 9.0 if s["mr_min_nrhs"] == 2 else 5.0)
+    assert tune.autotune(M, nrhs=3, cache=None, timer=t, device_name="G")["tuning"]["mr_min_nrhs"] == HLRC_MR_NEVER
+
+
+def test_bad_cache_entries_are_retuned(tmp_path):
+    path = tmp_path / "tuning.json"
+    path.write_text("not json")
+    M = FakeMatrix()
+    t, calls = timer_for(M, lambda s: 1.0)
+    r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="G")
+    assert not r["cached"] and len(calls) == 4
+    d = json.loads(path.read_text())
+    d[r["key"]]["tuning"] = {"nform_warps": 5, "ttform_warps": 8, "mr_min_nrhs": 2}   # rejected by the handle
+    path.write_text(json.dumps(d))
+    M2 = FakeMatrix()
+    t2, calls2 = timer_for(M2, lambda s: 1.0)
+    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 4
+
+
+def test_timer_failure_restores_setting():
+    M = FakeMatrix()
+    M.set_tuning(nform_warps=4)
+
+    def boom():
+        raise RuntimeError("timing failed")
+    with pytest.raises(RuntimeError):
+        tune.autotune(M, nrhs=1, cache=None, timer=boom, device_name="G")
+    assert M.tuning["nform_warps"] == 4
