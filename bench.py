@@ -389,20 +389,9 @@ def run_ours(args, rank, world, local_rank):
     alg = info["algorithmic_bytes"]
     passes = (nrhs + 7) // 8 if nrhs > 1 else 1      # the matrix is streamed once per block of 8 vectors
     gbs = alg * passes / (ms_max / 1e3 / args.steps) / 1e9
-    # dominant kernel = pass with the largest device time
-    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
-    roof = None
-    if dom:
-        name, (cnt, tot_ms, by) = dom
-        avg_ms = tot_ms / max(1, cnt)
-        achieved = by / (avg_ms / 1e3) / 1e9
-        # the summaries key a workload as config[/precision][/nrhs]
-        wl = args.config + ("" if prec == "f64" else "/" + prec) + ("" if nrhs == 1 else f"/{nrhs}")
-        traffic = traffic_from_profiles(name, wl)
-        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                "bytes_per_launch": by, "avg_ms": avg_ms,
-                "share_of_step": tot_ms / sum(v[1] for v in prof.values())}
+    # the summaries key a workload as config[/precision][/nrhs]
+    wl = args.config + ("" if prec == "f64" else "/" + prec) + ("" if nrhs == 1 else f"/{nrhs}")
+    roof = roofline_from_profile(prof, hbm_peak, peak_kind, wl)
     line = {
         "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -514,8 +503,12 @@ def run_batch(args, rank, world, local_rank):
         return max_over_ranks(e0.elapsed_time(e1), world, dev), M.launch_count() - l0
 
     y = torch.zeros_like(bt)
+    Alow.set_profiling(True)
+    Alow.last_profile()  # clear
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         ms, launches = timed(Alow, bt.T, y.T, args.steps)
+    prof = Alow.last_profile()
+    Alow.set_profiling(False)
     y64 = torch.zeros_like(bt)
     ms64, _ = timed(A64, bt.T, y64.T, args.steps)
     y1 = torch.zeros(N, dtype=torch.float64, device=dev)
@@ -572,6 +565,8 @@ def run_batch(args, rank, world, local_rank):
                    "build_s": round(t_build, 1), "l2": "inputs larger than L2",
                    "tuning": tuned, "tuning_f64": tuned64},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
+        "roofline": roofline_from_profile(prof, hbm_peak, peak_kind,
+                                          "c5" + ("" if inner == "f64" else "/" + inner) + f"/{nrhs}"),
         "rel_err_vs_fp64": rel_err,
         "fp64_gpu": {"value": v64, "ms_per_step": ms64 / args.steps, "speedup": value / world / v64,
                      "note": "same batch, same right-hand sides, FP64 store"},
@@ -587,6 +582,20 @@ def run_batch(args, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def roofline_from_profile(prof: dict, hbm_peak: float, peak_kind: str, workload: str):
+    """Roofline object of the dominant pass (largest device time) of a
+    per-pass CUDA-event profile {name: (launches, total ms, bytes/launch)}:
+    achieved = algorithmic bytes per launch / average launch time."""
+    if not prof:
+        return None
+    name, (cnt, tot_ms, by) = max(prof.items(), key=lambda kv: kv[1][1])
+    avg_ms = tot_ms / max(1, cnt)
+    achieved = by / (avg_ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "traffic": traffic_from_profiles(name, workload), "peak_kind": peak_kind,
+            "bytes_per_launch": by, "avg_ms": avg_ms, "share_of_step": tot_ms / sum(v[1] for v in prof.values())}
 
 
 def tune_handle(M, nrhs: int, args):

@@ -9,11 +9,12 @@ fastest:
 * several vectors: the 8-vector tensor-core kernels against a loop of
   one-vector products (``mr_min_nrhs`` 2 or ``HLRC_MR_NEVER``).
 
-Each candidate runs ``warmup`` untimed products and then ``reps`` products
-timed with CUDA events on the launching stream, on private random vectors
-(the caller's vectors are not touched).  The default setting is kept unless
-another one is faster by more than ``keep_default_within`` (2 %), so timing
-noise does not flip the choice.  Winners are cached in a JSON file keyed by
+Each candidate runs ``warmup`` untimed products and then at least ``reps``
+products (enough to last 20 ms) timed with CUDA events on the launching
+stream, on private random vectors (the caller's vectors are not touched).
+The candidates are swept twice, interleaved, and each keeps its best time.
+The default setting is kept unless another one is faster by more than
+``keep_default_within`` (2 %), so timing noise does not flip the choice.  Winners are cached in a JSON file keyed by
 the device name and the matrix's signature (kind, precision, shape, stored
 bytes, leaf counts, vector count, operation); a later call for the same
 signature takes the cached setting without timing anything.
@@ -70,9 +71,10 @@ def _store(path: Path, key: str, entry: dict) -> None:
     os.replace(tmp, path)
 
 
-def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2) -> Callable[[], float]:
-    """Returns a function timing one product of M (ms, mean of ``reps``) with
-    the handle's current setting, on private random device vectors."""
+def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2, min_ms: float = 20.0) -> Callable[[], float]:
+    """Returns a function timing one product of M (ms per product) with the
+    handle's current setting, on private random device vectors.  A timed run
+    covers ``reps`` products, or more if needed to last ``min_ms``."""
     import torch
 
     from . import apply_normal, mul_vec
@@ -89,23 +91,29 @@ def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2) -> Callab
         y = torch.zeros((nrhs, ny), dtype=torch.float64, device=dev).T
     stream = torch.cuda.current_stream(dev)
 
-    def run() -> float:
-        for _ in range(warmup):
-            mul_vec(1.0, op, M, x, y)
+    def timed(n: int) -> float:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(reps):
+        for _ in range(n):
             mul_vec(1.0, op, M, x, y)
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / reps
+        return e0.elapsed_time(e1) / n
+
+    def run() -> float:
+        for _ in range(warmup):
+            mul_vec(1.0, op, M, x, y)
+        t = timed(reps)
+        if t * reps < min_ms:
+            t = timed(min(10000, int(min_ms / max(t, 1e-3)) + 1))
+        return t
 
     return run
 
 
 def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "default", reps: int = 5,
              warmup: int = 2, keep_default_within: float = 0.02, timer: Optional[Callable[[], float]] = None,
-             device_name: Optional[str] = None) -> dict:
+             device_name: Optional[str] = None, sweeps: int = 2) -> dict:
     """Picks and sets the fastest launch shapes of M for ``nrhs`` vectors and
     operation ``op``.  ``cache`` is a JSON path, "default" for
     ``default_cache_path()``, or None for no cache.  ``timer`` (tests) times
@@ -130,14 +138,16 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
         timer = event_timer(M, nrhs, op, reps=reps, warmup=warmup)
     start = M.tuning
     cands = candidates(start, nrhs)
-    times = []
+    best = [float("inf")] * len(cands)
     try:
-        for c in cands:
-            M.set_tuning(**c)
-            times.append((dict(c), float(timer())))
+        for _ in range(sweeps):   # interleaved sweeps; a candidate keeps its best time
+            for i, c in enumerate(cands):
+                M.set_tuning(**c)
+                best[i] = min(best[i], float(timer()))
     except BaseException:
         M.set_tuning(**start)
         raise
+    times = [(dict(c), t) for c, t in zip(cands, best)]
     best_c, best_t = min(times, key=lambda ct: ct[1])
     first_c, first_t = times[0]
     if first_t <= best_t * (1.0 + keep_default_within):

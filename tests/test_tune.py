@@ -56,7 +56,7 @@ def test_picks_fastest_and_caches(tmp_path):
     t, calls = timer_for(M, lambda s: 1.0 if s["nform_warps"] == 4 and s["ttform_warps"] == 8 else 2.0)
     path = tmp_path / "tuning.json"
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
-    assert not r["cached"] and len(calls) == 4
+    assert not r["cached"] and len(calls) == 8      # two sweeps of four
     assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2}
     d = json.loads(path.read_text())
     assert d[r["key"]]["tuning"] == M.tuning
@@ -86,7 +86,7 @@ def test_multi_vector_choice():
     M = FakeMatrix()
     t, calls = timer_for(M, lambda s: 5.0 if s["mr_min_nrhs"] == 2 else 9.0)
     r = tune.autotune(M, nrhs=8, cache=None, timer=t, device_name="G")
-    assert r["tuning"]["mr_min_nrhs"] == 2 and len(calls) == 2
+    assert r["tuning"]["mr_min_nrhs"] == 2 and len(calls) == 4
     M = FakeMatrix()
     t, _ = timer_for(M, lambda s: 9.0 if s["mr_min_nrhs"] == 2 else 5.0)
     assert tune.autotune(M, nrhs=3, cache=None, timer=t, device_name="G")["tuning"]["mr_min_nrhs"] == HLRC_MR_NEVER
@@ -98,13 +98,13 @@ def test_bad_cache_entries_are_retuned(tmp_path):
     M = FakeMatrix()
     t, calls = timer_for(M, lambda s: 1.0)
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="G")
-    assert not r["cached"] and len(calls) == 4
+    assert not r["cached"] and len(calls) == 8      # two sweeps of four
     d = json.loads(path.read_text())
     d[r["key"]]["tuning"] = {"nform_warps": 5, "ttform_warps": 8, "mr_min_nrhs": 2}   # rejected by the handle
     path.write_text(json.dumps(d))
     M2 = FakeMatrix()
     t2, calls2 = timer_for(M2, lambda s: 1.0)
-    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 4
+    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 8
 
 
 def test_timer_failure_restores_setting():
