@@ -8,7 +8,7 @@ host by the library's own construction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config c2|c1|c3|c2s|c4|c5] [--precision P] [--nrhs K]
-                    [--no-cpu-baseline] [--no-autotune]
+                    [--no-cpu-baseline] [--no-autotune] [--no-graph]
 
 Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
 independent replica of the product on its own GPU (the MVM has no exchange
@@ -302,8 +302,25 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    l0 = M.launch_count()
+    step()                      # one more warm-up product, counting its launches
+    torch.cuda.synchronize()
+    per_product = M.launch_count() - l0
     M.set_profiling(True)
     M.last_profile()  # clear
+    # the reference's protocol: runs of nmvm = 50 products; here each run is
+    # one CUDA graph of `per_graph` captured products, replayed steps/per_graph
+    # times (per-pass profiling events are graph nodes, read after the last
+    # replay)
+    graph, per_graph = None, 0
+    if not args.no_graph:
+        per_graph = max(d for d in range(1, min(50, args.steps) + 1) if args.steps % d == 0)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(per_graph):
+                step()
+        graph.replay()          # untimed
+        torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -311,16 +328,21 @@ def run_ours(args, rank, world, local_rank):
     launches0 = M.launch_count()
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         e0.record(stream)
-        for _ in range(args.steps):
-            step()
+        if graph is not None:
+            for _ in range(args.steps // per_graph):
+                graph.replay()
+        else:
+            for _ in range(args.steps):
+                step()
         e1.record(stream)
         torch.cuda.synchronize()
-    timed_launches = M.launch_count() - launches0
+    timed_launches = per_product * args.steps if graph is not None else M.launch_count() - launches0
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
     prof = M.last_profile()
     M.set_profiling(False)
+    del graph
     ms_max = max_over_ranks(ms, world, dev)
 
     # correctness of the timed path: one product from zero; column 0 is
@@ -400,7 +422,9 @@ def run_ours(args, rank, world, local_rank):
                    "l2": f"inputs larger than L2 ({info['matrix_bytes'] / 1e9:.2f} GB matrix streamed per step)",
                    "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": alg, "flops": info["flops"],
                    "leaves": info["n_dense"] + info["n_lowrank"], "max_rank": info["max_rank"],
-                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2), "tuning": tuned},
+                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2), "tuning": tuned,
+                   "graph": {"products_per_graph": per_graph, "replays": args.steps // per_graph}
+                   if per_graph else None},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "roofline": roof,
         "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
@@ -636,6 +660,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--no-graph", action="store_true", help="launch every product directly (no CUDA graph)")
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed"],
                     help="storage precision (default: the config's)")
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")

@@ -619,6 +619,19 @@ double* bind(const Workspace& ws, int name, const double* x, double* y) {
     }
 }
 
+// Profiling events on a stream that is being captured into a CUDA graph are
+// recorded as external event-record nodes, so that every replay of the graph
+// records them again (a plain record during capture only orders the graph).
+void prof_record(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();   // not an error of the product: clear it
+        st = cudaStreamCaptureStatusNone;
+    }
+    if (st == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
+
 void prof_begin(hlrc_hmat M, const char* name, int64_t alg_bytes, cudaStream_t s) {
     if (!M->profiling) return;
     if (M->nprof >= int(M->prof.size())) {
@@ -629,11 +642,11 @@ void prof_begin(hlrc_hmat M, const char* name, int64_t alg_bytes, cudaStream_t s
     }
     M->prof[size_t(M->nprof)].name = name;
     M->prof[size_t(M->nprof)].alg_bytes = alg_bytes;
-    cudaEventRecord(M->prof[size_t(M->nprof)].e0, s);
+    prof_record(M->prof[size_t(M->nprof)].e0, s);
 }
 void prof_end(hlrc_hmat M, cudaStream_t s) {
     if (!M->profiling) return;
-    cudaEventRecord(M->prof[size_t(M->nprof)].e1, s);
+    prof_record(M->prof[size_t(M->nprof)].e1, s);
     ++M->nprof;
 }
 

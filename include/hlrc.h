@@ -285,7 +285,10 @@ hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t);
  * those events and returns, per pass *name* (static strings), the number of
  * launches, the summed milliseconds and the algorithmic bytes of one launch
  * (stored matrix bytes without padding, plus vector reads/writes), then
- * clears the records.  Returns the number of names written.                 */
+ * clears the records.  Returns the number of names written.  Products
+ * captured into a CUDA graph with profiling enabled record their events as
+ * external event-record nodes: after a replay, hlrc_last_profile returns
+ * that replay's pass times (read it before the next replay).                */
 hlrc_status hlrc_set_profiling(hlrc_hmat M, int enable);
 int         hlrc_last_profile(hlrc_hmat M, const char** names, int* count,
                               double* ms, int64_t* bytes, int cap);
