@@ -329,8 +329,11 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         e0.record(stream)
         if graph is not None:
+            marks = [e0]
             for _ in range(args.steps // per_graph):
                 graph.replay()
+                marks.append(torch.cuda.Event(enable_timing=True))
+                marks[-1].record(stream)
         else:
             for _ in range(args.steps):
                 step()
@@ -340,6 +343,12 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    # per-product time of each run (graph replay): min / median / max, as the
+    # reference reports its runs
+    runs = None
+    if graph is not None:
+        rt = [a.elapsed_time(b) / per_graph for a, b in zip(marks[:-1], marks[1:])]
+        runs = {"min": min(rt), "median": statistics.median(rt), "max": max(rt), "runs": len(rt)}
     prof = M.last_profile()
     M.set_profiling(False)
     del graph
@@ -423,8 +432,8 @@ def run_ours(args, rank, world, local_rank):
                    "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": alg, "flops": info["flops"],
                    "leaves": info["n_dense"] + info["n_lowrank"], "max_rank": info["max_rank"],
                    "build_s": round(t_build, 2), "upload_s": round(t_upload, 2), "tuning": tuned,
-                   "graph": {"products_per_graph": per_graph, "replays": args.steps // per_graph}
-                   if per_graph else None},
+                   "graph": {"products_per_graph": per_graph, "replays": args.steps // per_graph,
+                             "ms_per_product_of_runs": runs} if per_graph else None},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "roofline": roof,
         "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
