@@ -45,10 +45,10 @@ struct DevTPass {
 };
 
 struct DevNPass {
-    const NSeg* segs[4] = {};         // per StoreFmt
-    int nsegs[4] = {0, 0, 0, 0};
-    const MSeg* mseg[4] = {};         // multi-RHS column streams (reduced precision)
-    int nmseg[4] = {0, 0, 0, 0};
+    const NSeg* segs[NFMT] = {};         // per StoreFmt
+    int nsegs[NFMT] = {};
+    const MSeg* mseg[NFMT] = {};         // multi-RHS column streams (reduced precision)
+    int nmseg[NFMT] = {};
     const MCol* mcol = nullptr;
     const NSeg2* seg2 = nullptr;      // reduced precision: both formats of a tile in one CTA
     int nseg2 = 0;
@@ -59,16 +59,16 @@ struct DevNPass {
     int launches() const {
         if (nseg2 > 0) return 1;
         int n = 0;
-        for (int f = 0; f < 4; ++f) n += nsegs[f] > 0 ? 1 : 0;
+        for (int f = 0; f < NFMT; ++f) n += nsegs[f] > 0 ? 1 : 0;
         return n;
     }
 };
 
 struct DevTTPass {
-    const TTSeg* segs[4] = {};
-    int nsegs[4] = {0, 0, 0, 0};
-    const MSeg* mseg[4] = {};
-    int nmseg[4] = {0, 0, 0, 0};
+    const TTSeg* segs[NFMT] = {};
+    int nsegs[NFMT] = {};
+    const MSeg* mseg[NFMT] = {};
+    int nmseg[NFMT] = {};
     const MCol* mcol = nullptr;
     const void* chunks = nullptr;     // TTChunk (FP64 plan) or QTTChunk
     const TGroup* groups = nullptr;
@@ -81,9 +81,9 @@ struct DevTTPass {
     int launches() const {
         const int n = (ngroups > 0 ? 1 : 0) + (ngroups1 > 0 ? 1 : 0);
         // reduced-precision stores: one grid for the runs of all formats
-        if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] > 0) return n + 1;
+        if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] + nmseg[FMT_I16] > 0) return n + 1;
         int k = n;
-        for (int f = 0; f < 4; ++f) k += nsegs[f] > 0 ? 1 : 0;
+        for (int f = 0; f < NFMT; ++f) k += nsegs[f] > 0 ? 1 : 0;
         return k;
     }
 };
@@ -175,7 +175,7 @@ const char* stage_name(int kind, int nk, int idx) {
 struct ArenaLayout {
     size_t store = 0;
     std::vector<size_t> tu, ts, tg, nc, ttc, ttg, ttg1, n2;
-    std::vector<std::array<size_t, 4>> ns, tts;   // per pass, per StoreFmt
+    std::vector<std::array<size_t, NFMT>> ns, tts;   // per pass, per StoreFmt
     size_t t = 0, t2 = 0, part = 0, err = 0, total = 0;
     size_t part_elems = 0;
 };
@@ -195,19 +195,20 @@ ArenaLayout arena_layout(const Plan& p) {
         max_slots = std::max(max_slots, tp.nslots);
     }
     for (const NPass& np : p.npasses) {
-        std::array<size_t, 4> o{};
-        for (int f = 0; f < 4; ++f) o[size_t(f)] = take(np.segs[f].size() * sizeof(NSeg));
+        std::array<size_t, NFMT> o{};
+        for (int f = 0; f < NFMT; ++f) o[size_t(f)] = take(np.segs[f].size() * sizeof(NSeg));
         L.ns.push_back(o);
         L.nc.push_back(take(np.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(NChunk) : sizeof(QNPack))));
         L.n2.push_back(take(p.precision == HLRC_PREC_F64
                                 ? 0
-                                : (np.segs[FMT_F32].size() + np.segs[FMT_F16].size() + np.segs[FMT_BF16].size()) *
+                                : (np.segs[FMT_F32].size() + np.segs[FMT_F16].size() + np.segs[FMT_BF16].size() +
+                                   np.segs[FMT_I16].size()) *
                                       sizeof(NSeg2)));
     }
     size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
     for (const TTPass& tp : p.ttpasses) {
-        std::array<size_t, 4> o{};
-        for (int f = 0; f < 4; ++f) o[size_t(f)] = take(tp.segs[f].size() * sizeof(TTSeg));
+        std::array<size_t, NFMT> o{};
+        for (int f = 0; f < NFMT; ++f) o[size_t(f)] = take(tp.segs[f].size() * sizeof(TTSeg));
         L.tts.push_back(o);
         L.ttc.push_back(take(tp.chunks.size() * (p.precision == HLRC_PREC_F64 ? sizeof(TTChunk) : sizeof(QTTPack))));
         L.ttg.push_back(take(tp.groups.size() * sizeof(TGroup)));
@@ -298,14 +299,14 @@ std::vector<Seg> remap_segs(const std::vector<Seg>& segs, const std::vector<uint
 // segment, in store order, must form one contiguous run of columns; their
 // columns get one MCol entry each.
 struct StreamTables {
-    std::vector<MSeg> seg[4];
+    std::vector<MSeg> seg[NFMT];
     std::vector<MCol> col;
 };
 
 template <typename Seg, typename VoOf>
-hlrc_status build_streams(const std::vector<Seg> (&segs)[4], const std::vector<GChunk>& chunks, bool tt, VoOf vo_of,
+hlrc_status build_streams(const std::vector<Seg> (&segs)[NFMT], const std::vector<GChunk>& chunks, bool tt, VoOf vo_of,
                           StreamTables& out) {
-    for (int f = FMT_F32; f <= FMT_BF16; ++f) {
+    for (int f = FMT_F32; f < NFMT; ++f) {
         for (const Seg& s : segs[f]) {
             if (s.ce <= s.cb) continue;
             std::vector<uint32_t> idx(s.ce - s.cb);
@@ -346,20 +347,20 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
     std::vector<StreamTables> nt(p.npasses.size()), tt(p.ttpasses.size());
     size_t bytes = 0;
     auto take = [&](size_t b) { const size_t o = bytes; bytes = align_up(bytes + b, 256); return o; };
-    std::vector<std::array<size_t, 4>> n_seg_off(nt.size()), t_seg_off(tt.size());
+    std::vector<std::array<size_t, NFMT>> n_seg_off(nt.size()), t_seg_off(tt.size());
     std::vector<size_t> n_col_off(nt.size()), t_col_off(tt.size());
     for (size_t i = 0; i < nt.size(); ++i) {
         const hlrc_status st = build_streams(p.npasses[i].segs, p.npasses[i].chunks, false,
                                              [](const NSeg& s) { return s.out; }, nt[i]);
         if (st != HLRC_OK) return st;
-        for (int f = 0; f < 4; ++f) n_seg_off[i][size_t(f)] = take(nt[i].seg[f].size() * sizeof(MSeg));
+        for (int f = 0; f < NFMT; ++f) n_seg_off[i][size_t(f)] = take(nt[i].seg[f].size() * sizeof(MSeg));
         n_col_off[i] = take(nt[i].col.size() * sizeof(MCol));
     }
     for (size_t i = 0; i < tt.size(); ++i) {
         const hlrc_status st = build_streams(p.ttpasses[i].segs, p.ttpasses[i].chunks, true,
                                              [](const TTSeg& s) { return s.v_off; }, tt[i]);
         if (st != HLRC_OK) return st;
-        for (int f = 0; f < 4; ++f) t_seg_off[i][size_t(f)] = take(tt[i].seg[f].size() * sizeof(MSeg));
+        for (int f = 0; f < NFMT; ++f) t_seg_off[i][size_t(f)] = take(tt[i].seg[f].size() * sizeof(MSeg));
         t_col_off[i] = take(tt[i].col.size() * sizeof(MCol));
     }
     cudaError_t e = cudaMalloc(&h->mr_tables, std::max<size_t>(bytes, 256));
@@ -371,7 +372,7 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
         return b ? cudaMemcpy(h->mr_tables + off, src, b, cudaMemcpyHostToDevice) : cudaSuccess;
     };
     for (size_t i = 0; i < nt.size() && e == cudaSuccess; ++i) {
-        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+        for (int f = 0; f < NFMT && e == cudaSuccess; ++f) {
             e = put(n_seg_off[i][size_t(f)], nt[i].seg[f].data(), nt[i].seg[f].size() * sizeof(MSeg));
             h->n[i].mseg[f] = reinterpret_cast<const MSeg*>(h->mr_tables + n_seg_off[i][size_t(f)]);
             h->n[i].nmseg[f] = int(nt[i].seg[f].size());
@@ -380,7 +381,7 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
         h->n[i].mcol = reinterpret_cast<const MCol*>(h->mr_tables + n_col_off[i]);
     }
     for (size_t i = 0; i < tt.size() && e == cudaSuccess; ++i) {
-        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+        for (int f = 0; f < NFMT && e == cudaSuccess; ++f) {
             e = put(t_seg_off[i][size_t(f)], tt[i].seg[f].data(), tt[i].seg[f].size() * sizeof(MSeg));
             h->tt[i].mseg[f] = reinterpret_cast<const MSeg*>(h->mr_tables + t_seg_off[i][size_t(f)]);
             h->tt[i].nmseg[f] = int(tt[i].seg[f].size());
@@ -437,7 +438,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     h->n_part = int64_t(L.part_elems);
     const size_t o_store = L.store, o_t = L.t, o_t2 = L.t2, o_part = L.part;
     const std::vector<size_t>&o_tu = L.tu, &o_ts = L.ts, &o_tg = L.tg, &o_nc = L.nc;
-    const std::vector<std::array<size_t, 4>>& o_ns = L.ns;
+    const std::vector<std::array<size_t, NFMT>>& o_ns = L.ns;
     h->arena_bytes = L.total;
     cudaError_t e = cudaMalloc(&h->arena, h->arena_bytes);
     if (e != cudaSuccess) {
@@ -471,7 +472,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         DevNPass d;
         std::vector<uint32_t> pack_of;
         const std::vector<uint8_t> enc = encode_chunks(np.chunks, f64, false, pack_of);
-        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+        for (int f = 0; f < NFMT && e == cudaSuccess; ++f) {
             const std::vector<NSeg> sg = remap_segs(np.segs[f], pack_of);
             e = put(o_ns[i][size_t(f)], sg.data(), sg.size() * sizeof(NSeg));
             d.segs[f] = reinterpret_cast<const NSeg*>(hp->arena + o_ns[i][size_t(f)]);
@@ -482,7 +483,12 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
         if (!f64 && e == cudaSuccess) {
             // pair the FP32 and 16-bit segments of every output tile
-            d.f16 = np.segs[FMT_BF16].empty() ? FMT_F16 : FMT_BF16;
+            // the store's one 16-bit format
+            d.f16 = !np.segs[FMT_BF16].empty() ? FMT_BF16 : (!np.segs[FMT_I16].empty() ? FMT_I16 : FMT_F16);
+            if (int(!np.segs[FMT_F16].empty()) + int(!np.segs[FMT_BF16].empty()) + int(!np.segs[FMT_I16].empty()) > 1) {
+                cleanup();
+                return fail(HLRC_ERR_INTERNAL, "N-pass with two 16-bit formats");
+            }
             const std::vector<NSeg> s32 = remap_segs(np.segs[FMT_F32], pack_of);
             const std::vector<NSeg> s16 = remap_segs(np.segs[d.f16], pack_of);
             std::vector<NSeg2> pairs;
@@ -516,7 +522,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         DevTTPass d;
         std::vector<uint32_t> pack_of;
         const std::vector<uint8_t> enc = encode_chunks(tp.chunks, f64, true, pack_of);
-        for (int f = 0; f < 4 && e == cudaSuccess; ++f) {
+        for (int f = 0; f < NFMT && e == cudaSuccess; ++f) {
             const std::vector<TTSeg> sg = remap_segs(tp.segs[f], pack_of);
             e = put(L.tts[i][size_t(f)], sg.data(), sg.size() * sizeof(TTSeg));
             d.segs[f] = reinterpret_cast<const TTSeg*>(hp->arena + L.tts[i][size_t(f)]);
@@ -542,10 +548,10 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     // FP64 plans carry FP64 descriptors only, reduced-precision plans packs
     // only; a mix would hand one kind of kernel the other's descriptors
     for (const DevNPass& d : hp->n)
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < NFMT; ++f)
             if (d.nsegs[f] > 0 && ((f == FMT_F64) != f64)) { cleanup(); return fail(HLRC_ERR_INTERNAL, "format mix in plan"); }
     for (const DevTTPass& d : hp->tt)
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < NFMT; ++f)
             if (d.nsegs[f] > 0 && ((f == FMT_F64) != f64)) { cleanup(); return fail(HLRC_ERR_INTERNAL, "format mix in plan"); }
     hp->store = reinterpret_cast<const uint8_t*>(hp->arena + o_store);
     hp->ws_t = reinterpret_cast<double*>(hp->arena + o_t);
@@ -555,7 +561,9 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
 
     fill_info(p, L, hp->info);
-    if (o.max_nrhs > 1) {
+    // the 8-vector kernels take FP64, FP32 and FP16/BF16 columns; 16-bit
+    // integer (BFP16) stores loop the one-vector kernels instead
+    if (o.max_nrhs > 1 && p.precision != HLRC_PREC_BFP16) {
         const size_t nx = size_t(std::max(p.nrows, p.ncols)) * MR_RB;
         const size_t nt = size_t(std::max<int64_t>(1, p.n_t)) * MR_RB, nt2 = size_t(std::max<int64_t>(1, p.n_t2)) * MR_RB;
         const size_t np = size_t(std::max<int64_t>(1, hp->n_part)) * MR_RB;
@@ -725,6 +733,10 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                         k_ttform_qs<TW, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part, alpha,
                             add);
+                    else if (tp.nmseg[FMT_I16] > 0)
+                        k_ttform_qs<TW, FMT_I16><<<n32 + tp.nmseg[FMT_I16], TW * 32, 0, s>>>(
+                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_I16], tp.mcol, M->store, vin, vout, ws.part, alpha,
+                            add);
                     else if (n32 + tp.nmseg[FMT_F16] > 0)
                         k_ttform_qs<TW, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part, alpha,
@@ -763,6 +775,9 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                     if (np.f16 == FMT_BF16)
                         k_nform_q<NW, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
                                                                              add);
+                    else if (np.f16 == FMT_I16)
+                        k_nform_q<NW, FMT_I16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
+                                                                            add);
                     else
                         k_nform_q<NW, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
                                                                             add);

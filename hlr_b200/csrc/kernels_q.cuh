@@ -26,6 +26,41 @@ template <int FMT> struct QFmt;
 template <> struct QFmt<FMT_F32> { static constexpr int R = 4, G = 16, C = 2, LOG_G = 4; };
 template <> struct QFmt<FMT_F16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
 template <> struct QFmt<FMT_BF16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
+template <> struct QFmt<FMT_I16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
+
+// Packed FP32 pairs (sm_100 fma / sub .f32x2: two FP32 operations per
+// instruction) for the 16-bit integer format.
+__device__ __forceinline__ uint64_t pk2(uint32_t lo, uint32_t hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};\n" : "=l"(r) : "r"(lo), "r"(hi));
+    return r;
+}
+__device__ __forceinline__ uint64_t pk2f(float lo, float hi) { return pk2(__float_as_uint(lo), __float_as_uint(hi)); }
+__device__ __forceinline__ float2 upk2(uint64_t v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;\n" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ void fma2(uint64_t& d, uint64_t a, uint64_t b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;\n" : "+l"(d) : "l"(a), "l"(b));
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;\n" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// 8 offset-binary 16-bit integers (16 loaded bytes) -> 4 exact packed float
+// pairs: a value u = v + 2^15 becomes the low mantissa bits of 1.5 * 2^23,
+// and one exact packed subtraction removes 1.5 * 2^23 + 2^15 (no integer
+// conversion instruction).  Pair i holds rows 2i, 2i+1.
+__device__ __forceinline__ void i16_pairs(const uint4& u, uint64_t (&p)[4]) {
+    constexpr uint64_t BIAS = 0x4B4080004B408000ull;   // 1.5 * 2^23 + 2^15, twice
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        p[i] = sub2(pk2(__byte_perm(w[i], 0x4B400000u, 0x7610), __byte_perm(w[i], 0x4B400000u, 0x7632)), BIAS);
+}
 
 // 16 loaded bytes -> R floats
 template <int FMT>
@@ -40,6 +75,15 @@ __device__ __forceinline__ void unpack16(const uint4& u, float* f) {
             __half2 h;
             memcpy(&h, &w[i], 4);
             const float2 t = __half22float2(h);
+            f[2 * i] = t.x;
+            f[2 * i + 1] = t.y;
+        }
+    } else if constexpr (FMT == FMT_I16) {
+        uint64_t p[4];
+        i16_pairs(u, p);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 t = upk2(p[i]);
             f[2 * i] = t.x;
             f[2 * i + 1] = t.y;
         }
@@ -104,6 +148,26 @@ __device__ __forceinline__ void npack_q(const QNPack& pk, const uint8_t* A, cons
     const float vl = lane < ntot ? float(__ldg(v + (second ? lane - n0 : lane)) * double(sc)) : 0.f;
     uint4 m[8];
     load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m);
+    if constexpr (FMT == FMT_I16) {
+        // row pairs: one packed FMA per two rows
+        uint64_t s2[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float vj = __shfl_sync(0xffffffffu, vl, (g + F::C * i) & 31);
+            const uint64_t vv = pk2f(vj, vj);
+            uint64_t pr[4];
+            i16_pairs(m[i], pr);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) fma2(s2[k], pr[k], vv);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 t = upk2(s2[k]);
+            acc[2 * k] += double(t.x);
+            acc[2 * k + 1] += double(t.y);
+        }
+        return;
+    }
     float s[F::R];
 #pragma unroll
     for (int r = 0; r < F::R; ++r) s[r] = 0.f;
@@ -199,6 +263,23 @@ k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, cons
 template <int FMT>
 __device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float* p) {
     using F = QFmt<FMT>;
+    if constexpr (FMT == FMT_I16) {
+        // packed: rows 2k, 2k+1 in one FMA, the two halves added at the end
+        uint64_t x2[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) x2[k] = pk2f(xr[2 * k], xr[2 * k + 1]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            uint64_t pr[4];
+            i16_pairs(m[i], pr);
+            uint64_t a = 0ull;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) fma2(a, pr[k], x2[k]);
+            const float2 t = upk2(a);
+            p[i] = t.x + t.y;
+        }
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         float f[F::R];
@@ -286,7 +367,7 @@ __device__ __forceinline__ void ttform_qs(const MSeg& sg, const MCol* __restrict
 // The outputs of the two formats are disjoint, so their CTAs may run side
 // by side, and the pass has a single tail.
 template <int W, int F16>
-__global__ void __launch_bounds__(W * 32)
+__global__ void __launch_bounds__(W * 32, 24 / W)
 k_ttform_qs(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
             const uint8_t* __restrict__ A, const double* __restrict__ vin, double* __restrict__ out,
             double* __restrict__ part, double alpha, int add) {

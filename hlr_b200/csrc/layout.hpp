@@ -110,7 +110,9 @@ enum StoreFmt : uint8_t {
     FMT_F32 = 1,
     FMT_F16 = 2,     // IEEE binary16, scaled
     FMT_BF16 = 3,    // bfloat16, scaled
+    FMT_I16 = 4,     // 16-bit integer (block floating point), scaled; stored offset-binary (v + 2^15)
 };
+constexpr int NFMT = 5;   // number of storage formats
 
 inline constexpr int fmt_bytes(int f) { return f == FMT_F64 ? 8 : (f == FMT_F32 ? 4 : 2); }
 

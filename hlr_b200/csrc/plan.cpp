@@ -120,7 +120,7 @@ struct SSlab {
 // contiguous run of columns in every store this planner produces: FP64 D,U;
 // FP32 D,U; mixed D(FP32),U(FP32),U(FP16); FP16 / BF16 U,D.
 inline int layout_rank(int group, int fmt) {
-    static const int rank[4][2] = {{0, 1}, {2, 3}, {5, 4}, {7, 6}};   // [fmt][group]: D = 0, factor = 1
+    static const int rank[NFMT][2] = {{0, 1}, {2, 3}, {5, 4}, {7, 6}, {9, 8}};   // [fmt][group]: D = 0, factor = 1
     return rank[fmt][group];
 }
 
@@ -131,7 +131,7 @@ struct Store {
     std::vector<int32_t> crows;        // per chunk: rows of its slab
     size_t region_begin = 0;           // first chunk without a byte offset
     int64_t bytes = 0;
-    int64_t unpadded[4] = {0, 0, 0, 0};
+    int64_t unpadded[NFMT] = {};
 
     // rows [r0, r0+rows) x ncols of a column-major matrix; colfmt (per
     // column, may be null -> deffmt); chunks do not straddle `cuts`.  Byte
@@ -165,7 +165,7 @@ struct Store {
     // Places the chunks allocated since the last call: by layout_rank, then
     // in allocation order, each on a 16-byte boundary.
     void close_region() {
-        for (int r = 0; r < 8; ++r)
+        for (int r = 0; r < 2 * NFMT; ++r)
             for (size_t c = region_begin; c < chunks.size(); ++c) {
                 SChunk& ch = chunks[c];
                 if (layout_rank(group[c], ch.fmt) != r) continue;
@@ -206,6 +206,13 @@ struct Store {
                     for (int j = 0; j < ch.nc; ++j) {
                         uint16_t* d = reinterpret_cast<uint16_t*>(dst) + j * ldc;
                         for (int64_t i = 0; i < s.rows; ++i) {
+                            if (ch.fmt == FMT_I16) {
+                                // round to nearest, |value| < 2^15 after scaling;
+                                // stored offset-binary (value + 2^15)
+                                const double q = std::nearbyint(src[i + j * s.lds] * inv);
+                                d[i] = uint16_t(int(std::max(-32767.0, std::min(32767.0, q))) + 32768);
+                                continue;
+                            }
                             const float v = float(src[i + j * s.lds] * inv);
                             d[i] = ch.fmt == FMT_F16 ? to_f16(v) : to_bf16(v);
                         }
@@ -307,7 +314,7 @@ struct NBuilder {
     NPass& P;
     const Store& S;
     NBuilder(NPass& p, const Store& s) : P(p), S(s) {}
-    std::vector<std::pair<int64_t, NSeg>> tmp[4];
+    std::vector<std::pair<int64_t, NSeg>> tmp[NFMT];
     uint32_t cb = 0;
     int64_t bytes = 0, rows = 0, alg = 0;
     void begin(int64_t tile_rows) { cb = uint32_t(P.chunks.size()); bytes = 0; rows = tile_rows; alg = 0; }
@@ -341,7 +348,7 @@ struct NBuilder {
         P.alg_bytes += alg + int64_t(sizeof(double)) * rows_ * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
     }
     void finish() {
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < NFMT; ++f) {
             std::stable_sort(tmp[f].begin(), tmp[f].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
             P.segs[f].clear();
             for (auto& e : tmp[f]) {
@@ -360,7 +367,7 @@ struct NBuilder {
 struct TTBuilder {
     TTPass& P;
     const Store& S;
-    std::vector<std::pair<int64_t, TTSeg>> tmp[4];
+    std::vector<std::pair<int64_t, TTSeg>> tmp[NFMT];
     std::vector<int64_t> pbase, ncol;
     std::vector<uint32_t> oout;
     uint32_t cb = 0, voff = 0;
@@ -418,7 +425,7 @@ struct TTBuilder {
         P.alg_bytes += int64_t(sizeof(double)) * rows;
     }
     void finish() {
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < NFMT; ++f) {
             std::stable_sort(tmp[f].begin(), tmp[f].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
             P.segs[f].clear();
             for (auto& e : tmp[f]) {
@@ -497,7 +504,7 @@ std::vector<int64_t> inner_cuts(const Tiles& tc, int64_t col0, int64_t ncols) {
 // columns whose u_l asks for more than FP32 (possible when the block's
 // singular values span many orders of magnitude and the quadratic's root is
 // clamped) are stored in FP32.
-void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt) {
+void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt, int prec) {
     if (k <= 0) return;
     const double delta = eps * sv[0];
     double sum = 0;
@@ -510,7 +517,12 @@ void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt) {
     }
     for (int64_t l = 0; l < k; ++l) {
         const double u = sv[l] > 0 ? tol / sv[l] : 1.0;
-        fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : FMT_F32;
+        // MIXED: FP16 (unit roundoff 2^-11) where it suffices.  BFP16: the
+        // column's bit rate ceil(-log2 u) (bfp.hh:79-80) fits a 16-bit
+        // integer mantissa scaled to [2^14, 2^15), whose rounding error is
+        // at most 2^-15 of the chunk's largest entry.
+        if (prec == HLRC_PREC_BFP16) fmt[l] = u >= 0x1.0p-15 ? FMT_I16 : FMT_F32;
+        else fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : FMT_F32;
     }
 }
 
@@ -554,7 +566,7 @@ hlrc_status validate_plan(const Plan& p) {
     };
     for (size_t pi = 0; pi < p.npasses.size(); ++pi) {
         const NPass& np = p.npasses[pi];
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < NFMT; ++f)
             for (const NSeg& s : np.segs[f]) {
                 if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > np.chunks.size())
                     return fail(HLRC_ERR_INTERNAL, "N-pass %zu: bad segment", pi);
@@ -574,7 +586,7 @@ hlrc_status validate_plan(const Plan& p) {
     }
     for (size_t pi = 0; pi < p.ttpasses.size(); ++pi) {
         const TTPass& tp = p.ttpasses[pi];
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < NFMT; ++f)
             for (const TTSeg& s : tp.segs[f]) {
                 if (s.ld != pad_fmt(s.rows, f) || s.ce < s.cb || s.ce > tp.chunks.size())
                     return fail(HLRC_ERR_INTERNAL, "T-pass %zu: bad segment", pi);
@@ -618,10 +630,11 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
         return fail(HLRC_ERR_SHAPE, "matrix dimension exceeds 2^31-1");
-    if (o.precision < HLRC_PREC_F64 || o.precision > HLRC_PREC_MIXED)
+    if (o.precision < HLRC_PREC_F64 || o.precision > HLRC_PREC_BFP16)
         return fail(HLRC_ERR_ARG, "unknown precision %d", o.precision);
-    if (o.precision == HLRC_PREC_MIXED && !(o.mixed_eps > 0))
-        return fail(HLRC_ERR_ARG, "HLRC_PREC_MIXED needs mixed_eps > 0");
+    const bool valr = o.precision == HLRC_PREC_MIXED || o.precision == HLRC_PREC_BFP16;
+    if (valr && !(o.mixed_eps > 0))
+        return fail(HLRC_ERR_ARG, "HLRC_PREC_MIXED / HLRC_PREC_BFP16 need mixed_eps > 0");
     p = Plan();
     p.kind = 0;
     p.precision = o.precision;
@@ -681,9 +694,9 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
 
     // storage formats
     const uint8_t deffmt = default_format(o.precision);
-    const uint8_t densefmt = o.precision == HLRC_PREC_MIXED ? uint8_t(FMT_F32) : deffmt;
+    const uint8_t densefmt = valr ? uint8_t(FMT_F32) : deffmt;
     std::vector<std::vector<uint8_t>> colfmt(static_cast<size_t>(nb));
-    if (o.precision == HLRC_PREC_MIXED) {
+    if (valr) {
         for (int64_t i = 0; i < nb; ++i) {
             const hlrc_block& b = d.blocks[i];
             if (toff[size_t(i)] < 0) continue;
@@ -703,7 +716,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
             std::vector<double> svs(static_cast<size_t>(b.rank));
             for (int64_t l = 0; l < b.rank; ++l) svs[size_t(l)] = sv[size_t(ord[size_t(l)])];
             std::vector<uint8_t> fs(static_cast<size_t>(b.rank));
-            valr_formats(svs.data(), b.rank, o.mixed_eps, fs.data());
+            valr_formats(svs.data(), b.rank, o.mixed_eps, fs.data(), o.precision);
             colfmt[size_t(i)].assign(static_cast<size_t>(b.rank), FMT_F32);
             for (int64_t l = 0; l < b.rank; ++l) colfmt[size_t(i)][size_t(ord[size_t(l)])] = fs[size_t(l)];
         }
@@ -744,7 +757,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
         if ((ch.fmt == FMT_F64) != (o.precision == HLRC_PREC_F64))
             return fail(HLRC_ERR_INTERNAL, "chunk format %d in a plan of precision %d", ch.fmt, o.precision);
     st.fill(p.store);
-    for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
+    for (int f = 0; f < NFMT; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
     p.npasses.resize(2);
     p.ttpasses.resize(3);
@@ -848,7 +861,8 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
             p.max_rank = std::max(p.max_rank, b.rank);
         }
     }
-    p.matrix_bytes = st.unpadded[0] + st.unpadded[1] + st.unpadded[2] + st.unpadded[3];
+    p.matrix_bytes = 0;
+    for (int f = 0; f < NFMT; ++f) p.matrix_bytes += st.unpadded[f];
     p.algorithmic_bytes = p.matrix_bytes + 2 * 8 * (d.nrows + d.ncols);
     p.flops = int64_t(flops);
     return HLRC_OK;
@@ -976,7 +990,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     }
     st.close_region();   // one region: allocation order (FP64 only)
     st.fill(p.store);
-    for (int f = 0; f < 4; ++f) p.fmt_bytes[f] = st.unpadded[f];
+    for (int f = 0; f < NFMT; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
     p.tpasses.resize(1);
     p.npasses.resize(3);

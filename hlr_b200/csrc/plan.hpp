@@ -56,7 +56,7 @@ struct TPass {
 // a tile's chunks are grouped by format, and each format runs as its own
 // launch (FP64, FP32, FP16, BF16 in that fixed order).
 struct NPass {
-    std::vector<NSeg> segs[4];     // per StoreFmt, ordered by cost (descending)
+    std::vector<NSeg> segs[NFMT];     // per StoreFmt, ordered by cost (descending)
     std::vector<GChunk> chunks;
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0;
@@ -64,7 +64,7 @@ struct NPass {
 };
 
 struct TTPass {
-    std::vector<TTSeg> segs[4];    // per StoreFmt, ordered by cost (descending)
+    std::vector<TTSeg> segs[NFMT];    // per StoreFmt, ordered by cost (descending)
     std::vector<GChunk> chunks;
     std::vector<TGroup> groups;    // multi-tile outputs: partials summed in tile order
     // first level of the finish for outputs with many tiles: each entry sums
@@ -96,7 +96,7 @@ struct Plan {
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;
     int32_t max_rank = 0;
-    int64_t fmt_bytes[4] = {0, 0, 0, 0};  // stored bytes per StoreFmt (accounting of mixed precision)
+    int64_t fmt_bytes[NFMT] = {};  // stored bytes per StoreFmt (accounting of mixed precision)
 };
 
 // Returns HLRC_OK or an error (message recorded via fail()).  expected_area

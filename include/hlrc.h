@@ -71,9 +71,16 @@ typedef enum hlrc_precision {
     HLRC_PREC_F32  = 1,  /* FP32 storage, FP32 products, FP64 y accumulation     */
     HLRC_PREC_BF16 = 2,  /* BF16 storage, per-column FP32 scale, FP32 products   */
     HLRC_PREC_F16  = 3,  /* FP16 storage, per-column FP32 scale, FP32 products   */
-    HLRC_PREC_MIXED = 4  /* per-column choice FP32/FP16 from the singular values
+    HLRC_PREC_MIXED = 4, /* per-column choice FP32/FP16 from the singular values
                             (HLR's VALR rule, include/hlr/compress/valr.hh:402-510);
                             dense leaves FP32                                    */
+    HLRC_PREC_BFP16 = 5  /* per-column choice FP32/16-bit block floating point:
+                            VALR tolerances u_i as for MIXED, and a column whose
+                            bit rate ceil(-log2 u_i) (HLR's BFP rule,
+                            include/hlr/compress/bfp.hh:79-80) is at most 15
+                            is stored as 16-bit integers with a power-of-two
+                            scale per chunk; dense leaves FP32.  One-vector
+                            kernels only: multi-vector products loop them     */
 } hlrc_precision;
 
 /* ---------------------------------------------------------- host structures
