@@ -670,7 +670,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every product directly (no CUDA graph)")
-    ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed", "bfp16"],
+    ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed", "bfp"],
                     help="storage precision (default: the config's)")
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")
     args = ap.parse_args()

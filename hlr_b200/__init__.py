@@ -32,9 +32,9 @@ apply_transposed = 1
 apply_adjoint = 2
 
 # storage precisions (hlrc_precision)
-PREC_F64, PREC_F32, PREC_BF16, PREC_F16, PREC_MIXED, PREC_BFP16 = 0, 1, 2, 3, 4, 5
+PREC_F64, PREC_F32, PREC_BF16, PREC_F16, PREC_MIXED, PREC_BFP = 0, 1, 2, 3, 4, 5
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "bf16": PREC_BF16, "f16": PREC_F16, "mixed": PREC_MIXED,
-              "bfp16": PREC_BFP16}
+              "bfp": PREC_BFP}
 
 LEAF_DENSE, LEAF_LOWRANK = 0, 1
 PROBLEM_LOG1D, PROBLEM_EXP3D, PROBLEM_LAPLACE_SPH = 0, 1, 2

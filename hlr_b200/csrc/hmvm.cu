@@ -53,6 +53,7 @@ struct DevNPass {
     const NSeg2* seg2 = nullptr;      // reduced precision: both formats of a tile in one CTA
     int nseg2 = 0;
     int f16 = FMT_F16;                // the store's 16-bit format
+    int wide = FMT_F32;               // the store's wide format (FP32, or 24-bit for BFP)
     const void* chunks = nullptr;     // NChunk (FP64 plan) or QNChunk (reduced precision)
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0, alg_bytes = 0;
@@ -81,7 +82,7 @@ struct DevTTPass {
     int launches() const {
         const int n = (ngroups > 0 ? 1 : 0) + (ngroups1 > 0 ? 1 : 0);
         // reduced-precision stores: one grid for the runs of all formats
-        if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] + nmseg[FMT_I16] > 0) return n + 1;
+        if (nmseg[FMT_F32] + nmseg[FMT_F16] + nmseg[FMT_BF16] + nmseg[FMT_I16] + nmseg[FMT_I24] > 0) return n + 1;
         int k = n;
         for (int f = 0; f < NFMT; ++f) k += nsegs[f] > 0 ? 1 : 0;
         return k;
@@ -202,7 +203,7 @@ ArenaLayout arena_layout(const Plan& p) {
         L.n2.push_back(take(p.precision == HLRC_PREC_F64
                                 ? 0
                                 : (np.segs[FMT_F32].size() + np.segs[FMT_F16].size() + np.segs[FMT_BF16].size() +
-                                   np.segs[FMT_I16].size()) *
+                                   np.segs[FMT_I16].size() + np.segs[FMT_I24].size()) *
                                       sizeof(NSeg2)));
     }
     size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
@@ -483,13 +484,17 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
         if (!f64 && e == cudaSuccess) {
             // pair the FP32 and 16-bit segments of every output tile
-            // the store's one 16-bit format
-            d.f16 = !np.segs[FMT_BF16].empty() ? FMT_BF16 : (!np.segs[FMT_I16].empty() ? FMT_I16 : FMT_F16);
-            if (int(!np.segs[FMT_F16].empty()) + int(!np.segs[FMT_BF16].empty()) + int(!np.segs[FMT_I16].empty()) > 1) {
+            // the store's wide and 16-bit formats: 24-bit and 16-bit integers
+            // (block floating point), or FP32 and one of FP16 / BF16
+            auto has = [&](int f) { return !np.segs[f].empty(); };
+            const bool bfp = has(FMT_I24) || has(FMT_I16);
+            d.wide = bfp ? FMT_I24 : FMT_F32;
+            d.f16 = bfp ? FMT_I16 : (has(FMT_BF16) ? FMT_BF16 : FMT_F16);
+            if ((bfp && (has(FMT_F32) || has(FMT_F16) || has(FMT_BF16))) || (has(FMT_F16) && has(FMT_BF16))) {
                 cleanup();
-                return fail(HLRC_ERR_INTERNAL, "N-pass with two 16-bit formats");
+                return fail(HLRC_ERR_INTERNAL, "N-pass with an unsupported mix of formats");
             }
-            const std::vector<NSeg> s32 = remap_segs(np.segs[FMT_F32], pack_of);
+            const std::vector<NSeg> s32 = remap_segs(np.segs[d.wide], pack_of);
             const std::vector<NSeg> s16 = remap_segs(np.segs[d.f16], pack_of);
             std::vector<NSeg2> pairs;
             std::vector<int64_t> weight;
@@ -561,9 +566,9 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
 
     fill_info(p, L, hp->info);
-    // the 8-vector kernels take FP64, FP32 and FP16/BF16 columns; 16-bit
-    // integer (BFP16) stores loop the one-vector kernels instead
-    if (o.max_nrhs > 1 && p.precision != HLRC_PREC_BFP16) {
+    // the 8-vector kernels take FP64, FP32 and FP16/BF16 columns; block
+    // floating point (BFP) stores loop the one-vector kernels instead
+    if (o.max_nrhs > 1 && p.precision != HLRC_PREC_BFP) {
         const size_t nx = size_t(std::max(p.nrows, p.ncols)) * MR_RB;
         const size_t nt = size_t(std::max<int64_t>(1, p.n_t)) * MR_RB, nt2 = size_t(std::max<int64_t>(1, p.n_t2)) * MR_RB;
         const size_t np = size_t(std::max<int64_t>(1, hp->n_part)) * MR_RB;
@@ -728,19 +733,22 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 // reduced precision: each tile's run of columns, streamed in full
                 // 4 KB iterations; FP32 and 16-bit runs in one grid
                 if (!f64plan) {
-                    const int n32 = tp.nmseg[FMT_F32];
-                    if (tp.nmseg[FMT_BF16] > 0)
-                        k_ttform_qs<TW, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
-                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part, alpha,
+                    if (tp.nmseg[FMT_I24] + tp.nmseg[FMT_I16] > 0) {   // block floating point
+                        const int n24 = tp.nmseg[FMT_I24];
+                        k_ttform_qs<TW, FMT_I24, FMT_I16><<<n24 + tp.nmseg[FMT_I16], TW * 32, 0, s>>>(
+                            tp.mseg[FMT_I24], n24, tp.mseg[FMT_I16], tp.mcol, M->store, vin, vout, ws.part, alpha,
                             add);
-                    else if (tp.nmseg[FMT_I16] > 0)
-                        k_ttform_qs<TW, FMT_I16><<<n32 + tp.nmseg[FMT_I16], TW * 32, 0, s>>>(
-                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_I16], tp.mcol, M->store, vin, vout, ws.part, alpha,
-                            add);
-                    else if (n32 + tp.nmseg[FMT_F16] > 0)
-                        k_ttform_qs<TW, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
-                            tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part, alpha,
-                            add);
+                    } else {
+                        const int n32 = tp.nmseg[FMT_F32];
+                        if (tp.nmseg[FMT_BF16] > 0)
+                            k_ttform_qs<TW, FMT_F32, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
+                                tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part,
+                                alpha, add);
+                        else if (n32 + tp.nmseg[FMT_F16] > 0)
+                            k_ttform_qs<TW, FMT_F32, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
+                                tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part,
+                                alpha, add);
+                    }
                 }
             };
             if (M->ttform_warps == 4) ttform(Warps<4>{});
@@ -772,15 +780,15 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 // reduced precision: one CTA per tile takes the packs of both formats
                 const QNPack* qc = static_cast<const QNPack*>(np.chunks);
                 if (!f64plan && np.nseg2 > 0) {
-                    if (np.f16 == FMT_BF16)
-                        k_nform_q<NW, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
-                                                                             add);
-                    else if (np.f16 == FMT_I16)
-                        k_nform_q<NW, FMT_I16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
-                                                                            add);
+                    if (np.wide == FMT_I24)
+                        k_nform_q<NW, FMT_I24, FMT_I16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo,
+                                                                                    alpha, add);
+                    else if (np.f16 == FMT_BF16)
+                        k_nform_q<NW, FMT_F32, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt,
+                                                                                     vo, alpha, add);
                     else
-                        k_nform_q<NW, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo, alpha,
-                                                                            add);
+                        k_nform_q<NW, FMT_F32, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt,
+                                                                                    vo, alpha, add);
                 }
             };
             if (M->nform_warps == 4) nform(Warps<4>{});

@@ -27,6 +27,8 @@ template <> struct QFmt<FMT_F32> { static constexpr int R = 4, G = 16, C = 2, LO
 template <> struct QFmt<FMT_F16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
 template <> struct QFmt<FMT_BF16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
 template <> struct QFmt<FMT_I16> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
+// 24-bit: a lane's 8 rows are 16 bytes of high parts plus 8 bytes of low parts
+template <> struct QFmt<FMT_I24> { static constexpr int R = 8, G = 8, C = 4, LOG_G = 3; };
 
 // Packed FP32 pairs (sm_100 fma / sub .f32x2: two FP32 operations per
 // instruction) for the 16-bit integer format.
@@ -50,6 +52,7 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
     return d;
 }
 
+
 // 8 offset-binary 16-bit integers (16 loaded bytes) -> 4 exact packed float
 // pairs: a value u = v + 2^15 becomes the low mantissa bits of 1.5 * 2^23,
 // and one exact packed subtraction removes 1.5 * 2^23 + 2^15 (no integer
@@ -60,6 +63,24 @@ __device__ __forceinline__ void i16_pairs(const uint4& u, uint64_t (&p)[4]) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
         p[i] = sub2(pk2(__byte_perm(w[i], 0x4B400000u, 0x7610), __byte_perm(w[i], 0x4B400000u, 0x7632)), BIAS);
+}
+
+// 8 offset-binary 24-bit integers u = v + 2^22 < 2^23 (16 bytes of high
+// parts h = u >> 8, 8 bytes of low parts l) -> 4 exact packed float pairs:
+// the bytes l, h are placed under the exponent byte of 2^23 (u is the low 23
+// mantissa bits of 2^23 + u) by two byte permutes per row pair plus one that
+// interleaves the low parts with that exponent byte, and one packed
+// subtraction removes 2^23 + 2^22.
+__device__ __forceinline__ void i24_pairs(const uint4& hi, const uint2& lo, uint64_t (&p)[4]) {
+    constexpr uint64_t BIAS = 0x4B4000004B400000ull;   // 2^23 + 2^22, twice
+    const uint32_t h[4] = {hi.x, hi.y, hi.z, hi.w};
+    const uint32_t w[2] = {lo.x, lo.y};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        // [l(2i), 0x4B, l(2i+1), 0x4B]
+        const uint32_t L = __byte_perm(w[i >> 1], 0x4B4B4B4Bu, (i & 1) ? 0x5342 : 0x5140);
+        p[i] = sub2(pk2(__byte_perm(h[i], L, 0x5104), __byte_perm(h[i], L, 0x7326)), BIAS);
+    }
 }
 
 // 16 loaded bytes -> R floats
@@ -116,9 +137,11 @@ __device__ __forceinline__ QTTPack ld_pack(const QTTPack* p) {
 
 // The lane's 8 loads of a pack: column j = g + C*i of the pack lies in part 0
 // for j < n0, else in part 1.
+// For 24-bit chunks ml gets the lane's 8 bytes of low parts (2*ld bytes into
+// the column, 8 per lane).
 template <int FMT>
 __device__ __forceinline__ void load_pack(const uint8_t* A, uint32_t a0, uint32_t a1, int n0, int ntot, int ld,
-                                          int lane, uint4* m) {
+                                          int lane, uint4* m, uint2* ml = nullptr) {
     using F = QFmt<FMT>;
     const int g = lane >> F::LOG_G, l = lane & (F::G - 1);
     const bool active = l * F::R < ld;
@@ -128,7 +151,11 @@ __device__ __forceinline__ void load_pack(const uint8_t* A, uint32_t a0, uint32_
     for (int i = 0; i < 8; ++i) {
         const int j = g + F::C * i;
         const size_t off = j < n0 ? b0 + size_t(j) * colb : b1 + size_t(j - n0) * colb;
-        m[i] = (active && j < ntot) ? __ldcs(reinterpret_cast<const uint4*>(A + off)) : make_uint4(0u, 0u, 0u, 0u);
+        const bool ok = active && j < ntot;
+        m[i] = ok ? __ldcs(reinterpret_cast<const uint4*>(A + off)) : make_uint4(0u, 0u, 0u, 0u);
+        if constexpr (FMT == FMT_I24)
+            ml[i] = ok ? __ldcs(reinterpret_cast<const uint2*>(A + off + (ptrdiff_t(2 * ld) - ptrdiff_t(8 * l))))
+                       : make_uint2(0u, 0u);
     }
 }
 
@@ -147,8 +174,9 @@ __device__ __forceinline__ void npack_q(const QNPack& pk, const uint8_t* A, cons
     const double* v = (vo & VEC_T) ? vt + (vo & ~VEC_T) : vx + vo;
     const float vl = lane < ntot ? float(__ldg(v + (second ? lane - n0 : lane)) * double(sc)) : 0.f;
     uint4 m[8];
-    load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m);
-    if constexpr (FMT == FMT_I16) {
+    uint2 ml[FMT == FMT_I24 ? 8 : 1];
+    load_pack<FMT>(A, pk.p[0].a16, pk.p[1].a16, n0, ntot, ld, lane, m, ml);
+    if constexpr (FMT == FMT_I16 || FMT == FMT_I24) {
         // row pairs: one packed FMA per two rows
         uint64_t s2[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
@@ -156,7 +184,8 @@ __device__ __forceinline__ void npack_q(const QNPack& pk, const uint8_t* A, cons
             const float vj = __shfl_sync(0xffffffffu, vl, (g + F::C * i) & 31);
             const uint64_t vv = pk2f(vj, vj);
             uint64_t pr[4];
-            i16_pairs(m[i], pr);
+            if constexpr (FMT == FMT_I24) i24_pairs(m[i], ml[i], pr);
+            else i16_pairs(m[i], pr);
 #pragma unroll
             for (int k = 0; k < 4; ++k) fma2(s2[k], pr[k], vv);
         }
@@ -226,9 +255,10 @@ __device__ __forceinline__ void npacks_q(uint32_t cb, uint32_t ce, int ld, const
 }
 
 // N-form of a reduced-precision store: a CTA takes one output tile, both its
-// FP32 packs and its packs of the 16-bit format F16 (either may be empty),
-// sums them in FP64 and updates y once.
-template <int W, int F16>
+// packs of the wide format WIDE (FP32, or 24-bit for block floating point)
+// and its packs of the 16-bit format F16 (either may be empty), sums them in
+// FP64 and updates y once.
+template <int W, int WIDE, int F16>
 __global__ void __launch_bounds__(W * 32, 3)
 k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
           const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
@@ -236,14 +266,14 @@ k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, cons
     __shared__ double red[W][TILE];
     const NSeg2 sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double a32[QFmt<FMT_F32>::R], a16[QFmt<F16>::R];
+    double a32[QFmt<WIDE>::R], a16[QFmt<F16>::R];
 #pragma unroll
-    for (int r = 0; r < QFmt<FMT_F32>::R; ++r) a32[r] = 0.0;
+    for (int r = 0; r < QFmt<WIDE>::R; ++r) a32[r] = 0.0;
 #pragma unroll
     for (int r = 0; r < QFmt<F16>::R; ++r) a16[r] = 0.0;
-    npacks_q<W, FMT_F32>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
+    npacks_q<W, WIDE>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
     npacks_q<W, F16>(sg.cb16, sg.ce16, sg.ld16, packs, A, vx, vt, warp, lane, a16);
-    nflush_q<FMT_F32>(a32, lane, red[warp]);
+    nflush_q<WIDE>(a32, lane, red[warp]);
     __syncwarp();
     nflush_add_q<F16>(a16, lane, red[warp]);
     __syncthreads();
@@ -261,9 +291,9 @@ k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, cons
 // x of the lane's R rows
 // per-lane dot products of the 8 loaded column pieces with x
 template <int FMT>
-__device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float* p) {
+__device__ __forceinline__ void ttdots_q(const uint4* m, const uint2* ml, const float* xr, float* p) {
     using F = QFmt<FMT>;
-    if constexpr (FMT == FMT_I16) {
+    if constexpr (FMT == FMT_I16 || FMT == FMT_I24) {
         // packed: rows 2k, 2k+1 in one FMA, the two halves added at the end
         uint64_t x2[4];
 #pragma unroll
@@ -271,7 +301,8 @@ __device__ __forceinline__ void ttdots_q(const uint4* m, const float* xr, float*
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             uint64_t pr[4];
-            i16_pairs(m[i], pr);
+            if constexpr (FMT == FMT_I24) i24_pairs(m[i], ml[i], pr);
+            else i16_pairs(m[i], pr);
             uint64_t a = 0ull;
 #pragma unroll
             for (int k = 0; k < 4; ++k) fma2(a, pr[k], x2[k]);
@@ -326,12 +357,19 @@ __device__ __forceinline__ void ttform_qs(const MSeg& sg, const MCol* __restrict
     // after the reduction the lane holds column jown of the iteration
     const int jown = g + F::C * (l >> SH);
     const bool writer = (l & ((1 << SH) - 1)) == 0;
+    // 24-bit runs: the low parts of a lane's rows lie 2*ld - 8*l bytes after
+    // its high parts
+    const ptrdiff_t lo_off = 2 * ptrdiff_t(sg.ld) - 8 * ptrdiff_t(l);
+    uint2 ml[FMT == FMT_I24 ? 8 : 1];
     auto load = [&](int c0, uint4 (&m)[8]) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int j = c0 + g + F::C * i;
-            m[i] = (active && j < ncols) ? __ldcs(reinterpret_cast<const uint4*>(base + size_t(j) * colb))
-                                         : make_uint4(0u, 0u, 0u, 0u);
+            const bool ok = active && j < ncols;
+            m[i] = ok ? __ldcs(reinterpret_cast<const uint4*>(base + size_t(j) * colb)) : make_uint4(0u, 0u, 0u, 0u);
+            if constexpr (FMT == FMT_I24)
+                ml[i] = ok ? __ldcs(reinterpret_cast<const uint2*>(base + size_t(j) * colb + lo_off))
+                           : make_uint2(0u, 0u);
         }
     };
     int c0 = warp * BC;
@@ -341,7 +379,7 @@ __device__ __forceinline__ void ttform_qs(const MSeg& sg, const MCol* __restrict
     MCol mc = (writer && c0 + jown < ncols) ? ld_mcol(ctab + c0 + jown) : MCol{0u, 0.f};
     for (; c0 < ncols; c0 += W * BC) {
         float p[8];
-        ttdots_q<FMT>(m, xr, p);
+        ttdots_q<FMT>(m, ml, xr, p);
         const MCol done = mc;
         const int cd = c0;
         if (c0 + W * BC < ncols) {
@@ -363,15 +401,16 @@ __device__ __forceinline__ void ttform_qs(const MSeg& sg, const MCol* __restrict
 }
 
 // All stream segments of one tile T-form pass in one grid: the first n32
-// CTAs take the FP32 runs, the others the runs of the 16-bit format F16.
+// CTAs take the runs of the wide format WIDE (FP32, or 24-bit for block
+// floating point), the others the runs of the 16-bit format F16.
 // The outputs of the two formats are disjoint, so their CTAs may run side
 // by side, and the pass has a single tail.
-template <int W, int F16>
+template <int W, int WIDE, int F16>
 __global__ void __launch_bounds__(W * 32, 24 / W)
 k_ttform_qs(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
             const uint8_t* __restrict__ A, const double* __restrict__ vin, double* __restrict__ out,
             double* __restrict__ part, double alpha, int add) {
-    if (int(blockIdx.x) < n32) ttform_qs<W, FMT_F32>(segs32[blockIdx.x], cols, A, vin, out, part, alpha, add);
+    if (int(blockIdx.x) < n32) ttform_qs<W, WIDE>(segs32[blockIdx.x], cols, A, vin, out, part, alpha, add);
     else ttform_qs<W, F16>(segs16[blockIdx.x - n32], cols, A, vin, out, part, alpha, add);
 }
 

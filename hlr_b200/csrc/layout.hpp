@@ -111,10 +111,15 @@ enum StoreFmt : uint8_t {
     FMT_F16 = 2,     // IEEE binary16, scaled
     FMT_BF16 = 3,    // bfloat16, scaled
     FMT_I16 = 4,     // 16-bit integer (block floating point), scaled; stored offset-binary (v + 2^15)
+    FMT_I24 = 5,     // 24-bit integer (block floating point, |v| < 2^22), scaled; offset-binary
+                     // u = v + 2^22 stored per column as ld 16-bit high parts (u >> 8), then ld
+                     // 8-bit low parts
 };
-constexpr int NFMT = 5;   // number of storage formats
+constexpr int NFMT = 6;   // number of storage formats
 
-inline constexpr int fmt_bytes(int f) { return f == FMT_F64 ? 8 : (f == FMT_F32 ? 4 : 2); }
+inline constexpr int fmt_bytes(int f) {
+    return f == FMT_F64 ? 8 : (f == FMT_F32 ? 4 : (f == FMT_I24 ? 3 : 2));
+}
 
 struct QNChunk {           // N-form chunk of a reduced-precision store
     uint32_t a16;          // byte offset / 16 of the chunk's first column

@@ -96,8 +96,10 @@ uint16_t to_f16(float f) {
 // columns are padded so that every lane's 16-byte load is aligned: rows are
 // padded to 2 (FP64), 4 (FP32) or 8 (16-bit).
 inline int chunk_cols(int f) { return f == FMT_F64 ? 8 : (f == FMT_F32 ? 16 : 32); }
+// 24-bit columns pad to 16 rows: the 8-byte low-part loads of a lane then
+// start 16-byte aligned runs like the 16-byte high-part loads
 inline int64_t pad_fmt(int64_t rows, int f) {
-    const int64_t m = f == FMT_F64 ? 2 : (f == FMT_F32 ? 4 : 8);
+    const int64_t m = f == FMT_F64 ? 2 : (f == FMT_F32 ? 4 : (f == FMT_I24 ? 16 : 8));
     return (rows + m - 1) / m * m;
 }
 
@@ -120,7 +122,7 @@ struct SSlab {
 // contiguous run of columns in every store this planner produces: FP64 D,U;
 // FP32 D,U; mixed D(FP32),U(FP32),U(FP16); FP16 / BF16 U,D.
 inline int layout_rank(int group, int fmt) {
-    static const int rank[NFMT][2] = {{0, 1}, {2, 3}, {5, 4}, {7, 6}, {9, 8}};   // [fmt][group]: D = 0, factor = 1
+    static const int rank[NFMT][2] = {{0, 1}, {2, 3}, {5, 4}, {7, 6}, {9, 8}, {10, 11}};   // [fmt][group]: D = 0, factor = 1
     return rank[fmt][group];
 }
 
@@ -193,6 +195,28 @@ struct Store {
                         float* d = reinterpret_cast<float*>(dst) + j * ldc;
                         for (int64_t i = 0; i < s.rows; ++i) d[i] = float(src[i + j * s.lds]);
                     }
+                } else if (ch.fmt == FMT_I24) {
+                    // power-of-two scale bringing the chunk's largest entry to
+                    // [2^21, 2^22); u = v + 2^22 as 16-bit high and 8-bit low parts
+                    double amax = 0;
+                    for (int j = 0; j < ch.nc; ++j)
+                        for (int64_t i = 0; i < s.rows; ++i) amax = std::max(amax, std::fabs(src[i + j * s.lds]));
+                    int ex = 0;
+                    if (amax > 0) std::frexp(amax, &ex);
+                    const double scale = amax > 0 ? std::ldexp(1.0, ex - 22) : 1.0;
+                    ch.scale = float(scale);
+                    const double inv = 1.0 / scale;
+                    for (int j = 0; j < ch.nc; ++j) {
+                        uint16_t* hi = reinterpret_cast<uint16_t*>(dst + size_t(j) * size_t(ldc) * 3);
+                        uint8_t* lo = dst + size_t(j) * size_t(ldc) * 3 + size_t(ldc) * 2;
+                        for (int64_t i = 0; i < ldc; ++i) {   // padding rows decode to 0
+                            const double q =
+                                i < s.rows ? std::nearbyint(src[i + j * s.lds] * inv) : 0.0;
+                            const uint32_t u = uint32_t(int32_t(std::max(-4194303.0, std::min(4194303.0, q))) + 4194304);
+                            hi[i] = uint16_t(u >> 8);
+                            lo[i] = uint8_t(u & 0xffu);
+                        }
+                    }
                 } else {
                     // power-of-two scale bringing the chunk's largest entry to [2^14, 2^15)
                     double amax = 0;
@@ -205,6 +229,8 @@ struct Store {
                     const double inv = 1.0 / scale;
                     for (int j = 0; j < ch.nc; ++j) {
                         uint16_t* d = reinterpret_cast<uint16_t*>(dst) + j * ldc;
+                        if (ch.fmt == FMT_I16)   // padding rows decode to 0
+                            for (int64_t i = s.rows; i < ldc; ++i) d[i] = 0x8000u;
                         for (int64_t i = 0; i < s.rows; ++i) {
                             if (ch.fmt == FMT_I16) {
                                 // round to nearest, |value| < 2^15 after scaling;
@@ -517,11 +543,12 @@ void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt, int pre
     }
     for (int64_t l = 0; l < k; ++l) {
         const double u = sv[l] > 0 ? tol / sv[l] : 1.0;
-        // MIXED: FP16 (unit roundoff 2^-11) where it suffices.  BFP16: the
+        // MIXED: FP16 (unit roundoff 2^-11) where it suffices.  BFP: the
         // column's bit rate ceil(-log2 u) (bfp.hh:79-80) fits a 16-bit
         // integer mantissa scaled to [2^14, 2^15), whose rounding error is
-        // at most 2^-15 of the chunk's largest entry.
-        if (prec == HLRC_PREC_BFP16) fmt[l] = u >= 0x1.0p-15 ? FMT_I16 : FMT_F32;
+        // at most 2^-15 of the chunk's largest entry; other columns take 24
+        // bits (scaled to [2^21, 2^22): 2^-22)
+        if (prec == HLRC_PREC_BFP) fmt[l] = u >= 0x1.0p-15 ? FMT_I16 : FMT_I24;
         else fmt[l] = u >= 0x1.0p-11 ? FMT_F16 : FMT_F32;
     }
 }
@@ -630,11 +657,11 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
         return fail(HLRC_ERR_SHAPE, "matrix dimension exceeds 2^31-1");
-    if (o.precision < HLRC_PREC_F64 || o.precision > HLRC_PREC_BFP16)
+    if (o.precision < HLRC_PREC_F64 || o.precision > HLRC_PREC_BFP)
         return fail(HLRC_ERR_ARG, "unknown precision %d", o.precision);
-    const bool valr = o.precision == HLRC_PREC_MIXED || o.precision == HLRC_PREC_BFP16;
+    const bool valr = o.precision == HLRC_PREC_MIXED || o.precision == HLRC_PREC_BFP;
     if (valr && !(o.mixed_eps > 0))
-        return fail(HLRC_ERR_ARG, "HLRC_PREC_MIXED / HLRC_PREC_BFP16 need mixed_eps > 0");
+        return fail(HLRC_ERR_ARG, "HLRC_PREC_MIXED / HLRC_PREC_BFP need mixed_eps > 0");
     p = Plan();
     p.kind = 0;
     p.precision = o.precision;
@@ -694,7 +721,8 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
 
     // storage formats
     const uint8_t deffmt = default_format(o.precision);
-    const uint8_t densefmt = valr ? uint8_t(FMT_F32) : deffmt;
+    const uint8_t densefmt =
+        o.precision == HLRC_PREC_BFP ? uint8_t(FMT_I24) : (valr ? uint8_t(FMT_F32) : deffmt);
     std::vector<std::vector<uint8_t>> colfmt(static_cast<size_t>(nb));
     if (valr) {
         for (int64_t i = 0; i < nb; ++i) {

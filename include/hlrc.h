@@ -74,13 +74,15 @@ typedef enum hlrc_precision {
     HLRC_PREC_MIXED = 4, /* per-column choice FP32/FP16 from the singular values
                             (HLR's VALR rule, include/hlr/compress/valr.hh:402-510);
                             dense leaves FP32                                    */
-    HLRC_PREC_BFP16 = 5  /* per-column choice FP32/16-bit block floating point:
-                            VALR tolerances u_i as for MIXED, and a column whose
-                            bit rate ceil(-log2 u_i) (HLR's BFP rule,
-                            include/hlr/compress/bfp.hh:79-80) is at most 15
-                            is stored as 16-bit integers with a power-of-two
-                            scale per chunk; dense leaves FP32.  One-vector
-                            kernels only: multi-vector products loop them     */
+    HLRC_PREC_BFP = 5    /* block floating point, byte-aligned: VALR tolerances
+                            u_i as for MIXED; a column whose bit rate
+                            ceil(-log2 u_i) (HLR's BFP rule,
+                            include/hlr/compress/bfp.hh:79-80) is at most 15 is
+                            stored as 16-bit integers, every other column and
+                            the dense leaves as 24-bit integers (22 bits of
+                            magnitude), each chunk with a power-of-two scale.
+                            One-vector kernels only: multi-vector products
+                            loop them                                          */
 } hlrc_precision;
 
 /* ---------------------------------------------------------- host structures

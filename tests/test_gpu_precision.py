@@ -7,8 +7,8 @@ the same matrix, x ~ N(0,1)):
   mixed  <= 1e-6   (VALR: FP16 only for columns with sigma_l small enough)
   f16    <= 2e-3   (unit roundoff 4.9e-4)
   bf16   <= 1.5e-2 (unit roundoff 3.9e-3)
-  bfp16  <= 1e-6   (VALR: 16-bit block floating point only for columns whose
-                    bit rate is at most 15)
+  bfp    <= 1e-6   (VALR: 16-bit block floating point for columns whose bit
+                    rate is at most 15, 24-bit for the rest and the dense leaves)
 """
 import numpy as np
 import pytest
@@ -22,7 +22,7 @@ torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp16": 1e-6}
+TOL = {"f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp": 1e-6}
 
 
 def gpu(M, alpha, op, x, y0):
@@ -32,7 +32,7 @@ def gpu(M, alpha, op, x, y0):
     return y.cpu().numpy()
 
 
-@pytest.mark.parametrize("prec", ["f32", "mixed", "f16", "bf16", "bfp16"])
+@pytest.mark.parametrize("prec", ["f32", "mixed", "f16", "bf16", "bfp"])
 @pytest.mark.parametrize("op", [0, 1])
 def test_exp3d_reduced_precision_error(prec, op):
     hm = built("exp3d_16384_64", lambda: hlr.build(hlr.Problem.exp3d(16384)))
@@ -47,7 +47,7 @@ def test_exp3d_reduced_precision_error(prec, op):
     M.free()
 
 
-@pytest.mark.parametrize("prec", ["f32", "mixed", "f16", "bfp16"])
+@pytest.mark.parametrize("prec", ["f32", "mixed", "f16", "bfp"])
 def test_log1d_reduced_precision_error(c1, prec):
     M = hlr.upload(c1, precision=prec)
     x = np.random.default_rng(13).standard_normal(c1.n)
@@ -93,7 +93,7 @@ def test_exactly_representable_known_answer():
     A = np.zeros((6, 6))
     A[:3, :3], A[:3, 3:], A[3:, 3:] = D0, U @ V.T, D1
     x = rng.integers(-3, 4, 6).astype(float)
-    for prec in ("f32", "f16", "bf16", "mixed", "bfp16"):
+    for prec in ("f32", "f16", "bf16", "mixed", "bfp"):
         M = hlr.upload(ll, precision=prec)
         for op, Aop in ((0, A), (1, A.T)):
             np.testing.assert_allclose(gpu(M, 1.0, op, x, np.zeros(6)), Aop @ x, rtol=0, atol=1e-9)

@@ -13,7 +13,7 @@ torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"f64": 1e-13, "f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp16": 1e-6}
+TOL = {"f64": 1e-13, "f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp": 1e-6}
 
 
 def leaves(nrows, ncols, seed):
@@ -45,7 +45,7 @@ def leaves(nrows, ncols, seed):
 
 
 @pytest.mark.parametrize("shape", [(1, 1), (3, 7), (70, 33), (200, 130), (130, 200), (257, 257)])
-@pytest.mark.parametrize("prec", ["f64", "mixed", "f16", "bf16", "f32", "bfp16"])
+@pytest.mark.parametrize("prec", ["f64", "mixed", "f16", "bf16", "f32", "bfp"])
 def test_rectangular_and_tiny(shape, prec):
     nrows, ncols = shape
     ll, A = leaves(nrows, ncols, seed=nrows * 1000 + ncols)

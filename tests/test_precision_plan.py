@@ -13,12 +13,12 @@ def test_store_bytes_by_precision(request, fixture):
     b16 = hlr.plan_info(hm, precision="f16")["matrix_bytes"]
     bbf = hlr.plan_info(hm, precision="bf16")["matrix_bytes"]
     bmx = hlr.plan_info(hm, precision="mixed")["matrix_bytes"]
-    bbfp = hlr.plan_info(hm, precision="bfp16")["matrix_bytes"]
+    bbfp = hlr.plan_info(hm, precision="bfp")["matrix_bytes"]
     assert b32 * 2 == b64
     assert b16 == bbf and b64 / 4 < b16 < b64 / 4 * 1.2  # 16-bit data + one FP32 scale per chunk
     assert b16 < bmx < b32  # dense FP32, low-rank columns FP32 or FP16
-    # BFP16 moves every column whose bit rate is at most 15 to 16 bits: a
-    # superset of the FP16 columns of the mixed store
+    # BFP stores every column whose bit rate is at most 15 in 16 bits (a
+    # superset of the FP16 columns of the mixed store), the rest in 24
     assert b16 < bbfp < bmx
 
 
@@ -38,20 +38,22 @@ def test_mixed_store_never_holds_fp64_columns(c2_small):
     assert tight == hlr.plan_info(c2_small, precision="f32")["matrix_bytes"]
 
 
-def test_bfp16_tolerance_and_no_fp64_columns(c2_small):
+def test_bfp_tolerance_and_24_bit_floor(c2_small):
     with pytest.raises(hlr.HLRCError):
-        hlr.plan_info(c2_small, precision="bfp16", mixed_eps=0.0)
-    tight = hlr.plan_info(c2_small, precision="bfp16", mixed_eps=1e-14)["matrix_bytes"]
-    assert tight == hlr.plan_info(c2_small, precision="f32")["matrix_bytes"]
+        hlr.plan_info(c2_small, precision="bfp", mixed_eps=0.0)
+    # a tolerance no 16-bit column meets: every column and leaf takes 24 bits
+    tight = hlr.plan_info(c2_small, precision="bfp", mixed_eps=1e-14)["matrix_bytes"]
+    b32 = hlr.plan_info(c2_small, precision="f32")["matrix_bytes"]
+    assert 0.75 * b32 < tight < 0.76 * b32     # 3 bytes per entry plus chunk scales
 
 
-def test_bfp16_column_choice_and_accounting():
+def test_bfp_column_choice_and_accounting():
     # a rank-1 leaf at eps = 1e-2 has VALR tolerance u = 1e-2 >= 2^-15: U and
     # V are one 16-bit chunk each, counted as 2 rows x 2 bytes plus one FP32
     # chunk scale
     ll = hlr.LeafList(2, 2)
     ll.add_lowrank(0, 0, np.array([[1.0], [2.0]]), np.array([[3.0], [1.0]]))
-    info = hlr.plan_info(ll, precision="bfp16", mixed_eps=1e-2)
+    info = hlr.plan_info(ll, precision="bfp", mixed_eps=1e-2)
     assert info["matrix_bytes"] == 2 * (2 * 2 + 4)
 
 
