@@ -266,16 +266,34 @@ k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, cons
     __shared__ double red[W][TILE];
     const NSeg2 sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double a32[QFmt<WIDE>::R], a16[QFmt<F16>::R];
+    if constexpr (WIDE == FMT_I24) {
+        // the wide packs flushed before the 16-bit ones start: fewer live
+        // registers next to the 24-bit loads
+        {
+            double a32[QFmt<WIDE>::R];
 #pragma unroll
-    for (int r = 0; r < QFmt<WIDE>::R; ++r) a32[r] = 0.0;
+            for (int r = 0; r < QFmt<WIDE>::R; ++r) a32[r] = 0.0;
+            npacks_q<W, WIDE>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
+            nflush_q<WIDE>(a32, lane, red[warp]);
+        }
+        double a16[QFmt<F16>::R];
 #pragma unroll
-    for (int r = 0; r < QFmt<F16>::R; ++r) a16[r] = 0.0;
-    npacks_q<W, WIDE>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
-    npacks_q<W, F16>(sg.cb16, sg.ce16, sg.ld16, packs, A, vx, vt, warp, lane, a16);
-    nflush_q<WIDE>(a32, lane, red[warp]);
-    __syncwarp();
-    nflush_add_q<F16>(a16, lane, red[warp]);
+        for (int r = 0; r < QFmt<F16>::R; ++r) a16[r] = 0.0;
+        npacks_q<W, F16>(sg.cb16, sg.ce16, sg.ld16, packs, A, vx, vt, warp, lane, a16);
+        __syncwarp();
+        nflush_add_q<F16>(a16, lane, red[warp]);
+    } else {
+        double a32[QFmt<WIDE>::R], a16[QFmt<F16>::R];
+#pragma unroll
+        for (int r = 0; r < QFmt<WIDE>::R; ++r) a32[r] = 0.0;
+#pragma unroll
+        for (int r = 0; r < QFmt<F16>::R; ++r) a16[r] = 0.0;
+        npacks_q<W, WIDE>(sg.cb32, sg.ce32, sg.ld32, packs, A, vx, vt, warp, lane, a32);
+        npacks_q<W, F16>(sg.cb16, sg.ce16, sg.ld16, packs, A, vx, vt, warp, lane, a16);
+        nflush_q<WIDE>(a32, lane, red[warp]);
+        __syncwarp();
+        nflush_add_q<F16>(a16, lane, red[warp]);
+    }
     __syncthreads();
     if (threadIdx.x < sg.rows) {
         double s = 0.0;
