@@ -56,7 +56,9 @@ def lib() -> C.CDLL:
 
 
 def _p(a: np.ndarray):
-    assert a.dtype == np.float64
+    """Address of a float64 array the C code reads or writes as contiguous."""
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("oracle vectors must be contiguous float64 arrays")
     return a.ctypes.data
 
 
