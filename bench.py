@@ -8,7 +8,7 @@ host by the library's own construction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config c2|c1|c3|c2s|c4|c5] [--precision P] [--nrhs K]
-                    [--no-cpu-baseline] [--no-autotune] [--no-graph]
+                    [--no-cpu-baseline] [--no-autotune] [--no-graph] [--h2]
 
 Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
 independent replica of the product on its own GPU (the MVM has no exchange
@@ -138,10 +138,15 @@ def gpu_uuid(dev: int) -> str:
         return str(dev)
 
 
-def make_problem(cfg, nthreads):
+def make_problem(cfg, nthreads, h2=False):
+    """Problem of a config; with h2 the same problem in H^2 form (nested
+    cluster bases built from the H-matrix leaves) instead of H / uniform-H."""
     import hlr_b200 as hlr
     desc, kw, uniform, prec, nrhs = CONFIGS[cfg]
     kw = dict(kw)
+    if h2:
+        kw["nested"], kw["uniform"], uniform = True, False, False
+        desc = desc.replace("uniform-H", "H2 (nested cluster bases)").replace("FP64 H-MVM", "FP64 H2-MVM")
     kw.setdefault("leaf_size", 64)
     kw.setdefault("eta", 2.0)
     kw.setdefault("eps", 1e-6)
@@ -151,7 +156,10 @@ def make_problem(cfg, nthreads):
 
 def cpu_mvm(hm, uniform, desc_obj, x, y, nthreads):
     import oracle
-    if uniform:
+    from hlr_b200 import _capi
+    if isinstance(desc_obj, _capi.hlrc_h2_desc):
+        assert oracle.h2_mvm(desc_obj, 1.0, 0, x, y) == 0
+    elif uniform:
         st = oracle.uniform_mvm(desc_obj, 1.0, 0, x, y, nthreads)
         assert st == 0
     else:
@@ -168,9 +176,9 @@ def run_reference(args, rank, world):
     if args.config == "c5":
         run_reference_batch(args, nthreads)
         return
-    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads)
+    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads, args.h2)
     hm = hlr.build(prob)
-    d = hm.uniform_desc() if uniform else hm.h_desc()
+    d = hm.h2_desc() if args.h2 else (hm.uniform_desc() if uniform else hm.h_desc())
     x = np.random.default_rng(2).standard_normal(hm.n)
     y = np.zeros(hm.n)
     t0 = time.perf_counter()
@@ -179,7 +187,7 @@ def run_reference(args, rank, world):
     # bound the run: a step is a sample of the leaves when K full products would exceed ~120 s
     frac = 1.0
     dd = d
-    if not uniform and args.steps * t_full > 120.0:
+    if not uniform and not args.h2 and args.steps * t_full > 120.0:
         stride = int(np.ceil(args.steps * t_full / 120.0))
         sub = [d.blocks[i] for i in range(0, d.nblocks, stride)]
         import ctypes as C
@@ -207,9 +215,10 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "n": hm.n},
-        "cpu_baseline": {"value": value, "unit": "MVM/s", "cores": nthreads, "kind": "port",
-                         "sample": sample + "; oracle/oracle.c oracle_hmvm_chunk (restated hlr::tbb::mul_vec, "
-                                            "64-row chunk locks, OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "MVM/s", "cores": 1 if args.h2 else nthreads, "kind": "port",
+                         "sample": sample + ("; oracle/oracle.c oracle_h2_mvm (restated hlr::h2::mul_vec, sequential)"
+                                             if args.h2 else "; oracle/oracle.c oracle_hmvm_chunk (restated "
+                                             "hlr::tbb::mul_vec, 64-row chunk locks, OpenMP)")},
         "e2e": {"value": value, "unit": "MVM/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -269,7 +278,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     ncpu = os.cpu_count() or 1
     nthreads = max(1, ncpu // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", world))))
-    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads)
+    prob, desc, uniform, prec, nrhs = make_problem(args.config, nthreads, args.h2)
     if args.precision:
         prec = args.precision
         desc = desc.replace("FP64 ", f"{prec.upper()}-stored ") if prec != "f64" else desc
@@ -279,7 +288,7 @@ def run_ours(args, rank, world, local_rank):
     hm = hlr.build(prob)
     t_build = time.perf_counter() - tb
     tu = time.perf_counter()
-    M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs)
+    M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2)
     t_upload = time.perf_counter() - tu
     tuned = tune_handle(M, nrhs, args)
     info = M.info
@@ -366,7 +375,7 @@ def run_ours(args, rank, world, local_rank):
     # same way, is the error reference and the speed-up denominator
     fp64 = None
     if prec != "f64":
-        M64 = hlr.upload(hm, precision="f64", uniform=uniform, max_nrhs=nrhs)
+        M64 = hlr.upload(hm, precision="f64", uniform=uniform, max_nrhs=nrhs, h2=args.h2)
         tune_handle(M64, nrhs, args)
         y64 = dev_vec(np.zeros((nrhs, n)))
         hlr.mul_vec(1.0, hlr.apply_normal, M64, x, y64)
@@ -448,7 +457,7 @@ def run_ours(args, rank, world, local_rank):
         line["fp64_gpu"] = fp64
     # CPU baseline (oracle port on the host cores, bounded sample) and error
     if not args.no_cpu_baseline and world == 1:
-        d = hm.uniform_desc() if uniform else hm.h_desc()
+        d = hm.h2_desc() if args.h2 else (hm.uniform_desc() if uniform else hm.h_desc())
         ncores = os.cpu_count() or 1
         yo = np.zeros(n)
         t0 = time.perf_counter()
@@ -463,9 +472,10 @@ def run_ours(args, rank, world, local_rank):
             cpu_mvm(hm, uniform, d, np.ascontiguousarray(xh[0]), yy, ncores)
             el += time.perf_counter() - t0
             reps += 1
-        line["cpu_baseline"] = {"value": reps / el, "unit": "MVM/s", "cores": ncores, "kind": "port",
+        line["cpu_baseline"] = {"value": reps / el, "unit": "MVM/s", "cores": 1 if args.h2 else ncores, "kind": "port",
                                 "sample": f"{reps} full products of the same matrix and x after 1 warm-up "
-                                          f"({el:.1f} s); oracle/oracle.c restatement of hlr::tbb::mul_vec"}
+                                          f"({el:.1f} s); oracle/oracle.c restatement of "
+                                          + ("hlr::h2::mul_vec (sequential)" if args.h2 else "hlr::tbb::mul_vec")}
     print(json.dumps(line), flush=True)
 
 
@@ -618,12 +628,14 @@ def run_batch(args, rank, world, local_rank):
 
 
 def roofline_from_profile(prof: dict, hbm_peak: float, peak_kind: str, workload: str):
-    """Roofline object of the dominant pass (largest device time) of a
-    per-pass CUDA-event profile {name: (launches, total ms, bytes/launch)}:
+    """Roofline object of the dominant pass of a per-pass CUDA-event profile
+    {name: (launches, total ms, bytes/launch)}: the pass that moves the most
+    bytes (for the H and uniform-H products also the one with the largest
+    time; for H^2 the leaf pass rather than a level of small transfers).
     achieved = algorithmic bytes per launch / average launch time."""
     if not prof:
         return None
-    name, (cnt, tot_ms, by) = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (cnt, tot_ms, by) = max(prof.items(), key=lambda kv: kv[1][0] * kv[1][2])
     avg_ms = tot_ms / max(1, cnt)
     achieved = by / (avg_ms / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -670,6 +682,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every product directly (no CUDA graph)")
+    ap.add_argument("--h2", action="store_true", help="the config's problem in H2 form (nested cluster bases)")
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed", "bfp"],
                     help="storage precision (default: the config's)")
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")

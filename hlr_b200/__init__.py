@@ -54,6 +54,7 @@ class Problem:
     refine: int = 6
     uniform: bool = False
     nthreads: int = 0
+    nested: bool = False   # also build the H^2 form (nested cluster bases)
 
     @staticmethod
     def log1d(n: int, **kw) -> "Problem":
@@ -75,6 +76,7 @@ class Problem:
         p.kind, p.leaf_size, p.n, p.refine = self.kind, self.leaf_size, self.n, self.refine
         p.uniform, p.seed, p.eta, p.eps = int(self.uniform), self.seed, self.eta, self.eps
         p.ell, p.nugget, p.nthreads = self.ell, self.nugget, self.nthreads
+        p.nested = int(self.nested)
         return p
 
 
@@ -111,6 +113,12 @@ class HostMatrix:
     def uniform_desc(self) -> _capi.hlrc_uniform_desc:
         d = _capi.hlrc_uniform_desc()
         check(lib().hlrc_build_uniform_desc(self._h, C.byref(d)), "hlrc_build_uniform_desc")
+        d._owner = self
+        return d
+
+    def h2_desc(self) -> _capi.hlrc_h2_desc:
+        d = _capi.hlrc_h2_desc()
+        check(lib().hlrc_build_h2_desc(self._h, C.byref(d)), "hlrc_build_h2_desc")
         d._owner = self
         return d
 
@@ -195,6 +203,7 @@ class DeviceMatrix:
     def __init__(self, handle: C.c_void_p, uniform: bool):
         self._h = handle
         self.uniform = uniform
+        self.h2 = False
         inf = _capi.hlrc_info()
         check(lib().hlrc_get_info(self._h, C.byref(inf)), "hlrc_get_info")
         self.info = {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
@@ -260,12 +269,23 @@ class DeviceMatrix:
 
 
 def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
-           mixed_eps: float = 1e-6, device: int = -1) -> DeviceMatrix:
-    """Flatten and upload a matrix: ``src`` is a HostMatrix, LeafList or descriptor."""
+           mixed_eps: float = 1e-6, device: int = -1, h2: bool = False) -> DeviceMatrix:
+    """Flatten and upload a matrix: ``src`` is a HostMatrix, LeafList or
+    descriptor.  ``h2=True`` uploads the H^2 form (nested cluster bases) of
+    a HostMatrix built with ``Problem(..., nested=True)``, or an
+    ``hlrc_h2_desc``."""
+    if isinstance(src, _capi.hlrc_h2_desc):
+        h2 = True
     if uniform is None:
-        uniform = isinstance(src, HostMatrix) and src.problem.uniform
+        uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
     o = _options(precision, max_nrhs, mixed_eps, device)
     h = C.c_void_p()
+    if h2:
+        d = src.h2_desc() if hasattr(src, "h2_desc") else src
+        check(lib().hlrc_upload_h2(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_h2")
+        M = DeviceMatrix(h, False)
+        M.h2 = True
+        return M
     if uniform:
         d = src.uniform_desc() if hasattr(src, "uniform_desc") else src
         check(lib().hlrc_upload_uniform(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_uniform")
@@ -306,13 +326,18 @@ def upload_batch(members, precision="f64", max_nrhs: int = 1, pad_to: Optional[i
 
 
 def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
-              mixed_eps: float = 1e-6) -> dict:
+              mixed_eps: float = 1e-6, h2: bool = False) -> dict:
     """Dry run of :func:`upload`: validates and flattens on the host only."""
+    if isinstance(src, _capi.hlrc_h2_desc):
+        h2 = True
     if uniform is None:
-        uniform = isinstance(src, HostMatrix) and src.problem.uniform
+        uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
     o = _options(precision, max_nrhs, mixed_eps, -1)
     inf = _capi.hlrc_info()
-    if uniform:
+    if h2:
+        d = src.h2_desc() if hasattr(src, "h2_desc") else src
+        check(lib().hlrc_plan_info_h2(C.byref(d), C.byref(o), C.byref(inf)), "hlrc_plan_info_h2")
+    elif uniform:
         d = src.uniform_desc() if hasattr(src, "uniform_desc") else src
         check(lib().hlrc_plan_info_uniform(C.byref(d), C.byref(o), C.byref(inf)), "hlrc_plan_info_uniform")
     else:
@@ -378,6 +403,15 @@ def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
 mvm = mul_vec
 
 
+class h2:  # namespace mirroring hlr::h2
+    @staticmethod
+    def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
+        """y += alpha * op(M) x for an H^2 matrix (op N or adjoint)."""
+        if not getattr(M, "h2", False):
+            raise ValueError("h2.mul_vec needs an H^2 DeviceMatrix (upload(..., h2=True))")
+        mul_vec(alpha, op, M, x, y, stream)
+
+
 class uniform:  # namespace mirroring hlr::tbb::uniform
     @staticmethod
     def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
@@ -389,5 +423,5 @@ class uniform:  # namespace mirroring hlr::tbb::uniform
 
 __all__ = [
     "apply_normal", "apply_transposed", "apply_adjoint", "Problem", "HostMatrix", "LeafList", "DeviceMatrix",
-    "build", "upload", "mul_vec", "mvm", "uniform", "HLRCError", "PRECISIONS",
+    "build", "upload", "mul_vec", "mvm", "uniform", "h2", "HLRCError", "PRECISIONS",
 ]

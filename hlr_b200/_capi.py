@@ -49,6 +49,18 @@ class hlrc_uniform_desc(C.Structure):
                 ("nblocks", i64), ("blocks", C.POINTER(hlrc_uniform_block))]
 
 
+class hlrc_h2_cluster(C.Structure):
+    _fields_ = [("ofs", i64), ("size", i64), ("son", i32 * 2), ("parent", i32), ("rank", i32),
+                ("V", pdbl), ("ldv", i64), ("E", pdbl), ("lde", i64)]
+
+
+class hlrc_h2_desc(C.Structure):
+    _fields_ = [("nrows", i64), ("ncols", i64),
+                ("nrow_clusters", i64), ("row_clusters", C.POINTER(hlrc_h2_cluster)),
+                ("ncol_clusters", i64), ("col_clusters", C.POINTER(hlrc_h2_cluster)),
+                ("nblocks", i64), ("blocks", C.POINTER(hlrc_uniform_block))]
+
+
 class hlrc_options(C.Structure):
     _fields_ = [("precision", i32), ("max_nrhs", i32), ("mixed_eps", f64), ("device", i32),
                 ("reserved", i32 * 7)]
@@ -72,7 +84,7 @@ HLRC_MR_NEVER = 1000000
 class hlrc_problem(C.Structure):
     _fields_ = [("kind", i32), ("leaf_size", i32), ("n", i64), ("refine", i32), ("uniform", i32),
                 ("seed", u64), ("eta", f64), ("eps", f64), ("ell", f64), ("nugget", f64),
-                ("nthreads", i32), ("reserved", i32 * 5)]
+                ("nthreads", i32), ("nested", i32), ("reserved", i32 * 4)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/hlrc.h
@@ -87,6 +99,8 @@ PROTOTYPES = {
     "hlrc_plan_info_h": (C.c_int, [C.POINTER(hlrc_h_desc), C.POINTER(hlrc_options), C.POINTER(hlrc_info)]),
     "hlrc_plan_info_uniform": (C.c_int, [C.POINTER(hlrc_uniform_desc), C.POINTER(hlrc_options),
                                          C.POINTER(hlrc_info)]),
+    "hlrc_upload_h2": (C.c_int, [C.POINTER(hlrc_h2_desc), C.POINTER(hlrc_options), C.POINTER(C.c_void_p)]),
+    "hlrc_plan_info_h2": (C.c_int, [C.POINTER(hlrc_h2_desc), C.POINTER(hlrc_options), C.POINTER(hlrc_info)]),
     "hlrc_mvm": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64, C.c_void_p]),
     "hlrc_mvm_host": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64]),
     "hlrc_mvm_noalloc": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -102,6 +116,7 @@ PROTOTYPES = {
     "hlrc_build": (C.c_int, [C.POINTER(hlrc_problem), C.POINTER(C.c_void_p)]),
     "hlrc_build_h_desc": (C.c_int, [C.c_void_p, C.POINTER(hlrc_h_desc)]),
     "hlrc_build_uniform_desc": (C.c_int, [C.c_void_p, C.POINTER(hlrc_uniform_desc)]),
+    "hlrc_build_h2_desc": (C.c_int, [C.c_void_p, C.POINTER(hlrc_h2_desc)]),
     "hlrc_build_points": (C.c_int, [C.c_void_p, C.POINTER(pdbl), C.POINTER(C.c_int), C.POINTER(i64)]),
     "hlrc_build_weights": (C.c_int, [C.c_void_p, C.POINTER(pdbl)]),
     "hlrc_build_perm": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(i64))]),

@@ -127,6 +127,7 @@ struct hlrc_hmat_s {
     size_t hx_elems = 0, hy_elems = 0;
     int* dev_err = nullptr;   // device error word (bounded waits that ran out)
     int64_t launches = 0;     // kernels launched by this handle
+    std::vector<const char*> names[3];   // per-pass profile names (empty: fixed names)
     // launch shapes picked by the autotuner (hlrc_set_tuning)
     int nform_warps = 8;      // warps per CTA, single-vector N-form
     int ttform_warps = 8;     // warps per CTA, single-vector tile T-form
@@ -160,8 +161,11 @@ struct DeviceGuard {
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-const char* stage_name(int kind, int nk, int idx) {
-    // names used in profiles: kind 0 = H, 1 = uniform; nk = stage kind (0 T, 1 N, 2 tile T)
+const char* stage_name(hlrc_hmat M, int nk, int idx) {
+    // names used in profiles: kind 0 = H, 1 = uniform; nk = stage kind (0 T, 1 N, 2 tile T);
+    // plans with their own names (H^2) carry them per pass
+    if (!M->names[nk].empty()) return M->names[nk][size_t(idx)];
+    const int kind = M->kind;
     static const char* ht[] = {"tform_unused"};
     static const char* hn[] = {"nform_Ut_Dx", "nform_Vt"};
     static const char* htt[] = {"ttform_VtX", "ttform_UtX", "ttform_DtX"};
@@ -429,6 +433,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     }
     h->device = dev;
     h->kind = p.kind;
+    for (int k = 0; k < 3; ++k) h->names[k] = p.names[k];
     h->precision = p.precision;
     h->nrows = p.nrows;
     h->ncols = p.ncols;
@@ -688,7 +693,7 @@ bool debug_sync() {
     } while (0)
 
 // one right-hand side: x, y are column vectors; scratch from `ws`
-hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, const double* x, double* y,
+hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* x, double* y,
                        cudaStream_t s) {
     // FP64 plans carry 16-byte FP64 descriptors, reduced-precision plans
     // 32-byte packs: each kind of kernel only ever sees its own kind
@@ -700,8 +705,9 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             const DevTPass& tp = M->t[size_t(st.idx)];
             const double* vin = bind(ws, tp.in, x, y);
             double* vout = bind(ws, tp.out, x, y);
-            const int add = tp.mode == OUT_ADD_ALPHA;
-            if (ws.profile) prof_begin(M, stage_name(M->kind, 0, st.idx), tp.alg_bytes, s);
+            const int add = tp.mode != OUT_SET;
+            const double alpha = tp.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
+            if (ws.profile) prof_begin(M, stage_name(M, 0, st.idx), tp.alg_bytes, s);
             for (int c = 0; c < 3; ++c) {
                 const int nu = tp.cls_begin[c + 1] - tp.cls_begin[c];
                 if (nu <= 0) continue;
@@ -716,14 +722,15 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             if (tp.ngroups > 0)
                 k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
             if (ws.profile) prof_end(M, s);
-            HLRC_AFTER_LAUNCH(stage_name(M->kind, 0, st.idx));
+            HLRC_AFTER_LAUNCH(stage_name(M, 0, st.idx));
         } else if (st.kind == 2) {
             const DevTTPass& tp = M->tt[size_t(st.idx)];
             if (tp.launches() == 0) continue;
             const double* vin = bind(ws, tp.in, x, y);
             double* vout = bind(ws, tp.out, x, y);
-            const int add = tp.mode == OUT_ADD_ALPHA;
-            if (ws.profile) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
+            const int add = tp.mode != OUT_SET;
+            const double alpha = tp.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
+            if (ws.profile) prof_begin(M, stage_name(M, 2, st.idx), tp.alg_bytes, s);
             auto ttform = [&](auto wc) {
                 constexpr int TW = decltype(wc)::value;
                 if (f64plan && tp.nsegs[FMT_F64] > 0)
@@ -762,15 +769,16 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
                 k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
                 if (ws.profile) prof_end(M, s);
             }
-            HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));
+            HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
         } else {
             const DevNPass& np = M->n[size_t(st.idx)];
             if (np.launches() == 0) continue;
-            if (ws.profile) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
+            if (ws.profile) prof_begin(M, stage_name(M, 1, st.idx), np.alg_bytes, s);
             const double* vx = bind(ws, np.vx, x, y);
             const double* vt = bind(ws, np.vt, x, y);
             double* vo = bind(ws, np.out, x, y);
-            const int add = np.mode == OUT_ADD_ALPHA;
+            const int add = np.mode != OUT_SET;
+            const double alpha = np.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
             auto nform = [&](auto wc) {
                 constexpr int NW = decltype(wc)::value;
                 if (f64plan && np.nsegs[FMT_F64] > 0)
@@ -794,7 +802,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha, int op, c
             if (M->nform_warps == 4) nform(Warps<4>{});
             else nform(Warps<8>{});
             if (ws.profile) prof_end(M, s);
-            HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
+            HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
         }
     }
     const cudaError_t e = cudaGetLastError();
@@ -814,7 +822,7 @@ bool multi_rhs_ok(hlrc_hmat M, int op, int nrhs) {
 
 // y := y + alpha op(M) X for nrhs column vectors, MR_RB at a time: the matrix
 // is streamed once per block instead of once per vector.
-hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_t ldx, double* Y, int64_t ldy,
+hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int64_t ldx, double* Y, int64_t ldy,
                       int nrhs, cudaStream_t s) {
     const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
     for (int r0 = 0; r0 < nrhs; r0 += MR_RB) {
@@ -842,9 +850,10 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
         for (const Stage& st : M->stages[op]) {
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
-                const int add = tp.mode == OUT_ADD_ALPHA;
+                const int add = tp.mode != OUT_SET;
+                const double alpha = tp.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
                 const OutMap om = omap(tp.out);
-                if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 2, st.idx), tp.alg_bytes, s);
+                if (ws_profile(M)) prof_begin(M, stage_name(M, 2, st.idx), tp.alg_bytes, s);
                 constexpr int TW = DMMA_WARPS;
                 if (M->precision == HLRC_PREC_F64) {
                     if (tp.nsegs[FMT_F64] > 0)
@@ -883,12 +892,13 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                     }
                     if (ws_profile(M)) prof_end(M, s);
                 }
-                HLRC_AFTER_LAUNCH(stage_name(M->kind, 2, st.idx));
+                HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
             } else if (st.kind == 1) {
                 const DevNPass& np = M->n[size_t(st.idx)];
                 if (np.launches() == 0) continue;
-                if (ws_profile(M)) prof_begin(M, stage_name(M->kind, 1, st.idx), np.alg_bytes, s);
-                const int add = np.mode == OUT_ADD_ALPHA;
+                if (ws_profile(M)) prof_begin(M, stage_name(M, 1, st.idx), np.alg_bytes, s);
+                const int add = np.mode != OUT_SET;
+                const double alpha = np.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
                 const OutMap om = omap(np.out);
                 constexpr int NW = DMMA_WARPS;
                 const bool f64plan = M->precision == HLRC_PREC_F64;
@@ -906,7 +916,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha, int op, const double* X, int64_
                     k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.mseg[FMT_BF16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                 if (ws_profile(M)) prof_end(M, s);
-                HLRC_AFTER_LAUNCH(stage_name(M->kind, 1, st.idx));
+                HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
             }
         }
     }
@@ -1001,6 +1011,30 @@ extern "C" hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_opti
     if (opts) o = *opts; else hlrc_default_options(&o);
     Plan p;
     hlrc_status st = plan_h(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    fill_info(p, arena_layout(p), *info);
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_upload_h2(const hlrc_h2_desc* desc, const hlrc_options* opts, hlrc_hmat* out) {
+    clear_error();
+    if (!desc || !out) return fail(HLRC_ERR_ARG, "hlrc_upload_h2: null argument");
+    *out = nullptr;
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_h2(*desc, o, p);
+    if (st != HLRC_OK) return st;
+    return upload_plan(p, o, out);
+}
+
+extern "C" hlrc_status hlrc_plan_info_h2(const hlrc_h2_desc* desc, const hlrc_options* opts, hlrc_info* info) {
+    clear_error();
+    if (!desc || !info) return fail(HLRC_ERR_ARG, "hlrc_plan_info_h2: null argument");
+    hlrc_options o;
+    if (opts) o = *opts; else hlrc_default_options(&o);
+    Plan p;
+    hlrc_status st = plan_h2(*desc, o, p);
     if (st != HLRC_OK) return st;
     fill_info(p, arena_layout(p), *info);
     return HLRC_OK;

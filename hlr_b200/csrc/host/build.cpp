@@ -388,6 +388,16 @@ struct Basis {
     std::vector<double> sv;
 };
 
+// Node of a nested cluster basis: an explicit basis at the leaves, and the
+// transfer matrix to the parent's basis everywhere but at the root
+// (matrix/nested_cluster_basis.hh).
+struct NBasis {
+    int64_t ofs = 0, size = 0;
+    int rank = 0;
+    Mat V;   // leaves: size x rank
+    Mat E;   // non-root: rank x parent rank
+};
+
 struct UniBlock {
     int leaf = 0;      // index into leaves
     Mat S;             // coupling k_row x k_col
@@ -405,6 +415,12 @@ struct HBuild {
     std::vector<Mat> coupling;                     // per leaf (empty for dense)
     std::vector<hlrc_basis> desc_rowb, desc_colb;
     std::vector<hlrc_uniform_block> desc_ublocks;
+    // H^2 (nested bases)
+    bool nested = false;
+    std::vector<NBasis> rowh2, colh2;              // indexed by cluster id
+    std::vector<Mat> h2coupling;                   // per leaf (empty for dense)
+    std::vector<hlrc_h2_cluster> desc_rowh2, desc_colh2;
+    std::vector<hlrc_uniform_block> desc_h2blocks;
     double seconds = 0;
     int max_rank = 0;
     int64_t bytes = 0;
@@ -497,6 +513,207 @@ static void build_uniform(HBuild& B, double eps) {
     }
 }
 
+
+// Nested (H^2) cluster bases from the admissible leaves, bottom-up.  The
+// basis of cluster t must span the rows of t of every admissible block of t
+// and of its ancestors (the total cluster basis), weighted by the other
+// factor: a block b = U_b V_b^T contributes U_b|_t R_b^T with V_b = Q_b R_b.
+//   leaf t:   V_t = column_basis([U_b|_t R_b^T]_b)                  (size x k_t)
+//   parent t: Q_t = column_basis([P_t1[b] R_b^T ; P_t2[b] R_b^T]_b) and
+//             E_ti = rows of Q_t for son i, so V_t = [V_t1 E_t1; V_t2 E_t2]
+// where P_t[b] = V_t^T U_b|_t is carried upwards as P_t = sum_i E_ti^T P_ti.
+// The column bases are the same with the roles of U_b and V_b exchanged.
+// Couplings: S_b = P_rc[b] (P'_cc[b])^T, the projections at the block's own
+// clusters.
+static void build_nested(HBuild& B, double eps, bool row, std::vector<NBasis>& nb, std::vector<std::vector<Mat>>& own) {
+    const auto& ct = B.ct;
+    const int nc = int(ct.cl.size());
+    std::vector<int> parent(static_cast<size_t>(nc), -1);
+    for (int t = 0; t < nc; ++t)
+        for (int i = 0; i < 2; ++i)
+            if (ct.cl[t].son[i] >= 0) parent[size_t(ct.cl[t].son[i])] = t;
+    std::vector<std::vector<int>> lst(static_cast<size_t>(nc));   // admissible leaves by own cluster
+    for (int i = 0; i < int(B.leaves.size()); ++i) {
+        const Leaf& l = B.leaves[i];
+        if (l.kind == HLRC_LEAF_LOWRANK && l.rank > 0) lst[size_t(row ? l.rc : l.cc)].push_back(i);
+    }
+    // R factors of the other factor, per leaf
+    std::vector<Mat> R(B.leaves.size());
+    #pragma omp parallel for schedule(dynamic, 8)
+    for (int i = 0; i < int(B.leaves.size()); ++i) {
+        const Leaf& l = B.leaves[i];
+        if (l.kind != HLRC_LEAF_LOWRANK || l.rank == 0) continue;
+        Mat O(row ? l.ncols : l.nrows, l.rank);
+        std::memcpy(O.a.data(), (row ? l.V : l.U).data(), O.a.size() * sizeof(double));
+        qr(O, R[size_t(i)]);
+    }
+    // total lists: own leaves, then the ancestors'
+    std::vector<std::vector<int>> tot(static_cast<size_t>(nc));
+    for (int t = 0; t < nc; ++t) {
+        for (int a = t; a >= 0; a = parent[size_t(a)]) tot[size_t(t)].insert(tot[size_t(t)].end(), lst[size_t(a)].begin(), lst[size_t(a)].end());
+    }
+    int maxlev = 0;
+    for (const Cluster& c : ct.cl) maxlev = std::max(maxlev, c.level);
+    nb.assign(size_t(nc), NBasis{});
+    own.assign(size_t(nc), {});
+    std::vector<std::vector<Mat>> P(static_cast<size_t>(nc));   // P[t][j] for leaf tot[t][j]
+    for (int lev = maxlev; lev >= 0; --lev) {
+        std::vector<int> cls;
+        for (int t = 0; t < nc; ++t)
+            if (ct.cl[t].level == lev) cls.push_back(t);
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (int ci = 0; ci < int(cls.size()); ++ci) {
+            const int t = cls[size_t(ci)];
+            const Cluster& c = ct.cl[t];
+            NBasis& bs = nb[size_t(t)];
+            bs.ofs = c.ofs;
+            bs.size = c.size;
+            const auto& L = tot[size_t(t)];
+            int64_t cols = 0;
+            for (int i : L) cols += B.leaves[size_t(i)].rank;
+            // the rows of U_b in t (row side) or of V_b (column side)
+            auto factor_rows = [&](int i) {
+                const Leaf& l = B.leaves[size_t(i)];
+                const int64_t m = row ? l.nrows : l.ncols, o = c.ofs - (row ? l.row0 : l.col0);
+                const std::vector<double>& F = row ? l.U : l.V;
+                Mat A(c.size, l.rank);
+                for (int64_t j = 0; j < l.rank; ++j)
+                    std::memcpy(A.col(j), F.data() + j * m + o, size_t(c.size) * sizeof(double));
+                return A;
+            };
+            std::vector<double> sv;
+            if (c.leaf()) {
+                Mat Z(c.size, cols);
+                int64_t pos = 0;
+                for (int i : L) {
+                    const Mat AR = prod_nt(factor_rows(i), R[size_t(i)]);
+                    std::memcpy(Z.col(pos), AR.a.data(), AR.a.size() * sizeof(double));
+                    pos += AR.n;
+                }
+                bs.V = cols > 0 ? column_basis(Z, eps, sv) : Mat(c.size, 0);
+                bs.rank = int(bs.V.n);
+                P[size_t(t)].resize(L.size());
+                for (size_t j = 0; j < L.size(); ++j) P[size_t(t)][j] = prod_tn(bs.V, factor_rows(L[j]));
+            } else {
+                const int s0 = c.son[0], s1 = c.son[1];
+                const int k0 = s0 >= 0 ? nb[size_t(s0)].rank : 0, k1 = s1 >= 0 ? nb[size_t(s1)].rank : 0;
+                // son j's list starts with its own leaves; t's list is its tail
+                auto son_proj = [&](int s, size_t j) -> const Mat& {
+                    const size_t off = tot[size_t(s)].size() - L.size();
+                    return P[size_t(s)][off + j];
+                };
+                Mat Z(k0 + k1, cols);
+                int64_t pos = 0;
+                for (size_t j = 0; j < L.size(); ++j) {
+                    const Mat& Rb = R[size_t(L[j])];
+                    if (k0 > 0) {
+                        const Mat A = prod_nt(son_proj(s0, j), Rb);
+                        for (int64_t q = 0; q < A.n; ++q)
+                            for (int64_t r = 0; r < k0; ++r) Z(r, pos + q) = A(r, q);
+                    }
+                    if (k1 > 0) {
+                        const Mat A = prod_nt(son_proj(s1, j), Rb);
+                        for (int64_t q = 0; q < A.n; ++q)
+                            for (int64_t r = 0; r < k1; ++r) Z(k0 + r, pos + q) = A(r, q);
+                    }
+                    pos += Rb.n;
+                }
+                const Mat Q = (cols > 0 && k0 + k1 > 0) ? column_basis(Z, eps, sv) : Mat(k0 + k1, 0);
+                bs.rank = int(Q.n);
+                for (int si = 0; si < 2; ++si) {
+                    const int s = c.son[si];
+                    if (s < 0) continue;
+                    const int ks = si == 0 ? k0 : k1, r0 = si == 0 ? 0 : k0;
+                    Mat E(ks, Q.n);
+                    for (int64_t q = 0; q < Q.n; ++q)
+                        for (int64_t r = 0; r < ks; ++r) E(r, q) = Q(r0 + r, q);
+                    nb[size_t(s)].E = std::move(E);
+                }
+                P[size_t(t)].resize(L.size());
+                for (size_t j = 0; j < L.size(); ++j) {
+                    Mat Pj(bs.rank, B.leaves[size_t(L[j])].rank);
+                    for (int si = 0; si < 2; ++si) {
+                        const int s = c.son[si];
+                        if (s < 0 || nb[size_t(s)].rank == 0) continue;
+                        const Mat A = prod_tn(nb[size_t(s)].E, son_proj(s, j));
+                        for (size_t e = 0; e < A.a.size(); ++e) Pj.a[e] += A.a[e];
+                    }
+                    P[size_t(t)][j] = std::move(Pj);
+                }
+            }
+        }
+        // a cluster's own blocks keep their projections (couplings); the
+        // rest of the sons' projections is no longer needed
+        for (int t : cls) {
+            own[size_t(t)].assign(P[size_t(t)].begin(), P[size_t(t)].begin() + long(lst[size_t(t)].size()));
+            for (int si = 0; si < 2; ++si)
+                if (ct.cl[t].son[si] >= 0) std::vector<Mat>().swap(P[size_t(ct.cl[t].son[si])]);
+        }
+    }
+}
+
+static void build_h2(HBuild& B, double eps) {
+    const auto& ct = B.ct;
+    const int nc = int(ct.cl.size());
+    std::vector<std::vector<Mat>> ownr, ownc;
+    build_nested(B, eps, true, B.rowh2, ownr);
+    build_nested(B, eps, false, B.colh2, ownc);
+    // couplings S_b = (V_t^T U_b)(W_s^T V_b)^T; a leaf's position in its
+    // cluster's own list is its rank among that cluster's admissible leaves
+    std::vector<int> posr(B.leaves.size(), -1), posc(B.leaves.size(), -1);
+    std::vector<int> cntr(static_cast<size_t>(nc), 0), cntc(static_cast<size_t>(nc), 0);
+    for (size_t i = 0; i < B.leaves.size(); ++i) {
+        const Leaf& l = B.leaves[i];
+        if (l.kind != HLRC_LEAF_LOWRANK || l.rank == 0) continue;
+        posr[i] = cntr[size_t(l.rc)]++;
+        posc[i] = cntc[size_t(l.cc)]++;
+    }
+    B.h2coupling.assign(B.leaves.size(), Mat());
+    for (size_t i = 0; i < B.leaves.size(); ++i) {
+        const Leaf& l = B.leaves[i];
+        if (l.kind != HLRC_LEAF_LOWRANK) continue;
+        if (l.rank == 0) { B.h2coupling[i] = Mat(B.rowh2[size_t(l.rc)].rank, B.colh2[size_t(l.cc)].rank); continue; }
+        B.h2coupling[i] = prod_nt(ownr[size_t(l.rc)][size_t(posr[i])], ownc[size_t(l.cc)][size_t(posc[i])]);
+    }
+    std::vector<int> parent(static_cast<size_t>(nc), -1);
+    for (int t = 0; t < nc; ++t)
+        for (int j = 0; j < 2; ++j)
+            if (ct.cl[t].son[j] >= 0) parent[size_t(ct.cl[t].son[j])] = t;
+    for (int side = 0; side < 2; ++side) {
+        const std::vector<NBasis>& nbv = side == 0 ? B.rowh2 : B.colh2;
+        std::vector<hlrc_h2_cluster>& out = side == 0 ? B.desc_rowh2 : B.desc_colh2;
+        out.assign(size_t(nc), hlrc_h2_cluster{});
+        for (int t = 0; t < nc; ++t) {
+            const NBasis& b = nbv[size_t(t)];
+            hlrc_h2_cluster& d = out[size_t(t)];
+            std::memset(&d, 0, sizeof(d));
+            d.ofs = b.ofs; d.size = b.size;
+            d.son[0] = ct.cl[t].son[0]; d.son[1] = ct.cl[t].son[1];
+            d.parent = parent[size_t(t)];
+            d.rank = b.rank;
+            d.V = b.V.a.empty() ? nullptr : b.V.a.data();
+            d.ldv = std::max<int64_t>(1, b.size);
+            d.E = b.E.a.empty() ? nullptr : b.E.a.data();
+            d.lde = std::max<int64_t>(1, b.E.m);
+        }
+    }
+    B.desc_h2blocks.resize(B.leaves.size());
+    for (size_t i = 0; i < B.leaves.size(); ++i) {
+        const Leaf& l = B.leaves[i];
+        hlrc_uniform_block& d = B.desc_h2blocks[i];
+        std::memset(&d, 0, sizeof(d));
+        d.row0 = l.row0; d.nrows = l.nrows; d.col0 = l.col0; d.ncols = l.ncols;
+        d.kind = l.kind;
+        if (l.kind == HLRC_LEAF_LOWRANK) {
+            d.row_basis = l.rc; d.col_basis = l.cc;
+            d.S = B.h2coupling[i].a.empty() ? nullptr : B.h2coupling[i].a.data();
+            d.lds = std::max<int64_t>(1, B.h2coupling[i].m);
+        } else {
+            d.D = l.D.data(); d.ldd = l.nrows;
+        }
+    }
+}
+
 }  // namespace hlrc
 
 using namespace hlrc;
@@ -583,6 +800,11 @@ extern "C" hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out) {
         omp_set_num_threads(nthreads);
         build_uniform(B, eps);
     }
+    if (prob->nested) {
+        B.nested = true;
+        omp_set_num_threads(nthreads);
+        build_h2(B, eps);
+    }
     B.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = h.release();
     return HLRC_OK;
@@ -608,6 +830,20 @@ extern "C" hlrc_status hlrc_build_uniform_desc(hlrc_hbuild B, hlrc_uniform_desc*
     out->col_bases = B->b.desc_colb.data();
     out->nblocks = int64_t(B->b.desc_ublocks.size());
     out->blocks = B->b.desc_ublocks.data();
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_build_h2_desc(hlrc_hbuild B, hlrc_h2_desc* out) {
+    if (!B || !out) return fail(HLRC_ERR_ARG, "hlrc_build_h2_desc: null argument");
+    if (!B->b.nested) return fail(HLRC_ERR_ARG, "hlrc_build_h2_desc: problem was built without nested=1");
+    out->nrows = B->b.P.n;
+    out->ncols = B->b.P.n;
+    out->nrow_clusters = int64_t(B->b.desc_rowh2.size());
+    out->row_clusters = B->b.desc_rowh2.data();
+    out->ncol_clusters = int64_t(B->b.desc_colh2.size());
+    out->col_clusters = B->b.desc_colh2.data();
+    out->nblocks = int64_t(B->b.desc_h2blocks.size());
+    out->blocks = B->b.desc_h2blocks.data();
     return HLRC_OK;
 }
 

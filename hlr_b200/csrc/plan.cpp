@@ -260,7 +260,7 @@ struct TBuilder {
     // one output of `ncols` columns at `out`, fed by `slabs`
     void add(uint32_t out, int64_t ncols, const std::vector<TSlab>& slabs) {
         for (const TSlab& s : slabs) P.alg_bytes += int64_t(sizeof(double)) * s.rows * (ncols + 1);
-        P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
+        P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode != OUT_SET ? 2 : 1);
         for (int64_t c0 = 0; c0 < ncols; c0 += TCOLS) {
             const int nc = int(std::min<int64_t>(TCOLS, ncols - c0));
             std::vector<std::pair<uint32_t, uint32_t>> runs;
@@ -371,7 +371,7 @@ struct NBuilder {
             tmp[f].push_back({by, NSeg{s, e, out, uint16_t(rows_), uint16_t(pad_fmt(rows_, f))}});
             s = e;
         }
-        P.alg_bytes += alg + int64_t(sizeof(double)) * rows_ * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
+        P.alg_bytes += alg + int64_t(sizeof(double)) * rows_ * (P.mode != OUT_SET ? 2 : 1);
     }
     void finish() {
         for (int f = 0; f < NFMT; ++f) {
@@ -410,7 +410,7 @@ struct TTBuilder {
         } else {
             pbase[id] = -1;
         }
-        P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode == OUT_ADD_ALPHA ? 2 : 1);
+        P.alg_bytes += int64_t(sizeof(double)) * ncols * (P.mode != OUT_SET ? 2 : 1);
     }
     void begin(int64_t v_off, int64_t tile_rows) {
         cb = uint32_t(P.chunks.size());
@@ -1164,6 +1164,429 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
     }
     p.matrix_bytes = int64_t(mbytes + cbbytes + rbbytes);
     p.algorithmic_bytes = int64_t(cbbytes + 8.0 * d.ncols + mbytes + rbbytes + 8.0 * d.nrows);
+    p.flops = int64_t(flops);
+    return HLRC_OK;
+}
+
+// ------------------------------------------------------------------- H^2
+// The product of an H^2 matrix as a sequence of the same N-form and tile
+// T-form passes (arith/h2.hh:21-40, arith/detail/h2.hh:238-330).  op N:
+//   1. x^_s = W_s^T x for the leaf column clusters             (tile T-form)
+//   2. per level of the column tree, deepest first:
+//      x^_p = sum over the sons s of F_s^T x^_s                 (N-form over
+//      the transposed transfer matrices, one output per parent)
+//   3. y^_t = sum_s S_ts x^_s for every row cluster (zero if none)  (N-form)
+//   4. per level of the row tree, root first:
+//      y^_c += E_c y^_p for the sons c of the level's clusters  (N-form, add)
+//   5. y += alpha (V_t y^_t over the leaf row clusters + D x)    (N-form)
+// op C exchanges the trees: forward with the row bases, the couplings
+// transposed (unit T-form), backward down the column tree, leaf column
+// bases, and the near field transposed.
+hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
+    if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0 || d.nrow_clusters <= 0 || d.ncol_clusters <= 0)
+        return fail(HLRC_ERR_SHAPE, "H2: bad sizes or empty cluster tree");
+    if ((d.nblocks > 0 && !d.blocks) || !d.row_clusters || !d.col_clusters)
+        return fail(HLRC_ERR_ARG, "H2: NULL array in descriptor");
+    if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
+        return fail(HLRC_ERR_SHAPE, "matrix dimension exceeds 2^31-1");
+    if (o.precision != HLRC_PREC_F64)
+        return fail(HLRC_ERR_ARG, "precision %d not supported for H2 (FP64 only)", o.precision);
+    p = Plan();
+    p.kind = 2;
+    p.precision = o.precision;
+    p.nrows = d.nrows;
+    p.ncols = d.ncols;
+    const int64_t nb = d.nblocks;
+    // ---- cluster trees: index sets, parent/son links, levels, data
+    struct Tree {
+        const hlrc_h2_cluster* c;
+        int64_t n;
+        std::vector<int> level;
+        std::vector<int64_t> off;   // coefficient offsets (-1: rank 0)
+        int64_t ncoef = 0;
+        int maxlev = 0;
+        bool leaf(int64_t t) const { return c[t].son[0] < 0 && c[t].son[1] < 0; }
+    };
+    auto check_tree = [&](const hlrc_h2_cluster* cl, int64_t n, int64_t dim, Tree& T, const char* side) -> hlrc_status {
+        T.c = cl; T.n = n;
+        T.level.assign(size_t(n), -1);
+        T.off.assign(size_t(n), -1);
+        if (cl[0].parent != -1 || cl[0].ofs != 0 || cl[0].size != dim)
+            return fail(HLRC_ERR_SHAPE, "H2 %s tree: cluster 0 must be the root covering all indices", side);
+        std::vector<int64_t> stack{0};
+        T.level[0] = 0;
+        int64_t seen = 0;
+        while (!stack.empty()) {
+            const int64_t t = stack.back();
+            stack.pop_back();
+            ++seen;
+            const hlrc_h2_cluster& c = cl[t];
+            if (c.ofs < 0 || c.size < 0 || c.ofs + c.size > dim || c.rank < 0 || c.rank > 65535)
+                return fail(HLRC_ERR_SHAPE, "H2 %s cluster %lld: bad index set or rank", side, (long long)t);
+            const bool lf = c.son[0] < 0 && c.son[1] < 0;
+            if (lf && c.rank > 0 && c.size > 0 && (!c.V || c.ldv < c.size))
+                return fail(HLRC_ERR_ARG, "H2 %s cluster %lld: leaf basis missing", side, (long long)t);
+            if (t != 0) {
+                const int64_t pr = c.parent;
+                if (c.rank > 0 && cl[pr].rank > 0 && (!c.E || c.lde < c.rank))
+                    return fail(HLRC_ERR_ARG, "H2 %s cluster %lld: transfer matrix missing", side, (long long)t);
+            }
+            int64_t covered = 0;
+            for (int i = 0; i < 2; ++i) {
+                const int64_t s = c.son[i];
+                if (s < 0) continue;
+                if (s >= n || cl[s].parent != t || T.level[size_t(s)] >= 0)
+                    return fail(HLRC_ERR_SHAPE, "H2 %s cluster %lld: inconsistent son %lld", side, (long long)t, (long long)s);
+                if (cl[s].ofs != c.ofs + covered)
+                    return fail(HLRC_ERR_SHAPE, "H2 %s cluster %lld: sons do not partition it", side, (long long)t);
+                covered += cl[s].size;
+                T.level[size_t(s)] = T.level[size_t(t)] + 1;
+                T.maxlev = std::max(T.maxlev, T.level[size_t(s)]);
+                stack.push_back(s);
+            }
+            if (!lf && covered != c.size)
+                return fail(HLRC_ERR_SHAPE, "H2 %s cluster %lld: sons do not partition it", side, (long long)t);
+            if (!lf && c.rank > 0 && !((c.son[0] >= 0 && cl[c.son[0]].rank > 0) || (c.son[1] >= 0 && cl[c.son[1]].rank > 0)))
+                return fail(HLRC_ERR_SHAPE, "H2 %s cluster %lld: positive rank but no son of positive rank", side,
+                            (long long)t);
+        }
+        if (seen != n) return fail(HLRC_ERR_SHAPE, "H2 %s tree: %lld clusters unreachable from the root", side,
+                                    (long long)(n - seen));
+        for (int64_t t = 0; t < n; ++t)
+            if (cl[t].rank > 0) { T.off[size_t(t)] = T.ncoef; T.ncoef += cl[t].rank; }
+        return HLRC_OK;
+    };
+    Tree R, Cc;
+    if (hlrc_status st = check_tree(d.row_clusters, d.nrow_clusters, d.nrows, R, "row"); st != HLRC_OK) return st;
+    if (hlrc_status st = check_tree(d.col_clusters, d.ncol_clusters, d.ncols, Cc, "column"); st != HLRC_OK) return st;
+    if (std::max(R.ncoef, Cc.ncoef) >= (int64_t(1) << 31)) return fail(HLRC_ERR_SHAPE, "sum of basis ranks exceeds 2^31-1");
+    // ---- blocks
+    double area = 0;
+    std::vector<int64_t> rcuts, ccuts;
+    for (int64_t i = 0; i < nb; ++i) {
+        const hlrc_uniform_block& b = d.blocks[i];
+        if (b.nrows < 0 || b.ncols < 0 || b.row0 < 0 || b.col0 < 0 || b.row0 + b.nrows > d.nrows ||
+            b.col0 + b.ncols > d.ncols)
+            return fail(HLRC_ERR_SHAPE, "block %lld: index set outside the matrix", (long long)i);
+        if (b.kind == HLRC_LEAF_DENSE) {
+            if (b.nrows * b.ncols > 0 && (!b.D || b.ldd < b.nrows))
+                return fail(HLRC_ERR_ARG, "block %lld: dense data missing", (long long)i);
+        } else if (b.kind == HLRC_LEAF_LOWRANK) {
+            if (b.row_basis < 0 || b.row_basis >= R.n || b.col_basis < 0 || b.col_basis >= Cc.n)
+                return fail(HLRC_ERR_ARG, "block %lld: cluster index out of range", (long long)i);
+            const hlrc_h2_cluster& rc = R.c[b.row_basis];
+            const hlrc_h2_cluster& cc = Cc.c[b.col_basis];
+            if (rc.ofs != b.row0 || rc.size != b.nrows || cc.ofs != b.col0 || cc.size != b.ncols)
+                return fail(HLRC_ERR_SHAPE, "block %lld: cluster index sets differ from the block's", (long long)i);
+            if (rc.rank > 0 && cc.rank > 0 && (!b.S || b.lds < rc.rank))
+                return fail(HLRC_ERR_ARG, "block %lld: coupling missing or lds < row rank", (long long)i);
+        } else {
+            return fail(HLRC_ERR_ARG, "block %lld: unknown kind", (long long)i);
+        }
+        area += double(b.nrows) * double(b.ncols);
+        rcuts.push_back(b.row0); rcuts.push_back(b.row0 + b.nrows);
+        ccuts.push_back(b.col0); ccuts.push_back(b.col0 + b.ncols);
+    }
+    if (area != double(d.nrows) * double(d.ncols))
+        return fail(HLRC_ERR_SHAPE, "leaf blocks cover %.0f entries, matrix has %.0f", area,
+                    double(d.nrows) * double(d.ncols));
+    for (int64_t t = 0; t < R.n; ++t)
+        if (R.leaf(t)) { rcuts.push_back(R.c[t].ofs); rcuts.push_back(R.c[t].ofs + R.c[t].size); }
+    for (int64_t t = 0; t < Cc.n; ++t)
+        if (Cc.leaf(t)) { ccuts.push_back(Cc.c[t].ofs); ccuts.push_back(Cc.c[t].ofs + Cc.c[t].size); }
+    const Tiles tr = make_tiles(d.nrows, rcuts), tc = make_tiles(d.ncols, ccuts);
+    p.n_row_tiles = tr.n();
+    p.n_col_tiles = tc.n();
+    p.n_t = p.n_t2 = std::max(R.ncoef, Cc.ncoef);
+
+    // tiles -> leaf bases / dense blocks; clusters -> low-rank blocks
+    std::vector<std::vector<int64_t>> rbl(static_cast<size_t>(tr.n())), cbl(static_cast<size_t>(tc.n())),
+        rdl(static_cast<size_t>(tr.n()));
+    for (int64_t t = 0; t < R.n; ++t)
+        if (R.leaf(t) && R.c[t].rank > 0)
+            for (int64_t q = tr.first(R.c[t].ofs); q < tr.first(R.c[t].ofs + R.c[t].size); ++q) rbl[size_t(q)].push_back(t);
+    for (int64_t t = 0; t < Cc.n; ++t)
+        if (Cc.leaf(t) && Cc.c[t].rank > 0)
+            for (int64_t q = tc.first(Cc.c[t].ofs); q < tc.first(Cc.c[t].ofs + Cc.c[t].size); ++q) cbl[size_t(q)].push_back(t);
+    std::vector<std::vector<int64_t>> lr_by_row(static_cast<size_t>(R.n)), lr_by_col(static_cast<size_t>(Cc.n));
+    for (int64_t i = 0; i < nb; ++i) {
+        const hlrc_uniform_block& b = d.blocks[i];
+        if (b.nrows == 0 || b.ncols == 0) continue;
+        if (b.kind == HLRC_LEAF_DENSE) {
+            for (int64_t q = tr.first(b.row0); q < tr.first(b.row0 + b.nrows); ++q) rdl[size_t(q)].push_back(i);
+        } else if (R.c[b.row_basis].rank > 0 && Cc.c[b.col_basis].rank > 0) {
+            lr_by_row[size_t(b.row_basis)].push_back(i);
+            lr_by_col[size_t(b.col_basis)].push_back(i);
+        }
+    }
+
+    // ---- storage (FP64): leaf bases by tile, dense slabs, couplings and
+    // transfer matrices in pieces of at most TILE rows
+    Store st;
+    std::vector<std::vector<int>> sRB(static_cast<size_t>(R.n)), sCB(static_cast<size_t>(Cc.n)),
+        sER(static_cast<size_t>(R.n)), sEC(static_cast<size_t>(Cc.n)), sD(static_cast<size_t>(nb)),
+        sS(static_cast<size_t>(nb));
+    for (int64_t q = 0; q < tr.n(); ++q) {
+        for (int64_t t : rbl[size_t(q)]) {
+            const hlrc_h2_cluster& c = R.c[t];
+            sRB[size_t(t)].push_back(st.alloc(c.V, c.ldv, tr.lo(q) - c.ofs, tr.size(q), c.rank, nullptr, FMT_F64));
+        }
+        for (int64_t i : rdl[size_t(q)]) {
+            const hlrc_uniform_block& b = d.blocks[i];
+            const std::vector<int64_t> cuts = inner_cuts(tc, b.col0, b.ncols);
+            sD[size_t(i)].push_back(st.alloc(b.D, b.ldd, tr.lo(q) - b.row0, tr.size(q), b.ncols, nullptr, FMT_F64, &cuts));
+        }
+    }
+    for (int64_t q = 0; q < tc.n(); ++q)
+        for (int64_t t : cbl[size_t(q)]) {
+            const hlrc_h2_cluster& c = Cc.c[t];
+            sCB[size_t(t)].push_back(st.alloc(c.V, c.ldv, tc.lo(q) - c.ofs, tc.size(q), c.rank, nullptr, FMT_F64));
+        }
+    auto pieces = [&](const double* A, int64_t lda, int64_t rows, int64_t cols, std::vector<int>& out) {
+        for (int64_t r0 = 0; r0 < rows; r0 += TILE)
+            out.push_back(st.alloc(A, lda, r0, std::min<int64_t>(TILE, rows - r0), cols, nullptr, FMT_F64));
+    };
+    for (int64_t i = 0; i < nb; ++i) {
+        const hlrc_uniform_block& b = d.blocks[i];
+        if (b.kind != HLRC_LEAF_LOWRANK || b.nrows == 0 || b.ncols == 0) continue;
+        const int64_t kr = R.c[b.row_basis].rank, kc = Cc.c[b.col_basis].rank;
+        if (kr > 0 && kc > 0) pieces(b.S, b.lds, kr, kc, sS[size_t(i)]);
+    }
+    auto transfer_ok = [](const Tree& T, int64_t t) {
+        return t != 0 && T.c[t].rank > 0 && T.c[T.c[t].parent].rank > 0;
+    };
+    for (int64_t t = 0; t < R.n; ++t)
+        if (transfer_ok(R, t)) pieces(R.c[t].E, R.c[t].lde, R.c[t].rank, R.c[R.c[t].parent].rank, sER[size_t(t)]);
+    for (int64_t t = 0; t < Cc.n; ++t)
+        if (transfer_ok(Cc, t)) pieces(Cc.c[t].E, Cc.c[t].lde, Cc.c[t].rank, Cc.c[Cc.c[t].parent].rank, sEC[size_t(t)]);
+    // the forward transform takes the transposed transfer matrices (parent
+    // rank x son rank), so that a parent's coefficients are one N-form
+    // output over both sons, with no partial sums
+    std::vector<std::vector<double>> ET(static_cast<size_t>(R.n + Cc.n));
+    std::vector<std::vector<int>> sETR(static_cast<size_t>(R.n)), sETC(static_cast<size_t>(Cc.n));
+    auto transposed = [&](const hlrc_h2_cluster& c, int64_t kp, std::vector<double>& buf) {
+        buf.assign(size_t(kp * c.rank), 0.0);
+        for (int64_t j = 0; j < kp; ++j)
+            for (int64_t i = 0; i < c.rank; ++i) buf[size_t(j + i * kp)] = c.E[i + j * c.lde];
+    };
+    for (int64_t t = 0; t < R.n; ++t)
+        if (transfer_ok(R, t)) {
+            const int64_t kp = R.c[R.c[t].parent].rank;
+            transposed(R.c[t], kp, ET[size_t(t)]);
+            pieces(ET[size_t(t)].data(), kp, kp, R.c[t].rank, sETR[size_t(t)]);
+        }
+    for (int64_t t = 0; t < Cc.n; ++t)
+        if (transfer_ok(Cc, t)) {
+            const int64_t kp = Cc.c[Cc.c[t].parent].rank;
+            transposed(Cc.c[t], kp, ET[size_t(R.n + t)]);
+            pieces(ET[size_t(R.n + t)].data(), kp, kp, Cc.c[t].rank, sETC[size_t(t)]);
+        }
+    st.close_region();   // one region: allocation order (FP64 only)
+    st.fill(p.store);
+    for (int f = 0; f < NFMT; ++f) p.fmt_bytes[f] = st.unpadded[f];
+
+    // ---- pass builders
+    // forward leaf transform of a tree over its tiles: x^_s = W_s^T x
+    auto fwd_leaves = [&](TTPass& f, const Tree& T, const Tiles& tl, const std::vector<std::vector<int64_t>>& bl,
+                          const std::vector<std::vector<int>>& sB) {
+        f.in = V_X; f.out = V_T; f.mode = OUT_SET;
+        TTBuilder tb(f, st, size_t(T.n));
+        for (int64_t t = 0; t < T.n; ++t)
+            if (T.leaf(t) && T.c[t].rank > 0)
+                tb.object(size_t(t), uint32_t(T.off[size_t(t)]), T.c[t].rank,
+                          tl.first(T.c[t].ofs + T.c[t].size) - tl.first(T.c[t].ofs));
+        for (int64_t q = 0; q < tl.n(); ++q) {
+            tb.begin(tl.lo(q), tl.size(q));
+            for (int64_t t : bl[size_t(q)]) tb.slab(sB[size_t(t)][size_t(q - tl.first(T.c[t].ofs))], size_t(t), q - tl.first(T.c[t].ofs));
+            tb.end();
+        }
+        tb.finish();
+    };
+    // forward transfers into the clusters of level lev: x^_p = sum_s E_s^T x^_s,
+    // one N-form output per parent (pieces of at most TILE rows) over the
+    // transposed transfer matrices of its sons
+    auto fwd_transfer = [&](NPass& n, const Tree& T, const std::vector<std::vector<int>>& sET, int lev) -> bool {
+        n.vx = V_X; n.vt = V_T; n.out = V_T; n.mode = OUT_SET;
+        NBuilder nbld(n, st);
+        bool any = false;
+        for (int64_t t = 0; t < T.n; ++t) {
+            if (T.level[size_t(t)] != lev || T.leaf(t) || T.c[t].rank == 0) continue;
+            const int64_t kp = T.c[t].rank;
+            for (int64_t r0 = 0, piece = 0; r0 < kp; r0 += TILE, ++piece) {
+                const int64_t rows = std::min<int64_t>(TILE, kp - r0);
+                nbld.begin(rows);
+                for (int i = 0; i < 2; ++i) {
+                    const int64_t so = T.c[t].son[i];
+                    if (so >= 0 && !sET[size_t(so)].empty())
+                        nbld.slab(sET[size_t(so)][size_t(piece)], VEC_T | uint32_t(T.off[size_t(so)]));
+                }
+                nbld.end(uint32_t(T.off[size_t(t)] + r0), rows, true);
+                any = true;
+            }
+        }
+        nbld.finish();
+        return any;
+    };
+    // backward transfers into the sons of level lev: y^_c += E_c y^_p
+    auto bwd_transfer = [&](NPass& n, const Tree& T, const std::vector<std::vector<int>>& sE, int lev) -> bool {
+        n.vx = V_X; n.vt = V_T2; n.out = V_T2; n.mode = OUT_ADD;
+        NBuilder nbld(n, st);
+        bool any = false;
+        for (int64_t c = 0; c < T.n; ++c) {
+            if (T.level[size_t(c)] != lev + 1 || sE[size_t(c)].empty()) continue;
+            const int64_t pr = T.c[c].parent;
+            for (size_t pc = 0; pc < sE[size_t(c)].size(); ++pc) {
+                const int64_t r0 = int64_t(pc) * TILE, rows = std::min<int64_t>(TILE, T.c[c].rank - r0);
+                nbld.begin(rows);
+                nbld.slab(sE[size_t(c)][pc], VEC_T | uint32_t(T.off[size_t(pr)]));
+                nbld.end(uint32_t(T.off[size_t(c)] + r0), rows, false);
+                any = true;
+            }
+        }
+        nbld.finish();
+        return any;
+    };
+    // backward leaf transform (+ near field for op N): y += alpha (V_t y^_t + D x)
+    auto bwd_leaves = [&](NPass& n, const Tree& T, const Tiles& tl, const std::vector<std::vector<int64_t>>& bl,
+                          const std::vector<std::vector<int>>& sB, bool dense) {
+        n.vx = V_X; n.vt = V_T2; n.out = V_Y; n.mode = OUT_ADD_ALPHA;
+        NBuilder nbld(n, st);
+        std::vector<size_t> posD(static_cast<size_t>(nb), 0);
+        for (int64_t q = 0; q < tl.n(); ++q) {
+            nbld.begin(tl.size(q));
+            for (int64_t t : bl[size_t(q)])
+                nbld.slab(sB[size_t(t)][size_t(q - tl.first(T.c[t].ofs))], VEC_T | uint32_t(T.off[size_t(t)]));
+            if (dense)
+                for (int64_t i : rdl[size_t(q)]) nbld.slab(sD[size_t(i)][posD[size_t(i)]++], uint32_t(d.blocks[i].col0));
+            nbld.end(uint32_t(tl.lo(q)), tl.size(q), false);
+        }
+        nbld.finish();
+    };
+
+    // ---- op N
+    std::vector<Stage>& sn = p.stages[HLRC_OP_N];
+    auto add_tt = [&](const char* name) -> TTPass& {
+        p.ttpasses.emplace_back();
+        p.names[2].push_back(name);
+        return p.ttpasses.back();
+    };
+    auto add_n = [&](const char* name) -> NPass& {
+        p.npasses.emplace_back();
+        p.names[1].push_back(name);
+        return p.npasses.back();
+    };
+    // passes are appended, so stages record indices, not references
+    fwd_leaves(add_tt("h2_fwd_leaves"), Cc, tc, cbl, sCB);
+    sn.push_back({2, int(p.ttpasses.size()) - 1});
+    for (int lev = Cc.maxlev - 1; lev >= 0; --lev) {
+        if (fwd_transfer(add_n("h2_fwd_transfer"), Cc, sETC, lev)) sn.push_back({1, int(p.npasses.size()) - 1});
+        else { p.npasses.pop_back(); p.names[1].pop_back(); }
+    }
+    {   // couplings: every row cluster of positive rank is written (zero without blocks)
+        NPass& c = add_n("h2_coupling");
+        c.vx = V_X; c.vt = V_T; c.out = V_T2; c.mode = OUT_SET;
+        NBuilder nbld(c, st);
+        for (int64_t t = 0; t < R.n; ++t) {
+            if (R.c[t].rank == 0) continue;
+            const int64_t kr = R.c[t].rank;
+            for (int64_t r0 = 0, piece = 0; r0 < kr; r0 += TILE, ++piece) {
+                const int64_t rows = std::min<int64_t>(TILE, kr - r0);
+                nbld.begin(rows);
+                for (int64_t i : lr_by_row[size_t(t)])
+                    nbld.slab(sS[size_t(i)][size_t(piece)], VEC_T | uint32_t(Cc.off[size_t(d.blocks[i].col_basis)]));
+                nbld.end(uint32_t(R.off[size_t(t)] + r0), rows, true);
+            }
+        }
+        nbld.finish();
+        sn.push_back({1, int(p.npasses.size()) - 1});
+    }
+    for (int lev = 0; lev < R.maxlev; ++lev) {
+        if (bwd_transfer(add_n("h2_bwd_transfer"), R, sER, lev)) sn.push_back({1, int(p.npasses.size()) - 1});
+        else { p.npasses.pop_back(); p.names[1].pop_back(); }
+    }
+    bwd_leaves(add_n("h2_bwd_leaves_Dx"), R, tr, rbl, sRB, true);
+    sn.push_back({1, int(p.npasses.size()) - 1});
+
+    // ---- op C: the trees exchanged
+    std::vector<Stage>& sc = p.stages[HLRC_OP_C];
+    fwd_leaves(add_tt("h2_fwd_leaves"), R, tr, rbl, sRB);
+    sc.push_back({2, int(p.ttpasses.size()) - 1});
+    for (int lev = R.maxlev - 1; lev >= 0; --lev) {
+        if (fwd_transfer(add_n("h2_fwd_transfer"), R, sETR, lev)) sc.push_back({1, int(p.npasses.size()) - 1});
+        else { p.npasses.pop_back(); p.names[1].pop_back(); }
+    }
+    {   // couplings transposed: y^_s = sum_t S_ts^T x^_t (unit T-form; every
+        // column cluster of positive rank is written)
+        p.tpasses.emplace_back();
+        p.names[0].push_back("h2_couplingT");
+        TPass& c = p.tpasses.back();
+        c.in = V_T; c.out = V_T2; c.mode = OUT_SET;
+        TBuilder tb(c);
+        for (int64_t s = 0; s < Cc.n; ++s) {
+            if (Cc.c[s].rank == 0) continue;
+            std::vector<TSlab> sl;
+            for (int64_t i : lr_by_col[size_t(s)]) {
+                const hlrc_uniform_block& b = d.blocks[i];
+                const int64_t kr = R.c[b.row_basis].rank;
+                for (int64_t r0 = 0, piece = 0; r0 < kr; r0 += TILE, ++piece) {
+                    const int64_t rows = std::min<int64_t>(TILE, kr - r0);
+                    sl.push_back({uint64_t(st.slab_elem_off(sS[size_t(i)][size_t(piece)])),
+                                  uint32_t(R.off[size_t(b.row_basis)] + r0), uint16_t(rows), uint16_t(pad_rows(rows))});
+                }
+            }
+            tb.add(uint32_t(Cc.off[size_t(s)]), Cc.c[s].rank, sl);
+        }
+        tb.finish();
+        sc.push_back({0, int(p.tpasses.size()) - 1});
+    }
+    for (int lev = 0; lev < Cc.maxlev; ++lev) {
+        if (bwd_transfer(add_n("h2_bwd_transfer"), Cc, sEC, lev)) sc.push_back({1, int(p.npasses.size()) - 1});
+        else { p.npasses.pop_back(); p.names[1].pop_back(); }
+    }
+    bwd_leaves(add_n("h2_bwd_leaves"), Cc, tc, cbl, sCB, false);
+    sc.push_back({1, int(p.npasses.size()) - 1});
+    plan_dense_transposed(add_tt("h2_DtX"), st, tr, tc, rdl, sD, [&](int64_t i, int64_t& c0, int64_t& nc) {
+        c0 = d.blocks[i].col0;
+        nc = d.blocks[i].ncols;
+    });
+    sc.push_back({2, int(p.ttpasses.size()) - 1});
+    p.stages[HLRC_OP_T].clear();   // as uniform-H: no transposed product
+    for (const TTPass& tp : p.ttpasses)
+        if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
+
+    if (hlrc_status vs = validate_plan(p); vs != HLRC_OK) return vs;
+
+    // accounting: stored bytes (leaf bases, transfers, couplings, dense) plus
+    // the vectors, and GEMV flops (utils/flops.hh:41-42)
+    double flops = 0, mbytes = 0;
+    for (int side = 0; side < 2; ++side) {
+        const Tree& T = side == 0 ? R : Cc;
+        for (int64_t t = 0; t < T.n; ++t) {
+            const hlrc_h2_cluster& c = T.c[t];
+            if (c.rank == 0) continue;
+            if (T.leaf(t)) { flops += flops_gemv(double(c.size), c.rank); mbytes += 8.0 * c.rank * double(c.size); }
+            if (t != 0 && T.c[c.parent].rank > 0) {
+                flops += flops_gemv(c.rank, T.c[c.parent].rank);
+                mbytes += 8.0 * c.rank * T.c[c.parent].rank;
+            }
+            p.max_rank = std::max(p.max_rank, c.rank);
+        }
+    }
+    for (int64_t i = 0; i < nb; ++i) {
+        const auto& b = d.blocks[i];
+        if (b.kind == HLRC_LEAF_DENSE) {
+            ++p.n_dense;
+            flops += flops_gemv(double(b.nrows), double(b.ncols));
+            mbytes += 8.0 * double(b.nrows) * double(b.ncols);
+        } else {
+            ++p.n_lowrank;
+            const double kr = R.c[b.row_basis].rank, kc = Cc.c[b.col_basis].rank;
+            flops += flops_gemv(kr, kc);
+            mbytes += 8.0 * kr * kc;
+        }
+    }
+    p.matrix_bytes = int64_t(mbytes);
+    p.algorithmic_bytes = int64_t(mbytes + 8.0 * double(d.ncols) + 8.0 * double(d.nrows));
     p.flops = int64_t(flops);
     return HLRC_OK;
 }

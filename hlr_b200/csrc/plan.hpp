@@ -24,6 +24,7 @@ enum VecName : int {
 enum OutMode : int {
     OUT_SET = 0,        // out = s            (coefficients)
     OUT_ADD_ALPHA = 1,  // out += alpha * s   (y)
+    OUT_ADD = 2,        // out += s           (H^2: coefficients passed down the tree)
 };
 
 // A chunk of stored matrix data as the planner sees it, before it is
@@ -83,7 +84,7 @@ struct Stage {
 };
 
 struct Plan {
-    int kind = 0;                  // 0 = H, 1 = uniform-H
+    int kind = 0;                  // 0 = H, 1 = uniform-H, 2 = H^2
     int precision = HLRC_PREC_F64;
     int64_t nrows = 0, ncols = 0;
     std::vector<uint8_t> store;    // slab storage (FP64, or per-chunk formats)
@@ -97,6 +98,9 @@ struct Plan {
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;
     int32_t max_rank = 0;
     int64_t fmt_bytes[NFMT] = {};  // stored bytes per StoreFmt (accounting of mixed precision)
+    // profile names per pass (static strings), per stage kind; empty = the
+    // fixed names of kinds 0 and 1
+    std::vector<const char*> names[3];
 };
 
 // Returns HLRC_OK or an error (message recorded via fail()).  expected_area
@@ -104,5 +108,6 @@ struct Plan {
 // batch passes the sum over its members).
 hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area = -1.0);
 hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan& p);
+hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p);
 
 }  // namespace hlrc

@@ -149,6 +149,35 @@ typedef struct hlrc_uniform_desc {
     const hlrc_uniform_block*  blocks;
 } hlrc_uniform_desc;
 
+/* H^2 matrix (nested cluster bases), the structure of HLR's
+ * nested_cluster_basis (include/hlr/matrix/nested_cluster_basis.hh) and its
+ * product (include/hlr/arith/h2.hh:21-40, arith/detail/h2.hh:238-330): a
+ * cluster tree per side, an explicit basis V (size x rank) at the leaves,
+ * and for every non-root cluster the transfer matrix E (rank x rank of the
+ * parent) with V_parent = [V_son0 E_son0; V_son1 E_son1].  Blocks are
+ * hlrc_uniform_block entries whose row_basis / col_basis index the
+ * clusters; a low-rank block (t, s) is V_t S W_s^T.                          */
+typedef struct hlrc_h2_cluster {
+    int64_t       ofs, size;     /* index set                                   */
+    int32_t       son[2];        /* child clusters, -1 for none                 */
+    int32_t       parent;        /* -1 for the root                             */
+    int32_t       rank;
+    const double* V;             /* leaves: size x rank, col-major               */
+    int64_t       ldv;
+    const double* E;             /* non-root: rank x parent rank, col-major      */
+    int64_t       lde;
+} hlrc_h2_cluster;
+
+typedef struct hlrc_h2_desc {
+    int64_t                    nrows, ncols;
+    int64_t                    nrow_clusters;
+    const hlrc_h2_cluster*     row_clusters;
+    int64_t                    ncol_clusters;
+    const hlrc_h2_cluster*     col_clusters;
+    int64_t                    nblocks;
+    const hlrc_uniform_block*  blocks;
+} hlrc_h2_desc;
+
 typedef struct hlrc_options {
     int32_t precision;     /* hlrc_precision (default HLRC_PREC_F64)            */
     int32_t max_nrhs;      /* workspace sized for this many right-hand sides   */
@@ -209,6 +238,15 @@ hlrc_status hlrc_upload_h_batch(const hlrc_h_desc* descs, int count,
 hlrc_status hlrc_upload_uniform(const hlrc_uniform_desc* desc,
                                 const hlrc_options* opts, hlrc_hmat* out);
 
+/* Same for an H^2 matrix (nested cluster bases).  Replaces the H^2 product
+ * hlr::h2::mul_vec(alpha, op, M, x, y, rowcb, colcb) (arith/h2.hh:21-40):
+ * op N runs the forward transform (leaf bases, then transfer matrices level
+ * by level up the column tree), the couplings, the backward transform (level
+ * by level down the row tree, then the leaf bases) and the near field;
+ * op C the same with the roles of the trees exchanged.  op T is rejected
+ * (HLRC_ERR_UNSUPPORTED_OP), as for uniform-H.  FP64 only.                  */
+hlrc_status hlrc_upload_h2(const hlrc_h2_desc* desc, const hlrc_options* opts, hlrc_hmat* out);
+
 /* Dry run of hlrc_upload_h / hlrc_upload_uniform: validates the descriptor,
  * flattens it on the host and reports the accounting and the device
  * footprint that an upload would need, without touching a GPU.  Lets a
@@ -218,6 +256,7 @@ hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_options* opts,
                              hlrc_info* info);
 hlrc_status hlrc_plan_info_uniform(const hlrc_uniform_desc* desc,
                                    const hlrc_options* opts, hlrc_info* info);
+hlrc_status hlrc_plan_info_h2(const hlrc_h2_desc* desc, const hlrc_options* opts, hlrc_info* info);
 
 /* y := y + alpha * op(M) * x on `stream`.
  * x: ncols(op) x nrhs device array (leading dimension ldx),
@@ -337,7 +376,8 @@ typedef struct hlrc_problem {
     double   ell;          /* EXP3D correlation length                            */
     double   nugget;       /* EXP3D diagonal nugget                               */
     int32_t  nthreads;     /* host threads for the build (0 = all)                */
-    int32_t  reserved[5];
+    int32_t  nested;       /* 1: also build the H^2 form (nested cluster bases)   */
+    int32_t  reserved[4];
 } hlrc_problem;
 
 typedef struct hlrc_hbuild_s* hlrc_hbuild;
@@ -346,6 +386,7 @@ hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out);
 /* descriptors pointing into the build's host storage (valid until free)     */
 hlrc_status hlrc_build_h_desc(hlrc_hbuild B, hlrc_h_desc* out);
 hlrc_status hlrc_build_uniform_desc(hlrc_hbuild B, hlrc_uniform_desc* out);
+hlrc_status hlrc_build_h2_desc(hlrc_hbuild B, hlrc_h2_desc* out);
 /* coordinates in internal order: n x dim, row-major; dim returned           */
 hlrc_status hlrc_build_points(hlrc_hbuild B, const double** pts, int* dim,
                               int64_t* n);

@@ -46,10 +46,11 @@ def lib() -> C.CDLL:
         L.oracle_hmvm_seq.argtypes = [vp, f64, ci, vp, vp]
         L.oracle_hmvm_chunk.argtypes = [vp, f64, ci, vp, vp, ci]
         L.oracle_uniform_mvm.argtypes = [vp, f64, ci, vp, vp, ci]
+        L.oracle_h2_mvm.argtypes = [vp, f64, ci, vp, vp]
         L.oracle_dense_matvec.argtypes = [ci, i64, vp, vp, f64, f64, f64, ci, vp, vp, ci]
         L.oracle_leaf_max_error.argtypes = [vp, ci, vp, vp, f64, f64, i64]
         L.oracle_leaf_max_error.restype = f64
-        for f in ("oracle_hmvm_seq", "oracle_hmvm_chunk", "oracle_uniform_mvm", "oracle_dense_matvec"):
+        for f in ("oracle_hmvm_seq", "oracle_hmvm_chunk", "oracle_uniform_mvm", "oracle_h2_mvm", "oracle_dense_matvec"):
             getattr(L, f).restype = ci
         _lib = L
     return _lib
@@ -75,6 +76,11 @@ def hmvm_seq(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray) -> None:
 def hmvm_chunk(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray, nthreads: int = 0) -> None:
     """y += alpha op(M) x with 64-row chunk locks (hlr::tbb::mul_vec)."""
     _check(lib().oracle_hmvm_chunk(C.addressof(desc), alpha, op, _p(x), _p(y), nthreads), "oracle_hmvm_chunk")
+
+
+def h2_mvm(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray) -> int:
+    """y += alpha op(M) x for an H^2 matrix (hlr::h2::mul_vec); returns the status."""
+    return lib().oracle_h2_mvm(C.addressof(desc), alpha, op, _p(x), _p(y))
 
 
 def uniform_mvm(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray, nthreads: int = 0) -> int:

@@ -36,7 +36,8 @@ def test_abi_version():
 
 def test_struct_layouts_match_header(tmp_path):
     structs = ["hlrc_block", "hlrc_h_desc", "hlrc_basis", "hlrc_uniform_block", "hlrc_uniform_desc",
-               "hlrc_options", "hlrc_info", "hlrc_problem", "hlrc_tuning"]
+               "hlrc_options", "hlrc_info", "hlrc_problem", "hlrc_tuning",
+               "hlrc_h2_cluster", "hlrc_h2_desc"]
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include "hlrc.h"\nint main(void){\n' +
                    "".join(f'printf("{s} %zu\\n", sizeof({s}));\n' for s in structs) + "return 0;}\n")
