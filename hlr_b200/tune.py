@@ -14,10 +14,11 @@ products (enough to last 20 ms) timed with CUDA events on the launching
 stream, on private random vectors (the caller's vectors are not touched).
 The candidates are swept twice, interleaved, and each keeps its best time.
 The default setting is kept unless another one is faster by more than
-``keep_default_within`` (2 %), so timing noise does not flip the choice.  Winners are cached in a JSON file keyed by
-the device name and the matrix's signature (kind, precision, shape, stored
-bytes, leaf counts, vector count, operation); a later call for the same
-signature takes the cached setting without timing anything.
+``keep_default_within`` (2 %), so timing noise does not flip the choice.
+Winners are cached in a JSON file keyed by the device name and the matrix's
+signature (kind, precision, shape, stored bytes, leaf counts, vector count,
+operation); a later call for the same signature takes the cached setting
+without timing anything.
 
 The reference has no counterpart: its TBB products have no launch shapes.
 """
@@ -41,8 +42,9 @@ def default_cache_path() -> Path:
 
 def signature(M, nrhs: int, op: int, device_name: str) -> str:
     i = M.info
-    return "|".join(str(v) for v in (device_name, "uniform" if M.uniform else "h", i["precision"], i["n_rows"],
-                                      i["n_cols"], i["matrix_bytes"], i["n_dense"], i["n_lowrank"], nrhs, op))
+    kind = ("h", "uniform", "h2")[int(i.get("kind", 1 if M.uniform else 0))]
+    return "|".join(str(v) for v in (device_name, kind, i["precision"], i["n_rows"], i["n_cols"], i["matrix_bytes"],
+                                      i["n_dense"], i["n_lowrank"], nrhs, op))
 
 
 def candidates(current: dict, nrhs: int) -> list:
