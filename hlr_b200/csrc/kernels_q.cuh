@@ -195,21 +195,21 @@ __device__ __forceinline__ void npack_q(const QNPack& pk, const uint8_t* A, cons
             acc[2 * k] += double(t.x);
             acc[2 * k + 1] += double(t.y);
         }
-        return;
+    } else {
+        float s[F::R];
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) s[r] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float vj = __shfl_sync(0xffffffffu, vl, (g + F::C * i) & 31);
+            float f[F::R];
+            unpack16<FMT>(m[i], f);
+#pragma unroll
+            for (int r = 0; r < F::R; ++r) s[r] = fmaf(f[r], vj, s[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < F::R; ++r) acc[r] += double(s[r]);
     }
-    float s[F::R];
-#pragma unroll
-    for (int r = 0; r < F::R; ++r) s[r] = 0.f;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const float vj = __shfl_sync(0xffffffffu, vl, (g + F::C * i) & 31);
-        float f[F::R];
-        unpack16<FMT>(m[i], f);
-#pragma unroll
-        for (int r = 0; r < F::R; ++r) s[r] = fmaf(f[r], vj, s[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < F::R; ++r) acc[r] += double(s[r]);
 }
 
 // sum the C column groups of the accumulators and store rows to red[]
@@ -327,16 +327,16 @@ __device__ __forceinline__ void ttdots_q(const uint4* m, const uint2* ml, const 
             const float2 t = upk2(a);
             p[i] = t.x + t.y;
         }
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        float f[F::R];
-        unpack16<FMT>(m[i], f);
-        float s = 0.f;
+        for (int i = 0; i < 8; ++i) {
+            float f[F::R];
+            unpack16<FMT>(m[i], f);
+            float s = 0.f;
 #pragma unroll
-        for (int r = 0; r < F::R; ++r) s = fmaf(f[r], xr[r], s);
-        p[i] = s;
+            for (int r = 0; r < F::R; ++r) s = fmaf(f[r], xr[r], s);
+            p[i] = s;
+        }
     }
 }
 
