@@ -430,7 +430,8 @@ def run_ours(args, rank, world, local_rank):
     passes = (nrhs + 7) // 8 if nrhs > 1 else 1      # the matrix is streamed once per block of 8 vectors
     gbs = alg * passes / (ms_max / 1e3 / args.steps) / 1e9
     # the summaries key a workload as config[/precision][/nrhs]
-    wl = args.config + ("" if prec == "f64" else "/" + prec) + ("" if nrhs == 1 else f"/{nrhs}")
+    wl = (args.config + ("/h2" if args.h2 else "") + ("" if prec == "f64" else "/" + prec)
+          + ("" if nrhs == 1 else f"/{nrhs}"))
     roof = roofline_from_profile(prof, hbm_peak, peak_kind, wl)
     line = {
         "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": world, "steps": args.steps,
