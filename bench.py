@@ -660,8 +660,8 @@ def tune_handle(M, nrhs: int, args):
 def traffic_from_profiles(kernel: str, config: str):
     """DRAM bytes per launch of `kernel` from a committed ncu summary table
     row `| kernel | workload | bytes |` in profiles/*.md, if any; the
-    workload is the config, then /precision unless FP64, then /nrhs unless 1
-    (e.g. c2, c2/mixed, c2/mixed/8)."""
+    workload is the config, then /h2 for the H^2 form, then /precision unless
+    FP64, then /nrhs unless 1 (e.g. c2, c2/mixed, c2/mixed/8, c3/h2)."""
     for p in sorted((ROOT / "profiles").glob("*.md")):
         for ln in p.read_text().splitlines():
             parts = [s.strip() for s in ln.strip().strip("|").split("|")]
