@@ -57,8 +57,12 @@ struct DevNPass {
     const void* chunks = nullptr;     // NChunk (FP64 plan) or QNChunk (reduced precision)
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0, alg_bytes = 0;
+    // tree sweep (H^2 transfers): ncta CTAs, one cluster of TREE_CLUSTER per subtree
+    TreeArgs tree{};
+    int ncta = 0;
+    size_t tree_smem = 0;   // dynamic shared memory of the sweep
     int launches() const {
-        if (nseg2 > 0) return 1;
+        if (nseg2 > 0 || ncta > 0) return 1;
         int n = 0;
         for (int f = 0; f < NFMT; ++f) n += nsegs[f] > 0 ? 1 : 0;
         return n;
@@ -115,6 +119,7 @@ struct hlrc_hmat_s {
     std::vector<DevNPass> n;
     std::vector<DevTTPass> tt;
     std::vector<Stage> stages[3];
+    std::vector<Stage> stages_mr[3];   // multi-vector products, when they differ (H^2: no tree sweeps)
     hlrc_info info{};
     // multi-RHS workspace (FP64 plans, allocated at upload when max_nrhs > 1):
     // row-major blocks of MR_RB vectors
@@ -180,6 +185,7 @@ const char* stage_name(hlrc_hmat M, int nk, int idx) {
 struct ArenaLayout {
     size_t store = 0;
     std::vector<size_t> tu, ts, tg, nc, ttc, ttg, ttg1, n2;
+    std::vector<std::array<size_t, 7>> ntree;   // per N-pass: the tree sweep's seven arrays
     std::vector<std::array<size_t, NFMT>> ns, tts;   // per pass, per StoreFmt
     size_t t = 0, t2 = 0, part = 0, err = 0, total = 0;
     size_t part_elems = 0;
@@ -209,6 +215,10 @@ ArenaLayout arena_layout(const Plan& p) {
                                 : (np.segs[FMT_F32].size() + np.segs[FMT_F16].size() + np.segs[FMT_BF16].size() +
                                    np.segs[FMT_I16].size() + np.segs[FMT_I24].size()) *
                                       sizeof(NSeg2)));
+        L.ntree.push_back({take(np.cta_begin.size() * sizeof(int32_t)), take(np.tree_level.size() * sizeof(int32_t)),
+                           take(np.tree_seg.size() * sizeof(int32_t)), take(np.tree_chunk.size() * sizeof(TreeChunk)),
+                           take(np.tree_ext.size() * sizeof(TreeExt)), take(np.tree_cta_ext.size() * sizeof(int32_t)),
+                           take(np.tree_part.size() * sizeof(int32_t))});
     }
     size_t part_elems = size_t(std::max<uint32_t>(1, max_slots)) * 32;
     for (const TTPass& tp : p.ttpasses) {
@@ -487,6 +497,39 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         if (e == cudaSuccess) e = put(o_nc[i], enc.data(), enc.size());
         d.chunks = hp->arena + o_nc[i];
         d.vx = np.vx; d.vt = np.vt; d.out = np.out; d.mode = np.mode; d.bytes = np.bytes; d.alg_bytes = np.alg_bytes;
+        if (!np.cta_begin.empty() && e == cudaSuccess) {
+            if (!f64) {
+                cleanup();
+                return fail(HLRC_ERR_INTERNAL, "tree sweep in a reduced-precision plan");
+            }
+            const std::array<size_t, 7>& o = L.ntree[i];
+            e = put(o[0], np.cta_begin.data(), np.cta_begin.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = put(o[1], np.tree_level.data(), np.tree_level.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = put(o[2], np.tree_seg.data(), np.tree_seg.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = put(o[3], np.tree_chunk.data(), np.tree_chunk.size() * sizeof(TreeChunk));
+            if (e == cudaSuccess) e = put(o[4], np.tree_ext.data(), np.tree_ext.size() * sizeof(TreeExt));
+            if (e == cudaSuccess) e = put(o[5], np.tree_cta_ext.data(), np.tree_cta_ext.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = put(o[6], np.tree_part.data(), np.tree_part.size() * sizeof(int32_t));
+            TreeArgs& ta = d.tree;
+            ta.cta_begin = reinterpret_cast<const int*>(hp->arena + o[0]);
+            ta.level = reinterpret_cast<const int*>(hp->arena + o[1]);
+            ta.seg = reinterpret_cast<const int*>(hp->arena + o[2]);
+            ta.chunk = reinterpret_cast<const TreeChunk*>(hp->arena + o[3]);
+            ta.ext = reinterpret_cast<const TreeExt*>(hp->arena + o[4]);
+            ta.cta_ext = reinterpret_cast<const int*>(hp->arena + o[5]);
+            ta.part = reinterpret_cast<const int*>(hp->arena + o[6]);
+            ta.items = np.tree_items;
+            ta.stage = int(np.tree_stage);
+            ta.mirror = int(np.tree_mirror);
+            ta.levels = np.tree_levels;
+            ta.segs = np.tree_segs;
+            ta.chunks = np.tree_chunks;
+            d.ncta = (int(np.cta_begin.size()) - 1) * TREE_CLUSTER;
+            d.tree_smem = size_t(tree_smem_bytes(np.tree_stage, np.tree_mirror, np.tree_levels, np.tree_segs,
+                                                 np.tree_chunks, np.tree_items));
+            if (e == cudaSuccess && d.tree_smem > 48 * 1024)
+                e = cudaFuncSetAttribute(k_ntree_f64<TREE_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREE_SMEM);
+        }
         if (!f64 && e == cudaSuccess) {
             // pair the FP32 and 16-bit segments of every output tile
             // the store's wide and 16-bit formats: 24-bit and 16-bit integers
@@ -568,7 +611,10 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     hp->ws_t2 = reinterpret_cast<double*>(hp->arena + o_t2);
     hp->part = reinterpret_cast<double*>(hp->arena + o_part);
     hp->dev_err = reinterpret_cast<int*>(hp->arena + L.err);
-    for (int op = 0; op < 3; ++op) hp->stages[op] = p.stages[op];
+    for (int op = 0; op < 3; ++op) {
+        hp->stages[op] = p.stages[op];
+        hp->stages_mr[op] = p.stages_mr[op];
+    }
 
     fill_info(p, L, hp->info);
     // the 8-vector kernels take FP64, FP32 and FP16/BF16 columns; block
@@ -781,6 +827,12 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             const double alpha = np.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
             auto nform = [&](auto wc) {
                 constexpr int NW = decltype(wc)::value;
+                if (np.ncta > 0) {   // tree sweep (FP64 plans only)
+                    k_ntree_f64<TREE_WARPS><<<np.ncta, TREE_WARPS * 32, np.tree_smem, s>>>(
+                        np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), np.tree,
+                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add, M->dev_err);
+                    return;
+                }
                 if (f64plan && np.nsegs[FMT_F64] > 0)
                     k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
@@ -810,12 +862,18 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
     return HLRC_OK;
 }
 
+// The stages of a multi-vector product: the level passes where the
+// one-vector product sweeps trees.
+const std::vector<Stage>& mr_stages(hlrc_hmat M, int op) {
+    return M->stages_mr[op].empty() ? M->stages[op] : M->stages_mr[op];
+}
+
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
 // the multi-RHS workspace and no unit T-form stage (the uniform-H adjoint
 // coupling runs per vector).
 bool multi_rhs_ok(hlrc_hmat M, int op, int nrhs) {
     if (nrhs < 2 || nrhs < M->mr_min_nrhs || !M->mr_arena) return false;
-    for (const Stage& st : M->stages[op])
+    for (const Stage& st : mr_stages(M, op))
         if (st.kind == 0) return false;
     return true;
 }
@@ -831,7 +889,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
         k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, M->mr_x);
         M->launches += 1;
         HLRC_AFTER_LAUNCH("rows_from_cols");
-        for (const Stage& st : M->stages[op]) {
+        for (const Stage& st : mr_stages(M, op)) {
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
                 M->launches += M->tt[size_t(st.idx)].launches();
@@ -847,7 +905,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
             return OutMap{vec(name), MR_RB, 1, MR_RB};
         };
         const double* A = reinterpret_cast<const double*>(M->store);
-        for (const Stage& st : M->stages[op]) {
+        for (const Stage& st : mr_stages(M, op)) {
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
                 const int add = tp.mode != OUT_SET;
@@ -896,6 +954,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
             } else if (st.kind == 1) {
                 const DevNPass& np = M->n[size_t(st.idx)];
                 if (np.launches() == 0) continue;
+                if (np.ncta > 0) return fail(HLRC_ERR_INTERNAL, "tree sweep in a multi-vector product");
                 if (ws_profile(M)) prof_begin(M, stage_name(M, 1, st.idx), np.alg_bytes, s);
                 const int add = np.mode != OUT_SET;
                 const double alpha = np.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree

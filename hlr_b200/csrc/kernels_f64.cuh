@@ -5,11 +5,14 @@
 // small vectors x / t stay cache resident.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "layout.hpp"
 
 namespace hlrc {
+
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ double2 ld_stream(const double* p) {
     return __ldcs(reinterpret_cast<const double2*>(p));
@@ -92,6 +95,203 @@ k_nform_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, co
         if (add) *o += alpha * s;
         else *o = s;
     }
+}
+
+// Tree entries of a sweep pass (device copies of the planner's arrays) and
+// the maxima that size the CTAs' shared memory (tree_smem_bytes).
+struct TreeArgs {
+    const int* cta_begin;      // levels of subtree b: [cta_begin[b], cta_begin[b+1])
+    const int* level;          // segments of level g: [level[g], level[g+1])
+    const int* part;           // rank r of level g: segments [part[g*(TC+1)+r], part[g*(TC+1)+r+1])
+    const int* seg;            // mirror slot of each segment's first row
+    const TreeChunk* chunk;    // stage offset (owner's stage) and mirror slot of each chunk
+    const TreeExt* ext;        // coefficients copied in from outside the subtree
+    const int* cta_ext;        // subtree b's entries of ext: [cta_ext[b], cta_ext[b+1])
+    int stage, mirror, levels, segs, chunks, items;
+};
+
+// Bulk copies (TMA, no multicast) into this CTA's shared memory, completed
+// on an mbarrier per level.
+__device__ __forceinline__ unsigned tree_saddr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void tree_bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tree_saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void tree_bar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void tree_bar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(tree_saddr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void tree_bar_arrive(uint64_t* bar) {
+    uint64_t state;
+    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];\n" : "=l"(state) : "r"(tree_saddr(bar)) : "memory");
+    (void)state;
+}
+__device__ __forceinline__ void tree_bulk(double* dst, const double* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     tree_saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(tree_saddr(bar))
+                 : "memory");
+}
+// Waits for phase 0 of the barrier, at most TREE_WAIT_TRIES probes (each
+// may suspend the thread for a short while); false when they run out.
+constexpr int TREE_WAIT_TRIES = 1 << 20;
+__device__ __forceinline__ bool tree_bar_wait(uint64_t* bar) {
+    for (int i = 0; i < TREE_WAIT_TRIES; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(tree_saddr(bar))
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Tree sweep of the H^2 transfers: one cluster of TREE_CLUSTER CTAs per
+// subtree runs its levels one after the other; rank r of the cluster
+// computes its run of each level's segments.  Prologue (every CTA): the
+// subtree's segment and chunk descriptors are loaded; the matrix data of the
+// CTA's own chunks is copied into its stage by bulk copies (one per chunk,
+// each thread expecting the bytes of its own copies on the level's barrier),
+// so that the copies of later levels overlap the work of earlier ones; the
+// coefficients the subtree reads from outside (the leaves' going up, the
+// subtree root's going down) and, when adding, the current values of the
+// CTA's outputs are loaded into its mirror.  Level g: the CTA waits for its
+// own copies of the level; its chunks go to the half-warps (two rows per
+// lane, 32-row blocks), each writing a column partial to shared memory;
+// after a barrier every output row sums its segment's partials in chunk
+// order, and the result goes to the mirrors of all CTAs of the cluster
+// (distributed shared memory) and to the output array; a cluster barrier
+// ends the level.  Summation order is fixed: the result is deterministic.
+// A copy that never completes stops the CTA's work: it sets bit 1 of the
+// error word, keeps taking part in the cluster barriers, and waits
+// (bounded) for its other copies before returning.
+template <int W>
+__global__ void __cluster_dims__(TREE_CLUSTER, 1, 1) __launch_bounds__(W * 32)
+k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, TreeArgs t,
+            const double* __restrict__ A, const double* vx, const double* vt, double* out, double alpha, int add,
+            int* err) {
+    constexpr int TC = TREE_CLUSTER;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = int(cl.block_rank());
+    const int sub = int(blockIdx.x) / TC;
+    extern __shared__ double2 tree_smem[];
+    double* stage = reinterpret_cast<double*>(tree_smem);
+    double2* part2 = tree_smem + t.stage / 2;
+    double* mirror = reinterpret_cast<double*>(part2 + size_t(t.items) * (TILE / 2));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(mirror + ((t.mirror + 1) & ~1));
+    NSeg* sseg = reinterpret_cast<NSeg*>(bars + ((t.levels + 1) & ~1));
+    int* sseg_m = reinterpret_cast<int*>(sseg + t.segs);
+    NChunk* sch = reinterpret_cast<NChunk*>(sseg_m + ((t.segs + 3) & ~3));
+    TreeChunk* sct = reinterpret_cast<TreeChunk*>(sch + t.chunks);
+    int* srun = reinterpret_cast<int*>(sct + t.chunks);   // [2 * level]: this rank's run of the level's segments
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g0 = t.cta_begin[sub], g1 = t.cta_begin[sub + 1], nlev = g1 - g0;
+    const int S0 = t.level[g0], nseg = t.level[g1] - S0;
+    const uint32_t C0 = segs[S0].cb, nch = segs[S0 + nseg - 1].ce - C0;
+    if (tid == 0) {
+        for (int i = 0; i < nlev; ++i) tree_bar_init(&bars[i]);
+        tree_bar_init_fence();
+    }
+    for (int i = tid; i < nseg; i += W * 32) {
+        sseg[i] = segs[S0 + i];
+        sseg_m[i] = t.seg[S0 + i];
+    }
+    for (uint32_t i = tid; i < nch; i += W * 32) {
+        sch[i] = chunks[C0 + i];
+        sct[i] = t.chunk[C0 + i];
+    }
+    for (int i = tid; i < 2 * nlev; i += W * 32) srun[i] = t.part[size_t(g0 + i / 2) * (TC + 1) + rank + (i & 1)] - S0;
+    __syncthreads();
+    for (int gi = 0; gi < nlev; ++gi) {   // own matrix data: chunk k of the level's run to thread k % (32 W)
+        const int sb = srun[2 * gi], se = srun[2 * gi + 1];
+        if (sb >= se) continue;
+        const uint32_t k0 = sseg[sb].cb, k1 = sseg[se - 1].ce;
+        uint32_t bytes = 0;
+        int si = sb;
+        for (uint32_t c = k0 + tid; c < k1; c += W * 32) {
+            while (c >= sseg[si].ce) ++si;
+            bytes += uint32_t(sch[c - C0].nc) * sseg[si].ld * uint32_t(sizeof(double));
+        }
+        if (bytes == 0) continue;
+        tree_bar_expect(&bars[gi], bytes);
+        si = sb;
+        for (uint32_t c = k0 + tid; c < k1; c += W * 32) {
+            while (c >= sseg[si].ce) ++si;
+            const NChunk ch = sch[c - C0];
+            tree_bulk(stage + sct[c - C0].stage, A + ch.a_off, uint32_t(ch.nc) * sseg[si].ld * uint32_t(sizeof(double)),
+                      &bars[gi]);
+        }
+    }
+    __syncthreads();   // every expectation is set: the one arrival may complete a phase
+    if (tid == 0)
+        for (int i = 0; i < nlev; ++i) tree_bar_arrive(&bars[i]);
+    for (int e = t.cta_ext[sub] + tid; e < t.cta_ext[sub + 1]; e += W * 32) {
+        const TreeExt x = t.ext[e];
+        mirror[x.mirror] = __ldcg((x.v_off & VEC_T) ? vt + (x.v_off & ~VEC_T) : vx + x.v_off);
+    }
+    if (add)
+        for (int gi = 0; gi < nlev; ++gi) {
+            for (int q = srun[2 * gi] + warp; q < srun[2 * gi + 1]; q += W)
+                for (int i = lane; i < sseg[q].rows; i += 32) mirror[sseg_m[q] + i] = __ldcg(out + sseg[q].out + i);
+        }
+    cl.sync();   // every CTA of the cluster runs before any writes into its mirror
+    const int hw = 2 * warp + (lane >> 4), l16 = lane & 15;
+    bool failed = false;
+    for (int gi = 0; gi < nlev; ++gi) {
+        const bool ok = failed || tree_bar_wait(&bars[gi]);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0 && !failed) atomicOr(err, 1);
+            failed = true;
+        }
+        if (!failed) {
+            const int sb = srun[2 * gi], se = srun[2 * gi + 1];
+            const uint32_t k0 = sb < se ? sseg[sb].cb : 0, k1 = sb < se ? sseg[se - 1].ce : 0;
+            int si = sb;
+            for (uint32_t c = k0 + hw; c < k1; c += 2 * W) {
+                while (c >= sseg[si].ce) ++si;
+                const int ld = sseg[si].ld;
+                const NChunk ch = sch[c - C0];
+                const TreeChunk tc = sct[c - C0];
+                const double* v = mirror + tc.mirror;
+                for (int rr = 2 * l16; rr < ld; rr += 32) {
+                    const double* a = stage + tc.stage + rr;
+                    double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+                    for (int j = 0; j < NCHUNK; ++j)
+                        if (j < ch.nc) {
+                            const double2 m = *reinterpret_cast<const double2*>(a + j * ld);
+                            acc0 = fma(m.x, v[j], acc0);
+                            acc1 = fma(m.y, v[j], acc1);
+                        }
+                    part2[size_t(c - k0) * (TILE / 2) + rr / 2] = make_double2(acc0, acc1);
+                }
+            }
+            __syncthreads();
+            const double* part = reinterpret_cast<const double*>(part2);
+            for (int i = tid; i < (se - sb) * TILE; i += W * 32) {
+                const int q = sb + i / TILE, row = i % TILE;
+                const NSeg sg = sseg[q];
+                if (row < sg.rows) {
+                    double sum = 0.0;
+                    for (uint32_t c = sg.cb; c < sg.ce; ++c) sum += part[size_t(c - k0) * TILE + row];
+                    const int slot = sseg_m[q] + row;
+                    const double y = add ? mirror[slot] + alpha * sum : sum;
+#pragma unroll
+                    for (int r = 0; r < TC; ++r) *cl.map_shared_rank(mirror + slot, r) = y;
+                    out[sg.out + row] = y;
+                }
+            }
+        }
+        cl.sync();   // the level's rows are in every mirror; partials free
+    }
+    if (failed)
+        for (int k = 0; k < nlev; ++k) tree_bar_wait(&bars[k]);
 }
 
 // T-form: one warp per unit; lane l owns rows 2l, 2l+1 of every slab and

@@ -183,6 +183,34 @@ constexpr uint32_t MC_DIRECT = 0x80000000u;   // tile T-form column table: outpu
 // Longest run of partial slots one finish lane sums: longer outputs are
 // summed in two levels (runs of at most FINISH_SLOTS slots first).
 constexpr uint32_t FINISH_SLOTS = 16;
+// Tree sweeps (H^2 transfers): one thread-block cluster of TREE_CLUSTER
+// CTAs (TREE_WARPS warps each) per subtree.  Each level's segments are split
+// between the cluster's CTAs; a CTA stages the matrix data of its own
+// segments' chunks (`stage` doubles), keeps a mirror of the subtree's
+// coefficients (`mirror` doubles, the same layout in every CTA), one
+// mbarrier per level, the subtree's segment and chunk descriptors, its
+// level and run bounds, and the partial sums of its chunks of one level
+// (`items` x TILE doubles): at most
+// TREE_SMEM bytes (tree_smem_bytes).  Subtrees are rooted at the first level
+// with at least TREE_MIN_SUBTREES clusters, or deeper when one does not fit.
+constexpr int TREE_CLUSTER = 4;
+constexpr int TREE_WARPS = 16;
+constexpr int TREE_SMEM = 200 * 1024;
+constexpr int TREE_MIN_SUBTREES = 32;
+inline constexpr int64_t tree_smem_bytes(int64_t stage, int64_t mirror, int64_t levels, int64_t segs, int64_t chunks,
+                                         int64_t items) {
+    return 8 * stage + 8 * ((mirror + 1) & ~int64_t(1)) + 8 * ((levels + 1) & ~int64_t(1)) +
+           20 * ((segs + 3) & ~int64_t(3)) + 24 * chunks + 8 * TILE * items + 16 * (levels + 1);
+}
+struct TreeChunk {         // tree entry of a chunk
+    uint32_t stage;        // offset (doubles, even) of its data in its owner CTA's stage
+    uint32_t mirror;       // mirror slot of its first vector entry
+};
+struct TreeExt {           // coefficient read from outside the CTA, copied into the mirror
+    uint32_t mirror;       // mirror slot
+    uint32_t v_off;        // vector offset (| VEC_T: in t)
+};
+
 struct MCol {
     uint32_t idx;          // N-form: vector entry (| VEC_T: in t); T-form: output (| MC_DIRECT) or partial
     float scale;           // the chunk's scale (1 for FP32)

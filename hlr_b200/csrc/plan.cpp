@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <unordered_map>
 
 #include <omp.h>
 
@@ -339,6 +340,7 @@ void pack_chunks(std::vector<GChunk>& ch, uint32_t s, uint32_t e) {
 struct NBuilder {
     NPass& P;
     const Store& S;
+    bool keep_order = false;   // segments in the order built (tree sweeps), not by cost
     NBuilder(NPass& p, const Store& s) : P(p), S(s) {}
     std::vector<std::pair<int64_t, NSeg>> tmp[NFMT];
     uint32_t cb = 0;
@@ -375,7 +377,9 @@ struct NBuilder {
     }
     void finish() {
         for (int f = 0; f < NFMT; ++f) {
-            std::stable_sort(tmp[f].begin(), tmp[f].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            if (!keep_order)
+                std::stable_sort(tmp[f].begin(), tmp[f].end(),
+                                 [](const auto& a, const auto& b) { return a.first > b.first; });
             P.segs[f].clear();
             for (auto& e : tmp[f]) {
                 P.segs[f].push_back(e.second);
@@ -610,6 +614,60 @@ hlrc_status validate_plan(const Plan& p) {
                         return fail(HLRC_ERR_INTERNAL, "N-pass %zu: chunk %u vector outside its array", pi, c);
                 }
             }
+        // tree sweeps: FP64 segments whose chunks follow one another, levels
+        // and subtrees that partition them, rank runs that partition each
+        // level, stage and mirror entries inside the shared memory (16-byte
+        // aligned stage runs)
+        if (np.cta_begin.empty() && np.tree_level.empty()) continue;
+        const std::vector<NSeg>& sg = np.segs[FMT_F64];
+        const std::vector<int32_t>&cb = np.cta_begin, &tl = np.tree_level;
+        constexpr int TC = TREE_CLUSTER;
+        const size_t nsub = cb.size() - 1;
+        bool ok = cb.size() >= 2 && tl.size() >= 2 && cb.front() == 0 && tl.front() == 0 &&
+                  cb.back() == int32_t(tl.size()) - 1 && tl.back() == int32_t(sg.size()) && !sg.empty() &&
+                  sg.back().ce == np.chunks.size() && np.tree_seg.size() == sg.size() &&
+                  np.tree_part.size() == (tl.size() - 1) * (TC + 1) && np.tree_chunk.size() == np.chunks.size() &&
+                  np.tree_cta_ext.size() == nsub + 1 && np.tree_cta_ext.front() == 0 &&
+                  np.tree_cta_ext.back() == int32_t(np.tree_ext.size()) &&
+                  tree_smem_bytes(np.tree_stage, np.tree_mirror, np.tree_levels, np.tree_segs, np.tree_chunks,
+                                  np.tree_items) <= TREE_SMEM &&
+                  np.tree_stage % 2 == 0 && (np.vt == np.out) && (np.mode == OUT_SET || np.mode == OUT_ADD) &&
+                  nsub * TC < (size_t(1) << 31);
+        for (int f = 0; f < NFMT && ok; ++f) ok = f == FMT_F64 || np.segs[f].empty();
+        for (size_t i = 1; i < cb.size() && ok; ++i) ok = cb[i] > cb[i - 1];
+        for (size_t i = 1; i < tl.size() && ok; ++i) ok = tl[i] > tl[i - 1];
+        for (size_t i = 1; i < np.tree_cta_ext.size() && ok; ++i) ok = np.tree_cta_ext[i] >= np.tree_cta_ext[i - 1];
+        for (size_t s = 0; s < sg.size() && ok; ++s) ok = sg[s].cb == (s ? sg[s - 1].ce : 0u);
+        for (size_t b = 0; b < nsub && ok; ++b) {
+            const int32_t s0 = tl[size_t(cb[b])], s1 = tl[size_t(cb[b + 1])];
+            ok = cb[b + 1] - cb[b] <= np.tree_levels && s1 - s0 <= np.tree_segs &&
+                 int64_t(sg[size_t(s1 - 1)].ce) - int64_t(sg[size_t(s0)].cb) <= np.tree_chunks;
+            for (int32_t g = cb[b]; g < cb[b + 1] && ok; ++g) {
+                const int32_t* part = &np.tree_part[size_t(g) * (TC + 1)];
+                ok = part[0] == tl[size_t(g)] && part[TC] == tl[size_t(g) + 1];
+                for (int r = 0; r < TC && ok; ++r) {
+                    ok = part[r + 1] >= part[r];
+                    int64_t items = 0, stage_end = 0;
+                    for (int32_t q = part[r]; q < part[r + 1] && ok; ++q)
+                        for (uint32_t c = sg[size_t(q)].cb; c < sg[size_t(q)].ce && ok; ++c) {
+                            ++items;
+                            const TreeChunk& t = np.tree_chunk[c];
+                            stage_end = int64_t(t.stage) + int64_t(np.chunks[c].nc) * sg[size_t(q)].ld;
+                            ok = t.stage % 2 == 0 && stage_end <= np.tree_stage &&
+                                 int64_t(t.mirror) + np.chunks[c].nc <= np.tree_mirror;
+                        }
+                    ok = ok && items <= np.tree_items;
+                }
+            }
+            for (int32_t q = s0; q < s1 && ok; ++q)
+                ok = np.tree_seg[size_t(q)] >= 0 && np.tree_seg[size_t(q)] + sg[size_t(q)].rows <= np.tree_mirror;
+            for (int32_t e = np.tree_cta_ext[b]; e < np.tree_cta_ext[b + 1] && ok; ++e) {
+                const TreeExt& x = np.tree_ext[size_t(e)];
+                const bool t = (x.v_off & VEC_T) != 0;
+                ok = int64_t(x.mirror) < np.tree_mirror && int64_t(x.v_off & ~VEC_T) < vec_len(t ? np.vt : np.vx);
+            }
+        }
+        if (!ok) return fail(HLRC_ERR_INTERNAL, "N-pass %zu: malformed tree sweep", pi);
     }
     for (size_t pi = 0; pi < p.ttpasses.size(); ++pi) {
         const TTPass& tp = p.ttpasses[pi];
@@ -1402,49 +1460,187 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
         }
         tb.finish();
     };
-    // forward transfers into the clusters of level lev: x^_p = sum_s E_s^T x^_s,
-    // one N-form output per parent (pieces of at most TILE rows) over the
-    // transposed transfer matrices of its sons
+    // forward transfer into parent t: x^_t = sum_s E_s^T x^_s, one N-form
+    // output (pieces of at most TILE rows) over the transposed transfer
+    // matrices of its sons
+    auto fwd_parent = [&](NBuilder& nbld, const Tree& T, const std::vector<std::vector<int>>& sET, int64_t t) -> bool {
+        if (T.leaf(t) || T.c[t].rank == 0) return false;
+        const int64_t kp = T.c[t].rank;
+        for (int64_t r0 = 0, piece = 0; r0 < kp; r0 += TILE, ++piece) {
+            const int64_t rows = std::min<int64_t>(TILE, kp - r0);
+            nbld.begin(rows);
+            for (int i = 0; i < 2; ++i) {
+                const int64_t so = T.c[t].son[i];
+                if (so >= 0 && !sET[size_t(so)].empty())
+                    nbld.slab(sET[size_t(so)][size_t(piece)], VEC_T | uint32_t(T.off[size_t(so)]));
+            }
+            nbld.end(uint32_t(T.off[size_t(t)] + r0), rows, true);
+        }
+        return true;
+    };
+    // backward transfer into son c: y^_c += E_c y^_p
+    auto bwd_child = [&](NBuilder& nbld, const Tree& T, const std::vector<std::vector<int>>& sE, int64_t c) -> bool {
+        if (sE[size_t(c)].empty()) return false;
+        const int64_t pr = T.c[c].parent;
+        for (size_t pc = 0; pc < sE[size_t(c)].size(); ++pc) {
+            const int64_t r0 = int64_t(pc) * TILE, rows = std::min<int64_t>(TILE, T.c[c].rank - r0);
+            nbld.begin(rows);
+            nbld.slab(sE[size_t(c)][pc], VEC_T | uint32_t(T.off[size_t(pr)]));
+            nbld.end(uint32_t(T.off[size_t(c)] + r0), rows, false);
+        }
+        return true;
+    };
+    // one pass per level: the forward transfers into the clusters of level
+    // lev, the backward transfers into the sons of level lev
     auto fwd_transfer = [&](NPass& n, const Tree& T, const std::vector<std::vector<int>>& sET, int lev) -> bool {
         n.vx = V_X; n.vt = V_T; n.out = V_T; n.mode = OUT_SET;
         NBuilder nbld(n, st);
         bool any = false;
-        for (int64_t t = 0; t < T.n; ++t) {
-            if (T.level[size_t(t)] != lev || T.leaf(t) || T.c[t].rank == 0) continue;
-            const int64_t kp = T.c[t].rank;
-            for (int64_t r0 = 0, piece = 0; r0 < kp; r0 += TILE, ++piece) {
-                const int64_t rows = std::min<int64_t>(TILE, kp - r0);
-                nbld.begin(rows);
-                for (int i = 0; i < 2; ++i) {
-                    const int64_t so = T.c[t].son[i];
-                    if (so >= 0 && !sET[size_t(so)].empty())
-                        nbld.slab(sET[size_t(so)][size_t(piece)], VEC_T | uint32_t(T.off[size_t(so)]));
-                }
-                nbld.end(uint32_t(T.off[size_t(t)] + r0), rows, true);
-                any = true;
-            }
-        }
+        for (int64_t t = 0; t < T.n; ++t)
+            if (T.level[size_t(t)] == lev) any |= fwd_parent(nbld, T, sET, t);
         nbld.finish();
         return any;
     };
-    // backward transfers into the sons of level lev: y^_c += E_c y^_p
     auto bwd_transfer = [&](NPass& n, const Tree& T, const std::vector<std::vector<int>>& sE, int lev) -> bool {
         n.vx = V_X; n.vt = V_T2; n.out = V_T2; n.mode = OUT_ADD;
         NBuilder nbld(n, st);
         bool any = false;
-        for (int64_t c = 0; c < T.n; ++c) {
-            if (T.level[size_t(c)] != lev + 1 || sE[size_t(c)].empty()) continue;
-            const int64_t pr = T.c[c].parent;
-            for (size_t pc = 0; pc < sE[size_t(c)].size(); ++pc) {
-                const int64_t r0 = int64_t(pc) * TILE, rows = std::min<int64_t>(TILE, T.c[c].rank - r0);
-                nbld.begin(rows);
-                nbld.slab(sE[size_t(c)][pc], VEC_T | uint32_t(T.off[size_t(pr)]));
-                nbld.end(uint32_t(T.off[size_t(c)] + r0), rows, false);
-                any = true;
-            }
-        }
+        for (int64_t c = 0; c < T.n; ++c)
+            if (T.level[size_t(c)] == lev + 1) any |= bwd_child(nbld, T, sE, c);
         nbld.finish();
         return any;
+    };
+    // tree sweep: the levels lo..hi of every subtree rooted at level L0 in
+    // one pass, one CTA cluster per subtree, deepest level first (up) or
+    // shallowest first; emit adds a cluster's segments.  Fails when a
+    // subtree does not fit the CTAs' shared memory.
+    auto tree_pass = [&](NPass& n, const Tree& T, int L0, int lo, int hi, bool up, auto&& emit) -> bool {
+        NBuilder nbld(n, st);
+        nbld.keep_order = true;
+        n.cta_begin.assign(1, 0);
+        n.tree_level.assign(1, 0);
+        for (int64_t r = 0; r < T.n; ++r) {
+            if (T.level[size_t(r)] != L0) continue;
+            std::vector<std::vector<int64_t>> lv(size_t(T.maxlev) + 1);
+            for (std::vector<int64_t> stack{r}; !stack.empty();) {
+                const int64_t t = stack.back();
+                stack.pop_back();
+                lv[size_t(T.level[size_t(t)])].push_back(t);
+                for (int i = 0; i < 2; ++i)
+                    if (T.c[t].son[i] >= 0) stack.push_back(T.c[t].son[i]);
+            }
+            for (int k = 0; k <= hi - lo; ++k) {
+                std::vector<int64_t>& v = lv[size_t(up ? hi - k : lo + k)];
+                std::sort(v.begin(), v.end());
+                for (int64_t t : v) emit(nbld, t);
+                const int32_t ns = int32_t(nbld.tmp[FMT_F64].size());
+                if (ns > n.tree_level.back()) n.tree_level.push_back(ns);
+            }
+            const int32_t nl = int32_t(n.tree_level.size()) - 1;
+            if (nl > n.cta_begin.back()) n.cta_begin.push_back(nl);
+        }
+        nbld.finish();
+        if (n.cta_begin.size() < 2) return false;
+        // per subtree: each level's segments split into TREE_CLUSTER runs of
+        // about equal bytes (one per cluster rank); stage offsets of the
+        // chunks in their owner's stage; mirror slots for the rows of the
+        // segments, then for the coefficients read from outside (the leaves'
+        // or the subtree root's), one run per chunk
+        const std::vector<NSeg>& sg = n.segs[FMT_F64];
+        const std::vector<int32_t>& tl = n.tree_level;
+        constexpr int TC = TREE_CLUSTER;
+        auto seg_bytes = [&](int32_t q) { return int64_t(sg[size_t(q)].ce - sg[size_t(q)].cb) * sg[size_t(q)].ld; };
+        n.tree_part.assign((tl.size() - 1) * (TC + 1), 0);
+        n.tree_seg.assign(sg.size(), 0);
+        n.tree_chunk.assign(n.chunks.size(), TreeChunk{0, 0});
+        n.tree_ext.clear();
+        n.tree_cta_ext.assign(1, 0);
+        n.tree_stage = n.tree_mirror = 0;
+        n.tree_levels = n.tree_segs = n.tree_chunks = n.tree_items = 0;
+        for (size_t b = 0; b + 1 < n.cta_begin.size(); ++b) {
+            const int32_t s0 = tl[size_t(n.cta_begin[b])], s1 = tl[size_t(n.cta_begin[b + 1])];
+            uint32_t rows = 0;
+            for (int32_t q = s0; q < s1; ++q) {
+                n.tree_seg[size_t(q)] = int32_t(rows);
+                rows += sg[size_t(q)].rows;
+            }
+            uint32_t next = rows;
+            uint32_t stage[TC] = {};
+            int64_t load[TC] = {};   // stage doubles per rank so far
+            std::unordered_map<uint32_t, uint32_t> made;   // coefficient -> mirror slot, earlier levels
+            for (int32_t g = n.cta_begin[b]; g < n.cta_begin[b + 1]; ++g) {
+                const int32_t q0 = tl[size_t(g)], q1 = tl[size_t(g) + 1];
+                int64_t tot = 0;
+                for (int32_t q = q0; q < q1; ++q) tot += seg_bytes(q);
+                int32_t* part = &n.tree_part[size_t(g) * (TC + 1)];
+                part[0] = q0;
+                if (q1 - q0 <= TC) {   // one segment each for the least loaded ranks, in rank order
+                    int rk[TC];
+                    std::iota(rk, rk + TC, 0);
+                    std::stable_sort(rk, rk + TC, [&](int x, int y) { return load[x] < load[y]; });
+                    std::sort(rk, rk + (q1 - q0));
+                    int32_t q = q0;
+                    for (int r = 0, k = 0; r < TC; ++r) {
+                        if (k < q1 - q0 && rk[k] == r) { load[r] += seg_bytes(q++); ++k; }
+                        part[r + 1] = q;
+                    }
+                } else {   // runs of about equal bytes, rank r until its share is reached
+                    int64_t acc = 0;
+                    int32_t q = q0;
+                    for (int r = 0; r < TC; ++r) {
+                        const int64_t a0 = acc;
+                        while (q < q1 && (r == TC - 1 || acc * TC < tot * (r + 1) || acc == 0)) acc += seg_bytes(q++);
+                        part[r + 1] = q;
+                        load[r] += acc - a0;
+                    }
+                }
+                for (int r = 0; r < TC; ++r) {
+                    int items = 0;
+                    for (int32_t qq = part[r]; qq < part[r + 1]; ++qq)
+                        for (uint32_t c = sg[size_t(qq)].cb; c < sg[size_t(qq)].ce; ++c) {
+                            const GChunk& ch = n.chunks[c];
+                            TreeChunk& tc = n.tree_chunk[c];
+                            tc.stage = stage[r];
+                            stage[r] += uint32_t(ch.nc) * sg[size_t(qq)].ld;
+                            ++items;
+                            const auto f0 = made.find(ch.vo);
+                            bool run = f0 != made.end();
+                            for (uint32_t j = 1; j < ch.nc && run; ++j) {
+                                const auto fj = made.find(ch.vo + j);
+                                run = fj != made.end() && fj->second == f0->second + j;
+                            }
+                            if (run) {
+                                tc.mirror = f0->second;
+                            } else {
+                                tc.mirror = next;
+                                for (uint32_t j = 0; j < ch.nc; ++j) n.tree_ext.push_back(TreeExt{next++, ch.vo + j});
+                            }
+                        }
+                    n.tree_items = std::max(n.tree_items, items);
+                }
+                for (int32_t qq = q0; qq < q1; ++qq)
+                    for (uint32_t i = 0; i < sg[size_t(qq)].rows; ++i)
+                        made[(VEC_T | sg[size_t(qq)].out) + i] = uint32_t(n.tree_seg[size_t(qq)]) + i;
+            }
+            n.tree_cta_ext.push_back(int32_t(n.tree_ext.size()));
+            for (int r = 0; r < TC; ++r) n.tree_stage = std::max<int64_t>(n.tree_stage, stage[r]);
+            n.tree_mirror = std::max<int64_t>(n.tree_mirror, next);
+            n.tree_levels = std::max(n.tree_levels, int(n.cta_begin[b + 1] - n.cta_begin[b]));
+            n.tree_segs = std::max(n.tree_segs, int(s1 - s0));
+            n.tree_chunks = std::max(n.tree_chunks, int(sg[size_t(s1 - 1)].ce - sg[size_t(s0)].cb));
+        }
+        return tree_smem_bytes(n.tree_stage, n.tree_mirror, n.tree_levels, n.tree_segs, n.tree_chunks,
+                               n.tree_items) <= TREE_SMEM;
+    };
+    // subtrees rooted at the first level with at least TREE_MIN_SUBTREES
+    // clusters, or deeper while a level of a subtree holds too many chunks;
+    // -1 when fewer than two levels would be swept
+    auto tree_root = [&](const Tree& T) -> int {
+        std::vector<int64_t> cnt(size_t(T.maxlev) + 1, 0);
+        for (int64_t t = 0; t < T.n; ++t) ++cnt[size_t(T.level[size_t(t)])];
+        for (int l = 0; l <= T.maxlev; ++l)
+            if (cnt[size_t(l)] >= TREE_MIN_SUBTREES) return l;
+        return -1;
     };
     // backward leaf transform (+ near field for op N): y += alpha (V_t y^_t + D x)
     auto bwd_leaves = [&](NPass& n, const Tree& T, const Tiles& tl, const std::vector<std::vector<int64_t>>& bl,
@@ -1463,8 +1659,6 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
         nbld.finish();
     };
 
-    // ---- op N
-    std::vector<Stage>& sn = p.stages[HLRC_OP_N];
     auto add_tt = [&](const char* name) -> TTPass& {
         p.ttpasses.emplace_back();
         p.names[2].push_back(name);
@@ -1475,13 +1669,76 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
         p.names[1].push_back(name);
         return p.npasses.back();
     };
-    // passes are appended, so stages record indices, not references
+    auto drop_n = [&]() { p.npasses.pop_back(); p.names[1].pop_back(); };
+    // passes are appended, so stages record indices, not references.  Every
+    // level has its own pass (the multi-vector product runs those); the
+    // one-vector product runs the levels of the subtrees in one tree sweep
+    // per tree when one can be built.
+    // up: forward leaves + transfers of tree Tf; down: backward transfers of
+    // tree Tb.  `mid` is the coupling stage between them.
+    auto compose = [&](int op, const Tree& Tf, const std::vector<std::vector<int>>& sETf, const Tree& Tb,
+                       const std::vector<std::vector<int>>& sEb, const Stage& leaves_in, const Stage& mid,
+                       const std::vector<Stage>& tail) {
+        std::vector<int> up(size_t(Tf.maxlev) + 1, -1), down(size_t(Tb.maxlev) + 1, -1);
+        for (int lev = Tf.maxlev - 1; lev >= 0; --lev) {
+            if (fwd_transfer(add_n("h2_fwd_transfer"), Tf, sETf, lev)) up[size_t(lev)] = int(p.npasses.size()) - 1;
+            else drop_n();
+        }
+        for (int lev = 0; lev < Tb.maxlev; ++lev) {
+            if (bwd_transfer(add_n("h2_bwd_transfer"), Tb, sEb, lev)) down[size_t(lev)] = int(p.npasses.size()) - 1;
+            else drop_n();
+        }
+        // forward sweep: parents at levels L0..maxlev-1 of the subtrees
+        int upL0 = -1, upIdx = -1, downL0 = -1, downIdx = -1;
+        for (int L0 = tree_root(Tf); L0 >= 0 && L0 + 1 <= Tf.maxlev - 1 && upIdx < 0; ++L0) {
+            NPass& n = add_n("h2_fwd_tree");
+            n.vx = V_X; n.vt = V_T; n.out = V_T; n.mode = OUT_SET;
+            if (tree_pass(n, Tf, L0, L0, Tf.maxlev - 1, true,
+                          [&](NBuilder& nb, int64_t t) { fwd_parent(nb, Tf, sETf, t); })) {
+                upL0 = L0;
+                upIdx = int(p.npasses.size()) - 1;
+            } else {
+                drop_n();
+            }
+        }
+        // backward sweep: sons at levels L0+1..maxlev of the subtrees
+        for (int L0 = tree_root(Tb); L0 >= 0 && L0 + 2 <= Tb.maxlev && downIdx < 0; ++L0) {
+            NPass& n = add_n("h2_bwd_tree");
+            n.vx = V_X; n.vt = V_T2; n.out = V_T2; n.mode = OUT_ADD;
+            if (tree_pass(n, Tb, L0, L0 + 1, Tb.maxlev, false,
+                          [&](NBuilder& nb, int64_t c) { bwd_child(nb, Tb, sEb, c); })) {
+                downL0 = L0;
+                downIdx = int(p.npasses.size()) - 1;
+            } else {
+                drop_n();
+            }
+        }
+        std::vector<Stage>& lv = p.stages_mr[op];
+        std::vector<Stage>& sw = p.stages[op];
+        lv = {leaves_in};
+        sw = {leaves_in};
+        if (upIdx >= 0) sw.push_back({1, upIdx});
+        for (int lev = Tf.maxlev - 1; lev >= 0; --lev) {
+            if (up[size_t(lev)] < 0) continue;
+            lv.push_back({1, up[size_t(lev)]});
+            if (upIdx < 0 || lev < upL0) sw.push_back({1, up[size_t(lev)]});
+        }
+        lv.push_back(mid);
+        sw.push_back(mid);
+        for (int lev = 0; lev < Tb.maxlev; ++lev) {
+            if (down[size_t(lev)] < 0) continue;
+            lv.push_back({1, down[size_t(lev)]});
+            if (downIdx < 0 || lev < downL0) sw.push_back({1, down[size_t(lev)]});
+        }
+        if (downIdx >= 0) sw.push_back({1, downIdx});
+        lv.insert(lv.end(), tail.begin(), tail.end());
+        sw.insert(sw.end(), tail.begin(), tail.end());
+        if (upIdx < 0 && downIdx < 0) lv.clear();   // the same stages
+    };
+
+    // ---- op N
     fwd_leaves(add_tt("h2_fwd_leaves"), Cc, tc, cbl, sCB);
-    sn.push_back({2, int(p.ttpasses.size()) - 1});
-    for (int lev = Cc.maxlev - 1; lev >= 0; --lev) {
-        if (fwd_transfer(add_n("h2_fwd_transfer"), Cc, sETC, lev)) sn.push_back({1, int(p.npasses.size()) - 1});
-        else { p.npasses.pop_back(); p.names[1].pop_back(); }
-    }
+    const Stage n_leaves{2, int(p.ttpasses.size()) - 1};
     {   // couplings: every row cluster of positive rank is written (zero without blocks)
         NPass& c = add_n("h2_coupling");
         c.vx = V_X; c.vt = V_T; c.out = V_T2; c.mode = OUT_SET;
@@ -1498,23 +1755,15 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
             }
         }
         nbld.finish();
-        sn.push_back({1, int(p.npasses.size()) - 1});
     }
-    for (int lev = 0; lev < R.maxlev; ++lev) {
-        if (bwd_transfer(add_n("h2_bwd_transfer"), R, sER, lev)) sn.push_back({1, int(p.npasses.size()) - 1});
-        else { p.npasses.pop_back(); p.names[1].pop_back(); }
-    }
+    const Stage n_coupling{1, int(p.npasses.size()) - 1};
     bwd_leaves(add_n("h2_bwd_leaves_Dx"), R, tr, rbl, sRB, true);
-    sn.push_back({1, int(p.npasses.size()) - 1});
+    const Stage n_out{1, int(p.npasses.size()) - 1};
+    compose(HLRC_OP_N, Cc, sETC, R, sER, n_leaves, n_coupling, {n_out});
 
     // ---- op C: the trees exchanged
-    std::vector<Stage>& sc = p.stages[HLRC_OP_C];
     fwd_leaves(add_tt("h2_fwd_leaves"), R, tr, rbl, sRB);
-    sc.push_back({2, int(p.ttpasses.size()) - 1});
-    for (int lev = R.maxlev - 1; lev >= 0; --lev) {
-        if (fwd_transfer(add_n("h2_fwd_transfer"), R, sETR, lev)) sc.push_back({1, int(p.npasses.size()) - 1});
-        else { p.npasses.pop_back(); p.names[1].pop_back(); }
-    }
+    const Stage c_leaves{2, int(p.ttpasses.size()) - 1};
     {   // couplings transposed: y^_s = sum_t S_ts^T x^_t (unit T-form; every
         // column cluster of positive rank is written)
         p.tpasses.emplace_back();
@@ -1537,19 +1786,16 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
             tb.add(uint32_t(Cc.off[size_t(s)]), Cc.c[s].rank, sl);
         }
         tb.finish();
-        sc.push_back({0, int(p.tpasses.size()) - 1});
     }
-    for (int lev = 0; lev < Cc.maxlev; ++lev) {
-        if (bwd_transfer(add_n("h2_bwd_transfer"), Cc, sEC, lev)) sc.push_back({1, int(p.npasses.size()) - 1});
-        else { p.npasses.pop_back(); p.names[1].pop_back(); }
-    }
+    const Stage c_coupling{0, int(p.tpasses.size()) - 1};
     bwd_leaves(add_n("h2_bwd_leaves"), Cc, tc, cbl, sCB, false);
-    sc.push_back({1, int(p.npasses.size()) - 1});
+    const Stage c_out{1, int(p.npasses.size()) - 1};
     plan_dense_transposed(add_tt("h2_DtX"), st, tr, tc, rdl, sD, [&](int64_t i, int64_t& c0, int64_t& nc) {
         c0 = d.blocks[i].col0;
         nc = d.blocks[i].ncols;
     });
-    sc.push_back({2, int(p.ttpasses.size()) - 1});
+    const Stage c_dense{2, int(p.ttpasses.size()) - 1};
+    compose(HLRC_OP_C, R, sETR, Cc, sEC, c_leaves, c_coupling, {c_out, c_dense});
     p.stages[HLRC_OP_T].clear();   // as uniform-H: no transposed product
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");

@@ -59,6 +59,23 @@ struct TPass {
 struct NPass {
     std::vector<NSeg> segs[NFMT];     // per StoreFmt, ordered by cost (descending)
     std::vector<GChunk> chunks;
+    // tree sweep (H^2 transfers, FP64 only; empty: one CTA per segment).
+    // Subtree b (one cluster of TREE_CLUSTER CTAs) runs the levels
+    // [cta_begin[b], cta_begin[b+1]) one after the other, with a cluster
+    // barrier between them; level g is the segments [tree_level[g],
+    // tree_level[g+1]) of segs[FMT_F64], of which cluster rank r computes
+    // [tree_part[g*(TREE_CLUSTER+1)+r], tree_part[g*(TREE_CLUSTER+1)+r+1]).
+    // Segments keep the order built, and their chunks follow one another in
+    // that order.  tree_seg[s]: mirror slot of segment s's first row;
+    // tree_chunk[c]: the chunk's stage offset (in its owner's stage) and
+    // mirror slot; subtree b copies the coefficients
+    // tree_ext[tree_cta_ext[b] .. tree_cta_ext[b+1]) into its mirrors first.
+    std::vector<int32_t> cta_begin, tree_level, tree_part, tree_seg, tree_cta_ext;
+    std::vector<TreeChunk> tree_chunk;
+    std::vector<TreeExt> tree_ext;
+    int64_t tree_stage = 0, tree_mirror = 0;   // most stage doubles (one CTA) / mirror slots (one subtree)
+    int tree_levels = 0, tree_segs = 0, tree_chunks = 0;   // most levels / segments / chunks of one subtree
+    int tree_items = 0;                        // most chunks of one level computed by one CTA
     int vx = V_X, vt = V_T, out = V_Y, mode = OUT_ADD_ALPHA;
     int64_t bytes = 0;
     int64_t alg_bytes = 0;
@@ -93,6 +110,7 @@ struct Plan {
     std::vector<NPass> npasses;
     std::vector<TTPass> ttpasses;
     std::vector<Stage> stages[3];  // per op (N, T, C); empty = unsupported
+    std::vector<Stage> stages_mr[3];  // multi-vector products when they differ (H^2: level passes, no tree sweeps)
     // accounting (per product, one rhs)
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;

@@ -63,3 +63,39 @@ def test_h2_rejects_transposed_and_other_precisions():
     M.free()
     with pytest.raises(hlr.HLRCError):
         hlr.upload(hm, h2=True, precision="mixed")
+
+
+@pytest.mark.parametrize("op", [0, 2])
+def test_h2_tree_sweeps(op):
+    """The sphere with 8192 triangles has 32 clusters at level 5 and three
+    levels below them: the one-vector product sweeps those levels of each
+    tree in one launch (one CTA per subtree), the 8-vector product runs them
+    level by level, and both match the oracle."""
+    hm = built("sphere5_h2", CASES["sphere5"])
+    M = hlr.upload(hm, h2=True, max_nrhs=8)
+    M.set_profiling(True)
+    M.last_profile()
+    rng = np.random.default_rng(77 + op)
+    x = rng.standard_normal(hm.n)
+    y = torch.zeros(hm.n, dtype=torch.float64, device="cuda")
+    hlr.mul_vec(-0.5, op, M, torch.from_numpy(x).cuda(), y)
+    torch.cuda.synchronize()
+    prof = M.last_profile()
+    assert prof["h2_fwd_tree"][0] == 1 and prof["h2_bwd_tree"][0] == 1
+    # the levels above the subtree roots keep one pass each
+    assert prof["h2_fwd_transfer"][0] == 1 and prof["h2_bwd_transfer"][0] == 1
+    yref = np.zeros(hm.n)
+    oracle.h2_mvm(hm.h2_desc(), -0.5, op, x, yref)
+    assert relerr(y.cpu().numpy(), yref) <= TOL
+    # the level passes of the multi-vector product give the same result
+    X = np.stack([x, rng.standard_normal(hm.n)], axis=1)
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).cuda().T
+    Yd = torch.zeros((2, hm.n), dtype=torch.float64, device="cuda").T
+    hlr.mul_vec(-0.5, op, M, Xd, Yd)
+    torch.cuda.synchronize()
+    prof = M.last_profile()
+    if op == 0:   # op C loops the one-vector product (unit T-form coupling)
+        assert "h2_fwd_tree" not in prof and prof["h2_fwd_transfer"][0] == 3   # parents at levels 4-6
+    assert relerr(Yd[:, 0].cpu().numpy(), yref) <= TOL
+    assert M.device_error() == 0
+    M.free()
