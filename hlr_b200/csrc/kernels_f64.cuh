@@ -168,7 +168,7 @@ __device__ __forceinline__ bool tree_bar_wait(uint64_t* bar) {
 // order, and the result goes to the mirrors of all CTAs of the cluster
 // (distributed shared memory) and to the output array; a cluster barrier
 // ends the level.  Summation order is fixed: the result is deterministic.
-// A copy that never completes stops the CTA's work: it sets bit 1 of the
+// A copy that never completes stops the CTA's work: it sets bit 0 of the
 // error word, keeps taking part in the cluster barriers, and waits
 // (bounded) for its other copies before returning.
 template <int W>

@@ -349,7 +349,8 @@ hlrc_status hlrc_free(hlrc_hmat M);
 
 /* Reads and clears the handle's device error word (synchronous).  Kernels
  * that wait with a bound set it when a wait runs out; the products launched
- * since then are incomplete.  0 means no error.                              */
+ * since then are incomplete.  0 means no error; bit 0 (value 1): a copy wait
+ * of an H^2 tree sweep ran out.                                              */
 hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code);
 
 /* ----------------------------------------------------- host construction
