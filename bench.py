@@ -8,11 +8,13 @@ host by the library's own construction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config c2|c1|c3|c2s|c4|c5] [--precision P] [--nrhs K]
-                    [--no-cpu-baseline] [--no-autotune] [--no-graph] [--h2]
+                    [--no-cpu-baseline] [--no-autotune] [--no-graph] [--h2] [--shard]
 
 Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
-independent replica of the product on its own GPU (the MVM has no exchange
-step on one matrix; weak scaling), time = max over ranks.
+independent replica of the product on its own GPU (weak scaling), time = max
+over ranks.  With --shard the ranks share one product instead: each owns a
+run of rows of about equal bytes, and every step all-gathers x (strong
+scaling).
 """
 from __future__ import annotations
 
@@ -644,6 +646,143 @@ def roofline_from_profile(prof: dict, hbm_peak: float, peak_kind: str, workload:
             "bytes_per_launch": by, "avg_ms": avg_ms, "share_of_step": tot_ms / sum(v[1] for v in prof.values())}
 
 
+def run_shard(args, rank, world, local_rank):
+    """--shard: one product over all ranks.  The rows are cut into runs of
+    about equal stored bytes (hlr_b200.dist.row_cuts); each rank uploads its
+    shard and owns the matching slices of x and y.  A step all-gathers x and
+    multiplies the shard, so the exchange is inside the timed region; value
+    is whole products per second (strong scaling).  The check compares the
+    sharded product with the whole matrix's product on the same GPU."""
+    import torch
+    import torch.distributed as dist
+
+    import hlr_b200 as hlr
+    from hlr_b200 import dist as hdist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ncpu = os.cpu_count() or 1
+    nthreads = max(1, ncpu // max(1, int(os.environ.get("LOCAL_WORLD_SIZE", world))))
+    prob, desc, uniform, prec, _ = make_problem(args.config, nthreads)
+    if uniform or args.h2 or args.config == "c5":
+        raise SystemExit("--shard takes the H-matrix configs (c1, c2, c2s, c4)")
+    if args.precision:
+        prec = args.precision
+    tb = time.perf_counter()
+    hm = hlr.build(prob)
+    t_build = time.perf_counter() - tb
+    n = hm.n
+    cuts = hdist.row_cuts(hm, world)
+    sh = hdist.RowShards(cuts, rank, world)
+    M = hdist.upload_shard(hm, cuts, rank, precision=prec)
+    tuned = tune_handle(M, 1, args)
+    xh = np.random.default_rng(2).standard_normal(n)
+    x_local = torch.from_numpy(xh[sh.r0:sh.r1].copy()).to(dev)
+    y_local = torch.zeros(sh.r1 - sh.r0, dtype=torch.float64, device=dev)
+
+    def local(a, op, xx, yy):
+        hlr.mul_vec(a, op, M, xx, yy)
+
+    def step():
+        sh.mul_vec(2.0, hlr.apply_normal, local, x_local, y_local)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = M.launch_count()
+    with ClockSampler(gpu_uuid(local_rank)) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = M.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world, dev)
+
+    # check: the sharded product against the whole matrix's product
+    Mf = hlr.upload(hm, precision=prec)
+    yfull = torch.zeros(n, dtype=torch.float64, device=dev)
+    hlr.mul_vec(1.0, hlr.apply_normal, Mf, torch.from_numpy(xh).to(dev), yfull)
+    y1 = torch.zeros_like(y_local)
+    sh.mul_vec(1.0, hlr.apply_normal, local, x_local, y1)
+    torch.cuda.synchronize()
+    ref = yfull[sh.r0:sh.r1]
+    err_num = torch.tensor([float(torch.linalg.norm(y1 - ref)) ** 2, float(torch.linalg.norm(ref)) ** 2],
+                           dtype=torch.float64, device=dev)
+    Mf.free()
+    del yfull
+    if world > 1:
+        dist.all_reduce(err_num)
+    err = float(err_num[0].sqrt() / err_num[1].sqrt()) if float(err_num[1]) > 0 else 0.0
+
+    # e2e: this rank's x slice from pinned host memory, the product, y slice back
+    xp = torch.from_numpy(xh[sh.r0:sh.r1].copy()).pin_memory()
+    yp = torch.empty(sh.r1 - sh.r0, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        x_local.copy_(xp, non_blocking=True)
+        y_local.zero_()
+        step()
+        yp.copy_(y_local, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    h1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(h0.elapsed_time(h1), world, dev)
+    info = M.info
+    sizes = torch.tensor([info["algorithmic_bytes"], sh.r1 - sh.r0], dtype=torch.float64, device=dev)
+    all_sizes = [torch.zeros_like(sizes) for _ in range(world)]
+    if world > 1:
+        dist.all_gather(all_sizes, sizes)
+    else:
+        all_sizes = [sizes]
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = peaks()
+    alg0 = info["algorithmic_bytes"]
+    achieved = alg0 / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": args.steps / (ms_max / 1e3), "unit": "MVM/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if prec == "f64" else prec, "data": "synthetic",
+        "config": {"workload": desc + ", rows sharded over the ranks", "n": n, "nrhs": 1, "precision": prec,
+                   "parallelism": f"row shards x{world}", "cuts": cuts,
+                   "shard_algorithmic_bytes": [int(t[0]) for t in all_sizes],
+                   "l2": "inputs larger than L2 (each shard streams its matrix bytes per step)",
+                   "exchange": {"op": "all_gather of x" if world > 1 else "none", "bytes_per_step": 8 * n},
+                   "build_s": round(t_build, 2), "tuning": tuned},
+        "roofline": {"bound": "hbm", "kernel": "rank 0 shard, whole step (exchange included)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": alg0,
+                     "avg_ms": ms / args.steps},
+        "gpu_launches": launches,
+        "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "MVM/s",
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "rel_err_vs_unsharded": err,
+        "cpu_baseline": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def tune_handle(M, nrhs: int, args):
     """Launch shapes from the autotuner, before any timed region: warps per
     CTA for one vector, then (nrhs > 1) the 8-vector kernels against a loop
@@ -687,6 +826,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "bf16", "f16", "mixed", "bfp"],
                     help="storage precision (default: the config's)")
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -704,7 +845,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.config == "c5":
+        if args.shard:
+            run_shard(args, rank, world, local_rank)
+        elif args.config == "c5":
             run_batch(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
