@@ -343,7 +343,9 @@ def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: in
     else:
         d = src.h_desc() if hasattr(src, "h_desc") else src
         check(lib().hlrc_plan_info_h(C.byref(d), C.byref(o), C.byref(inf)), "hlrc_plan_info_h")
-    return {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
+    out = {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
+    out["launches"] = list(inf.launches)   # one-vector product, per op N / T / C
+    return out
 
 
 def _vec_args(v, n: int):

@@ -239,8 +239,38 @@ ArenaLayout arena_layout(const Plan& p) {
     return L;
 }
 
+// Kernel launches of a one-vector product of `op`, counted from the plan as
+// the device passes count them (the dry runs report this; an upload counts
+// its device passes).
+int plan_launches(const Plan& p, int op) {
+    const bool f64 = p.precision == HLRC_PREC_F64;
+    int n = 0;
+    auto formats = [](const auto& segs) {
+        int k = 0;
+        for (int f = 0; f < NFMT; ++f) k += segs[f].empty() ? 0 : 1;
+        return k;
+    };
+    for (const Stage& st : p.stages[op]) {
+        if (st.kind == 0) {
+            const TPass& t = p.tpasses[size_t(st.idx)];
+            n += t.groups.empty() ? 0 : 1;
+            for (int c = 0; c < 3; ++c) n += t.cls_begin[c + 1] > t.cls_begin[c] ? 1 : 0;
+        } else if (st.kind == 1) {
+            const NPass& q = p.npasses[size_t(st.idx)];
+            const int k = formats(q.segs);
+            n += !q.cta_begin.empty() ? 1 : (f64 ? k : (k > 0 ? 1 : 0));
+        } else {
+            const TTPass& t = p.ttpasses[size_t(st.idx)];
+            const int k = formats(t.segs);
+            n += (t.groups.empty() ? 0 : 1) + (t.groups1.empty() ? 0 : 1) + (f64 ? k : (k > 0 ? 1 : 0));
+        }
+    }
+    return n;
+}
+
 void fill_info(const Plan& p, const ArenaLayout& L, hlrc_info& in) {
     std::memset(&in, 0, sizeof(in));
+    for (int op = 0; op < 3; ++op) in.launches[op] = plan_launches(p, op);
     in.n_rows = p.nrows; in.n_cols = p.ncols;
     in.n_dense = p.n_dense; in.n_lowrank = p.n_lowrank;
     in.n_row_tiles = p.n_row_tiles; in.n_col_tiles = p.n_col_tiles;

@@ -99,3 +99,15 @@ def test_h2_tree_sweeps(op):
     assert relerr(Yd[:, 0].cpu().numpy(), yref) <= TOL
     assert M.device_error() == 0
     M.free()
+
+
+def test_plan_info_launches_match_upload():
+    """The dry run's launch counts equal those of the uploaded handle."""
+    cases = [(built("sphere5_h2", CASES["sphere5"]), dict(h2=True)),
+             (built("log1d_2048_h", lambda: hlr.build(hlr.Problem.log1d(2048))), dict(precision="f64")),
+             (built("log1d_2048_h", lambda: hlr.build(hlr.Problem.log1d(2048))), dict(precision="mixed")),
+             (built("log1d_2048_h", lambda: hlr.build(hlr.Problem.log1d(2048))), dict(precision="bfp"))]
+    for hm, kw in cases:
+        M = hlr.upload(hm, **kw)
+        assert hlr.plan_info(hm, **kw)["launches"] == M.info["launches"], kw
+        M.free()

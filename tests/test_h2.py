@@ -84,3 +84,19 @@ def test_h2_plan_info_and_validation(sphere_h2):
     assert e.value.status == 2
     with pytest.raises(hlr.HLRCError):
         hlr.plan_info(sphere_h2, h2=True, precision="mixed")
+
+
+def test_h2_tree_sweeps_planned():
+    """On the sphere with 8192 triangles the one-vector product sweeps the
+    transfer levels below the 32 clusters of level 5 in one launch per tree:
+    op N is the leaf transform, the forward sweep, the level-4 transfer, the
+    couplings, the level-5 transfer, the backward sweep and the leaf pass
+    (the planner and its checks of the sweep's arrays run here, on the
+    host)."""
+    hm = built("sphere5_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=5, nested=True)))
+    info = hlr.plan_info(hm, h2=True)
+    assert info["launches"][0] == 7
+    assert info["launches"][1] == 0   # op T unsupported
+    # without levels below the subtree roots there is no sweep: one pass per level
+    small = built("sphere4_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=4, nested=True)))
+    assert hlr.plan_info(small, h2=True)["launches"][0] == 5
