@@ -142,8 +142,15 @@ class RowShards:
             return x_local
         pad = torch.zeros(self.width, dtype=x_local.dtype, device=x_local.device)
         pad[: x_local.shape[0]] = x_local
-        parts = [torch.empty_like(pad) for _ in range(self.world)]
-        dist.all_gather(parts, pad, group=self.group)
+        if self._nccl():   # one contiguous buffer: no gather list, and no copy when the shards are equal
+            buf = torch.empty(self.world * self.width, dtype=x_local.dtype, device=x_local.device)
+            dist.all_gather_into_tensor(buf, pad, group=self.group)
+            if self.world * self.width == self.n:
+                return buf
+            parts = [buf[i * self.width:(i + 1) * self.width] for i in range(self.world)]
+        else:
+            parts = [torch.empty_like(pad) for _ in range(self.world)]
+            dist.all_gather(parts, pad, group=self.group)
         return torch.cat([parts[i][: self.cuts[i + 1] - self.cuts[i]] for i in range(self.world)])
 
     def reduce(self, part):
