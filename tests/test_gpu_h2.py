@@ -111,3 +111,29 @@ def test_plan_info_launches_match_upload():
         M = hlr.upload(hm, **kw)
         assert hlr.plan_info(hm, **kw)["launches"] == M.info["launches"], kw
         M.free()
+
+
+@pytest.mark.parametrize("op", [0, 2])
+def test_h2_tree_sweeps_high_rank(op):
+    """3D exponential kernel, n = 16384: cluster ranks up to about 110, so
+    transfer matrices span two 64-row pieces, segments are 64 rows tall (two
+    32-row blocks per half-warp) and the shared-memory budget puts the
+    subtree roots below the first level with 32 clusters."""
+    hm = built("exp3d_16384_h2", lambda: hlr.build(hlr.Problem.exp3d(16384, nested=True)))
+    assert hm.h2_desc().nrow_clusters > 0
+    M = hlr.upload(hm, h2=True)
+    M.set_profiling(True)
+    M.last_profile()
+    rng = np.random.default_rng(90 + op)
+    x = rng.standard_normal(hm.n)
+    y0 = rng.standard_normal(hm.n)
+    y = torch.from_numpy(y0.copy()).cuda()
+    hlr.mul_vec(0.5, op, M, torch.from_numpy(x).cuda(), y)
+    torch.cuda.synchronize()
+    prof = M.last_profile()
+    assert prof["h2_fwd_tree"][0] == 1 and prof["h2_bwd_tree"][0] == 1
+    yref = y0.copy()
+    assert oracle.h2_mvm(hm.h2_desc(), 0.5, op, x, yref) == 0
+    assert relerr(y.cpu().numpy() - y0, yref - y0) <= TOL
+    assert M.device_error() == 0
+    M.free()
