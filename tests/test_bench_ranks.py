@@ -58,11 +58,11 @@ def test_single_rank_needs_no_process_group():
 
 
 def test_l2_label_marks_small_workloads_resident():
-    """Products streaming less than twice the 126 MB L2 (C1's 68 MB, the H^2
+    """Products streaming less than twice the 126 MB L2 (C1's 19 MB, the H^2
     form of C3 at 248 MB) are labelled L2-resident; C2's 11 GB is not."""
     sys.path.insert(0, str(ROOT))
     import bench
-    assert bench.l2_label(68e6).startswith("L2-resident")
+    assert bench.l2_label(19e6).startswith("L2-resident")
     assert bench.l2_label(248e6).startswith("L2-resident")
     assert bench.l2_label(295e6).startswith("inputs larger than L2")
     assert bench.l2_label(11.07e9).startswith("inputs larger than L2")
