@@ -137,3 +137,32 @@ def test_h2_tree_sweeps_high_rank(op):
     assert relerr(y.cpu().numpy() - y0, yref - y0) <= TOL
     assert M.device_error() == 0
     M.free()
+
+
+SWEEP_CASES = {
+    "exp3d_2048_leaf16": lambda: hlr.Problem.exp3d(2048, nested=True, leaf_size=16),
+    "log1d_4096_leaf32": lambda: hlr.Problem.log1d(4096, nested=True, leaf_size=32),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SWEEP_CASES))
+@pytest.mark.parametrize("op", [0, 2])
+def test_h2_sweeps_small_leaves(case, op):
+    """Tree sweeps over segments of 2 to 56 rows (ranks 6 to 55) match the
+    oracle to 1e-13."""
+    hm = built(case + "_h2", lambda: hlr.build(SWEEP_CASES[case]()))
+    M = hlr.upload(hm, h2=True)
+    M.set_profiling(True)
+    M.last_profile()
+    rng = np.random.default_rng(120 + op)
+    x = rng.standard_normal(hm.n)
+    y = torch.zeros(hm.n, dtype=torch.float64, device="cuda")
+    hlr.mul_vec(1.0, op, M, torch.from_numpy(x).cuda(), y)
+    torch.cuda.synchronize()
+    prof = M.last_profile()
+    assert "h2_fwd_tree" in prof and "h2_bwd_tree" in prof
+    yref = np.zeros(hm.n)
+    assert oracle.h2_mvm(hm.h2_desc(), 1.0, op, x, yref) == 0
+    assert relerr(y.cpu().numpy(), yref) <= TOL
+    assert M.device_error() == 0
+    M.free()

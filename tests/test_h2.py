@@ -100,3 +100,24 @@ def test_h2_tree_sweeps_planned():
     # without levels below the subtree roots there is no sweep: one pass per level
     small = built("sphere4_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=4, nested=True)))
     assert hlr.plan_info(small, h2=True)["launches"][0] == 5
+
+
+SMALL_TREES = {
+    # (problem, launches of the one-vector op N product with the sweeps)
+    "exp3d_4096_leaf32": (lambda: hlr.Problem.exp3d(4096, nested=True, leaf_size=32), 7),
+    "log1d_4096_leaf32": (lambda: hlr.Problem.log1d(4096, nested=True, leaf_size=32), 11),
+    "sphere4_leaf32": (lambda: hlr.Problem.laplace_sphere(refine=4, nested=True, leaf_size=32), 7),
+    "exp3d_2048_leaf16": (lambda: hlr.Problem.exp3d(2048, nested=True, leaf_size=16), 7),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SMALL_TREES))
+def test_h2_sweeps_planned_for_small_leaves(case):
+    """Leaves of 16 or 32 rows give deep trees at small n: the planner builds
+    the sweeps where at least two levels lie below the subtree roots (not on
+    the 2048-triangle sphere), over segments from 2 to 56 rows tall, and its
+    checks of the sweep arrays pass."""
+    make, launches = SMALL_TREES[case]
+    hm = built(case + "_h2", lambda: hlr.build(make()))
+    info = hlr.plan_info(hm, h2=True)
+    assert info["launches"][0] == launches
