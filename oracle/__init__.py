@@ -47,10 +47,12 @@ def lib() -> C.CDLL:
         L.oracle_hmvm_chunk.argtypes = [vp, f64, ci, vp, vp, ci]
         L.oracle_uniform_mvm.argtypes = [vp, f64, ci, vp, vp, ci]
         L.oracle_h2_mvm.argtypes = [vp, f64, ci, vp, vp]
+        L.oracle_h2_mvm_par.argtypes = [vp, f64, ci, vp, vp, ci]
         L.oracle_dense_matvec.argtypes = [ci, i64, vp, vp, f64, f64, f64, ci, vp, vp, ci]
         L.oracle_leaf_max_error.argtypes = [vp, ci, vp, vp, f64, f64, i64]
         L.oracle_leaf_max_error.restype = f64
-        for f in ("oracle_hmvm_seq", "oracle_hmvm_chunk", "oracle_uniform_mvm", "oracle_h2_mvm", "oracle_dense_matvec"):
+        for f in ("oracle_hmvm_seq", "oracle_hmvm_chunk", "oracle_uniform_mvm", "oracle_h2_mvm", "oracle_h2_mvm_par",
+                  "oracle_dense_matvec"):
             getattr(L, f).restype = ci
         _lib = L
     return _lib
@@ -78,9 +80,12 @@ def hmvm_chunk(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray, nthrea
     _check(lib().oracle_hmvm_chunk(C.addressof(desc), alpha, op, _p(x), _p(y), nthreads), "oracle_hmvm_chunk")
 
 
-def h2_mvm(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray) -> int:
-    """y += alpha op(M) x for an H^2 matrix (hlr::h2::mul_vec); returns the status."""
-    return lib().oracle_h2_mvm(C.addressof(desc), alpha, op, _p(x), _p(y))
+def h2_mvm(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray, nthreads: int = 1) -> int:
+    """y += alpha op(M) x for an H^2 matrix (hlr::h2::mul_vec); returns the
+    status.  nthreads != 1: the threaded form (0 = all cores), bit-identical."""
+    if nthreads == 1:
+        return lib().oracle_h2_mvm(C.addressof(desc), alpha, op, _p(x), _p(y))
+    return lib().oracle_h2_mvm_par(C.addressof(desc), alpha, op, _p(x), _p(y), nthreads)
 
 
 def uniform_mvm(desc, alpha: float, op: int, x: np.ndarray, y: np.ndarray, nthreads: int = 0) -> int:

@@ -121,3 +121,23 @@ def test_h2_sweeps_planned_for_small_leaves(case):
     hm = built(case + "_h2", lambda: hlr.build(make()))
     info = hlr.plan_info(hm, h2=True)
     assert info["launches"][0] == launches
+
+
+@pytest.mark.parametrize("op", [0, 2])
+@pytest.mark.parametrize("case", ["sphere4", "exp3d_2048_leaf16", "log1d_4096_leaf32"])
+def test_h2_threaded_oracle_is_bit_identical(case, op):
+    """The threaded oracle (OpenMP tasks over subtrees, couplings per output
+    cluster, near field per row group) performs the sequential oracle's
+    operations in the same order for every output: identical bits."""
+    if case == "sphere4":
+        hm = built("sphere4_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=4, nested=True)))
+    else:
+        make, _ = SMALL_TREES[case]
+        hm = built(case + "_h2", lambda: hlr.build(make()))
+    rng = np.random.default_rng(3 + op)
+    x = rng.standard_normal(hm.n)
+    y0 = rng.standard_normal(hm.n)
+    ys, yp = y0.copy(), y0.copy()
+    assert oracle.h2_mvm(hm.h2_desc(), 1.75, op, x, ys) == 0
+    assert oracle.h2_mvm(hm.h2_desc(), 1.75, op, x, yp, nthreads=4) == 0
+    assert np.array_equal(ys, yp)
