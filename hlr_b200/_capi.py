@@ -101,6 +101,7 @@ PROTOTYPES = {
                                          C.POINTER(hlrc_info)]),
     "hlrc_upload_h2": (C.c_int, [C.POINTER(hlrc_h2_desc), C.POINTER(hlrc_options), C.POINTER(C.c_void_p)]),
     "hlrc_plan_info_h2": (C.c_int, [C.POINTER(hlrc_h2_desc), C.POINTER(hlrc_options), C.POINTER(hlrc_info)]),
+    "hlrc_row_cuts": (C.c_int, [C.POINTER(hlrc_h_desc), C.c_int, C.POINTER(i64)]),
     "hlrc_mvm": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64, C.c_void_p]),
     "hlrc_mvm_host": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64]),
     "hlrc_mvm_noalloc": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -1838,3 +1838,52 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
 }
 
 }  // namespace hlrc
+
+// Row partition of an H-matrix for one product shared by several processes:
+// candidate cuts are the rows no leaf straddles; cut k is the candidate
+// whose preceding leaves' stored bytes are closest to k/parts of the total
+// (the last of equally close ones).  No counterpart in HLR's product.
+extern "C" hlrc_status hlrc_row_cuts(const hlrc_h_desc* desc, int parts, int64_t* cuts) {
+    using namespace hlrc;
+    clear_error();
+    if (!desc || !cuts || parts < 1) return fail(HLRC_ERR_ARG, "hlrc_row_cuts: null argument or parts < 1");
+    const int64_t n = desc->nrows;
+    if (n < 0 || desc->nblocks < 0 || (desc->nblocks > 0 && !desc->blocks))
+        return fail(HLRC_ERR_ARG, "hlrc_row_cuts: bad descriptor");
+    std::vector<int64_t> cover(size_t(n) + 2, 0);
+    std::vector<double> done(size_t(n) + 1, 0.0);   // bytes of the leaves ending at a row
+    for (int64_t i = 0; i < desc->nblocks; ++i) {
+        const hlrc_block& b = desc->blocks[i];
+        const int64_t r0 = b.row0, r1 = b.row0 + b.nrows;
+        if (r0 < 0 || b.nrows < 0 || r1 > n) return fail(HLRC_ERR_SHAPE, "hlrc_row_cuts: block %lld outside the rows",
+                                                          (long long)i);
+        if (r1 - r0 > 1) {
+            ++cover[size_t(r0) + 1];
+            --cover[size_t(r1)];
+        }
+        done[size_t(r1)] += b.kind == HLRC_LEAF_DENSE ? 8.0 * double(b.nrows) * double(b.ncols)
+                                                      : 8.0 * double(b.rank) * double(b.nrows + b.ncols);
+    }
+    std::vector<int64_t> cand;
+    std::vector<double> prefix;
+    int64_t run = 0;
+    double acc = 0.0;
+    for (int64_t c = 0; c <= n; ++c) {
+        run += cover[size_t(c)];
+        acc += done[size_t(c)];
+        if (run == 0) {
+            cand.push_back(c);
+            prefix.push_back(acc);
+        }
+    }
+    const double total = prefix.empty() ? 0.0 : prefix.back();
+    cuts[0] = 0;
+    size_t j = 0;
+    for (int k = 1; k < parts; ++k) {
+        const double target = total * k / parts;
+        while (j + 1 < cand.size() && std::fabs(prefix[j + 1] - target) <= std::fabs(prefix[j] - target)) ++j;
+        cuts[k] = std::max(cuts[k - 1], cand.empty() ? int64_t(0) : cand[j]);
+    }
+    cuts[parts] = n;
+    return HLRC_OK;
+}

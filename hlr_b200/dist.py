@@ -43,40 +43,15 @@ def row_cuts(src, parts: int) -> List[int]:
     """Cut positions 0 = c_0 <= c_1 <= ... <= c_parts = nrows of an H-matrix
     (HostMatrix, LeafList or ``hlrc_h_desc``): no leaf block straddles a
     cut, and the stored bytes of the leaves between consecutive cuts are
-    about equal.  Shards may be empty when there are fewer cut positions than
-    parts."""
+    about equal (``hlrc_row_cuts``).  Shards may be empty when there are
+    fewer cut positions than parts."""
+    from . import check, lib
     if parts < 1:
         raise ValueError("parts must be >= 1")
     desc = src.h_desc() if hasattr(src, "h_desc") else src
-    n = int(desc.nrows)
-    blocks = _blocks(desc)
-    # a position c is a cut when no block has row0 < c < row0 + nrows
-    cover = [0] * (n + 2)
-    done = [0] * (n + 1)   # bytes of blocks that end at row e
-    for b in blocks:
-        r0, r1 = int(b.row0), int(b.row0) + int(b.nrows)
-        if r1 - r0 > 1:
-            cover[r0 + 1] += 1
-            cover[r1] -= 1
-        done[r1] += _block_bytes(b)
-    cand, prefix = [], []
-    run, acc = 0, 0
-    for c in range(n + 1):
-        run += cover[c]
-        acc += done[c]
-        if run == 0:
-            cand.append(c)
-            prefix.append(acc)
-    total = prefix[-1] if prefix else 0
-    cuts = [0]
-    j = 0
-    for k in range(1, parts):
-        target = total * k / parts
-        while j + 1 < len(cand) and abs(prefix[j + 1] - target) <= abs(prefix[j] - target):
-            j += 1
-        cuts.append(max(cuts[-1], cand[j]))
-    cuts.append(n)
-    return cuts
+    out = (C.c_int64 * (parts + 1))()
+    check(lib().hlrc_row_cuts(C.byref(desc), parts, out), "hlrc_row_cuts")
+    return [int(c) for c in out]
 
 
 def shard_desc(src, r0: int, r1: int) -> _capi.hlrc_h_desc:

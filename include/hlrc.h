@@ -258,6 +258,17 @@ hlrc_status hlrc_plan_info_uniform(const hlrc_uniform_desc* desc,
                                    const hlrc_options* opts, hlrc_info* info);
 hlrc_status hlrc_plan_info_h2(const hlrc_h2_desc* desc, const hlrc_options* opts, hlrc_info* info);
 
+/* Row partition of an H-matrix for one product shared by `parts` processes
+ * (one per GPU): cuts[0] = 0 <= cuts[1] <= ... <= cuts[parts] = nrows (cuts
+ * holds parts + 1 entries), no leaf straddles a cut, and the leaves between
+ * consecutive cuts hold about equal stored bytes.  Rank r then uploads the
+ * leaves of rows [cuts[r], cuts[r+1]) as an (rows x ncols) H-matrix, rows
+ * shifted by -cuts[r], and owns those entries of x and y: op N all-gathers
+ * x before its product, op T / C sums the ranks' full-length results (the
+ * per-cluster ownership of y in HLR's mul_vec_cl, tbb/detail/arith.hh:
+ * 406-448, spread over processes).  Host only.                              */
+hlrc_status hlrc_row_cuts(const hlrc_h_desc* desc, int parts, int64_t* cuts);
+
 /* y := y + alpha * op(M) * x on `stream`.
  * x: ncols(op) x nrhs device array (leading dimension ldx),
  * y: nrows(op) x nrhs device array (leading dimension ldy).

@@ -139,3 +139,19 @@ def test_sharded_product_two_gloo_ranks():
     for rank, _, res in results:
         for op, (err, ref) in res.items():
             assert err <= 1e-13 * ref, (rank, op)
+
+
+def test_row_cuts_c_abi_arguments():
+    """hlrc_row_cuts refuses a missing descriptor, parts < 1 and leaves
+    outside the rows (HLRC_ERR_ARG / HLRC_ERR_SHAPE)."""
+    import ctypes as C
+    hm = _log1d()
+    d = hm.h_desc()
+    out = (C.c_int64 * 3)()
+    assert hlr.lib().hlrc_row_cuts(None, 2, out) == 1
+    assert hlr.lib().hlrc_row_cuts(C.byref(d), 0, out) == 1
+    bad = hdist.shard_desc(hm, 0, hm.n)
+    bad.nrows = 100   # leaves now reach past the rows
+    assert hlr.lib().hlrc_row_cuts(C.byref(bad), 2, out) == 2
+    assert hlr.lib().hlrc_row_cuts(C.byref(d), 2, out) == 0
+    assert list(out) == hdist.row_cuts(hm, 2)
