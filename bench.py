@@ -284,6 +284,125 @@ def run_reference_batch(args, nthreads):
     print(json.dumps(line), flush=True)
 
 
+def products_per_graph(steps: int) -> int:
+    """Products captured in one CUDA graph: the reference times runs of
+    nmvm = 50 products; here the K timed products are split into at least
+    five equal runs where K allows it (each run one graph replay), so that
+    every line carries a min / median / max over runs."""
+    want = min(steps, 5)
+    return max(d for d in range(1, min(50, steps) + 1) if steps % d == 0 and steps // d >= want)
+
+
+def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int, dev, clocks_id=None):
+    """Times `steps` products of handle M issued by step() on torch's current
+    stream: `warmup` untimed products, then the timed region bracketed by a
+    barrier and synchronisations, as replays of one CUDA graph of
+    products_per_graph(steps) products (or direct launches).  Per-pass CUDA
+    events of the handle's profiling API are recorded inside the graph and
+    read after the last replay.  Returns a dict with the region's ms, the
+    per-run min / median / max per product, the pass profile, the kernels
+    launched per product and the clock samples."""
+    import torch
+    import torch.distributed as dist
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = M.launch_count()
+    step()                      # one more warm-up product, counting its launches
+    torch.cuda.synchronize()
+    per_product = M.launch_count() - l0
+    M.set_profiling(True)
+    M.last_profile()  # clear
+    graph, per_graph = None, 0
+    if use_graph:
+        per_graph = products_per_graph(steps)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(per_graph):
+                step()
+        graph.replay()          # untimed
+        torch.cuda.synchronize()
+        M.last_profile()        # drop the untimed replay's pass records
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = M.launch_count()
+    marks = [e0]
+    with ClockSampler(clocks_id) if clocks_id is not None else _NoClocks() as clocks:
+        e0.record(stream)
+        if graph is not None:
+            for _ in range(steps // per_graph):
+                graph.replay()
+                marks.append(torch.cuda.Event(enable_timing=True))
+                marks[-1].record(stream)
+        else:
+            for _ in range(steps):
+                step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = per_product * steps if graph is not None else M.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    runs = None
+    if graph is not None:
+        rt = [a.elapsed_time(b) / per_graph for a, b in zip(marks[:-1], marks[1:])]
+        runs = {"min": min(rt), "median": statistics.median(rt), "max": max(rt), "runs": len(rt)}
+    prof = M.last_profile()
+    M.set_profiling(False)
+    del graph
+    return {"ms": ms, "runs": runs, "prof": prof, "per_product": per_product, "launches": launches,
+            "per_graph": per_graph, "clocks": clocks.summary()}
+
+
+class _NoClocks:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+    def summary(self):
+        return None
+
+
+def reduced_arms(hlr, hm, x, n, alpha, args, world, dev, y_oracle, v64, peak):
+    """The mixed-precision half of the metric on the same matrix and x: the
+    block floating point store (24/16-bit, VALR bit rates) and the VALR mixed
+    FP32/FP16 store, each timed like the FP64 arm, with its error against
+    the oracle's FP64 product and its speed-up over the FP64 GPU product."""
+    import torch
+    hbm_peak, peak_kind = peak
+    out = {}
+    for prec in args.reduced:
+        Mr = hlr.upload(hm, precision=prec, max_nrhs=1)
+        tuned = tune_handle(Mr, 1, args)
+        yr = torch.zeros(n, dtype=torch.float64, device=dev)
+        r = time_products(Mr, lambda: hlr.mul_vec(alpha, hlr.apply_normal, Mr, x, yr), args.steps, args.warmup,
+                          not args.no_graph, world, dev, gpu_uuid(dev.index))
+        yr.zero_()
+        hlr.mul_vec(1.0, hlr.apply_normal, Mr, x, yr)
+        torch.cuda.synchronize()
+        yh = yr.cpu().numpy()
+        ms_max = max_over_ranks(r["ms"], world, dev)
+        value = world * args.steps / (ms_max / 1e3)
+        info = Mr.info
+        arm = {"value": value, "unit": "MVM/s", "ms_per_step": ms_max / args.steps,
+               "ms_per_product_of_runs": r["runs"], "speedup_vs_fp64": (value / world) / v64,
+               "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": info["algorithmic_bytes"],
+               "hbm_gbs": info["algorithmic_bytes"] / (ms_max / 1e3 / args.steps) / 1e9,
+               "roofline": roofline_from_profile(r["prof"], hbm_peak, peak_kind, args.config + "/" + prec),
+               "gpu_launches": r["launches"], "tuning": tuned, "clocks": r["clocks"]}
+        if y_oracle is not None:
+            arm["rel_err_vs_oracle"] = float(np.linalg.norm(yh - y_oracle) / np.linalg.norm(y_oracle))
+        out[prec] = arm
+        Mr.free()
+        del yr
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -319,64 +438,14 @@ def run_ours(args, rank, world, local_rank):
     x = dev_vec(xh)
     y = dev_vec(np.zeros((nrhs, n)))
     alpha = 2.0
-    stream = torch.cuda.current_stream(dev)
 
     def step():
         hlr.mul_vec(alpha, hlr.apply_normal, M, x, y)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    l0 = M.launch_count()
-    step()                      # one more warm-up product, counting its launches
-    torch.cuda.synchronize()
-    per_product = M.launch_count() - l0
-    M.set_profiling(True)
-    M.last_profile()  # clear
-    # the reference's protocol: runs of nmvm = 50 products; here each run is
-    # one CUDA graph of `per_graph` captured products, replayed steps/per_graph
-    # times (per-pass profiling events are graph nodes, read after the last
-    # replay)
-    graph, per_graph = None, 0
-    if not args.no_graph:
-        per_graph = max(d for d in range(1, min(50, args.steps) + 1) if args.steps % d == 0)
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            for _ in range(per_graph):
-                step()
-        graph.replay()          # untimed
-        torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = M.launch_count()
-    with ClockSampler(gpu_uuid(local_rank)) as clocks:
-        e0.record(stream)
-        if graph is not None:
-            marks = [e0]
-            for _ in range(args.steps // per_graph):
-                graph.replay()
-                marks.append(torch.cuda.Event(enable_timing=True))
-                marks[-1].record(stream)
-        else:
-            for _ in range(args.steps):
-                step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-    timed_launches = per_product * args.steps if graph is not None else M.launch_count() - launches0
-    if world > 1:
-        dist.barrier()
-    ms = e0.elapsed_time(e1)
-    # per-product time of each run (graph replay): min / median / max, as the
-    # reference reports its runs
-    runs = None
-    if graph is not None:
-        rt = [a.elapsed_time(b) / per_graph for a, b in zip(marks[:-1], marks[1:])]
-        runs = {"min": min(rt), "median": statistics.median(rt), "max": max(rt), "runs": len(rt)}
-    prof = M.last_profile()
-    M.set_profiling(False)
-    del graph
+    # the reference's protocol: runs of products (nmvm = 50 there); here each
+    # run is one replay of a CUDA graph of captured products
+    tm = time_products(M, step, args.steps, args.warmup, not args.no_graph, world, dev, gpu_uuid(local_rank))
+    ms, runs, prof, timed_launches, per_graph = tm["ms"], tm["runs"], tm["prof"], tm["launches"], tm["per_graph"]
     ms_max = max_over_ranks(ms, world, dev)
 
     # correctness of the timed path: one product from zero; column 0 is
@@ -386,6 +455,19 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ygpu_all = (yc if nrhs > 1 else yc[:, None]).cpu().numpy()
     ygpu = ygpu_all[:, 0].copy()
+    # the oracle's FP64 product of column 0 (the checker of every arm)
+    y_oracle = None
+    if world == 1 and not (args.no_cpu_baseline and not args.reduced):
+        d_or = hm.h2_desc() if args.h2 else (hm.uniform_desc() if uniform else hm.h_desc())
+        y_oracle = np.zeros(n)
+        cpu_mvm(hm, uniform, d_or, np.ascontiguousarray(xh[0]), y_oracle, os.cpu_count() or 1)
+
+    # the metric's reduced-precision half, on the same matrix and x: only for
+    # the FP64 one-vector H-matrix line (the default)
+    reduced = None
+    if args.reduced and prec == "f64" and nrhs == 1 and not uniform and not args.h2:
+        v64 = args.steps / (ms / 1e3)
+        reduced = reduced_arms(hlr, hm, x, n, alpha, args, world, dev, y_oracle, v64, peaks())
 
     # reduced precision: the FP64 GPU product of the same matrix, timed the
     # same way, is the error reference and the speed-up denominator
@@ -442,9 +524,10 @@ def run_ours(args, rank, world, local_rank):
     hbm_peak, peak_kind = peaks()
     # every right-hand side counts as one matrix-vector product
     value = world * args.steps * nrhs / (ms_max / 1e3)
-    alg = info["algorithmic_bytes"]
-    passes = (nrhs + 7) // 8 if nrhs > 1 else 1      # the matrix is streamed once per block of 8 vectors
-    gbs = alg * passes / (ms_max / 1e3 / args.steps) / 1e9
+    # HLR's mul_vec_datasize for nrhs vectors: the matrix once, the vectors
+    # (x read, y read and written) once per right-hand side
+    alg = info["algorithmic_bytes"] + (nrhs - 1) * 2 * 8 * (info["n_rows"] + info["n_cols"])
+    gbs = alg / (ms_max / 1e3 / args.steps) / 1e9
     # the summaries key a workload as config[/precision][/nrhs]
     wl = (args.config + ("/h2" if args.h2 else "") + ("" if prec == "f64" else "/" + prec)
           + ("" if nrhs == 1 else f"/{nrhs}"))
@@ -467,8 +550,10 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": timed_launches,
         "e2e": {"value": world * ksteps * nrhs / (e2e_ms / 1e3), "unit": "MVM/s",
                 "h2d_bytes_per_step": 2 * 8 * n * nrhs, "d2h_bytes_per_step": 8 * n * nrhs},
-        "clocks": clocks.summary(),
+        "clocks": tm["clocks"],
     }
+    if reduced is not None:
+        line["reduced"] = reduced
     if fp64 is not None:
         fp64["speedup"] = (value / world) / fp64["value"]
         line["fp64_gpu"] = fp64
@@ -476,11 +561,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu_baseline and world == 1:
         d = hm.h2_desc() if args.h2 else (hm.uniform_desc() if uniform else hm.h_desc())
         ncores = os.cpu_count() or 1
-        yo = np.zeros(n)
-        t0 = time.perf_counter()
-        cpu_mvm(hm, uniform, d, np.ascontiguousarray(xh[0]), yo, ncores)
-        t1 = time.perf_counter() - t0
-        line["rel_err_vs_oracle"] = float(np.linalg.norm(ygpu - yo) / np.linalg.norm(yo))
+        line["rel_err_vs_oracle"] = float(np.linalg.norm(ygpu - y_oracle) / np.linalg.norm(y_oracle))
         reps, el = 0, 0.0
         budget = 15.0
         while el < budget and reps < 50:
@@ -609,11 +690,11 @@ def run_batch(args, rank, world, local_rank):
         return
     hbm_peak, peak_kind = peaks()
     per_step = ms / 1e3 / args.steps
-    passes = (nrhs + 7) // 8        # the matrix is streamed once per block of 8 right-hand sides
     value = world * nrhs * count / per_step
     v64 = nrhs * count / (ms64 / 1e3 / args.steps)
     v64_1 = count / (ms64_1 / 1e3 / args.steps)
-    gbs = Alow.info["matrix_bytes"] * passes / per_step / 1e9
+    # mul_vec_datasize for nrhs vectors: the matrix once, x and y per vector
+    gbs = (Alow.info["matrix_bytes"] + nrhs * 2 * 8 * 2 * N) / per_step / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -843,7 +924,11 @@ def main():
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")
     ap.add_argument("--shard", action="store_true",
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
+    ap.add_argument("--reduced", default="bfp,mixed",
+                    help="reduced-precision stores timed beside the FP64 one-vector H-matrix line "
+                         "(comma list of bfp, mixed, f32, f16, bf16; 'none' for none)")
     args = ap.parse_args()
+    args.reduced = [] if args.reduced in ("", "none") else args.reduced.split(",")
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -268,6 +268,39 @@ class DeviceMatrix:
             pass
 
 
+class Workspace:
+    """Caller-owned scratch for one handle's products (``hlrc_workspace``).
+
+    A DeviceMatrix is immutable; all the scratch a product writes lives in a
+    workspace.  Products of one handle on several streams run concurrently
+    when each passes its own workspace to :func:`mul_vec` — the counterpart
+    of calling ``hlr::tbb::mul_vec`` on one matrix from several threads with
+    different y (tbb/arith.hh:312-323).  ``max_nrhs > 1`` adds the
+    multi-vector kernels' scratch.
+    """
+
+    def __init__(self, M: "DeviceMatrix", max_nrhs: int = 1):
+        h = C.c_void_p()
+        check(lib().hlrc_workspace_create(M.handle, int(max_nrhs), C.byref(h)), "hlrc_workspace_create")
+        self._h = h
+        self.device_matrix = M
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def free(self) -> None:
+        if self._h:
+            lib().hlrc_workspace_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
            mixed_eps: float = 1e-6, device: int = -1, h2: bool = False) -> DeviceMatrix:
     """Flatten and upload a matrix: ``src`` is a HostMatrix, LeafList or
@@ -375,11 +408,14 @@ def _vec_args(v, n: int):
     return a.ctypes.data, a.shape[1], a.shape[0], False
 
 
-def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
+def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None, workspace: Optional[Workspace] = None) -> None:
     """y += alpha * op(M) x  (drop-in for hlr::tbb::mul_vec / hlr::seq::mul_vec).
 
     Device tensors run on ``stream`` (default: torch's current stream) without
     synchronising; numpy arrays take the host-buffer path (copies included).
+    With ``workspace`` (device tensors only) the product's scratch is that
+    workspace instead of the handle's, so products on other streams with
+    other workspaces may run at the same time.
     """
     xp, xn, ldx, xdev = _vec_args(x, 0)
     yp, yn, ldy, ydev = _vec_args(y, 0)
@@ -395,9 +431,15 @@ def mul_vec(alpha: float, op: int, M: DeviceMatrix, x, y, stream=None) -> None:
         if stream is None:
             import torch
             stream = torch.cuda.current_stream(x.device).cuda_stream
+        if workspace is not None:
+            check(lib().hlrc_mvm_ws(M.handle, workspace.handle, float(alpha), int(op), C.c_void_p(xp),
+                                    C.c_void_p(yp), xn, ldx, ldy, C.c_void_p(stream)), "hlrc_mvm_ws")
+            return
         check(lib().hlrc_mvm(M.handle, float(alpha), int(op), C.c_void_p(xp), C.c_void_p(yp), xn, ldx, ldy,
                              C.c_void_p(stream)), "hlrc_mvm")
     else:
+        if workspace is not None:
+            raise ValueError("a workspace serves device vectors; host vectors use the handle's staging")
         check(lib().hlrc_mvm_host(M.handle, float(alpha), int(op), C.c_void_p(xp), C.c_void_p(yp), xn, ldx, ldy),
               "hlrc_mvm_host")
 
@@ -425,5 +467,5 @@ class uniform:  # namespace mirroring hlr::tbb::uniform
 
 __all__ = [
     "apply_normal", "apply_transposed", "apply_adjoint", "Problem", "HostMatrix", "LeafList", "DeviceMatrix",
-    "build", "upload", "mul_vec", "mvm", "uniform", "h2", "HLRCError", "PRECISIONS",
+    "build", "upload", "mul_vec", "mvm", "uniform", "h2", "HLRCError", "PRECISIONS", "Workspace",
 ]

@@ -71,7 +71,7 @@ class hlrc_info(C.Structure):
                 ("n_row_tiles", i64), ("n_col_tiles", i64), ("matrix_bytes", i64),
                 ("algorithmic_bytes", i64), ("flops", i64), ("workspace_bytes", i64),
                 ("device_bytes", i64), ("precision", i32), ("kind", i32), ("max_rank", i32),
-                ("launches", i32 * 3), ("reserved", i32 * 2)]
+                ("launches", i32 * 3), ("scratch_bytes", i64)]
 
 
 class hlrc_tuning(C.Structure):
@@ -106,6 +106,10 @@ PROTOTYPES = {
     "hlrc_mvm_host": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64]),
     "hlrc_mvm_noalloc": (C.c_int, [C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hlrc_get_info": (C.c_int, [C.c_void_p, C.POINTER(hlrc_info)]),
+    "hlrc_workspace_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "hlrc_mvm_ws": (C.c_int, [C.c_void_p, C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64,
+                              C.c_void_p]),
+    "hlrc_workspace_free": (C.c_int, [C.c_void_p]),
     "hlrc_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
     "hlrc_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
     "hlrc_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -126,12 +127,14 @@ struct hlrc_hmat_s {
     char* mr_arena = nullptr;
     double *mr_x = nullptr, *mr_t = nullptr, *mr_t2 = nullptr, *mr_part = nullptr;
     char* mr_tables = nullptr;   // column streams of reduced-precision stores (MSeg / MCol)
-    // host-pointer entry point staging
+    // host-pointer entry point staging (hlrc_mvm_host holds host_mu while it
+    // uses these and the handle's workspace)
     double* hx = nullptr;
     double* hy = nullptr;
     size_t hx_elems = 0, hy_elems = 0;
+    std::mutex host_mu;
     int* dev_err = nullptr;   // device error word (bounded waits that ran out)
-    int64_t launches = 0;     // kernels launched by this handle
+    std::atomic<int64_t> launches{0};   // kernels launched by this handle (any thread)
     std::vector<const char*> names[3];   // per-pass profile names (empty: fixed names)
     // launch shapes picked by the autotuner (hlrc_set_tuning)
     int nform_warps = 8;      // warps per CTA, single-vector N-form
@@ -279,6 +282,8 @@ void fill_info(const Plan& p, const ArenaLayout& L, hlrc_info& in) {
     in.flops = p.flops;
     in.workspace_bytes = int64_t(L.total - L.t);
     in.device_bytes = int64_t(L.total);
+    in.scratch_bytes = int64_t(sizeof(double)) * (std::max<int64_t>(1, p.n_t) + std::max<int64_t>(1, p.n_t2) +
+                                                  int64_t(L.part_elems));
     in.precision = p.precision;
     in.kind = p.kind;
     in.max_rank = p.max_rank;
@@ -459,6 +464,38 @@ hlrc_status enable_tc_smem(int dev) {
                                    tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32)));
     done.push_back(dev);
     return HLRC_OK;
+}
+
+// Does the handle have 8-vector kernels?  Block floating point stores loop
+// the one-vector kernels instead.
+bool has_multi_kernels(hlrc_hmat M) { return M->precision != HLRC_PREC_BFP; }
+
+// Sizes of the multi-vector scratch of a handle: x, t, t2 and the partial
+// sums as row-major blocks of MR_RB vectors, each array 256-byte aligned.
+struct MrSizes {
+    size_t nx = 0, nt = 0, nt2 = 0, np = 0, bytes = 0;
+    void carve(char* base, double*& x, double*& t, double*& t2, double*& part) const {
+        size_t off = 0;
+        auto take = [&](size_t elems) {
+            double* q = reinterpret_cast<double*>(base + off);
+            off = align_up(off + elems * sizeof(double), 256);
+            return q;
+        };
+        x = take(nx);
+        t = take(nt);
+        t2 = take(nt2);
+        part = take(np);
+    }
+};
+
+MrSizes mr_sizes(hlrc_hmat M) {
+    MrSizes z;
+    z.nx = size_t(std::max(M->nrows, M->ncols)) * MR_RB;
+    z.nt = size_t(std::max<int64_t>(1, M->n_t)) * MR_RB;
+    z.nt2 = size_t(std::max<int64_t>(1, M->n_t2)) * MR_RB;
+    z.np = size_t(std::max<int64_t>(1, M->n_part)) * MR_RB;
+    z.bytes = (z.nx + z.nt + z.nt2 + z.np) * sizeof(double) + 4 * 256;
+    return z;
 }
 
 hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
@@ -649,29 +686,17 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     fill_info(p, L, hp->info);
     // the 8-vector kernels take FP64, FP32 and FP16/BF16 columns; block
     // floating point (BFP) stores loop the one-vector kernels instead
-    if (o.max_nrhs > 1 && p.precision != HLRC_PREC_BFP) {
-        const size_t nx = size_t(std::max(p.nrows, p.ncols)) * MR_RB;
-        const size_t nt = size_t(std::max<int64_t>(1, p.n_t)) * MR_RB, nt2 = size_t(std::max<int64_t>(1, p.n_t2)) * MR_RB;
-        const size_t np = size_t(std::max<int64_t>(1, hp->n_part)) * MR_RB;
-        const size_t bytes = (nx + nt + nt2 + np) * sizeof(double) + 4 * 256;
-        e = cudaMalloc(&hp->mr_arena, bytes);
+    if (o.max_nrhs > 1 && has_multi_kernels(hp)) {
+        const MrSizes z = mr_sizes(hp);
+        e = cudaMalloc(&hp->mr_arena, z.bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
             cleanup();
-            return fail(HLRC_ERR_OOM, "multi-RHS workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
+            return fail(HLRC_ERR_OOM, "multi-RHS workspace of %zu bytes: %s", z.bytes, cudaGetErrorString(e));
         }
-        size_t off = 0;
-        auto carve = [&](size_t elems) {
-            double* q = reinterpret_cast<double*>(hp->mr_arena + off);
-            off = align_up(off + elems * sizeof(double), 256);
-            return q;
-        };
-        hp->mr_x = carve(nx);
-        hp->mr_t = carve(nt);
-        hp->mr_t2 = carve(nt2);
-        hp->mr_part = carve(np);
-        hp->info.workspace_bytes += int64_t(bytes);
-        hp->info.device_bytes += int64_t(bytes);
+        z.carve(hp->mr_arena, hp->mr_x, hp->mr_t, hp->mr_t2, hp->mr_part);
+        hp->info.workspace_bytes += int64_t(z.bytes);
+        hp->info.device_bytes += int64_t(z.bytes);
     }
     if (p.precision != HLRC_PREC_F64) {
         const hlrc_status st = upload_streams(p, hp);
@@ -693,16 +718,30 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     return HLRC_OK;
 }
 
-// Scratch used by one product: the coefficient vectors and the partial sums.
+// Scratch used by one product: the coefficient vectors and the partial sums
+// of a one-vector product, and (when present) the same arrays as row-major
+// blocks of MR_RB vectors for the multi-vector kernels.  A product reads
+// every scratch entry only after writing it in the same product.
 struct Workspace {
-    double* t;
-    double* t2;
-    double* part;
-    bool profile;
+    double* t = nullptr;
+    double* t2 = nullptr;
+    double* part = nullptr;
+    double* mr_x = nullptr;      // null: no multi-vector arrays
+    double* mr_t = nullptr;
+    double* mr_t2 = nullptr;
+    double* mr_part = nullptr;
+    bool profile = false;        // record per-pass events in the handle's profile
 };
 
-Workspace handle_workspace(hlrc_hmat M) { return {M->ws_t, M->ws_t2, M->part, M->profiling}; }
-bool ws_profile(hlrc_hmat M) { return M->profiling; }
+// the handle's own workspace (hlrc_mvm, hlrc_mvm_host); only products on it
+// are profiled
+Workspace handle_workspace(hlrc_hmat M) {
+    Workspace w;
+    w.t = M->ws_t; w.t2 = M->ws_t2; w.part = M->part;
+    w.mr_x = M->mr_x; w.mr_t = M->mr_t; w.mr_t2 = M->mr_t2; w.mr_part = M->mr_part;
+    w.profile = M->profiling;
+    return w;
+}
 
 double* bind(const Workspace& ws, int name, const double* x, double* y) {
     switch (name) {
@@ -760,9 +799,20 @@ bool debug_sync() {
     return on;
 }
 
+// A stream that is being captured is left alone: a synchronisation there
+// would invalidate the capture.
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
 #define HLRC_AFTER_LAUNCH(name)                                                                        \
     do {                                                                                               \
-        if (debug_sync()) {                                                                            \
+        if (debug_sync() && !capturing(s)) {                                                           \
             const cudaError_t e_ = cudaStreamSynchronize(s);                                           \
             if (e_ != cudaSuccess) return fail(HLRC_ERR_CUDA, "%s: %s", name, cudaGetErrorString(e_)); \
         }                                                                                              \
@@ -901,8 +951,8 @@ const std::vector<Stage>& mr_stages(hlrc_hmat M, int op) {
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
 // the multi-RHS workspace and no unit T-form stage (the uniform-H adjoint
 // coupling runs per vector).
-bool multi_rhs_ok(hlrc_hmat M, int op, int nrhs) {
-    if (nrhs < 2 || nrhs < M->mr_min_nrhs || !M->mr_arena) return false;
+bool multi_rhs_ok(hlrc_hmat M, const Workspace& ws, int op, int nrhs) {
+    if (nrhs < 2 || nrhs < M->mr_min_nrhs || !ws.mr_x) return false;
     for (const Stage& st : mr_stages(M, op))
         if (st.kind == 0) return false;
     return true;
@@ -910,13 +960,13 @@ bool multi_rhs_ok(hlrc_hmat M, int op, int nrhs) {
 
 // y := y + alpha op(M) X for nrhs column vectors, MR_RB at a time: the matrix
 // is streamed once per block instead of once per vector.
-hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int64_t ldx, double* Y, int64_t ldy,
-                      int nrhs, cudaStream_t s) {
+hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* X, int64_t ldx,
+                      double* Y, int64_t ldy, int nrhs, cudaStream_t s) {
     const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
     for (int r0 = 0; r0 < nrhs; r0 += MR_RB) {
         const int nr = std::min(MR_RB, nrhs - r0);
         const int64_t tot = nx * MR_RB;
-        k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, M->mr_x);
+        k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, ws.mr_x);
         M->launches += 1;
         HLRC_AFTER_LAUNCH("rows_from_cols");
         for (const Stage& st : mr_stages(M, op)) {
@@ -928,7 +978,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
             }
         }
         auto vec = [&](int name) -> double* {
-            return name == V_X ? M->mr_x : (name == V_T ? M->mr_t : M->mr_t2);
+            return name == V_X ? ws.mr_x : (name == V_T ? ws.mr_t : ws.mr_t2);
         };
         auto omap = [&](int name) -> OutMap {
             if (name == V_Y) return OutMap{Y + int64_t(r0) * ldy, 1, ldy, nr};
@@ -941,16 +991,16 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
                 const int add = tp.mode != OUT_SET;
                 const double alpha = tp.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
                 const OutMap om = omap(tp.out);
-                if (ws_profile(M)) prof_begin(M, stage_name(M, 2, st.idx), tp.alg_bytes, s);
+                if (ws.profile) prof_begin(M, stage_name(M, 2, st.idx), tp.alg_bytes, s);
                 constexpr int TW = DMMA_WARPS;
                 if (M->precision == HLRC_PREC_F64) {
                     if (tp.nsegs[FMT_F64] > 0)
                         k_ttform_dmma<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
-                            tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, M->mr_part,
+                            tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, ws.mr_part,
                             alpha, add);
                 } else {
                     const int n32 = tp.nmseg[FMT_F32];
-                    float* fpart = reinterpret_cast<float*>(M->mr_part);
+                    float* fpart = reinterpret_cast<float*>(ws.mr_part);
                     if (tp.nmseg[FMT_BF16] > 0)
                         k_ttform_mr<FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
@@ -958,18 +1008,18 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
                         k_ttform_mr<FMT_F16><<<n32 + tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
                 }
-                if (ws_profile(M)) prof_end(M, s);
+                if (ws.profile) prof_end(M, s);
                 if (tp.ngroups > 0) {
-                    if (ws_profile(M))
+                    if (ws.profile)
                         prof_begin(M, "ttfinish", tp.npart * MR_RB * (M->precision == HLRC_PREC_F64 ? 8 : 4), s);
                     // first level: runs of slots into the scratch part of the partials
-                    const OutMap pm{M->mr_part, MR_RB, 1, MR_RB};
-                    float* fpart = reinterpret_cast<float*>(M->mr_part);
+                    const OutMap pm{ws.mr_part, MR_RB, 1, MR_RB};
+                    float* fpart = reinterpret_cast<float*>(ws.mr_part);
                     if (M->precision == HLRC_PREC_F64) {
                         if (tp.ngroups1 > 0)
-                            k_ttfinish_f64_mr<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, M->mr_part,
+                            k_ttfinish_f64_mr<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, ws.mr_part,
                                                                                    pm, 1.0, 0);
-                        k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, M->mr_part, om,
+                        k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.mr_part, om,
                                                                               alpha, add);
                     } else {
                         if (tp.ngroups1 > 0)
@@ -978,14 +1028,14 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
                         k_ttfinish_f32_mr<false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, fpart, om,
                                                                                      nullptr, alpha, add);
                     }
-                    if (ws_profile(M)) prof_end(M, s);
+                    if (ws.profile) prof_end(M, s);
                 }
                 HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
             } else if (st.kind == 1) {
                 const DevNPass& np = M->n[size_t(st.idx)];
                 if (np.launches() == 0) continue;
                 if (np.ncta > 0) return fail(HLRC_ERR_INTERNAL, "tree sweep in a multi-vector product");
-                if (ws_profile(M)) prof_begin(M, stage_name(M, 1, st.idx), np.alg_bytes, s);
+                if (ws.profile) prof_begin(M, stage_name(M, 1, st.idx), np.alg_bytes, s);
                 const int add = np.mode != OUT_SET;
                 const double alpha = np.mode == OUT_ADD ? 1.0 : alpha_in;   // plain adds pass coefficients down a tree
                 const OutMap om = omap(np.out);
@@ -1004,7 +1054,7 @@ hlrc_status run_multi(hlrc_hmat M, double alpha_in, int op, const double* X, int
                 if (!f64plan && np.nmseg[FMT_BF16] > 0)
                     k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.mseg[FMT_BF16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
-                if (ws_profile(M)) prof_end(M, s);
+                if (ws.profile) prof_end(M, s);
                 HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
             }
         }
@@ -1151,8 +1201,8 @@ extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double*
     DeviceGuard g(M->device);
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (multi_rhs_ok(M, op, nrhs)) return run_multi(M, alpha, op, x, ldx, y, ldy, nrhs, s);
     const Workspace ws = handle_workspace(M);
+    if (multi_rhs_ok(M, ws, op, nrhs)) return run_multi(M, ws, alpha, op, x, ldx, y, ldy, nrhs, s);
     for (int r = 0; r < nrhs; ++r) {
         st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
         if (st != HLRC_OK) return st;
@@ -1171,6 +1221,8 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
     const int64_t ny = op == HLRC_OP_N ? M->nrows : M->ncols;
     const size_t ex = size_t(nx) * size_t(nrhs), ey = size_t(ny) * size_t(nrhs);
+    // the staging buffers and the handle's workspace serve one host call at a time
+    std::lock_guard<std::mutex> lock(M->host_mu);
     if (ex > M->hx_elems) {
         cudaFree(M->hx);
         M->hx = nullptr;
@@ -1186,11 +1238,11 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     const int64_t lx = nrhs > 1 ? ldx : nx, ly = nrhs > 1 ? ldy : ny;
     HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
-    if (multi_rhs_ok(M, op, nrhs)) {
-        st = run_multi(M, alpha, op, M->hx, nx, M->hy, ny, nrhs, nullptr);
+    const Workspace ws = handle_workspace(M);
+    if (multi_rhs_ok(M, ws, op, nrhs)) {
+        st = run_multi(M, ws, alpha, op, M->hx, nx, M->hy, ny, nrhs, nullptr);
         if (st != HLRC_OK) return st;
     } else {
-        const Workspace ws = handle_workspace(M);
         for (int r = 0; r < nrhs; ++r) {
             st = run_single(M, ws, alpha, op, M->hx + size_t(r) * size_t(nx), M->hy + size_t(r) * size_t(ny), nullptr);
             if (st != HLRC_OK) return st;
@@ -1331,12 +1383,105 @@ extern "C" hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op, const
     // every scratch entry a product reads is written earlier in the same
     // product (coefficients with OUT_SET, each partial by its chunk), so the
     // previous call's contents need no clearing
-    const Workspace ws{base, base + std::max<int64_t>(1, M->n_t),
-                       base + std::max<int64_t>(1, M->n_t) + std::max<int64_t>(1, M->n_t2), false};
+    Workspace ws;
+    ws.t = base;
+    ws.t2 = base + std::max<int64_t>(1, M->n_t);
+    ws.part = base + std::max<int64_t>(1, M->n_t) + std::max<int64_t>(1, M->n_t2);
     return run_single(M, ws, alpha, op, x, y, static_cast<cudaStream_t>(stream));
 }
 
-extern "C" int64_t hlrc_launch_count(hlrc_hmat M) { return M ? M->launches : 0; }
+extern "C" int64_t hlrc_launch_count(hlrc_hmat M) { return M ? M->launches.load() : 0; }
+
+// ------------------------------------------------------------------------
+// Workspaces: scratch owned by the caller, one per concurrent stream.
+//
+// A handle is immutable after upload; everything a product writes besides y
+// is scratch.  HLR's TBB product may run concurrently on one matrix with
+// different y (tbb/arith.hh:312-323, y locked per 64-row chunk in
+// tbb/detail/arith.hh:95-124); here the same is had by giving each stream
+// its own workspace.
+struct hlrc_workspace_s {
+    int device = 0;
+    int64_t n_t = 0, n_t2 = 0, n_part = 0;   // one-vector capacities (doubles)
+    size_t mr_nx = 0, mr_nt = 0, mr_nt2 = 0, mr_np = 0;   // multi-vector capacities (0: none)
+    char* arena = nullptr;
+    size_t bytes = 0;
+    Workspace ws;
+};
+
+extern "C" hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_workspace* out) {
+    clear_error();
+    if (!M || !out) return fail(HLRC_ERR_ARG, "hlrc_workspace_create: null argument");
+    *out = nullptr;
+    if (max_nrhs < 1) return fail(HLRC_ERR_ARG, "hlrc_workspace_create: max_nrhs %d < 1", max_nrhs);
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    auto W = std::make_unique<hlrc_workspace_s>();
+    W->device = M->device;
+    W->n_t = std::max<int64_t>(1, M->n_t);
+    W->n_t2 = std::max<int64_t>(1, M->n_t2);
+    W->n_part = std::max<int64_t>(1, M->n_part);
+    size_t off = 0;
+    auto take = [&](size_t elems) { const size_t o_ = off; off = align_up(off + elems * sizeof(double), 256); return o_; };
+    const size_t o_t = take(size_t(W->n_t)), o_t2 = take(size_t(W->n_t2)), o_p = take(size_t(W->n_part));
+    MrSizes z;
+    size_t o_mr = 0;
+    if (max_nrhs > 1 && has_multi_kernels(M)) {
+        z = mr_sizes(M);
+        o_mr = take(z.bytes / sizeof(double) + 1);
+        W->mr_nx = z.nx; W->mr_nt = z.nt; W->mr_nt2 = z.nt2; W->mr_np = z.np;
+    }
+    W->bytes = off;
+    const cudaError_t e = cudaMalloc(&W->arena, W->bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HLRC_ERR_OOM, "hlrc_workspace_create: cudaMalloc of %zu bytes failed: %s", W->bytes,
+                    cudaGetErrorString(e));
+    }
+    W->ws.t = reinterpret_cast<double*>(W->arena + o_t);
+    W->ws.t2 = reinterpret_cast<double*>(W->arena + o_t2);
+    W->ws.part = reinterpret_cast<double*>(W->arena + o_p);
+    if (W->mr_nx) z.carve(W->arena + o_mr, W->ws.mr_x, W->ws.mr_t, W->ws.mr_t2, W->ws.mr_part);
+    W->ws.profile = false;
+    *out = W.release();
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_workspace_free(hlrc_workspace W) {
+    if (!W) return HLRC_OK;
+    DeviceGuard g(W->device);
+    cudaFree(W->arena);
+    delete W;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_mvm_ws(hlrc_hmat M, hlrc_workspace W, double alpha, int op, const double* x, double* y,
+                                   int nrhs, int64_t ldx, int64_t ldy, void* stream) {
+    clear_error();
+    hlrc_status st = check_mvm_args(M, op, x, y, nrhs, ldx, ldy);
+    if (st != HLRC_OK) return st;
+    if (!W) return fail(HLRC_ERR_ARG, "hlrc_mvm_ws: workspace is NULL");
+    if (W->device != M->device)
+        return fail(HLRC_ERR_ARG, "hlrc_mvm_ws: workspace on device %d, matrix on device %d", W->device, M->device);
+    if (W->n_t < M->n_t || W->n_t2 < M->n_t2 || W->n_part < M->n_part)
+        return fail(HLRC_ERR_SHAPE, "hlrc_mvm_ws: workspace too small for this matrix (create it for this handle)");
+    if (alpha == 0.0 || nrhs == 0) return HLRC_OK;
+    DeviceGuard g(M->device);
+    if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Workspace ws = W->ws;
+    if (ws.mr_x) {   // the multi-vector arrays serve only handles they fit
+        const MrSizes z = mr_sizes(M);
+        if (!has_multi_kernels(M) || z.nx > W->mr_nx || z.nt > W->mr_nt || z.nt2 > W->mr_nt2 || z.np > W->mr_np)
+            ws.mr_x = nullptr;
+    }
+    if (multi_rhs_ok(M, ws, op, nrhs)) return run_multi(M, ws, alpha, op, x, ldx, y, ldy, nrhs, s);
+    for (int r = 0; r < nrhs; ++r) {
+        st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
+        if (st != HLRC_OK) return st;
+    }
+    return HLRC_OK;
+}
 
 extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     if (!M) return HLRC_OK;

@@ -24,8 +24,12 @@
  *  - y is accumulated (y += ...), never overwritten; alpha == 0 is a no-op,
  *    as in hlr::tbb::mul_vec (include/hlr/tbb/arith.hh:54-55).
  *  - A device handle is immutable after upload.  Each handle owns one
- *    scratch workspace, so two hlrc_mvm calls on the same handle must be
- *    ordered on one stream (or use separate handles / hlrc_workspace).
+ *    scratch workspace, used by hlrc_mvm and hlrc_mvm_host, so two hlrc_mvm
+ *    calls on the same handle must be ordered on one stream.  Concurrent
+ *    products on one handle (several streams, several host threads) each
+ *    pass their own hlrc_workspace to hlrc_mvm_ws.  The host API is
+ *    thread-safe except for hlrc_free / hlrc_workspace_free of an object in
+ *    use and hlrc_set_tuning / hlrc_set_profiling during products.
  *  - Device pointers (x, y) are plain CUDA device pointers; `stream` is a
  *    cudaStream_t passed as void* (NULL = legacy default stream).
  *
@@ -202,7 +206,10 @@ typedef struct hlrc_info {
     int32_t max_rank;
     int32_t launches[3];               /* kernel launches per product, op N/T/C
                                           (0 = op unsupported)                  */
-    int32_t reserved[2];
+    int64_t scratch_bytes;             /* scratch of one one-vector product:
+                                          low-rank coefficients and per-tile
+                                          partial sums (what hlrc_mvm_noalloc
+                                          takes from its static array)          */
 } hlrc_info;
 
 typedef struct hlrc_hmat_s* hlrc_hmat;
@@ -218,8 +225,10 @@ const char* hlrc_last_error(void);
 void        hlrc_default_options(hlrc_options* opts);
 
 /* Flatten an H-matrix into the device layout and upload it.
- * Replaces building nothing on the HLR side: the caller's adapter walks its
- * Hpro::TMatrix tree and fills hlrc_block entries.      */
+ * Replaces nothing on the HLR side, which multiplies its Hpro::TMatrix tree
+ * in place: the caller walks that tree in hlr::mul_vec's recursion order
+ * (arith/mulvec.hh:38-60) and fills one hlrc_block per leaf, pointing at the
+ * leaf's own column-major arrays (dense_matrix::mat(), lrmatrix::U() / V()). */
 hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options* opts,
                           hlrc_hmat* out);
 
@@ -282,7 +291,9 @@ hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double* x,
 
 /* Same with x, y in host memory: copies x and y to the device, runs the
  * product, copies y back, synchronises.  Matches the reference's call on
- * host-resident scalar_vectors.                                              */
+ * host-resident scalar_vectors.  Uses the handle's staging buffers and
+ * workspace under a per-handle lock, so concurrent host calls on one handle
+ * are correct but run one after the other.                                   */
 hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x,
                           double* y, int nrhs, int64_t ldx, int64_t ldy);
 
@@ -309,11 +320,34 @@ hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x,
  *    call's contents (each call writes every entry before reading it).  Calls
  *    that overlap on the GPU — on different streams, or with different
  *    handles on the same device — race; order them on one stream.
- *  - Uniform-H handles are accepted (op N and C).                          */
+ *  - Uniform-H and H^2 handles are accepted (op N and C).                 */
 hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op,
                              const double* x, double* y, void* stream);
 
 hlrc_status hlrc_get_info(hlrc_hmat M, hlrc_info* info);
+
+/* Caller-owned scratch for concurrent products on one handle.
+ * HLR's TBB product may be called concurrently on one matrix with different
+ * y (include/hlr/tbb/arith.hh:312-323; y is updated under per-chunk locks,
+ * tbb/detail/arith.hh:95-124).  Here a handle is immutable and all scratch a
+ * product writes lives in a workspace, so products of one handle on several
+ * streams (or host threads) run concurrently when each passes its own
+ * workspace; products that share a workspace must be ordered on one stream.
+ *   hlrc_workspace_create: device scratch sized for M (one-vector products,
+ *     and with max_nrhs > 1 the multi-vector kernels' blocks as well; a
+ *     multi-vector product on a workspace without them loops one-vector
+ *     products).  Allocates with cudaMalloc on M's device.
+ *   hlrc_mvm_ws: hlrc_mvm with the workspace's scratch instead of the
+ *     handle's; same arguments, results and status codes.  A workspace fits
+ *     any handle on the same device whose scratch is not larger (typically
+ *     the handle it was created for); otherwise HLRC_ERR_SHAPE.  Products on
+ *     a workspace are not recorded by hlrc_set_profiling.
+ *   hlrc_workspace_free: releases it (after the products using it ended).  */
+typedef struct hlrc_workspace_s* hlrc_workspace;
+hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_workspace* out);
+hlrc_status hlrc_mvm_ws(hlrc_hmat M, hlrc_workspace ws, double alpha, int op, const double* x, double* y,
+                        int nrhs, int64_t ldx, int64_t ldy, void* stream);
+hlrc_status hlrc_workspace_free(hlrc_workspace ws);
 
 /* Launch shapes of a handle's products, chosen per matrix and device by the
  * autotuner (hlr_b200.tune.autotune times the candidates and caches the

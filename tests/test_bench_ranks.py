@@ -66,3 +66,14 @@ def test_l2_label_marks_small_workloads_resident():
     assert bench.l2_label(248e6).startswith("L2-resident")
     assert bench.l2_label(295e6).startswith("inputs larger than L2")
     assert bench.l2_label(11.07e9).startswith("inputs larger than L2")
+
+
+def test_products_per_graph_gives_several_runs():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    # the driver's 20 timed products run as 5 replays of 4, the default 300 as 6 of 50
+    assert bench.products_per_graph(20) == 4
+    assert bench.products_per_graph(300) == 50
+    for k in (1, 3, 7, 10, 64, 97, 500):
+        d = bench.products_per_graph(k)
+        assert k % d == 0 and d <= 50 and k // d >= min(k, 5)
