@@ -323,7 +323,9 @@ def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int,
                 step()
         graph.replay()          # untimed
         torch.cuda.synchronize()
-        M.last_profile()        # drop the untimed replay's pass records
+        # the capture recorded the pass events as graph nodes: every replay
+        # records them again, and last_profile() after the last timed replay
+        # returns that replay's pass times (reading clears the records)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
