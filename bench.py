@@ -480,19 +480,12 @@ def run_ours(args, rank, world, local_rank):
         y64 = dev_vec(np.zeros((nrhs, n)))
         hlr.mul_vec(1.0, hlr.apply_normal, M64, x, y64)
         yy = dev_vec(np.zeros((nrhs, n)))
-        for _ in range(args.warmup):
-            hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy)
-        torch.cuda.synchronize()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.steps):
-            hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy)
-        f1.record(stream)
-        torch.cuda.synchronize()
-        ms64 = f0.elapsed_time(f1)
+        r64 = time_products(M64, lambda: hlr.mul_vec(alpha, hlr.apply_normal, M64, x, yy), args.steps, args.warmup,
+                            not args.no_graph, world, dev)
+        ms64 = r64["ms"]
         y64h = (y64 if nrhs > 1 else y64[:, None]).cpu().numpy()
         fp64 = {"value": nrhs * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
-                "matrix_bytes": M64.info["matrix_bytes"],
+                "ms_per_product_of_runs": r64["runs"], "matrix_bytes": M64.info["matrix_bytes"],
                 "rel_err_vs_fp64": float(np.linalg.norm(ygpu_all - y64h) / np.linalg.norm(y64h))}
         M64.free()
         del yy, y64

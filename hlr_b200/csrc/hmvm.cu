@@ -26,6 +26,7 @@
 #include "kernels_mr.cuh"
 #include "kernels_q.cuh"
 #include "kernels_tc.cuh"
+#include "kernels_wide.cuh"
 #include "plan.hpp"
 
 namespace hlrc {
@@ -127,6 +128,16 @@ struct hlrc_hmat_s {
     char* mr_arena = nullptr;
     double *mr_x = nullptr, *mr_t = nullptr, *mr_t2 = nullptr, *mr_part = nullptr;
     char* mr_tables = nullptr;   // column streams of reduced-precision stores (MSeg / MCol)
+    // one-pass 64-vector products of 16-bit H stores (op N): eligibility and
+    // the workspace (allocated at upload when max_nrhs > MR_RB)
+    bool wide = false;
+    char* w_arena = nullptr;
+    uint32_t* w_xs = nullptr;
+    uint32_t* w_ts = nullptr;
+    int8_t* w_texp = nullptr;
+    float* w_part = nullptr;
+    unsigned long long* w_xmax = nullptr;
+    int* w_g = nullptr;
     // host-pointer entry point staging (hlrc_mvm_host holds host_mu while it
     // uses these and the handle's workspace)
     double* hx = nullptr;
@@ -140,6 +151,7 @@ struct hlrc_hmat_s {
     int nform_warps = 8;      // warps per CTA, single-vector N-form
     int ttform_warps = 8;     // warps per CTA, single-vector tile T-form
     int mr_min_nrhs = 2;      // fewest vectors that take the 8-vector kernels
+    int wide_min_nrhs = MR_RB + 1;   // fewest vectors that take the 64-vector kernels (when the handle has them)
     // profiling
     bool profiling = false;
     std::vector<ProfileRec> prof;
@@ -147,6 +159,30 @@ struct hlrc_hmat_s {
 };
 
 namespace {
+
+// Scratch used by one product: the coefficient vectors and the partial sums
+// of a one-vector product, and (when present) the same arrays as row-major
+// blocks of MR_RB vectors for the multi-vector kernels.  A product reads
+// every scratch entry only after writing it in the same product.
+struct Workspace {
+    double* t = nullptr;
+    double* t2 = nullptr;
+    double* part = nullptr;
+    double* mr_x = nullptr;      // null: no multi-vector arrays
+    double* mr_t = nullptr;
+    double* mr_t2 = nullptr;
+    double* mr_part = nullptr;
+    // one-pass 64-vector kernels of 16-bit stores (null: none): split rows of
+    // x and t, the exponents of t's rows, FP32 partials, per-vector maxima
+    // and scale exponents of x
+    uint32_t* w_xs = nullptr;
+    uint32_t* w_ts = nullptr;
+    int8_t* w_texp = nullptr;
+    float* w_part = nullptr;
+    unsigned long long* w_xmax = nullptr;
+    int* w_g = nullptr;
+    bool profile = false;        // record per-pass events in the handle's profile
+};
 
 struct DeviceGuard {
     int prev = -1;
@@ -498,6 +534,66 @@ MrSizes mr_sizes(hlrc_hmat M) {
     return z;
 }
 
+// Sizes of the one-pass 64-vector workspace: split rows of x (the longer
+// side) and of t, t's row exponents, FP32 partials (64 per entry), the
+// per-vector maxima and scale exponents of x.
+struct WideSizes {
+    size_t xs = 0, ts = 0, texp = 0, part = 0, bytes = 0;
+    void carve(char* base, Workspace& w) const {
+        size_t off = 0;
+        auto take = [&](size_t b) { char* q = base + off; off = align_up(off + b, 256); return q; };
+        w.w_xs = reinterpret_cast<uint32_t*>(take(xs));
+        w.w_ts = reinterpret_cast<uint32_t*>(take(ts));
+        w.w_texp = reinterpret_cast<int8_t*>(take(texp));
+        w.w_part = reinterpret_cast<float*>(take(part));
+        w.w_xmax = reinterpret_cast<unsigned long long*>(take(WIDE_RHS * sizeof(unsigned long long)));
+        w.w_g = reinterpret_cast<int*>(take(WIDE_RHS * sizeof(int)));
+    }
+};
+
+WideSizes wide_sizes(hlrc_hmat M) {
+    WideSizes z;
+    z.xs = size_t(std::max(M->nrows, M->ncols)) * WIDE_ROWB;
+    z.ts = size_t(std::max<int64_t>(1, M->n_t)) * WIDE_ROWB;
+    z.texp = size_t(std::max<int64_t>(1, M->n_t));
+    z.part = size_t(std::max<int64_t>(1, M->n_part)) * WIDE_RHS * sizeof(float);
+    z.bytes = z.xs + z.ts + z.texp + z.part + 2 * WIDE_RHS * 8 + 8 * 256;
+    return z;
+}
+
+// The store format of a 16-bit H-matrix handle whose op N product is one
+// tile T-form pass (t = V^T x) followed by one N-form pass (y += alpha (U t
+// + D x)) over 16-bit column runs only: the shape the 64-vector kernels
+// take.  -1 otherwise.
+int wide_format(hlrc_hmat M) {
+    if (M->kind != 0 || (M->precision != HLRC_PREC_F16 && M->precision != HLRC_PREC_BF16)) return -1;
+    const std::vector<Stage>& st = M->stages[HLRC_OP_N];
+    if (st.size() != 2 || st[0].kind != 2 || st[1].kind != 1) return -1;
+    const DevTTPass& tp = M->tt[size_t(st[0].idx)];
+    const DevNPass& np = M->n[size_t(st[1].idx)];
+    const int f = M->precision == HLRC_PREC_BF16 ? FMT_BF16 : FMT_F16;
+    if (tp.in != V_X || tp.out != V_T || tp.mode != OUT_SET) return -1;
+    if (np.vx != V_X || np.vt != V_T || np.out != V_Y || np.mode != OUT_ADD_ALPHA || np.ncta > 0) return -1;
+    for (int g = 0; g < NFMT; ++g)
+        if (g != f && (tp.nmseg[g] > 0 || np.nmseg[g] > 0)) return -1;
+    return f;
+}
+
+// The wide kernels use more than 48 KB of dynamic shared memory; raised once
+// per device, as for the 8-vector kernels.
+hlrc_status enable_wide_smem(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_t()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_t()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_n()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_n()));
+    done.push_back(dev);
+    return HLRC_OK;
+}
+
 hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     auto h = std::make_unique<hlrc_hmat_s>();
     int dev = o.device;
@@ -707,6 +803,30 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             return st;
         }
     }
+    hp->wide = wide_format(hp) >= 0;
+    if (hp->wide && o.max_nrhs > MR_RB) {
+        hlrc_status st = enable_wide_smem(dev);
+        const WideSizes z = wide_sizes(hp);
+        if (st == HLRC_OK) {
+            e = cudaMalloc(&hp->w_arena, z.bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                st = fail(HLRC_ERR_OOM, "64-vector workspace of %zu bytes: %s", z.bytes, cudaGetErrorString(e));
+            }
+        }
+        if (st != HLRC_OK) {
+            cudaFree(hp->mr_tables);
+            cudaFree(hp->mr_arena);
+            cleanup();
+            return st;
+        }
+        Workspace w;
+        z.carve(hp->w_arena, w);
+        hp->w_xs = w.w_xs; hp->w_ts = w.w_ts; hp->w_texp = w.w_texp; hp->w_part = w.w_part;
+        hp->w_xmax = w.w_xmax; hp->w_g = w.w_g;
+        hp->info.workspace_bytes += int64_t(z.bytes);
+        hp->info.device_bytes += int64_t(z.bytes);
+    }
     for (int op = 0; op < 3; ++op) {
         int nl = 0;
         for (const Stage& st : hp->stages[op])
@@ -718,27 +838,14 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     return HLRC_OK;
 }
 
-// Scratch used by one product: the coefficient vectors and the partial sums
-// of a one-vector product, and (when present) the same arrays as row-major
-// blocks of MR_RB vectors for the multi-vector kernels.  A product reads
-// every scratch entry only after writing it in the same product.
-struct Workspace {
-    double* t = nullptr;
-    double* t2 = nullptr;
-    double* part = nullptr;
-    double* mr_x = nullptr;      // null: no multi-vector arrays
-    double* mr_t = nullptr;
-    double* mr_t2 = nullptr;
-    double* mr_part = nullptr;
-    bool profile = false;        // record per-pass events in the handle's profile
-};
-
 // the handle's own workspace (hlrc_mvm, hlrc_mvm_host); only products on it
 // are profiled
 Workspace handle_workspace(hlrc_hmat M) {
     Workspace w;
     w.t = M->ws_t; w.t2 = M->ws_t2; w.part = M->part;
     w.mr_x = M->mr_x; w.mr_t = M->mr_t; w.mr_t2 = M->mr_t2; w.mr_part = M->mr_part;
+    w.w_xs = M->w_xs; w.w_ts = M->w_ts; w.w_texp = M->w_texp; w.w_part = M->w_part;
+    w.w_xmax = M->w_xmax; w.w_g = M->w_g;
     w.profile = M->profiling;
     return w;
 }
@@ -1064,6 +1171,89 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
     return HLRC_OK;
 }
 
+// Can the product take the one-pass 64-vector kernels?  16-bit H stores,
+// op N, a workspace with their arrays, and at least wide_min_nrhs vectors.
+bool wide_ok(hlrc_hmat M, const Workspace& ws, int op, int nrhs) {
+    return M->wide && op == HLRC_OP_N && ws.w_xs && nrhs >= M->wide_min_nrhs && nrhs >= 2;
+}
+
+// y := y + alpha M X for nrhs vectors, WIDE_RHS per pass: x is split into
+// 16-bit terms once, the tile T-form writes t's split rows (multi-tile
+// outputs through FP32 partials and the finish), and the N-form adds
+// alpha (U t + D x) to Y.  The matrix is streamed once per 64 vectors.
+hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const double* X, int64_t ldx, double* Y,
+                     int64_t ldy, int nrhs, cudaStream_t s) {
+    const int f = wide_format(M);
+    if (f < 0) return fail(HLRC_ERR_INTERNAL, "64-vector product on a handle without 64-vector passes");
+    const std::vector<Stage>& st = M->stages[HLRC_OP_N];
+    const DevTTPass& tp = M->tt[size_t(st[0].idx)];
+    const DevNPass& np = M->n[size_t(st[1].idx)];
+    const int64_t nx = M->ncols;
+    for (int r0 = 0; r0 < nrhs; r0 += WIDE_RHS) {
+        const int nr = std::min(WIDE_RHS, nrhs - r0);
+        const double* Xr = X + int64_t(r0) * ldx;
+        if (ws.profile) prof_begin(M, "wide_xsplit", nx * int64_t(nr) * 8 + nx * WIDE_ROWB, s);
+        HLRC_CUDA(cudaMemsetAsync(ws.w_xmax, 0, WIDE_RHS * sizeof(unsigned long long), s));
+        const unsigned gx = unsigned(std::min<int64_t>((nx + 255) / 256, 4 * 148));
+        k_wide_xmax<<<dim3(std::max(1u, gx), unsigned(nr)), 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax);
+        const unsigned gs = unsigned(std::max<int64_t>(1, (nx + TILE - 1) / TILE));
+        if (f == FMT_BF16) k_wide_xsplit<FMT_BF16><<<gs, 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax, ws.w_xs, ws.w_g);
+        else k_wide_xsplit<FMT_F16><<<gs, 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax, ws.w_xs, ws.w_g);
+        if (ws.profile) prof_end(M, s);
+        M->launches += 2;
+        HLRC_AFTER_LAUNCH("wide_xsplit");
+        if (tp.nmseg[f] > 0) {
+            if (ws.profile) prof_begin(M, stage_name(M, 2, st[0].idx), tp.alg_bytes, s);
+            if (f == FMT_BF16)
+                k_ttform_wide<FMT_BF16><<<tp.nmseg[f], WIDE_THREADS, wide_smem_t(), s>>>(
+                    tp.mseg[f], tp.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_part, M->dev_err);
+            else
+                k_ttform_wide<FMT_F16><<<tp.nmseg[f], WIDE_THREADS, wide_smem_t(), s>>>(
+                    tp.mseg[f], tp.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_part, M->dev_err);
+            if (ws.profile) prof_end(M, s);
+            M->launches += 1;
+            HLRC_AFTER_LAUNCH(stage_name(M, 2, st[0].idx));
+        }
+        if (tp.ngroups > 0) {
+            if (ws.profile) prof_begin(M, "ttfinish", tp.npart * WIDE_RHS * 4, s);
+            if (tp.ngroups1 > 0) {
+                if (f == FMT_BF16)
+                    k_ttfinish_wide<FMT_BF16, true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1,
+                                                                                           ws.w_part, ws.w_ts, ws.w_texp);
+                else
+                    k_ttfinish_wide<FMT_F16, true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1,
+                                                                                          ws.w_part, ws.w_ts, ws.w_texp);
+                M->launches += 1;
+            }
+            if (f == FMT_BF16)
+                k_ttfinish_wide<FMT_BF16, false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.w_part,
+                                                                                       ws.w_ts, ws.w_texp);
+            else
+                k_ttfinish_wide<FMT_F16, false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.w_part,
+                                                                                      ws.w_ts, ws.w_texp);
+            M->launches += 1;
+            if (ws.profile) prof_end(M, s);
+            HLRC_AFTER_LAUNCH("ttfinish");
+        }
+        if (np.nmseg[f] > 0) {
+            const OutMap om{Y + int64_t(r0) * ldy, 1, ldy, nr};
+            if (ws.profile) prof_begin(M, stage_name(M, 1, st[1].idx), np.alg_bytes, s);
+            if (f == FMT_BF16)
+                k_nform_wide<FMT_BF16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
+                    np.mseg[f], np.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_g, om, alpha, 1, M->dev_err);
+            else
+                k_nform_wide<FMT_F16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
+                    np.mseg[f], np.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_g, om, alpha, 1, M->dev_err);
+            if (ws.profile) prof_end(M, s);
+            M->launches += 1;
+            HLRC_AFTER_LAUNCH(stage_name(M, 1, st[1].idx));
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return HLRC_OK;
+}
+
 hlrc_status check_mvm_args(hlrc_hmat M, int op, const double* x, double* y, int nrhs, int64_t ldx, int64_t ldy) {
     if (!M) return fail(HLRC_ERR_ARG, "matrix handle is NULL");
     if (op < 0 || op > 2) return fail(HLRC_ERR_ARG, "op %d is not a valid hlrc_op", op);
@@ -1202,6 +1392,7 @@ extern "C" hlrc_status hlrc_mvm(hlrc_hmat M, double alpha, int op, const double*
     if (!g.ok) return fail(HLRC_ERR_CUDA, "cannot select device %d", M->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const Workspace ws = handle_workspace(M);
+    if (wide_ok(M, ws, op, nrhs)) return run_wide(M, ws, alpha, x, ldx, y, ldy, nrhs, s);
     if (multi_rhs_ok(M, ws, op, nrhs)) return run_multi(M, ws, alpha, op, x, ldx, y, ldy, nrhs, s);
     for (int r = 0; r < nrhs; ++r) {
         st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
@@ -1239,7 +1430,10 @@ extern "C" hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const do
     HLRC_CUDA(cudaMemcpy2D(M->hx, size_t(nx) * 8, x, size_t(lx) * 8, size_t(nx) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     HLRC_CUDA(cudaMemcpy2D(M->hy, size_t(ny) * 8, y, size_t(ly) * 8, size_t(ny) * 8, size_t(nrhs), cudaMemcpyHostToDevice));
     const Workspace ws = handle_workspace(M);
-    if (multi_rhs_ok(M, ws, op, nrhs)) {
+    if (wide_ok(M, ws, op, nrhs)) {
+        st = run_wide(M, ws, alpha, M->hx, nx, M->hy, ny, nrhs, nullptr);
+        if (st != HLRC_OK) return st;
+    } else if (multi_rhs_ok(M, ws, op, nrhs)) {
         st = run_multi(M, ws, alpha, op, M->hx, nx, M->hy, ny, nrhs, nullptr);
         if (st != HLRC_OK) return st;
     } else {
@@ -1264,6 +1458,7 @@ extern "C" hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t) {
     t->nform_warps = M->nform_warps;
     t->ttform_warps = M->ttform_warps;
     t->mr_min_nrhs = M->mr_min_nrhs;
+    t->wide_min_nrhs = M->wide_min_nrhs;
     return HLRC_OK;
 }
 
@@ -1276,9 +1471,13 @@ extern "C" hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t) {
     if (t->mr_min_nrhs < 2 || t->mr_min_nrhs > HLRC_MR_NEVER)
         return fail(HLRC_ERR_ARG, "hlrc_set_tuning: mr_min_nrhs must be in [2, %d] (got %d)", HLRC_MR_NEVER,
                     t->mr_min_nrhs);
+    if (t->wide_min_nrhs < 2 || t->wide_min_nrhs > HLRC_MR_NEVER)
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: wide_min_nrhs must be in [2, %d] (got %d)", HLRC_MR_NEVER,
+                    t->wide_min_nrhs);
     M->nform_warps = t->nform_warps;
     M->ttform_warps = t->ttform_warps;
     M->mr_min_nrhs = t->mr_min_nrhs;
+    M->wide_min_nrhs = t->wide_min_nrhs;
     return HLRC_OK;
 }
 
@@ -1404,6 +1603,7 @@ struct hlrc_workspace_s {
     int device = 0;
     int64_t n_t = 0, n_t2 = 0, n_part = 0;   // one-vector capacities (doubles)
     size_t mr_nx = 0, mr_nt = 0, mr_nt2 = 0, mr_np = 0;   // multi-vector capacities (0: none)
+    size_t w_xs = 0, w_ts = 0, w_part = 0;                // 64-vector capacities in bytes (0: none)
     char* arena = nullptr;
     size_t bytes = 0;
     Workspace ws;
@@ -1431,6 +1631,15 @@ extern "C" hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_wor
         o_mr = take(z.bytes / sizeof(double) + 1);
         W->mr_nx = z.nx; W->mr_nt = z.nt; W->mr_nt2 = z.nt2; W->mr_np = z.np;
     }
+    WideSizes zw;
+    size_t o_w = 0;
+    if (max_nrhs > MR_RB && M->wide) {
+        const hlrc_status st = enable_wide_smem(M->device);
+        if (st != HLRC_OK) return st;
+        zw = wide_sizes(M);
+        o_w = take(zw.bytes / sizeof(double) + 1);
+        W->w_xs = zw.xs; W->w_ts = zw.ts; W->w_part = zw.part;
+    }
     W->bytes = off;
     const cudaError_t e = cudaMalloc(&W->arena, W->bytes);
     if (e != cudaSuccess) {
@@ -1442,6 +1651,7 @@ extern "C" hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_wor
     W->ws.t2 = reinterpret_cast<double*>(W->arena + o_t2);
     W->ws.part = reinterpret_cast<double*>(W->arena + o_p);
     if (W->mr_nx) z.carve(W->arena + o_mr, W->ws.mr_x, W->ws.mr_t, W->ws.mr_t2, W->ws.mr_part);
+    if (W->w_xs) zw.carve(W->arena + o_w, W->ws);
     W->ws.profile = false;
     *out = W.release();
     return HLRC_OK;
@@ -1475,6 +1685,11 @@ extern "C" hlrc_status hlrc_mvm_ws(hlrc_hmat M, hlrc_workspace W, double alpha, 
         if (!has_multi_kernels(M) || z.nx > W->mr_nx || z.nt > W->mr_nt || z.nt2 > W->mr_nt2 || z.np > W->mr_np)
             ws.mr_x = nullptr;
     }
+    if (ws.w_xs) {
+        const WideSizes z = wide_sizes(M);
+        if (!M->wide || z.xs > W->w_xs || z.ts > W->w_ts || z.part > W->w_part) ws.w_xs = nullptr;
+    }
+    if (wide_ok(M, ws, op, nrhs)) return run_wide(M, ws, alpha, x, ldx, y, ldy, nrhs, s);
     if (multi_rhs_ok(M, ws, op, nrhs)) return run_multi(M, ws, alpha, op, x, ldx, y, ldy, nrhs, s);
     for (int r = 0; r < nrhs; ++r) {
         st = run_single(M, ws, alpha, op, x + size_t(r) * size_t(ldx), y + size_t(r) * size_t(ldy), s);
@@ -1494,6 +1709,7 @@ extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     cudaFree(M->hy);
     cudaFree(M->mr_arena);
     cudaFree(M->mr_tables);
+    cudaFree(M->w_arena);
     cudaFree(M->arena);
     delete M;
     return HLRC_OK;

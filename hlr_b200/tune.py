@@ -7,7 +7,9 @@ fastest:
 * one vector: warps per CTA (4 or 8) of the N-form and of the tile T-form
   kernels, four combinations;
 * several vectors: the 8-vector tensor-core kernels against a loop of
-  one-vector products (``mr_min_nrhs`` 2 or ``HLRC_MR_NEVER``).
+  one-vector products (``mr_min_nrhs`` 2 or ``HLRC_MR_NEVER``); with more
+  than 8 vectors also the one-pass 64-vector kernels of 16-bit stores
+  (``wide_min_nrhs`` 9 or ``HLRC_MR_NEVER``).
 
 Each candidate runs ``warmup`` untimed products and then at least ``reps``
 products (enough to last 20 ms) timed with CUDA events on the launching
@@ -31,7 +33,7 @@ from typing import Callable, Optional
 
 from ._capi import HLRC_MR_NEVER
 
-DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2}
+DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9}
 
 
 def default_cache_path() -> Path:
@@ -51,7 +53,10 @@ def candidates(current: dict, nrhs: int) -> list:
     """Settings to time; the first is the default for this vector count."""
     if nrhs <= 1:
         return [dict(current, nform_warps=a, ttform_warps=b) for a in (8, 4) for b in (8, 4)]
-    return [dict(current, mr_min_nrhs=2), dict(current, mr_min_nrhs=HLRC_MR_NEVER)]
+    if nrhs <= 8:
+        return [dict(current, mr_min_nrhs=2), dict(current, mr_min_nrhs=HLRC_MR_NEVER)]
+    return [dict(current, wide_min_nrhs=9, mr_min_nrhs=2), dict(current, wide_min_nrhs=HLRC_MR_NEVER, mr_min_nrhs=2),
+            dict(current, wide_min_nrhs=HLRC_MR_NEVER, mr_min_nrhs=HLRC_MR_NEVER)]
 
 
 def _load(path: Path) -> dict:

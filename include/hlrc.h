@@ -358,15 +358,20 @@ hlrc_status hlrc_workspace_free(hlrc_workspace ws);
  *     N-form and tile T-form kernels;
  *   mr_min_nrhs: products with at least this many vectors use the
  *     8-vector tensor-core kernels, smaller ones loop the one-vector kernels
- *     (2..HLRC_MR_NEVER; HLRC_MR_NEVER always loops).
- * Defaults: 8, 8, 2.  hlrc_set_tuning rejects other values (HLRC_ERR_ARG)
+ *     (2..HLRC_MR_NEVER; HLRC_MR_NEVER always loops);
+ *   wide_min_nrhs: op N products of FP16 / BF16 H-matrix handles uploaded
+ *     with max_nrhs > 8 with at least this many vectors run the one-pass
+ *     kernels on the tcgen05 tensor cores, 64 vectors per pass of the
+ *     matrix; smaller ones use the 8-vector kernels (2..HLRC_MR_NEVER).
+ * Defaults: 8, 8, 2, 9.  hlrc_set_tuning rejects other values (HLRC_ERR_ARG)
  * and must not race with products of the same handle.                     */
 #define HLRC_MR_NEVER 1000000
 typedef struct hlrc_tuning {
     int32_t nform_warps;
     int32_t ttform_warps;
     int32_t mr_min_nrhs;
-    int32_t reserved[5];
+    int32_t wide_min_nrhs;
+    int32_t reserved[4];
 } hlrc_tuning;
 
 hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t);

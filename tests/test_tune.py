@@ -57,7 +57,7 @@ def test_picks_fastest_and_caches(tmp_path):
     path = tmp_path / "tuning.json"
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
     assert not r["cached"] and len(calls) == 8      # two sweeps of four
-    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2}
+    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9}
     d = json.loads(path.read_text())
     assert d[r["key"]]["tuning"] == M.tuning
     # a fresh handle of the same signature takes the cached setting untimed
@@ -116,3 +116,15 @@ def test_timer_failure_restores_setting():
     with pytest.raises(RuntimeError):
         tune.autotune(M, nrhs=1, cache=None, timer=boom, device_name="G")
     assert M.tuning["nform_warps"] == 4
+
+
+def test_wide_candidates_above_eight_vectors():
+    """More than 8 vectors: the 64-vector kernels, the 8-vector kernels, and
+    the loop of one-vector products; the fastest wins."""
+    M = FakeMatrix()
+    c = tune.candidates(M.tuning, 64)
+    assert [(x["wide_min_nrhs"], x["mr_min_nrhs"]) for x in c] == [(9, 2), (HLRC_MR_NEVER, 2),
+                                                                   (HLRC_MR_NEVER, HLRC_MR_NEVER)]
+    t, calls = timer_for(M, lambda s: 3.0 if s["wide_min_nrhs"] == HLRC_MR_NEVER and s["mr_min_nrhs"] == 2 else 6.0)
+    r = tune.autotune(M, nrhs=64, cache=None, timer=t, device_name="G")
+    assert r["tuning"]["wide_min_nrhs"] == HLRC_MR_NEVER and r["tuning"]["mr_min_nrhs"] == 2 and len(calls) == 6
