@@ -111,6 +111,8 @@ PROTOTYPES = {
     "hlrc_mvm_ws": (C.c_int, [C.c_void_p, C.c_void_p, f64, C.c_int, C.c_void_p, C.c_void_p, C.c_int, i64, i64,
                               C.c_void_p]),
     "hlrc_workspace_free": (C.c_int, [C.c_void_p]),
+    "hlrc_fp64_peak": (C.c_int, [C.c_int, C.POINTER(f64)]),
+    "hlrc_debug_waits": (C.c_int, [C.c_void_p, i64, C.c_int]),
     "hlrc_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
     "hlrc_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(hlrc_tuning)]),
     "hlrc_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

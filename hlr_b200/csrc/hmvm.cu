@@ -53,6 +53,7 @@ struct DevNPass {
     int nmseg[NFMT] = {};
     const MCol* mcol = nullptr;
     const NSeg2* seg2 = nullptr;      // reduced precision: both formats of a tile in one CTA
+    const WCol* wcol = nullptr;       // 64-vector N-form: per column of the 16-bit runs
     int nseg2 = 0;
     int f16 = FMT_F16;                // the store's 16-bit format
     int wide = FMT_F32;               // the store's wide format (FP32, or 24-bit for BFP)
@@ -131,10 +132,18 @@ struct hlrc_hmat_s {
     // one-pass 64-vector products of 16-bit H stores (op N): eligibility and
     // the workspace (allocated at upload when max_nrhs > MR_RB)
     bool wide = false;
-    char* w_arena = nullptr;
+    char* w_static = nullptr;         // the column-cluster T-form tables and t's exponents
+    const WTUnit* w_units = nullptr;
+    const WTBlk* w_blks = nullptr;
+    const uint32_t* w_slabs = nullptr;
+    const WTTile* w_tiles = nullptr;
+    const TGroup* w_groups = nullptr;
+    const int8_t* w_texp = nullptr;
+    int w_nunits = 0, w_ngroups = 0;
+    int64_t w_npart = 0;
+    char* w_arena = nullptr;          // workspace of the handle's own 64-vector products
     uint32_t* w_xs = nullptr;
     uint32_t* w_ts = nullptr;
-    int8_t* w_texp = nullptr;
     float* w_part = nullptr;
     unsigned long long* w_xmax = nullptr;
     int* w_g = nullptr;
@@ -145,6 +154,9 @@ struct hlrc_hmat_s {
     size_t hx_elems = 0, hy_elems = 0;
     std::mutex host_mu;
     int* dev_err = nullptr;   // device error word (bounded waits that ran out)
+    // bound of the device waits and the test hook of hlrc_debug_waits
+    uint64_t wait_ns = 2000000000ull;
+    int wait_skip = 0;
     std::atomic<int64_t> launches{0};   // kernels launched by this handle (any thread)
     std::vector<const char*> names[3];   // per-pass profile names (empty: fixed names)
     // launch shapes picked by the autotuner (hlrc_set_tuning)
@@ -173,11 +185,10 @@ struct Workspace {
     double* mr_t2 = nullptr;
     double* mr_part = nullptr;
     // one-pass 64-vector kernels of 16-bit stores (null: none): split rows of
-    // x and t, the exponents of t's rows, FP32 partials, per-vector maxima
-    // and scale exponents of x
+    // x and t, FP32 partials of long column clusters, per-vector maxima and
+    // scale exponents of x
     uint32_t* w_xs = nullptr;
     uint32_t* w_ts = nullptr;
-    int8_t* w_texp = nullptr;
     float* w_part = nullptr;
     unsigned long long* w_xmax = nullptr;
     int* w_g = nullptr;
@@ -428,17 +439,58 @@ hlrc_status build_streams(const std::vector<Seg> (&segs)[NFMT], const std::vecto
     return HLRC_OK;
 }
 
-// Builds and uploads the column streams of every N-form and tile T-form pass.
+// 2^d (d <= 0) as two packed 16-bit values of the store's format; 0 below
+// the format's subnormal range
+uint32_t pow2_pair(int d, bool bf16) {
+    uint32_t b = 0;
+    if (bf16) b = d >= -126 ? uint32_t(d + 127) << 7 : (d >= -133 ? 1u << (d + 133) : 0u);
+    else b = d >= -14 ? uint32_t(d + 15) << 10 : (d >= -24 ? 1u << (d + 24) : 0u);
+    return b | (b << 16);
+}
+
+// The 64-vector N-form's column table of one pass (WCol) and each run's
+// factor exponent E (in MSeg.pad): f = chunk scale, times 2^c of the t entry
+// for t columns; E = the largest exponent of f over the run; the column's
+// factor is 2^(exponent of f - E).
+void wide_columns(StreamTables& tab, int f, const std::vector<int8_t>& t_exp, bool bf16, std::vector<WCol>& out) {
+    out.assign(tab.col.size(), WCol{0u, 0u});
+    for (MSeg& m : tab.seg[f]) {
+        auto fexp = [&](const MCol& c) {
+            const int es = std::ilogb(c.scale);
+            return (c.idx & VEC_T) ? es + int(t_exp[size_t(c.idx & ~VEC_T)]) : es;
+        };
+        int E = INT32_MIN;
+        for (uint32_t j = 0; j < m.ncols; ++j) E = std::max(E, fexp(tab.col[size_t(m.col0 + j)]));
+        if (m.ncols == 0) E = 0;
+        m.pad = uint32_t(E);
+        for (uint32_t j = 0; j < m.ncols; ++j) {
+            const MCol& c = tab.col[size_t(m.col0 + j)];
+            out[size_t(m.col0 + j)] = WCol{c.idx, pow2_pair(fexp(c) - E, bf16)};
+        }
+    }
+}
+
+// Builds and uploads the column streams of every N-form and tile T-form pass
+// (and, for plans with a 64-vector product, that N-form's column table).
 hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
     std::vector<StreamTables> nt(p.npasses.size()), tt(p.ttpasses.size());
     size_t bytes = 0;
     auto take = [&](size_t b) { const size_t o = bytes; bytes = align_up(bytes + b, 256); return o; };
     std::vector<std::array<size_t, NFMT>> n_seg_off(nt.size()), t_seg_off(tt.size());
     std::vector<size_t> n_col_off(nt.size()), t_col_off(tt.size());
+    // the op N N-form of a 16-bit H plan with a 64-vector product
+    const int wide_pass = !p.wide.empty() && p.stages[HLRC_OP_N].size() == 2 ? p.stages[HLRC_OP_N][1].idx : -1;
+    const bool bf16 = p.precision == HLRC_PREC_BF16;
+    std::vector<WCol> wcol;
+    size_t wcol_off = 0;
     for (size_t i = 0; i < nt.size(); ++i) {
         const hlrc_status st = build_streams(p.npasses[i].segs, p.npasses[i].chunks, false,
                                              [](const NSeg& s) { return s.out; }, nt[i]);
         if (st != HLRC_OK) return st;
+        if (int(i) == wide_pass) {
+            wide_columns(nt[i], bf16 ? FMT_BF16 : FMT_F16, p.wide.t_exp, bf16, wcol);
+            wcol_off = take(wcol.size() * sizeof(WCol));
+        }
         for (int f = 0; f < NFMT; ++f) n_seg_off[i][size_t(f)] = take(nt[i].seg[f].size() * sizeof(MSeg));
         n_col_off[i] = take(nt[i].col.size() * sizeof(MCol));
     }
@@ -465,6 +517,10 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
         }
         if (e == cudaSuccess) e = put(n_col_off[i], nt[i].col.data(), nt[i].col.size() * sizeof(MCol));
         h->n[i].mcol = reinterpret_cast<const MCol*>(h->mr_tables + n_col_off[i]);
+        if (int(i) == wide_pass) {
+            if (e == cudaSuccess) e = put(wcol_off, wcol.data(), wcol.size() * sizeof(WCol));
+            h->n[i].wcol = reinterpret_cast<const WCol*>(h->mr_tables + wcol_off);
+        }
     }
     for (size_t i = 0; i < tt.size() && e == cudaSuccess; ++i) {
         for (int f = 0; f < NFMT && e == cudaSuccess; ++f) {
@@ -535,16 +591,15 @@ MrSizes mr_sizes(hlrc_hmat M) {
 }
 
 // Sizes of the one-pass 64-vector workspace: split rows of x (the longer
-// side) and of t, t's row exponents, FP32 partials (64 per entry), the
-// per-vector maxima and scale exponents of x.
+// side) and of t, FP32 partials (64 per entry), the per-vector maxima and
+// scale exponents of x.
 struct WideSizes {
-    size_t xs = 0, ts = 0, texp = 0, part = 0, bytes = 0;
+    size_t xs = 0, ts = 0, part = 0, bytes = 0;
     void carve(char* base, Workspace& w) const {
         size_t off = 0;
         auto take = [&](size_t b) { char* q = base + off; off = align_up(off + b, 256); return q; };
         w.w_xs = reinterpret_cast<uint32_t*>(take(xs));
         w.w_ts = reinterpret_cast<uint32_t*>(take(ts));
-        w.w_texp = reinterpret_cast<int8_t*>(take(texp));
         w.w_part = reinterpret_cast<float*>(take(part));
         w.w_xmax = reinterpret_cast<unsigned long long*>(take(WIDE_RHS * sizeof(unsigned long long)));
         w.w_g = reinterpret_cast<int*>(take(WIDE_RHS * sizeof(int)));
@@ -555,9 +610,8 @@ WideSizes wide_sizes(hlrc_hmat M) {
     WideSizes z;
     z.xs = size_t(std::max(M->nrows, M->ncols)) * WIDE_ROWB;
     z.ts = size_t(std::max<int64_t>(1, M->n_t)) * WIDE_ROWB;
-    z.texp = size_t(std::max<int64_t>(1, M->n_t));
-    z.part = size_t(std::max<int64_t>(1, M->n_part)) * WIDE_RHS * sizeof(float);
-    z.bytes = z.xs + z.ts + z.texp + z.part + 2 * WIDE_RHS * 8 + 8 * 256;
+    z.part = size_t(std::max<int64_t>(1, M->w_npart)) * WIDE_RHS * sizeof(float);
+    z.bytes = z.xs + z.ts + z.part + 2 * WIDE_RHS * 8 + 6 * 256;
     return z;
 }
 
@@ -566,14 +620,14 @@ WideSizes wide_sizes(hlrc_hmat M) {
 // + D x)) over 16-bit column runs only: the shape the 64-vector kernels
 // take.  -1 otherwise.
 int wide_format(hlrc_hmat M) {
-    if (M->kind != 0 || (M->precision != HLRC_PREC_F16 && M->precision != HLRC_PREC_BF16)) return -1;
+    if (M->kind != 0 || (M->precision != HLRC_PREC_F16 && M->precision != HLRC_PREC_BF16) || !M->w_static) return -1;
     const std::vector<Stage>& st = M->stages[HLRC_OP_N];
     if (st.size() != 2 || st[0].kind != 2 || st[1].kind != 1) return -1;
     const DevTTPass& tp = M->tt[size_t(st[0].idx)];
     const DevNPass& np = M->n[size_t(st[1].idx)];
     const int f = M->precision == HLRC_PREC_BF16 ? FMT_BF16 : FMT_F16;
     if (tp.in != V_X || tp.out != V_T || tp.mode != OUT_SET) return -1;
-    if (np.vx != V_X || np.vt != V_T || np.out != V_Y || np.mode != OUT_ADD_ALPHA || np.ncta > 0) return -1;
+    if (np.vx != V_X || np.vt != V_T || np.out != V_Y || np.mode != OUT_ADD_ALPHA || np.ncta > 0 || !np.wcol) return -1;
     for (int g = 0; g < NFMT; ++g)
         if (g != f && (tp.nmseg[g] > 0 || np.nmseg[g] > 0)) return -1;
     return f;
@@ -586,8 +640,8 @@ hlrc_status enable_wide_smem(int dev) {
     static std::vector<int> done;
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_t()));
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_t()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_c()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_c()));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_n()));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_n()));
     done.push_back(dev);
@@ -803,6 +857,40 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             return st;
         }
     }
+    if (!p.wide.empty()) {
+        const WidePlan& W = p.wide;
+        size_t wb = 0;
+        auto take = [&](size_t b) { const size_t o_ = wb; wb = align_up(wb + b, 256); return o_; };
+        const size_t o_u = take(W.units.size() * sizeof(WTUnit)), o_b = take(W.blks.size() * sizeof(WTBlk)),
+                     o_s = take(W.slabs.size() * sizeof(uint32_t)), o_t = take(W.tiles.size() * sizeof(WTTile)),
+                     o_g = take(W.groups.size() * sizeof(TGroup)), o_e = take(W.t_exp.size());
+        e = cudaMalloc(&hp->w_static, std::max<size_t>(wb, 256));
+        if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_u, W.units.data(), W.units.size() * sizeof(WTUnit), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_b, W.blks.data(), W.blks.size() * sizeof(WTBlk), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_s, W.slabs.data(), W.slabs.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_t, W.tiles.data(), W.tiles.size() * sizeof(WTTile), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !W.groups.empty())
+            e = cudaMemcpy(hp->w_static + o_g, W.groups.data(), W.groups.size() * sizeof(TGroup), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_e, W.t_exp.data(), W.t_exp.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(hp->w_static);
+            cudaFree(hp->mr_tables);
+            cudaFree(hp->mr_arena);
+            cleanup();
+            return fail(HLRC_ERR_OOM, "64-vector tables of %zu bytes: %s", wb, cudaGetErrorString(e));
+        }
+        hp->w_units = reinterpret_cast<const WTUnit*>(hp->w_static + o_u);
+        hp->w_blks = reinterpret_cast<const WTBlk*>(hp->w_static + o_b);
+        hp->w_slabs = reinterpret_cast<const uint32_t*>(hp->w_static + o_s);
+        hp->w_tiles = reinterpret_cast<const WTTile*>(hp->w_static + o_t);
+        hp->w_groups = reinterpret_cast<const TGroup*>(hp->w_static + o_g);
+        hp->w_texp = reinterpret_cast<const int8_t*>(hp->w_static + o_e);
+        hp->w_nunits = int(W.units.size());
+        hp->w_ngroups = int(W.groups.size());
+        hp->w_npart = W.npart;
+        hp->info.device_bytes += int64_t(wb);
+    }
     hp->wide = wide_format(hp) >= 0;
     if (hp->wide && o.max_nrhs > MR_RB) {
         hlrc_status st = enable_wide_smem(dev);
@@ -815,6 +903,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             }
         }
         if (st != HLRC_OK) {
+            cudaFree(hp->w_static);
             cudaFree(hp->mr_tables);
             cudaFree(hp->mr_arena);
             cleanup();
@@ -822,7 +911,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         }
         Workspace w;
         z.carve(hp->w_arena, w);
-        hp->w_xs = w.w_xs; hp->w_ts = w.w_ts; hp->w_texp = w.w_texp; hp->w_part = w.w_part;
+        hp->w_xs = w.w_xs; hp->w_ts = w.w_ts; hp->w_part = w.w_part;
         hp->w_xmax = w.w_xmax; hp->w_g = w.w_g;
         hp->info.workspace_bytes += int64_t(z.bytes);
         hp->info.device_bytes += int64_t(z.bytes);
@@ -844,7 +933,7 @@ Workspace handle_workspace(hlrc_hmat M) {
     Workspace w;
     w.t = M->ws_t; w.t2 = M->ws_t2; w.part = M->part;
     w.mr_x = M->mr_x; w.mr_t = M->mr_t; w.mr_t2 = M->mr_t2; w.mr_part = M->mr_part;
-    w.w_xs = M->w_xs; w.w_ts = M->w_ts; w.w_texp = M->w_texp; w.w_part = M->w_part;
+    w.w_xs = M->w_xs; w.w_ts = M->w_ts; w.w_part = M->w_part;
     w.w_xmax = M->w_xmax; w.w_g = M->w_g;
     w.profile = M->profiling;
     return w;
@@ -1017,7 +1106,8 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
                 if (np.ncta > 0) {   // tree sweep (FP64 plans only)
                     k_ntree_f64<TREE_WARPS><<<np.ncta, TREE_WARPS * 32, np.tree_smem, s>>>(
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), np.tree,
-                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add, M->dev_err);
+                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add, M->dev_err, M->wait_ns,
+                        M->wait_skip);
                     return;
                 }
                 if (f64plan && np.nsegs[FMT_F64] > 0)
@@ -1189,6 +1279,7 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
     const DevTTPass& tp = M->tt[size_t(st[0].idx)];
     const DevNPass& np = M->n[size_t(st[1].idx)];
     const int64_t nx = M->ncols;
+    const bool bf = f == FMT_BF16;
     for (int r0 = 0; r0 < nrhs; r0 += WIDE_RHS) {
         const int nr = std::min(WIDE_RHS, nrhs - r0);
         const double* Xr = X + int64_t(r0) * ldx;
@@ -1197,53 +1288,48 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
         const unsigned gx = unsigned(std::min<int64_t>((nx + 255) / 256, 4 * 148));
         k_wide_xmax<<<dim3(std::max(1u, gx), unsigned(nr)), 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax);
         const unsigned gs = unsigned(std::max<int64_t>(1, (nx + TILE - 1) / TILE));
-        if (f == FMT_BF16) k_wide_xsplit<FMT_BF16><<<gs, 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax, ws.w_xs, ws.w_g);
+        if (bf) k_wide_xsplit<FMT_BF16><<<gs, 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax, ws.w_xs, ws.w_g);
         else k_wide_xsplit<FMT_F16><<<gs, 256, 0, s>>>(Xr, ldx, nx, nr, ws.w_xmax, ws.w_xs, ws.w_g);
         if (ws.profile) prof_end(M, s);
         M->launches += 2;
         HLRC_AFTER_LAUNCH("wide_xsplit");
-        if (tp.nmseg[f] > 0) {
+        if (M->w_nunits > 0) {
             if (ws.profile) prof_begin(M, stage_name(M, 2, st[0].idx), tp.alg_bytes, s);
-            if (f == FMT_BF16)
-                k_ttform_wide<FMT_BF16><<<tp.nmseg[f], WIDE_THREADS, wide_smem_t(), s>>>(
-                    tp.mseg[f], tp.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_part, M->dev_err);
+            if (bf)
+                k_ctform_wide<FMT_BF16><<<M->w_nunits, WIDE_THREADS, wide_smem_c(), s>>>(
+                    M->w_units, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
+                    M->dev_err, WaitCfg{M->wait_ns, M->wait_skip});
             else
-                k_ttform_wide<FMT_F16><<<tp.nmseg[f], WIDE_THREADS, wide_smem_t(), s>>>(
-                    tp.mseg[f], tp.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_part, M->dev_err);
+                k_ctform_wide<FMT_F16><<<M->w_nunits, WIDE_THREADS, wide_smem_c(), s>>>(
+                    M->w_units, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
+                    M->dev_err, WaitCfg{M->wait_ns, M->wait_skip});
             if (ws.profile) prof_end(M, s);
             M->launches += 1;
             HLRC_AFTER_LAUNCH(stage_name(M, 2, st[0].idx));
         }
-        if (tp.ngroups > 0) {
-            if (ws.profile) prof_begin(M, "ttfinish", tp.npart * WIDE_RHS * 4, s);
-            if (tp.ngroups1 > 0) {
-                if (f == FMT_BF16)
-                    k_ttfinish_wide<FMT_BF16, true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1,
-                                                                                           ws.w_part, ws.w_ts, ws.w_texp);
-                else
-                    k_ttfinish_wide<FMT_F16, true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1,
-                                                                                          ws.w_part, ws.w_ts, ws.w_texp);
-                M->launches += 1;
-            }
-            if (f == FMT_BF16)
-                k_ttfinish_wide<FMT_BF16, false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.w_part,
-                                                                                       ws.w_ts, ws.w_texp);
+        if (M->w_ngroups > 0) {
+            if (ws.profile) prof_begin(M, "ttfinish", M->w_npart * WIDE_RHS * 4, s);
+            if (bf)
+                k_ttfinish_wide<FMT_BF16><<<(M->w_ngroups + 7) / 8, 256, 0, s>>>(M->w_groups, M->w_ngroups, ws.w_part,
+                                                                                  ws.w_ts, M->w_texp);
             else
-                k_ttfinish_wide<FMT_F16, false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.w_part,
-                                                                                      ws.w_ts, ws.w_texp);
-            M->launches += 1;
+                k_ttfinish_wide<FMT_F16><<<(M->w_ngroups + 7) / 8, 256, 0, s>>>(M->w_groups, M->w_ngroups, ws.w_part,
+                                                                                 ws.w_ts, M->w_texp);
             if (ws.profile) prof_end(M, s);
+            M->launches += 1;
             HLRC_AFTER_LAUNCH("ttfinish");
         }
         if (np.nmseg[f] > 0) {
             const OutMap om{Y + int64_t(r0) * ldy, 1, ldy, nr};
             if (ws.profile) prof_begin(M, stage_name(M, 1, st[1].idx), np.alg_bytes, s);
-            if (f == FMT_BF16)
+            if (bf)
                 k_nform_wide<FMT_BF16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
-                    np.mseg[f], np.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_g, om, alpha, 1, M->dev_err);
+                    np.mseg[f], np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err,
+                    WaitCfg{M->wait_ns, M->wait_skip});
             else
                 k_nform_wide<FMT_F16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
-                    np.mseg[f], np.mcol, M->store, ws.w_xs, ws.w_ts, ws.w_texp, ws.w_g, om, alpha, 1, M->dev_err);
+                    np.mseg[f], np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err,
+                    WaitCfg{M->wait_ns, M->wait_skip});
             if (ws.profile) prof_end(M, s);
             M->launches += 1;
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st[1].idx));
@@ -1514,6 +1600,15 @@ extern "C" int hlrc_last_profile(hlrc_hmat M, const char** names, int* count, do
     return n;
 }
 
+extern "C" hlrc_status hlrc_debug_waits(hlrc_hmat M, int64_t limit_ns, int skip_handover) {
+    clear_error();
+    if (!M) return fail(HLRC_ERR_ARG, "hlrc_debug_waits: null handle");
+    if (limit_ns < 0 || limit_ns > int64_t(60) * 1000000000) return fail(HLRC_ERR_ARG, "hlrc_debug_waits: limit out of range");
+    M->wait_ns = limit_ns > 0 ? uint64_t(limit_ns) : 2000000000ull;
+    M->wait_skip = skip_handover != 0;
+    return HLRC_OK;
+}
+
 extern "C" hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code) {
     clear_error();
     if (!M || !code) return fail(HLRC_ERR_ARG, "hlrc_check_device_error: null argument");
@@ -1710,6 +1805,7 @@ extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     cudaFree(M->mr_arena);
     cudaFree(M->mr_tables);
     cudaFree(M->w_arena);
+    cudaFree(M->w_static);
     cudaFree(M->arena);
     delete M;
     return HLRC_OK;

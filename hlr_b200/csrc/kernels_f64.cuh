@@ -136,11 +136,16 @@ __device__ __forceinline__ void tree_bulk(double* dst, const double* src, uint32
                  "l"(src), "r"(bytes), "r"(tree_saddr(bar))
                  : "memory");
 }
-// Waits for phase 0 of the barrier, at most TREE_WAIT_TRIES probes (each
-// may suspend the thread for a short while); false when they run out.
-constexpr int TREE_WAIT_TRIES = 1 << 20;
-__device__ __forceinline__ bool tree_bar_wait(uint64_t* bar) {
-    for (int i = 0; i < TREE_WAIT_TRIES; ++i) {
+// Waits for phase 0 of the barrier for at most limit_ns of wall-clock time
+// (%globaltimer); false when the time ran out.
+__device__ __forceinline__ uint64_t tree_clock() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool tree_bar_wait(uint64_t* bar, uint64_t limit_ns) {
+    const uint64_t t0 = tree_clock();
+    for (uint32_t i = 0;; ++i) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -148,8 +153,8 @@ __device__ __forceinline__ bool tree_bar_wait(uint64_t* bar) {
             : "r"(tree_saddr(bar))
             : "memory");
         if (done) return true;
+        if ((i & 15u) == 15u && tree_clock() - t0 > limit_ns) return false;
     }
-    return false;
 }
 
 // Tree sweep of the H^2 transfers: one cluster of TREE_CLUSTER CTAs per
@@ -170,12 +175,15 @@ __device__ __forceinline__ bool tree_bar_wait(uint64_t* bar) {
 // ends the level.  Summation order is fixed: the result is deterministic.
 // A copy that never completes stops the CTA's work: it sets bit 0 of the
 // error word, keeps taking part in the cluster barriers, and waits
-// (bounded) for its other copies before returning.
+// (bounded) for its other copies before returning.  Each wait lasts at most
+// wait_ns; skip != 0 (the test hook of hlrc_debug_waits) announces 16 bytes
+// more on the first level's barrier than its copies deliver, so that its
+// wait runs out with no copy left in flight.
 template <int W>
 __global__ void __cluster_dims__(TREE_CLUSTER, 1, 1) __launch_bounds__(W * 32)
 k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, TreeArgs t,
             const double* __restrict__ A, const double* vx, const double* vt, double* out, double alpha, int add,
-            int* err) {
+            int* err, uint64_t wait_ns, int skip) {
     constexpr int TC = TREE_CLUSTER;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = int(cl.block_rank());
@@ -228,6 +236,7 @@ k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, Tr
                       &bars[gi]);
         }
     }
+    if (skip && tid == 0 && nlev > 0) tree_bar_expect(&bars[0], 16u);
     __syncthreads();   // every expectation is set: the one arrival may complete a phase
     if (tid == 0)
         for (int i = 0; i < nlev; ++i) tree_bar_arrive(&bars[i]);
@@ -244,7 +253,7 @@ k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, Tr
     const int hw = 2 * warp + (lane >> 4), l16 = lane & 15;
     bool failed = false;
     for (int gi = 0; gi < nlev; ++gi) {
-        const bool ok = failed || tree_bar_wait(&bars[gi]);
+        const bool ok = failed || tree_bar_wait(&bars[gi], wait_ns);
         if (__syncthreads_or(!ok)) {
             if (tid == 0 && !failed) atomicOr(err, 1);
             failed = true;
@@ -291,7 +300,7 @@ k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, Tr
         cl.sync();   // the level's rows are in every mirror; partials free
     }
     if (failed)
-        for (int k = 0; k < nlev; ++k) tree_bar_wait(&bars[k]);
+        for (int k = 0; k < nlev; ++k) tree_bar_wait(&bars[k], wait_ns);
 }
 
 // T-form: one warp per unit; lane l owns rows 2l, 2l+1 of every slab and

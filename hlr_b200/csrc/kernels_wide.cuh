@@ -14,40 +14,42 @@
 // up in neighbouring accumulator lanes (N-form) or columns (T-form).
 //   x: one power-of-two scale 2^g_r per vector (max |x_r| 2^g_r in
 //      [2^13, 2^14)), split once per pass into xs.
-//   t = V^T x (per low-rank column, times 2^g_r): the T-form epilogue writes
-//      it as a split row with its own power-of-two exponent e (the row's
-//      largest |t| 2^g_r 2^-e in [2^13, 2^14)), into ts and texp.
+//   t = V^T x (per low-rank column i, times 2^g_r): split rows with a static
+//      exponent c_i (2^c_i > ||V(:,i)||_1, so |t_i| 2^g_r 2^-c_i < 2^14),
+//      into ts; c_i comes from the planner (WidePlan::t_exp).
 //
 // Kernels (op N):
 //   k_wide_xmax / k_wide_xsplit   x -> xs (and g_r)
-//   k_ttform_wide   one CTA per input tile: t = V^T x for the tile's run of V
-//                   columns; A = 128 columns (K-major), B = the tile's xs
-//                   rows (MN-major), D = 128 columns x 128 terms in TMEM
-//                   (two buffers, so the epilogue of one block overlaps the
-//                   MMAs of the next); single-tile outputs go straight to
-//                   ts, the others to FP32 partials
-//   k_ttfinish_wide   partials of multi-tile outputs summed in tile order
-//                   (FP64), then split into ts
+//   k_ctform_wide   one CTA per unit of the column-cluster T-form: the V
+//                   slabs of blocks sharing a column cluster, stacked as the
+//                   N operand (<= 128 columns, K-major), times the split rows
+//                   of one column tile as the M operand (128 terms,
+//                   MN-major), accumulated over all the unit's tiles in TMEM;
+//                   t rows go straight to ts (or, for a piece of a long
+//                   cluster, to FP32 partials)
+//   k_ttfinish_wide   partials of the pieces summed in piece order (FP64),
+//                   then split into ts
 //   k_nform_wide    one CTA per output tile: y += U t + D x over the tile's
 //                   run of columns; A = 128 terms of 32 columns (MN-major,
 //                   gathered split rows), B = the 32 matrix columns
 //                   (MN-major), D = 128 terms x 64 rows in TMEM
 //
-// Scales in the N-form.  Column c of the run carries its chunk's scale s_c
-// and (t columns) the exponent e of its split row, f_c = s_c 2^e.  The CTA
-// first finds the largest f over its run, F, and multiplies the staged
-// matrix column by f_c / F (a power of two <= 1, exact unless the values
-// drop below the 16-bit range, where they are negligible against the run's
-// largest terms), so that one accumulator serves the whole run:
-// y_r += alpha F 2^-g_r (acc_hi + acc_lo).  The tensor cores accumulate in
-// FP32 over WIDE_FLUSH stages (64 columns) into one of two TMEM buffers; the
-// epilogue warps add each finished buffer to an FP64 accumulator in shared
-// memory while the MMAs fill the other, so long runs keep FP64 sums.
+// Scales in the N-form.  Column c of the run has the factor f_c = its chunk
+// scale (x columns) or its chunk scale times 2^c_i (t columns); with F = 2^E
+// the largest f over the run, the staged matrix column is multiplied by
+// f_c / F (a power of two <= 1: exact unless the values drop below the
+// 16-bit range, where they are negligible against the run's largest terms),
+// so that one accumulator serves the whole run:
+// y_r += alpha F 2^-g_r (acc_hi + acc_lo).  All factors are fixed at upload
+// (WCol, E per run).  The tensor cores accumulate in FP32 over WIDE_FLUSH
+// stages (64 columns) into one of two TMEM buffers; the epilogue warps add
+// each finished buffer to an FP64 accumulator in shared memory while the
+// MMAs fill the other, so long runs keep FP64 sums.
 //
 // Roles (224 threads): warps 0-3 read the accumulators (warp w reads TMEM
 // lanes 32w .. 32w + 31), warp 4 allocates TMEM and issues the MMAs (one
-// thread), warps 5-6 stage operands with 16-byte cp.async copies into the
-// 128-byte-swizzled layouts, zero-filling everything outside the run.
+// thread), warps 5-6 stage operands with cp.async copies into the
+// 128-byte-swizzled layouts, zero-filling everything outside the data.
 // Stages are handed over with mbarriers: "full" (copies landed, made
 // visible to the tensor cores' proxy, 64 producer arrivals), "empty" (the
 // stage's MMAs completed, tcgen05.commit).  Every wait is bounded
@@ -73,9 +75,11 @@ constexpr int WIDE_THREADS = 224;     // 4 epilogue warps, 1 MMA warp, 2 produce
 constexpr int WIDE_PRODUCERS = 64;
 constexpr int WIDE_NS_N = 6;          // N-form stages (32 columns each): 2 CTAs per SM
 constexpr int WIDE_FLUSH = 2;         // N-form stages per FP32 accumulation (64 columns), then added in FP64
-constexpr int WIDE_NS_T = 4;          // tile T-form stages (128 columns each): 2 CTAs per SM (TMEM: 256 columns each)
+constexpr int WIDE_NS_C = 3;          // column-cluster T-form stages (one tile each): 2 CTAs per SM
 constexpr int WIDE_LAG_N = WIDE_NS_N - 2;   // copy groups a producer keeps in flight
-constexpr int WIDE_LAG_T = WIDE_NS_T - 1;
+constexpr int WIDE_LAG_C = WIDE_NS_C - 1;
+constexpr int WIDE_PF = WIDE_LAG_N + 1;     // N-form: column-table entries prefetched this many stages ahead
+constexpr int WIDE_WQ = WIDE_PF + WIDE_LAG_N + 1;   // ring of prefetched column-table entries
 constexpr int WIDE_ERR_WAIT = 2;      // device error word bit: a wait of a wide kernel ran out
 
 // N-form stage: A (vector terms, 2 M-atoms x 4 K-atoms) 8 KB, B (matrix, 4 K-atoms) 4 KB
@@ -84,12 +88,17 @@ constexpr int WIDE_N_STAGE = 12288;
 // (the 16 lanes that add one row of 16 vectors hit 16 different bank pairs)
 constexpr int WIDE_ACC_LD = TILE + 1;
 constexpr int WIDE_ACC_BYTES = WIDE_RHS * WIDE_ACC_LD * 8;
-// tile T-form: B (the tile's split rows: 2 N-atoms x 8 K-atoms) 16 KB, stages of A (16 M-atoms) 16 KB
-constexpr int WIDE_T_B = 16384;
-constexpr int WIDE_T_STAGE = 16384;
+constexpr int WIDE_WQ_BYTES = WIDE_WQ * WIDE_PRODUCERS * 8;
+// column-cluster T-form stage: A (split rows of a tile: 2 M-atoms x 8 K-atoms)
+// 16 KB, B (<= 128 stacked V columns: 16 atoms) 16 KB
+constexpr int WIDE_C_STAGE = 32768;
+constexpr int WIDE_C_TABLES = WT_MAXB * 16 + WT_MAXN * 4 + WT_MAXT * WT_MAXB * 4;
 constexpr int WIDE_BAR_BYTES = 256;   // mbarriers and the TMEM address
-constexpr int wide_smem_n() { return 1024 + WIDE_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES + WIDE_BAR_BYTES; }
-constexpr int wide_smem_t() { return 1024 + WIDE_T_B + WIDE_NS_T * WIDE_T_STAGE + WIDE_BAR_BYTES; }
+constexpr int wide_smem_n() {
+    return 1024 + WIDE_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES + WIDE_WQ_BYTES + WIDE_BAR_BYTES;
+}
+constexpr int wide_smem_c() { return 1024 + WIDE_NS_C * WIDE_C_STAGE + WIDE_C_TABLES + WIDE_BAR_BYTES; }
+static_assert(WIDE_NS_C * WIDE_C_STAGE >= WT_MAXN * WIDE_TERMS * 4, "T-form epilogue transpose fits the stages");
 
 template <int FMT> struct WideT;
 template <> struct WideT<FMT_F16> {
@@ -136,18 +145,27 @@ __device__ __forceinline__ uint32_t wide_split(double v) {
 constexpr int WIDE_NOEXP = -100000;
 __device__ __forceinline__ int wide_ilogb(double a) { return a > 0.0 ? ilogb(a) : WIDE_NOEXP; }
 
+// Wait bound of the kernels that hand work over with mbarriers, and the
+// test hook of hlrc_debug_waits: skip != 0 leaves the first hand-over of
+// every CTA undone (its producers never signal stage 0), so that the
+// consumer's wait runs out, as a wait on a flag that nothing sets.
+struct WaitCfg {
+    uint64_t limit_ns;
+    int skip;
+};
+
 // error flag shared by all CTAs of a pass: a bounded wait that ran out
 __device__ __forceinline__ bool wide_aborted(const int* err) {
     return (*reinterpret_cast<const volatile int*>(err) & WIDE_ERR_WAIT) != 0;
 }
-__device__ __forceinline__ bool wide_wait(uint64_t* bar, uint32_t parity, int* err) {
+__device__ __forceinline__ bool wide_wait(uint64_t* bar, uint32_t parity, int* err, uint64_t limit_ns) {
     if (tc5::mbar_try(bar, parity)) return true;
     const uint64_t t0 = tc5::globaltimer();
     for (uint32_t it = 1;; ++it) {
         if (tc5::mbar_try(bar, parity)) return true;
         if ((it & 63u) == 0u) {
             if (wide_aborted(err)) return false;
-            if (tc5::globaltimer() - t0 > tc5::WAIT_LIMIT_NS) {
+            if (tc5::globaltimer() - t0 > limit_ns) {
                 atomicOr(err, WIDE_ERR_WAIT);
                 return false;
             }
@@ -211,30 +229,22 @@ k_wide_xsplit(const double* __restrict__ X, int64_t ldx, int64_t n, int nr, cons
     }
 }
 
-// split row of 64 values (already times 2^g_r) with its own exponent e:
-// |v| 2^-e < 2^14; a lane holds vectors 2l, 2l + 1
+// split row of 64 values (times 2^g_r) with the static exponent e of its t
+// entry; a lane holds vectors 2l, 2l + 1
 template <int FMT>
-__device__ __forceinline__ void wide_store_row(double v0, double v1, uint32_t* __restrict__ row, int8_t* texp,
-                                               int lane) {
-    int e = max(wide_ilogb(fabs(v0)), wide_ilogb(fabs(v1)));
-    for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
-    e = e == WIDE_NOEXP ? 0 : min(120, max(-120, e - 13));
-    const uint32_t a = wide_split<FMT>(ldexp(v0, -e)), b = wide_split<FMT>(ldexp(v1, -e));
-    reinterpret_cast<uint2*>(row)[lane] = make_uint2(a, b);
-    if (lane == 0) *texp = int8_t(e);
+__device__ __forceinline__ void wide_store_row(double v0, double v1, int e, uint32_t* __restrict__ row, int lane) {
+    reinterpret_cast<uint2*>(row)[lane] = make_uint2(wide_split<FMT>(ldexp(v0, -e)), wide_split<FMT>(ldexp(v1, -e)));
 }
 
-// Partials of multi-tile outputs (FP32, 64 per entry: part[entry * 64 + r]):
-// group g sums slots i < nslots of its nc columns, slot i of column j at
-// entry slot0 + i * nc + j, in tile order (FP64).  One warp per group, its
-// columns one after the other; lane l takes vectors 2l, 2l + 1.  TO_PART:
-// the first level of a two-level finish, written as FP32 partials at entry
-// g.out + j; otherwise the sums become split rows of ts (entry g.out + j)
-// with their exponents.
-template <int FMT, bool TO_PART>
+// Partials of the pieces of long column clusters (FP32, 64 per entry:
+// part[entry * 64 + r]): group g sums pieces i < nslots of its nc columns,
+// piece i of column j at entry slot0 + i * nc + j, in piece order (FP64),
+// into the split rows of ts (entry g.out + j).  One warp per group, its
+// columns one after the other; lane l takes vectors 2l, 2l + 1.
+template <int FMT>
 __global__ void __launch_bounds__(256)
-k_ttfinish_wide(const TGroup* __restrict__ groups, int ngroups, float* part, uint32_t* __restrict__ ts,
-                int8_t* __restrict__ texp) {
+k_ttfinish_wide(const TGroup* __restrict__ groups, int ngroups, const float* __restrict__ part,
+                uint32_t* __restrict__ ts, const int8_t* __restrict__ texp) {
     const int gid = int(blockIdx.x) * 8 + int(threadIdx.x >> 5);
     if (gid >= ngroups) return;
     const int lane = threadIdx.x & 31;
@@ -252,225 +262,193 @@ k_ttfinish_wide(const TGroup* __restrict__ groups, int ngroups, float* part, uin
             const float2 a = __ldcs(p + size_t(i) * step);
             s0[0] += a.x; s1[0] += a.y;
         }
-        const double v0 = s0[0] + s0[1], v1 = s1[0] + s1[1];
         const size_t e = size_t(gr.out) + j;
-        if constexpr (TO_PART) {
-            reinterpret_cast<float2*>(part)[e * 32 + lane] = make_float2(float(v0), float(v1));
-        } else {
-            wide_store_row<FMT>(v0, v1, ts + e * (WIDE_TERMS / 2), texp + e, lane);
-        }
+        wide_store_row<FMT>(s0[0] + s0[1], s1[0] + s1[1], int(texp[e]), ts + e * (WIDE_TERMS / 2), lane);
     }
 }
 
-// ------------------------------------------------------------ tile T-form
-// t (x 2^g) of the columns of each tile's run of V: a CTA per run (MSeg),
-// 128 columns per block.  Column m of a block at run column c = 128 b + m:
-// its 64 values (x 2^g) -> split row of ts (MCol: output entry | MC_DIRECT)
-// or FP32 partial entry.
+// ------------------------------------------------------ column-cluster T-form
+// One CTA per unit (WTUnit): for each of its tiles, A = the tile's split rows
+// of x (M = 128 terms, K = 64 tile rows, MN-major) and B = the V slabs of the
+// unit's blocks in that tile (N = the stacked columns, K-major); D (128 terms
+// x N) accumulates over all tiles.  The epilogue transposes D through shared
+// memory and writes one split row (or FP32 partial) per column.
 template <int FMT>
 __global__ void __launch_bounds__(WIDE_THREADS, 2)
-k_ttform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-              const uint32_t* __restrict__ xs, uint32_t* __restrict__ ts, int8_t* __restrict__ texp,
-              float* __restrict__ part, int* err) {
+k_ctform_wide(const WTUnit* __restrict__ units, const WTBlk* __restrict__ blks, const uint32_t* __restrict__ slabs,
+              const WTTile* __restrict__ tiles, const uint8_t* __restrict__ A, const uint32_t* __restrict__ xs,
+              uint32_t* __restrict__ ts, const int8_t* __restrict__ texp, float* __restrict__ part, int* err,
+              WaitCfg wc) {
     using namespace tc5;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    uint8_t* sB = sm;                                   // the tile's split rows
-    uint8_t* sA = sm + WIDE_T_B;                        // stages
-    uint64_t* full = reinterpret_cast<uint64_t*>(sA + WIDE_NS_T * WIDE_T_STAGE);
-    uint64_t* empty = full + WIDE_NS_T;
-    uint64_t* tfull = empty + WIDE_NS_T;                // accumulator buffers ready
-    uint64_t* tempty = tfull + 2;                       // accumulator buffers read
-    uint64_t* done = tempty + 2;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    WTBlk* sblk = reinterpret_cast<WTBlk*>(sm + WIDE_NS_C * WIDE_C_STAGE);
+    uint32_t* scol = reinterpret_cast<uint32_t*>(sblk + WT_MAXB);           // stacked column -> (block << 16) | column
+    uint32_t* sslab = scol + WT_MAXN;                                       // [tile][block] store offsets / 16
+    uint64_t* full = reinterpret_cast<uint64_t*>(sslab + WT_MAXT * WT_MAXB);
+    uint64_t* empty = full + WIDE_NS_C;
+    uint64_t* accf = empty + WIDE_NS_C;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(accf + 1);
 
-    const MSeg sg = segs[blockIdx.x];
-    const int ncols = int(sg.ncols);
-    const int nblk = (ncols + 127) / 128;
+    const WTUnit u = units[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (nblk == 0) return;
+    const int nt = u.ntiles, nb = u.nblk, nc = u.ncols, npad = (nc + 15) & ~15;
+    if (nt == 0 || nc == 0) return;
+    for (int j = threadIdx.x; j < nb; j += WIDE_THREADS) sblk[j] = blks[u.blk0 + j];
+    for (int i = threadIdx.x; i < nt * nb; i += WIDE_THREADS) sslab[i] = slabs[u.slab0 + i];
     if (threadIdx.x == 0) {
-        for (int i = 0; i < WIDE_NS_T; ++i) {
+        for (int i = 0; i < WIDE_NS_C; ++i) {
             mbar_init(full + i, WIDE_PRODUCERS);
             mbar_init(empty + i, 1);
         }
-        for (int i = 0; i < 2; ++i) {
-            mbar_init(tfull + i, 1);
-            mbar_init(tempty + i, 128);
-        }
-        mbar_init(done, 1);
+        mbar_init(accf, 1);
         mbar_init_fence();
     }
-    if (warp == 4) tmem_alloc(tslot, 256);
+    if (warp == 4) tmem_alloc(tslot, 128);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    for (int j = threadIdx.x; j < nb; j += WIDE_THREADS)
+        for (int l = 0; l < sblk[j].k; ++l) scol[sblk[j].off + l] = (uint32_t(j) << 16) | uint32_t(l);
+    __syncthreads();
     const uint32_t tmem = *tslot;
-    const uint8_t* base = A + size_t(sg.a16) * 16;
-    const int colb = int(sg.ld) * 2;
-    const MCol* ctab = cols + sg.col0;
 
     if (warp >= 5) {
         // ---------------------------------------------------- producers
         const int p = threadIdx.x - 160;
-        const uint32_t b0 = smem_u32(sB), a0 = smem_u32(sA);
-        // the tile's split rows (B operand, 1024 units): row k (tile entry),
-        // unit u -> N-atom u / 8 (8 KB apart), K-atom k / 8, row k % 8
-        for (int q = p; q < 1024; q += WIDE_PRODUCERS) {
-            const int k = q >> 4, u = q & 15;
-            const bool ok = k < int(sg.rows);
-            const uint32_t dst = b0 + uint32_t(u >> 3) * 8192u + uint32_t(k >> 3) * 1024u + swz(k & 7, u & 7);
-            tc5::cp16(dst, ok ? static_cast<const void*>(xs + (size_t(sg.vo) + k) * (WIDE_TERMS / 2) + u * 4)
-                         : static_cast<const void*>(xs),
-                 ok ? 16u : 0u);
-        }
+        const uint32_t s0 = smem_u32(sm);
         bool ok = true;
-        for (int s = 0; s < nblk && ok; ++s) {
-            const int slot = s % WIDE_NS_T;
-            if (s >= WIDE_NS_T) ok = wide_wait(empty + slot, uint32_t((s / WIDE_NS_T) - 1) & 1u, err);
+        for (int q = 0; q < nt && ok; ++q) {
+            const int slot = q % WIDE_NS_C;
+            if (q >= WIDE_NS_C) ok = wide_wait(empty + slot, uint32_t((q / WIDE_NS_C) - 1) & 1u, err, wc.limit_ns);
             if (!ok) break;
-            // 128 columns x 8 units: column m (M index) -> atom m / 8, row m % 8; unit j = rows 8j..8j+7
-            const uint32_t sa = a0 + uint32_t(slot) * WIDE_T_STAGE;
-            for (int q = p; q < 1024; q += WIDE_PRODUCERS) {
-                const int m = q >> 3, j = q & 7;
-                const int c = 128 * s + m;
-                const bool v = c < ncols && 8 * j < int(sg.ld);
-                const uint32_t dst = sa + uint32_t(m >> 3) * 1024u + swz(m & 7, j);
-                tc5::cp16(dst, v ? static_cast<const void*>(base + size_t(c) * colb + 16 * j) : static_cast<const void*>(A),
-                     v ? 16u : 0u);
+            const WTTile tl = tiles[u.tile0 + q];
+            const uint32_t sa = s0 + uint32_t(slot) * WIDE_C_STAGE, sb = sa + 16384u;
+            // A: split row k (tile entry), unit v -> M-atom v / 8 (8 KB apart), K-atom k / 8, row k % 8
+            for (int i = p; i < 1024; i += WIDE_PRODUCERS) {
+                const int k = i >> 4, v = i & 15;
+                const bool in = k < int(tl.rows);
+                tc5::cp16(sa + uint32_t(v >> 3) * 8192u + uint32_t(k >> 3) * 1024u + swz(k & 7, v & 7),
+                          in ? static_cast<const void*>(xs + (size_t(tl.v_off) + k) * (WIDE_TERMS / 2) + v * 4)
+                             : static_cast<const void*>(xs),
+                          in ? 16u : 0u);
+            }
+            // B: stacked column n, unit jj (tile rows 8jj .. 8jj+7) -> atom n / 8, row n % 8
+            for (int i = p; i < npad * 8; i += WIDE_PRODUCERS) {
+                const int n = i >> 3, jj = i & 7;
+                bool in = n < nc && 8 * jj < int(tl.ld);
+                const uint8_t* src = A;
+                if (in) {
+                    const uint32_t cm = scol[n];
+                    src = A + size_t(sslab[q * nb + int(cm >> 16)]) * 16 + size_t(cm & 0xffffu) * tl.ld * 2 + 16 * jj;
+                }
+                tc5::cp16(sb + uint32_t(n >> 3) * 1024u + swz(n & 7, jj), src, in ? 16u : 0u);
             }
             tc5::cp_commit();
-            if (s >= WIDE_LAG_T) {
-                tc5::cp_wait<WIDE_LAG_T>();
+            if (q >= WIDE_LAG_C) {
+                tc5::cp_wait<WIDE_LAG_C>();
                 fence_async_smem();
-                mbar_arrive(full + (s - WIDE_LAG_T) % WIDE_NS_T);
+                if (!(wc.skip && q == WIDE_LAG_C)) mbar_arrive(full + (q - WIDE_LAG_C) % WIDE_NS_C);
             }
         }
         tc5::cp_wait<0>();
         fence_async_smem();
         if (ok)
-            for (int s = max(0, nblk - WIDE_LAG_T); s < nblk; ++s) mbar_arrive(full + s % WIDE_NS_T);
+            for (int q = max(0, nt - WIDE_LAG_C); q < nt; ++q)
+                if (!(wc.skip && q == 0)) mbar_arrive(full + q % WIDE_NS_C);
     } else if (warp == 4) {
         // ------------------------------------------------------- MMA issue
         if (lane == 0) {
-            constexpr uint32_t ID = tc5::idesc_f16(128, 128, WideT<FMT>::bf16, false, true);
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-            bool ok = true;
-            for (int s = 0; s < nblk; ++s) {
-                const int slot = s % WIDE_NS_T, buf = s & 1;
-                ok = wide_wait(full + slot, uint32_t(s / WIDE_NS_T) & 1u, err);
-                if (ok && s >= 2) ok = wide_wait(tempty + buf, uint32_t((s >> 1) - 1) & 1u, err);
-                if (!ok) break;
+            const uint32_t id = tc5::idesc_f16(128, npad, WideT<FMT>::bf16, true, false);
+            const uint32_t s0 = smem_u32(sm);
+            for (int q = 0; q < nt; ++q) {
+                const int slot = q % WIDE_NS_C;
+                if (!wide_wait(full + slot, uint32_t(q / WIDE_NS_C) & 1u, err, wc.limit_ns)) break;
                 tc_fence_after();
-                const uint32_t d = tmem + uint32_t(buf) * 128u;
-                const uint32_t sa = a0 + uint32_t(slot) * WIDE_T_STAGE;
+                const uint32_t sa = s0 + uint32_t(slot) * WIDE_C_STAGE, sb = sa + 16384u;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    mma_f16(d, sdesc(sa + 32u * j, 16u, 1024u), sdesc(b0 + 2048u * j, 8192u, 1024u), ID, j > 0);
+                    mma_f16(tmem, sdesc(sa + 2048u * j, 8192u, 1024u), sdesc(sb + 32u * j, 16u, 1024u), id,
+                            (q > 0 || j > 0) ? 1u : 0u);
                 mma_commit(empty + slot);
-                mma_commit(tfull + buf);
             }
-            // every MMA issued has completed before TMEM is freed (this wait
-            // does not give up on the error flag: MMAs always finish)
-            mma_commit(done);
-            if (!mbar_wait(done, 0u)) atomicOr(err, WIDE_ERR_WAIT);
+            // every MMA issued has completed before the epilogue reads TMEM
+            // and before TMEM is freed (this wait does not give up on the
+            // error flag: MMAs always finish)
+            mma_commit(accf);
+            if (!mbar_wait(accf, 0u, wc.limit_ns)) atomicOr(err, WIDE_ERR_WAIT);
         }
         __syncwarp();
     } else {
         // -------------------------------------------------------- epilogue
-        const uint32_t lanebase = tmem + (uint32_t(32 * warp) << 16);
-        for (int s = 0; s < nblk; ++s) {
-            const int buf = s & 1;
-            // warp-uniform: the TMEM loads below are collective
-            if (!__all_sync(0xffffffffu, wide_wait(tfull + buf, uint32_t(s >> 1) & 1u, err))) break;
-            tc_fence_after();
-            const int m = 32 * warp + lane, c = 128 * s + m;
-            const bool have = c < ncols;
-            const MCol mc = have ? ctab[c] : MCol{0u, 0.f};
-            const uint32_t ta = lanebase + uint32_t(buf) * 128u;
-            const double sc = double(mc.scale);
-            const bool direct = (mc.idx & MC_DIRECT) != 0;
-            // TMEM loads are collective: every lane runs both passes, and
-            // only the stores depend on the lane's column.  Pass 1: the
-            // column's largest value (the exponent of its split row); pass
-            // 2: the split terms (direct outputs) or the FP32 partials.
-            int ex = WIDE_NOEXP;
-#pragma unroll 1
-            for (int h = 0; h < 4; ++h) {
+        bool ok = __all_sync(0xffffffffu, wide_wait(accf, 0u, err, wc.limit_ns) && !wide_aborted(err));
+        tc_fence_after();
+        // every stage has been consumed: the stage memory holds the
+        // transpose red[n][m] (FP32, 128 terms per stacked column)
+        float* red = reinterpret_cast<float*>(sm);
+        if (ok) {
+            const uint32_t la = tmem + (uint32_t(32 * warp) << 16);
+            const int m = 32 * warp + lane;
+            for (int c = 0; c < npad; c += 32) {
                 float f[32];
-                tc5::tmem_ld32(ta + uint32_t(32 * h), f);
+                tmem_ld32(la + uint32_t(c), f);
 #pragma unroll
-                for (int i = 0; i < 16; ++i)
-                    ex = max(ex, wide_ilogb(fabs((double(f[2 * i]) + double(f[2 * i + 1])) * sc)));
+                for (int i = 0; i < 32; ++i)
+                    if (c + i < nc) red[(c + i) * WIDE_TERMS + m] = f[i];
             }
-            ex = ex == WIDE_NOEXP ? 0 : min(120, max(-120, ex - 13));
-            uint4* row = reinterpret_cast<uint4*>(ts + size_t(mc.idx & ~MC_DIRECT) * (WIDE_TERMS / 2));
-            float4* o = reinterpret_cast<float4*>(part + size_t(mc.idx & ~MC_DIRECT) * WIDE_RHS);
-#pragma unroll 1
-            for (int h = 0; h < 4; ++h) {
-                float f[32];
-                tc5::tmem_ld32(ta + uint32_t(32 * h), f);
-                if (!have) continue;
-                if (direct) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        uint32_t w[4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            const int k = 4 * q + i;
-                            w[i] = wide_split<FMT>(ldexp((double(f[2 * k]) + double(f[2 * k + 1])) * sc, -ex));
-                        }
-                        row[4 * h + q] = make_uint4(w[0], w[1], w[2], w[3]);
-                    }
+        }
+        tc_fence_before();
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        if (__all_sync(0xffffffffu, ok)) {
+            for (int n = warp; n < nc; n += 4) {
+                const uint32_t cm = scol[n];
+                const WTBlk& b = sblk[cm >> 16];
+                const int l = int(cm & 0xffffu);
+                const float4 t4 = reinterpret_cast<const float4*>(red + n * WIDE_TERMS)[lane];
+                const double sc = double(b.scale);
+                const double v0 = (double(t4.x) + double(t4.y)) * sc, v1 = (double(t4.z) + double(t4.w)) * sc;
+                if (u.npieces == 1) {
+                    const size_t e = size_t(b.toff) + size_t(l);
+                    wide_store_row<FMT>(v0, v1, int(texp[e]), ts + e * (WIDE_TERMS / 2), lane);
                 } else {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float w[4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            const int k = 4 * q + i;
-                            w[i] = float((double(f[2 * k]) + double(f[2 * k + 1])) * sc);
-                        }
-                        o[4 * h + q] = make_float4(w[0], w[1], w[2], w[3]);
-                    }
+                    const size_t e = size_t(b.pbase) + size_t(u.piece) * b.k + size_t(l);
+                    reinterpret_cast<float2*>(part)[e * 32 + lane] = make_float2(float(v0), float(v1));
                 }
             }
-            if (have && direct) texp[mc.idx & ~MC_DIRECT] = int8_t(ex);
-            tc_fence_before();
-            mbar_arrive(tempty + buf);
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 4) {
         tc_fence_after();
-        tmem_dealloc(tmem, 256);
+        tmem_dealloc(tmem, 128);
     }
 }
 
 // ----------------------------------------------------------------- N-form
 // y (+)= alpha op(M) X for the WIDE_RHS vectors: a CTA per output tile's run
-// (MSeg), 32 columns per stage.  om maps (row, vector) to y.
+// (MSeg; E = the run's factor exponent in MSeg.pad), 32 columns per stage;
+// wcol[col0 + c]: the vector entry and factor of run column c.  om maps
+// (row, vector) to y.
 template <int FMT>
 __global__ void __launch_bounds__(WIDE_THREADS, 2)
-k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
-             const uint32_t* __restrict__ xs, const uint32_t* __restrict__ ts, const int8_t* __restrict__ texp,
-             const int* __restrict__ g, OutMap om, double alpha, int add, int* err) {
+k_nform_wide(const MSeg* __restrict__ segs, const WCol* __restrict__ wcol, const uint8_t* __restrict__ A,
+             const uint32_t* __restrict__ xs, const uint32_t* __restrict__ ts, const int* __restrict__ g, OutMap om,
+             double alpha, int add, int* err, WaitCfg wc) {
     using namespace tc5;
     using W = WideT<FMT>;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     double* acc = reinterpret_cast<double*>(sm + WIDE_NS_N * WIDE_N_STAGE);   // [r][row], ld WIDE_ACC_LD
-    uint64_t* full = reinterpret_cast<uint64_t*>(sm + WIDE_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES);
+    uint2* wq = reinterpret_cast<uint2*>(sm + WIDE_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES);   // [slot][producer]
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + WIDE_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES + WIDE_WQ_BYTES);
     uint64_t* empty = full + WIDE_NS_N;
     uint64_t* tfull = empty + WIDE_NS_N;                // accumulator buffers ready
     uint64_t* tempty = tfull + 2;                       // accumulator buffers drained
     uint64_t* done = tempty + 2;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-    int* sref = reinterpret_cast<int*>(tslot + 1);      // largest column exponent of the run
-    int* wred = sref + 1;                               // per-warp maxima (7)
 
     const MSeg sg = segs[blockIdx.x];
     const int ncols = int(sg.ncols);
@@ -478,16 +456,7 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
     const int ngrp = (nst + WIDE_FLUSH - 1) / WIDE_FLUSH;   // FP32 accumulations
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (nst == 0) return;
-    const MCol* ctab = cols + sg.col0;
-    // exponent of column c's factor: its chunk scale times 2^e of its split row
-    auto col_exp = [&](const MCol& m) {
-        const int es = ilogbf(m.scale);
-        return (m.idx & VEC_T) ? es + int(texp[m.idx & ~VEC_T]) : es;
-    };
-    int emax = WIDE_NOEXP;
-    for (int c = threadIdx.x; c < ncols; c += WIDE_THREADS) emax = max(emax, col_exp(ctab[c]));
-    for (int o = 16; o > 0; o >>= 1) emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-    if (lane == 0) wred[warp] = emax;
+    const int E = int(sg.pad);
     for (int i = threadIdx.x; i < WIDE_RHS * WIDE_ACC_LD; i += WIDE_THREADS) acc[i] = 0.0;
     if (threadIdx.x == 0) {
         for (int i = 0; i < WIDE_NS_N; ++i) {
@@ -505,43 +474,64 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (threadIdx.x == 0) {
-        int m = wred[0];
-        for (int w = 1; w < WIDE_THREADS / 32; ++w) m = max(m, wred[w]);
-        *sref = m;
-    }
-    __syncthreads();
-    const int E = *sref;
     const uint32_t tmem = *tslot;
 
     if (warp >= 5) {
         // ---------------------------------------------------- producers
-        // thread p stages column p / 2 of every stage: half p % 2 of its
+        // thread p stages column k = p / 2 of every stage: half p % 2 of its
         // split row (8 units, M-atom p % 2) and units 4 (p % 2) .. +3 of the
-        // matrix column
+        // matrix column.  Its column-table entries arrive WIDE_PF stages
+        // ahead in the shared ring wq (cp.async, so no load stalls the
+        // loop); an entry stays there until its stage has been handed over.
         const int p = threadIdx.x - 160, k = p >> 1, half = p & 1;
         const uint8_t* base = A + size_t(sg.a16) * 16;
         const int colb = int(sg.ld) * 2;
         const uint32_t s0 = smem_u32(sm);
-        typename W::h2 fac[WIDE_LAG_N + 1];
+        const WCol* wtab = wcol + sg.col0;
+        auto prefetch = [&](int st) {   // column-table entry of stage st into its ring slot
+            const int c = 32 * st + k;
+            const bool in = c < ncols;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                             smem_u32(wq + (st % WIDE_WQ) * WIDE_PRODUCERS + p)),
+                         "l"(in ? static_cast<const void*>(wtab + c) : static_cast<const void*>(wcol)), "r"(in ? 8u : 0u)
+                         : "memory");
+        };
+        for (int st = 0; st < WIDE_PF && st < nst; ++st) prefetch(st);
+        tc5::cp_commit();
+        tc5::cp_wait<0>();
+        auto finish = [&](int sd) {   // stage sd has landed: scale its matrix column, hand it over
+            const uint32_t fb = wq[(sd % WIDE_WQ) * WIDE_PRODUCERS + p].y;
+            const typename W::h2 f = *reinterpret_cast<const typename W::h2*>(&fb);
+            uint8_t* col = sm + (sd % WIDE_NS_N) * WIDE_N_STAGE + 8192 + (k >> 3) * 1024;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                uint4* q = reinterpret_cast<uint4*>(col + swz(k & 7, 4 * half + i));
+                uint4 w = *q;
+                w.x = W::mul(w.x, f); w.y = W::mul(w.y, f); w.z = W::mul(w.z, f); w.w = W::mul(w.w, f);
+                *q = w;
+            }
+            fence_async_smem();
+            if (!(wc.skip && sd == 0)) mbar_arrive(full + sd % WIDE_NS_N);
+        };
         bool ok = true;
         for (int s = 0; s < nst && ok; ++s) {
             const int slot = s % WIDE_NS_N;
-            if (s >= WIDE_NS_N) ok = wide_wait(empty + slot, uint32_t((s / WIDE_NS_N) - 1) & 1u, err);
+            if (s >= WIDE_NS_N) ok = wide_wait(empty + slot, uint32_t((s / WIDE_NS_N) - 1) & 1u, err, wc.limit_ns);
             if (!ok) break;
             const int c = 32 * s + k;
             const bool have = c < ncols;
-            const MCol mc = have ? ctab[c] : MCol{0u, 1.f};
-            fac[s % (WIDE_LAG_N + 1)] = W::pow2(have ? col_exp(mc) - E : 0);
-            const uint32_t* vrow = (mc.idx & VEC_T) ? ts + size_t(mc.idx & ~VEC_T) * (WIDE_TERMS / 2)
-                                                    : xs + size_t(mc.idx) * (WIDE_TERMS / 2);
+            const uint2 wce = wq[(s % WIDE_WQ) * WIDE_PRODUCERS + p];
+            const uint32_t idx = wce.x;
+            const uint32_t* vrow = (idx & VEC_T) ? ts + size_t(idx & ~VEC_T) * (WIDE_TERMS / 2)
+                                                 : xs + size_t(idx) * (WIDE_TERMS / 2);
             const uint32_t sa = s0 + uint32_t(slot) * WIDE_N_STAGE, sb = sa + 8192u;
             // vector terms: unit u of the row -> M-atom u / 8 (4 KB apart), K-atom k / 8, row k % 8
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const int u = 8 * half + i;
+                const int uu = 8 * half + i;
                 tc5::cp16(sa + uint32_t(half) * 4096u + uint32_t(k >> 3) * 1024u + swz(k & 7, i),
-                          have ? static_cast<const void*>(vrow + 4 * u) : static_cast<const void*>(xs), have ? 16u : 0u);
+                          have ? static_cast<const void*>(vrow + 4 * uu) : static_cast<const void*>(xs),
+                          have ? 16u : 0u);
             }
             // matrix column: unit j (rows 8j .. 8j+7) -> K-atom k / 8, row k % 8
 #pragma unroll
@@ -552,20 +542,8 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
                           v ? static_cast<const void*>(base + size_t(c) * colb + 16 * j) : static_cast<const void*>(A),
                           v ? 16u : 0u);
             }
+            if (s + WIDE_PF < nst) prefetch(s + WIDE_PF);
             tc5::cp_commit();
-            auto finish = [&](int sd) {   // stage sd has landed: scale its matrix column, hand it over
-                const typename W::h2 f = fac[sd % (WIDE_LAG_N + 1)];
-                uint8_t* col = sm + (sd % WIDE_NS_N) * WIDE_N_STAGE + 8192 + (k >> 3) * 1024;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    uint4* q = reinterpret_cast<uint4*>(col + swz(k & 7, 4 * half + i));
-                    uint4 w = *q;
-                    w.x = W::mul(w.x, f); w.y = W::mul(w.y, f); w.z = W::mul(w.z, f); w.w = W::mul(w.w, f);
-                    *q = w;
-                }
-                fence_async_smem();
-                mbar_arrive(full + sd % WIDE_NS_N);
-            };
             if (s >= WIDE_LAG_N) {
                 tc5::cp_wait<WIDE_LAG_N>();
                 finish(s - WIDE_LAG_N);
@@ -586,8 +564,8 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
             for (int s = 0; s < nst && ok; ++s) {
                 const int slot = s % WIDE_NS_N, q = s / WIDE_FLUSH, buf = q & 1;
                 const bool first = s % WIDE_FLUSH == 0, last = s % WIDE_FLUSH == WIDE_FLUSH - 1 || s == nst - 1;
-                if (first && q >= 2) ok = wide_wait(tempty + buf, uint32_t((q >> 1) - 1) & 1u, err);
-                if (ok) ok = wide_wait(full + slot, uint32_t(s / WIDE_NS_N) & 1u, err);
+                if (first && q >= 2) ok = wide_wait(tempty + buf, uint32_t((q >> 1) - 1) & 1u, err, wc.limit_ns);
+                if (ok) ok = wide_wait(full + slot, uint32_t(s / WIDE_NS_N) & 1u, err, wc.limit_ns);
                 if (!ok) break;
                 tc_fence_after();
                 const uint32_t sa = s0 + uint32_t(slot) * WIDE_N_STAGE, sb = sa + 8192u;
@@ -602,7 +580,7 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
             // every MMA issued has completed before TMEM is freed (this wait
             // does not give up on the error flag: MMAs always finish)
             mma_commit(done);
-            if (!mbar_wait(done, 0u)) atomicOr(err, WIDE_ERR_WAIT);
+            if (!mbar_wait(done, 0u, wc.limit_ns)) atomicOr(err, WIDE_ERR_WAIT);
         }
         __syncwarp();
     } else {
@@ -615,7 +593,7 @@ k_nform_wide(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const
         bool ok = true;
         for (int q = 0; q < ngrp; ++q) {
             const int buf = q & 1;
-            ok = __all_sync(0xffffffffu, wide_wait(tfull + buf, uint32_t(q >> 1) & 1u, err));
+            ok = __all_sync(0xffffffffu, wide_wait(tfull + buf, uint32_t(q >> 1) & 1u, err, wc.limit_ns));
             if (!ok) break;
             tc_fence_after();
 #pragma unroll

@@ -217,4 +217,53 @@ struct MCol {
 };
 static_assert(sizeof(MCol) == 8, "MCol is 8 bytes");
 
+// ------------------------------------- one-pass 64-vector products (op N)
+// N-form: per column of a 16-bit run, its vector entry (| VEC_T) and the
+// factor f / F its staged matrix column is multiplied by (a power of two
+// <= 1 as two packed 16-bit values of the store's format); F = 2^E with E in
+// the run's MSeg.pad.  f = chunk scale (x columns) or chunk scale times 2^c
+// of the t entry (t columns).
+struct WCol {
+    uint32_t idx;
+    uint32_t fac;
+};
+static_assert(sizeof(WCol) == 8, "WCol is 8 bytes");
+
+// Column-cluster T-form: one CTA per unit, t = V^T x of a set of low-rank
+// blocks that share a column cluster, over consecutive column tiles
+// [tile0, tile0 + ntiles) (a whole cluster, or a piece of a long one).  The
+// blocks' V slabs of one tile are stacked as the N dimension (ncols <=
+// WT_MAXN columns); the tile's split rows of x are the M operand; the
+// accumulator covers all the unit's tiles, so no per-tile partials.
+constexpr int WT_MAXN = 128;       // stacked columns per unit
+constexpr int WT_MAXT = 32;        // tiles per unit; longer clusters are cut into pieces
+constexpr int WT_MAXB = 32;        // blocks (or rank slices) per unit
+struct WTUnit {
+    uint32_t tile0;
+    uint16_t ntiles;
+    uint16_t ncols;
+    uint32_t blk0;         // blocks [blk0, blk0 + nblk) of the block table
+    uint32_t slab0;        // slab table: ntiles x nblk store offsets (/16), tile-major
+    uint16_t nblk;
+    uint16_t piece;        // piece index p of `npieces` (npieces 1: outputs are final)
+    uint16_t npieces;
+    uint16_t pad;
+    uint32_t part0;        // pieces: partial entries of the unit's blocks (see WTBlk)
+};
+static_assert(sizeof(WTUnit) == 28, "WTUnit is 28 bytes");
+struct WTBlk {
+    uint32_t toff;         // first t entry of the block's columns
+    uint16_t k;            // columns (rank, or a slice of it)
+    uint16_t off;          // first stacked column of the unit
+    float scale;           // the V chunks' common scale (value = stored * scale)
+    uint32_t pbase;        // pieces: partial entry of piece i, column l = pbase + i * k + l
+};
+static_assert(sizeof(WTBlk) == 16, "WTBlk is 16 bytes");
+struct WTTile {
+    uint32_t v_off;        // first x entry of the column tile
+    uint16_t rows;
+    uint16_t ld;           // 16-bit slab leading dimension (rows padded to 8)
+};
+static_assert(sizeof(WTTile) == 8, "WTTile is 8 bytes");
+
 }  // namespace hlrc

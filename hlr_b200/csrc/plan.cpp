@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <unordered_map>
 
@@ -132,6 +133,9 @@ struct Store {
     std::vector<SChunk> chunks;
     std::vector<uint8_t> group;        // per chunk: 0 = dense slab, 1 = factor slab
     std::vector<int32_t> crows;        // per chunk: rows of its slab
+    // per chunk: scale group (-1: the chunk's own scale).  Scaled chunks of
+    // one group share the scale of the group's largest entry.
+    std::vector<int32_t> sgrp;
     size_t region_begin = 0;           // first chunk without a byte offset
     int64_t bytes = 0;
     int64_t unpadded[NFMT] = {};
@@ -140,7 +144,7 @@ struct Store {
     // column, may be null -> deffmt); chunks do not straddle `cuts`.  Byte
     // offsets are assigned by close_region().
     int alloc(const double* src, int64_t lds, int64_t r0, int64_t rows, int64_t ncols, const uint8_t* colfmt,
-              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr, int grp = 1) {
+              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr, int grp = 1, int32_t scale_group = -1) {
         SSlab s{src, lds, r0, rows, pad_rows(rows), int32_t(chunks.size()), 0};
         int64_t j = 0;
         size_t ci = 0;
@@ -158,6 +162,7 @@ struct Store {
             chunks.push_back(ch);
             group.push_back(uint8_t(grp));
             crows.push_back(int32_t(rows));
+            sgrp.push_back(scale_group);
             ++s.nch;
             j = e;
         }
@@ -178,8 +183,32 @@ struct Store {
         region_begin = chunks.size();
     }
 
+    // largest |entry| of each chunk's slab rows and columns
+    double chunk_amax(const SSlab& s, const SChunk& ch) const {
+        double amax = 0;
+        const double* src = s.src + s.r0 + int64_t(ch.col0) * s.lds;
+        for (int j = 0; j < ch.nc; ++j)
+            for (int64_t i = 0; i < s.rows; ++i) amax = std::max(amax, std::fabs(src[i + j * s.lds]));
+        return amax;
+    }
+
     void fill(std::vector<uint8_t>& st) {
         st.assign(size_t(bytes), 0);
+        // scale groups: the largest entry over all chunks of a group
+        int32_t ngrp = 0;
+        for (int32_t g : sgrp) ngrp = std::max(ngrp, g + 1);
+        std::vector<double> gmax(size_t(ngrp), 0.0);
+        if (ngrp > 0) {
+            std::vector<double> cmax(chunks.size(), 0.0);
+            #pragma omp parallel for schedule(dynamic, 64)
+            for (int64_t si = 0; si < int64_t(slabs.size()); ++si) {
+                const SSlab& sl = slabs[size_t(si)];
+                for (int32_t c = sl.c0; c < sl.c0 + sl.nch; ++c)
+                    if (sgrp[size_t(c)] >= 0) cmax[size_t(c)] = chunk_amax(sl, chunks[size_t(c)]);
+            }
+            for (size_t c = 0; c < chunks.size(); ++c)
+                if (sgrp[c] >= 0) gmax[size_t(sgrp[c])] = std::max(gmax[size_t(sgrp[c])], cmax[c]);
+        }
         #pragma omp parallel for schedule(dynamic, 64)
         for (int64_t si = 0; si < int64_t(slabs.size()); ++si) {
             const SSlab& s = slabs[size_t(si)];
@@ -219,10 +248,10 @@ struct Store {
                         }
                     }
                 } else {
-                    // power-of-two scale bringing the chunk's largest entry to [2^14, 2^15)
-                    double amax = 0;
-                    for (int j = 0; j < ch.nc; ++j)
-                        for (int64_t i = 0; i < s.rows; ++i) amax = std::max(amax, std::fabs(src[i + j * s.lds]));
+                    // power-of-two scale bringing the chunk's (or its scale
+                    // group's) largest entry to [2^14, 2^15)
+                    const int32_t g = sgrp[size_t(c)];
+                    const double amax = g >= 0 ? gmax[size_t(g)] : chunk_amax(s, ch);
                     int ex = 0;
                     if (amax > 0) std::frexp(amax, &ex);
                     const double scale = amax > 0 ? std::ldexp(1.0, ex - 15) : 1.0;
@@ -710,6 +739,116 @@ uint8_t default_format(int prec) {
 }  // namespace
 
 // --------------------------------------------------------------------- H
+// The 64-vector product of a 16-bit H store, op N (WidePlan): units of the
+// column-cluster T-form and the static exponents of t.  Low-rank blocks are
+// grouped by their column index set (blocks of one group read the same x
+// rows); a group's columns are stacked in units of at most WT_MAXN (a block
+// of higher rank is cut into slices), and a group spanning more than
+// WT_MAXT tiles is cut into pieces, each writing FP32 partials that a finish
+// group per block sums in piece order.
+hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<int64_t>& toff,
+                      const std::vector<std::vector<int>>& slabV, const Store& st, Plan& p) {
+    WidePlan& W = p.wide;
+    W = WidePlan();
+    for (int64_t t = 0; t < tc.n(); ++t)
+        W.tiles.push_back(WTTile{uint32_t(tc.lo(t)), uint16_t(tc.size(t)), uint16_t(pad_fmt(tc.size(t), FMT_F16))});
+    W.t_exp.assign(size_t(std::max<int64_t>(1, p.n_t)), 0);
+    std::map<std::pair<int64_t, int64_t>, std::vector<int64_t>> groups;   // (col0, ncols) -> blocks
+    for (int64_t i = 0; i < d.nblocks; ++i) {
+        const hlrc_block& b = d.blocks[i];
+        if (toff[size_t(i)] < 0) continue;
+        for (int64_t l = 0; l < b.rank; ++l) {   // c = ceil-ish log2 ||V(:,l)||_1: 2^c > the norm
+            double s1 = 0;
+            for (int64_t r = 0; r < b.ncols; ++r) s1 += std::fabs(b.V[r + l * b.ldv]);
+            W.t_exp[size_t(toff[size_t(i)] + l)] = int8_t(s1 > 0 ? std::max(-120, std::min(120, std::ilogb(s1) + 1)) : 0);
+        }
+        groups[{b.col0, b.ncols}].push_back(i);
+    }
+    struct Item { int64_t blk, l0, k; };
+    auto slab_a16 = [&](int64_t i, int64_t ti, int64_t l0) -> uint64_t {
+        const SSlab& sl = st.slabs[size_t(slabV[size_t(i)][size_t(ti)])];
+        const uint64_t off = uint64_t(st.chunks[size_t(sl.c0)].byte_off) + uint64_t(l0) * uint64_t(pad_fmt(sl.rows, FMT_F16)) * 2;
+        return off / 16;
+    };
+    std::vector<std::pair<int64_t, size_t>> cost;   // (cost, unit index) for the order
+    for (const auto& kv : groups) {
+        const int64_t col0 = kv.first.first, ncols = kv.first.second;
+        const int64_t t0 = tc.first(col0), T = tc.first(col0 + ncols) - t0;
+        std::vector<Item> items;
+        for (int64_t i : kv.second)
+            for (int64_t l0 = 0; l0 < d.blocks[i].rank; l0 += WT_MAXN)
+                items.push_back({i, l0, std::min<int64_t>(WT_MAXN, d.blocks[i].rank - l0)});
+        size_t a = 0;
+        while (a < items.size()) {   // one subset: items [a, e) with at most WT_MAXN columns
+            size_t e = a;
+            int64_t nc = 0;
+            while (e < items.size() && nc + items[e].k <= WT_MAXN && int(e - a) < WT_MAXB) nc += items[e++].k;
+            const int64_t P = (T + WT_MAXT - 1) / WT_MAXT;
+            const int64_t part0 = P > 1 ? W.npart : 0;
+            if (P > 1) W.npart += P * nc;
+            for (int64_t q = 0; q < P; ++q) {
+                const int64_t q0 = t0 + (T * q) / P, q1 = t0 + (T * (q + 1)) / P;
+                WTUnit u{};
+                u.tile0 = uint32_t(q0);
+                u.ntiles = uint16_t(q1 - q0);
+                u.ncols = uint16_t(nc);
+                u.blk0 = uint32_t(W.blks.size());
+                u.slab0 = uint32_t(W.slabs.size());
+                u.nblk = uint16_t(e - a);
+                u.piece = uint16_t(q);
+                u.npieces = uint16_t(P);
+                u.part0 = uint32_t(part0);
+                int64_t off = 0;
+                for (size_t j = a; j < e; ++j) {
+                    const Item& it = items[j];
+                    const SSlab& s0 = st.slabs[size_t(slabV[size_t(it.blk)][0])];
+                    WTBlk wb{};
+                    wb.toff = uint32_t(toff[size_t(it.blk)] + it.l0);
+                    wb.k = uint16_t(it.k);
+                    wb.off = uint16_t(off);
+                    wb.scale = st.chunks[size_t(s0.c0)].scale;
+                    wb.pbase = uint32_t(part0 + P * off);
+                    W.blks.push_back(wb);
+                    off += it.k;
+                }
+                for (int64_t t = q0; t < q1; ++t)
+                    for (size_t j = a; j < e; ++j) {
+                        const Item& it = items[j];
+                        const uint64_t a16 = slab_a16(it.blk, t - tc.first(d.blocks[it.blk].col0), it.l0);
+                        if (a16 >= (uint64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "store offset beyond 2^36 bytes");
+                        W.slabs.push_back(uint32_t(a16));
+                    }
+                cost.push_back({(q1 - q0) * (16384 + nc * 128), W.units.size()});
+                W.units.push_back(u);
+            }
+            if (P > 1)
+                for (size_t j = a; j < e; ++j) {
+                    const WTBlk& wb = W.blks[W.blks.size() - (e - j)];
+                    W.groups.push_back(TGroup{wb.pbase, uint32_t(P), wb.toff, wb.k});
+                }
+            a = e;
+        }
+    }
+    if (W.npart >= (int64_t(1) << 32) || W.slabs.size() >= (size_t(1) << 32))
+        return fail(HLRC_ERR_SHAPE, "64-vector tables exceed 2^32 entries");
+    std::stable_sort(cost.begin(), cost.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<WTUnit> sorted;
+    sorted.reserve(W.units.size());
+    for (const auto& c : cost) sorted.push_back(W.units[c.second]);
+    W.units.swap(sorted);
+    // every V column a unit stages lies inside the store
+    for (const WTUnit& u : W.units)
+        for (int t = 0; t < u.ntiles; ++t)
+            for (int j = 0; j < u.nblk; ++j) {
+                const uint64_t a16 = W.slabs[size_t(u.slab0) + size_t(t) * u.nblk + size_t(j)];
+                const uint64_t end = a16 * 16 + uint64_t(W.blks[size_t(u.blk0) + size_t(j)].k) *
+                                                     uint64_t(W.tiles[size_t(u.tile0) + size_t(t)].ld) * 2;
+                if (a16 * 16 % 16 != 0 || end > uint64_t(p.store.size()))
+                    return fail(HLRC_ERR_INTERNAL, "64-vector unit reads outside the store");
+            }
+    return HLRC_OK;
+}
+
 hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area) {
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0) return fail(HLRC_ERR_SHAPE, "negative matrix size");
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
@@ -827,11 +966,17 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
         }
         st.close_region();
     }
+    // 16-bit stores: the V chunks of one block share one scale over all its
+    // column tiles, so the 64-vector T-form can sum a block's tiles in one
+    // accumulator (the per-element precision of a 16-bit float does not
+    // depend on the scale)
+    const bool wide16 = o.precision == HLRC_PREC_F16 || o.precision == HLRC_PREC_BF16;
     for (int64_t t = 0; t < tc.n(); ++t) {
         for (int64_t i : collist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
             if (b.kind != HLRC_LEAF_LOWRANK) continue;
-            slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank, cf(i), deffmt));
+            slabV[size_t(i)].push_back(st.alloc(b.V, b.ldv, tc.lo(t) - b.col0, tc.size(t), b.rank, cf(i), deffmt,
+                                                nullptr, 1, wide16 ? int32_t(i) : -1));
         }
         st.close_region();
     }
@@ -931,6 +1076,9 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     p.stages[HLRC_OP_C] = p.stages[HLRC_OP_T];
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
+    if (wide16) {
+        if (hlrc_status ws = plan_wide(d, tc, toff, slabV, st, p); ws != HLRC_OK) return ws;
+    }
 
     if (hlrc_status vs = validate_plan(p); vs != HLRC_OK) return vs;
 

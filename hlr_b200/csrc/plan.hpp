@@ -94,6 +94,22 @@ struct TTPass {
     int64_t bytes = 0, alg_bytes = 0;
 };
 
+// The one-pass 64-vector product of a 16-bit H store (op N): the
+// column-cluster T-form units and their tables, the finish groups of
+// clusters cut into pieces, and the static exponents of t's split rows
+// (c_i = ceil(log2 ||V(:,i)||_1), so |t_i| 2^g / 2^c_i <= 2^14 whenever
+// max |x| 2^g < 2^14).  Empty when the plan has no such product.
+struct WidePlan {
+    std::vector<WTUnit> units;     // by cost, descending
+    std::vector<WTBlk> blks;
+    std::vector<uint32_t> slabs;
+    std::vector<WTTile> tiles;
+    std::vector<TGroup> groups;    // per block of a cut cluster: sums its pieces' partials into t
+    int64_t npart = 0;             // partial entries (WIDE_RHS FP32 values each)
+    std::vector<int8_t> t_exp;     // per t entry
+    bool empty() const { return units.empty(); }
+};
+
 // One stage of a product: exactly one of the passes is used.
 struct Stage {
     int kind;                      // 0 = T-form (units), 1 = N-form, 2 = tile T-form
@@ -119,6 +135,7 @@ struct Plan {
     // profile names per pass (static strings), per stage kind; empty = the
     // fixed names of kinds 0 and 1
     std::vector<const char*> names[3];
+    WidePlan wide;                 // 16-bit H stores: the 64-vector op N product
 };
 
 // Returns HLRC_OK or an error (message recorded via fail()).  expected_area

@@ -397,11 +397,31 @@ int64_t     hlrc_launch_count(hlrc_hmat M);
 
 hlrc_status hlrc_free(hlrc_hmat M);
 
+/* Measured FP64 tensor-core (DMMA) throughput of `device` (-1 = current),
+ * in TFLOP/s: a register-resident loop of m8n8k4 f64 MMAs timed with CUDA
+ * events.  The compute roof of FP64 products with several right-hand sides,
+ * reported beside the HBM roof.  No counterpart in the reference; changes
+ * no device setting.                                                         */
+hlrc_status hlrc_fp64_peak(int device, double* tflops);
+
 /* Reads and clears the handle's device error word (synchronous).  Kernels
  * that wait with a bound set it when a wait runs out; the products launched
  * since then are incomplete.  0 means no error; bit 0 (value 1): a copy wait
- * of an H^2 tree sweep ran out.                                              */
+ * of an H^2 tree sweep ran out; bit 1 (value 2): a stage hand-over of the
+ * 64-vector kernels ran out.                                                 */
 hlrc_status hlrc_check_device_error(hlrc_hmat M, int* code);
+
+/* Test hook of the bounded device waits (no counterpart in the reference).
+ * limit_ns > 0 replaces the 2 s bound of every device wait of the handle's
+ * products (0 restores it).  skip_handover != 0 makes the next products
+ * leave one hand-over undone in every CTA that waits: an H^2 tree sweep
+ * announces 16 bytes more on its first level's barrier than its copies
+ * deliver, and the producers of the 64-vector kernels never signal their
+ * first stage.  The waiting kernel then gives up after the bound, records
+ * the error bit, finishes its copies and MMAs, frees its tensor memory and
+ * returns; the product is incomplete and hlrc_check_device_error reports
+ * it, and the context stays usable.  Not for use during captures.           */
+hlrc_status hlrc_debug_waits(hlrc_hmat M, int64_t limit_ns, int skip_handover);
 
 /* ----------------------------------------------------- host construction
  * HLR builds its matrices with HLIBpro's clustering (TBSPCTBuilder,
