@@ -7,6 +7,8 @@
 // product is a fixed sequence of 2-4 batched passes over a flattened layout,
 // and every output tile is written by exactly one CTA, so the result is
 // deterministic and needs no atomics.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +29,7 @@
 #include "kernels_q.cuh"
 #include "kernels_tc.cuh"
 #include "kernels_wide.cuh"
+#include "kernels_wtma.cuh"
 #include "plan.hpp"
 
 namespace hlrc {
@@ -54,6 +57,11 @@ struct DevNPass {
     const MCol* mcol = nullptr;
     const NSeg2* seg2 = nullptr;      // reduced precision: both formats of a tile in one CTA
     const WCol* wcol = nullptr;       // 64-vector N-form: per column of the 16-bit runs
+    const WSeg* wseg = nullptr;       // 64-vector N-form with TMA: full 64-row tiles
+    const WStage* wstage = nullptr;
+    int nwseg = 0;
+    const MSeg* mseg_cp = nullptr;    // 64-vector N-form with cp.async: the other tiles
+    int nmseg_cp = 0;
     int nseg2 = 0;
     int f16 = FMT_F16;                // the store's 16-bit format
     int wide = FMT_F32;               // the store's wide format (FP32, or 24-bit for BFP)
@@ -94,6 +102,32 @@ struct DevTTPass {
         for (int f = 0; f < NFMT; ++f) k += nsegs[f] > 0 ? 1 : 0;
         return k;
     }
+};
+
+// Scratch used by one product: the coefficient vectors and the partial sums
+// of a one-vector product, and (when present) the same arrays as row-major
+// blocks of MR_RB vectors for the multi-vector kernels.  A product reads
+// every scratch entry only after writing it in the same product.
+struct Workspace {
+    double* t = nullptr;
+    double* t2 = nullptr;
+    double* part = nullptr;
+    double* mr_x = nullptr;      // null: no multi-vector arrays
+    double* mr_t = nullptr;
+    double* mr_t2 = nullptr;
+    double* mr_part = nullptr;
+    // one-pass 64-vector kernels of 16-bit stores (null: none): split rows of
+    // x and t, FP32 partials of long column clusters, per-vector maxima and
+    // scale exponents of x
+    uint32_t* w_xs = nullptr;
+    uint32_t* w_ts = nullptr;
+    float* w_part = nullptr;
+    unsigned long long* w_xmax = nullptr;
+    int* w_g = nullptr;
+    // TMA views of w_xs (boxes of 16 and 64 split rows) and w_ts (16 rows)
+    bool has_tm = false;
+    CUtensorMap tm_x16, tm_x64, tm_t16;
+    bool profile = false;        // record per-pass events in the handle's profile
 };
 
 struct ProfileRec {
@@ -141,12 +175,13 @@ struct hlrc_hmat_s {
     const int8_t* w_texp = nullptr;
     int w_nunits = 0, w_ngroups = 0;
     int64_t w_npart = 0;
+    const WTUnit* w_units_tma = nullptr;   // units whose tiles are all full: TMA kernel
+    int w_nunits_tma = 0;
+    bool tma = false;                      // store maps valid (full-tile TMA kernels usable)
+    int sms = 148;                         // multiprocessors of the device (persistent grids)
+    CUtensorMap tm_s16, tm_s8;             // the store as 128-byte rows, boxes of 16 and 8 rows
     char* w_arena = nullptr;          // workspace of the handle's own 64-vector products
-    uint32_t* w_xs = nullptr;
-    uint32_t* w_ts = nullptr;
-    float* w_part = nullptr;
-    unsigned long long* w_xmax = nullptr;
-    int* w_g = nullptr;
+    Workspace wws;                    // its arrays and tensor maps (only the w_* members are used)
     // host-pointer entry point staging (hlrc_mvm_host holds host_mu while it
     // uses these and the handle's workspace)
     double* hx = nullptr;
@@ -172,28 +207,37 @@ struct hlrc_hmat_s {
 
 namespace {
 
-// Scratch used by one product: the coefficient vectors and the partial sums
-// of a one-vector product, and (when present) the same arrays as row-major
-// blocks of MR_RB vectors for the multi-vector kernels.  A product reads
-// every scratch entry only after writing it in the same product.
-struct Workspace {
-    double* t = nullptr;
-    double* t2 = nullptr;
-    double* part = nullptr;
-    double* mr_x = nullptr;      // null: no multi-vector arrays
-    double* mr_t = nullptr;
-    double* mr_t2 = nullptr;
-    double* mr_part = nullptr;
-    // one-pass 64-vector kernels of 16-bit stores (null: none): split rows of
-    // x and t, FP32 partials of long column clusters, per-vector maxima and
-    // scale exponents of x
-    uint32_t* w_xs = nullptr;
-    uint32_t* w_ts = nullptr;
-    float* w_part = nullptr;
-    unsigned long long* w_xmax = nullptr;
-    int* w_g = nullptr;
-    bool profile = false;        // record per-pass events in the handle's profile
-};
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// against the driver library)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    return fn;
+}
+
+// A 2-D tensor map of 16-bit elements: `rows` rows of `inner` elements,
+// `row_bytes` apart; boxes of box_inner x box_rows, 128-byte swizzle, zero
+// fill outside the tensor.
+bool make_map(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint64_t row_bytes, uint32_t box_inner,
+              uint32_t box_rows) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || rows == 0) return false;
+    const cuuint64_t dims[2] = {inner, rows};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {box_inner, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 struct DeviceGuard {
     int prev = -1;
@@ -470,6 +514,36 @@ void wide_columns(StreamTables& tab, int f, const std::vector<int8_t>& t_exp, bo
     }
 }
 
+// The 64-vector N-form's runs of full 64-row tiles become TMA segments
+// (WSeg): a stage per run of <= 32 columns with consecutive vector entries
+// of one array, its matrix columns at store row a16 / 8 + column (128-byte
+// rows).  A run qualifies when its tile has 64 rows, it starts on a 128-byte
+// boundary, and every column's factor is 1.  The other runs stay for the
+// cp.async kernel.
+void wide_tma_split(const StreamTables& tab, int f, const std::vector<WCol>& wcol, bool bf16, std::vector<WSeg>& segs,
+                    std::vector<WStage>& stages, std::vector<MSeg>& rest) {
+    const uint32_t one = pow2_pair(0, bf16);
+    for (const MSeg& m : tab.seg[f]) {
+        bool ok = m.rows == TILE && m.ld == TILE && m.a16 % 8 == 0 && m.ncols > 0;
+        for (uint32_t j = 0; ok && j < m.ncols; ++j) ok = wcol[size_t(m.col0 + j)].fac == one;
+        if (!ok) {
+            rest.push_back(m);
+            continue;
+        }
+        WSeg w{uint32_t(stages.size()), 0u, m.vo, int32_t(m.pad)};
+        uint32_t j = 0;
+        while (j < m.ncols) {
+            const uint32_t i0 = tab.col[size_t(m.col0 + j)].idx;
+            uint32_t n = 1;
+            while (j + n < m.ncols && n < 32 && tab.col[size_t(m.col0 + j + n)].idx == i0 + n) ++n;
+            stages.push_back(WStage{m.a16 / 8 + j, i0, n});
+            j += n;
+        }
+        w.nst = uint32_t(stages.size()) - w.st0;
+        segs.push_back(w);
+    }
+}
+
 // Builds and uploads the column streams of every N-form and tile T-form pass
 // (and, for plans with a 64-vector product, that N-form's column table).
 hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
@@ -482,14 +556,22 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
     const int wide_pass = !p.wide.empty() && p.stages[HLRC_OP_N].size() == 2 ? p.stages[HLRC_OP_N][1].idx : -1;
     const bool bf16 = p.precision == HLRC_PREC_BF16;
     std::vector<WCol> wcol;
-    size_t wcol_off = 0;
+    std::vector<WSeg> wsegs;
+    std::vector<WStage> wstages;
+    std::vector<MSeg> wrest;
+    size_t wcol_off = 0, wseg_off = 0, wstage_off = 0, wrest_off = 0;
     for (size_t i = 0; i < nt.size(); ++i) {
         const hlrc_status st = build_streams(p.npasses[i].segs, p.npasses[i].chunks, false,
                                              [](const NSeg& s) { return s.out; }, nt[i]);
         if (st != HLRC_OK) return st;
         if (int(i) == wide_pass) {
-            wide_columns(nt[i], bf16 ? FMT_BF16 : FMT_F16, p.wide.t_exp, bf16, wcol);
+            const int f = bf16 ? FMT_BF16 : FMT_F16;
+            wide_columns(nt[i], f, p.wide.t_exp, bf16, wcol);
+            wide_tma_split(nt[i], f, wcol, bf16, wsegs, wstages, wrest);
             wcol_off = take(wcol.size() * sizeof(WCol));
+            wseg_off = take(wsegs.size() * sizeof(WSeg));
+            wstage_off = take(wstages.size() * sizeof(WStage));
+            wrest_off = take(wrest.size() * sizeof(MSeg));
         }
         for (int f = 0; f < NFMT; ++f) n_seg_off[i][size_t(f)] = take(nt[i].seg[f].size() * sizeof(MSeg));
         n_col_off[i] = take(nt[i].col.size() * sizeof(MCol));
@@ -519,7 +601,16 @@ hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
         h->n[i].mcol = reinterpret_cast<const MCol*>(h->mr_tables + n_col_off[i]);
         if (int(i) == wide_pass) {
             if (e == cudaSuccess) e = put(wcol_off, wcol.data(), wcol.size() * sizeof(WCol));
-            h->n[i].wcol = reinterpret_cast<const WCol*>(h->mr_tables + wcol_off);
+            if (e == cudaSuccess) e = put(wseg_off, wsegs.data(), wsegs.size() * sizeof(WSeg));
+            if (e == cudaSuccess) e = put(wstage_off, wstages.data(), wstages.size() * sizeof(WStage));
+            if (e == cudaSuccess) e = put(wrest_off, wrest.data(), wrest.size() * sizeof(MSeg));
+            DevNPass& d = h->n[i];
+            d.wcol = reinterpret_cast<const WCol*>(h->mr_tables + wcol_off);
+            d.wseg = reinterpret_cast<const WSeg*>(h->mr_tables + wseg_off);
+            d.wstage = reinterpret_cast<const WStage*>(h->mr_tables + wstage_off);
+            d.nwseg = int(wsegs.size());
+            d.mseg_cp = reinterpret_cast<const MSeg*>(h->mr_tables + wrest_off);
+            d.nmseg_cp = int(wrest.size());
         }
     }
     for (size_t i = 0; i < tt.size() && e == cudaSuccess; ++i) {
@@ -615,6 +706,14 @@ WideSizes wide_sizes(hlrc_hmat M) {
     return z;
 }
 
+// TMA views of a workspace's split rows (x: the longer side, t: n_t rows)
+void wide_ws_maps(hlrc_hmat M, Workspace& w) {
+    const uint64_t nx = uint64_t(std::max(M->nrows, M->ncols)), nt = uint64_t(std::max<int64_t>(1, M->n_t));
+    w.has_tm = w.w_xs && make_map(&w.tm_x16, w.w_xs, 128, nx, WIDE_ROWB, 64, 16) &&
+               make_map(&w.tm_x64, w.w_xs, 128, nx, WIDE_ROWB, 64, 64) &&
+               make_map(&w.tm_t16, w.w_ts, 128, nt, WIDE_ROWB, 64, 16);
+}
+
 // The store format of a 16-bit H-matrix handle whose op N product is one
 // tile T-form pass (t = V^T x) followed by one N-form pass (y += alpha (U t
 // + D x)) over 16-bit column runs only: the shape the 64-vector kernels
@@ -640,6 +739,10 @@ hlrc_status enable_wide_smem(int dev) {
     static std::vector<int> done;
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_wtma<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wtma_smem_n()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_wtma<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wtma_smem_n()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wtma<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wtma_smem_c()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wtma<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wtma_smem_c()));
     HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_c()));
     HLRC_CUDA(cudaFuncSetAttribute(k_ctform_wide<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_c()));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_wide<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem_n()));
@@ -858,7 +961,21 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         }
     }
     if (!p.wide.empty()) {
-        const WidePlan& W = p.wide;
+        // units whose tiles are all full and whose slabs start on 128-byte
+        // boundaries take the TMA kernel; they go first in the unit array
+        WidePlan W = p.wide;
+        {
+            std::vector<WTUnit> tma_u, cp_u;
+            for (const WTUnit& u : W.units) {
+                bool ok = true;
+                for (int t = 0; ok && t < u.ntiles; ++t) ok = W.tiles[size_t(u.tile0) + size_t(t)].rows == TILE;
+                for (size_t k = 0; ok && k < size_t(u.ntiles) * u.nblk; ++k) ok = W.slabs[u.slab0 + k] % 8 == 0;
+                (ok ? tma_u : cp_u).push_back(u);
+            }
+            hp->w_nunits_tma = int(tma_u.size());
+            W.units = tma_u;
+            W.units.insert(W.units.end(), cp_u.begin(), cp_u.end());
+        }
         size_t wb = 0;
         auto take = [&](size_t b) { const size_t o_ = wb; wb = align_up(wb + b, 256); return o_; };
         const size_t o_u = take(W.units.size() * sizeof(WTUnit)), o_b = take(W.blks.size() * sizeof(WTBlk)),
@@ -880,16 +997,25 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             cleanup();
             return fail(HLRC_ERR_OOM, "64-vector tables of %zu bytes: %s", wb, cudaGetErrorString(e));
         }
-        hp->w_units = reinterpret_cast<const WTUnit*>(hp->w_static + o_u);
+        hp->w_units_tma = reinterpret_cast<const WTUnit*>(hp->w_static + o_u);
+        hp->w_units = hp->w_units_tma + hp->w_nunits_tma;   // the cp.async units
         hp->w_blks = reinterpret_cast<const WTBlk*>(hp->w_static + o_b);
         hp->w_slabs = reinterpret_cast<const uint32_t*>(hp->w_static + o_s);
         hp->w_tiles = reinterpret_cast<const WTTile*>(hp->w_static + o_t);
         hp->w_groups = reinterpret_cast<const TGroup*>(hp->w_static + o_g);
         hp->w_texp = reinterpret_cast<const int8_t*>(hp->w_static + o_e);
-        hp->w_nunits = int(W.units.size());
+        hp->w_nunits = int(W.units.size()) - hp->w_nunits_tma;
         hp->w_ngroups = int(W.groups.size());
         hp->w_npart = W.npart;
         hp->info.device_bytes += int64_t(wb);
+    }
+    // the store as rows of 128 bytes for the full-tile TMA kernels
+    cudaDeviceGetAttribute(&hp->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (hp->sms <= 0) hp->sms = 148;
+    if (!p.wide.empty()) {
+        const uint64_t rows = uint64_t(p.store.size()) / 128;
+        hp->tma = rows > 0 && make_map(&hp->tm_s16, hp->store, 64, rows, 128, 64, 16) &&
+                  make_map(&hp->tm_s8, hp->store, 64, rows, 128, 64, 8);
     }
     hp->wide = wide_format(hp) >= 0;
     if (hp->wide && o.max_nrhs > MR_RB) {
@@ -909,10 +1035,8 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             cleanup();
             return st;
         }
-        Workspace w;
-        z.carve(hp->w_arena, w);
-        hp->w_xs = w.w_xs; hp->w_ts = w.w_ts; hp->w_part = w.w_part;
-        hp->w_xmax = w.w_xmax; hp->w_g = w.w_g;
+        z.carve(hp->w_arena, hp->wws);
+        wide_ws_maps(hp, hp->wws);
         hp->info.workspace_bytes += int64_t(z.bytes);
         hp->info.device_bytes += int64_t(z.bytes);
     }
@@ -933,8 +1057,10 @@ Workspace handle_workspace(hlrc_hmat M) {
     Workspace w;
     w.t = M->ws_t; w.t2 = M->ws_t2; w.part = M->part;
     w.mr_x = M->mr_x; w.mr_t = M->mr_t; w.mr_t2 = M->mr_t2; w.mr_part = M->mr_part;
-    w.w_xs = M->w_xs; w.w_ts = M->w_ts; w.w_part = M->w_part;
-    w.w_xmax = M->w_xmax; w.w_g = M->w_g;
+    w.w_xs = M->wws.w_xs; w.w_ts = M->wws.w_ts; w.w_part = M->wws.w_part;
+    w.w_xmax = M->wws.w_xmax; w.w_g = M->wws.w_g;
+    w.has_tm = M->wws.has_tm;
+    if (w.has_tm) { w.tm_x16 = M->wws.tm_x16; w.tm_x64 = M->wws.tm_x64; w.tm_t16 = M->wws.tm_t16; }
     w.profile = M->profiling;
     return w;
 }
@@ -1293,18 +1419,39 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
         if (ws.profile) prof_end(M, s);
         M->launches += 2;
         HLRC_AFTER_LAUNCH("wide_xsplit");
-        if (M->w_nunits > 0) {
+        // full-tile units through TMA (persistent CTAs, two per SM), the
+        // others through cp.async; the same outputs are never written by both
+        const bool tma = M->tma && ws.has_tm;
+        const int ntma = tma ? M->w_nunits_tma : 0;
+        const WTUnit* ucp = tma ? M->w_units : M->w_units_tma;   // without TMA every unit takes cp.async
+        const int ncp = tma ? M->w_nunits : M->w_nunits + M->w_nunits_tma;
+        const WaitCfg wc{M->wait_ns, M->wait_skip};
+        if (ntma + ncp > 0) {
             if (ws.profile) prof_begin(M, stage_name(M, 2, st[0].idx), tp.alg_bytes, s);
-            if (bf)
-                k_ctform_wide<FMT_BF16><<<M->w_nunits, WIDE_THREADS, wide_smem_c(), s>>>(
-                    M->w_units, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
-                    M->dev_err, WaitCfg{M->wait_ns, M->wait_skip});
-            else
-                k_ctform_wide<FMT_F16><<<M->w_nunits, WIDE_THREADS, wide_smem_c(), s>>>(
-                    M->w_units, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
-                    M->dev_err, WaitCfg{M->wait_ns, M->wait_skip});
+            if (ntma > 0) {
+                const int grid = std::min(ntma, 2 * M->sms);
+                if (bf)
+                    k_ctform_wtma<FMT_BF16><<<grid, WTMA_THREADS, wtma_smem_c(), s>>>(
+                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
+                        M->w_texp, ws.w_part, M->dev_err, wc);
+                else
+                    k_ctform_wtma<FMT_F16><<<grid, WTMA_THREADS, wtma_smem_c(), s>>>(
+                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
+                        M->w_texp, ws.w_part, M->dev_err, wc);
+                M->launches += 1;
+            }
+            if (ncp > 0) {
+                if (bf)
+                    k_ctform_wide<FMT_BF16><<<ncp, WIDE_THREADS, wide_smem_c(), s>>>(
+                        ucp, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
+                        M->dev_err, wc);
+                else
+                    k_ctform_wide<FMT_F16><<<ncp, WIDE_THREADS, wide_smem_c(), s>>>(
+                        ucp, M->w_blks, M->w_slabs, M->w_tiles, M->store, ws.w_xs, ws.w_ts, M->w_texp, ws.w_part,
+                        M->dev_err, wc);
+                M->launches += 1;
+            }
             if (ws.profile) prof_end(M, s);
-            M->launches += 1;
             HLRC_AFTER_LAUNCH(stage_name(M, 2, st[0].idx));
         }
         if (M->w_ngroups > 0) {
@@ -1319,19 +1466,33 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
             M->launches += 1;
             HLRC_AFTER_LAUNCH("ttfinish");
         }
-        if (np.nmseg[f] > 0) {
+        // full 64-row tiles through TMA, the other tiles (and everything,
+        // when TMA is unavailable) through cp.async
+        const int nwt = tma ? np.nwseg : 0;
+        const MSeg* mcp = tma ? np.mseg_cp : np.mseg[f];
+        const int nmcp = tma ? np.nmseg_cp : np.nmseg[f];
+        if (nwt + nmcp > 0) {
             const OutMap om{Y + int64_t(r0) * ldy, 1, ldy, nr};
             if (ws.profile) prof_begin(M, stage_name(M, 1, st[1].idx), np.alg_bytes, s);
-            if (bf)
-                k_nform_wide<FMT_BF16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
-                    np.mseg[f], np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err,
-                    WaitCfg{M->wait_ns, M->wait_skip});
-            else
-                k_nform_wide<FMT_F16><<<np.nmseg[f], WIDE_THREADS, wide_smem_n(), s>>>(
-                    np.mseg[f], np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err,
-                    WaitCfg{M->wait_ns, M->wait_skip});
+            if (nwt > 0) {
+                if (bf)
+                    k_nform_wtma<FMT_BF16><<<nwt, WTMA_THREADS, wtma_smem_n(), s>>>(
+                        np.wseg, np.wstage, M->tm_s16, ws.tm_x16, ws.tm_t16, ws.w_g, om, alpha, M->dev_err, wc);
+                else
+                    k_nform_wtma<FMT_F16><<<nwt, WTMA_THREADS, wtma_smem_n(), s>>>(
+                        np.wseg, np.wstage, M->tm_s16, ws.tm_x16, ws.tm_t16, ws.w_g, om, alpha, M->dev_err, wc);
+                M->launches += 1;
+            }
+            if (nmcp > 0) {
+                if (bf)
+                    k_nform_wide<FMT_BF16><<<nmcp, WIDE_THREADS, wide_smem_n(), s>>>(
+                        mcp, np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err, wc);
+                else
+                    k_nform_wide<FMT_F16><<<nmcp, WIDE_THREADS, wide_smem_n(), s>>>(
+                        mcp, np.wcol, M->store, ws.w_xs, ws.w_ts, ws.w_g, om, alpha, 1, M->dev_err, wc);
+                M->launches += 1;
+            }
             if (ws.profile) prof_end(M, s);
-            M->launches += 1;
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st[1].idx));
         }
     }
@@ -1746,7 +1907,10 @@ extern "C" hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_wor
     W->ws.t2 = reinterpret_cast<double*>(W->arena + o_t2);
     W->ws.part = reinterpret_cast<double*>(W->arena + o_p);
     if (W->mr_nx) z.carve(W->arena + o_mr, W->ws.mr_x, W->ws.mr_t, W->ws.mr_t2, W->ws.mr_part);
-    if (W->w_xs) zw.carve(W->arena + o_w, W->ws);
+    if (W->w_xs) {
+        zw.carve(W->arena + o_w, W->ws);
+        wide_ws_maps(M, W->ws);
+    }
     W->ws.profile = false;
     *out = W.release();
     return HLRC_OK;

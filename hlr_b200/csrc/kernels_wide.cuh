@@ -81,6 +81,7 @@ constexpr int WIDE_LAG_C = WIDE_NS_C - 1;
 constexpr int WIDE_PF = WIDE_LAG_N + 1;     // N-form: column-table entries prefetched this many stages ahead
 constexpr int WIDE_WQ = WIDE_PF + WIDE_LAG_N + 1;   // ring of prefetched column-table entries
 constexpr int WIDE_ERR_WAIT = 2;      // device error word bit: a wait of a wide kernel ran out
+constexpr uint32_t WT_EMPTY = 0xffffffffu;   // stacked column without data
 
 // N-form stage: A (vector terms, 2 M-atoms x 4 K-atoms) 8 KB, B (matrix, 4 K-atoms) 4 KB
 constexpr int WIDE_N_STAGE = 12288;
@@ -309,6 +310,10 @@ k_ctform_wide(const WTUnit* __restrict__ units, const WTBlk* __restrict__ blks, 
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // stacked column -> (block, column); columns between a block's rank and
+    // its 8-column boundary stay empty (zero-filled, not written out)
+    for (int n = threadIdx.x; n < WT_MAXN; n += WIDE_THREADS) scol[n] = WT_EMPTY;
+    __syncthreads();
     for (int j = threadIdx.x; j < nb; j += WIDE_THREADS)
         for (int l = 0; l < sblk[j].k; ++l) scol[sblk[j].off + l] = (uint32_t(j) << 16) | uint32_t(l);
     __syncthreads();
@@ -337,12 +342,11 @@ k_ctform_wide(const WTUnit* __restrict__ units, const WTBlk* __restrict__ blks, 
             // B: stacked column n, unit jj (tile rows 8jj .. 8jj+7) -> atom n / 8, row n % 8
             for (int i = p; i < npad * 8; i += WIDE_PRODUCERS) {
                 const int n = i >> 3, jj = i & 7;
-                bool in = n < nc && 8 * jj < int(tl.ld);
+                const uint32_t cm = n < nc ? scol[n] : WT_EMPTY;
+                const bool in = cm != WT_EMPTY && 8 * jj < int(tl.ld);
                 const uint8_t* src = A;
-                if (in) {
-                    const uint32_t cm = scol[n];
+                if (in)
                     src = A + size_t(sslab[q * nb + int(cm >> 16)]) * 16 + size_t(cm & 0xffffu) * tl.ld * 2 + 16 * jj;
-                }
                 tc5::cp16(sb + uint32_t(n >> 3) * 1024u + swz(n & 7, jj), src, in ? 16u : 0u);
             }
             tc5::cp_commit();
@@ -403,6 +407,7 @@ k_ctform_wide(const WTUnit* __restrict__ units, const WTBlk* __restrict__ blks, 
         if (__all_sync(0xffffffffu, ok)) {
             for (int n = warp; n < nc; n += 4) {
                 const uint32_t cm = scol[n];
+                if (cm == WT_EMPTY) continue;
                 const WTBlk& b = sblk[cm >> 16];
                 const int l = int(cm & 0xffffu);
                 const float4 t4 = reinterpret_cast<const float4*>(red + n * WIDE_TERMS)[lane];

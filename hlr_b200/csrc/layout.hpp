@@ -266,4 +266,22 @@ struct WTTile {
 };
 static_assert(sizeof(WTTile) == 8, "WTTile is 8 bytes");
 
+// 64-vector N-form of full 64-row tiles with TMA: a segment (output tile) is
+// a list of stages, one per run of at most 32 columns whose vector entries
+// are consecutive; the matrix columns of a stage are consecutive 128-byte
+// rows of the store (srow = byte offset / 128).  Every column of the
+// segment has factor 1 (the store's row-group scales), E as in MSeg.pad.
+struct WSeg {
+    uint32_t st0, nst;     // stages [st0, st0 + nst)
+    uint32_t out;          // first output row
+    int32_t E;
+};
+static_assert(sizeof(WSeg) == 16, "WSeg is 16 bytes");
+struct WStage {
+    uint32_t srow;         // first matrix column: store row of 128 bytes
+    uint32_t e0;           // first vector entry (| VEC_T: in t)
+    uint32_t nc;           // columns (1 .. 32)
+};
+static_assert(sizeof(WStage) == 12, "WStage is 12 bytes");
+
 }  // namespace hlrc

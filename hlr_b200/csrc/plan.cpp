@@ -136,6 +136,15 @@ struct Store {
     // per chunk: scale group (-1: the chunk's own scale).  Scaled chunks of
     // one group share the scale of the group's largest entry.
     std::vector<int32_t> sgrp;
+    // per chunk: row group (-1: none) and exponent c.  The chunks of a row
+    // group get scale F 2^-c, where F is the largest of the chunks' own
+    // scales times 2^c: one output tile's chunks then need no factors when
+    // the vector entries of a chunk with exponent c are kept times 2^-c.
+    std::vector<int32_t> rgrp;
+    std::vector<int32_t> cexp;
+    // 16-bit chunks of a region start each layout group on a 128-byte
+    // boundary (full-height columns are then 128-byte rows for 2-D TMA)
+    bool align128 = false;
     size_t region_begin = 0;           // first chunk without a byte offset
     int64_t bytes = 0;
     int64_t unpadded[NFMT] = {};
@@ -144,7 +153,8 @@ struct Store {
     // column, may be null -> deffmt); chunks do not straddle `cuts`.  Byte
     // offsets are assigned by close_region().
     int alloc(const double* src, int64_t lds, int64_t r0, int64_t rows, int64_t ncols, const uint8_t* colfmt,
-              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr, int grp = 1, int32_t scale_group = -1) {
+              uint8_t deffmt, const std::vector<int64_t>* cuts = nullptr, int grp = 1, int32_t scale_group = -1,
+              int32_t row_group = -1, int32_t c_exp = 0) {
         SSlab s{src, lds, r0, rows, pad_rows(rows), int32_t(chunks.size()), 0};
         int64_t j = 0;
         size_t ci = 0;
@@ -163,6 +173,8 @@ struct Store {
             group.push_back(uint8_t(grp));
             crows.push_back(int32_t(rows));
             sgrp.push_back(scale_group);
+            rgrp.push_back(row_group);
+            cexp.push_back(c_exp);
             ++s.nch;
             j = e;
         }
@@ -173,13 +185,18 @@ struct Store {
     // Places the chunks allocated since the last call: by layout_rank, then
     // in allocation order, each on a 16-byte boundary.
     void close_region() {
-        for (int r = 0; r < 2 * NFMT; ++r)
+        for (int r = 0; r < 2 * NFMT; ++r) {
+            bool first = true;
             for (size_t c = region_begin; c < chunks.size(); ++c) {
                 SChunk& ch = chunks[c];
                 if (layout_rank(group[c], ch.fmt) != r) continue;
                 ch.byte_off = align16(bytes);
+                if (first && align128 && (ch.fmt == FMT_F16 || ch.fmt == FMT_BF16))
+                    ch.byte_off = (ch.byte_off + 127) / 128 * 128;
+                first = false;
                 bytes = ch.byte_off + pad_fmt(crows[c], ch.fmt) * ch.nc * fmt_bytes(ch.fmt);
             }
+        }
         region_begin = chunks.size();
     }
 
@@ -194,20 +211,30 @@ struct Store {
 
     void fill(std::vector<uint8_t>& st) {
         st.assign(size_t(bytes), 0);
-        // scale groups: the largest entry over all chunks of a group
-        int32_t ngrp = 0;
+        // scale groups: the largest entry over all chunks of a group; row
+        // groups: the largest exponent of (own scale x 2^c) over the group's
+        // nonzero chunks
+        int32_t ngrp = 0, nrg = 0;
         for (int32_t g : sgrp) ngrp = std::max(ngrp, g + 1);
+        for (int32_t g : rgrp) nrg = std::max(nrg, g + 1);
         std::vector<double> gmax(size_t(ngrp), 0.0);
-        if (ngrp > 0) {
+        std::vector<int> rexp(size_t(nrg), INT32_MIN);
+        if (ngrp > 0 || nrg > 0) {
             std::vector<double> cmax(chunks.size(), 0.0);
             #pragma omp parallel for schedule(dynamic, 64)
             for (int64_t si = 0; si < int64_t(slabs.size()); ++si) {
                 const SSlab& sl = slabs[size_t(si)];
                 for (int32_t c = sl.c0; c < sl.c0 + sl.nch; ++c)
-                    if (sgrp[size_t(c)] >= 0) cmax[size_t(c)] = chunk_amax(sl, chunks[size_t(c)]);
+                    if (sgrp[size_t(c)] >= 0 || rgrp[size_t(c)] >= 0) cmax[size_t(c)] = chunk_amax(sl, chunks[size_t(c)]);
             }
-            for (size_t c = 0; c < chunks.size(); ++c)
+            for (size_t c = 0; c < chunks.size(); ++c) {
                 if (sgrp[c] >= 0) gmax[size_t(sgrp[c])] = std::max(gmax[size_t(sgrp[c])], cmax[c]);
+                if (rgrp[c] >= 0 && cmax[c] > 0) {
+                    int ex = 0;
+                    std::frexp(cmax[c], &ex);   // own scale 2^(ex - 15)
+                    rexp[size_t(rgrp[c])] = std::max(rexp[size_t(rgrp[c])], ex - 15 + cexp[c]);
+                }
+            }
         }
         #pragma omp parallel for schedule(dynamic, 64)
         for (int64_t si = 0; si < int64_t(slabs.size()); ++si) {
@@ -249,12 +276,14 @@ struct Store {
                     }
                 } else {
                     // power-of-two scale bringing the chunk's (or its scale
-                    // group's) largest entry to [2^14, 2^15)
-                    const int32_t g = sgrp[size_t(c)];
+                    // group's) largest entry to [2^14, 2^15); row groups: F 2^-c
+                    const int32_t g = sgrp[size_t(c)], rg = rgrp[size_t(c)];
                     const double amax = g >= 0 ? gmax[size_t(g)] : chunk_amax(s, ch);
                     int ex = 0;
                     if (amax > 0) std::frexp(amax, &ex);
-                    const double scale = amax > 0 ? std::ldexp(1.0, ex - 15) : 1.0;
+                    double scale = amax > 0 ? std::ldexp(1.0, ex - 15) : 1.0;
+                    if (rg >= 0 && rexp[size_t(rg)] != INT32_MIN)
+                        scale = std::ldexp(1.0, rexp[size_t(rg)] - cexp[size_t(c)]);
                     ch.scale = float(scale);
                     const double inv = 1.0 / scale;
                     for (int j = 0; j < ch.nc; ++j) {
@@ -747,7 +776,8 @@ uint8_t default_format(int prec) {
 // WT_MAXT tiles is cut into pieces, each writing FP32 partials that a finish
 // group per block sums in piece order.
 hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<int64_t>& toff,
-                      const std::vector<std::vector<int>>& slabV, const Store& st, Plan& p) {
+                      const std::vector<int32_t>& cblk, const std::vector<std::vector<int>>& slabV, const Store& st,
+                      Plan& p) {
     WidePlan& W = p.wide;
     W = WidePlan();
     for (int64_t t = 0; t < tc.n(); ++t)
@@ -757,11 +787,7 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
     for (int64_t i = 0; i < d.nblocks; ++i) {
         const hlrc_block& b = d.blocks[i];
         if (toff[size_t(i)] < 0) continue;
-        for (int64_t l = 0; l < b.rank; ++l) {   // c = ceil-ish log2 ||V(:,l)||_1: 2^c > the norm
-            double s1 = 0;
-            for (int64_t r = 0; r < b.ncols; ++r) s1 += std::fabs(b.V[r + l * b.ldv]);
-            W.t_exp[size_t(toff[size_t(i)] + l)] = int8_t(s1 > 0 ? std::max(-120, std::min(120, std::ilogb(s1) + 1)) : 0);
-        }
+        for (int64_t l = 0; l < b.rank; ++l) W.t_exp[size_t(toff[size_t(i)] + l)] = int8_t(cblk[size_t(i)]);
         groups[{b.col0, b.ncols}].push_back(i);
     }
     struct Item { int64_t blk, l0, k; };
@@ -782,7 +808,9 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
         while (a < items.size()) {   // one subset: items [a, e) with at most WT_MAXN columns
             size_t e = a;
             int64_t nc = 0;
-            while (e < items.size() && nc + items[e].k <= WT_MAXN && int(e - a) < WT_MAXB) nc += items[e++].k;
+            // stacked columns start on multiples of 8 (8-column TMA boxes)
+            while (e < items.size() && nc + (items[e].k + 7) / 8 * 8 <= WT_MAXN && int(e - a) < WT_MAXB)
+                nc += (items[e++].k + 7) / 8 * 8;
             const int64_t P = (T + WT_MAXT - 1) / WT_MAXT;
             const int64_t part0 = P > 1 ? W.npart : 0;
             if (P > 1) W.npart += P * nc;
@@ -809,7 +837,7 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
                     wb.scale = st.chunks[size_t(s0.c0)].scale;
                     wb.pbase = uint32_t(part0 + P * off);
                     W.blks.push_back(wb);
-                    off += it.k;
+                    off += (it.k + 7) / 8 * 8;
                 }
                 for (int64_t t = q0; t < q1; ++t)
                     for (size_t j = a; j < e; ++j) {
@@ -952,16 +980,38 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     // ordered by column tile, so that each pass streams one contiguous
     // range per tile
     Store st;
+    // 16-bit stores also serve the 64-vector product (plan_wide): the chunks
+    // of a row tile form a row group with exponent c_b for the U slabs of
+    // block b (2^c_b > ||V(:,l)||_1 for all l), so that the tile's run needs
+    // no per-column factors, and 16-bit groups start on 128-byte boundaries
+    const bool wide16 = o.precision == HLRC_PREC_F16 || o.precision == HLRC_PREC_BF16;
+    std::vector<int32_t> cblk(static_cast<size_t>(nb), 0);
+    if (wide16) {
+        st.align128 = true;
+        for (int64_t i = 0; i < nb; ++i) {
+            const hlrc_block& b = d.blocks[i];
+            if (toff[size_t(i)] < 0) continue;
+            int c = INT32_MIN;
+            for (int64_t l = 0; l < b.rank; ++l) {
+                double s1 = 0;
+                for (int64_t r = 0; r < b.ncols; ++r) s1 += std::fabs(b.V[r + l * b.ldv]);
+                if (s1 > 0) c = std::max(c, std::ilogb(s1) + 1);
+            }
+            cblk[size_t(i)] = c == INT32_MIN ? 0 : std::max(-120, std::min(120, c));
+        }
+    }
     std::vector<std::vector<int>> slabA(static_cast<size_t>(nb)), slabV(static_cast<size_t>(nb));
     for (int64_t t = 0; t < tr.n(); ++t) {
+        const int32_t rg = wide16 ? int32_t(t) : -1;
         for (int64_t i : rowlist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
             const int64_t r0 = tr.lo(t) - b.row0, rows = tr.size(t);
             if (b.kind == HLRC_LEAF_DENSE) {
                 const std::vector<int64_t> cuts = inner_cuts(tc, b.col0, b.ncols);
-                slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols, nullptr, densefmt, &cuts, 0));
+                slabA[size_t(i)].push_back(st.alloc(b.D, b.ldd, r0, rows, b.ncols, nullptr, densefmt, &cuts, 0, -1, rg, 0));
             } else {
-                slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank, cf(i), deffmt));
+                slabA[size_t(i)].push_back(st.alloc(b.U, b.ldu, r0, rows, b.rank, cf(i), deffmt, nullptr, 1, -1, rg,
+                                                    cblk[size_t(i)]));
             }
         }
         st.close_region();
@@ -970,7 +1020,6 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     // column tiles, so the 64-vector T-form can sum a block's tiles in one
     // accumulator (the per-element precision of a 16-bit float does not
     // depend on the scale)
-    const bool wide16 = o.precision == HLRC_PREC_F16 || o.precision == HLRC_PREC_BF16;
     for (int64_t t = 0; t < tc.n(); ++t) {
         for (int64_t i : collist[size_t(t)]) {
             const hlrc_block& b = d.blocks[i];
@@ -1077,7 +1126,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     for (const TTPass& tp : p.ttpasses)
         if (tp.npart >= (int64_t(1) << 32)) return fail(HLRC_ERR_SHAPE, "partial array exceeds 2^32 entries");
     if (wide16) {
-        if (hlrc_status ws = plan_wide(d, tc, toff, slabV, st, p); ws != HLRC_OK) return ws;
+        if (hlrc_status ws = plan_wide(d, tc, toff, cblk, slabV, st, p); ws != HLRC_OK) return ws;
     }
 
     if (hlrc_status vs = validate_plan(p); vs != HLRC_OK) return vs;

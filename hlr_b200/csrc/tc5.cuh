@@ -106,6 +106,27 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// --------------------------------------------------------------------- TMA
+// 2-D tile load (cp.async.bulk.tensor, no multicast) of this GPU's memory
+// into shared memory, completing on `bar`; tmap points to a CUtensorMap
+// kernel parameter (__grid_constant__).  c0 is the inner coordinate (in
+// elements, a multiple of 16 bytes), c1 the row.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int c0, int c1, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            dst),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+// one arrival on `bar` that also announces `bytes` of asynchronous copies
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
 // ----------------------------------------------------------------- TMEM
 // allocation by one whole warp; the address lands in *slot (shared memory)
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {

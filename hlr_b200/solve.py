@@ -13,14 +13,24 @@ per-system reductions view them as (nrhs, count, pad).  Padding rows stay
 zero throughout.  Refinement converges when kappa(A) * u_inner < 1 (u_inner
 is the inner operator's relative error); systems where it stalls are
 reported as not converged.
+
+Preconditioning.  The reference preconditions its linear iteration with an
+H-LU factorisation applied by triangular solves (iterrefine.hh:125-184,
+matrix/luinv_eval.hh).  Here the inner CG can be preconditioned with a
+block-Jacobi operator W = diag(A_kk^-1): the dense inverses of the diagonal
+blocks of A (contiguous index ranges of `block` entries, assembled from the
+leaves inside them), uploaded as a block-diagonal H-matrix of dense leaves,
+so that applying W is one more product with the same kernels.  H-LU itself
+(H-matrix arithmetic with recompression) is not built.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass, field
 
+import numpy as np
 import torch
 
-from . import apply_normal, mul_vec
+from . import LeafList, apply_normal, mul_vec, upload, upload_batch
 
 
 @dataclass
@@ -42,23 +52,98 @@ def _axpy_(y, coef, x, count, pad):
     y.view(y.shape[0], count, pad).add_(coef[:, :, None] * x.view(x.shape[0], count, pad))
 
 
-class _InnerCG:
-    """Static-tensor CG state so that a block of iterations can be captured
-    in a CUDA graph and replayed."""
+def _leaf_array(ptr, ld, rows, cols):
+    """The (rows x cols) column-major matrix behind a leaf pointer (a view)."""
+    if rows == 0 or cols == 0:
+        return np.zeros((rows, cols))
+    a = np.ctypeslib.as_array(ptr, shape=(ld * cols,))
+    return a.reshape(cols, ld).T[:rows]
 
-    def __init__(self, A, nrhs, N, count, pad, device):
-        self.A, self.count, self.pad = A, count, pad
+
+def diagonal_blocks(src, block: int = 256):
+    """The dense diagonal blocks A_kk of an H-matrix (HostMatrix, LeafList or
+    hlrc_h_desc): index ranges [k block, (k + 1) block), each assembled from
+    the parts of the leaves (D, or U V^T) that fall inside it.  Returns a
+    list of (first index, dense block)."""
+    d = src.h_desc() if hasattr(src, "h_desc") else src
+    n = int(d.nrows)
+    starts = list(range(0, n, block))
+    out = [np.zeros((min(block, n - i0), min(block, n - i0))) for i0 in starts]
+    for i in range(int(d.nblocks)):
+        b = d.blocks[i]
+        r0, nr, c0, nc = int(b.row0), int(b.nrows), int(b.col0), int(b.ncols)
+        if nr == 0 or nc == 0:
+            continue
+        for k in range(max(r0, c0) // block, min(r0 + nr - 1, c0 + nc - 1) // block + 1):
+            i0, i1 = starts[k], min(starts[k] + block, n)
+            ra, rb = max(r0, i0), min(r0 + nr, i1)
+            ca, cb = max(c0, i0), min(c0 + nc, i1)
+            if ra >= rb or ca >= cb:
+                continue
+            if b.kind == 0:
+                D = _leaf_array(b.D, int(b.ldd), nr, nc)
+                part = D[ra - r0:rb - r0, ca - c0:cb - c0]
+            else:
+                if b.rank == 0:
+                    continue
+                U = _leaf_array(b.U, int(b.ldu), nr, int(b.rank))
+                V = _leaf_array(b.V, int(b.ldv), nc, int(b.rank))
+                part = U[ra - r0:rb - r0] @ V[ca - c0:cb - c0].T
+            out[k][ra - i0:rb - i0, ca - i0:cb - i0] += part
+    return list(zip(starts, out))
+
+
+def block_jacobi_leaves(src, block: int = 256) -> LeafList:
+    """W = diag(A_kk^-1) as a leaf list of dense blocks (A_kk symmetric
+    positive definite: inverted through its Cholesky factor)."""
+    d = src.h_desc() if hasattr(src, "h_desc") else src
+    n = int(d.nrows)
+    W = LeafList(n, n)
+    for i0, Akk in diagonal_blocks(d, block):
+        L = np.linalg.cholesky(0.5 * (Akk + Akk.T))
+        Li = np.linalg.solve(L, np.eye(L.shape[0]))
+        W.add_dense(i0, i0, Li.T @ Li)
+    return W
+
+
+def block_jacobi(src, block: int = 256, precision="f64", max_nrhs: int = 1):
+    """The block-Jacobi preconditioner of one H-matrix, uploaded (a
+    DeviceMatrix applied with mul_vec)."""
+    return upload(block_jacobi_leaves(src, block), precision=precision, max_nrhs=max_nrhs)
+
+
+def block_jacobi_batch(members, pad: int, block: int = 256, precision="f64", max_nrhs: int = 1):
+    """The same for the members of a batched handle uploaded with pad_to=pad."""
+    return upload_batch([block_jacobi_leaves(m, block) for m in members], precision=precision, max_nrhs=max_nrhs,
+                        pad_to=pad)
+
+
+class _InnerCG:
+    """Static-tensor (preconditioned) CG state so that a block of iterations
+    can be captured in a CUDA graph and replayed.  With W (a DeviceMatrix)
+    the iteration is PCG with z = W r."""
+
+    def __init__(self, A, nrhs, N, count, pad, device, W=None):
+        self.A, self.W, self.count, self.pad = A, W, count, pad
         z = lambda: torch.zeros(nrhs, N, dtype=torch.float64, device=device)
         self.d, self.res, self.p, self.q = z(), z(), z(), z()
+        self.z = z() if W is not None else self.res
         zs = lambda: torch.zeros(nrhs, count, dtype=torch.float64, device=device)
-        self.rr, self.stop = zs(), zs()
+        self.rr, self.rz, self.stop = zs(), zs(), zs()
         self.active = torch.zeros(nrhs, count, dtype=torch.bool, device=device)
+
+    def _precondition(self):
+        if self.W is not None:
+            self.z.zero_()
+            mul_vec(1.0, apply_normal, self.W, self.res.T, self.z.T)
 
     def reset(self, r, rtol):
         self.d.zero_()
         self.res.copy_(r)
-        self.p.copy_(r)
+        self._precondition()
+        self.p.copy_(self.z)
         self.rr.copy_(_dots(r, r, self.count, self.pad))
+        self.rz.copy_(_dots(r, self.z, self.count, self.pad))
         self.stop.copy_(rtol * rtol * self.rr)
         self.active.copy_(self.rr > 0)
 
@@ -68,32 +153,38 @@ class _InnerCG:
         mul_vec(1.0, apply_normal, self.A, self.p.T, self.q.T)
         pq = _dots(self.p, self.q, c, p)
         ok = self.active & (pq > 0)
-        a = torch.where(ok, self.rr / torch.where(ok, pq, torch.ones_like(pq)), torch.zeros_like(pq))
+        a = torch.where(ok, self.rz / torch.where(ok, pq, torch.ones_like(pq)), torch.zeros_like(pq))
         _axpy_(self.d, a, self.p, c, p)
         _axpy_(self.res, -a, self.q, c, p)
         rr_new = _dots(self.res, self.res, c, p)
         self.active &= rr_new > self.stop
-        beta = torch.where(self.active, rr_new / torch.where(self.rr > 0, self.rr, torch.ones_like(self.rr)),
-                           torch.zeros_like(rr_new))
-        self.p.view(self.p.shape[0], c, p).mul_(beta[:, :, None]).add_(self.res.view(self.res.shape[0], c, p))
+        self._precondition()
+        rz_new = _dots(self.res, self.z, c, p) if self.W is not None else rr_new
+        beta = torch.where(self.active, rz_new / torch.where(self.rz > 0, self.rz, torch.ones_like(self.rz)),
+                           torch.zeros_like(rz_new))
+        self.p.view(self.p.shape[0], c, p).mul_(beta[:, :, None]).add_(self.z.view(self.z.shape[0], c, p))
         self.rr.copy_(rr_new)
+        self.rz.copy_(rz_new)
 
 
 def cg_refine(A64, Alow, b: torch.Tensor, count: int, pad: int, tol: float = 1e-10, inner_rtol: float = 1e-6,
-              max_outer: int = 20, max_inner: int = 20000, check_every: int = 20, use_graph: bool = True) -> CGResult:
+              max_outer: int = 20, max_inner: int = 20000, check_every: int = 20, use_graph: bool = True,
+              precond=None) -> CGResult:
     """Solve A x = b for every member and right-hand side of a batched handle.
 
     A64: FP64 batched DeviceMatrix (outer residual); Alow: the same matrices
     in reduced precision (inner CG operator; may be A64 itself).  b is
-    (nrhs, count * pad).  Stops when every system reaches ||b - A x|| <= tol
-    ||b|| with the FP64 product, or when refinement stops improving.
+    (nrhs, count * pad).  precond: an optional preconditioner W (a batched
+    DeviceMatrix, e.g. block_jacobi_batch) for the inner CG.  Stops when
+    every system reaches ||b - A x|| <= tol ||b|| with the FP64 product, or
+    when refinement stops improving.
     """
     nrhs, N = b.shape
     dev = b.device
     bnorm = _dots(b, b, count, pad).sqrt()
     x = torch.zeros_like(b)
     r = torch.zeros_like(b)
-    cg = _InnerCG(Alow, nrhs, N, count, pad, dev)
+    cg = _InnerCG(Alow, nrhs, N, count, pad, dev, precond)
     graph = None
     if use_graph:
         # warm up on a side stream, then capture `check_every` iterations

@@ -34,6 +34,8 @@ MATS = {
     # full 64-row tiles, blocks spanning many column tiles (two-level finish)
     "exp3d_16384_64": lambda: hlr.build(hlr.Problem.exp3d(16384)),
     "log1d_8192": lambda: hlr.build(hlr.Problem.log1d(8192)),
+    # 64-row and 32/33-row tiles: the TMA kernels and the cp.async kernels in one product
+    "exp3d_8200_64": lambda: hlr.build(hlr.Problem.exp3d(8200)),
 }
 
 
