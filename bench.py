@@ -425,9 +425,23 @@ def run_ours(args, rank, world, local_rank):
     hm = hlr.build(prob)
     t_build = time.perf_counter() - tb
     tu = time.perf_counter()
-    M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2)
+    plan_tuned = None
+    if args.tune_plan and not args.no_autotune:
+        # plan-level choices: the 64-vector T-form's piece length for wide
+        # 16-bit products, the finish's two-level threshold otherwise
+        from hlr_b200.tune import autotune_plan
+        knobs = ("piece_tiles",) if prec in ("f16", "bf16") and nrhs > 8 and not uniform and not args.h2 \
+            else ("finish_slots",)
+        M, plan_tuned = autotune_plan(
+            lambda p: hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2, plan=p),
+            nrhs=nrhs, knobs=knobs)
+    else:
+        M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2)
     t_upload = time.perf_counter() - tu
     tuned = tune_handle(M, nrhs, args)
+    if tuned is not None:
+        tuned = dict(tuned, plan=M.plan or "defaults",
+                     plan_times_ms=plan_tuned["times_ms"] if plan_tuned else None)
     info = M.info
     n = hm.n
     # x ~ N(0,1), one column per right-hand side (column-major (n, nrhs))
@@ -608,10 +622,27 @@ def run_batch(args, rank, world, local_rank):
     hms = [hlr.build(p) for p in c5_problems(count, nthreads=os.cpu_count() or 0)]
     t_build = time.perf_counter() - tb
     pad = (max(h.n for h in hms) + 63) // 64 * 64
-    A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
-    Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
+    plan64 = planlow = None
+    if args.tune_plan and not args.no_autotune:
+        # the two-level finish threshold, per store (many small multi-tile outputs)
+        from hlr_b200.tune import autotune_plan
+        A64, plan64 = autotune_plan(lambda p: hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad, plan=p),
+                                    nrhs=nrhs, knobs=("finish_slots",))
+        if inner == "f64":
+            Alow = A64
+        else:
+            Alow, planlow = autotune_plan(
+                lambda p: hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad, plan=p), nrhs=nrhs,
+                knobs=("finish_slots",))
+    else:
+        A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
+        Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
     tuned64 = tune_handle(A64, nrhs, args)
     tuned = tune_handle(Alow, nrhs, args) if Alow is not A64 else tuned64
+    if tuned is not None:
+        tuned = dict(tuned, plan=Alow.plan or "defaults", plan_times_ms=planlow["times_ms"] if planlow else None)
+    if tuned64 is not None:
+        tuned64 = dict(tuned64, plan=A64.plan or "defaults", plan_times_ms=plan64["times_ms"] if plan64 else None)
     N = count * pad
     rng = np.random.default_rng(9)
     b = np.zeros((nrhs, N))
@@ -919,11 +950,15 @@ def main():
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per product (default: the config's)")
     ap.add_argument("--shard", action="store_true",
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
+    ap.add_argument("--tune-plan", action="store_true", default=None,
+                    help="also tune plan-level choices by re-uploading (default: on for c4 and c5)")
     ap.add_argument("--reduced", default="bfp,mixed",
                     help="reduced-precision stores timed beside the FP64 one-vector H-matrix line "
                          "(comma list of bfp, mixed, f32, f16, bf16; 'none' for none)")
     args = ap.parse_args()
     args.reduced = [] if args.reduced in ("", "none") else args.reduced.split(",")
+    if args.tune_plan is None:
+        args.tune_plan = args.config in ("c4", "c5")
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

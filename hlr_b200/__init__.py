@@ -189,11 +189,17 @@ class LeafList:
         return d
 
 
-def _options(precision="f64", max_nrhs: int = 1, mixed_eps: float = 1e-6, device: int = -1):
+def _options(precision="f64", max_nrhs: int = 1, mixed_eps: float = 1e-6, device: int = -1, plan=None):
     o = _capi.hlrc_options()
     lib().hlrc_default_options(C.byref(o))
     o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     o.max_nrhs, o.mixed_eps, o.device = max_nrhs, mixed_eps, device
+    plan = plan or {}
+    unknown = set(plan) - {"finish_slots", "piece_tiles"}
+    if unknown:
+        raise ValueError(f"unknown plan options {sorted(unknown)}")
+    o.finish_slots = int(plan.get("finish_slots", 0))
+    o.piece_tiles = int(plan.get("piece_tiles", 0))
     return o
 
 
@@ -204,6 +210,7 @@ class DeviceMatrix:
         self._h = handle
         self.uniform = uniform
         self.h2 = False
+        self.plan = {}     # plan-level choices it was uploaded with
         inf = _capi.hlrc_info()
         check(lib().hlrc_get_info(self._h, C.byref(inf)), "hlrc_get_info")
         self.info = {f: getattr(inf, f) for f, _ in _capi.hlrc_info._fields_ if f not in ("reserved", "launches")}
@@ -304,22 +311,24 @@ class Workspace:
 
 
 def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
-           mixed_eps: float = 1e-6, device: int = -1, h2: bool = False) -> DeviceMatrix:
+           mixed_eps: float = 1e-6, device: int = -1, h2: bool = False, plan: Optional[dict] = None) -> DeviceMatrix:
     """Flatten and upload a matrix: ``src`` is a HostMatrix, LeafList or
     descriptor.  ``h2=True`` uploads the H^2 form (nested cluster bases) of
     a HostMatrix built with ``Problem(..., nested=True)``, or an
-    ``hlrc_h2_desc``."""
+    ``hlrc_h2_desc``.  ``plan``: plan-level choices (``finish_slots``,
+    ``piece_tiles``; see hlrc_options), e.g. from tune.autotune_plan."""
     if isinstance(src, _capi.hlrc_h2_desc):
         h2 = True
     if uniform is None:
         uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
-    o = _options(precision, max_nrhs, mixed_eps, device)
+    o = _options(precision, max_nrhs, mixed_eps, device, plan)
     h = C.c_void_p()
     if h2:
         d = src.h2_desc() if hasattr(src, "h2_desc") else src
         check(lib().hlrc_upload_h2(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_h2")
         M = DeviceMatrix(h, False)
         M.h2 = True
+        M.plan = dict(plan or {})
         return M
     if uniform:
         d = src.uniform_desc() if hasattr(src, "uniform_desc") else src
@@ -327,11 +336,13 @@ def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int =
     else:
         d = src.h_desc() if hasattr(src, "h_desc") else src
         check(lib().hlrc_upload_h(C.byref(d), C.byref(o), C.byref(h)), "hlrc_upload_h")
-    return DeviceMatrix(h, uniform)
+    M = DeviceMatrix(h, uniform)
+    M.plan = dict(plan or {})
+    return M
 
 
 def upload_batch(members, precision="f64", max_nrhs: int = 1, pad_to: Optional[int] = None,
-                 mixed_eps: float = 1e-6, device: int = -1) -> DeviceMatrix:
+                 mixed_eps: float = 1e-6, device: int = -1, plan: Optional[dict] = None) -> DeviceMatrix:
     """Upload many H-matrices as one block-diagonal handle.
 
     Member i occupies rows/columns [offsets[i], offsets[i] + n_i); with
@@ -351,23 +362,24 @@ def upload_batch(members, precision="f64", max_nrhs: int = 1, pad_to: Optional[i
             offsets.append(offsets[-1] + s)
     arr = (_capi.hlrc_h_desc * len(descs))(*descs)
     offs = (C.c_int64 * len(offsets))(*offsets)
-    o = _options(precision, max_nrhs, mixed_eps, device)
+    o = _options(precision, max_nrhs, mixed_eps, device, plan)
     h = C.c_void_p()
     check(lib().hlrc_upload_h_batch(arr, len(descs), offs, C.byref(o), C.byref(h)), "hlrc_upload_h_batch")
     M = DeviceMatrix(h, False)
+    M.plan = dict(plan or {})
     M.offsets = offsets
     M.sizes = sizes
     return M
 
 
 def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int = 1,
-              mixed_eps: float = 1e-6, h2: bool = False) -> dict:
+              mixed_eps: float = 1e-6, h2: bool = False, plan: Optional[dict] = None) -> dict:
     """Dry run of :func:`upload`: validates and flattens on the host only."""
     if isinstance(src, _capi.hlrc_h2_desc):
         h2 = True
     if uniform is None:
         uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
-    o = _options(precision, max_nrhs, mixed_eps, -1)
+    o = _options(precision, max_nrhs, mixed_eps, -1, plan)
     inf = _capi.hlrc_info()
     if h2:
         d = src.h2_desc() if hasattr(src, "h2_desc") else src

@@ -63,7 +63,7 @@ class hlrc_h2_desc(C.Structure):
 
 class hlrc_options(C.Structure):
     _fields_ = [("precision", i32), ("max_nrhs", i32), ("mixed_eps", f64), ("device", i32),
-                ("reserved", i32 * 7)]
+                ("finish_slots", i32), ("piece_tiles", i32), ("reserved", i32 * 5)]
 
 
 class hlrc_info(C.Structure):

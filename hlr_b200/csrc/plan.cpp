@@ -452,6 +452,29 @@ struct NBuilder {
 // input tile.  Objects fed by one slab write their chunks' results directly;
 // objects fed by several write per-slab partials that a finish pass sums in
 // slab order.
+// Plan-level choices of the running planner call (hlrc_options), read by the
+// builders; set for the duration of a plan_* call by KnobScope.
+struct PlanKnobs {
+    uint32_t finish_slots = FINISH_SLOTS;
+    int piece_tiles = WT_MAXT;
+};
+thread_local PlanKnobs g_knobs;
+struct KnobScope {
+    PlanKnobs saved;
+    explicit KnobScope(const hlrc_options& o) : saved(g_knobs) {
+        g_knobs.finish_slots = o.finish_slots > 0 ? uint32_t(o.finish_slots) : FINISH_SLOTS;
+        g_knobs.piece_tiles = o.piece_tiles > 0 ? o.piece_tiles : WT_MAXT;
+    }
+    ~KnobScope() { g_knobs = saved; }
+};
+hlrc_status check_knobs(const hlrc_options& o) {
+    if (o.finish_slots != 0 && (o.finish_slots < 2 || o.finish_slots > 64))
+        return fail(HLRC_ERR_ARG, "finish_slots %d outside 2..64", o.finish_slots);
+    if (o.piece_tiles != 0 && (o.piece_tiles < 1 || o.piece_tiles > WT_MAXT))
+        return fail(HLRC_ERR_ARG, "piece_tiles %d outside 1..%d", o.piece_tiles, WT_MAXT);
+    return HLRC_OK;
+}
+
 struct TTBuilder {
     TTPass& P;
     const Store& S;
@@ -528,12 +551,13 @@ struct TTBuilder {
         // the output's group then sums the runs.  The order of all additions
         // depends on the shapes only.
         for (TGroup& g : P.groups) {
-            if (g.nslots <= FINISH_SLOTS) continue;
-            const uint32_t nrun = (g.nslots + FINISH_SLOTS - 1) / FINISH_SLOTS;
+            const uint32_t FS = g_knobs.finish_slots;
+            if (g.nslots <= FS) continue;
+            const uint32_t nrun = (g.nslots + FS - 1) / FS;
             const uint32_t scratch = uint32_t(P.npart);
             for (uint32_t r = 0; r < nrun; ++r) {
-                const uint32_t s0 = r * FINISH_SLOTS;
-                P.groups1.push_back({g.slot0 + s0 * g.nc, std::min(FINISH_SLOTS, g.nslots - s0), scratch + r * g.nc, g.nc});
+                const uint32_t s0 = r * FS;
+                P.groups1.push_back({g.slot0 + s0 * g.nc, std::min(FS, g.nslots - s0), scratch + r * g.nc, g.nc});
             }
             P.npart += int64_t(nrun) * g.nc;
             g.slot0 = scratch;
@@ -811,7 +835,8 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
             // stacked columns start on multiples of 8 (8-column TMA boxes)
             while (e < items.size() && nc + (items[e].k + 7) / 8 * 8 <= WT_MAXN && int(e - a) < WT_MAXB)
                 nc += (items[e++].k + 7) / 8 * 8;
-            const int64_t P = (T + WT_MAXT - 1) / WT_MAXT;
+            const int64_t PT = g_knobs.piece_tiles;
+            const int64_t P = (T + PT - 1) / PT;
             const int64_t part0 = P > 1 ? W.npart : 0;
             if (P > 1) W.npart += P * nc;
             for (int64_t q = 0; q < P; ++q) {
@@ -878,6 +903,8 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
 }
 
 hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area) {
+    if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
+    const KnobScope knobs(o);
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0) return fail(HLRC_ERR_SHAPE, "negative matrix size");
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
@@ -1153,6 +1180,8 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
 
 // ------------------------------------------------------------- uniform-H
 hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan& p) {
+    if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
+    const KnobScope knobs(o);
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0 || d.nrow_bases < 0 || d.ncol_bases < 0)
         return fail(HLRC_ERR_SHAPE, "negative size");
     if ((d.nblocks > 0 && !d.blocks) || (d.nrow_bases > 0 && !d.row_bases) || (d.ncol_bases > 0 && !d.col_bases))
@@ -1438,6 +1467,8 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
 // transposed (unit T-form), backward down the column tree, leaf column
 // bases, and the near field transposed.
 hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
+    if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
+    const KnobScope knobs(o);
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0 || d.nrow_clusters <= 0 || d.ncol_clusters <= 0)
         return fail(HLRC_ERR_SHAPE, "H2: bad sizes or empty cluster tree");
     if ((d.nblocks > 0 && !d.blocks) || !d.row_clusters || !d.col_clusters)

@@ -164,3 +164,51 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
     if path is not None:
         _store(path, key, {"tuning": out["tuning"], "times_ms": times})
     return out
+
+
+# ------------------------------------------------------------ plan level
+PLAN_CANDIDATES = {
+    # tile T-form outputs with more partials than this are summed in two levels
+    "finish_slots": (16, 8, 32),
+    # 64-vector T-form: tiles per piece of a long column cluster
+    "piece_tiles": (32, 16, 8),
+}
+
+
+def autotune_plan(upload_fn: Callable[[dict], object], nrhs: int = 1, op: int = 0, knobs=("finish_slots",),
+                  keep_default_within: float = 0.02, timer_for: Optional[Callable] = None, sweeps: int = 2):
+    """Plan-level choices, timed by uploading the matrix once per candidate.
+
+    ``upload_fn(plan)`` uploads the matrix with hlrc_options plan choices
+    ``plan`` (e.g. ``lambda p: upload(hm, precision="f16", max_nrhs=64,
+    plan=p)``); each knob in ``knobs`` is tried over PLAN_CANDIDATES (the
+    first value is the default), one knob at a time, the others at their
+    current choice, and products are timed with CUDA events as in
+    ``autotune``.  The default is kept unless another value is faster by more
+    than ``keep_default_within``.  Returns (handle of the chosen plan,
+    {"plan": choice, "times_ms": [(plan, ms), ...]}); the other handles are
+    freed.  ``timer_for(M)`` (tests) replaces the event timer."""
+    choice, times = {}, []
+    best_M = None
+    for knob in knobs:
+        cands = []
+        for v in PLAN_CANDIDATES[knob]:
+            plan = dict(choice, **{knob: v})
+            M = upload_fn(plan)
+            timer = timer_for(M) if timer_for is not None else event_timer(M, nrhs, op)
+            cands.append([plan, M, timer, float("inf")])
+        for _ in range(sweeps):
+            for c in cands:
+                c[3] = min(c[3], float(c[2]()))
+        times += [(dict(c[0]), c[3]) for c in cands]
+        best = min(cands, key=lambda c: c[3])
+        if cands[0][3] <= best[3] * (1.0 + keep_default_within):
+            best = cands[0]
+        choice = dict(best[0])
+        for c in cands:
+            if c is not best:
+                c[1].free()
+        if best_M is not None and best_M is not best[1]:
+            best_M.free()
+        best_M = best[1]
+    return best_M, {"plan": choice, "times_ms": times}

@@ -187,7 +187,14 @@ typedef struct hlrc_options {
     int32_t max_nrhs;      /* workspace sized for this many right-hand sides   */
     double  mixed_eps;     /* HLRC_PREC_MIXED: target accuracy (e.g. 1e-6)      */
     int32_t device;        /* CUDA device ordinal (-1 = current)                */
-    int32_t reserved[7];
+    /* plan-level choices (0 = default), picked by hlr_b200.tune.autotune_plan:
+     * finish_slots: outputs of the tile T-form with more tile partials than
+     *   this are summed in two levels (2..64, default 16);
+     * piece_tiles: column clusters of the 64-vector T-form longer than this
+     *   many tiles are cut into pieces summed by a finish (1..32, default 32) */
+    int32_t finish_slots;
+    int32_t piece_tiles;
+    int32_t reserved[5];
 } hlrc_options;
 
 /* accounting of one product, following HLR's mul_vec_flops /

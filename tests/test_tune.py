@@ -128,3 +128,41 @@ def test_wide_candidates_above_eight_vectors():
     t, calls = timer_for(M, lambda s: 3.0 if s["wide_min_nrhs"] == HLRC_MR_NEVER and s["mr_min_nrhs"] == 2 else 6.0)
     r = tune.autotune(M, nrhs=64, cache=None, timer=t, device_name="G")
     assert r["tuning"]["wide_min_nrhs"] == HLRC_MR_NEVER and r["tuning"]["mr_min_nrhs"] == 2 and len(calls) == 6
+
+
+class FakePlanned:
+    """An uploaded handle whose speed depends on its plan choices."""
+    def __init__(self, plan):
+        self.plan = dict(plan)
+        self.freed = False
+
+    def free(self):
+        self.freed = True
+
+
+def test_autotune_plan_times_each_knob_and_frees_the_losers():
+    made = []
+
+    def upload_fn(plan):
+        M = FakePlanned(plan)
+        made.append(M)
+        return M
+
+    def ms(M):
+        p = M.plan
+        return 1.0 + (0.0 if p.get("finish_slots") == 8 else 0.5) + (0.0 if p.get("piece_tiles", 32) == 16 else 0.25)
+
+    M, out = tune.autotune_plan(upload_fn, nrhs=64, knobs=("finish_slots", "piece_tiles"),
+                                timer_for=lambda M: (lambda: ms(M)))
+    assert out["plan"] == {"finish_slots": 8, "piece_tiles": 16}
+    assert M.plan == out["plan"] and not M.freed
+    assert all(m.freed for m in made if m is not M)
+    assert len(out["times_ms"]) == 6
+
+
+def test_autotune_plan_keeps_default_within_noise():
+    def upload_fn(plan):
+        return FakePlanned(plan)
+    M, out = tune.autotune_plan(upload_fn, knobs=("finish_slots",),
+                                timer_for=lambda M: (lambda: 1.0 if M.plan["finish_slots"] == 16 else 0.995))
+    assert out["plan"] == {"finish_slots": 16}
