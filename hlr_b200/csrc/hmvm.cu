@@ -544,6 +544,37 @@ void wide_tma_split(const StreamTables& tab, int f, const std::vector<WCol>& wco
     }
 }
 
+// The stream tables of a reduced-precision plan built on the host only (the
+// dry run of upload_streams behind hlrc_plan_info_*): fails where an upload
+// of the plan would.
+hlrc_status check_streams(const Plan& p) {
+    if (p.precision == HLRC_PREC_F64) return HLRC_OK;
+    const int wide_pass = !p.wide.empty() && p.stages[HLRC_OP_N].size() == 2 ? p.stages[HLRC_OP_N][1].idx : -1;
+    const bool bf16 = p.precision == HLRC_PREC_BF16;
+    for (size_t i = 0; i < p.npasses.size(); ++i) {
+        StreamTables t;
+        const hlrc_status st = build_streams(p.npasses[i].segs, p.npasses[i].chunks, false,
+                                             [](const NSeg& s) { return s.out; }, t);
+        if (st != HLRC_OK) return st;
+        if (int(i) == wide_pass) {
+            const int f = bf16 ? FMT_BF16 : FMT_F16;
+            std::vector<WCol> wcol;
+            std::vector<WSeg> wsegs;
+            std::vector<WStage> wstages;
+            std::vector<MSeg> wrest;
+            wide_columns(t, f, p.wide.t_exp, bf16, wcol);
+            wide_tma_split(t, f, wcol, bf16, wsegs, wstages, wrest);
+        }
+    }
+    for (size_t i = 0; i < p.ttpasses.size(); ++i) {
+        StreamTables t;
+        const hlrc_status st = build_streams(p.ttpasses[i].segs, p.ttpasses[i].chunks, true,
+                                             [](const TTSeg& s) { return s.v_off; }, t);
+        if (st != HLRC_OK) return st;
+    }
+    return HLRC_OK;
+}
+
 // Builds and uploads the column streams of every N-form and tile T-form pass
 // (and, for plans with a 64-vector product, that N-form's column table).
 hlrc_status upload_streams(const Plan& p, hlrc_hmat_s* h) {
@@ -1588,6 +1619,7 @@ extern "C" hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_opti
     Plan p;
     hlrc_status st = plan_h(*desc, o, p);
     if (st != HLRC_OK) return st;
+    if (st = check_streams(p); st != HLRC_OK) return st;
     fill_info(p, arena_layout(p), *info);
     return HLRC_OK;
 }
@@ -1612,6 +1644,7 @@ extern "C" hlrc_status hlrc_plan_info_h2(const hlrc_h2_desc* desc, const hlrc_op
     Plan p;
     hlrc_status st = plan_h2(*desc, o, p);
     if (st != HLRC_OK) return st;
+    if (st = check_streams(p); st != HLRC_OK) return st;
     fill_info(p, arena_layout(p), *info);
     return HLRC_OK;
 }
@@ -1625,6 +1658,7 @@ extern "C" hlrc_status hlrc_plan_info_uniform(const hlrc_uniform_desc* desc, con
     Plan p;
     hlrc_status st = plan_uniform(*desc, o, p);
     if (st != HLRC_OK) return st;
+    if (st = check_streams(p); st != HLRC_OK) return st;
     fill_info(p, arena_layout(p), *info);
     return HLRC_OK;
 }

@@ -183,17 +183,21 @@ struct Store {
     }
 
     // Places the chunks allocated since the last call: by layout_rank, then
-    // in allocation order, each on a 16-byte boundary.
+    // in allocation order, each on a 16-byte boundary.  With align128 the
+    // region's first 16-bit chunk starts on a 128-byte boundary; the chunks
+    // after it follow without a gap, since a pass segment may span the
+    // factor and dense groups and must stay one contiguous column run.
     void close_region() {
+        bool first16 = true;
         for (int r = 0; r < 2 * NFMT; ++r) {
-            bool first = true;
             for (size_t c = region_begin; c < chunks.size(); ++c) {
                 SChunk& ch = chunks[c];
                 if (layout_rank(group[c], ch.fmt) != r) continue;
                 ch.byte_off = align16(bytes);
-                if (first && align128 && (ch.fmt == FMT_F16 || ch.fmt == FMT_BF16))
+                if (first16 && align128 && (ch.fmt == FMT_F16 || ch.fmt == FMT_BF16)) {
                     ch.byte_off = (ch.byte_off + 127) / 128 * 128;
-                first = false;
+                    first16 = false;
+                }
                 bytes = ch.byte_off + pad_fmt(crows[c], ch.fmt) * ch.nc * fmt_bytes(ch.fmt);
             }
         }

@@ -69,3 +69,16 @@ def test_fp16_conversion_is_round_to_nearest_even():
     ll.add_dense(0, 0, np.array([[1.0, -2.5], [0.125, 1024.0]]))
     info = hlr.plan_info(ll, precision="f16")
     assert info["matrix_bytes"] == 2 * 4 + 4
+
+
+@pytest.mark.parametrize("prec", ["f16", "bf16", "f32", "mixed", "bfp"])
+@pytest.mark.parametrize("n,leaf", [(5000, 48), (8200, 64)])
+def test_reduced_plans_form_column_streams(prec, n, leaf):
+    # plan_info builds the column-stream tables of the multi-vector and
+    # 64-vector kernels on the host (every pass segment of one format must be
+    # one contiguous run of columns in the store), so a layout that an upload
+    # would reject fails here without a GPU
+    from conftest import built
+    hm = built(f"exp3d_{n}_{leaf}", lambda: hlr.build(hlr.Problem.exp3d(n, leaf_size=leaf)))
+    info = hlr.plan_info(hm, precision=prec, max_nrhs=64)
+    assert info["matrix_bytes"] > 0
