@@ -71,6 +71,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp64_roof(hlr, flops: float, alg_bytes: float, ms_per_product: float, hbm_peak: float, device: int) -> dict:
+    """The roof of an FP64 multi-vector product: min(HBM bandwidth x
+    intensity, FP64 tensor peak), the peak measured here by a DMMA loop of
+    the library (hlrc_fp64_peak).  frac = achieved flop rate / that roof."""
+    peak = hlr.fp64_peak(device)
+    intensity = flops / alg_bytes
+    roof = min(hbm_peak * 1e9 * intensity, peak * 1e12) / 1e12
+    achieved = flops / (ms_per_product / 1e3) / 1e12
+    return {"fp64_tflops_measured": peak, "flops_per_product": flops, "intensity_flop_per_byte": intensity,
+            "roof_tflops": roof, "bound": "hbm" if roof < peak else "fp64", "achieved_tflops": achieved,
+            "frac": achieved / roof}
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """The job's time: the largest of the ranks' times.  Every rank calls it
     at the same point (one all-reduce); with one rank it returns ms."""
@@ -554,6 +567,8 @@ def run_ours(args, rank, world, local_rank):
                              "ms_per_product_of_runs": runs} if per_graph else None},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "roofline": roof,
+        "compute_roof": fp64_roof(hlr, info["flops"] * nrhs, alg, ms_max / args.steps, hbm_peak, local_rank)
+        if prec == "f64" and nrhs > 1 else None,
         "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
                    for k, v in prof.items()},
         "gpu_launches": timed_launches,

@@ -479,7 +479,15 @@ class uniform:  # namespace mirroring hlr::tbb::uniform
         mul_vec(alpha, op, M, x, y, stream)
 
 
+def fp64_peak(device: int = 0) -> float:
+    """Measured FP64 tensor-core throughput of ``device`` in TFLOP/s
+    (hlrc_fp64_peak: a timed DMMA loop; no clock or other setting changes)."""
+    t = C.c_double(0.0)
+    check(lib().hlrc_fp64_peak(int(device), C.byref(t)), "hlrc_fp64_peak")
+    return float(t.value)
+
+
 __all__ = [
     "apply_normal", "apply_transposed", "apply_adjoint", "Problem", "HostMatrix", "LeafList", "DeviceMatrix",
-    "build", "upload", "mul_vec", "mvm", "uniform", "h2", "HLRCError", "PRECISIONS", "Workspace",
+    "build", "upload", "mul_vec", "mvm", "uniform", "h2", "HLRCError", "PRECISIONS", "Workspace", "fp64_peak",
 ]

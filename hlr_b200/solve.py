@@ -93,9 +93,24 @@ def diagonal_blocks(src, block: int = 256):
     return list(zip(starts, out))
 
 
+def _zero_offdiagonal(W: LeafList, lo: int, hi: int, block: int) -> None:
+    """Rank-0 leaves for the off-diagonal part of [lo, hi)^2, split in halves
+    at multiples of `block` down to single diagonal blocks (about two leaves
+    per diagonal block), so that the leaves of W cover the whole matrix."""
+    nb = (hi - lo + block - 1) // block
+    if nb <= 1:
+        return
+    mid = lo + (nb // 2) * block
+    W.add_lowrank(lo, mid, np.zeros((mid - lo, 0)), np.zeros((hi - mid, 0)))
+    W.add_lowrank(mid, lo, np.zeros((hi - mid, 0)), np.zeros((mid - lo, 0)))
+    _zero_offdiagonal(W, lo, mid, block)
+    _zero_offdiagonal(W, mid, hi, block)
+
+
 def block_jacobi_leaves(src, block: int = 256) -> LeafList:
-    """W = diag(A_kk^-1) as a leaf list of dense blocks (A_kk symmetric
-    positive definite: inverted through its Cholesky factor)."""
+    """W = diag(A_kk^-1) as a leaf list: dense inverses of the diagonal
+    blocks (A_kk symmetric positive definite: inverted through its Cholesky
+    factor) and rank-0 leaves elsewhere."""
     d = src.h_desc() if hasattr(src, "h_desc") else src
     n = int(d.nrows)
     W = LeafList(n, n)
@@ -103,6 +118,7 @@ def block_jacobi_leaves(src, block: int = 256) -> LeafList:
         L = np.linalg.cholesky(0.5 * (Akk + Akk.T))
         Li = np.linalg.solve(L, np.eye(L.shape[0]))
         W.add_dense(i0, i0, Li.T @ Li)
+    _zero_offdiagonal(W, 0, n, block)
     return W
 
 

@@ -42,9 +42,18 @@ def test_block_jacobi_leaves_are_inverses():
     ll, A = _random_h(12, seed=3)
     W = block_jacobi_leaves(ll, 4)
     d = W.h_desc()
-    assert d.nblocks == 3
-    for k in range(3):
-        b = d.blocks[k]
+    dense = [d.blocks[k] for k in range(d.nblocks) if d.blocks[k].kind == hlr.LEAF_DENSE]
+    assert len(dense) == 3
+    for b in dense:
         Wk = np.ctypeslib.as_array(b.D, shape=(b.ldd * b.ncols,)).reshape(b.ncols, b.ldd).T[:b.nrows]
         i0 = int(b.row0)
         assert np.allclose(Wk @ A[i0:i0 + 4, i0:i0 + 4], np.eye(4), atol=1e-10)
+    # the other leaves have rank 0 and, with the dense ones, cover the matrix
+    # exactly once (the planner rejects gaps and overlaps)
+    cover = np.zeros((12, 12), dtype=int)
+    for k in range(d.nblocks):
+        b = d.blocks[k]
+        assert b.kind == hlr.LEAF_DENSE or b.rank == 0
+        cover[b.row0:b.row0 + b.nrows, b.col0:b.col0 + b.ncols] += 1
+    assert (cover == 1).all()
+    assert hlr.plan_info(W)["matrix_bytes"] == 3 * 16 * 8
