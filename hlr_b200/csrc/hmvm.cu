@@ -24,6 +24,7 @@
 
 #include "common.hpp"
 #include "hlrc.h"
+#include "kernels_bfp8.cuh"
 #include "kernels_f64.cuh"
 #include "kernels_mr.cuh"
 #include "kernels_q.cuh"
@@ -676,13 +677,16 @@ hlrc_status enable_tc_smem(int dev) {
                                    tc_smem_bytes(TC_STAGE_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_bfp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_n(true)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_nform_bfp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_n(false)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_bfp, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_t()));
     done.push_back(dev);
     return HLRC_OK;
 }
 
-// Does the handle have 8-vector kernels?  Block floating point stores loop
-// the one-vector kernels instead.
-bool has_multi_kernels(hlrc_hmat M) { return M->precision != HLRC_PREC_BFP; }
+// Does the handle have 8-vector kernels?  Every store format has them (FP64
+// on DMMA, FP32 columns on DMMA, 16-bit and BFP columns on FP16 MMA).
+bool has_multi_kernels(hlrc_hmat) { return true; }
 
 // Sizes of the multi-vector scratch of a handle: x, t, t2 and the partial
 // sums as row-major blocks of MR_RB vectors, each array 256-byte aligned.
@@ -1323,14 +1327,7 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
         k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, ws.mr_x);
         M->launches += 1;
         HLRC_AFTER_LAUNCH("rows_from_cols");
-        for (const Stage& st : mr_stages(M, op)) {
-            if (st.kind == 2) {
-                const DevTTPass& tp = M->tt[size_t(st.idx)];
-                M->launches += M->tt[size_t(st.idx)].launches();
-            } else if (st.kind == 1) {
-                M->launches += M->n[size_t(st.idx)].launches();
-            }
-        }
+        int nl = 0;   // kernels launched below, counted at their launch sites
         auto vec = [&](int name) -> double* {
             return name == V_X ? ws.mr_x : (name == V_T ? ws.mr_t : ws.mr_t2);
         };
@@ -1348,19 +1345,32 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                 if (ws.profile) prof_begin(M, stage_name(M, 2, st.idx), tp.alg_bytes, s);
                 constexpr int TW = DMMA_WARPS;
                 if (M->precision == HLRC_PREC_F64) {
-                    if (tp.nsegs[FMT_F64] > 0)
+                    if (tp.nsegs[FMT_F64] > 0) {
                         k_ttform_dmma<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
                             tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks), A, vec(tp.in), om, ws.mr_part,
                             alpha, add);
+                        ++nl;
+                    }
+                } else if (M->precision == HLRC_PREC_BFP) {
+                    const int n24 = tp.nmseg[FMT_I24];
+                    if (n24 + tp.nmseg[FMT_I16] > 0) {
+                        k_ttform_bfp<<<n24 + tp.nmseg[FMT_I16], TC_WARPS * 32, bq_smem_t(), s>>>(
+                            tp.mseg[FMT_I24], n24, tp.mseg[FMT_I16], tp.mcol, M->store, vec(tp.in), om,
+                            reinterpret_cast<float*>(ws.mr_part), alpha, add);
+                        ++nl;
+                    }
                 } else {
                     const int n32 = tp.nmseg[FMT_F32];
                     float* fpart = reinterpret_cast<float*>(ws.mr_part);
-                    if (tp.nmseg[FMT_BF16] > 0)
+                    if (tp.nmseg[FMT_BF16] > 0) {
                         k_ttform_mr<FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
-                    else if (n32 + tp.nmseg[FMT_F16] > 0)
+                        ++nl;
+                    } else if (n32 + tp.nmseg[FMT_F16] > 0) {
                         k_ttform_mr<FMT_F16><<<n32 + tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
+                        ++nl;
+                    }
                 }
                 if (ws.profile) prof_end(M, s);
                 if (tp.ngroups > 0) {
@@ -1382,6 +1392,7 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                         k_ttfinish_f32_mr<false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, fpart, om,
                                                                                      nullptr, alpha, add);
                     }
+                    nl += 1 + (tp.ngroups1 > 0 ? 1 : 0);
                     if (ws.profile) prof_end(M, s);
                 }
                 HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
@@ -1395,23 +1406,44 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                 const OutMap om = omap(np.out);
                 constexpr int NW = DMMA_WARPS;
                 const bool f64plan = M->precision == HLRC_PREC_F64;
-                if (f64plan && np.nsegs[FMT_F64] > 0)
+                // the formats of one output tile run as separate grids, each
+                // adding its share to the output in a fixed launch order
+                if (f64plan && np.nsegs[FMT_F64] > 0) {
                     k_nform_dmma<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
                         np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), A, vec(np.vx), vec(np.vt), om, alpha,
                         add);
-                if (!f64plan && np.nmseg[FMT_F32] > 0)
+                    ++nl;
+                }
+                if (!f64plan && np.nmseg[FMT_F32] > 0) {
                     k_nform_d32<<<np.nmseg[FMT_F32], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32), s>>>(
                         np.mseg[FMT_F32], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
-                if (!f64plan && np.nmseg[FMT_F16] > 0)
+                    ++nl;
+                }
+                if (!f64plan && np.nmseg[FMT_F16] > 0) {
                     k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.mseg[FMT_F16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
-                if (!f64plan && np.nmseg[FMT_BF16] > 0)
+                    ++nl;
+                }
+                if (!f64plan && np.nmseg[FMT_BF16] > 0) {
                     k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
                         np.mseg[FMT_BF16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                    ++nl;
+                }
+                if (!f64plan && np.nmseg[FMT_I24] > 0) {
+                    k_nform_bfp<true><<<np.nmseg[FMT_I24], TC_WARPS * 32, bq_smem_n(true), s>>>(
+                        np.mseg[FMT_I24], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                    ++nl;
+                }
+                if (!f64plan && np.nmseg[FMT_I16] > 0) {
+                    k_nform_bfp<false><<<np.nmseg[FMT_I16], TC_WARPS * 32, bq_smem_n(false), s>>>(
+                        np.mseg[FMT_I16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
+                    ++nl;
+                }
                 if (ws.profile) prof_end(M, s);
                 HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
             }
         }
+        M->launches += nl;
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));

@@ -18,7 +18,8 @@
 // of both operands; matrix rows past the run's columns (the next run's
 // data) are zeroed by the MMA warp before its MMAs.  All of a tile's columns
 // have factor 1 (the store's row-group scales), so the staged data is used
-// as it lands.
+// as it lands, and the whole run accumulates in one FP32 TMEM accumulator
+// (FP32 accumulation per output tile, FP64 y), drained once.
 //
 // Column-cluster T-form (k_ctform_wtma): persistent CTAs, each taking every
 // (gridDim)-th unit; a stage is one tile of a unit: its split rows of x
@@ -36,14 +37,11 @@
 namespace hlrc {
 
 constexpr int WTMA_THREADS = 192;     // 4 epilogue warps, MMA warp, producer warp
-constexpr int WTMA_NS_N = 6;          // N-form stages
+constexpr int WTMA_NS_N = 8;          // N-form stages (12 KB each)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
-constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per transpose round
-constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES + 64 + WIDE_BAR_BYTES; }
-constexpr int wtma_smem_c() {
-    return 1024 + WTMA_NS_C * WIDE_C_STAGE + WTMA_RED_COLS * WIDE_TERMS * 4 + WT_MAXN * 4 + WT_MAXB * 16 +
-           WIDE_BAR_BYTES;
-}
+constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
+constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
+constexpr int wtma_smem_c() { return 1024 + WTMA_NS_C * WIDE_C_STAGE + WT_MAXN * 4 + WT_MAXB * 16 + WIDE_BAR_BYTES; }
 
 // 16 consecutive FP32 columns of the warp's 32 lanes (as tmem_ld32)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
@@ -59,6 +57,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// AND of p over the 128 epilogue threads, which all arrive (named barrier 1)
+__device__ __forceinline__ bool bar_and_128(bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\tbar.red.and.pred po, 1, 128, pi;\n\t"
+        "selp.u32 %0, 1, 0, po;\n\t}\n"
+        : "=r"(r)
+        : "r"(uint32_t(p))
+        : "memory");
+    return r != 0;
+}
+
 // ----------------------------------------------------------------- N-form
 template <int FMT>
 __global__ void __launch_bounds__(WTMA_THREADS, 2)
@@ -69,34 +79,27 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    double* acc = reinterpret_cast<double*>(sm + WTMA_NS_N * WIDE_N_STAGE);   // [r][row], ld WIDE_ACC_LD
-    int* snc = reinterpret_cast<int*>(sm + WTMA_NS_N * WIDE_N_STAGE + WIDE_ACC_BYTES);   // columns per slot
+    int* snc = reinterpret_cast<int*>(sm + WTMA_NS_N * WIDE_N_STAGE);   // columns per slot
     uint64_t* full = reinterpret_cast<uint64_t*>(snc + 16);
     uint64_t* empty = full + WTMA_NS_N;
     uint64_t* tfull = empty + WTMA_NS_N;
-    uint64_t* tempty = tfull + 2;
-    uint64_t* done = tempty + 2;
+    uint64_t* done = tfull + 1;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
 
     const WSeg sg = segs[blockIdx.x];
     const int nst = int(sg.nst);
-    const int ngrp = (nst + WIDE_FLUSH - 1) / WIDE_FLUSH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (nst == 0) return;
-    for (int i = threadIdx.x; i < WIDE_RHS * WIDE_ACC_LD; i += WTMA_THREADS) acc[i] = 0.0;
     if (threadIdx.x == 0) {
         for (int i = 0; i < WTMA_NS_N; ++i) {
             mbar_init(full + i, 1);
             mbar_init(empty + i, 1);
         }
-        for (int i = 0; i < 2; ++i) {
-            mbar_init(tfull + i, 1);
-            mbar_init(tempty + i, 128);
-        }
+        mbar_init(tfull, 1);
         mbar_init(done, 1);
         mbar_init_fence();
     }
-    if (warp == 4) tmem_alloc(tslot, 128);
+    if (warp == 4) tmem_alloc(tslot, 64);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -150,13 +153,9 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
         constexpr uint32_t ID16 = tc5::idesc_f16(128, 64, WideT<FMT>::bf16, true, true);
         bool ok = true;
         for (int s = 0; s < nst && ok; ++s) {
-            const int slot = s % WTMA_NS_N, q = s / WIDE_FLUSH, buf = q & 1;
-            const bool first = s % WIDE_FLUSH == 0, last = s % WIDE_FLUSH == WIDE_FLUSH - 1 || s == nst - 1;
+            const int slot = s % WTMA_NS_N;
             bool w = true;
-            if (lane == 0) {
-                if (first && q >= 2) w = wide_wait(tempty + buf, uint32_t((q >> 1) - 1) & 1u, err, wc.limit_ns);
-                if (w) w = wide_wait(full + slot, uint32_t(s / WTMA_NS_N) & 1u, err, wc.limit_ns);
-            }
+            if (lane == 0) w = wide_wait(full + slot, uint32_t(s / WTMA_NS_N) & 1u, err, wc.limit_ns);
             ok = __shfl_sync(0xffffffffu, w, 0);
             if (!ok) break;
             __syncwarp();   // lane 0's wait orders the producer's snc write before these reads
@@ -174,12 +173,11 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
             if (lane == 0) {
                 tc_fence_after();
                 const uint32_t sa = s0 + uint32_t(slot) * WIDE_N_STAGE, sb = sa + 8192u;
-                const uint32_t d = tmem + uint32_t(buf) * 64u;
                 for (int j = 0; j < R / 16; ++j)
-                    mma_f16(d, sdesc(sa + 2048u * j, 4096u, 1024u), sdesc(sb + 2048u * j, 4096u, 1024u), ID16,
-                            (!first || j > 0) ? 1u : 0u);
+                    mma_f16(tmem, sdesc(sa + 2048u * j, 4096u, 1024u), sdesc(sb + 2048u * j, 4096u, 1024u), ID16,
+                            (s > 0 || j > 0) ? 1u : 0u);
                 mma_commit(empty + slot);
-                if (last) mma_commit(tfull + buf);
+                if (s == nst - 1) mma_commit(tfull);
             }
             __syncwarp();
         }
@@ -190,37 +188,29 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
         __syncwarp();
     } else {
         // -------------------------------------------------------- epilogue
+        // lane m holds term m (vector m / 2, high or low part) of the 64
+        // rows; the two lanes of a vector exchange halves: the high-part
+        // lane sums rows 0-31, the low-part lane rows 32-63
         const uint32_t la = tmem + (uint32_t(32 * warp) << 16);
-        const int m = 32 * warp + lane;
-        double* arow = acc + (m >> 1) * WIDE_ACC_LD;
-        bool ok = true;
-        for (int q = 0; q < ngrp; ++q) {
-            const int buf = q & 1;
-            ok = __all_sync(0xffffffffu, wide_wait(tfull + buf, uint32_t(q >> 1) & 1u, err, wc.limit_ns));
-            if (!ok) break;
-            tc_fence_after();
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float f[32];
-                tmem_ld32(la + uint32_t(buf) * 64u + uint32_t(32 * h), f);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const float o = __shfl_xor_sync(0xffffffffu, f[i], 1);
-                    if ((lane & 1) == 0) arow[32 * h + i] += double(f[i]) + double(o);
-                }
-            }
-            tc_fence_before();
-            mbar_arrive(tempty + buf);
-        }
-        asm volatile("bar.sync 1, 128;\n" ::: "memory");
-        ok = __all_sync(0xffffffffu, ok) && !wide_aborted(err);
+        const int m = 32 * warp + lane, r = m >> 1;
+        const bool lo = (m & 1) != 0;
+        const bool ok = __all_sync(0xffffffffu, wide_wait(tfull, 0u, err, wc.limit_ns)) && !wide_aborted(err);
         if (ok) {
-            for (int q = threadIdx.x; q < WIDE_RHS * TILE; q += 128) {
-                const int r = q / TILE, row = q % TILE;
-                if (r >= om.nr) continue;
-                const double val = ldexp(acc[r * WIDE_ACC_LD + row], sg.E - g[r]);
-                double* o = om.base + int64_t(sg.out + row) * om.rs + int64_t(r) * om.cs;
-                *o += alpha * val;
+            tc_fence_after();
+            float a[32], b[32];
+            tmem_ld32(la, a);
+            tmem_ld32(la + 32u, b);
+            double v[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const float other = __shfl_xor_sync(0xffffffffu, lo ? a[i] : b[i], 1);
+                v[i] = double(lo ? b[i] : a[i]) + double(other);
+            }
+            if (r < om.nr) {
+                const double f = alpha * ldexp(1.0, sg.E - g[r]);
+                double* o = om.base + int64_t(sg.out + (lo ? 32 : 0)) * om.rs + int64_t(r) * om.cs;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) o[int64_t(i) * om.rs] += f * v[i];
             }
         }
     }
@@ -228,7 +218,7 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
     __syncthreads();
     if (warp == 4) {
         tc_fence_after();
-        tmem_dealloc(tmem, 128);
+        tmem_dealloc(tmem, 64);
     }
 }
 
@@ -244,8 +234,7 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    float* red = reinterpret_cast<float*>(sm + WTMA_NS_C * WIDE_C_STAGE);       // [16 columns][128 terms]
-    uint32_t* scol = reinterpret_cast<uint32_t*>(red + WTMA_RED_COLS * WIDE_TERMS);
+    uint32_t* scol = reinterpret_cast<uint32_t*>(sm + WTMA_NS_C * WIDE_C_STAGE);
     WTBlk* sblk = reinterpret_cast<WTBlk*>(scol + WT_MAXN);
     uint64_t* full = reinterpret_cast<uint64_t*>(sblk + WT_MAXB);
     uint64_t* empty = full + WTMA_NS_C;
@@ -358,7 +347,9 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
         int i = 0;
         for (int ui = int(blockIdx.x); ui < nunits; ui += int(gridDim.x), ++i) {
             const int buf = i & 1;
-            if (!__all_sync(0xffffffffu, wide_wait(tfull + buf, uint32_t(i >> 1) & 1u, err, wc.limit_ns))) break;
+            // all four warps take the same branch (the named barriers below
+            // need every one of them)
+            if (!bar_and_128(wide_wait(tfull + buf, uint32_t(i >> 1) & 1u, err, wc.limit_ns))) break;
             tc_fence_after();
             const WTUnit u = units[ui];
             const int nc = int(u.ncols);
@@ -374,33 +365,36 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
                 scol[m] = cm;
             }
             asm volatile("bar.sync 1, 128;\n" ::: "memory");
+            // lane m holds term m (vector r = m / 2, high or low part) of 16
+            // columns per TMEM load; the two lanes of a vector exchange
+            // halves, the high-part lane sums the even columns, the low-part
+            // lane the odd ones, and each stores its columns' entries of
+            // vector r (t split rows, or FP32 partials of a piece)
             const uint32_t la = la0 + uint32_t(buf) * 128u;
+            const int r = m >> 1, odd = m & 1;
             for (int c0 = 0; c0 < nc; c0 += WTMA_RED_COLS) {
                 float f[16];
                 tmem_ld16(la + uint32_t(c0), f);
 #pragma unroll
-                for (int k = 0; k < 16; ++k) red[k * WIDE_TERMS + m] = f[k];
-                asm volatile("bar.sync 1, 128;\n" ::: "memory");
-#pragma unroll
-                for (int k4 = 0; k4 < 4; ++k4) {
-                    const int k = 4 * k4 + warp, n = c0 + k;
+                for (int i = 0; i < 8; ++i) {
+                    const float other = __shfl_xor_sync(0xffffffffu, odd ? f[2 * i] : f[2 * i + 1], 1);
+                    const int n = c0 + 2 * i + odd;
                     const uint32_t cm = n < nc ? scol[n] : WT_EMPTY;
                     if (cm == WT_EMPTY) continue;
                     const WTBlk& b = sblk[cm >> 16];
                     const int l = int(cm & 0xffffu);
-                    const float4 t4 = reinterpret_cast<const float4*>(red + k * WIDE_TERMS)[lane];
-                    const double sc = double(b.scale);
-                    const double v0 = (double(t4.x) + double(t4.y)) * sc, v1 = (double(t4.z) + double(t4.w)) * sc;
+                    const double v = (double(odd ? f[2 * i + 1] : f[2 * i]) + double(other)) * double(b.scale);
                     if (u.npieces == 1) {
                         const size_t e = size_t(b.toff) + size_t(l);
-                        wide_store_row<FMT>(v0, v1, int(texp[e]), ts + e * (WIDE_TERMS / 2), lane);
+                        ts[e * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -int(texp[e])));
                     } else {
                         const size_t e = size_t(b.pbase) + size_t(u.piece) * b.k + size_t(l);
-                        reinterpret_cast<float2*>(part)[e * 32 + lane] = make_float2(float(v0), float(v1));
+                        part[e * WIDE_RHS + r] = float(v);
                     }
                 }
-                asm volatile("bar.sync 1, 128;\n" ::: "memory");
             }
+            // the next unit's tables overwrite these only after every lane is done
+            asm volatile("bar.sync 1, 128;\n" ::: "memory");
             tc_fence_before();
             mbar_arrive(tempty + buf);
         }

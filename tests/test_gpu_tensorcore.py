@@ -1,6 +1,7 @@
 """Multi-right-hand-side products of reduced-precision stores (16-bit chunks
-on tensor cores, FP32 chunks on CUDA cores) against the FP64 oracle and
-against the single-vector reduced-precision product of the same store.
+and block-floating-point byte planes on FP16 tensor cores, FP32 chunks on
+FP64 tensor cores) against the FP64 oracle and against the single-vector
+reduced-precision product of the same store.
 
 The tensor-core path splits each vector entry into two 16-bit terms, so it
 differs from the single-vector path (FP32 vector) only by about 2^-22
@@ -18,8 +19,8 @@ torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2}
-SAME_STORE = {"f32": 1e-6, "mixed": 2e-6, "f16": 2e-6, "bf16": 1e-4}
+TOL = {"f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp": 1e-6}
+SAME_STORE = {"f32": 1e-6, "mixed": 2e-6, "f16": 2e-6, "bf16": 1e-4, "bfp": 1e-6}
 
 
 def colmajor_dev(A):
@@ -34,7 +35,7 @@ def matrices():
 
 
 @pytest.mark.parametrize("name", ["exp3d_5000_48", "exp3d_16384_64"])
-@pytest.mark.parametrize("prec", ["mixed", "f16", "bf16", "f32"])
+@pytest.mark.parametrize("prec", ["mixed", "f16", "bf16", "f32", "bfp"])
 @pytest.mark.parametrize("op", [0, 1])
 def test_multi_rhs_reduced_precision(name, prec, op):
     hm = matrices()[name]
@@ -43,8 +44,12 @@ def test_multi_rhs_reduced_precision(name, prec, op):
     rng = np.random.default_rng(90 + op)
     X = rng.standard_normal((hm.n, nrhs))
     Yd = colmajor_dev(np.zeros((hm.n, nrhs)))
+    l0 = M.launch_count()
     hlr.mul_vec(1.0, op, M, colmajor_dev(X), Yd)
     torch.cuda.synchronize()
+    # two blocks of 8 vectors, each a handful of grids (a loop of one-vector
+    # products would take 11 times the one-vector launches)
+    assert M.launch_count() - l0 <= 2 * 7
     Y = Yd.cpu().numpy()
     for j in (0, 5, 8, 10):
         yref = np.zeros(hm.n)
@@ -58,7 +63,7 @@ def test_multi_rhs_reduced_precision(name, prec, op):
     M.free()
 
 
-@pytest.mark.parametrize("prec", ["mixed", "f16", "bf16"])
+@pytest.mark.parametrize("prec", ["mixed", "f16", "bf16", "bfp"])
 def test_each_rhs_is_scaled_on_its_own(prec):
     """Right-hand sides of very different magnitude in one block: each one
     keeps its own relative accuracy (per-vector power-of-two scales on the
@@ -99,7 +104,7 @@ def test_multi_rhs_exactly_representable_known_answer():
     A = np.zeros((n, n))
     A[:h, :h], A[:h, h:], A[h:, :h], A[h:, h:] = D0, U @ V.T, U2 @ V2.T, D1
     X = rng.integers(-3, 4, (n, 8)).astype(float)
-    for prec in ("f16", "bf16", "mixed", "f32"):
+    for prec in ("f16", "bf16", "mixed", "f32", "bfp"):
         M = hlr.upload(ll, precision=prec, max_nrhs=8)
         for op, Aop in ((0, A), (1, A.T)):
             Yd = colmajor_dev(np.zeros((n, 8)))

@@ -4,9 +4,11 @@ the tcgen05 tensor cores (kernels_wide.cuh): the matrix is streamed once per
 (include/hlr/matrix/lrmatrix.hh:681-746) over all leaves at once.
 
 Checked against the FP64 oracle (to the store's own accuracy), against the
-8-vector tensor-core kernels and the one-vector kernels on the same store
-(the vector split keeps about 22 bits (FP16) or 16 bits (BF16), so the paths
-agree to 2e-6 / 1e-4; a layout mistake shows as an O(1) difference)."""
+8-vector tensor-core kernels and the one-vector kernels on the same store:
+the vector split keeps about 22 bits (FP16) or 16 bits (BF16) and the
+full-tile N-form accumulates a whole output tile's run in FP32 (FP64 y), so
+the paths agree to 2e-5 / 1e-4, far inside the store's own error (2e-3 /
+1.5e-2); a layout mistake shows as an O(1) difference."""
 import numpy as np
 import pytest
 
@@ -21,7 +23,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 TOL = {"f16": 2e-3, "bf16": 1.5e-2}            # against the FP64 oracle
-SAME_STORE = {"f16": 2e-6, "bf16": 1e-4}       # against the other kernels on the same store
+SAME_STORE = {"f16": 2e-5, "bf16": 1e-4}       # against the other kernels on the same store
 
 
 def colmajor_dev(A):
