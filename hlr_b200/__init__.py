@@ -236,11 +236,12 @@ class DeviceMatrix:
     @property
     def tuning(self) -> dict:
         """Launch shapes of this handle's products (hlrc_get_tuning):
-        nform_warps, ttform_warps (4 or 8), mr_min_nrhs and wide_min_nrhs."""
+        nform_warps, ttform_warps (4 or 8), mr_min_nrhs, wide_min_nrhs and
+        overlap (programmatic dependent launch of the one-vector kernels)."""
         t = _capi.hlrc_tuning()
         check(lib().hlrc_get_tuning(self._h, C.byref(t)), "hlrc_get_tuning")
         return {"nform_warps": t.nform_warps, "ttform_warps": t.ttform_warps, "mr_min_nrhs": t.mr_min_nrhs,
-                "wide_min_nrhs": t.wide_min_nrhs}
+                "wide_min_nrhs": t.wide_min_nrhs, "overlap": t.overlap}
 
     def set_tuning(self, **kw) -> None:
         """Changes some launch shapes (hlrc_set_tuning); the others keep their
@@ -251,7 +252,7 @@ class DeviceMatrix:
             raise ValueError(f"unknown tuning keys {sorted(unknown)}")
         cur.update(kw)
         t = _capi.hlrc_tuning(int(cur["nform_warps"]), int(cur["ttform_warps"]), int(cur["mr_min_nrhs"]),
-                              int(cur["wide_min_nrhs"]))
+                              int(cur["wide_min_nrhs"]), int(cur["overlap"]))
         check(lib().hlrc_set_tuning(self._h, C.byref(t)), "hlrc_set_tuning")
 
     def launch_count(self) -> int:

@@ -200,6 +200,7 @@ struct hlrc_hmat_s {
     int ttform_warps = 8;     // warps per CTA, single-vector tile T-form
     int mr_min_nrhs = 2;      // fewest vectors that take the 8-vector kernels
     int wide_min_nrhs = MR_RB + 1;   // fewest vectors that take the 64-vector kernels (when the handle has them)
+    int overlap = 1;          // one-vector kernels launched with programmatic dependent launch
     // profiling
     bool profiling = false;
     std::vector<ProfileRec> prof;
@@ -1176,11 +1177,34 @@ bool capturing(cudaStream_t s) {
     } while (0)
 
 // one right-hand side: x, y are column vectors; scratch from `ws`
+// Launches k on stream s.  With `overlap` the launch carries the
+// programmatic-stream-serialization attribute: the kernel may be scheduled
+// while the preceding kernel of the stream still runs, and waits for it
+// inside (pdl_wait) before it touches the vectors.
+template <typename... P, typename... A>
+cudaError_t launch_k(bool overlap, void (*k)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                     A... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* x, double* y,
                        cudaStream_t s) {
     // FP64 plans carry 16-byte FP64 descriptors, reduced-precision plans
     // 32-byte packs: each kind of kernel only ever sees its own kind
     const bool f64plan = M->precision == HLRC_PREC_F64;
+    const bool ov = M->overlap != 0;
+    cudaError_t le = cudaSuccess;   // the first failed launch
+    auto L = [&](cudaError_t e) { if (le == cudaSuccess) le = e; };
     for (const Stage& st : M->stages[op]) {
         M->launches += st.kind == 0 ? M->t[size_t(st.idx)].launches()
                                     : (st.kind == 1 ? M->n[size_t(st.idx)].launches() : M->tt[size_t(st.idx)].launches());
@@ -1198,12 +1222,13 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
                 const int grid = (nu + 7) / 8;
                 static_assert(TCOLS == 8, "T-form units are launched with the 8-column kernel");
                 const double* A = reinterpret_cast<const double*>(M->store);  // unit T-form: FP64 plans only
-                if (c == 0) k_tform_f64<8><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
-                else if (c == 1) k_tform_f64<16><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
-                else k_tform_f64<32><<<grid, 256, 0, s>>>(u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add);
+                if (c == 0) L(launch_k(ov, k_tform_f64<8>, grid, 256, 0, s, u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add));
+                else if (c == 1) L(launch_k(ov, k_tform_f64<16>, grid, 256, 0, s, u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add));
+                else L(launch_k(ov, k_tform_f64<32>, grid, 256, 0, s, u, nu, tp.slabs, A, vin, vout, ws.part, alpha, add));
             }
             if (tp.ngroups > 0)
-                k_tfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+                L(launch_k(ov, k_tfinish_f64, unsigned((tp.ngroups + 7) / 8), 256, 0, s, tp.groups, tp.ngroups,
+                           static_cast<const double*>(ws.part), vout, alpha, add));
             if (ws.profile) prof_end(M, s);
             HLRC_AFTER_LAUNCH(stage_name(M, 0, st.idx));
         } else if (st.kind == 2) {
@@ -1217,27 +1242,27 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             auto ttform = [&](auto wc) {
                 constexpr int TW = decltype(wc)::value;
                 if (f64plan && tp.nsegs[FMT_F64] > 0)
-                    k_ttform_f64<TW><<<tp.nsegs[FMT_F64], TW * 32, 0, s>>>(
-                        tp.segs[FMT_F64], static_cast<const TTChunk*>(tp.chunks),
-                        reinterpret_cast<const double*>(M->store), vin, vout, ws.part, alpha, add);
+                    L(launch_k(ov, k_ttform_f64<TW>, unsigned(tp.nsegs[FMT_F64]), TW * 32, 0, s, tp.segs[FMT_F64],
+                               static_cast<const TTChunk*>(tp.chunks), reinterpret_cast<const double*>(M->store), vin,
+                               vout, ws.part, alpha, add));
                 // reduced precision: each tile's run of columns, streamed in full
                 // 4 KB iterations; FP32 and 16-bit runs in one grid
                 if (!f64plan) {
                     if (tp.nmseg[FMT_I24] + tp.nmseg[FMT_I16] > 0) {   // block floating point
                         const int n24 = tp.nmseg[FMT_I24];
-                        k_ttform_qs<TW, FMT_I24, FMT_I16><<<n24 + tp.nmseg[FMT_I16], TW * 32, 0, s>>>(
-                            tp.mseg[FMT_I24], n24, tp.mseg[FMT_I16], tp.mcol, M->store, vin, vout, ws.part, alpha,
-                            add);
+                        L(launch_k(ov, k_ttform_qs<TW, FMT_I24, FMT_I16>, unsigned(n24 + tp.nmseg[FMT_I16]), TW * 32, 0,
+                                   s, tp.mseg[FMT_I24], n24, tp.mseg[FMT_I16], tp.mcol, M->store, vin, vout, ws.part,
+                                   alpha, add));
                     } else {
                         const int n32 = tp.nmseg[FMT_F32];
                         if (tp.nmseg[FMT_BF16] > 0)
-                            k_ttform_qs<TW, FMT_F32, FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TW * 32, 0, s>>>(
-                                tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin, vout, ws.part,
-                                alpha, add);
+                            L(launch_k(ov, k_ttform_qs<TW, FMT_F32, FMT_BF16>, unsigned(n32 + tp.nmseg[FMT_BF16]),
+                                       TW * 32, 0, s, tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vin,
+                                       vout, ws.part, alpha, add));
                         else if (n32 + tp.nmseg[FMT_F16] > 0)
-                            k_ttform_qs<TW, FMT_F32, FMT_F16><<<n32 + tp.nmseg[FMT_F16], TW * 32, 0, s>>>(
-                                tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin, vout, ws.part,
-                                alpha, add);
+                            L(launch_k(ov, k_ttform_qs<TW, FMT_F32, FMT_F16>, unsigned(n32 + tp.nmseg[FMT_F16]),
+                                       TW * 32, 0, s, tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vin,
+                                       vout, ws.part, alpha, add));
                     }
                 }
             };
@@ -1247,9 +1272,10 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
                 if (tp.ngroups1 > 0)   // first level: runs of slots into the scratch part of the partials
-                    k_ttfinish_f64<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, ws.part, ws.part, 1.0,
-                                                                         0);
-                k_ttfinish_f64<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.part, vout, alpha, add);
+                    L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups1 + 7) / 8), 256, 0, s, tp.groups1, tp.ngroups1,
+                               static_cast<const double*>(ws.part), ws.part, 1.0, 0));
+                L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups + 7) / 8), 256, 0, s, tp.groups, tp.ngroups,
+                           static_cast<const double*>(ws.part), vout, alpha, add));
                 if (ws.profile) prof_end(M, s);
             }
             HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
@@ -1272,21 +1298,21 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
                     return;
                 }
                 if (f64plan && np.nsegs[FMT_F64] > 0)
-                    k_nform_f64<NW><<<np.nsegs[FMT_F64], NW * 32, 0, s>>>(
-                        np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks),
-                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add);
+                    L(launch_k(ov, k_nform_f64<NW>, unsigned(np.nsegs[FMT_F64]), NW * 32, 0, s, np.segs[FMT_F64],
+                               static_cast<const NChunk*>(np.chunks), reinterpret_cast<const double*>(M->store), vx, vt,
+                               vo, alpha, add));
                 // reduced precision: one CTA per tile takes the packs of both formats
                 const QNPack* qc = static_cast<const QNPack*>(np.chunks);
                 if (!f64plan && np.nseg2 > 0) {
                     if (np.wide == FMT_I24)
-                        k_nform_q<NW, FMT_I24, FMT_I16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt, vo,
-                                                                                    alpha, add);
+                        L(launch_k(ov, k_nform_q<NW, FMT_I24, FMT_I16>, unsigned(np.nseg2), NW * 32, 0, s, np.seg2, qc,
+                                   M->store, vx, vt, vo, alpha, add));
                     else if (np.f16 == FMT_BF16)
-                        k_nform_q<NW, FMT_F32, FMT_BF16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt,
-                                                                                     vo, alpha, add);
+                        L(launch_k(ov, k_nform_q<NW, FMT_F32, FMT_BF16>, unsigned(np.nseg2), NW * 32, 0, s, np.seg2, qc,
+                                   M->store, vx, vt, vo, alpha, add));
                     else
-                        k_nform_q<NW, FMT_F32, FMT_F16><<<np.nseg2, NW * 32, 0, s>>>(np.seg2, qc, M->store, vx, vt,
-                                                                                    vo, alpha, add);
+                        L(launch_k(ov, k_nform_q<NW, FMT_F32, FMT_F16>, unsigned(np.nseg2), NW * 32, 0, s, np.seg2, qc,
+                                   M->store, vx, vt, vo, alpha, add));
                 }
             };
             if (M->nform_warps == 4) nform(Warps<4>{});
@@ -1295,7 +1321,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
         }
     }
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e = le != cudaSuccess ? le : cudaGetLastError();
     if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
     return HLRC_OK;
 }
@@ -1772,6 +1798,7 @@ extern "C" hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t) {
     t->ttform_warps = M->ttform_warps;
     t->mr_min_nrhs = M->mr_min_nrhs;
     t->wide_min_nrhs = M->wide_min_nrhs;
+    t->overlap = M->overlap;
     return HLRC_OK;
 }
 
@@ -1790,7 +1817,10 @@ extern "C" hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t) {
     M->nform_warps = t->nform_warps;
     M->ttform_warps = t->ttform_warps;
     M->mr_min_nrhs = t->mr_min_nrhs;
+    if (t->overlap != 0 && t->overlap != 1)
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: overlap must be 0 or 1 (got %d)", t->overlap);
     M->wide_min_nrhs = t->wide_min_nrhs;
+    M->overlap = t->overlap;
     return HLRC_OK;
 }
 

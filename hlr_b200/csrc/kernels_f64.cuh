@@ -18,6 +18,15 @@ __device__ __forceinline__ double2 ld_stream(const double* p) {
     return __ldcs(reinterpret_cast<const double2*>(p));
 }
 
+// Programmatic dependent launch.  The one-vector kernels are launched so
+// that the next kernel in the stream may start while they run: each lets
+// its successor launch as soon as it has started (pdl_trigger), reads only
+// its static descriptors before pdl_wait, and after pdl_wait (which returns
+// once the preceding kernel has completed and its writes are visible) reads
+// and writes the vectors.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // Butterfly transpose-reduction of N per-lane column partials (N = 2^g,
 // g <= 5): at each step a lane keeps one half of its values and trades the
 // other half with its partner, so 32 columns cost 31 shuffles instead of
@@ -55,11 +64,13 @@ k_nform_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, co
             const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
             int add) {
     __shared__ double red[W][TILE];
+    pdl_trigger();
     const NSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = 2 * lane;
     const bool active = r < sg.ld;
     double acc0 = 0.0, acc1 = 0.0;
+    pdl_wait();
     for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
         const NChunk ch = chunks[c];
         const double* v = (ch.v_off & VEC_T) ? vt + (ch.v_off & ~VEC_T) : vx + ch.v_off;
@@ -310,10 +321,12 @@ __global__ void __launch_bounds__(256)
 k_tform_f64(const TUnit* __restrict__ units, int nunits, const TSlab* __restrict__ slabs,
             const double* __restrict__ A, const double* __restrict__ vin, double* __restrict__ out,
             double* __restrict__ part, double alpha, int add) {
+    pdl_trigger();
     const int wid = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (wid >= nunits) return;
     const int lane = threadIdx.x & 31;
     const TUnit u = units[wid];
+    pdl_wait();
     double p[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) p[j] = 0.0;
@@ -357,10 +370,12 @@ __global__ void __launch_bounds__(W * 32)
 k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks, const double* __restrict__ A,
              const double* __restrict__ vin, double* __restrict__ out, double* __restrict__ part, double alpha,
              int add) {
+    pdl_trigger();
     const TTSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = 2 * lane;
     const bool active = r < sg.ld;
+    pdl_wait();
     const double v0 = (r < sg.rows) ? __ldg(vin + sg.v_off + r) : 0.0;
     const double v1 = (r + 1 < sg.rows) ? __ldg(vin + sg.v_off + r + 1) : 0.0;
     // software pipeline: the loads of chunk c + W are issued before chunk c
@@ -406,10 +421,12 @@ k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks,
 __global__ void __launch_bounds__(256)
 k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,
                double* __restrict__ out, double alpha, int add) {
+    pdl_trigger();
     const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (gid >= ngroups) return;
     const int lane = threadIdx.x & 31;
     const TGroup g = groups[gid];
+    pdl_wait();
     for (uint32_t j = lane; j < g.nc; j += 32) {
         // four interleaved partial sums keep four loads in flight; they are
         // combined in a fixed order, so the result is deterministic
@@ -434,10 +451,12 @@ k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __r
 __global__ void __launch_bounds__(256)
 k_tfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,
               double* __restrict__ out, double alpha, int add) {
+    pdl_trigger();
     const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (gid >= ngroups) return;
     const int lane = threadIdx.x & 31;
     const TGroup g = groups[gid];
+    pdl_wait();
     if (lane >= int(g.nc)) return;
     double s = 0.0;
     for (uint32_t i = 0; i < g.nslots; ++i) s += part[size_t(g.slot0 + i) * 32 + lane];

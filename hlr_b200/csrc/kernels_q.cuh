@@ -264,8 +264,10 @@ k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, cons
           const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
           int add) {
     __shared__ double red[W][TILE];
+    pdl_trigger();
     const NSeg2 sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    pdl_wait();
     if constexpr (WIDE == FMT_I24) {
         // the wide packs flushed before the 16-bit ones start: fewer live
         // registers next to the 24-bit loads
@@ -428,6 +430,8 @@ __global__ void __launch_bounds__(W * 32, 24 / W)
 k_ttform_qs(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
             const uint8_t* __restrict__ A, const double* __restrict__ vin, double* __restrict__ out,
             double* __restrict__ part, double alpha, int add) {
+    pdl_trigger();
+    pdl_wait();
     if (int(blockIdx.x) < n32) ttform_qs<W, WIDE>(segs32[blockIdx.x], cols, A, vin, out, part, alpha, add);
     else ttform_qs<W, F16>(segs16[blockIdx.x - n32], cols, A, vin, out, part, alpha, add);
 }

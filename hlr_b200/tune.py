@@ -33,7 +33,7 @@ from typing import Callable, Optional
 
 from ._capi import HLRC_MR_NEVER
 
-DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9}
+DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1}
 
 
 def default_cache_path() -> Path:

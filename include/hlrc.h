@@ -369,16 +369,21 @@ hlrc_status hlrc_workspace_free(hlrc_workspace ws);
  *   wide_min_nrhs: op N products of FP16 / BF16 H-matrix handles uploaded
  *     with max_nrhs > 8 with at least this many vectors run the one-pass
  *     kernels on the tcgen05 tensor cores, 64 vectors per pass of the
- *     matrix; smaller ones use the 8-vector kernels (2..HLRC_MR_NEVER).
- * Defaults: 8, 8, 2, 9.  hlrc_set_tuning rejects other values (HLRC_ERR_ARG)
- * and must not race with products of the same handle.                     */
+ *     matrix; smaller ones use the 8-vector kernels (2..HLRC_MR_NEVER);
+ *   overlap: 1 launches the one-vector kernels with programmatic dependent
+ *     launch (each may be scheduled while its predecessor in the stream
+ *     still runs and waits for it on the device before touching vectors),
+ *     0 launches them plainly; the results are the same.
+ * Defaults: 8, 8, 2, 9, 1.  hlrc_set_tuning rejects other values
+ * (HLRC_ERR_ARG) and must not race with products of the same handle.      */
 #define HLRC_MR_NEVER 1000000
 typedef struct hlrc_tuning {
     int32_t nform_warps;
     int32_t ttform_warps;
     int32_t mr_min_nrhs;
     int32_t wide_min_nrhs;
-    int32_t reserved[4];
+    int32_t overlap;
+    int32_t reserved[3];
 } hlrc_tuning;
 
 hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t);

@@ -47,3 +47,45 @@ def test_graph_replay_matches_direct_and_profiles(c2_small, prec):
     assert per_product > 0
     del g
     M.free()
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed", "bfp"])
+@pytest.mark.parametrize("op", [0, 1])
+def test_overlapped_launches_match_plain_launches(c2_small, prec, op):
+    """Programmatic dependent launch (tuning overlap = 1, the default) lets
+    each one-vector kernel start while its predecessor runs; every kernel
+    waits for its predecessor on the device before it reads or writes a
+    vector, so chains of products, direct and in a CUDA graph, give exactly
+    the plain launches' results (same kernels, same summation order)."""
+    M = hlr.upload(c2_small, precision=prec)
+    assert M.tuning["overlap"] == 1
+    x = torch.from_numpy(np.random.default_rng(3).standard_normal(c2_small.n)).cuda()
+
+    def chain(overlap, graph):
+        M.set_tuning(overlap=overlap)
+        y = torch.zeros_like(x)
+        if not graph:
+            for k in range(8):
+                hlr.mul_vec(0.5 + k, op, M, x, y)
+        else:
+            hlr.mul_vec(1.0, op, M, x, y)          # warm-up outside the graph
+            torch.cuda.synchronize()
+            y.zero_()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                for k in range(8):
+                    hlr.mul_vec(0.5 + k, op, M, x, y)
+            g.replay()
+            torch.cuda.synchronize()
+            del g
+        torch.cuda.synchronize()
+        return y.cpu().numpy()
+
+    plain = chain(0, False)
+    assert np.array_equal(chain(1, False), plain)
+    assert np.array_equal(chain(1, True), plain)
+    assert np.array_equal(chain(0, True), plain)
+    with pytest.raises(hlr.HLRCError):
+        M.set_tuning(overlap=2)
+    assert M.device_error() == 0
+    M.free()

@@ -57,7 +57,7 @@ def test_picks_fastest_and_caches(tmp_path):
     path = tmp_path / "tuning.json"
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
     assert not r["cached"] and len(calls) == 8      # two sweeps of four
-    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9}
+    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1}
     d = json.loads(path.read_text())
     assert d[r["key"]]["tuning"] == M.tuning
     # a fresh handle of the same signature takes the cached setting untimed
