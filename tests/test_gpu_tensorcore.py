@@ -20,7 +20,9 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 TOL = {"f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp": 1e-6}
-SAME_STORE = {"f32": 1e-6, "mixed": 2e-6, "f16": 2e-6, "bf16": 1e-4, "bfp": 1e-6}
+# FP16 / BF16 handles uploaded with max_nrhs > 8 take the 64-vector kernels
+# for more than 8 vectors, which sum a whole output tile in FP32
+SAME_STORE = {"f32": 1e-6, "mixed": 2e-6, "f16": 2e-5, "bf16": 1e-4, "bfp": 1e-6}
 
 
 def colmajor_dev(A):
