@@ -434,6 +434,10 @@ def run_ours(args, rank, world, local_rank):
         desc = desc.replace("FP64 ", f"{prec.upper()}-stored ") if prec != "f64" else desc
     if args.nrhs:
         nrhs = args.nrhs
+    # leaves assembled on the GPU (dense evaluation, ACA, QR/SVD) for the H
+    # configs unless --host-build; the oracle arms fetch them to the host
+    # after the timed products
+    prob.on_device = not args.host_build and not uniform and not args.h2
     tb = time.perf_counter()
     hm = hlr.build(prob)
     t_build = time.perf_counter() - tb
@@ -477,6 +481,11 @@ def run_ours(args, rank, world, local_rank):
     ms, runs, prof, timed_launches, per_graph = tm["ms"], tm["runs"], tm["prof"], tm["launches"], tm["per_graph"]
     ms_max = max_over_ranks(ms, world, dev)
 
+    t_fetch = None
+    if hm.leaves_on_device:
+        tf = time.perf_counter()
+        hm.fetch()
+        t_fetch = time.perf_counter() - tf
     # correctness of the timed path: one product from zero; column 0 is
     # compared with the oracle below
     yc = dev_vec(np.zeros((nrhs, n)))
@@ -562,7 +571,9 @@ def run_ours(args, rank, world, local_rank):
                    "l2": l2_label(info["matrix_bytes"]),
                    "matrix_bytes": info["matrix_bytes"], "algorithmic_bytes": alg, "flops": info["flops"],
                    "leaves": info["n_dense"] + info["n_lowrank"], "max_rank": info["max_rank"],
-                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2), "tuning": tuned,
+                   "construction": "device" if prob.on_device else "host",
+                   "build_s": round(t_build, 2), "upload_s": round(t_upload, 2),
+                   "fetch_s": round(t_fetch, 2) if t_fetch is not None else None, "tuning": tuned,
                    "graph": {"products_per_graph": per_graph, "replays": args.steps // per_graph,
                              "ms_per_product_of_runs": runs} if per_graph else None},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
@@ -634,7 +645,10 @@ def run_batch(args, rank, world, local_rank):
     inner = args.precision or "mixed"
     count = 32
     tb = time.perf_counter()
-    hms = [hlr.build(p) for p in c5_problems(count, nthreads=os.cpu_count() or 0)]
+    probs = c5_problems(count, nthreads=os.cpu_count() or 0)
+    for p in probs:
+        p.on_device = not args.host_build
+    hms = [hlr.build(p) for p in probs]
     t_build = time.perf_counter() - tb
     pad = (max(h.n for h in hms) + 63) // 64 * 64
     plan64 = planlow = None
@@ -745,6 +759,7 @@ def run_batch(args, rank, world, local_rank):
                                f"{inner}, CG + FP64 refinement to 1e-10",
                    "members": count, "n_total": sum(h.n for h in hms), "pad": pad, "nrhs": nrhs,
                    "matrix_bytes_inner": Alow.info["matrix_bytes"], "matrix_bytes_f64": A64.info["matrix_bytes"],
+                   "construction": "host" if args.host_build else "device",
                    "build_s": round(t_build, 1), "l2": l2_label(Alow.info["matrix_bytes"]),
                    "tuning": tuned, "tuning_f64": tuned64},
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
@@ -967,6 +982,8 @@ def main():
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
     ap.add_argument("--tune-plan", action="store_true", default=None,
                     help="also tune plan-level choices by re-uploading (default: on for c4 and c5)")
+    ap.add_argument("--host-build", action="store_true",
+                    help="assemble the leaves on the host (default: on the GPU for the H-matrix configs)")
     ap.add_argument("--reduced", default="bfp,mixed",
                     help="reduced-precision stores timed beside the FP64 one-vector H-matrix line "
                          "(comma list of bfp, mixed, f32, f16, bf16; 'none' for none)")

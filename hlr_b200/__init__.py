@@ -55,6 +55,7 @@ class Problem:
     uniform: bool = False
     nthreads: int = 0
     nested: bool = False   # also build the H^2 form (nested cluster bases)
+    on_device: bool = False  # assemble the leaves on the current CUDA device (H form only)
 
     @staticmethod
     def log1d(n: int, **kw) -> "Problem":
@@ -77,6 +78,7 @@ class Problem:
         p.uniform, p.seed, p.eta, p.eps = int(self.uniform), self.seed, self.eta, self.eps
         p.ell, p.nugget, p.nthreads = self.ell, self.nugget, self.nthreads
         p.nested = int(self.nested)
+        p.on_device = int(self.on_device)
         return p
 
 
@@ -103,6 +105,20 @@ class HostMatrix:
         secs, nl, mr, by = C.c_double(), C.c_int64(), C.c_int32(), C.c_int64()
         check(lib().hlrc_build_stats(h, C.byref(secs), C.byref(nl), C.byref(mr), C.byref(by)), "hlrc_build_stats")
         self.build_seconds, self.nleaves, self.max_rank, self.bytes = secs.value, nl.value, mr.value, by.value
+
+    @property
+    def leaves_on_device(self) -> bool:
+        """True while the leaf data of an on_device build is in device memory
+        (h_desc() then holds device pointers; upload passes that on)."""
+        v = C.c_int(0)
+        check(lib().hlrc_build_leaves_on_device(self._h, C.byref(v)), "hlrc_build_leaves_on_device")
+        return bool(v.value)
+
+    def fetch(self) -> "HostMatrix":
+        """Copies device-resident leaf data to host memory (hlrc_build_fetch);
+        afterwards the matrix behaves like a host build.  Returns self."""
+        check(lib().hlrc_build_fetch(self._h), "hlrc_build_fetch")
+        return self
 
     def h_desc(self) -> _capi.hlrc_h_desc:
         d = _capi.hlrc_h_desc()
@@ -187,6 +203,12 @@ class LeafList:
         d.blocks = C.cast(arr, C.POINTER(_capi.hlrc_block))
         d._owner = (self, arr)
         return d
+
+
+def _on_device(src) -> bool:
+    """Whether src's leaf data is in device memory (an on_device build not
+    fetched to the host)."""
+    return isinstance(src, HostMatrix) and src.leaves_on_device
 
 
 def _options(precision="f64", max_nrhs: int = 1, mixed_eps: float = 1e-6, device: int = -1, plan=None):
@@ -323,6 +345,7 @@ def upload(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: int =
     if uniform is None:
         uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
     o = _options(precision, max_nrhs, mixed_eps, device, plan)
+    o.leaves_on_device = int(_on_device(src))
     h = C.c_void_p()
     if h2:
         d = src.h2_desc() if hasattr(src, "h2_desc") else src
@@ -364,6 +387,10 @@ def upload_batch(members, precision="f64", max_nrhs: int = 1, pad_to: Optional[i
     arr = (_capi.hlrc_h_desc * len(descs))(*descs)
     offs = (C.c_int64 * len(offsets))(*offsets)
     o = _options(precision, max_nrhs, mixed_eps, device, plan)
+    dev = {_on_device(m) for m in members}
+    if len(dev) > 1:
+        raise ValueError("upload_batch: members with device-resident and host leaves (fetch() the former)")
+    o.leaves_on_device = int(dev.pop())
     h = C.c_void_p()
     check(lib().hlrc_upload_h_batch(arr, len(descs), offs, C.byref(o), C.byref(h)), "hlrc_upload_h_batch")
     M = DeviceMatrix(h, False)
@@ -381,6 +408,7 @@ def plan_info(src, precision="f64", uniform: Optional[bool] = None, max_nrhs: in
     if uniform is None:
         uniform = (not h2) and isinstance(src, HostMatrix) and src.problem.uniform
     o = _options(precision, max_nrhs, mixed_eps, -1, plan)
+    o.leaves_on_device = int(_on_device(src))
     inf = _capi.hlrc_info()
     if h2:
         d = src.h2_desc() if hasattr(src, "h2_desc") else src

@@ -63,7 +63,7 @@ class hlrc_h2_desc(C.Structure):
 
 class hlrc_options(C.Structure):
     _fields_ = [("precision", i32), ("max_nrhs", i32), ("mixed_eps", f64), ("device", i32),
-                ("finish_slots", i32), ("piece_tiles", i32), ("reserved", i32 * 5)]
+                ("finish_slots", i32), ("piece_tiles", i32), ("leaves_on_device", i32), ("reserved", i32 * 4)]
 
 
 class hlrc_info(C.Structure):
@@ -85,7 +85,7 @@ HLRC_MR_NEVER = 1000000
 class hlrc_problem(C.Structure):
     _fields_ = [("kind", i32), ("leaf_size", i32), ("n", i64), ("refine", i32), ("uniform", i32),
                 ("seed", u64), ("eta", f64), ("eps", f64), ("ell", f64), ("nugget", f64),
-                ("nthreads", i32), ("nested", i32), ("reserved", i32 * 4)]
+                ("nthreads", i32), ("nested", i32), ("on_device", i32), ("reserved", i32 * 3)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/hlrc.h
@@ -130,6 +130,8 @@ PROTOTYPES = {
     "hlrc_build_perm": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(i64))]),
     "hlrc_build_stats": (C.c_int, [C.c_void_p, C.POINTER(f64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]),
     "hlrc_build_free": (C.c_int, [C.c_void_p]),
+    "hlrc_build_leaves_on_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "hlrc_build_fetch": (C.c_int, [C.c_void_p]),
     "hlrc_build_entry": (f64, [C.c_void_p, i64, i64]),
 }
 

@@ -27,7 +27,7 @@ CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-march=x86-64-v3", "-Wall
 NVCCFLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr"]
 
 CXX_SOURCES = ["common.cpp", "plan.cpp", "host/build.cpp"]
-CU_SOURCES = ["hmvm.cu", "measure.cu"]
+CU_SOURCES = ["hmvm.cu", "measure.cu", "build_gpu.cu"]
 
 
 def _sources() -> list[Path]:

@@ -293,7 +293,7 @@ ArenaLayout arena_layout(const Plan& p) {
     auto take = [&](size_t bytes) { const size_t o_ = off; off = align_up(off + bytes, 256); return o_; };
     static_assert(sizeof(NChunk) == sizeof(QNChunk) && sizeof(TTChunk) == sizeof(QTTChunk),
                   "FP64 and reduced-precision chunk descriptors share one size");
-    L.store = take(p.store.size());
+    L.store = take(size_t(p.store_size()));
     uint32_t max_slots = 0;
     for (const TPass& tp : p.tpasses) {
         L.tu.push_back(take(tp.units.size() * sizeof(TUnit)));
@@ -787,6 +787,111 @@ hlrc_status enable_wide_smem(int dev) {
     return HLRC_OK;
 }
 
+// Checks that every column block of a device-filled store lies inside an
+// allocation of device `dev` (a leaf pointer of another device or of host
+// memory would make the gather kernel fault): the allocation range of a
+// pointer comes from cuMemGetAddressRange, its device from
+// cudaPointerGetAttributes, and confirmed ranges are cached.
+hlrc_status check_dev_copies(const std::vector<DevCopy>& cps, int dev) {
+    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static RangeFn range = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<RangeFn>(f);
+    }();
+    if (!range) return fail(HLRC_ERR_CUDA, "leaves_on_device: cuMemGetAddressRange is unavailable");
+    std::vector<std::pair<uintptr_t, uintptr_t>> ok;   // confirmed [begin, end)
+    for (const DevCopy& c : cps) {
+        if (c.nc <= 0 || c.rows <= 0) continue;
+        const uintptr_t b = reinterpret_cast<uintptr_t>(c.src);
+        const uintptr_t e = b + (uintptr_t(c.lds) * uintptr_t(c.nc - 1) + uintptr_t(c.rows)) * sizeof(double);
+        bool hit = false;
+        for (const auto& r : ok)
+            if (b >= r.first && e <= r.second) { hit = true; break; }
+        if (hit) continue;
+        cudaPointerAttributes at{};
+        CUdeviceptr base = 0;
+        size_t size = 0;
+        if (cudaPointerGetAttributes(&at, c.src) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+            at.device != dev || range(&base, &size, CUdeviceptr(b)) != CUDA_SUCCESS) {
+            cudaGetLastError();
+            return fail(HLRC_ERR_ARG, "leaves_on_device: leaf data at %p is not device memory of device %d", c.src, dev);
+        }
+        if (e > uintptr_t(base) + size)
+            return fail(HLRC_ERR_ARG, "leaves_on_device: leaf data at %p runs past its allocation", c.src);
+        ok.emplace_back(uintptr_t(base), uintptr_t(base) + size);
+    }
+    return HLRC_OK;
+}
+
+// The FP64 store of device-resident leaves: one warp per column block
+// (DevCopy), columns one after the other, rows across the lanes.
+__global__ void __launch_bounds__(256)
+k_store_gather(const DevCopy* __restrict__ copies, int64_t n, char* __restrict__ store) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const DevCopy c = copies[i];
+        double* dst = reinterpret_cast<double*>(store + c.dst);
+        for (int j = 0; j < c.nc; ++j)
+            for (int r = lane; r < c.rows; r += 32) dst[int64_t(j) * c.ldc + r] = c.src[int64_t(j) * c.lds + r];
+    }
+}
+
+// Host copies of the leaf data of device-resident blocks (for stores that
+// are planned from host data): every block of `blocks` re-pointed at them.
+struct HostLeaves {
+    std::vector<hlrc_block> blocks;
+    std::vector<std::vector<double>> data;
+};
+
+hlrc_status leaves_to_host(const hlrc_block* blocks, int64_t nb, HostLeaves& h) {
+    h.blocks.assign(blocks, blocks + nb);
+    h.data.clear();
+    h.data.reserve(size_t(nb) * 3);
+    auto take = [&](const double*& ptr, int64_t ld, int64_t rows, int64_t cols) -> cudaError_t {
+        if (!ptr || rows <= 0 || cols <= 0) return cudaSuccess;
+        const int64_t n = ld * (cols - 1) + rows;
+        h.data.emplace_back(size_t(n));
+        const cudaError_t e = cudaMemcpy(h.data.back().data(), ptr, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost);
+        ptr = h.data.back().data();
+        return e;
+    };
+    for (hlrc_block& b : h.blocks) {
+        cudaError_t e = cudaSuccess;
+        if (b.kind == HLRC_LEAF_DENSE) {
+            e = take(b.D, b.ldd, b.nrows, b.ncols);
+        } else if (b.rank > 0) {
+            e = take(b.U, b.ldu, b.nrows, b.rank);
+            if (e == cudaSuccess) e = take(b.V, b.ldv, b.ncols, b.rank);
+            if (e == cudaSuccess) e = take(b.sv, b.rank, b.rank, 1);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HLRC_ERR_CUDA, "copying device-resident leaves to the host: %s", cudaGetErrorString(e));
+        }
+    }
+    return HLRC_OK;
+}
+
+// plan_h for host- or device-resident leaves: FP64 stores of device leaves
+// are gathered on the device; other precisions are planned from host copies.
+hlrc_status plan_h_leaves(const hlrc_h_desc& d, hlrc_options o, Plan& p, double area = -1.0) {
+    if (!o.leaves_on_device || o.precision == HLRC_PREC_F64) return plan_h(d, o, p, area);
+    if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
+    HostLeaves hl;
+    const hlrc_status st = leaves_to_host(d.blocks, std::max<int64_t>(0, d.nblocks), hl);
+    if (st != HLRC_OK) return st;
+    const hlrc_h_desc hd{d.nrows, d.ncols, d.nblocks, hl.blocks.data()};
+    o.leaves_on_device = 0;
+    return plan_h(hd, o, p, area);
+}
+
 hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     auto h = std::make_unique<hlrc_hmat_s>();
     int dev = o.device;
@@ -824,7 +929,29 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         return cudaMemcpy(hp->arena + o_, src, bytes, cudaMemcpyHostToDevice);
     };
     const bool f64 = p.precision == HLRC_PREC_F64;
-    e = put(o_store, p.store.data(), p.store.size());
+    if (!p.dev_src) {
+        e = put(o_store, p.store.data(), p.store.size());
+    } else {
+        // leaves in device memory: the store is gathered on the device
+        if (const hlrc_status cs = check_dev_copies(p.dev_copies, dev); cs != HLRC_OK) {
+            cleanup();
+            return cs;
+        }
+        e = cudaMemset(hp->arena + o_store, 0, size_t(p.dev_store_bytes));
+        const size_t nc = p.dev_copies.size();
+        if (e == cudaSuccess && nc > 0) {
+            DevCopy* dc = nullptr;
+            e = cudaMalloc(&dc, nc * sizeof(DevCopy));
+            if (e == cudaSuccess) e = cudaMemcpy(dc, p.dev_copies.data(), nc * sizeof(DevCopy), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) {
+                const unsigned grid = unsigned(std::min<size_t>((nc + 7) / 8, size_t(148) * 16));
+                k_store_gather<<<grid, 256>>>(dc, int64_t(nc), hp->arena + o_store);
+                e = cudaGetLastError();
+                if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            }
+            if (dc) cudaFree(dc);
+        }
+    }
     for (size_t i = 0; e == cudaSuccess && i < p.tpasses.size(); ++i) {
         const TPass& tp = p.tpasses[i];
         e = put(o_tu[i], tp.units.data(), tp.units.size() * sizeof(TUnit));
@@ -1049,7 +1176,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     cudaDeviceGetAttribute(&hp->sms, cudaDevAttrMultiProcessorCount, dev);
     if (hp->sms <= 0) hp->sms = 148;
     if (!p.wide.empty()) {
-        const uint64_t rows = uint64_t(p.store.size()) / 128;
+        const uint64_t rows = uint64_t(p.store_size()) / 128;
         hp->tma = rows > 0 && make_map(&hp->tm_s16, hp->store, 64, rows, 128, 64, 16) &&
                   make_map(&hp->tm_s8, hp->store, 64, rows, 128, 64, 8);
     }
@@ -1612,7 +1739,7 @@ extern "C" hlrc_status hlrc_upload_h(const hlrc_h_desc* desc, const hlrc_options
     hlrc_options o;
     if (opts) o = *opts; else hlrc_default_options(&o);
     Plan p;
-    hlrc_status st = plan_h(*desc, o, p);
+    const hlrc_status st = plan_h_leaves(*desc, o, p);
     if (st != HLRC_OK) return st;
     return upload_plan(p, o, out);
 }
@@ -1650,9 +1777,9 @@ extern "C" hlrc_status hlrc_upload_h_batch(const hlrc_h_desc* descs, int count, 
                         double(d.nrows) * double(d.ncols));
         area += a;
     }
-    const hlrc_h_desc cd{offsets[count], offsets[count], int64_t(all.size()), all.data()};
     Plan p;
-    hlrc_status st = plan_h(cd, o, p, area);
+    const hlrc_h_desc cd{offsets[count], offsets[count], int64_t(all.size()), all.data()};
+    const hlrc_status st = plan_h_leaves(cd, o, p, area);
     if (st != HLRC_OK) return st;
     return upload_plan(p, o, out);
 }
@@ -1675,7 +1802,7 @@ extern "C" hlrc_status hlrc_plan_info_h(const hlrc_h_desc* desc, const hlrc_opti
     hlrc_options o;
     if (opts) o = *opts; else hlrc_default_options(&o);
     Plan p;
-    hlrc_status st = plan_h(*desc, o, p);
+    hlrc_status st = plan_h_leaves(*desc, o, p);
     if (st != HLRC_OK) return st;
     if (st = check_streams(p); st != HLRC_OK) return st;
     fill_info(p, arena_layout(p), *info);

@@ -27,6 +27,7 @@
 #include <omp.h>
 
 #include "../common.hpp"
+#include "build_gpu.hpp"
 #include "la.hpp"
 
 namespace hlrc {
@@ -720,6 +721,10 @@ using namespace hlrc;
 
 struct hlrc_hbuild_s {
     HBuild b;
+    double* dev_arena = nullptr;   // on_device builds: the leaf data (until fetched)
+    int64_t dev_doubles = 0;
+    std::vector<GpuLeaf> gl;       // per leaf: offsets into dev_arena
+    ~hlrc_hbuild_s() { gpu_free(dev_arena); }
 };
 
 extern "C" hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out) {
@@ -729,6 +734,8 @@ extern "C" hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out) {
     if (prob->leaf_size < 2) return fail(HLRC_ERR_ARG, "hlrc_build: leaf_size must be >= 2");
     if (prob->kind != HLRC_PROBLEM_LAPLACE_SPH && prob->n < 1) return fail(HLRC_ERR_ARG, "hlrc_build: n must be >= 1");
     if (!(prob->eps > 0) || !(prob->eta > 0)) return fail(HLRC_ERR_ARG, "hlrc_build: eps and eta must be > 0");
+    if (prob->on_device && (prob->uniform || prob->nested))
+        return fail(HLRC_ERR_ARG, "hlrc_build: on_device builds the H form only (uniform and nested need host leaves)");
     const auto t0 = std::chrono::steady_clock::now();
     auto h = std::make_unique<hlrc_hbuild_s>();
     HBuild& B = h->b;
@@ -761,6 +768,45 @@ extern "C" hlrc_status hlrc_build(const hlrc_problem* prob, hlrc_hbuild* out) {
         return ca > cb || (ca == cb && a < b);
     });
     const double eps = prob->eps;
+    if (prob->on_device) {
+        GpuProblem gp;
+        gp.kind = P.kind; gp.dim = P.dim; gp.n = P.n;
+        gp.pts = P.pts.data();
+        gp.wts = P.wts.empty() ? nullptr : P.wts.data();
+        gp.ell = P.ell; gp.nugget = P.nugget; gp.h = P.h;
+        h->gl.resize(B.leaves.size());
+        for (size_t i = 0; i < B.leaves.size(); ++i) {
+            const Leaf& l = B.leaves[i];
+            GpuLeaf& g = h->gl[i];
+            g.row0 = l.row0; g.nrows = l.nrows; g.col0 = l.col0; g.ncols = l.ncols; g.kind = l.kind;
+        }
+        const hlrc_status st = gpu_assemble(gp, h->gl, eps, &h->dev_arena, &h->dev_doubles);
+        if (st != HLRC_OK) return st;
+        B.desc_blocks.resize(B.leaves.size());
+        for (size_t i = 0; i < B.leaves.size(); ++i) {
+            Leaf& l = B.leaves[i];
+            const GpuLeaf& g = h->gl[i];
+            l.rank = g.rank;
+            hlrc_block& d = B.desc_blocks[i];
+            std::memset(&d, 0, sizeof(d));
+            d.row0 = l.row0; d.nrows = l.nrows; d.col0 = l.col0; d.ncols = l.ncols;
+            d.kind = l.kind; d.rank = l.rank;
+            if (l.kind == HLRC_LEAF_DENSE) {
+                d.D = g.d >= 0 ? h->dev_arena + g.d : nullptr;
+                d.ldd = std::max<int64_t>(1, l.nrows);
+                B.bytes += l.nrows * l.ncols * 8;
+            } else {
+                d.U = l.rank ? h->dev_arena + g.u : nullptr; d.ldu = std::max<int64_t>(1, l.nrows);
+                d.V = l.rank ? h->dev_arena + g.v : nullptr; d.ldv = std::max<int64_t>(1, l.ncols);
+                d.sv = l.rank ? h->dev_arena + g.s : nullptr;
+                B.bytes += (l.nrows + l.ncols) * l.rank * 8;
+                B.max_rank = std::max(B.max_rank, l.rank);
+            }
+        }
+        B.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        *out = h.release();
+        return HLRC_OK;
+    }
     #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
     for (int oi = 0; oi < int(order.size()); ++oi) {
         Leaf& l = B.leaves[order[oi]];
@@ -874,6 +920,43 @@ extern "C" hlrc_status hlrc_build_stats(hlrc_hbuild B, double* seconds, int64_t*
     if (nleaves) *nleaves = int64_t(B->b.leaves.size());
     if (max_rank) *max_rank = B->b.max_rank;
     if (bytes) *bytes = B->b.bytes;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_build_leaves_on_device(hlrc_hbuild B, int* on_device) {
+    if (!B || !on_device) return fail(HLRC_ERR_ARG, "hlrc_build_leaves_on_device: null argument");
+    *on_device = B->dev_arena ? 1 : 0;
+    return HLRC_OK;
+}
+
+extern "C" hlrc_status hlrc_build_fetch(hlrc_hbuild B) {
+    clear_error();
+    if (!B) return fail(HLRC_ERR_ARG, "hlrc_build_fetch: null argument");
+    if (!B->dev_arena) return HLRC_OK;
+    HBuild& b = B->b;
+    for (size_t i = 0; i < b.leaves.size(); ++i) {
+        Leaf& l = b.leaves[i];
+        const GpuLeaf& g = B->gl[i];
+        hlrc_block& d = b.desc_blocks[i];
+        hlrc_status st = HLRC_OK;
+        if (l.kind == HLRC_LEAF_DENSE) {
+            l.D.resize(size_t(l.nrows * l.ncols));
+            if (!l.D.empty()) st = gpu_copy_to_host(l.D.data(), B->dev_arena + g.d, int64_t(l.D.size()));
+            d.D = l.D.empty() ? nullptr : l.D.data();
+        } else if (l.rank > 0) {
+            l.U.resize(size_t(l.nrows * l.rank));
+            l.V.resize(size_t(l.ncols * l.rank));
+            l.sv.resize(size_t(l.rank));
+            st = gpu_copy_to_host(l.U.data(), B->dev_arena + g.u, int64_t(l.U.size()));
+            if (st == HLRC_OK) st = gpu_copy_to_host(l.V.data(), B->dev_arena + g.v, int64_t(l.V.size()));
+            if (st == HLRC_OK) st = gpu_copy_to_host(l.sv.data(), B->dev_arena + g.s, int64_t(l.sv.size()));
+            d.U = l.U.data(); d.V = l.V.data(); d.sv = l.sv.data();
+        }
+        if (st != HLRC_OK) return st;
+    }
+    gpu_free(B->dev_arena);
+    B->dev_arena = nullptr;
+    B->dev_doubles = 0;
     return HLRC_OK;
 }
 

@@ -310,6 +310,19 @@ struct Store {
             }
         }
     }
+    // FP64 stores of device-resident leaves: the copies fill() would make
+    void fill_device(Plan& p) const {
+        p.dev_src = true;
+        p.dev_store_bytes = bytes;
+        p.dev_copies.clear();
+        for (const SSlab& sl : slabs)
+            for (int32_t c = sl.c0; c < sl.c0 + sl.nch; ++c) {
+                const SChunk& ch = chunks[size_t(c)];
+                p.dev_copies.push_back(DevCopy{uint64_t(ch.byte_off), sl.src + sl.r0 + int64_t(ch.col0) * sl.lds,
+                                               sl.lds, int32_t(sl.rows), int32_t(ch.nc),
+                                               int32_t(pad_fmt(sl.rows, ch.fmt)), 0});
+            }
+    }
     int64_t slab_elem_off(int id) const {  // FP64 stores only: element offset of column 0
         return chunks[size_t(slabs[size_t(id)].c0)].byte_off / 8;
     }
@@ -476,6 +489,8 @@ hlrc_status check_knobs(const hlrc_options& o) {
         return fail(HLRC_ERR_ARG, "finish_slots %d outside 2..64", o.finish_slots);
     if (o.piece_tiles != 0 && (o.piece_tiles < 1 || o.piece_tiles > WT_MAXT))
         return fail(HLRC_ERR_ARG, "piece_tiles %d outside 1..%d", o.piece_tiles, WT_MAXT);
+    if (o.leaves_on_device != 0 && o.leaves_on_device != 1)
+        return fail(HLRC_ERR_ARG, "leaves_on_device must be 0 or 1 (got %d)", o.leaves_on_device);
     return HLRC_OK;
 }
 
@@ -649,7 +664,7 @@ void valr_formats(const double* sv, int64_t k, double eps, uint8_t* fmt, int pre
 // the padded column).  A violation is a planner bug: the upload is refused
 // instead of handing the GPU an out-of-bounds address.
 hlrc_status validate_plan(const Plan& p) {
-    const int64_t store = int64_t(p.store.size());
+    const int64_t store = p.store_size();
     auto vec_len = [&](int name) -> int64_t {
         switch (name) {
             case V_X: return std::max(p.nrows, p.ncols);
@@ -900,7 +915,7 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
                 const uint64_t a16 = W.slabs[size_t(u.slab0) + size_t(t) * u.nblk + size_t(j)];
                 const uint64_t end = a16 * 16 + uint64_t(W.blks[size_t(u.blk0) + size_t(j)].k) *
                                                      uint64_t(W.tiles[size_t(u.tile0) + size_t(t)].ld) * 2;
-                if (a16 * 16 % 16 != 0 || end > uint64_t(p.store.size()))
+                if (a16 * 16 % 16 != 0 || end > uint64_t(p.store_size()))
                     return fail(HLRC_ERR_INTERNAL, "64-vector unit reads outside the store");
             }
     return HLRC_OK;
@@ -909,6 +924,11 @@ hlrc_status plan_wide(const hlrc_h_desc& d, const Tiles& tc, const std::vector<i
 hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double expected_area) {
     if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
     const KnobScope knobs(o);
+    // leaf data in device memory is never read here: FP64 stores become
+    // device copies (Store::fill_device), other precisions are planned from
+    // a host copy of the leaves (hlrc_upload_h)
+    if (o.leaves_on_device && o.precision != HLRC_PREC_F64)
+        return fail(HLRC_ERR_INTERNAL, "device-resident leaves reach the planner with an FP64 store only");
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0) return fail(HLRC_ERR_SHAPE, "negative matrix size");
     if (d.nblocks > 0 && !d.blocks) return fail(HLRC_ERR_ARG, "blocks == NULL");
     if (d.nrows >= (int64_t(1) << 31) || d.ncols >= (int64_t(1) << 31))
@@ -1067,7 +1087,11 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
     for (const SChunk& ch : st.chunks)
         if ((ch.fmt == FMT_F64) != (o.precision == HLRC_PREC_F64))
             return fail(HLRC_ERR_INTERNAL, "chunk format %d in a plan of precision %d", ch.fmt, o.precision);
-    st.fill(p.store);
+    if (o.leaves_on_device) {
+        st.fill_device(p);
+    } else {
+        st.fill(p.store);
+    }
     for (int f = 0; f < NFMT; ++f) p.fmt_bytes[f] = st.unpadded[f];
 
     p.npasses.resize(2);
@@ -1185,6 +1209,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
 // ------------------------------------------------------------- uniform-H
 hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan& p) {
     if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
+    if (o.leaves_on_device) return fail(HLRC_ERR_ARG, "leaves_on_device: H-matrix descriptors only");
     const KnobScope knobs(o);
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0 || d.nrow_bases < 0 || d.ncol_bases < 0)
         return fail(HLRC_ERR_SHAPE, "negative size");
@@ -1472,6 +1497,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
 // bases, and the near field transposed.
 hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
     if (hlrc_status ks = check_knobs(o); ks != HLRC_OK) return ks;
+    if (o.leaves_on_device) return fail(HLRC_ERR_ARG, "leaves_on_device: H-matrix descriptors only");
     const KnobScope knobs(o);
     if (d.nrows < 0 || d.ncols < 0 || d.nblocks < 0 || d.nrow_clusters <= 0 || d.ncol_clusters <= 0)
         return fail(HLRC_ERR_SHAPE, "H2: bad sizes or empty cluster tree");

@@ -116,11 +116,28 @@ struct Stage {
     int idx;                       // index into Plan::tpasses / npasses / ttpasses
 };
 
+// One column block of an FP64 store whose source leaves are in device
+// memory: nc columns of `rows` doubles from src (leading dimension lds) to
+// store byte offset dst (leading dimension ldc; rows past `rows` stay zero).
+struct DevCopy {
+    uint64_t dst;
+    const double* src;
+    int64_t lds;
+    int32_t rows, nc, ldc, pad;
+};
+static_assert(sizeof(DevCopy) == 40, "DevCopy is 40 bytes");
+
 struct Plan {
     int kind = 0;                  // 0 = H, 1 = uniform-H, 2 = H^2
     int precision = HLRC_PREC_F64;
     int64_t nrows = 0, ncols = 0;
     std::vector<uint8_t> store;    // slab storage (FP64, or per-chunk formats)
+    // device-resident leaves (FP64): the store is filled on the device by
+    // these copies instead of from `store`, which stays empty
+    bool dev_src = false;
+    int64_t dev_store_bytes = 0;
+    std::vector<DevCopy> dev_copies;
+    int64_t store_size() const { return dev_src ? dev_store_bytes : int64_t(store.size()); }
     int64_t n_t = 0, n_t2 = 0;     // workspace vector lengths (per rhs)
     std::vector<TPass> tpasses;
     std::vector<NPass> npasses;

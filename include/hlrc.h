@@ -194,7 +194,11 @@ typedef struct hlrc_options {
      *   many tiles are cut into pieces summed by a finish (1..32, default 32) */
     int32_t finish_slots;
     int32_t piece_tiles;
-    int32_t reserved[5];
+    /* 1: the descriptor's leaf data (D, U, V, sv) is in device memory of this
+     * device (an on_device build); FP64 stores are filled on the device,
+     * other precisions copy the leaves to the host first                   */
+    int32_t leaves_on_device;
+    int32_t reserved[4];
 } hlrc_options;
 
 /* accounting of one product, following HLR's mul_vec_flops /
@@ -460,7 +464,12 @@ typedef struct hlrc_problem {
     double   nugget;       /* EXP3D diagonal nugget                               */
     int32_t  nthreads;     /* host threads for the build (0 = all)                */
     int32_t  nested;       /* 1: also build the H^2 form (nested cluster bases)   */
-    int32_t  reserved[4];
+    int32_t  on_device;    /* 1: assemble the leaves on the current CUDA device
+                              (dense evaluation, ACA, QR + SVD recompression);
+                              H only (not with uniform or nested); the leaf data
+                              stays in device memory (hlrc_build_h_desc then
+                              returns device pointers, see hlrc_build_fetch)   */
+    int32_t  reserved[3];
 } hlrc_problem;
 
 typedef struct hlrc_hbuild_s* hlrc_hbuild;
@@ -477,6 +486,14 @@ hlrc_status hlrc_build_points(hlrc_hbuild B, const double** pts, int* dim,
 hlrc_status hlrc_build_weights(hlrc_hbuild B, const double** w);
 /* internal -> external permutation (perm_i2e), length n                     */
 hlrc_status hlrc_build_perm(hlrc_hbuild B, const int64_t** perm_i2e);
+/* on_device builds: 1 while the leaf data is in device memory (the
+ * descriptor's D, U, V and sv are device pointers; upload it with
+ * hlrc_options.leaves_on_device = 1), 0 once hlrc_build_fetch copied it to
+ * the host (and for host builds)                                           */
+hlrc_status hlrc_build_leaves_on_device(hlrc_hbuild B, int* on_device);
+/* copies device-resident leaf data to host storage and points the
+ * descriptor at it (a no-op for host builds); the device copy is freed     */
+hlrc_status hlrc_build_fetch(hlrc_hbuild B);
 /* build statistics: seconds, number of leaves, max rank, stored bytes       */
 hlrc_status hlrc_build_stats(hlrc_hbuild B, double* seconds, int64_t* nleaves,
                              int32_t* max_rank, int64_t* bytes);

@@ -106,3 +106,20 @@ def test_odd_sizes_and_leaf_sizes():
     yd = np.zeros(hm.n)
     oracle.dense_matvec(hm, 1.0, 0, x, yd)
     assert np.linalg.norm(y - yd) / np.linalg.norm(yd) < 2e-6
+
+
+def test_device_build_arguments():
+    # the device build assembles the H form only
+    with pytest.raises(hlr.HLRCError) as e:
+        hlr.build(hlr.Problem.laplace_sphere(2, uniform=True, on_device=True))
+    assert e.value.status == 1
+    # without a usable GPU it fails with a CUDA status, not a crash
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        with pytest.raises(hlr.HLRCError) as e:
+            hlr.build(hlr.Problem.exp3d(500, on_device=True))
+        assert e.value.status == 4
+    # a host build reports host leaves and fetch() is a no-op
+    hm = hlr.build(hlr.Problem.log1d(300))
+    assert not hm.leaves_on_device
+    assert hm.fetch() is hm and not hm.leaves_on_device
