@@ -440,6 +440,8 @@ def run_ours(args, rank, world, local_rank):
     prob.on_device = not args.host_build and not uniform and not args.h2
     tb = time.perf_counter()
     hm = hlr.build(prob)
+    if hm.leaves_on_device and prec != "f64":
+        hm.fetch()   # reduced-precision stores are planned from host leaves: one bulk copy here
     t_build = time.perf_counter() - tb
     tu = time.perf_counter()
     plan_tuned = None
@@ -648,6 +650,8 @@ def run_batch(args, rank, world, local_rank):
     probs = c5_problems(count, nthreads=os.cpu_count() or 0)
     for p in probs:
         p.on_device = not args.host_build
+    # the FP64 store is gathered on the device; the leaves are then fetched
+    # to the host (one bulk copy per member) for the reduced-precision store
     hms = [hlr.build(p) for p in probs]
     t_build = time.perf_counter() - tb
     pad = (max(h.n for h in hms) + 63) // 64 * 64
@@ -660,11 +664,16 @@ def run_batch(args, rank, world, local_rank):
         if inner == "f64":
             Alow = A64
         else:
+            for h in hms:
+                h.fetch()
             Alow, planlow = autotune_plan(
                 lambda p: hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad, plan=p), nrhs=nrhs,
                 knobs=("finish_slots",))
     else:
         A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
+        if inner != "f64":
+            for h in hms:
+                h.fetch()
         Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
     tuned64 = tune_handle(A64, nrhs, args)
     tuned = tune_handle(Alow, nrhs, args) if Alow is not A64 else tuned64

@@ -792,9 +792,9 @@ hlrc_status enable_wide_smem(int dev) {
 // memory would make the gather kernel fault): the allocation range of a
 // pointer comes from cuMemGetAddressRange, its device from
 // cudaPointerGetAttributes, and confirmed ranges are cached.
-hlrc_status check_dev_copies(const std::vector<DevCopy>& cps, int dev) {
-    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
-    static RangeFn range = [] {
+using AddrRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddrRangeFn addr_range_fn() {
+    static AddrRangeFn fn = [] {
         void* f = nullptr;
         cudaDriverEntryPointQueryResult q{};
         if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
@@ -802,8 +802,13 @@ hlrc_status check_dev_copies(const std::vector<DevCopy>& cps, int dev) {
             cudaGetLastError();
             f = nullptr;
         }
-        return reinterpret_cast<RangeFn>(f);
+        return reinterpret_cast<AddrRangeFn>(f);
     }();
+    return fn;
+}
+
+hlrc_status check_dev_copies(const std::vector<DevCopy>& cps, int dev) {
+    const AddrRangeFn range = addr_range_fn();
     if (!range) return fail(HLRC_ERR_CUDA, "leaves_on_device: cuMemGetAddressRange is unavailable");
     std::vector<std::pair<uintptr_t, uintptr_t>> ok;   // confirmed [begin, end)
     for (const DevCopy& c : cps) {
@@ -844,7 +849,9 @@ k_store_gather(const DevCopy* __restrict__ copies, int64_t n, char* __restrict__
 }
 
 // Host copies of the leaf data of device-resident blocks (for stores that
-// are planned from host data): every block of `blocks` re-pointed at them.
+// are planned from host data): each device allocation the blocks point into
+// is copied to the host in one piece, and every block is re-pointed at the
+// copy.
 struct HostLeaves {
     std::vector<hlrc_block> blocks;
     std::vector<std::vector<double>> data;
@@ -853,28 +860,46 @@ struct HostLeaves {
 hlrc_status leaves_to_host(const hlrc_block* blocks, int64_t nb, HostLeaves& h) {
     h.blocks.assign(blocks, blocks + nb);
     h.data.clear();
-    h.data.reserve(size_t(nb) * 3);
-    auto take = [&](const double*& ptr, int64_t ld, int64_t rows, int64_t cols) -> cudaError_t {
-        if (!ptr || rows <= 0 || cols <= 0) return cudaSuccess;
-        const int64_t n = ld * (cols - 1) + rows;
-        h.data.emplace_back(size_t(n));
-        const cudaError_t e = cudaMemcpy(h.data.back().data(), ptr, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost);
-        ptr = h.data.back().data();
-        return e;
+    const AddrRangeFn range = addr_range_fn();
+    if (!range) return fail(HLRC_ERR_CUDA, "leaves_on_device: cuMemGetAddressRange is unavailable");
+    struct Copied { uintptr_t base, end; double* host; };
+    std::vector<Copied> copied;
+    auto rebase = [&](const double*& ptr, int64_t ld, int64_t rows, int64_t cols) -> hlrc_status {
+        if (!ptr || rows <= 0 || cols <= 0) return HLRC_OK;
+        const uintptr_t b = reinterpret_cast<uintptr_t>(ptr);
+        const uintptr_t e = b + uintptr_t(ld * (cols - 1) + rows) * sizeof(double);
+        for (const Copied& c : copied)
+            if (b >= c.base && e <= c.end) {
+                ptr = reinterpret_cast<const double*>(reinterpret_cast<const char*>(c.host) + (b - c.base));
+                return HLRC_OK;
+            }
+        CUdeviceptr base = 0;
+        size_t size = 0;
+        if (range(&base, &size, CUdeviceptr(b)) != CUDA_SUCCESS || e > uintptr_t(base) + size)
+            return fail(HLRC_ERR_ARG, "leaves_on_device: leaf data at %p is not inside a device allocation", ptr);
+        if ((uintptr_t(base) % sizeof(double)) != 0 || (b - uintptr_t(base)) % sizeof(double) != 0)
+            return fail(HLRC_ERR_ARG, "leaves_on_device: leaf data at %p is not 8-byte aligned", ptr);
+        h.data.emplace_back((size + sizeof(double) - 1) / sizeof(double));
+        const cudaError_t ce = cudaMemcpy(h.data.back().data(), reinterpret_cast<const void*>(base), size,
+                                          cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HLRC_ERR_CUDA, "copying device-resident leaves to the host: %s", cudaGetErrorString(ce));
+        }
+        copied.push_back(Copied{uintptr_t(base), uintptr_t(base) + size, h.data.back().data()});
+        ptr = reinterpret_cast<const double*>(reinterpret_cast<const char*>(copied.back().host) + (b - uintptr_t(base)));
+        return HLRC_OK;
     };
     for (hlrc_block& b : h.blocks) {
-        cudaError_t e = cudaSuccess;
+        hlrc_status st = HLRC_OK;
         if (b.kind == HLRC_LEAF_DENSE) {
-            e = take(b.D, b.ldd, b.nrows, b.ncols);
+            st = rebase(b.D, b.ldd, b.nrows, b.ncols);
         } else if (b.rank > 0) {
-            e = take(b.U, b.ldu, b.nrows, b.rank);
-            if (e == cudaSuccess) e = take(b.V, b.ldv, b.ncols, b.rank);
-            if (e == cudaSuccess) e = take(b.sv, b.rank, b.rank, 1);
+            st = rebase(b.U, b.ldu, b.nrows, b.rank);
+            if (st == HLRC_OK) st = rebase(b.V, b.ldv, b.ncols, b.rank);
+            if (st == HLRC_OK) st = rebase(b.sv, b.rank, b.rank, 1);
         }
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(HLRC_ERR_CUDA, "copying device-resident leaves to the host: %s", cudaGetErrorString(e));
-        }
+        if (st != HLRC_OK) return st;
     }
     return HLRC_OK;
 }
@@ -1647,11 +1672,11 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
             if (ntma > 0) {
                 const int grid = std::min(ntma, 2 * M->sms);
                 if (bf)
-                    k_ctform_wtma<FMT_BF16><<<grid, WTMA_THREADS, wtma_smem_c(), s>>>(
+                    k_ctform_wtma<FMT_BF16><<<grid, WTMA_THREADS_C, wtma_smem_c(), s>>>(
                         M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
                         M->w_texp, ws.w_part, M->dev_err, wc);
                 else
-                    k_ctform_wtma<FMT_F16><<<grid, WTMA_THREADS, wtma_smem_c(), s>>>(
+                    k_ctform_wtma<FMT_F16><<<grid, WTMA_THREADS_C, wtma_smem_c(), s>>>(
                         M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
                         M->w_texp, ws.w_part, M->dev_err, wc);
                 M->launches += 1;

@@ -724,6 +724,7 @@ struct hlrc_hbuild_s {
     double* dev_arena = nullptr;   // on_device builds: the leaf data (until fetched)
     int64_t dev_doubles = 0;
     std::vector<GpuLeaf> gl;       // per leaf: offsets into dev_arena
+    std::vector<double> host_arena;   // fetched on_device builds: the same data on the host
     ~hlrc_hbuild_s() { gpu_free(dev_arena); }
 };
 
@@ -934,25 +935,20 @@ extern "C" hlrc_status hlrc_build_fetch(hlrc_hbuild B) {
     if (!B) return fail(HLRC_ERR_ARG, "hlrc_build_fetch: null argument");
     if (!B->dev_arena) return HLRC_OK;
     HBuild& b = B->b;
+    // one bulk copy of the arena; the descriptors keep their offsets
+    B->host_arena.resize(size_t(std::max<int64_t>(1, B->dev_doubles)));
+    const hlrc_status st = gpu_copy_to_host(B->host_arena.data(), B->dev_arena, B->dev_doubles);
+    if (st != HLRC_OK) return st;
+    double* h = B->host_arena.data();
     for (size_t i = 0; i < b.leaves.size(); ++i) {
-        Leaf& l = b.leaves[i];
+        const Leaf& l = b.leaves[i];
         const GpuLeaf& g = B->gl[i];
         hlrc_block& d = b.desc_blocks[i];
-        hlrc_status st = HLRC_OK;
         if (l.kind == HLRC_LEAF_DENSE) {
-            l.D.resize(size_t(l.nrows * l.ncols));
-            if (!l.D.empty()) st = gpu_copy_to_host(l.D.data(), B->dev_arena + g.d, int64_t(l.D.size()));
-            d.D = l.D.empty() ? nullptr : l.D.data();
+            d.D = g.d >= 0 && l.nrows * l.ncols > 0 ? h + g.d : nullptr;
         } else if (l.rank > 0) {
-            l.U.resize(size_t(l.nrows * l.rank));
-            l.V.resize(size_t(l.ncols * l.rank));
-            l.sv.resize(size_t(l.rank));
-            st = gpu_copy_to_host(l.U.data(), B->dev_arena + g.u, int64_t(l.U.size()));
-            if (st == HLRC_OK) st = gpu_copy_to_host(l.V.data(), B->dev_arena + g.v, int64_t(l.V.size()));
-            if (st == HLRC_OK) st = gpu_copy_to_host(l.sv.data(), B->dev_arena + g.s, int64_t(l.sv.size()));
-            d.U = l.U.data(); d.V = l.V.data(); d.sv = l.sv.data();
+            d.U = h + g.u; d.V = h + g.v; d.sv = h + g.s;
         }
-        if (st != HLRC_OK) return st;
     }
     gpu_free(B->dev_arena);
     B->dev_arena = nullptr;

@@ -160,9 +160,7 @@ __device__ __forceinline__ void tree_bar_expect(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 __device__ __forceinline__ void tree_bar_arrive(uint64_t* bar) {
-    uint64_t state;
-    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];\n" : "=l"(state) : "r"(tree_saddr(bar)) : "memory");
-    (void)state;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tree_saddr(bar)) : "memory");
 }
 __device__ __forceinline__ void tree_bulk(double* dst, const double* src, uint32_t bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
@@ -456,6 +454,19 @@ k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __r
         const double* p = part + size_t(g.slot0) + j;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         uint32_t i = 0;
+        // sixteen loads in flight, then the same sums in the same order
+        for (; i + 16 <= g.nslots; i += 16) {
+            double v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = p[size_t(i + q) * g.nc];
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) {
+                s0 += v[q];
+                s1 += v[q + 1];
+                s2 += v[q + 2];
+                s3 += v[q + 3];
+            }
+        }
         for (; i + 4 <= g.nslots; i += 4) {
             s0 += p[size_t(i) * g.nc];
             s1 += p[size_t(i + 1) * g.nc];

@@ -36,12 +36,17 @@
 
 namespace hlrc {
 
-constexpr int WTMA_THREADS = 192;     // 4 epilogue warps, MMA warp, producer warp
+constexpr int WTMA_THREADS = 192;     // N-form: 4 epilogue warps, MMA warp, producer warp
+constexpr int WTMA_THREADS_C = 320;   // T-form: 8 epilogue warps (two per TMEM lane quarter), MMA, producer
+constexpr int WTMA_EPI_C = 256;       // T-form epilogue threads
+constexpr uint32_t WT_NODST = 0xffffffffu;   // T-form column table: no output (padding column)
 constexpr int WTMA_NS_N = 8;          // N-form stages (12 KB each)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
 constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
 constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
-constexpr int wtma_smem_c() { return 1024 + WTMA_NS_C * WIDE_C_STAGE + WT_MAXN * 4 + WT_MAXB * 16 + WIDE_BAR_BYTES; }
+constexpr int wtma_smem_c() {
+    return 1024 + WTMA_NS_C * WIDE_C_STAGE + WT_MAXN * 12 + WT_MAXB * 16 + WIDE_BAR_BYTES;
+}
 
 // 16 consecutive FP32 columns of the warp's 32 lanes (as tmem_ld32)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
@@ -57,17 +62,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// AND of p over the 128 epilogue threads, which all arrive (named barrier 1)
-__device__ __forceinline__ bool bar_and_128(bool p) {
+// AND of p over the T-form's 256 epilogue threads, which all arrive
+// (named barrier 1)
+__device__ __forceinline__ bool bar_and_epi(bool p) {
     uint32_t r;
     asm volatile(
-        "{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\tbar.red.and.pred po, 1, 128, pi;\n\t"
+        "{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\tbar.red.and.pred po, 1, 256, pi;\n\t"
         "selp.u32 %0, 1, 0, po;\n\t}\n"
         : "=r"(r)
         : "r"(uint32_t(p))
         : "memory");
     return r != 0;
 }
+__device__ __forceinline__ void bar_epi() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
 
 // ----------------------------------------------------------------- N-form
 template <int FMT>
@@ -224,18 +231,23 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
 
 // ------------------------------------------------- column-cluster T-form
 template <int FMT>
-__global__ void __launch_bounds__(WTMA_THREADS, 2)
+__global__ void __launch_bounds__(WTMA_THREADS_C, 2)
 k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restrict__ blks,
               const uint32_t* __restrict__ slabs, const WTTile* __restrict__ tiles,
               const __grid_constant__ CUtensorMap tm_s8, const __grid_constant__ CUtensorMap tm_x64,
               uint32_t* __restrict__ ts, const int8_t* __restrict__ texp, float* __restrict__ part, int* err,
               WaitCfg wc) {
     using namespace tc5;
+    constexpr int MMA_WARP = 8, PROD_WARP = 9;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    uint32_t* scol = reinterpret_cast<uint32_t*>(sm + WTMA_NS_C * WIDE_C_STAGE);
-    WTBlk* sblk = reinterpret_cast<WTBlk*>(scol + WT_MAXN);
+    // per stacked column of the current unit: output entry (t row or
+    // partial entry; WT_NODST for padding), factor, static exponent
+    uint32_t* sdst = reinterpret_cast<uint32_t*>(sm + WTMA_NS_C * WIDE_C_STAGE);
+    float* sfac = reinterpret_cast<float*>(sdst + WT_MAXN);
+    int* sexp = reinterpret_cast<int*>(sfac + WT_MAXN);
+    WTBlk* sblk = reinterpret_cast<WTBlk*>(sexp + WT_MAXN);
     uint64_t* full = reinterpret_cast<uint64_t*>(sblk + WT_MAXB);
     uint64_t* empty = full + WTMA_NS_C;
     uint64_t* tfull = empty + WTMA_NS_C;
@@ -252,19 +264,19 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(tfull + i, 1);
-            mbar_init(tempty + i, 128);
+            mbar_init(tempty + i, WTMA_EPI_C);
         }
         mbar_init(done, 1);
         mbar_init_fence();
     }
-    if (warp == 4) tmem_alloc(tslot, 256);
+    if (warp == MMA_WARP) tmem_alloc(tslot, 256);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t s0 = smem_u32(sm);
 
-    if (warp == 5) {
+    if (warp == PROD_WARP) {
         // ---------------------------------------------------- producer warp
         // lane j stages block j of the unit (its V columns in 8-column
         // boxes); lane 0 also the split rows of x and the stage's byte count
@@ -310,7 +322,7 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
             for (int sd = max(0, last - WTMA_NS_C + 1); sd <= last; ++sd)
                 if (!(wc.skip && sd == 0)) mbar_wait(full + sd % WTMA_NS_C, uint32_t(sd / WTMA_NS_C) & 1u, wc.limit_ns);
         __syncwarp();
-    } else if (warp == 4) {
+    } else if (warp == MMA_WARP) {
         // ------------------------------------------------------- MMA issue
         if (lane == 0) {
             bool ok = true;
@@ -342,66 +354,75 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
         __syncwarp();
     } else {
         // -------------------------------------------------------- epilogue
-        const uint32_t la0 = tmem + (uint32_t(32 * warp) << 16);
-        const int m = 32 * warp + lane;
+        // warps w and w + 4 read TMEM lanes 32 (w % 4) ... (term m = lane
+        // quarter row), alternating 16-column groups; the two lanes of a
+        // vector exchange halves, the high-part lane sums hi + lo for the
+        // even columns, the low-part lane for the odd ones, and each stores
+        // its columns' entries of vector r = m / 2
+        const int et = threadIdx.x;                 // 0 .. 255
+        const uint32_t la0 = tmem + (uint32_t(32 * (warp & 3)) << 16);
+        const int m = 32 * (warp & 3) + lane, r = m >> 1, odd = m & 1;
+        const int half = warp >> 2;
         int i = 0;
         for (int ui = int(blockIdx.x); ui < nunits; ui += int(gridDim.x), ++i) {
             const int buf = i & 1;
-            // all four warps take the same branch (the named barriers below
+            // all eight warps take the same branch (the named barriers below
             // need every one of them)
-            if (!bar_and_128(wide_wait(tfull + buf, uint32_t(i >> 1) & 1u, err, wc.limit_ns))) break;
+            if (!bar_and_epi(wide_wait(tfull + buf, uint32_t(i >> 1) & 1u, err, wc.limit_ns))) break;
             tc_fence_after();
             const WTUnit u = units[ui];
             const int nc = int(u.ncols);
-            // the unit's blocks, and stacked column -> (block, column)
-            if (m < int(u.nblk)) sblk[m] = blks[u.blk0 + m];
-            asm volatile("bar.sync 1, 128;\n" ::: "memory");
-            if (m < WT_MAXN) {
-                uint32_t cm = WT_EMPTY;
+            const bool final_t = u.npieces == 1;
+            if (et < int(u.nblk)) sblk[et] = blks[u.blk0 + et];
+            bar_epi();
+            // stacked column -> output entry, factor, exponent
+            if (et < WT_MAXN) {
+                uint32_t dst = WT_NODST;
+                float fac = 0.f;
+                int ex = 0;
                 for (int j = 0; j < int(u.nblk); ++j) {
-                    const int o = int(sblk[j].off);
-                    if (m >= o && m < o + int(sblk[j].k)) cm = (uint32_t(j) << 16) | uint32_t(m - o);
+                    const WTBlk& b = sblk[j];
+                    const int l = et - int(b.off);
+                    if (l >= 0 && l < int(b.k)) {
+                        fac = b.scale;
+                        if (final_t) {
+                            dst = b.toff + uint32_t(l);
+                            ex = int(texp[dst]);
+                        } else {
+                            dst = b.pbase + uint32_t(u.piece) * b.k + uint32_t(l);
+                        }
+                    }
                 }
-                scol[m] = cm;
+                sdst[et] = dst;
+                sfac[et] = fac;
+                sexp[et] = ex;
             }
-            asm volatile("bar.sync 1, 128;\n" ::: "memory");
-            // lane m holds term m (vector r = m / 2, high or low part) of 16
-            // columns per TMEM load; the two lanes of a vector exchange
-            // halves, the high-part lane sums the even columns, the low-part
-            // lane the odd ones, and each stores its columns' entries of
-            // vector r (t split rows, or FP32 partials of a piece)
+            bar_epi();
             const uint32_t la = la0 + uint32_t(buf) * 128u;
-            const int r = m >> 1, odd = m & 1;
-            for (int c0 = 0; c0 < nc; c0 += WTMA_RED_COLS) {
+            for (int c0 = 16 * half; c0 < nc; c0 += 32) {
                 float f[16];
                 tmem_ld16(la + uint32_t(c0), f);
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const float other = __shfl_xor_sync(0xffffffffu, odd ? f[2 * i] : f[2 * i + 1], 1);
-                    const int n = c0 + 2 * i + odd;
-                    const uint32_t cm = n < nc ? scol[n] : WT_EMPTY;
-                    if (cm == WT_EMPTY) continue;
-                    const WTBlk& b = sblk[cm >> 16];
-                    const int l = int(cm & 0xffffu);
-                    const double v = (double(odd ? f[2 * i + 1] : f[2 * i]) + double(other)) * double(b.scale);
-                    if (u.npieces == 1) {
-                        const size_t e = size_t(b.toff) + size_t(l);
-                        ts[e * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -int(texp[e])));
-                    } else {
-                        const size_t e = size_t(b.pbase) + size_t(u.piece) * b.k + size_t(l);
-                        part[e * WIDE_RHS + r] = float(v);
+                for (int k = 0; k < 8; ++k) {
+                    const float other = __shfl_xor_sync(0xffffffffu, odd ? f[2 * k] : f[2 * k + 1], 1);
+                    const int n = c0 + 2 * k + odd;   // < WT_MAXN: c0 <= 112
+                    const uint32_t dst = sdst[n];
+                    const double v = (double(odd ? f[2 * k + 1] : f[2 * k]) + double(other)) * double(sfac[n]);
+                    if (dst != WT_NODST) {
+                        if (final_t) ts[size_t(dst) * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -sexp[n]));
+                        else part[size_t(dst) * WIDE_RHS + r] = float(v);
                     }
                 }
             }
-            // the next unit's tables overwrite these only after every lane is done
-            asm volatile("bar.sync 1, 128;\n" ::: "memory");
             tc_fence_before();
             mbar_arrive(tempty + buf);
+            // the next unit's tables overwrite these only after every thread is done
+            bar_epi();
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == MMA_WARP) {
         tc_fence_after();
         tmem_dealloc(tmem, 256);
     }
