@@ -73,23 +73,53 @@ def test_device_build_matches_host_build(name):
     M2.free()
 
 
+def _leaf_data(hm):
+    """All leaf entries of a host-resident build, concatenated."""
+    parts = []
+    for b in _blocks(hm):
+        if b.kind == 0:
+            parts.append(np.ctypeslib.as_array(b.D, shape=(b.ldd * b.ncols,)).copy())
+        elif b.rank > 0:
+            parts.append(np.ctypeslib.as_array(b.U, shape=(b.ldu * b.rank,)).copy())
+            parts.append(np.ctypeslib.as_array(b.V, shape=(b.ldv * b.rank,)).copy())
+    return np.concatenate(parts)
+
+
+def test_device_build_is_deterministic():
+    p = hlr.Problem.exp3d(3500, seed=4, on_device=True)
+    a = hlr.build(p).fetch()
+    b = hlr.build(p).fetch()
+    assert [x.rank for x in _blocks(a)] == [x.rank for x in _blocks(b)]
+    da, db = _leaf_data(a), _leaf_data(b)
+    assert da.shape == db.shape
+    assert np.array_equal(da, db), float(np.abs(da - db).max())
+
+
 def test_device_leaves_in_reduced_precision_and_batches():
     probs = [hlr.Problem.exp3d(n, seed=s, on_device=True) for n, s in ((2000, 3), (3500, 4))]
     hds = [hlr.build(p) for p in probs]
     hhs = [hlr.build(hlr.Problem.exp3d(p.n, seed=p.seed, on_device=True)).fetch() for p in probs]
     x = np.random.default_rng(6).standard_normal(hds[1].n)
-    for prec in ("mixed", "f16", "bfp"):
-        a = hlr.upload(hds[1], precision=prec)         # host copies made inside the upload
-        b = hlr.upload(hhs[1], precision=prec)
-        ya = torch.zeros(hds[1].n, dtype=torch.float64, device="cuda")
-        yb = torch.zeros_like(ya)
-        xt = torch.from_numpy(x).cuda()
-        hlr.mul_vec(1.0, 0, a, xt, ya)
-        hlr.mul_vec(1.0, 0, b, xt, yb)
+    xt = torch.from_numpy(x).cuda()
+
+    def product(M):
+        y = torch.zeros(hds[1].n, dtype=torch.float64, device="cuda")
+        hlr.mul_vec(1.0, 0, M, xt, y)
         torch.cuda.synchronize()
-        assert np.array_equal(ya.cpu().numpy(), yb.cpu().numpy()), prec
-        a.free()
-        b.free()
+        M.free()
+        return y.cpu().numpy()
+
+    precs = ("mixed", "f16", "bfp")
+    # reduced precisions: the upload makes host copies of the device leaves
+    ya = {prec: product(hlr.upload(hds[1], precision=prec)) for prec in precs}
+    yb = {prec: product(hlr.upload(hhs[1], precision=prec)) for prec in precs}
+    hds[1].fetch()
+    for prec in precs:
+        # the same leaves copied by the upload or fetched: the same store
+        assert np.array_equal(product(hlr.upload(hds[1], precision=prec)), ya[prec]), prec
+        # another device build of the same problem
+        assert np.array_equal(yb[prec], ya[prec]), prec
+    hds[1] = hlr.build(probs[1])
     pad = 3584
     A = hlr.upload_batch(hds, precision="f64", pad_to=pad)
     B = hlr.upload_batch(hhs, precision="f64", pad_to=pad)
