@@ -177,6 +177,7 @@ struct hlrc_hmat_s {
     int w_nunits = 0, w_ngroups = 0;
     int64_t w_npart = 0;
     const WTUnit* w_units_tma = nullptr;   // units whose tiles are all full: TMA kernel
+    const WCDst* w_ctab = nullptr;         // their column tables (WT_MAXN entries per unit)
     int w_nunits_tma = 0;
     bool tma = false;                      // store maps valid (full-tile TMA kernels usable)
     int sms = 148;                         // multiprocessors of the device (persistent grids)
@@ -1164,11 +1165,31 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
             W.units = tma_u;
             W.units.insert(W.units.end(), cp_u.begin(), cp_u.end());
         }
+        // the full-tile units' column tables (WT_MAXN entries each): output
+        // entry, factor and exponent of every stacked column
+        std::vector<WCDst> ctab(size_t(hp->w_nunits_tma) * WT_MAXN, WCDst{WT_NODST, 0.f, 0, 0u});
+        for (int ui = 0; ui < hp->w_nunits_tma; ++ui) {
+            const WTUnit& u = W.units[size_t(ui)];
+            for (int j = 0; j < u.nblk; ++j) {
+                const WTBlk& b = W.blks[size_t(u.blk0) + size_t(j)];
+                for (int l = 0; l < b.k; ++l) {
+                    WCDst& d = ctab[size_t(ui) * WT_MAXN + size_t(b.off) + size_t(l)];
+                    d.fac = b.scale;
+                    if (u.npieces == 1) {
+                        d.dst = b.toff + uint32_t(l);
+                        d.exp = W.t_exp[size_t(d.dst)];
+                    } else {
+                        d.dst = b.pbase + uint32_t(u.piece) * b.k + uint32_t(l);
+                    }
+                }
+            }
+        }
         size_t wb = 0;
         auto take = [&](size_t b) { const size_t o_ = wb; wb = align_up(wb + b, 256); return o_; };
         const size_t o_u = take(W.units.size() * sizeof(WTUnit)), o_b = take(W.blks.size() * sizeof(WTBlk)),
                      o_s = take(W.slabs.size() * sizeof(uint32_t)), o_t = take(W.tiles.size() * sizeof(WTTile)),
-                     o_g = take(W.groups.size() * sizeof(TGroup)), o_e = take(W.t_exp.size());
+                     o_g = take(W.groups.size() * sizeof(TGroup)), o_e = take(W.t_exp.size()),
+                     o_c = take(ctab.size() * sizeof(WCDst));
         e = cudaMalloc(&hp->w_static, std::max<size_t>(wb, 256));
         if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_u, W.units.data(), W.units.size() * sizeof(WTUnit), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_b, W.blks.data(), W.blks.size() * sizeof(WTBlk), cudaMemcpyHostToDevice);
@@ -1177,6 +1198,8 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         if (e == cudaSuccess && !W.groups.empty())
             e = cudaMemcpy(hp->w_static + o_g, W.groups.data(), W.groups.size() * sizeof(TGroup), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(hp->w_static + o_e, W.t_exp.data(), W.t_exp.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !ctab.empty())
+            e = cudaMemcpy(hp->w_static + o_c, ctab.data(), ctab.size() * sizeof(WCDst), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
             cudaGetLastError();
             cudaFree(hp->w_static);
@@ -1192,6 +1215,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         hp->w_tiles = reinterpret_cast<const WTTile*>(hp->w_static + o_t);
         hp->w_groups = reinterpret_cast<const TGroup*>(hp->w_static + o_g);
         hp->w_texp = reinterpret_cast<const int8_t*>(hp->w_static + o_e);
+        hp->w_ctab = reinterpret_cast<const WCDst*>(hp->w_static + o_c);
         hp->w_nunits = int(W.units.size()) - hp->w_nunits_tma;
         hp->w_ngroups = int(W.groups.size());
         hp->w_npart = W.npart;
@@ -1673,12 +1697,12 @@ hlrc_status run_wide(hlrc_hmat M, const Workspace& ws, double alpha, const doubl
                 const int grid = std::min(ntma, 2 * M->sms);
                 if (bf)
                     k_ctform_wtma<FMT_BF16><<<grid, WTMA_THREADS_C, wtma_smem_c(), s>>>(
-                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
-                        M->w_texp, ws.w_part, M->dev_err, wc);
+                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->w_ctab, M->tm_s8, ws.tm_x64,
+                        ws.w_ts, ws.w_part, M->dev_err, wc);
                 else
                     k_ctform_wtma<FMT_F16><<<grid, WTMA_THREADS_C, wtma_smem_c(), s>>>(
-                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->tm_s8, ws.tm_x64, ws.w_ts,
-                        M->w_texp, ws.w_part, M->dev_err, wc);
+                        M->w_units_tma, ntma, M->w_blks, M->w_slabs, M->w_tiles, M->w_ctab, M->tm_s8, ws.tm_x64,
+                        ws.w_ts, ws.w_part, M->dev_err, wc);
                 M->launches += 1;
             }
             if (ncp > 0) {

@@ -39,14 +39,11 @@ namespace hlrc {
 constexpr int WTMA_THREADS = 192;     // N-form: 4 epilogue warps, MMA warp, producer warp
 constexpr int WTMA_THREADS_C = 320;   // T-form: 8 epilogue warps (two per TMEM lane quarter), MMA, producer
 constexpr int WTMA_EPI_C = 256;       // T-form epilogue threads
-constexpr uint32_t WT_NODST = 0xffffffffu;   // T-form column table: no output (padding column)
 constexpr int WTMA_NS_N = 8;          // N-form stages (12 KB each)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
 constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
 constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
-constexpr int wtma_smem_c() {
-    return 1024 + WTMA_NS_C * WIDE_C_STAGE + WT_MAXN * 12 + WT_MAXB * 16 + WIDE_BAR_BYTES;
-}
+constexpr int wtma_smem_c() { return 1024 + WTMA_NS_C * WIDE_C_STAGE + 2 * WT_MAXN * 16 + WIDE_BAR_BYTES; }
 
 // 16 consecutive FP32 columns of the warp's 32 lanes (as tmem_ld32)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
@@ -233,22 +230,19 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
 template <int FMT>
 __global__ void __launch_bounds__(WTMA_THREADS_C, 2)
 k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restrict__ blks,
-              const uint32_t* __restrict__ slabs, const WTTile* __restrict__ tiles,
+              const uint32_t* __restrict__ slabs, const WTTile* __restrict__ tiles, const WCDst* __restrict__ ctab,
               const __grid_constant__ CUtensorMap tm_s8, const __grid_constant__ CUtensorMap tm_x64,
-              uint32_t* __restrict__ ts, const int8_t* __restrict__ texp, float* __restrict__ part, int* err,
-              WaitCfg wc) {
+              uint32_t* __restrict__ ts, float* __restrict__ part, int* err, WaitCfg wc) {
     using namespace tc5;
     constexpr int MMA_WARP = 8, PROD_WARP = 9;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    // per stacked column of the current unit: output entry (t row or
-    // partial entry; WT_NODST for padding), factor, static exponent
-    uint32_t* sdst = reinterpret_cast<uint32_t*>(sm + WTMA_NS_C * WIDE_C_STAGE);
-    float* sfac = reinterpret_cast<float*>(sdst + WT_MAXN);
-    int* sexp = reinterpret_cast<int*>(sfac + WT_MAXN);
-    WTBlk* sblk = reinterpret_cast<WTBlk*>(sexp + WT_MAXN);
-    uint64_t* full = reinterpret_cast<uint64_t*>(sblk + WT_MAXB);
+    // two buffers of a unit's column table (output entry, factor, static
+    // exponent per stacked column), the next unit's copied in while the
+    // current one is written out
+    WCDst* stab = reinterpret_cast<WCDst*>(sm + WTMA_NS_C * WIDE_C_STAGE);
+    uint64_t* full = reinterpret_cast<uint64_t*>(stab + 2 * WT_MAXN);
     uint64_t* empty = full + WTMA_NS_C;
     uint64_t* tfull = empty + WTMA_NS_C;
     uint64_t* tempty = tfull + 2;
@@ -358,46 +352,36 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
         // quarter row), alternating 16-column groups; the two lanes of a
         // vector exchange halves, the high-part lane sums hi + lo for the
         // even columns, the low-part lane for the odd ones, and each stores
-        // its columns' entries of vector r = m / 2
+        // its columns' entries of vector r = m / 2.  The column tables come
+        // from the host-built table (WT_MAXN entries per unit), copied one
+        // unit ahead.
         const int et = threadIdx.x;                 // 0 .. 255
         const uint32_t la0 = tmem + (uint32_t(32 * (warp & 3)) << 16);
         const int m = 32 * (warp & 3) + lane, r = m >> 1, odd = m & 1;
         const int half = warp >> 2;
+        auto prefetch = [&](int uix, int b) {
+            if (uix < nunits && et < WT_MAXN)
+                tc5::cp16(smem_u32(stab + b * WT_MAXN + et), ctab + size_t(uix) * WT_MAXN + et, 16u);
+            tc5::cp_commit();
+        };
+        prefetch(int(blockIdx.x), 0);
+        WTUnit un = units[blockIdx.x];
         int i = 0;
         for (int ui = int(blockIdx.x); ui < nunits; ui += int(gridDim.x), ++i) {
             const int buf = i & 1;
+            const WTUnit u = un;
+            const int nxt = ui + int(gridDim.x);
+            if (nxt < nunits) un = units[nxt];
             // all eight warps take the same branch (the named barriers below
             // need every one of them)
             if (!bar_and_epi(wide_wait(tfull + buf, uint32_t(i >> 1) & 1u, err, wc.limit_ns))) break;
             tc_fence_after();
-            const WTUnit u = units[ui];
+            prefetch(nxt, buf ^ 1);
+            tc5::cp_wait<1>();   // this unit's table has landed (own copies) ...
+            bar_epi();      // ... and everyone's
+            const WCDst* tab = stab + buf * WT_MAXN;
             const int nc = int(u.ncols);
             const bool final_t = u.npieces == 1;
-            if (et < int(u.nblk)) sblk[et] = blks[u.blk0 + et];
-            bar_epi();
-            // stacked column -> output entry, factor, exponent
-            if (et < WT_MAXN) {
-                uint32_t dst = WT_NODST;
-                float fac = 0.f;
-                int ex = 0;
-                for (int j = 0; j < int(u.nblk); ++j) {
-                    const WTBlk& b = sblk[j];
-                    const int l = et - int(b.off);
-                    if (l >= 0 && l < int(b.k)) {
-                        fac = b.scale;
-                        if (final_t) {
-                            dst = b.toff + uint32_t(l);
-                            ex = int(texp[dst]);
-                        } else {
-                            dst = b.pbase + uint32_t(u.piece) * b.k + uint32_t(l);
-                        }
-                    }
-                }
-                sdst[et] = dst;
-                sfac[et] = fac;
-                sexp[et] = ex;
-            }
-            bar_epi();
             const uint32_t la = la0 + uint32_t(buf) * 128u;
             for (int c0 = 16 * half; c0 < nc; c0 += 32) {
                 float f[16];
@@ -405,20 +389,20 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const float other = __shfl_xor_sync(0xffffffffu, odd ? f[2 * k] : f[2 * k + 1], 1);
-                    const int n = c0 + 2 * k + odd;   // < WT_MAXN: c0 <= 112
-                    const uint32_t dst = sdst[n];
-                    const double v = (double(odd ? f[2 * k + 1] : f[2 * k]) + double(other)) * double(sfac[n]);
-                    if (dst != WT_NODST) {
-                        if (final_t) ts[size_t(dst) * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -sexp[n]));
-                        else part[size_t(dst) * WIDE_RHS + r] = float(v);
+                    const WCDst d = tab[c0 + 2 * k + odd];   // < WT_MAXN: c0 <= 112
+                    const double v = (double(odd ? f[2 * k + 1] : f[2 * k]) + double(other)) * double(d.fac);
+                    if (d.dst != WT_NODST) {
+                        if (final_t) ts[size_t(d.dst) * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -d.exp));
+                        else part[size_t(d.dst) * WIDE_RHS + r] = float(v);
                     }
                 }
             }
             tc_fence_before();
             mbar_arrive(tempty + buf);
-            // the next unit's tables overwrite these only after every thread is done
+            // the next prefetch overwrites this buffer only after every thread is done
             bar_epi();
         }
+        tc5::cp_wait<0>();   // no copy in flight at exit
     }
     tc_fence_before();
     __syncthreads();

@@ -259,6 +259,18 @@ struct WTBlk {
     uint32_t pbase;        // pieces: partial entry of piece i, column l = pbase + i * k + l
 };
 static_assert(sizeof(WTBlk) == 16, "WTBlk is 16 bytes");
+// T-form column table of a full-tile unit (WT_MAXN entries per unit, unit
+// by unit): per stacked column its output entry (t row or partial entry;
+// WT_NODST for padding), the V chunks' scale and the t entry's exponent.
+struct WCDst {
+    uint32_t dst;
+    float fac;
+    int32_t exp;
+    uint32_t pad;
+};
+static_assert(sizeof(WCDst) == 16, "WCDst is 16 bytes");
+constexpr uint32_t WT_NODST = 0xffffffffu;   // WCDst.dst of a padding column
+
 struct WTTile {
     uint32_t v_off;        // first x entry of the column tile
     uint16_t rows;
