@@ -681,7 +681,8 @@ hlrc_status enable_tc_smem(int dev) {
                                    tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_bfp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_n(true)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_bfp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_n(false)));
-    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_bfp, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_t()));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_bfp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_t(true)));
+    HLRC_CUDA(cudaFuncSetAttribute(k_ttform_bfp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_t(false)));
     done.push_back(dev);
     return HLRC_OK;
 }
@@ -1554,11 +1555,15 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                         ++nl;
                     }
                 } else if (M->precision == HLRC_PREC_BFP) {
-                    const int n24 = tp.nmseg[FMT_I24];
-                    if (n24 + tp.nmseg[FMT_I16] > 0) {
-                        k_ttform_bfp<<<n24 + tp.nmseg[FMT_I16], TC_WARPS * 32, bq_smem_t(), s>>>(
-                            tp.mseg[FMT_I24], n24, tp.mseg[FMT_I16], tp.mcol, M->store, vec(tp.in), om,
-                            reinterpret_cast<float*>(ws.mr_part), alpha, add);
+                    float* fpart = reinterpret_cast<float*>(ws.mr_part);
+                    if (tp.nmseg[FMT_I24] > 0) {
+                        k_ttform_bfp<true><<<tp.nmseg[FMT_I24], TC_WARPS * 32, bq_smem_t(true), s>>>(
+                            tp.mseg[FMT_I24], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
+                        ++nl;
+                    }
+                    if (tp.nmseg[FMT_I16] > 0) {
+                        k_ttform_bfp<false><<<tp.nmseg[FMT_I16], TC_WARPS * 32, bq_smem_t(false), s>>>(
+                            tp.mseg[FMT_I16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
                         ++nl;
                     }
                 } else {

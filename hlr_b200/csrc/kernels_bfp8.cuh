@@ -36,14 +36,15 @@ constexpr int BQ_STAGE_N16 = TC_STAGE_N16;                        // as FP16
 constexpr int BQ_STAGE_N24 = 32 * TC_A16_STRIDE + 32 * BQ_LO_STRIDE + 32 * TC_V_STRIDE + 32 * 4;
 constexpr int BQ_STAGE_T16 = TC_STAGE_T16;
 constexpr int BQ_STAGE_T24 = 32 * TC_A16_STRIDE + 32 * BQ_LO_STRIDE + 32 * 8;
-constexpr int BQ_STAGE_T = BQ_STAGE_T24;                          // the T-form grid takes both formats
 
 // dynamic shared memory of a launch: per warp a ring of stages, plus the
 // widened low-byte plane for 24-bit columns
 constexpr int bq_smem_n(bool i24) {
     return TC_WARPS * (TC_STAGES * (i24 ? BQ_STAGE_N24 : BQ_STAGE_N16) + (i24 ? BQ_PLANE : 0));
 }
-constexpr int bq_smem_t() { return TC_WARPS * (TC_STAGES * BQ_STAGE_T + BQ_PLANE); }
+constexpr int bq_smem_t(bool i24) {
+    return TC_WARPS * (TC_STAGES * (i24 ? BQ_STAGE_T24 : BQ_STAGE_T16) + (i24 ? BQ_PLANE : 0));
+}
 
 // FP16 pairs 1024 + byte of the two 16-bit words of r: high bytes, low bytes
 __device__ __forceinline__ uint32_t plane_hi(uint32_t r) { return __byte_perm(r, 0x64646464u, 0x4341); }
@@ -276,9 +277,10 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
     constexpr int NT = I24 ? 3 : 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * BQ_STAGE_T + BQ_PLANE);
-    uint8_t* lo_plane = ring + TC_STAGES * BQ_STAGE_T;
-    constexpr int TABOFF = BQ_PLANE + 32 * BQ_LO_STRIDE;   // column table of a stage
+    constexpr int STAGE = I24 ? BQ_STAGE_T24 : BQ_STAGE_T16;
+    uint8_t* ring = smem + warp * (TC_STAGES * STAGE + (I24 ? BQ_PLANE : 0));
+    uint8_t* lo_plane = ring + TC_STAGES * STAGE;             // 24-bit: this warp's widened bytes
+    constexpr int TABOFF = I24 ? BQ_PLANE + 32 * BQ_LO_STRIDE : BQ_PLANE;   // column table of a stage
     // x entries of the lane: rows 16kt + 2t + {0, 1, 8, 9} (kt < 4), right-hand side g
     double xv[4][4];
     int E = 0;
@@ -318,7 +320,7 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
     warp_stream(
         (ncols + 31) / 32, warp,
         [&](int slot, int st) {
-            uint8_t* sa = ring + slot * BQ_STAGE_T;
+            uint8_t* sa = ring + slot * STAGE;
             const int c0 = 32 * st;
             stage_bfp<I24>(sa, base, c0, ncols, sg.ld, lane);
             reinterpret_cast<MCol*>(sa + TABOFF)[lane] = mc;
@@ -326,7 +328,7 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
             mc = cn < ncols ? ld_mcol(ctab + cn) : MCol{0u, 0.f};
         },
         [&](int slot, int st) {
-            const uint8_t* sa = ring + slot * BQ_STAGE_T;
+            const uint8_t* sa = ring + slot * STAGE;
             if constexpr (I24) {
                 widen_lo(sa + BQ_PLANE, lo_plane, lane);
                 __syncwarp();
@@ -380,16 +382,15 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
         });
 }
 
-// One tile T-form pass of a BFP store in one grid: the first n24 CTAs take
-// the 24-bit runs, the others the 16-bit runs (disjoint outputs).  Dynamic
-// shared memory: bq_smem_t().
+// Tile T-form of the runs of one BFP format (the 24-bit and the 16-bit runs
+// write disjoint outputs and run as two grids, each with its own stage
+// size).  Dynamic shared memory: bq_smem_t(I24).
+template <bool I24>
 __global__ void __launch_bounds__(TC_WARPS * 32)
-k_ttform_bfp(const MSeg* __restrict__ segs24, int n24, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
-             const uint8_t* __restrict__ A, const double* __restrict__ vin, OutMap om, float* __restrict__ part,
-             double alpha, int add) {
+k_ttform_bfp(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
+             const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
-    if (int(blockIdx.x) < n24) ttform_bfp<true>(segs24[blockIdx.x], smem, cols, A, vin, om, part, alpha, add);
-    else ttform_bfp<false>(segs16[blockIdx.x - n24], smem, cols, A, vin, om, part, alpha, add);
+    ttform_bfp<I24>(segs[blockIdx.x], smem, cols, A, vin, om, part, alpha, add);
 }
 
 }  // namespace hlrc
