@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(BT) k_dense(const DenseTask* __restrict__ task
 }
 
 // ------------------------------------------------------------------ ACA
-// dynamic shared memory: cap doubles (pivot row / column coefficients),
-// cap doubles (dot products), ceil(n / 32) words (used columns)
+// dynamic shared memory: cap doubles (pivot row / column coefficients) and
+// ceil(n / 32) words (used columns)
 __global__ void __launch_bounds__(BT) k_aca(LrTask* __restrict__ tasks, DevProblem P, double* __restrict__ scr,
                                             double eps, int* __restrict__ err) {
     extern __shared__ double dyn[];
@@ -155,6 +155,8 @@ __global__ void __launch_bounds__(BT) k_aca(LrTask* __restrict__ tasks, DevProbl
         block_argmax(amax, pr, redv, redi);
         if (pr < 0) break;             // no comparable entry (NaN column)
         const double maxv = col[pr];   // written by the thread that owns pr, visible after the barriers
+        // every thread has read the pivot before its owner scales it below
+        __syncthreads();
         if (fabs(maxv) <= zero_val) break;
         const double inv = 1.0 / maxv;
         double ss = 0.0;
