@@ -7,6 +7,7 @@
 // product is a fixed sequence of 2-4 batched passes over a flattened layout,
 // and every output tile is written by exactly one CTA, so the result is
 // deterministic and needs no atomics.
+#include <cfloat>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -1175,13 +1176,15 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
                 const WTBlk& b = W.blks[size_t(u.blk0) + size_t(j)];
                 for (int l = 0; l < b.k; ++l) {
                     WCDst& d = ctab[size_t(ui) * WT_MAXN + size_t(b.off) + size_t(l)];
-                    d.fac = b.scale;
                     if (u.npieces == 1) {
                         d.dst = b.toff + uint32_t(l);
                         d.exp = W.t_exp[size_t(d.dst)];
                     } else {
                         d.dst = b.pbase + uint32_t(u.piece) * b.k + uint32_t(l);
                     }
+                    // chunk scale times 2^-c, kept inside the FP32 normal range
+                    const double f = std::ldexp(double(b.scale), -d.exp);
+                    d.fac = f == 0.0 ? 0.f : float(std::min(std::max(f, double(FLT_MIN)), double(FLT_MAX)));
                 }
             }
         }

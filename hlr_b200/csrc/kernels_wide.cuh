@@ -142,6 +142,20 @@ __device__ __forceinline__ uint32_t wide_split(double v) {
     return uint32_t(hi) | (uint32_t(lo) << 16);
 }
 
+// the same from an FP32 value (FP32 keeps 24 bits, the split 22 or 16)
+template <int FMT>
+__device__ __forceinline__ uint32_t wide_split_f(float v) {
+    if constexpr (FMT == FMT_F16) {
+        const __half hi = __float2half_rn(v);
+        const __half lo = __float2half_rn(v - __half2float(hi));
+        return uint32_t(__half_as_ushort(hi)) | (uint32_t(__half_as_ushort(lo)) << 16);
+    } else {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        return uint32_t(__bfloat16_as_ushort(hi)) | (uint32_t(__bfloat16_as_ushort(lo)) << 16);
+    }
+}
+
 // exponent of the largest |v| (ilogb), or INT_MIN-like sentinel for 0
 constexpr int WIDE_NOEXP = -100000;
 __device__ __forceinline__ int wide_ilogb(double a) { return a > 0.0 ? ilogb(a) : WIDE_NOEXP; }

@@ -390,10 +390,11 @@ k_ctform_wtma(const WTUnit* __restrict__ units, int nunits, const WTBlk* __restr
                 for (int k = 0; k < 8; ++k) {
                     const float other = __shfl_xor_sync(0xffffffffu, odd ? f[2 * k] : f[2 * k + 1], 1);
                     const WCDst d = tab[c0 + 2 * k + odd];   // < WT_MAXN: c0 <= 112
-                    const double v = (double(odd ? f[2 * k + 1] : f[2 * k]) + double(other)) * double(d.fac);
+                    // hi + lo terms, times the chunk scale and (t rows) 2^-c: FP32
+                    const float v = ((odd ? f[2 * k + 1] : f[2 * k]) + other) * d.fac;
                     if (d.dst != WT_NODST) {
-                        if (final_t) ts[size_t(d.dst) * (WIDE_TERMS / 2) + r] = wide_split<FMT>(ldexp(v, -d.exp));
-                        else part[size_t(d.dst) * WIDE_RHS + r] = float(v);
+                        if (final_t) ts[size_t(d.dst) * (WIDE_TERMS / 2) + r] = wide_split_f<FMT>(v);
+                        else part[size_t(d.dst) * WIDE_RHS + r] = v;
                     }
                 }
             }

@@ -261,7 +261,8 @@ struct WTBlk {
 static_assert(sizeof(WTBlk) == 16, "WTBlk is 16 bytes");
 // T-form column table of a full-tile unit (WT_MAXN entries per unit, unit
 // by unit): per stacked column its output entry (t row or partial entry;
-// WT_NODST for padding), the V chunks' scale and the t entry's exponent.
+// WT_NODST for padding) and its factor: the V chunks' scale, times 2^-c of
+// the t entry for final outputs (a power of two in FP32 range).
 struct WCDst {
     uint32_t dst;
     float fac;
