@@ -57,6 +57,19 @@ k_ttfinish_f64_mr(const TGroup* __restrict__ groups, int ngroups, const double* 
         const double2* p = p0 + q;
         double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
         uint32_t i = 0;
+        // sixteen loads in flight, then the same sums in the same order
+        for (; i + 16 <= g.nslots; i += 16) {
+            double2 v[16];
+#pragma unroll
+            for (int a = 0; a < 16; ++a) v[a] = __ldcs(p + size_t(i + a) * n2);
+#pragma unroll
+            for (int a = 0; a < 16; a += 4) {
+                s0.x += v[a].x; s0.y += v[a].y;
+                s1.x += v[a + 1].x; s1.y += v[a + 1].y;
+                s2.x += v[a + 2].x; s2.y += v[a + 2].y;
+                s3.x += v[a + 3].x; s3.y += v[a + 3].y;
+            }
+        }
         for (; i + 4 <= g.nslots; i += 4) {
             const double2 a = __ldcs(p + size_t(i) * n2), b = __ldcs(p + size_t(i + 1) * n2);
             const double2 c = __ldcs(p + size_t(i + 2) * n2), d = __ldcs(p + size_t(i + 3) * n2);

@@ -248,6 +248,16 @@ k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* p
         const float4* p = p0 + q;
         double s[4][4] = {};
         uint32_t i = 0;
+        // sixteen loads in flight, then the same sums in the same order
+        for (; i + 16 <= g.nslots; i += 16) {
+            float4 v[16];
+#pragma unroll
+            for (int a = 0; a < 16; ++a) v[a] = __ldcs(p + size_t(i + a) * n4);
+#pragma unroll
+            for (int a = 0; a < 16; ++a) {
+                s[a & 3][0] += v[a].x; s[a & 3][1] += v[a].y; s[a & 3][2] += v[a].z; s[a & 3][3] += v[a].w;
+            }
+        }
         for (; i + 4 <= g.nslots; i += 4) {
 #pragma unroll
             for (int a = 0; a < 4; ++a) {

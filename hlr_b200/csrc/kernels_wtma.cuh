@@ -39,7 +39,10 @@ namespace hlrc {
 constexpr int WTMA_THREADS = 192;     // N-form: 4 epilogue warps, MMA warp, producer warp
 constexpr int WTMA_THREADS_C = 320;   // T-form: 8 epilogue warps (two per TMEM lane quarter), MMA, producer
 constexpr int WTMA_EPI_C = 256;       // T-form epilogue threads
-constexpr int WTMA_NS_N = 8;          // N-form stages (12 KB each)
+#ifndef HLRC_WTMA_NS_N
+#define HLRC_WTMA_NS_N 8
+#endif
+constexpr int WTMA_NS_N = HLRC_WTMA_NS_N;   // N-form stages (12 KB each)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
 constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
 constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
