@@ -269,6 +269,17 @@ k_ttfinish_wide(const TGroup* __restrict__ groups, int ngroups, const float* __r
         const float2* p = reinterpret_cast<const float2*>(part) + (size_t(gr.slot0) + j) * 32 + lane;
         double s0[2] = {0.0, 0.0}, s1[2] = {0.0, 0.0};
         uint32_t i = 0;
+        // eight loads in flight, then the same sums in the same order
+        for (; i + 8 <= gr.nslots; i += 8) {
+            float2 v[8];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) v[a] = __ldcs(p + size_t(i + a) * step);
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                s0[a & 1] += v[a].x;
+                s1[a & 1] += v[a].y;
+            }
+        }
         for (; i + 2 <= gr.nslots; i += 2) {
             const float2 a = __ldcs(p + size_t(i) * step), b = __ldcs(p + size_t(i + 1) * step);
             s0[0] += a.x; s1[0] += a.y; s0[1] += b.x; s1[1] += b.y;

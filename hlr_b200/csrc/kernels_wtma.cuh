@@ -40,9 +40,9 @@ constexpr int WTMA_THREADS = 192;     // N-form: 4 epilogue warps, MMA warp, pro
 constexpr int WTMA_THREADS_C = 320;   // T-form: 8 epilogue warps (two per TMEM lane quarter), MMA, producer
 constexpr int WTMA_EPI_C = 256;       // T-form epilogue threads
 #ifndef HLRC_WTMA_NS_N
-#define HLRC_WTMA_NS_N 8
+#define HLRC_WTMA_NS_N 6
 #endif
-constexpr int WTMA_NS_N = HLRC_WTMA_NS_N;   // N-form stages (12 KB each)
+constexpr int WTMA_NS_N = HLRC_WTMA_NS_N;   // N-form stages (12 KB each; 3 CTAs per SM at 6)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
 constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
 constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
@@ -78,7 +78,7 @@ __device__ __forceinline__ void bar_epi() { asm volatile("bar.sync 1, 256;\n" ::
 
 // ----------------------------------------------------------------- N-form
 template <int FMT>
-__global__ void __launch_bounds__(WTMA_THREADS, 2)
+__global__ void __launch_bounds__(WTMA_THREADS, 3)
 k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, const __grid_constant__ CUtensorMap tm_a,
              const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_t,
              const int* __restrict__ g, OutMap om, double alpha, int* err, WaitCfg wc) {
@@ -196,28 +196,27 @@ k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, c
     } else {
         // -------------------------------------------------------- epilogue
         // lane m holds term m (vector m / 2, high or low part) of the 64
-        // rows; the two lanes of a vector exchange halves: the high-part
-        // lane sums rows 0-31, the low-part lane rows 32-63
+        // rows, read 16 rows at a time; the two lanes of a vector exchange
+        // their terms, and the high-part lane adds rows 0-31 to y, the
+        // low-part lane rows 32-63
         const uint32_t la = tmem + (uint32_t(32 * warp) << 16);
         const int m = 32 * warp + lane, r = m >> 1;
         const bool lo = (m & 1) != 0;
         const bool ok = __all_sync(0xffffffffu, wide_wait(tfull, 0u, err, wc.limit_ns)) && !wide_aborted(err);
         if (ok) {
             tc_fence_after();
-            float a[32], b[32];
-            tmem_ld32(la, a);
-            tmem_ld32(la + 32u, b);
-            double v[32];
+            const double fr = r < om.nr ? alpha * ldexp(1.0, sg.E - g[r]) : 0.0;
+            double* o = om.base + int64_t(sg.out) * om.rs + int64_t(r) * om.cs;
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const float other = __shfl_xor_sync(0xffffffffu, lo ? a[i] : b[i], 1);
-                v[i] = double(lo ? b[i] : a[i]) + double(other);
-            }
-            if (r < om.nr) {
-                const double f = alpha * ldexp(1.0, sg.E - g[r]);
-                double* o = om.base + int64_t(sg.out + (lo ? 32 : 0)) * om.rs + int64_t(r) * om.cs;
+            for (int q = 0; q < 4; ++q) {
+                float f[16];
+                tmem_ld16(la + uint32_t(16 * q), f);
+                const bool own = (q >= 2) == lo;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) o[int64_t(i) * om.rs] += f * v[i];
+                for (int i = 0; i < 16; ++i) {
+                    const float other = __shfl_xor_sync(0xffffffffu, f[i], 1);
+                    if (own && r < om.nr) o[int64_t(16 * q + i) * om.rs] += fr * (double(f[i]) + double(other));
+                }
             }
         }
     }
