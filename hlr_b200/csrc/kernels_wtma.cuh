@@ -40,9 +40,9 @@ constexpr int WTMA_THREADS = 192;     // N-form: 4 epilogue warps, MMA warp, pro
 constexpr int WTMA_THREADS_C = 320;   // T-form: 8 epilogue warps (two per TMEM lane quarter), MMA, producer
 constexpr int WTMA_EPI_C = 256;       // T-form epilogue threads
 #ifndef HLRC_WTMA_NS_N
-#define HLRC_WTMA_NS_N 6
+#define HLRC_WTMA_NS_N 4
 #endif
-constexpr int WTMA_NS_N = HLRC_WTMA_NS_N;   // N-form stages (12 KB each; 3 CTAs per SM at 6)
+constexpr int WTMA_NS_N = HLRC_WTMA_NS_N;   // N-form stages (12 KB each; 4 CTAs per SM at 4)
 constexpr int WTMA_NS_C = 3;          // T-form stages (32 KB each)
 constexpr int WTMA_RED_COLS = 16;     // T-form epilogue: columns per TMEM load
 constexpr int wtma_smem_n() { return 1024 + WTMA_NS_N * WIDE_N_STAGE + 64 + WIDE_BAR_BYTES; }
@@ -78,7 +78,7 @@ __device__ __forceinline__ void bar_epi() { asm volatile("bar.sync 1, 256;\n" ::
 
 // ----------------------------------------------------------------- N-form
 template <int FMT>
-__global__ void __launch_bounds__(WTMA_THREADS, 3)
+__global__ void __launch_bounds__(WTMA_THREADS, 4)
 k_nform_wtma(const WSeg* __restrict__ segs, const WStage* __restrict__ stages, const __grid_constant__ CUtensorMap tm_a,
              const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_t,
              const int* __restrict__ g, OutMap om, double alpha, int* err, WaitCfg wc) {
