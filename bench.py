@@ -990,7 +990,7 @@ def main():
     ap.add_argument("--shard", action="store_true",
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
     ap.add_argument("--tune-plan", action="store_true", default=None,
-                    help="also tune plan-level choices by re-uploading (default: on for c4 and c5)")
+                    help="also tune plan-level choices by re-uploading (default: on for c1, c4 and c5)")
     ap.add_argument("--host-build", action="store_true",
                     help="assemble the leaves on the host (default: on the GPU for the H-matrix configs)")
     ap.add_argument("--reduced", default="bfp,mixed",
@@ -999,7 +999,7 @@ def main():
     args = ap.parse_args()
     args.reduced = [] if args.reduced in ("", "none") else args.reduced.split(",")
     if args.tune_plan is None:
-        args.tune_plan = args.config in ("c4", "c5")
+        args.tune_plan = args.config in ("c1", "c4", "c5")
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -169,7 +169,7 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
 # ------------------------------------------------------------ plan level
 PLAN_CANDIDATES = {
     # tile T-form outputs with more partials than this are summed in two levels
-    "finish_slots": (16, 8, 32),
+    "finish_slots": (16, 8, 32, 64),
     # 64-vector T-form: tiles per piece of a long column cluster
     "piece_tiles": (32, 16, 8),
 }
