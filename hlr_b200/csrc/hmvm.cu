@@ -1471,10 +1471,10 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             auto nform = [&](auto wc) {
                 constexpr int NW = decltype(wc)::value;
                 if (np.ncta > 0) {   // tree sweep (FP64 plans only)
-                    k_ntree_f64<TREE_WARPS><<<np.ncta, TREE_WARPS * 32, np.tree_smem, s>>>(
-                        np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), np.tree,
-                        reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add, M->dev_err, M->wait_ns,
-                        M->wait_skip);
+                    L(launch_k(ov, k_ntree_f64<TREE_WARPS>, unsigned(np.ncta), TREE_WARPS * 32, np.tree_smem, s,
+                               np.segs[FMT_F64], static_cast<const NChunk*>(np.chunks), np.tree,
+                               reinterpret_cast<const double*>(M->store), vx, vt, vo, alpha, add, M->dev_err,
+                               M->wait_ns, M->wait_skip));
                     return;
                 }
                 if (f64plan && np.nsegs[FMT_F64] > 0)

@@ -217,6 +217,7 @@ k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, Tr
             const double* __restrict__ A, const double* vx, const double* vt, double* out, double alpha, int add,
             int* err, uint64_t wait_ns, int skip) {
     constexpr int TC = TREE_CLUSTER;
+    pdl_trigger();
     cg::cluster_group cl = cg::this_cluster();
     const int rank = int(cl.block_rank());
     const int sub = int(blockIdx.x) / TC;
@@ -272,6 +273,9 @@ k_ntree_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, Tr
     __syncthreads();   // every expectation is set: the one arrival may complete a phase
     if (tid == 0)
         for (int i = 0; i < nlev; ++i) tree_bar_arrive(&bars[i]);
+    // the matrix copies above read static data; the vectors below are
+    // written by the preceding kernel
+    pdl_wait();
     for (int e = t.cta_ext[sub] + tid; e < t.cta_ext[sub + 1]; e += W * 32) {
         const TreeExt x = t.ext[e];
         mirror[x.mirror] = __ldcg((x.v_off & VEC_T) ? vt + (x.v_off & ~VEC_T) : vx + x.v_off);
