@@ -71,51 +71,28 @@ k_nform_f64(const NSeg* __restrict__ segs, const NChunk* __restrict__ chunks, co
     const bool active = r < sg.ld;
     double acc0 = 0.0, acc1 = 0.0;
     pdl_wait();
-    // software pipeline: the loads of chunk c + W are in flight while chunk
-    // c is multiplied, and descriptors are read two chunks ahead (two
-    // operand sets in registers); the sum order is chunk order per warp
-    auto issue = [&](const NChunk& ch, double2 (&m)[NCHUNK], double (&vv)[NCHUNK]) {
+    for (uint32_t c = sg.cb + warp; c < sg.ce; c += W) {
+        const NChunk ch = chunks[c];
         const double* v = (ch.v_off & VEC_T) ? vt + (ch.v_off & ~VEC_T) : vx + ch.v_off;
-        const double* a = A + ch.a_off + r;
+        if (active) {
+            const double* a = A + ch.a_off + r;
+            double2 m[NCHUNK];
+            double vv[NCHUNK];
 #pragma unroll
-        for (int j = 0; j < NCHUNK; ++j) {
-            if (active && j < ch.nc) {
-                m[j] = ld_stream(a + size_t(j) * sg.ld);
-                vv[j] = __ldg(v + j);
-            } else {
-                m[j] = make_double2(0.0, 0.0);
-                vv[j] = 0.0;
+            for (int j = 0; j < NCHUNK; ++j) {
+                if (j < ch.nc) {
+                    m[j] = ld_stream(a + size_t(j) * sg.ld);
+                    vv[j] = __ldg(v + j);
+                } else {
+                    m[j] = make_double2(0.0, 0.0);
+                    vv[j] = 0.0;
+                }
             }
-        }
-    };
-    auto compute = [&](const double2 (&m)[NCHUNK], const double (&vv)[NCHUNK]) {
 #pragma unroll
-        for (int j = 0; j < NCHUNK; ++j) {
-            acc0 = fma(m[j].x, vv[j], acc0);
-            acc1 = fma(m[j].y, vv[j], acc1);
-        }
-    };
-    uint32_t c = sg.cb + warp;
-    if (c < sg.ce) {
-        const NChunk none{0, 0, 0, 0};
-        double2 mA[NCHUNK], mB[NCHUNK];
-        double vA[NCHUNK], vB[NCHUNK];
-        issue(chunks[c], mA, vA);
-        NChunk qn = c + W < sg.ce ? chunks[c + W] : none;
-        for (;;) {
-            const bool hasB = c + W < sg.ce;
-            const NChunk qnn = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
-            if (hasB) issue(qn, mB, vB);
-            compute(mA, vA);
-            if (!hasB) break;
-            c += W;
-            const bool hasA = c + W < sg.ce;
-            const NChunk q3 = c + 2 * W < sg.ce ? chunks[c + 2 * W] : none;
-            if (hasA) issue(qnn, mA, vA);
-            compute(mB, vB);
-            if (!hasA) break;
-            c += W;
-            qn = q3;
+            for (int j = 0; j < NCHUNK; ++j) {
+                acc0 = fma(m[j].x, vv[j], acc0);
+                acc1 = fma(m[j].y, vv[j], acc1);
+            }
         }
     }
     red[warp][r] = acc0;
