@@ -258,7 +258,7 @@ class DeviceMatrix:
     @property
     def tuning(self) -> dict:
         """Launch shapes of this handle's products (hlrc_get_tuning):
-        nform_warps, ttform_warps (4 or 8), mr_min_nrhs, wide_min_nrhs and
+        nform_warps, ttform_warps (4, 8 or 16), mr_min_nrhs, wide_min_nrhs and
         overlap (programmatic dependent launch of the one-vector kernels)."""
         t = _capi.hlrc_tuning()
         check(lib().hlrc_get_tuning(self._h, C.byref(t)), "hlrc_get_tuning")

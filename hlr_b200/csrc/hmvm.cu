@@ -1447,6 +1447,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
                 }
             };
             if (M->ttform_warps == 4) ttform(Warps<4>{});
+            else if (M->ttform_warps == 16) ttform(Warps<16>{});
             else ttform(Warps<8>{});
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
@@ -1496,6 +1497,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
                 }
             };
             if (M->nform_warps == 4) nform(Warps<4>{});
+            else if (M->nform_warps == 16) nform(Warps<16>{});
             else nform(Warps<8>{});
             if (ws.profile) prof_end(M, s);
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
@@ -1988,9 +1990,9 @@ extern "C" hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t) {
 
 extern "C" hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t) {
     if (!M || !t) return fail(HLRC_ERR_ARG, "hlrc_set_tuning: null argument");
-    auto warps_ok = [](int w) { return w == 4 || w == 8; };
+    auto warps_ok = [](int w) { return w == 4 || w == 8 || w == 16; };
     if (!warps_ok(t->nform_warps) || !warps_ok(t->ttform_warps))
-        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: warps per CTA must be 4 or 8 (got %d, %d)", t->nform_warps,
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: warps per CTA must be 4, 8 or 16 (got %d, %d)", t->nform_warps,
                     t->ttform_warps);
     if (t->mr_min_nrhs < 2 || t->mr_min_nrhs > HLRC_MR_NEVER)
         return fail(HLRC_ERR_ARG, "hlrc_set_tuning: mr_min_nrhs must be in [2, %d] (got %d)", HLRC_MR_NEVER,

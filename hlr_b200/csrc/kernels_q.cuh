@@ -259,7 +259,7 @@ __device__ __forceinline__ void npacks_q(uint32_t cb, uint32_t ce, int ld, const
 // and its packs of the 16-bit format F16 (either may be empty), sums them in
 // FP64 and updates y once.
 template <int W, int WIDE, int F16>
-__global__ void __launch_bounds__(W * 32, 3)
+__global__ void __launch_bounds__(W * 32, W >= 16 ? 1 : 3)
 k_nform_q(const NSeg2* __restrict__ segs, const QNPack* __restrict__ packs, const uint8_t* __restrict__ A,
           const double* __restrict__ vx, const double* __restrict__ vt, double* __restrict__ out, double alpha,
           int add) {

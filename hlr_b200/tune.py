@@ -4,8 +4,8 @@ For one matrix, right-hand-side count and operation, ``autotune`` times the
 candidate settings of ``hlrc_tuning`` on the current device and keeps the
 fastest:
 
-* one vector: warps per CTA (4 or 8) of the N-form and of the tile T-form
-  kernels, four combinations;
+* one vector: warps per CTA (4, 8 or 16) of the N-form and of the tile
+  T-form kernels, nine combinations;
 * several vectors: the 8-vector tensor-core kernels against a loop of
   one-vector products (``mr_min_nrhs`` 2 or ``HLRC_MR_NEVER``); with more
   than 8 vectors also the one-pass 64-vector kernels of 16-bit stores
@@ -52,7 +52,7 @@ def signature(M, nrhs: int, op: int, device_name: str) -> str:
 def candidates(current: dict, nrhs: int) -> list:
     """Settings to time; the first is the default for this vector count."""
     if nrhs <= 1:
-        return [dict(current, nform_warps=a, ttform_warps=b) for a in (8, 4) for b in (8, 4)]
+        return [dict(current, nform_warps=a, ttform_warps=b) for a in (8, 4, 16) for b in (8, 4, 16)]
     if nrhs <= 8:
         return [dict(current, mr_min_nrhs=2), dict(current, mr_min_nrhs=HLRC_MR_NEVER)]
     return [dict(current, wide_min_nrhs=9, mr_min_nrhs=2), dict(current, wide_min_nrhs=HLRC_MR_NEVER, mr_min_nrhs=2),

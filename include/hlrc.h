@@ -365,8 +365,9 @@ hlrc_status hlrc_workspace_free(hlrc_workspace ws);
  * winner).  No counterpart in the reference, whose TBB products have no
  * launch shapes; every setting computes the same product (the order of the
  * per-warp partial sums differs, so results agree to rounding).
- *   nform_warps, ttform_warps: warps per CTA (4 or 8) of the one-vector
- *     N-form and tile T-form kernels;
+ *   nform_warps, ttform_warps: warps per CTA (4, 8 or 16) of the one-vector
+ *     N-form and tile T-form kernels (16 for small matrices, where each
+ *     output tile's chain of loads sets the time);
  *   mr_min_nrhs: products with at least this many vectors use the
  *     8-vector tensor-core kernels, smaller ones loop the one-vector kernels
  *     (2..HLRC_MR_NEVER; HLRC_MR_NEVER always loops);

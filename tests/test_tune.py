@@ -26,7 +26,7 @@ class FakeMatrix:
     def set_tuning(self, **kw):
         if set(kw) - set(self._t):
             raise ValueError("unknown key")
-        if kw.get("nform_warps", 8) not in (4, 8) or kw.get("ttform_warps", 8) not in (4, 8):
+        if kw.get("nform_warps", 8) not in (4, 8, 16) or kw.get("ttform_warps", 8) not in (4, 8, 16):
             raise ValueError("bad warps")
         self._t.update(kw)
         self.sets += 1
@@ -45,8 +45,8 @@ def timer_for(M, table):
 
 def test_candidates():
     one = tune.candidates(dict(tune.DEFAULT), 1)
-    assert one[0] == tune.DEFAULT and len(one) == 4
-    assert {(c["nform_warps"], c["ttform_warps"]) for c in one} == {(8, 8), (8, 4), (4, 8), (4, 4)}
+    assert one[0] == tune.DEFAULT and len(one) == 9
+    assert {(c["nform_warps"], c["ttform_warps"]) for c in one} == {(a, b) for a in (4, 8, 16) for b in (4, 8, 16)}
     many = tune.candidates(dict(tune.DEFAULT), 8)
     assert [c["mr_min_nrhs"] for c in many] == [2, HLRC_MR_NEVER]
 
@@ -56,7 +56,7 @@ def test_picks_fastest_and_caches(tmp_path):
     t, calls = timer_for(M, lambda s: 1.0 if s["nform_warps"] == 4 and s["ttform_warps"] == 8 else 2.0)
     path = tmp_path / "tuning.json"
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
-    assert not r["cached"] and len(calls) == 8      # two sweeps of four
+    assert not r["cached"] and len(calls) == 18     # two sweeps of nine
     assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1}
     d = json.loads(path.read_text())
     assert d[r["key"]]["tuning"] == M.tuning
@@ -98,13 +98,13 @@ def test_bad_cache_entries_are_retuned(tmp_path):
     M = FakeMatrix()
     t, calls = timer_for(M, lambda s: 1.0)
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="G")
-    assert not r["cached"] and len(calls) == 8      # two sweeps of four
+    assert not r["cached"] and len(calls) == 18     # two sweeps of nine
     d = json.loads(path.read_text())
     d[r["key"]]["tuning"] = {"nform_warps": 5, "ttform_warps": 8, "mr_min_nrhs": 2}   # rejected by the handle
     path.write_text(json.dumps(d))
     M2 = FakeMatrix()
     t2, calls2 = timer_for(M2, lambda s: 1.0)
-    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 8
+    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 18
 
 
 def test_timer_failure_restores_setting():
