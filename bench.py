@@ -310,10 +310,11 @@ def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int,
     """Times `steps` products of handle M issued by step() on torch's current
     stream: `warmup` untimed products, then the timed region bracketed by a
     barrier and synchronisations, as replays of one CUDA graph of
-    products_per_graph(steps) products (or direct launches).  Per-pass CUDA
-    events of the handle's profiling API are recorded inside the graph and
-    read after the last replay.  Returns a dict with the region's ms, the
-    per-run min / median / max per product, the pass profile, the kernels
+    products_per_graph(steps) products (or direct launches).  The timed
+    products carry no profiling events.  The per-pass profile comes from one
+    more, untimed run with the handle's per-pass CUDA events (recorded as
+    graph nodes when graphs are used).  Returns a dict with the region's ms,
+    the per-run min / median / max per product, the pass profile, the kernels
     launched per product and the clock samples."""
     import torch
     import torch.distributed as dist
@@ -325,8 +326,7 @@ def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int,
     step()                      # one more warm-up product, counting its launches
     torch.cuda.synchronize()
     per_product = M.launch_count() - l0
-    M.set_profiling(True)
-    M.last_profile()  # clear
+    M.set_profiling(False)
     graph, per_graph = None, 0
     if use_graph:
         per_graph = products_per_graph(steps)
@@ -336,9 +336,6 @@ def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int,
                 step()
         graph.replay()          # untimed
         torch.cuda.synchronize()
-        # the capture recorded the pass events as graph nodes: every replay
-        # records them again, and last_profile() after the last timed replay
-        # returns that replay's pass times (reading clears the records)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -365,9 +362,25 @@ def time_products(M, step, steps: int, warmup: int, use_graph: bool, world: int,
     if graph is not None:
         rt = [a.elapsed_time(b) / per_graph for a, b in zip(marks[:-1], marks[1:])]
         runs = {"min": min(rt), "median": statistics.median(rt), "max": max(rt), "runs": len(rt)}
-    prof = M.last_profile()
-    M.set_profiling(False)
     del graph
+    # the pass profile: one untimed run with per-pass events
+    M.set_profiling(True)
+    M.last_profile()  # clear
+    if use_graph:
+        pgraph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(pgraph):
+            for _ in range(per_graph):
+                step()
+        pgraph.replay()
+        torch.cuda.synchronize()
+        prof = M.last_profile()
+        del pgraph
+    else:
+        for _ in range(max(1, min(steps, 4))):
+            step()
+        torch.cuda.synchronize()
+        prof = M.last_profile()
+    M.set_profiling(False)
     return {"ms": ms, "runs": runs, "prof": prof, "per_product": per_product, "launches": launches,
             "per_graph": per_graph, "clocks": clocks.summary()}
 

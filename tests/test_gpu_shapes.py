@@ -14,6 +14,10 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 TOL = {"f64": 1e-13, "f32": 1e-6, "mixed": 1e-6, "f16": 2e-3, "bf16": 1.5e-2, "bfp": 1e-6}
+# the 8-vector BFP kernels accumulate byte-plane products on the FP16 tensor
+# cores in FP32 per 32-column stage: about 1e-7 on top of the store's own
+# error, which VALR sets near 1e-6 on these random leaves
+TOL8 = dict(TOL, bfp=2e-6)
 
 
 def leaves(nrows, ncols, seed):
@@ -69,7 +73,7 @@ def test_rectangular_and_tiny(shape, prec):
         R = Aop @ X
         for j in range(8):
             if np.linalg.norm(R[:, j]) > 0:
-                assert relerr(Yd[:, j].cpu().numpy(), R[:, j]) <= TOL[prec], (prec, op, j)
+                assert relerr(Yd[:, j].cpu().numpy(), R[:, j]) <= TOL8[prec], (prec, op, j)
     assert M.device_error() == 0
     M.free()
 
