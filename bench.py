@@ -463,12 +463,13 @@ def run_ours(args, rank, world, local_rank):
         # 16-bit products, the finish's two-level threshold otherwise
         from hlr_b200.tune import autotune_plan
         knobs = ("piece_tiles",) if prec in ("f16", "bf16") and nrhs > 8 and not uniform and not args.h2 \
-            else ("finish_slots",)
+            else (("near_field", "finish_slots") if nrhs == 1 else ("finish_slots",))
         M, plan_tuned = autotune_plan(
-            lambda p: hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2, plan=p),
-            nrhs=nrhs, knobs=knobs)
+            lambda p: hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2,
+                                 plan=dict(args.plan, **p)),
+            nrhs=nrhs, knobs=knobs, graph=not args.no_graph)
     else:
-        M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2)
+        M = hlr.upload(hm, precision=prec, uniform=uniform, max_nrhs=nrhs, h2=args.h2, plan=args.plan)
     t_upload = time.perf_counter() - tu
     tuned = tune_handle(M, nrhs, args)
     if tuned is not None:
@@ -804,6 +805,9 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+SIDE_PASSES = {"nform_Dx", "h2_Dx"}   # passes launched on the side stream (hlrc_options.near_field)
+
+
 def roofline_from_profile(prof: dict, hbm_peak: float, peak_kind: str, workload: str):
     """Roofline object of the dominant pass of a per-pass CUDA-event profile
     {name: (launches, total ms, bytes/launch)}: the pass that moves the most
@@ -817,7 +821,10 @@ def roofline_from_profile(prof: dict, hbm_peak: float, peak_kind: str, workload:
     achieved = by / (avg_ms / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "traffic": traffic_from_profiles(name, workload), "peak_kind": peak_kind,
-            "bytes_per_launch": by, "avg_ms": avg_ms, "share_of_step": tot_ms / sum(v[1] for v in prof.values())}
+            "bytes_per_launch": by, "avg_ms": avg_ms, "share_of_step": tot_ms / sum(v[1] for v in prof.values()),
+            # the near field on the side stream shares HBM with the low-rank
+            # passes while its events run: its fraction is a lower bound
+            "beside_other_passes": name in SIDE_PASSES}
 
 
 def run_shard(args, rank, world, local_rank):
@@ -960,13 +967,14 @@ def run_shard(args, rank, world, local_rank):
 def tune_handle(M, nrhs: int, args):
     """Launch shapes from the autotuner, before any timed region: warps per
     CTA for one vector, then (nrhs > 1) the 8-vector kernels against a loop
-    of one-vector products.  No cache file: each run times its own device."""
+    of one-vector products.  No cache file: each run times its own device,
+    in CUDA graph replays unless the products are timed without graphs."""
     if args.no_autotune:
         return None
     from hlr_b200.tune import autotune
-    autotune(M, nrhs=1, cache=None)
+    autotune(M, nrhs=1, cache=None, graph=not args.no_graph)
     if nrhs > 1:
-        autotune(M, nrhs=nrhs, cache=None)
+        autotune(M, nrhs=nrhs, cache=None, graph=not args.no_graph)
     return M.tuning
 
 
@@ -1004,6 +1012,8 @@ def main():
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
     ap.add_argument("--tune-plan", action="store_true", default=None,
                     help="also tune plan-level choices by re-uploading (default: on for c1, c4 and c5)")
+    ap.add_argument("--plan", default="", help="plan-level choices k=v[,k=v] (finish_slots, piece_tiles, "
+                    "near_field), before any plan tuning")
     ap.add_argument("--host-build", action="store_true",
                     help="assemble the leaves on the host (default: on the GPU for the H-matrix configs)")
     ap.add_argument("--reduced", default="bfp,mixed",
@@ -1011,6 +1021,7 @@ def main():
                          "(comma list of bfp, mixed, f32, f16, bf16; 'none' for none)")
     args = ap.parse_args()
     args.reduced = [] if args.reduced in ("", "none") else args.reduced.split(",")
+    args.plan = {k: int(v) for k, v in (kv.split("=") for kv in args.plan.split(",") if kv)}
     if args.tune_plan is None:
         args.tune_plan = args.config in ("c1", "c4", "c5")
     args.warmup = max(3, args.warmup)

@@ -217,11 +217,12 @@ def _options(precision="f64", max_nrhs: int = 1, mixed_eps: float = 1e-6, device
     o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     o.max_nrhs, o.mixed_eps, o.device = max_nrhs, mixed_eps, device
     plan = plan or {}
-    unknown = set(plan) - {"finish_slots", "piece_tiles"}
+    unknown = set(plan) - {"finish_slots", "piece_tiles", "near_field"}
     if unknown:
         raise ValueError(f"unknown plan options {sorted(unknown)}")
     o.finish_slots = int(plan.get("finish_slots", 0))
     o.piece_tiles = int(plan.get("piece_tiles", 0))
+    o.near_field = int(plan.get("near_field", 0))
     return o
 
 

@@ -63,7 +63,8 @@ class hlrc_h2_desc(C.Structure):
 
 class hlrc_options(C.Structure):
     _fields_ = [("precision", i32), ("max_nrhs", i32), ("mixed_eps", f64), ("device", i32),
-                ("finish_slots", i32), ("piece_tiles", i32), ("leaves_on_device", i32), ("reserved", i32 * 4)]
+                ("finish_slots", i32), ("piece_tiles", i32), ("leaves_on_device", i32), ("near_field", i32),
+                ("reserved", i32 * 3)]
 
 
 class hlrc_info(C.Structure):

@@ -130,7 +130,38 @@ struct Workspace {
     bool has_tm = false;
     CUtensorMap tm_x16, tm_x64, tm_t16;
     bool profile = false;        // record per-pass events in the handle's profile
+    // the side stream of one-vector products whose near field runs beside the
+    // low-rank passes, and the events that fork it from and join it to the
+    // caller's stream (null: side stages run on the caller's stream, first)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
+
+// Side stream and events for a workspace of a handle with side stages; the
+// stream does not synchronise with the legacy default stream, the events
+// only order.
+hlrc_status side_create(Workspace& w) {
+    if (cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&w.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&w.ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        const cudaError_t e = cudaGetLastError();
+        return fail(HLRC_ERR_CUDA, "side stream: %s", cudaGetErrorString(e));
+    }
+    return HLRC_OK;
+}
+void side_destroy(Workspace& w) {
+    if (w.ev_join) cudaEventDestroy(w.ev_join);
+    if (w.ev_fork) cudaEventDestroy(w.ev_fork);
+    if (w.side) cudaStreamDestroy(w.side);
+    w.side = nullptr;
+    w.ev_fork = w.ev_join = nullptr;
+}
+bool has_side(const std::vector<Stage>* nf) {
+    for (int op = 0; op < 3; ++op)
+        for (const Stage& st : nf[op])
+            if (st.side) return true;
+    return false;
+}
 
 struct ProfileRec {
     const char* name;
@@ -159,6 +190,8 @@ struct hlrc_hmat_s {
     std::vector<DevTTPass> tt;
     std::vector<Stage> stages[3];
     std::vector<Stage> stages_mr[3];   // multi-vector products, when they differ (H^2: no tree sweeps)
+    std::vector<Stage> stages_nf[3];   // one-vector products with side stages, when present
+    Workspace side_ws;                 // the handle's side stream and events (side stages only)
     hlrc_info info{};
     // multi-RHS workspace (FP64 plans, allocated at upload when max_nrhs > 1):
     // row-major blocks of MR_RB vectors
@@ -270,10 +303,10 @@ const char* stage_name(hlrc_hmat M, int nk, int idx) {
     if (!M->names[nk].empty()) return M->names[nk][size_t(idx)];
     const int kind = M->kind;
     static const char* ht[] = {"tform_unused"};
-    static const char* hn[] = {"nform_Ut_Dx", "nform_Vt"};
+    static const char* hn[] = {"nform_Ut_Dx", "nform_Vt", "nform_Dx", "nform_Ut"};
     static const char* htt[] = {"ttform_VtX", "ttform_UtX", "ttform_DtX"};
     static const char* ut[] = {"tform_coupT"};
-    static const char* un[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col"};
+    static const char* un[] = {"nform_coupling", "nform_bwd_row_Dx", "nform_bwd_col", "nform_Dx", "nform_bwd_row"};
     static const char* utt[] = {"ttform_fwd_col", "ttform_fwd_row", "ttform_DtX"};
     if (kind == 0) return nk == 0 ? ht[idx] : (nk == 1 ? hn[idx] : htt[idx]);
     return nk == 0 ? ut[idx] : (nk == 1 ? un[idx] : utt[idx]);
@@ -348,7 +381,7 @@ int plan_launches(const Plan& p, int op) {
         for (int f = 0; f < NFMT; ++f) k += segs[f].empty() ? 0 : 1;
         return k;
     };
-    for (const Stage& st : p.stages[op]) {
+    for (const Stage& st : p.stages_nf[op].empty() ? p.stages[op] : p.stages_nf[op]) {
         if (st.kind == 0) {
             const TPass& t = p.tpasses[size_t(st.idx)];
             n += t.groups.empty() ? 0 : 1;
@@ -951,7 +984,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         return fail(HLRC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", h->arena_bytes, cudaGetErrorString(e));
     }
     hlrc_hmat_s* hp = h.get();
-    auto cleanup = [&]() { cudaFree(hp->arena); hp->arena = nullptr; };
+    auto cleanup = [&]() { cudaFree(hp->arena); hp->arena = nullptr; side_destroy(hp->side_ws); };
     auto put = [&](size_t o_, const void* src, size_t bytes) -> cudaError_t {
         if (bytes == 0) return cudaSuccess;
         return cudaMemcpy(hp->arena + o_, src, bytes, cudaMemcpyHostToDevice);
@@ -1125,6 +1158,13 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     for (int op = 0; op < 3; ++op) {
         hp->stages[op] = p.stages[op];
         hp->stages_mr[op] = p.stages_mr[op];
+        hp->stages_nf[op] = p.stages_nf[op];
+    }
+    if (has_side(hp->stages_nf)) {
+        if (const hlrc_status ss = side_create(hp->side_ws); ss != HLRC_OK) {
+            cleanup();
+            return ss;
+        }
     }
 
     fill_info(p, L, hp->info);
@@ -1258,7 +1298,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
     }
     for (int op = 0; op < 3; ++op) {
         int nl = 0;
-        for (const Stage& st : hp->stages[op])
+        for (const Stage& st : hp->stages_nf[op].empty() ? hp->stages[op] : hp->stages_nf[op])
             nl += st.kind == 0 ? hp->t[size_t(st.idx)].launches()
                                : (st.kind == 1 ? hp->n[size_t(st.idx)].launches() : hp->tt[size_t(st.idx)].launches());
         hp->info.launches[op] = nl;
@@ -1278,6 +1318,9 @@ Workspace handle_workspace(hlrc_hmat M) {
     w.has_tm = M->wws.has_tm;
     if (w.has_tm) { w.tm_x16 = M->wws.tm_x16; w.tm_x64 = M->wws.tm_x64; w.tm_t16 = M->wws.tm_t16; }
     w.profile = M->profiling;
+    w.side = M->side_ws.side;
+    w.ev_fork = M->side_ws.ev_fork;
+    w.ev_join = M->side_ws.ev_join;
     return w;
 }
 
@@ -1378,14 +1421,37 @@ cudaError_t launch_k(bool overlap, void (*k)(P...), unsigned grid, unsigned bloc
 }
 
 hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* x, double* y,
-                       cudaStream_t s) {
+                       cudaStream_t s0) {
     // FP64 plans carry 16-byte FP64 descriptors, reduced-precision plans
     // 32-byte packs: each kind of kernel only ever sees its own kind
     const bool f64plan = M->precision == HLRC_PREC_F64;
     const bool ov = M->overlap != 0;
     cudaError_t le = cudaSuccess;   // the first failed launch
     auto L = [&](cudaError_t e) { if (le == cudaSuccess) le = e; };
-    for (const Stage& st : M->stages[op]) {
+    auto writes_y = [&](const Stage& st) {
+        const int out = st.kind == 0 ? M->t[size_t(st.idx)].out
+                                     : (st.kind == 1 ? M->n[size_t(st.idx)].out : M->tt[size_t(st.idx)].out);
+        return out == V_Y;
+    };
+    // Side stages (the near field) run on the workspace's side stream, forked
+    // from s0 before them; the first other stage that writes y waits for
+    // them.  Without a side stream they run first on s0.
+    bool forked = false, joined = false;
+    auto join = [&]() {
+        L(cudaEventRecord(ws.ev_join, ws.side));
+        L(cudaStreamWaitEvent(s0, ws.ev_join, 0));
+        joined = true;
+    };
+    const std::vector<Stage>& stl = M->stages_nf[op].empty() ? M->stages[op] : M->stages_nf[op];
+    for (const Stage& st : stl) {
+        const bool on_side = st.side && ws.side;
+        if (on_side && !forked) {
+            L(cudaEventRecord(ws.ev_fork, s0));
+            L(cudaStreamWaitEvent(ws.side, ws.ev_fork, 0));
+            forked = true;
+        }
+        if (!st.side && forked && !joined && writes_y(st)) join();
+        const cudaStream_t s = on_side ? ws.side : s0;
         M->launches += st.kind == 0 ? M->t[size_t(st.idx)].launches()
                                     : (st.kind == 1 ? M->n[size_t(st.idx)].launches() : M->tt[size_t(st.idx)].launches());
         if (st.kind == 0) {
@@ -1503,6 +1569,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
         }
     }
+    if (forked && !joined) join();
     const cudaError_t e = le != cudaSuccess ? le : cudaGetLastError();
     if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
     return HLRC_OK;
@@ -2194,6 +2261,13 @@ extern "C" hlrc_status hlrc_workspace_create(hlrc_hmat M, int max_nrhs, hlrc_wor
         wide_ws_maps(M, W->ws);
     }
     W->ws.profile = false;
+    if (has_side(M->stages_nf)) {
+        if (const hlrc_status ss = side_create(W->ws); ss != HLRC_OK) {
+            side_destroy(W->ws);
+            cudaFree(W->arena);
+            return ss;
+        }
+    }
     *out = W.release();
     return HLRC_OK;
 }
@@ -2202,6 +2276,7 @@ extern "C" hlrc_status hlrc_workspace_free(hlrc_workspace W) {
     if (!W) return HLRC_OK;
     DeviceGuard g(W->device);
     cudaFree(W->arena);
+    side_destroy(W->ws);
     delete W;
     return HLRC_OK;
 }
@@ -2253,6 +2328,7 @@ extern "C" hlrc_status hlrc_free(hlrc_hmat M) {
     cudaFree(M->w_arena);
     cudaFree(M->w_static);
     cudaFree(M->arena);
+    side_destroy(M->side_ws);
     delete M;
     return HLRC_OK;
 }

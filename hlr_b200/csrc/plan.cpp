@@ -474,6 +474,11 @@ struct NBuilder {
 struct PlanKnobs {
     uint32_t finish_slots = FINISH_SLOTS;
     int piece_tiles = WT_MAXT;
+    int near_field = 0;            // hlrc_options.near_field (0: the planner's default)
+    // the near field on a side stream for a plan of this kind (0 H, 1
+    // uniform-H, 2 H^2): by default for uniform-H and H^2, whose low-rank
+    // part is a chain of small dependent passes
+    bool side_dense(int kind) const { return near_field == 2 || (near_field == 0 && kind != 0); }
 };
 thread_local PlanKnobs g_knobs;
 struct KnobScope {
@@ -481,6 +486,7 @@ struct KnobScope {
     explicit KnobScope(const hlrc_options& o) : saved(g_knobs) {
         g_knobs.finish_slots = o.finish_slots > 0 ? uint32_t(o.finish_slots) : FINISH_SLOTS;
         g_knobs.piece_tiles = o.piece_tiles > 0 ? o.piece_tiles : WT_MAXT;
+        g_knobs.near_field = o.near_field;
     }
     ~KnobScope() { g_knobs = saved; }
 };
@@ -489,6 +495,8 @@ hlrc_status check_knobs(const hlrc_options& o) {
         return fail(HLRC_ERR_ARG, "finish_slots %d outside 2..64", o.finish_slots);
     if (o.piece_tiles != 0 && (o.piece_tiles < 1 || o.piece_tiles > WT_MAXT))
         return fail(HLRC_ERR_ARG, "piece_tiles %d outside 1..%d", o.piece_tiles, WT_MAXT);
+    if (o.near_field < 0 || o.near_field > 2)
+        return fail(HLRC_ERR_ARG, "near_field %d outside 0..2", o.near_field);
     if (o.leaves_on_device != 0 && o.leaves_on_device != 1)
         return fail(HLRC_ERR_ARG, "leaves_on_device must be 0 or 1 (got %d)", o.leaves_on_device);
     return HLRC_OK;
@@ -795,6 +803,21 @@ hlrc_status validate_plan(const Plan& p) {
         for (const TGroup& g : tp.groups1)
             if (int64_t(g.slot0) + int64_t(g.nslots) * g.nc > tp.npart || int64_t(g.out) + g.nc > tp.npart)
                 return fail(HLRC_ERR_INTERNAL, "T-pass %zu: first-level finish group outside the partials", pi);
+    }
+    // side stages lead their list and are plain N-form passes adding into y
+    // from x and the store only: they run beside the stages after them
+    for (int op = 0; op < 3; ++op) {
+        bool main_seen = false;
+        for (const Stage& sg : p.stages_nf[op]) {
+            if (!sg.side) { main_seen = true; continue; }
+            if (main_seen || sg.kind != 1 || sg.idx < 0 || size_t(sg.idx) >= p.npasses.size())
+                return fail(HLRC_ERR_INTERNAL, "op %d: side stage out of place", op);
+            const NPass& np = p.npasses[size_t(sg.idx)];
+            if (np.out != V_Y || np.mode != OUT_ADD_ALPHA || !np.cta_begin.empty())
+                return fail(HLRC_ERR_INTERNAL, "op %d: side stage is not a plain pass into y", op);
+            for (const GChunk& g : np.chunks)
+                if (g.vo & VEC_T) return fail(HLRC_ERR_INTERNAL, "op %d: side stage reads coefficients", op);
+        }
     }
     return HLRC_OK;
 }
@@ -1175,6 +1198,31 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
         c0 = d.blocks[i].col0;
         nc = d.blocks[i].ncols;
     });
+    // op N with the near field on a side stream: y += alpha D x per row tile
+    // (npasses[2]), then y += alpha U t (npasses[3]) after stage A
+    if (g_knobs.side_dense(0)) {
+        p.npasses.resize(4);
+        for (int half = 0; half < 2; ++half) {
+            NPass& q = p.npasses[size_t(2 + half)];
+            q.vx = V_X; q.vt = V_T; q.out = V_Y; q.mode = OUT_ADD_ALPHA;
+            NBuilder nbld(q, st);
+            std::vector<size_t> pos(static_cast<size_t>(nb), 0);
+            for (int64_t t = 0; t < tr.n(); ++t) {
+                nbld.begin(tr.size(t));
+                for (int64_t i : rowlist[size_t(t)]) {
+                    const hlrc_block& b = d.blocks[i];
+                    const int sid = slabA[size_t(i)][pos[size_t(i)]++];
+                    const bool dense = b.kind == HLRC_LEAF_DENSE;
+                    if (dense != (half == 0)) continue;
+                    if (dense) nbld.slab(sid, uint32_t(b.col0));
+                    else nbld.slab(sid, VEC_T | uint32_t(toff[size_t(i)]));
+                }
+                nbld.end(uint32_t(tr.lo(t)), tr.size(t), false);
+            }
+            nbld.finish();
+        }
+        p.stages_nf[HLRC_OP_N] = {{1, 2, 1}, {2, 0}, {1, 3}};
+    }
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}};
     p.stages[HLRC_OP_T] = {{2, 1}, {1, 1}, {2, 2}};
     p.stages[HLRC_OP_C] = p.stages[HLRC_OP_T];
@@ -1443,6 +1491,28 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
         c0 = d.blocks[i].col0;
         nc = d.blocks[i].ncols;
     });
+    // op N with the near field on a side stream: y += alpha D x per row tile
+    // (npasses[3]), then y += alpha V_t uy_t (npasses[4]) after the coupling
+    if (g_knobs.side_dense(1)) {
+        p.npasses.resize(5);
+        for (int half = 0; half < 2; ++half) {
+            NPass& q = p.npasses[size_t(3 + half)];
+            q.vx = V_X; q.vt = V_T2; q.out = V_Y; q.mode = OUT_ADD_ALPHA;
+            NBuilder nbld(q, st);
+            std::vector<size_t> posRB(static_cast<size_t>(nrb), 0), posD(static_cast<size_t>(nb), 0);
+            for (int64_t t = 0; t < tr.n(); ++t) {
+                nbld.begin(tr.size(t));
+                if (half == 1)
+                    for (int64_t i : rbl[size_t(t)])
+                        nbld.slab(sRB[size_t(i)][posRB[size_t(i)]++], VEC_T | uint32_t(rboff[size_t(i)]));
+                if (half == 0)
+                    for (int64_t i : rdl[size_t(t)]) nbld.slab(sD[size_t(i)][posD[size_t(i)]++], uint32_t(d.blocks[i].col0));
+                nbld.end(uint32_t(tr.lo(t)), tr.size(t), false);
+            }
+            nbld.finish();
+        }
+        p.stages_nf[HLRC_OP_N] = {{1, 3, 1}, {2, 0}, {1, 0}, {1, 4}};
+    }
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}, {1, 1}};
     p.stages[HLRC_OP_T].clear();  // uniform_lrmatrix::uni_apply_add asserts on apply_transposed
     p.stages[HLRC_OP_C] = {{2, 1}, {0, 0}, {1, 2}, {2, 2}};
@@ -1959,11 +2029,13 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
                 drop_n();
             }
         }
-        // backward sweep: sons at levels L0+1..maxlev of the subtrees
+        // backward sweep: sons at levels L0..maxlev of the subtrees; a
+        // subtree root's own transfer reads its parent's y^, which the
+        // passes before the sweep complete
         for (int L0 = tree_root(Tb); L0 >= 0 && L0 + 2 <= Tb.maxlev && downIdx < 0; ++L0) {
             NPass& n = add_n("h2_bwd_tree");
             n.vx = V_X; n.vt = V_T2; n.out = V_T2; n.mode = OUT_ADD;
-            if (tree_pass(n, Tb, L0, L0 + 1, Tb.maxlev, false,
+            if (tree_pass(n, Tb, L0, L0, Tb.maxlev, false,
                           [&](NBuilder& nb, int64_t c) { bwd_child(nb, Tb, sEb, c); })) {
                 downL0 = L0;
                 downIdx = int(p.npasses.size()) - 1;
@@ -1986,7 +2058,7 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
         for (int lev = 0; lev < Tb.maxlev; ++lev) {
             if (down[size_t(lev)] < 0) continue;
             lv.push_back({1, down[size_t(lev)]});
-            if (downIdx < 0 || lev < downL0) sw.push_back({1, down[size_t(lev)]});
+            if (downIdx < 0 || lev + 1 < downL0) sw.push_back({1, down[size_t(lev)]});
         }
         if (downIdx >= 0) sw.push_back({1, downIdx});
         lv.insert(lv.end(), tail.begin(), tail.end());
@@ -2018,6 +2090,30 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
     bwd_leaves(add_n("h2_bwd_leaves_Dx"), R, tr, rbl, sRB, true);
     const Stage n_out{1, int(p.npasses.size()) - 1};
     compose(HLRC_OP_N, Cc, sETC, R, sER, n_leaves, n_coupling, {n_out});
+    if (g_knobs.side_dense(2)) {
+        // the one-vector product with the near field on a side stream: y +=
+        // alpha D x per row tile first, the leaf bases' V_t y^_t after the
+        // backward transfers
+        NPass& dx = add_n("h2_Dx");
+        dx.vx = V_X; dx.vt = V_T2; dx.out = V_Y; dx.mode = OUT_ADD_ALPHA;
+        {
+            NBuilder nbld(dx, st);
+            std::vector<size_t> posD(static_cast<size_t>(nb), 0);
+            for (int64_t q = 0; q < tr.n(); ++q) {
+                nbld.begin(tr.size(q));
+                for (int64_t i : rdl[size_t(q)]) nbld.slab(sD[size_t(i)][posD[size_t(i)]++], uint32_t(d.blocks[i].col0));
+                nbld.end(uint32_t(tr.lo(q)), tr.size(q), false);
+            }
+            nbld.finish();
+        }
+        const int dxi = int(p.npasses.size()) - 1;
+        bwd_leaves(add_n("h2_bwd_leaves"), R, tr, rbl, sRB, false);
+        const Stage lu{1, int(p.npasses.size()) - 1};
+        std::vector<Stage>& nf = p.stages_nf[HLRC_OP_N];
+        nf = {Stage{1, dxi, 1}};
+        for (const Stage& sg : p.stages[HLRC_OP_N])
+            nf.push_back(sg.kind == n_out.kind && sg.idx == n_out.idx ? lu : sg);
+    }
 
     // ---- op C: the trees exchanged
     fwd_leaves(add_tt("h2_fwd_leaves"), R, tr, rbl, sRB);

@@ -114,6 +114,10 @@ struct WidePlan {
 struct Stage {
     int kind;                      // 0 = T-form (units), 1 = N-form, 2 = tile T-form
     int idx;                       // index into Plan::tpasses / npasses / ttpasses
+    // 1: launched on the workspace's side stream at the start of the product
+    // (an N-form pass that writes y and reads only x and the store); the
+    // first stage after it that writes y waits for it
+    int side = 0;
 };
 
 // One column block of an FP64 store whose source leaves are in device
@@ -144,6 +148,9 @@ struct Plan {
     std::vector<TTPass> ttpasses;
     std::vector<Stage> stages[3];  // per op (N, T, C); empty = unsupported
     std::vector<Stage> stages_mr[3];  // multi-vector products when they differ (H^2: level passes, no tree sweeps)
+    // one-vector products with the near field on a side stream
+    // (hlrc_options.near_field): replaces stages[op] there when not empty
+    std::vector<Stage> stages_nf[3];
     // accounting (per product, one rhs)
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;

@@ -78,10 +78,14 @@ def _store(path: Path, key: str, entry: dict) -> None:
     os.replace(tmp, path)
 
 
-def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2, min_ms: float = 20.0) -> Callable[[], float]:
+def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2, min_ms: float = 20.0,
+                graph: bool = False) -> Callable[[], float]:
     """Returns a function timing one product of M (ms per product) with the
     handle's current setting, on private random device vectors.  A timed run
-    covers ``reps`` products, or more if needed to last ``min_ms``."""
+    covers ``reps`` products, or more if needed to last ``min_ms``.  With
+    ``graph`` the products are captured into a CUDA graph and its replay is
+    timed: the launch cost the caller pays when it replays graphs (small
+    products are otherwise bound by the host's launch rate)."""
     import torch
 
     from . import apply_normal, mul_vec
@@ -100,6 +104,20 @@ def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2, min_ms: f
 
     def timed(n: int) -> float:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if graph:
+            n = min(n, 2000)
+            torch.cuda.synchronize(dev)
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gr):
+                for _ in range(n):
+                    mul_vec(1.0, op, M, x, y)
+            gr.replay()   # first replay uploads the graph
+            e0.record(stream)
+            gr.replay()
+            e1.record(stream)
+            e1.synchronize()
+            del gr
+            return e0.elapsed_time(e1) / n
         e0.record(stream)
         for _ in range(n):
             mul_vec(1.0, op, M, x, y)
@@ -120,11 +138,12 @@ def event_timer(M, nrhs: int, op: int, reps: int = 5, warmup: int = 2, min_ms: f
 
 def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "default", reps: int = 5,
              warmup: int = 2, keep_default_within: float = 0.02, timer: Optional[Callable[[], float]] = None,
-             device_name: Optional[str] = None, sweeps: int = 2) -> dict:
+             device_name: Optional[str] = None, sweeps: int = 2, graph: bool = False) -> dict:
     """Picks and sets the fastest launch shapes of M for ``nrhs`` vectors and
     operation ``op``.  ``cache`` is a JSON path, "default" for
     ``default_cache_path()``, or None for no cache.  ``timer`` (tests) times
-    one product with the handle's current setting; by default CUDA events.
+    one product with the handle's current setting; by default CUDA events
+    (around a CUDA graph replay with ``graph``, which is part of the key).
 
     Returns {"tuning": chosen setting, "times_ms": [(setting, ms), ...],
     "cached": whether the setting came from the cache, "key": cache key}."""
@@ -132,7 +151,7 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
         import torch
         device_name = torch.cuda.get_device_name(torch.cuda.current_device())
     path = default_cache_path() if cache == "default" else (Path(cache) if cache is not None else None)
-    key = signature(M, nrhs, op, device_name)
+    key = signature(M, nrhs, op, device_name) + ("|graph" if graph else "")
     if path is not None:
         hit = _load(path).get(key)
         if isinstance(hit, dict) and isinstance(hit.get("tuning"), dict):
@@ -142,7 +161,7 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
             except Exception:
                 pass  # stale or foreign entry: tune afresh
     if timer is None:
-        timer = event_timer(M, nrhs, op, reps=reps, warmup=warmup)
+        timer = event_timer(M, nrhs, op, reps=reps, warmup=warmup, graph=graph)
     start = M.tuning
     cands = candidates(start, nrhs)
     best = [float("inf")] * len(cands)
@@ -172,11 +191,15 @@ PLAN_CANDIDATES = {
     "finish_slots": (16, 8, 32, 64),
     # 64-vector T-form: tiles per piece of a long column cluster
     "piece_tiles": (32, 16, 8),
+    # one-vector products: the near field fused into the last pass (1) or
+    # its own pass on a side stream (2); 0 is the planner's default
+    "near_field": (0, 1, 2),
 }
 
 
 def autotune_plan(upload_fn: Callable[[dict], object], nrhs: int = 1, op: int = 0, knobs=("finish_slots",),
-                  keep_default_within: float = 0.02, timer_for: Optional[Callable] = None, sweeps: int = 2):
+                  keep_default_within: float = 0.02, timer_for: Optional[Callable] = None, sweeps: int = 2,
+                  graph: bool = False):
     """Plan-level choices, timed by uploading the matrix once per candidate.
 
     ``upload_fn(plan)`` uploads the matrix with hlrc_options plan choices
@@ -187,7 +210,8 @@ def autotune_plan(upload_fn: Callable[[dict], object], nrhs: int = 1, op: int = 
     ``autotune``.  The default is kept unless another value is faster by more
     than ``keep_default_within``.  Returns (handle of the chosen plan,
     {"plan": choice, "times_ms": [(plan, ms), ...]}); the other handles are
-    freed.  ``timer_for(M)`` (tests) replaces the event timer."""
+    freed.  ``timer_for(M)`` (tests) replaces the event timer; ``graph``
+    times CUDA graph replays, as ``event_timer``."""
     choice, times = {}, []
     best_M = None
     for knob in knobs:
@@ -195,7 +219,7 @@ def autotune_plan(upload_fn: Callable[[dict], object], nrhs: int = 1, op: int = 
         for v in PLAN_CANDIDATES[knob]:
             plan = dict(choice, **{knob: v})
             M = upload_fn(plan)
-            timer = timer_for(M) if timer_for is not None else event_timer(M, nrhs, op)
+            timer = timer_for(M) if timer_for is not None else event_timer(M, nrhs, op, graph=graph)
             cands.append([plan, M, timer, float("inf")])
         for _ in range(sweeps):
             for c in cands:

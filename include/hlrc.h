@@ -198,7 +198,15 @@ typedef struct hlrc_options {
      * device (an on_device build); FP64 stores are filled on the device,
      * other precisions copy the leaves to the host first                   */
     int32_t leaves_on_device;
-    int32_t reserved[4];
+    /* near_field (one-vector products of op N): 1 = the dense leaves' D x is
+     * summed in the last pass with the low-rank part (as HLR's mul_vec sums
+     * every block of a row, tbb/detail/arith.hh:95-124); 2 = D x is its own
+     * pass, launched on a side stream at the start of the product and joined
+     * before the pass that adds the low-rank part to y, so that it overlaps
+     * the dependent low-rank passes; 0 = default (2 for uniform-H and H2, 1
+     * for H).  Both add D x first, then the low-rank part, per row tile.   */
+    int32_t near_field;
+    int32_t reserved[3];
 } hlrc_options;
 
 /* accounting of one product, following HLR's mul_vec_flops /

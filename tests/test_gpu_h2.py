@@ -69,8 +69,8 @@ def test_h2_rejects_transposed_and_other_precisions():
 def test_h2_tree_sweeps(op):
     """The sphere with 8192 triangles has 32 clusters at level 5 and three
     levels below them: the one-vector product sweeps those levels of each
-    tree in one launch (one CTA per subtree), the 8-vector product runs them
-    level by level, and both match the oracle."""
+    tree in one launch (one cluster of CTAs per subtree), the 8-vector
+    product runs them level by level, and both match the oracle."""
     hm = built("sphere5_h2", CASES["sphere5"])
     M = hlr.upload(hm, h2=True, max_nrhs=8)
     M.set_profiling(True)
@@ -82,8 +82,11 @@ def test_h2_tree_sweeps(op):
     torch.cuda.synchronize()
     prof = M.last_profile()
     assert prof["h2_fwd_tree"][0] == 1 and prof["h2_bwd_tree"][0] == 1
-    # the levels above the subtree roots keep one pass each
-    assert prof["h2_fwd_transfer"][0] == 1 and prof["h2_bwd_transfer"][0] == 1
+    # the forward transfer into level 4 keeps its own pass; the backward
+    # transfer into the subtree roots is the first level of their sweep
+    assert prof["h2_fwd_transfer"][0] == 1 and "h2_bwd_transfer" not in prof
+    # op N: the near field on the side stream (the default for H2)
+    assert ("h2_Dx" in prof) == (op == 0)
     yref = np.zeros(hm.n)
     oracle.h2_mvm(hm.h2_desc(), -0.5, op, x, yref)
     assert relerr(y.cpu().numpy(), yref) <= TOL

@@ -90,24 +90,30 @@ def test_h2_tree_sweeps_planned():
     """On the sphere with 8192 triangles the one-vector product sweeps the
     transfer levels below the 32 clusters of level 5 in one launch per tree:
     op N is the leaf transform, the forward sweep, the level-4 transfer, the
-    couplings, the level-5 transfer, the backward sweep and the leaf pass
-    (the planner and its checks of the sweep's arrays run here, on the
-    host)."""
+    couplings, the backward sweep (from the level-5 transfer down) and the
+    leaf pass, and by default the near field D x as its own pass on a side
+    stream (the planner and its checks of the sweep's arrays run here, on
+    the host)."""
     hm = built("sphere5_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=5, nested=True)))
     info = hlr.plan_info(hm, h2=True)
     assert info["launches"][0] == 7
     assert info["launches"][1] == 0   # op T unsupported
+    assert hlr.plan_info(hm, h2=True, plan={"near_field": 1})["launches"][0] == 6
+    assert hlr.plan_info(hm, h2=True, plan={"near_field": 2})["launches"][0] == 7
     # without levels below the subtree roots there is no sweep: one pass per level
     small = built("sphere4_h2", lambda: hlr.build(hlr.Problem.laplace_sphere(refine=4, nested=True)))
-    assert hlr.plan_info(small, h2=True)["launches"][0] == 5
+    assert hlr.plan_info(small, h2=True, plan={"near_field": 1})["launches"][0] == 5
+    with pytest.raises(hlr.HLRCError):
+        hlr.plan_info(small, h2=True, plan={"near_field": 3})
 
 
 SMALL_TREES = {
-    # (problem, launches of the one-vector op N product with the sweeps)
-    "exp3d_4096_leaf32": (lambda: hlr.Problem.exp3d(4096, nested=True, leaf_size=32), 7),
-    "log1d_4096_leaf32": (lambda: hlr.Problem.log1d(4096, nested=True, leaf_size=32), 11),
+    # (problem, launches of the one-vector op N product with the sweeps and
+    # the near field fused into the leaf pass; one more with it on the side)
+    "exp3d_4096_leaf32": (lambda: hlr.Problem.exp3d(4096, nested=True, leaf_size=32), 6),
+    "log1d_4096_leaf32": (lambda: hlr.Problem.log1d(4096, nested=True, leaf_size=32), 10),
     "sphere4_leaf32": (lambda: hlr.Problem.laplace_sphere(refine=4, nested=True, leaf_size=32), 7),
-    "exp3d_2048_leaf16": (lambda: hlr.Problem.exp3d(2048, nested=True, leaf_size=16), 7),
+    "exp3d_2048_leaf16": (lambda: hlr.Problem.exp3d(2048, nested=True, leaf_size=16), 6),
 }
 
 
@@ -119,8 +125,8 @@ def test_h2_sweeps_planned_for_small_leaves(case):
     checks of the sweep arrays pass."""
     make, launches = SMALL_TREES[case]
     hm = built(case + "_h2", lambda: hlr.build(make()))
-    info = hlr.plan_info(hm, h2=True)
-    assert info["launches"][0] == launches
+    assert hlr.plan_info(hm, h2=True, plan={"near_field": 1})["launches"][0] == launches
+    assert hlr.plan_info(hm, h2=True)["launches"][0] == launches + 1
 
 
 @pytest.mark.parametrize("op", [0, 2])
