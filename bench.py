@@ -405,8 +405,17 @@ def reduced_arms(hlr, hm, x, n, alpha, args, world, dev, y_oracle, v64, peak):
     hbm_peak, peak_kind = peak
     out = {}
     for prec in args.reduced:
-        Mr = hlr.upload(hm, precision=prec, max_nrhs=1)
+        plan_times = None
+        if args.no_autotune:
+            Mr = hlr.upload(hm, precision=prec, max_nrhs=1, plan=args.plan)
+        else:   # the near field beside the low-rank passes or fused, as for the FP64 line
+            from hlr_b200.tune import autotune_plan
+            Mr, pt = autotune_plan(lambda p: hlr.upload(hm, precision=prec, max_nrhs=1, plan=dict(args.plan, **p)),
+                                   nrhs=1, knobs=("near_field",), graph=not args.no_graph)
+            plan_times = pt["times_ms"]
         tuned = tune_handle(Mr, 1, args)
+        if tuned is not None:
+            tuned = dict(tuned, plan=Mr.plan or "defaults", plan_times_ms=plan_times)
         yr = torch.zeros(n, dtype=torch.float64, device=dev)
         r = time_products(Mr, lambda: hlr.mul_vec(alpha, hlr.apply_normal, Mr, x, yr), args.steps, args.warmup,
                           not args.no_graph, world, dev, gpu_uuid(dev.index))
@@ -673,22 +682,24 @@ def run_batch(args, rank, world, local_rank):
     if args.tune_plan and not args.no_autotune:
         # the two-level finish threshold, per store (many small multi-tile outputs)
         from hlr_b200.tune import autotune_plan
-        A64, plan64 = autotune_plan(lambda p: hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad, plan=p),
-                                    nrhs=nrhs, knobs=("finish_slots",))
+        A64, plan64 = autotune_plan(lambda p: hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad,
+                                                               plan=dict(args.plan, **p)),
+                                    nrhs=nrhs, knobs=("near_field", "finish_slots"))
         if inner == "f64":
             Alow = A64
         else:
             for h in hms:
                 h.fetch()
             Alow, planlow = autotune_plan(
-                lambda p: hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad, plan=p), nrhs=nrhs,
-                knobs=("finish_slots",))
+                lambda p: hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad, plan=dict(args.plan, **p)),
+                nrhs=nrhs, knobs=("near_field", "finish_slots"))
     else:
-        A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad)
+        A64 = hlr.upload_batch(hms, precision="f64", max_nrhs=nrhs, pad_to=pad, plan=args.plan)
         if inner != "f64":
             for h in hms:
                 h.fetch()
-        Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad)
+        Alow = A64 if inner == "f64" else hlr.upload_batch(hms, precision=inner, max_nrhs=nrhs, pad_to=pad,
+                                                           plan=args.plan)
     tuned64 = tune_handle(A64, nrhs, args)
     tuned = tune_handle(Alow, nrhs, args) if Alow is not A64 else tuned64
     if tuned is not None:

@@ -259,12 +259,14 @@ class DeviceMatrix:
     @property
     def tuning(self) -> dict:
         """Launch shapes of this handle's products (hlrc_get_tuning):
-        nform_warps, ttform_warps (4, 8 or 16), mr_min_nrhs, wide_min_nrhs and
-        overlap (programmatic dependent launch of the one-vector kernels)."""
+        nform_warps, ttform_warps (4, 8 or 16), mr_min_nrhs, wide_min_nrhs,
+        overlap (programmatic dependent launch of the one-vector kernels) and
+        side_at (how many other passes launch before the near field's side
+        pass is forked)."""
         t = _capi.hlrc_tuning()
         check(lib().hlrc_get_tuning(self._h, C.byref(t)), "hlrc_get_tuning")
         return {"nform_warps": t.nform_warps, "ttform_warps": t.ttform_warps, "mr_min_nrhs": t.mr_min_nrhs,
-                "wide_min_nrhs": t.wide_min_nrhs, "overlap": t.overlap}
+                "wide_min_nrhs": t.wide_min_nrhs, "overlap": t.overlap, "side_at": t.side_at}
 
     def set_tuning(self, **kw) -> None:
         """Changes some launch shapes (hlrc_set_tuning); the others keep their
@@ -275,7 +277,7 @@ class DeviceMatrix:
             raise ValueError(f"unknown tuning keys {sorted(unknown)}")
         cur.update(kw)
         t = _capi.hlrc_tuning(int(cur["nform_warps"]), int(cur["ttform_warps"]), int(cur["mr_min_nrhs"]),
-                              int(cur["wide_min_nrhs"]), int(cur["overlap"]))
+                              int(cur["wide_min_nrhs"]), int(cur["overlap"]), int(cur["side_at"]))
         check(lib().hlrc_set_tuning(self._h, C.byref(t)), "hlrc_set_tuning")
 
     def launch_count(self) -> int:

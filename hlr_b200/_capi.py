@@ -77,7 +77,7 @@ class hlrc_info(C.Structure):
 
 class hlrc_tuning(C.Structure):
     _fields_ = [("nform_warps", i32), ("ttform_warps", i32), ("mr_min_nrhs", i32), ("wide_min_nrhs", i32),
-                ("overlap", i32), ("reserved", i32 * 3)]
+                ("overlap", i32), ("side_at", i32), ("reserved", i32 * 2)]
 
 
 HLRC_MR_NEVER = 1000000

@@ -236,6 +236,7 @@ struct hlrc_hmat_s {
     int mr_min_nrhs = 2;      // fewest vectors that take the 8-vector kernels
     int wide_min_nrhs = MR_RB + 1;   // fewest vectors that take the 64-vector kernels (when the handle has them)
     int overlap = 1;          // one-vector kernels launched with programmatic dependent launch
+    int side_at = 0;          // side stages forked after this many other stages
     // profiling
     bool profiling = false;
     std::vector<ProfileRec> prof;
@@ -1420,6 +1421,74 @@ cudaError_t launch_k(bool overlap, void (*k)(P...), unsigned grid, unsigned bloc
     return cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+// Side stages (the near field) run on the workspace's side stream, forked
+// from the caller's stream s0 before the first of them; the first other
+// stage that writes y waits for them.  Without a side stream they run on s0
+// in list order (first).
+struct SideFork {
+    hlrc_hmat M;
+    const Workspace& ws;
+    cudaStream_t s0;
+    bool forked = false, joined = false;
+    cudaError_t err = cudaSuccess;   // the first failed fork or join call
+    void check(cudaError_t e) { if (err == cudaSuccess) err = e; }
+    bool writes_y(const Stage& st) const {
+        const int out = st.kind == 0 ? M->t[size_t(st.idx)].out
+                                     : (st.kind == 1 ? M->n[size_t(st.idx)].out : M->tt[size_t(st.idx)].out);
+        return out == V_Y;
+    }
+    // the stream stage st launches on
+    cudaStream_t before(const Stage& st) {
+        const bool on_side = st.side && ws.side;
+        if (on_side && !forked) {
+            check(cudaEventRecord(ws.ev_fork, s0));
+            check(cudaStreamWaitEvent(ws.side, ws.ev_fork, 0));
+            forked = true;
+        }
+        if (!st.side && forked && !joined && writes_y(st)) join();
+        return on_side ? ws.side : s0;
+    }
+    void join() {
+        check(cudaEventRecord(ws.ev_join, ws.side));
+        check(cudaStreamWaitEvent(s0, ws.ev_join, 0));
+        joined = true;
+    }
+    // after the last stage: every side stage is joined
+    cudaError_t end() {
+        if (forked && !joined) join();
+        return err;
+    }
+};
+
+// Launch order of a stage list: the other stages in list order, with the
+// side stages inserted before the side_at-th of them (at most before the
+// first that writes y, which waits for them).  Returns indices into stl.
+const std::vector<int>& stage_order(hlrc_hmat M, const std::vector<Stage>& stl, std::vector<int>& order) {
+    order.clear();
+    int at = -1, m = 0;
+    for (size_t i = 0; i < stl.size(); ++i) {
+        if (stl[i].side) continue;
+        const Stage& st = stl[i];
+        const int out = st.kind == 0 ? M->t[size_t(st.idx)].out
+                                     : (st.kind == 1 ? M->n[size_t(st.idx)].out : M->tt[size_t(st.idx)].out);
+        if (out == V_Y) { at = m; break; }
+        ++m;
+    }
+    at = at < 0 ? std::min(M->side_at, m) : std::min(M->side_at, at);
+    auto sides = [&]() {
+        for (size_t i = 0; i < stl.size(); ++i)
+            if (stl[i].side) order.push_back(int(i));
+    };
+    m = 0;
+    for (size_t i = 0; i < stl.size(); ++i) {
+        if (stl[i].side) continue;
+        if (m++ == at) sides();
+        order.push_back(int(i));
+    }
+    if (at >= m) sides();
+    return order;
+}
+
 hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* x, double* y,
                        cudaStream_t s0) {
     // FP64 plans carry 16-byte FP64 descriptors, reduced-precision plans
@@ -1428,30 +1497,12 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
     const bool ov = M->overlap != 0;
     cudaError_t le = cudaSuccess;   // the first failed launch
     auto L = [&](cudaError_t e) { if (le == cudaSuccess) le = e; };
-    auto writes_y = [&](const Stage& st) {
-        const int out = st.kind == 0 ? M->t[size_t(st.idx)].out
-                                     : (st.kind == 1 ? M->n[size_t(st.idx)].out : M->tt[size_t(st.idx)].out);
-        return out == V_Y;
-    };
-    // Side stages (the near field) run on the workspace's side stream, forked
-    // from s0 before them; the first other stage that writes y waits for
-    // them.  Without a side stream they run first on s0.
-    bool forked = false, joined = false;
-    auto join = [&]() {
-        L(cudaEventRecord(ws.ev_join, ws.side));
-        L(cudaStreamWaitEvent(s0, ws.ev_join, 0));
-        joined = true;
-    };
+    SideFork side{M, ws, s0};
     const std::vector<Stage>& stl = M->stages_nf[op].empty() ? M->stages[op] : M->stages_nf[op];
-    for (const Stage& st : stl) {
-        const bool on_side = st.side && ws.side;
-        if (on_side && !forked) {
-            L(cudaEventRecord(ws.ev_fork, s0));
-            L(cudaStreamWaitEvent(ws.side, ws.ev_fork, 0));
-            forked = true;
-        }
-        if (!st.side && forked && !joined && writes_y(st)) join();
-        const cudaStream_t s = on_side ? ws.side : s0;
+    thread_local std::vector<int> order;
+    for (const int oi : stage_order(M, stl, order)) {
+        const Stage& st = stl[size_t(oi)];
+        const cudaStream_t s = side.before(st);
         M->launches += st.kind == 0 ? M->t[size_t(st.idx)].launches()
                                     : (st.kind == 1 ? M->n[size_t(st.idx)].launches() : M->tt[size_t(st.idx)].launches());
         if (st.kind == 0) {
@@ -1569,7 +1620,7 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             HLRC_AFTER_LAUNCH(stage_name(M, 1, st.idx));
         }
     }
-    if (forked && !joined) join();
+    L(side.end());
     const cudaError_t e = le != cudaSuccess ? le : cudaGetLastError();
     if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
     return HLRC_OK;
@@ -1578,7 +1629,8 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
 // The stages of a multi-vector product: the level passes where the
 // one-vector product sweeps trees.
 const std::vector<Stage>& mr_stages(hlrc_hmat M, int op) {
-    return M->stages_mr[op].empty() ? M->stages[op] : M->stages_mr[op];
+    if (!M->stages_mr[op].empty()) return M->stages_mr[op];
+    return M->stages_nf[op].empty() ? M->stages[op] : M->stages_nf[op];
 }
 
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs
@@ -1594,9 +1646,13 @@ bool multi_rhs_ok(hlrc_hmat M, const Workspace& ws, int op, int nrhs) {
 // y := y + alpha op(M) X for nrhs column vectors, MR_RB at a time: the matrix
 // is streamed once per block instead of once per vector.
 hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op, const double* X, int64_t ldx,
-                      double* Y, int64_t ldy, int nrhs, cudaStream_t s) {
+                      double* Y, int64_t ldy, int nrhs, cudaStream_t s0) {
     const int64_t nx = op == HLRC_OP_N ? M->ncols : M->nrows;
     for (int r0 = 0; r0 < nrhs; r0 += MR_RB) {
+        const cudaStream_t s = s0;
+        // side stages read the block of x staged below and add into Y; the
+        // next block overwrites it only after the join
+        SideFork side{M, ws, s0};
         const int nr = std::min(MR_RB, nrhs - r0);
         const int64_t tot = nx * MR_RB;
         k_rows_from_cols<<<unsigned((tot + 255) / 256), 256, 0, s>>>(X, ldx, nx, r0, nr, ws.mr_x);
@@ -1611,7 +1667,11 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
             return OutMap{vec(name), MR_RB, 1, MR_RB};
         };
         const double* A = reinterpret_cast<const double*>(M->store);
-        for (const Stage& st : mr_stages(M, op)) {
+        const std::vector<Stage>& stl = mr_stages(M, op);
+        thread_local std::vector<int> order;
+        for (const int oi : stage_order(M, stl, order)) {
+            const Stage& st = stl[size_t(oi)];
+            const cudaStream_t s = side.before(st);
             if (st.kind == 2) {
                 const DevTTPass& tp = M->tt[size_t(st.idx)];
                 const int add = tp.mode != OUT_SET;
@@ -1723,6 +1783,8 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
             }
         }
         M->launches += nl;
+        if (const cudaError_t fe = side.end(); fe != cudaSuccess)
+            return fail(HLRC_ERR_CUDA, "side stream: %s", cudaGetErrorString(fe));
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(HLRC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -2052,6 +2114,7 @@ extern "C" hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t) {
     t->mr_min_nrhs = M->mr_min_nrhs;
     t->wide_min_nrhs = M->wide_min_nrhs;
     t->overlap = M->overlap;
+    t->side_at = M->side_at;
     return HLRC_OK;
 }
 
@@ -2067,13 +2130,17 @@ extern "C" hlrc_status hlrc_set_tuning(hlrc_hmat M, const hlrc_tuning* t) {
     if (t->wide_min_nrhs < 2 || t->wide_min_nrhs > HLRC_MR_NEVER)
         return fail(HLRC_ERR_ARG, "hlrc_set_tuning: wide_min_nrhs must be in [2, %d] (got %d)", HLRC_MR_NEVER,
                     t->wide_min_nrhs);
+    if (t->overlap != 0 && t->overlap != 1)
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: overlap must be 0 or 1 (got %d)", t->overlap);
+    if (t->side_at < 0 || t->side_at > 16)
+        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: side_at must be in [0, 16] (got %d)", t->side_at);
+    // every field is checked before any is set
     M->nform_warps = t->nform_warps;
     M->ttform_warps = t->ttform_warps;
     M->mr_min_nrhs = t->mr_min_nrhs;
-    if (t->overlap != 0 && t->overlap != 1)
-        return fail(HLRC_ERR_ARG, "hlrc_set_tuning: overlap must be 0 or 1 (got %d)", t->overlap);
     M->wide_min_nrhs = t->wide_min_nrhs;
     M->overlap = t->overlap;
+    M->side_at = t->side_at;
     return HLRC_OK;
 }
 

@@ -474,11 +474,10 @@ struct NBuilder {
 struct PlanKnobs {
     uint32_t finish_slots = FINISH_SLOTS;
     int piece_tiles = WT_MAXT;
-    int near_field = 0;            // hlrc_options.near_field (0: the planner's default)
-    // the near field on a side stream for a plan of this kind (0 H, 1
-    // uniform-H, 2 H^2): by default for uniform-H and H^2, whose low-rank
-    // part is a chain of small dependent passes
-    bool side_dense(int kind) const { return near_field == 2 || (near_field == 0 && kind != 0); }
+    int near_field = 0;            // hlrc_options.near_field (0: the default, 2)
+    // the near field on a side stream (every kind of plan: 0 H, 1 uniform-H,
+    // 2 H^2), unless the caller asks for it fused
+    bool side_dense(int /*kind*/) const { return near_field != 1; }
 };
 thread_local PlanKnobs g_knobs;
 struct KnobScope {

@@ -33,7 +33,10 @@ from typing import Callable, Optional
 
 from ._capi import HLRC_MR_NEVER
 
-DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1}
+DEFAULT = {"nform_warps": 8, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1, "side_at": 0}
+# one vector, second phase at the chosen launch shapes: where the near
+# field's side pass is forked (a handle without one times the same for all)
+SIDE_AT = (0, 1, 2, 3)
 
 
 def default_cache_path() -> Path:
@@ -163,21 +166,27 @@ def autotune(M, nrhs: int = 1, op: int = 0, cache: Optional[os.PathLike] = "defa
     if timer is None:
         timer = event_timer(M, nrhs, op, reps=reps, warmup=warmup, graph=graph)
     start = M.tuning
-    cands = candidates(start, nrhs)
-    best = [float("inf")] * len(cands)
-    try:
-        for _ in range(sweeps):   # interleaved sweeps; a candidate keeps its best time
-            for i, c in enumerate(cands):
-                M.set_tuning(**c)
-                best[i] = min(best[i], float(timer()))
-    except BaseException:
-        M.set_tuning(**start)
-        raise
-    times = [(dict(c), t) for c, t in zip(cands, best)]
-    best_c, best_t = min(times, key=lambda ct: ct[1])
-    first_c, first_t = times[0]
-    if first_t <= best_t * (1.0 + keep_default_within):
-        best_c = first_c
+
+    def pick(cands):
+        best = [float("inf")] * len(cands)
+        try:
+            for _ in range(sweeps):   # interleaved sweeps; a candidate keeps its best time
+                for i, c in enumerate(cands):
+                    M.set_tuning(**c)
+                    best[i] = min(best[i], float(timer()))
+        except BaseException:
+            M.set_tuning(**start)
+            raise
+        tm = [(dict(c), t) for c, t in zip(cands, best)]
+        best_c, best_t = min(tm, key=lambda ct: ct[1])
+        if tm[0][1] <= best_t * (1.0 + keep_default_within):
+            best_c = tm[0][0]
+        return best_c, tm
+
+    best_c, times = pick(candidates(start, nrhs))
+    if nrhs <= 1:
+        best_c, t2 = pick([dict(best_c, side_at=k) for k in SIDE_AT])
+        times += t2[1:]
     M.set_tuning(**best_c)
     out = {"tuning": M.tuning, "times_ms": times, "cached": False, "key": key}
     if path is not None:
@@ -191,9 +200,9 @@ PLAN_CANDIDATES = {
     "finish_slots": (16, 8, 32, 64),
     # 64-vector T-form: tiles per piece of a long column cluster
     "piece_tiles": (32, 16, 8),
-    # one-vector products: the near field fused into the last pass (1) or
-    # its own pass on a side stream (2); 0 is the planner's default
-    "near_field": (0, 1, 2),
+    # one-vector products: the near field on a side stream (0, the default)
+    # or fused into the last pass (1)
+    "near_field": (0, 1),
 }
 
 
@@ -208,31 +217,39 @@ def autotune_plan(upload_fn: Callable[[dict], object], nrhs: int = 1, op: int = 
     first value is the default), one knob at a time, the others at their
     current choice, and products are timed with CUDA events as in
     ``autotune``.  The default is kept unless another value is faster by more
-    than ``keep_default_within``.  Returns (handle of the chosen plan,
+    than ``keep_default_within``.  Candidates are uploaded and timed one after
+    another, so that at most two handles (the best so far and the newest)
+    hold device memory at once.  Returns (handle of the chosen plan,
     {"plan": choice, "times_ms": [(plan, ms), ...]}); the other handles are
     freed.  ``timer_for(M)`` (tests) replaces the event timer; ``graph``
     times CUDA graph replays, as ``event_timer``."""
     choice, times = {}, []
-    best_M = None
+    best_M = None   # the handle of `choice`
+
+    def timed(M):
+        timer = timer_for(M) if timer_for is not None else event_timer(M, nrhs, op, graph=graph)
+        return min(float(timer()) for _ in range(sweeps))
+
     for knob in knobs:
-        cands = []
-        for v in PLAN_CANDIDATES[knob]:
+        vals = PLAN_CANDIDATES[knob]
+        # the incumbent: the choice so far with the knob at its default
+        # (the handle of the previous knob's choice is that plan)
+        plan0 = dict(choice, **{knob: vals[0]})
+        if best_M is None:
+            best_M = upload_fn(plan0)
+        t0 = timed(best_M)
+        times.append((plan0, t0))
+        best_plan, best_t, best_is_default = plan0, t0, True
+        # one candidate at a time: at most two handles exist at once
+        for v in vals[1:]:
             plan = dict(choice, **{knob: v})
             M = upload_fn(plan)
-            timer = timer_for(M) if timer_for is not None else event_timer(M, nrhs, op, graph=graph)
-            cands.append([plan, M, timer, float("inf")])
-        for _ in range(sweeps):
-            for c in cands:
-                c[3] = min(c[3], float(c[2]()))
-        times += [(dict(c[0]), c[3]) for c in cands]
-        best = min(cands, key=lambda c: c[3])
-        if cands[0][3] <= best[3] * (1.0 + keep_default_within):
-            best = cands[0]
-        choice = dict(best[0])
-        for c in cands:
-            if c is not best:
-                c[1].free()
-        if best_M is not None and best_M is not best[1]:
-            best_M.free()
-        best_M = best[1]
+            t = timed(M)
+            times.append((plan, t))
+            if t * (1.0 + keep_default_within if best_is_default else 1.0) < best_t:
+                best_M.free()
+                best_M, best_plan, best_t, best_is_default = M, plan, t, False
+            else:
+                M.free()
+        choice = dict(best_plan)
     return best_M, {"plan": choice, "times_ms": times}

@@ -203,8 +203,9 @@ typedef struct hlrc_options {
      * every block of a row, tbb/detail/arith.hh:95-124); 2 = D x is its own
      * pass, launched on a side stream at the start of the product and joined
      * before the pass that adds the low-rank part to y, so that it overlaps
-     * the dependent low-rank passes; 0 = default (2 for uniform-H and H2, 1
-     * for H).  Both add D x first, then the low-rank part, per row tile.   */
+     * the dependent low-rank passes; 0 = default (2).  With 2, D x is added
+     * first, then the low-rank part, per row tile; the 64-vector product of
+     * 16-bit stores always takes the fused pass.                          */
     int32_t near_field;
     int32_t reserved[3];
 } hlrc_options;
@@ -396,7 +397,12 @@ typedef struct hlrc_tuning {
     int32_t mr_min_nrhs;
     int32_t wide_min_nrhs;
     int32_t overlap;
-    int32_t reserved[3];
+    /* products with the near field on a side stream (hlrc_options.near_field):
+     * the side pass is forked after this many of the other passes have been
+     * launched (0 = at the start; 0..16, clamped to the pass that adds the
+     * low-rank part to y).  Results do not depend on it.                   */
+    int32_t side_at;
+    int32_t reserved[2];
 } hlrc_tuning;
 
 hlrc_status hlrc_get_tuning(hlrc_hmat M, hlrc_tuning* t);

@@ -1,5 +1,5 @@
 """The near field of a one-vector product as its own pass on a side stream
-(hlrc_options.near_field = 2, the default for uniform-H and H2).
+(hlrc_options.near_field = 2, the default).
 
 HLR sums every block of a row into y (tbb/detail/arith.hh:95-124); here the
 dense leaves' D x is one pass and the low-rank part another, both per row
@@ -118,6 +118,13 @@ def test_side_stream_products_are_bit_identical_on_every_path(kind):
     other = torch.cuda.Stream()
     assert np.array_equal(chain(1, False, W, other), plain)
     assert np.array_equal(chain(1, True, W, other), plain)
+    # the side pass forked later (after 1..3 other passes, clamped before
+    # the pass that joins it): the same kernels in the same order on y
+    for k in (1, 2, 3, 16):
+        M.set_tuning(side_at=k)
+        assert np.array_equal(chain(1, True), plain), k
+        assert np.array_equal(chain(1, False, W, other), plain), k
+    M.set_tuning(side_at=0)
     # the no-alloc entry point has no side stream: D x runs first in line
     y = torch.zeros_like(x)
     for a in alphas:
@@ -155,3 +162,36 @@ def test_graph_replay_profiles_the_side_pass(kind):
         assert cnt == 3 and ms > 0 and by > 0, (name, cnt, ms, by)
     del g
     M.free()
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed", "bfp"])
+def test_side_stream_in_eight_vector_products(prec):
+    """The 8-vector kernels take the same split: D X on the side stream after
+    x is staged, U T after the join.  Against the fused plan the result
+    differs by summation order only; against the oracle, by the store's
+    precision."""
+    hm = CASES["h"]()
+    M1 = hlr.upload(hm, precision=prec, max_nrhs=8, plan={"near_field": 1})
+    M2 = hlr.upload(hm, precision=prec, max_nrhs=8, plan={"near_field": 2})
+    rng = np.random.default_rng(21)
+    X = rng.standard_normal((hm.n, 8))
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).cuda().T
+    outs = []
+    for M in (M1, M2):
+        M.set_profiling(True)
+        M.last_profile()
+        Yd = torch.zeros((8, hm.n), dtype=torch.float64, device="cuda").T
+        hlr.mul_vec(0.75, 0, M, Xd, Yd)
+        torch.cuda.synchronize()
+        prof = M.last_profile()
+        M.set_profiling(False)
+        outs.append((Yd.cpu().numpy(), prof))
+    assert "nform_Dx" in outs[1][1] and "nform_Dx" not in outs[0][1]
+    tol = 1e-13 if prec == "f64" else 2e-6
+    for j in range(8):
+        yo = _oracle(hm, "h", 0.75, 0, np.ascontiguousarray(X[:, j]), np.zeros(hm.n))
+        for Y, _ in outs:
+            assert relerr(Y[:, j], yo) <= tol, (prec, j)
+        assert relerr(outs[0][0][:, j], outs[1][0][:, j]) <= (1e-14 if prec == "f64" else 1e-6), (prec, j)
+    M1.free()
+    M2.free()

@@ -38,7 +38,7 @@ def test_all_settings_agree(c2_small, prec):
     X = np.random.default_rng(5).standard_normal((c2_small.n, 8))
     ref1 = run(M, X, 1)
     ref8 = run(M, X, 8)
-    for c in tune.candidates(M.tuning, 1):
+    for c in tune.candidates(M.tuning, 1) + [dict(tune.DEFAULT, side_at=k) for k in tune.SIDE_AT]:
         M.set_tuning(**c)
         assert M.tuning == c
         assert relerr(run(M, X, 1), ref1) <= TOL[prec], c
@@ -54,7 +54,7 @@ def test_all_settings_agree(c2_small, prec):
 def test_invalid_settings_rejected(c2_small):
     M = hlr.upload(c2_small, precision="f64")
     for bad in ({"nform_warps": 6}, {"ttform_warps": 32}, {"mr_min_nrhs": 1}, {"mr_min_nrhs": HLRC_MR_NEVER + 1},
-                {"overlap": 2}):
+                {"overlap": 2}, {"side_at": -1}, {"side_at": 17}, {"nform_warps": 4, "side_at": 99}):
         with pytest.raises(hlr.HLRCError):
             M.set_tuning(**bad)
         assert M.tuning == tune.DEFAULT
@@ -67,7 +67,8 @@ def test_autotune_on_device(c2_small, tmp_path):
     r1 = tune.autotune(M, nrhs=1, cache=path, reps=2, warmup=1)
     r8 = tune.autotune(M, nrhs=8, cache=path, reps=2, warmup=1)
     assert not r1["cached"] and not r8["cached"]
-    assert len(r1["times_ms"]) == len(tune.candidates(tune.DEFAULT, 1)) and len(r8["times_ms"]) == 2
+    assert len(r1["times_ms"]) == len(tune.candidates(tune.DEFAULT, 1)) + len(tune.SIDE_AT) - 1
+    assert len(r8["times_ms"]) == 2
     assert all(t > 0 for _, t in r1["times_ms"] + r8["times_ms"])
     assert M.tuning["nform_warps"] in (4, 8, 16) and M.tuning["mr_min_nrhs"] in (2, HLRC_MR_NEVER)
     assert len(json.loads(path.read_text())) == 2

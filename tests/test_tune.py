@@ -56,8 +56,9 @@ def test_picks_fastest_and_caches(tmp_path):
     t, calls = timer_for(M, lambda s: 1.0 if s["nform_warps"] == 4 and s["ttform_warps"] == 8 else 2.0)
     path = tmp_path / "tuning.json"
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="GPU-X")
-    assert not r["cached"] and len(calls) == 18     # two sweeps of nine
-    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1}
+    assert not r["cached"] and len(calls) == 18 + 8   # two sweeps of nine, then of the four fork points
+    assert M.tuning == {"nform_warps": 4, "ttform_warps": 8, "mr_min_nrhs": 2, "wide_min_nrhs": 9, "overlap": 1,
+                        "side_at": 0}
     d = json.loads(path.read_text())
     assert d[r["key"]]["tuning"] == M.tuning
     # a fresh handle of the same signature takes the cached setting untimed
@@ -82,6 +83,18 @@ def test_default_kept_within_noise():
     assert tune.autotune(M, nrhs=1, cache=None, timer=t, device_name="G")["tuning"] != tune.DEFAULT
 
 
+def test_side_fork_point_tuned_at_the_chosen_warps():
+    """One vector: the fork point of the near field's side pass is timed in
+    a second phase, at the launch shapes the first phase picked."""
+    M = FakeMatrix()
+    t, calls = timer_for(M, lambda s: (1.0 if s["nform_warps"] == 16 else 2.0) - (0.5 if s["side_at"] == 2 else 0.0))
+    r = tune.autotune(M, nrhs=1, cache=None, timer=t, device_name="G")
+    assert r["tuning"]["nform_warps"] == 16 and r["tuning"]["side_at"] == 2
+    assert all(c["nform_warps"] == 16 for c in calls[18:])
+    assert [c["side_at"] for c in calls[18:22]] == list(tune.SIDE_AT)
+    assert len(r["times_ms"]) == 9 + 3
+
+
 def test_multi_vector_choice():
     M = FakeMatrix()
     t, calls = timer_for(M, lambda s: 5.0 if s["mr_min_nrhs"] == 2 else 9.0)
@@ -98,13 +111,13 @@ def test_bad_cache_entries_are_retuned(tmp_path):
     M = FakeMatrix()
     t, calls = timer_for(M, lambda s: 1.0)
     r = tune.autotune(M, nrhs=1, cache=path, timer=t, device_name="G")
-    assert not r["cached"] and len(calls) == 18     # two sweeps of nine
+    assert not r["cached"] and len(calls) == 26
     d = json.loads(path.read_text())
     d[r["key"]]["tuning"] = {"nform_warps": 5, "ttform_warps": 8, "mr_min_nrhs": 2}   # rejected by the handle
     path.write_text(json.dumps(d))
     M2 = FakeMatrix()
     t2, calls2 = timer_for(M2, lambda s: 1.0)
-    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 18
+    assert not tune.autotune(M2, nrhs=1, cache=path, timer=t2, device_name="G")["cached"] and len(calls2) == 26
 
 
 def test_timer_failure_restores_setting():
@@ -158,6 +171,29 @@ def test_autotune_plan_times_each_knob_and_frees_the_losers():
     assert M.plan == out["plan"] and not M.freed
     assert all(m.freed for m in made if m is not M)
     assert len(out["times_ms"]) == len(tune.PLAN_CANDIDATES["finish_slots"]) + len(tune.PLAN_CANDIDATES["piece_tiles"])
+
+
+def test_autotune_plan_holds_at_most_two_handles():
+    """Candidates are uploaded one at a time; a loser is freed before the
+    next upload, so a plan whose store takes most of the device still
+    tunes."""
+    live, peak = [], [0]
+
+    class Tracked(FakePlanned):
+        def __init__(self, plan):
+            super().__init__(plan)
+            live.append(self)
+            peak[0] = max(peak[0], len(live))
+
+        def free(self):
+            super().free()
+            live.remove(self)
+
+    M, out = tune.autotune_plan(Tracked, knobs=("finish_slots", "near_field"),
+                                timer_for=lambda M: (lambda: 1.0 - 0.1 * (M.plan.get("finish_slots") == 64)))
+    assert out["plan"]["finish_slots"] == 64 and out["plan"]["near_field"] == 0
+    assert peak[0] == 2 and live == [M]
+    assert len(out["times_ms"]) == len(tune.PLAN_CANDIDATES["finish_slots"]) + len(tune.PLAN_CANDIDATES["near_field"])
 
 
 def test_autotune_plan_keeps_default_within_noise():
