@@ -734,10 +734,12 @@ def run_batch(args, rank, world, local_rank):
         return max_over_ranks(e0.elapsed_time(e1), world, dev), M.launch_count() - l0
 
     y = torch.zeros_like(bt)
-    Alow.set_profiling(True)
-    Alow.last_profile()  # clear
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         ms, launches = timed(Alow, bt.T, y.T, args.steps)
+    # the pass profile: a few more products with per-pass events, untimed
+    Alow.set_profiling(True)
+    Alow.last_profile()  # clear
+    timed(Alow, bt.T, y.T, min(args.steps, 4))
     prof = Alow.last_profile()
     Alow.set_profiling(False)
     y64 = torch.zeros_like(bt)
@@ -799,6 +801,8 @@ def run_batch(args, rank, world, local_rank):
         "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "peak_kind": peak_kind,
         "roofline": roofline_from_profile(prof, hbm_peak, peak_kind,
                                           "c5" + ("" if inner == "f64" else "/" + inner) + f"/{nrhs}"),
+        "passes": {k: {"launches": v[0], "avg_ms": v[1] / max(1, v[0]), "bytes_per_launch": v[2]}
+                   for k, v in prof.items()},
         "rel_err_vs_fp64": rel_err,
         "fp64_gpu": {"value": v64, "ms_per_step": ms64 / args.steps, "speedup": value / world / v64,
                      "note": "same batch, same right-hand sides, FP64 store"},
