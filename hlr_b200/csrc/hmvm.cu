@@ -1569,11 +1569,14 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
+                const int b1 = fin_gpb(tp.ngroups1), b2 = fin_gpb(tp.ngroups);
                 if (tp.ngroups1 > 0)   // first level: runs of slots into the scratch part of the partials
-                    L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups1 + 7) / 8), 256, 0, s, tp.groups1, tp.ngroups1,
-                               static_cast<const double*>(ws.part), ws.part, 1.0, 0));
-                L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups + 7) / 8), 256, 0, s, tp.groups, tp.ngroups,
-                           static_cast<const double*>(ws.part), vout, alpha, add));
+                    L(launch_k(ov, k_ttfinish_flat<1, double, false>, unsigned((tp.ngroups1 + b1 - 1) / b1), 256, 0,
+                               s, tp.groups1, tp.ngroups1, b1, static_cast<const double*>(ws.part),
+                               OutMap{ws.part, 1, 0, 1}, static_cast<double*>(nullptr), 1.0, 0));
+                L(launch_k(ov, k_ttfinish_flat<1, double, false>, unsigned((tp.ngroups + b2 - 1) / b2), 256, 0, s,
+                           tp.groups, tp.ngroups, b2, static_cast<const double*>(ws.part), OutMap{vout, 1, 0, 1},
+                           static_cast<double*>(nullptr), alpha, add));
                 if (ws.profile) prof_end(M, s);
             }
             HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));
@@ -1718,18 +1721,21 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                     // first level: runs of slots into the scratch part of the partials
                     const OutMap pm{ws.mr_part, MR_RB, 1, MR_RB};
                     float* fpart = reinterpret_cast<float*>(ws.mr_part);
+                    const int b1 = fin_gpb(tp.ngroups1), b2 = fin_gpb(tp.ngroups);
+                    const unsigned fg1 = unsigned((tp.ngroups1 + b1 - 1) / b1);
+                    const unsigned fg = unsigned((tp.ngroups + b2 - 1) / b2);
                     if (M->precision == HLRC_PREC_F64) {
                         if (tp.ngroups1 > 0)
-                            k_ttfinish_f64_mr<<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, ws.mr_part,
-                                                                                   pm, 1.0, 0);
-                        k_ttfinish_f64_mr<<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, ws.mr_part, om,
-                                                                              alpha, add);
+                            k_ttfinish_flat<MR_RB, double, false><<<fg1, 256, 0, s>>>(
+                                tp.groups1, tp.ngroups1, b1, ws.mr_part, pm, static_cast<double*>(nullptr), 1.0, 0);
+                        k_ttfinish_flat<MR_RB, double, false><<<fg, 256, 0, s>>>(
+                            tp.groups, tp.ngroups, b2, ws.mr_part, om, static_cast<double*>(nullptr), alpha, add);
                     } else {
                         if (tp.ngroups1 > 0)
-                            k_ttfinish_f32_mr<true><<<(tp.ngroups1 + 7) / 8, 256, 0, s>>>(tp.groups1, tp.ngroups1, fpart,
-                                                                                         pm, fpart, 1.0, 0);
-                        k_ttfinish_f32_mr<false><<<(tp.ngroups + 7) / 8, 256, 0, s>>>(tp.groups, tp.ngroups, fpart, om,
-                                                                                     nullptr, alpha, add);
+                            k_ttfinish_flat<MR_RB, float, true><<<fg1, 256, 0, s>>>(tp.groups1, tp.ngroups1, b1, fpart,
+                                                                                    pm, fpart, 1.0, 0);
+                        k_ttfinish_flat<MR_RB, float, false><<<fg, 256, 0, s>>>(
+                            tp.groups, tp.ngroups, b2, fpart, om, static_cast<float*>(nullptr), alpha, add);
                     }
                     nl += 1 + (tp.ngroups1 > 0 ? 1 : 0);
                     if (ws.profile) prof_end(M, s);

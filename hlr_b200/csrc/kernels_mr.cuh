@@ -13,6 +13,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels_f64.cuh"
 #include "layout.hpp"
 
@@ -36,59 +38,106 @@ struct OutMap {            // output element (i, r) lives at base[i * rs + r * c
     int nr;                // valid right-hand sides
 };
 
-// Sums per-tile partials (row-major, MR_RB vectors) of multi-tile outputs:
-// slot i, column j, vector k of a group is part[(slot0 + i*nc + j)*MR_RB + k].
-// A lane owns a pair of vectors of one column and keeps four interleaved
-// sums (four 16-byte loads in flight), combined in a fixed order.
+// Finish of the tile T-form with a flat thread map: a CTA takes gpb (at most
+// FIN_GROUPS, fin_gpb) consecutive groups, and each thread one vector of VEC
+// entries (output
+// column j, right-hand sides k .. k+VEC-1) of them, NR right-hand sides per
+// partial entry (1 for one-vector products, MR_RB for the multi-vector
+// kernels).  Slot i of a group holds its entries at
+// part[(slot0 + i*nc + j)*NR + k].  Each entry is summed in a fixed order:
+// four FP64 accumulators, slot a going to accumulator a mod 4 when
+// a < (nslots rounded down to a multiple of 4) and to the first otherwise,
+// each accumulator taking its slots in increasing order; the result is
+// (s0 + s1) + (s2 + s3).  The loads of FIN_BATCH slots are issued before
+// their sums, so a short group (a few slots of a few columns, the common
+// case) costs one round trip, and the short groups of a CTA fill its
+// threads together.  TO_PART writes the sums (as T) to
+// part_out[(out + j)*NR + k] (the first level of long outputs); otherwise
+// they go to the output map, with alpha/add.
+constexpr int FIN_GROUPS = 32;
+constexpr int FIN_BATCH = 8;
+
+// Groups per CTA of a finish launch: about 16 CTAs per SM of the 148, so
+// that few long groups (the first level) still spread over the GPU.
+inline int fin_gpb(int ngroups) {
+    constexpr int target = 148 * 16;
+    return std::max(1, std::min(FIN_GROUPS, (ngroups + target - 1) / target));
+}
+
+template <typename T, int VEC> struct FinVec { using type = T; };
+template <> struct FinVec<float, 2> { using type = float2; };
+template <> struct FinVec<double, 2> { using type = double2; };
+
+template <int NR, typename T, bool TO_PART>
 __global__ void __launch_bounds__(256)
-k_ttfinish_f64_mr(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part, OutMap om,
-                  double alpha, int add) {
-    const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (gid >= ngroups) return;
-    const int lane = threadIdx.x & 31;
-    const TGroup g = groups[gid];
-    constexpr uint32_t PAIRS = MR_RB / 2;
-    const uint32_t n2 = g.nc * PAIRS;
-    const double2* p0 = reinterpret_cast<const double2*>(part + size_t(g.slot0) * MR_RB);
-    for (uint32_t q = lane; q < n2; q += 32) {
-        const uint32_t j = q / PAIRS;
-        const int k = int(2 * (q % PAIRS));
+k_ttfinish_flat(const TGroup* __restrict__ groups, int ngroups, int gpb, const T* part, OutMap om, T* part_out,
+                double alpha, int add) {
+    // 8-byte (FP32 pairs) or 16-byte (FP64 pairs) loads
+    constexpr int VEC = NR % 2 == 0 ? 2 : 1;
+    constexpr int PER = NR / VEC;   // vectors per column entry
+    using V = typename FinVec<T, VEC>::type;
+    static_assert(sizeof(V) == VEC * sizeof(T), "vector type");
+    static_assert(FIN_BATCH % 4 == 0, "a batch keeps the accumulator of a slot at a mod 4");
+    __shared__ TGroup sg[FIN_GROUPS];
+    __shared__ uint32_t pre[FIN_GROUPS + 1];
+    pdl_trigger();
+    const int g0 = int(blockIdx.x) * gpb;
+    const int ng = min(gpb, ngroups - g0);
+    if (int(threadIdx.x) < ng) sg[threadIdx.x] = groups[g0 + int(threadIdx.x)];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int q = 0; q < ng; ++q) {
+            pre[q] = acc;
+            acc += sg[q].nc * uint32_t(PER);
+        }
+        pre[ng] = acc;
+    }
+    __syncthreads();
+    pdl_wait();
+    const uint32_t total = pre[ng];
+    int lo = 0;   // the group holding item `it` (pre[lo] <= it < pre[lo + 1]); items only move forward
+    for (uint32_t it = threadIdx.x; it < total; it += blockDim.x) {
+        while (pre[lo + 1] <= it) ++lo;
+        const TGroup g = sg[lo];
+        const uint32_t e = it - pre[lo];
+        const uint32_t j = e / PER;
+        const int k = int(e % PER) * VEC;
         if (k >= om.nr) continue;
-        const double2* p = p0 + q;
-        double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
-        uint32_t i = 0;
-        // sixteen loads in flight, then the same sums in the same order
-        for (; i + 16 <= g.nslots; i += 16) {
-            double2 v[16];
+        const size_t stride = size_t(g.nc) * PER;
+        const V* p = reinterpret_cast<const V*>(part + size_t(g.slot0) * NR) + e;
+        const uint32_t f4 = g.nslots & ~3u;
+        double s[4][VEC] = {};
+        for (uint32_t i = 0; i < g.nslots; i += FIN_BATCH) {
+            V v[FIN_BATCH];
 #pragma unroll
-            for (int a = 0; a < 16; ++a) v[a] = __ldcs(p + size_t(i + a) * n2);
+            for (int a = 0; a < FIN_BATCH; ++a)
+                if (i + a < g.nslots) v[a] = __ldcs(p + (i + a) * stride);
 #pragma unroll
-            for (int a = 0; a < 16; a += 4) {
-                s0.x += v[a].x; s0.y += v[a].y;
-                s1.x += v[a + 1].x; s1.y += v[a + 1].y;
-                s2.x += v[a + 2].x; s2.y += v[a + 2].y;
-                s3.x += v[a + 3].x; s3.y += v[a + 3].y;
+            for (int a = 0; a < FIN_BATCH; ++a) {
+                const uint32_t sl = i + a;
+                if (sl >= g.nslots) break;
+                const T* x = reinterpret_cast<const T*>(&v[a]);
+                if (sl < f4) {   // i is a multiple of 4: sl mod 4 == a mod 4
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) s[a & 3][q] += double(x[q]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) s[0][q] += double(x[q]);
+                }
             }
         }
-        for (; i + 4 <= g.nslots; i += 4) {
-            const double2 a = __ldcs(p + size_t(i) * n2), b = __ldcs(p + size_t(i + 1) * n2);
-            const double2 c = __ldcs(p + size_t(i + 2) * n2), d = __ldcs(p + size_t(i + 3) * n2);
-            s0.x += a.x; s0.y += a.y;
-            s1.x += b.x; s1.y += b.y;
-            s2.x += c.x; s2.y += c.y;
-            s3.x += d.x; s3.y += d.y;
-        }
-        for (; i < g.nslots; ++i) {
-            const double2 a = __ldcs(p + size_t(i) * n2);
-            s0.x += a.x; s0.y += a.y;
-        }
-        const double r0 = (s0.x + s1.x) + (s2.x + s3.x), r1 = (s0.y + s1.y) + (s2.y + s3.y);
-        double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
-        if (add) *o += alpha * r0;
-        else *o = r0;
-        if (k + 1 < om.nr) {
-            if (add) o[om.cs] += alpha * r1;
-            else o[om.cs] = r1;
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const double r = (s[0][q] + s[1][q]) + (s[2][q] + s[3][q]);
+            if constexpr (TO_PART) {
+                part_out[size_t(g.out + j) * NR + k + q] = T(r);
+            } else {
+                if (k + q >= om.nr) break;
+                double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k + q) * om.cs;
+                if (add) *o += alpha * r;
+                else *o = r;
+            }
         }
     }
 }

@@ -224,68 +224,6 @@ __device__ __forceinline__ void tt_out(const MCol& m, int n, double val, const O
     }
 }
 
-// Sums FP32 per-tile partials (row-major, MR_RB vectors) of multi-tile
-// outputs in FP64: slot i, column j, vector k of a group is
-// part[(slot0 + i*nc + j)*MR_RB + k].  A lane owns four vectors of one
-// column and keeps four interleaved sums; fixed order.
-// With TO_PART the sums are written as FP32 partials (the first level of a
-// two-level finish) to part_out[(g.out + j)*MR_RB + k] instead of to om.
-template <bool TO_PART>
-__global__ void __launch_bounds__(256)
-k_ttfinish_f32_mr(const TGroup* __restrict__ groups, int ngroups, const float* part, OutMap om, float* part_out,
-                  double alpha, int add) {
-    const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (gid >= ngroups) return;
-    const int lane = threadIdx.x & 31;
-    const TGroup g = groups[gid];
-    constexpr uint32_t QUADS = MR_RB / 4;
-    const uint32_t n4 = g.nc * QUADS;
-    const float4* p0 = reinterpret_cast<const float4*>(part + size_t(g.slot0) * MR_RB);
-    for (uint32_t q = lane; q < n4; q += 32) {
-        const uint32_t j = q / QUADS;
-        const int k = int(4 * (q % QUADS));
-        if (k >= om.nr) continue;
-        const float4* p = p0 + q;
-        double s[4][4] = {};
-        uint32_t i = 0;
-        // sixteen loads in flight, then the same sums in the same order
-        for (; i + 16 <= g.nslots; i += 16) {
-            float4 v[16];
-#pragma unroll
-            for (int a = 0; a < 16; ++a) v[a] = __ldcs(p + size_t(i + a) * n4);
-#pragma unroll
-            for (int a = 0; a < 16; ++a) {
-                s[a & 3][0] += v[a].x; s[a & 3][1] += v[a].y; s[a & 3][2] += v[a].z; s[a & 3][3] += v[a].w;
-            }
-        }
-        for (; i + 4 <= g.nslots; i += 4) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const float4 v = __ldcs(p + size_t(i + a) * n4);
-                s[a][0] += v.x; s[a][1] += v.y; s[a][2] += v.z; s[a][3] += v.w;
-            }
-        }
-        for (; i < g.nslots; ++i) {
-            const float4 v = __ldcs(p + size_t(i) * n4);
-            s[0][0] += v.x; s[0][1] += v.y; s[0][2] += v.z; s[0][3] += v.w;
-        }
-        if constexpr (TO_PART) {
-            float* o = part_out + size_t(g.out + j) * MR_RB + k;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) o[e] = float((s[0][e] + s[1][e]) + (s[2][e] + s[3][e]));
-        } else {
-            double* o = om.base + int64_t(g.out + j) * om.rs + int64_t(k) * om.cs;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                if (k + e >= om.nr) break;
-                const double r = (s[0][e] + s[1][e]) + (s[2][e] + s[3][e]);
-                if (add) o[e * om.cs] += alpha * r;
-                else o[e * om.cs] = r;
-            }
-        }
-    }
-}
-
 // Fixed-order sum of the per-warp accumulators of an N-form tile
 // (red[(w * TILE + row) * MR_RB + k]) and the update of the output rows.
 __device__ __forceinline__ void nform_store(const double* red, int out, int rows, const OutMap& om, double alpha,
