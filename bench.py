@@ -259,7 +259,7 @@ def run_reference_batch(args, nthreads):
     would take more than ~120 s for all steps, a step covers every k-th
     member and the rate is scaled by the matrix bytes covered."""
     import hlr_b200 as hlr
-    hms = [hlr.build(p) for p in c5_problems(nthreads=nthreads)]
+    hms = [hlr.build(p) for p in c5_problems(args.members, nthreads=nthreads)]
     rng = np.random.default_rng(9)
     xs = [rng.standard_normal(h.n) for h in hms]
     descs = [h.h_desc() for h in hms]
@@ -282,7 +282,7 @@ def run_reference_batch(args, nthreads):
         step(idx)
     el = time.perf_counter() - t0
     value = len(hms) * args.steps * frac / el
-    sample = ("all 32 members per step" if stride == 1 else
+    sample = (f"all {len(hms)} members per step" if stride == 1 else
               f"every {stride}-th member per step ({frac * 100:.1f}% of matrix bytes), scaled")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "MVM/s", "n_gpus": args.gpus,
@@ -668,7 +668,7 @@ def run_batch(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     nrhs = args.nrhs or 8
     inner = args.precision or "mixed"
-    count = 32
+    count = args.members
     tb = time.perf_counter()
     probs = c5_problems(count, nthreads=os.cpu_count() or 0)
     for p in probs:
@@ -1027,6 +1027,8 @@ def main():
                     help="one product over all ranks: rows sharded, x all-gathered per step (strong scaling)")
     ap.add_argument("--tune-plan", action="store_true", default=None,
                     help="also tune plan-level choices by re-uploading (default: on for c1, c4 and c5)")
+    ap.add_argument("--members", type=int, default=32,
+                    help="c5: the first N members of the batch (32, the workload; fewer for profiling)")
     ap.add_argument("--plan", default="", help="plan-level choices k=v[,k=v] (finish_slots, piece_tiles, "
                     "near_field), before any plan tuning")
     ap.add_argument("--host-build", action="store_true",
