@@ -709,9 +709,9 @@ hlrc_status enable_tc_smem(int dev) {
     HLRC_CUDA(cudaFuncSetAttribute(k_ttform_mr<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_TT)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_N16)));
+                                   tc_smem_bytes(TC_STAGE_N16, TC_STAGES_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_N16)));
+                                   tc_smem_bytes(TC_STAGE_N16, TC_STAGES_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_d32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N32, TC_STAGES_D32)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_bfp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bq_smem_n(true)));
@@ -1765,12 +1765,14 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                     ++nl;
                 }
                 if (!f64plan && np.nmseg[FMT_F16] > 0) {
-                    k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
+                    k_nform_tc<FMT_F16><<<np.nmseg[FMT_F16], TC_WARPS * 32,
+                                          tc_smem_bytes(TC_STAGE_N16, TC_STAGES_N16), s>>>(
                         np.mseg[FMT_F16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                     ++nl;
                 }
                 if (!f64plan && np.nmseg[FMT_BF16] > 0) {
-                    k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_N16), s>>>(
+                    k_nform_tc<FMT_BF16><<<np.nmseg[FMT_BF16], TC_WARPS * 32,
+                                           tc_smem_bytes(TC_STAGE_N16, TC_STAGES_N16), s>>>(
                         np.mseg[FMT_BF16], np.mcol, M->store, vec(np.vx), vec(np.vt), om, alpha, add);
                     ++nl;
                 }

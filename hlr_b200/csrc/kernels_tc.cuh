@@ -51,6 +51,13 @@ constexpr int TC_STAGE_T32 = 16 * TC_A32_STRIDE + 16 * 8;
 #define HLRC_D32_STAGES 2
 #endif
 constexpr int TC_STAGES_D32 = HLRC_D32_STAGES;   // ring depth of the FP32 N-form
+#ifndef HLRC_N16_STAGES
+#define HLRC_N16_STAGES 2
+#endif
+constexpr int TC_STAGES_N16 = HLRC_N16_STAGES;   // ring depth of the 16-bit N-form
+#ifndef HLRC_N16_MINB
+#define HLRC_N16_MINB 1
+#endif
 
 // dynamic shared memory of a launch: one ring of `nst` stages per warp
 constexpr int tc_smem_bytes(int stage, int nst = TC_STAGES) { return TC_WARPS * nst * stage; }
@@ -335,7 +342,7 @@ __device__ __forceinline__ void ttform_tc(const MSeg& sg, uint8_t* smem, const M
 // (g, t) accumulates rows 16i + g, 16i + g + 8 (i < 4) for right-hand sides
 // 2t, 2t+1; fixed-order cross-warp sum at the end.
 template <int FMT>
-__global__ void __launch_bounds__(TC_WARPS * 32)
+__global__ void __launch_bounds__(TC_WARPS * 32, HLRC_N16_MINB)
 k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
            const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     using O = TcOp<FMT>;
@@ -343,7 +350,7 @@ k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const u
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_N16);
+    uint8_t* ring = smem + warp * (TC_STAGES_N16 * TC_STAGE_N16);
     const int colb = sg.ld * 2, ncols = int(sg.ncols);
     const uint8_t* base = A + size_t(sg.a16) * 16;
     const MCol* ctab = cols + sg.col0;
@@ -354,7 +361,7 @@ k_nform_tc(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const u
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
     MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<TC_STAGES_N16>(
         (ncols + 31) / 32, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_N16;
