@@ -340,7 +340,10 @@ hlrc_status hlrc_mvm_host(hlrc_hmat M, double alpha, int op, const double* x,
  *    call's contents (each call writes every entry before reading it).  Calls
  *    that overlap on the GPU — on different streams, or with different
  *    handles on the same device — race; order them on one stream.
- *  - Uniform-H and H^2 handles are accepted (op N and C).                 */
+ *  - Uniform-H and H^2 handles are accepted (op N and C).
+ *  - A near field planned as its own pass (hlrc_options.near_field) runs
+ *    first on `stream`, not beside the other passes: the same kernels in
+ *    the same order on y, so the same result as hlrc_mvm.               */
 hlrc_status hlrc_mvm_noalloc(hlrc_hmat M, double alpha, int op,
                              const double* x, double* y, void* stream);
 
