@@ -30,6 +30,18 @@
 
 namespace hlrc {
 
+// One stage per warp and at least 3 CTAs per SM: on a 4-member batched
+// problem (BFP store, 8 vectors) the N-form passes took 0.151 / 0.200 ms and
+// the tile T-form 0.277 ms, against 0.184 / 0.200 / 0.309 ms with two
+// stages and no register bound (the N-forms then held 164 and 204
+// registers and 2 CTAs per SM).
+#ifndef HLRC_BQ_STAGES
+#define HLRC_BQ_STAGES 1
+#endif
+constexpr int BQ_STAGES = HLRC_BQ_STAGES;                         // ring depth per warp
+#ifndef HLRC_BQ_MINB
+#define HLRC_BQ_MINB 3
+#endif
 constexpr int BQ_LO_STRIDE = 80;                                  // raw low bytes of a 24-bit column (<= 64) + pad
 constexpr int BQ_PLANE = 32 * TC_A16_STRIDE;                      // one widened low-byte plane of a stage
 constexpr int BQ_STAGE_N16 = TC_STAGE_N16;                        // as FP16
@@ -40,10 +52,10 @@ constexpr int BQ_STAGE_T24 = 32 * TC_A16_STRIDE + 32 * BQ_LO_STRIDE + 32 * 8;
 // dynamic shared memory of a launch: per warp a ring of stages, plus the
 // widened low-byte plane for 24-bit columns
 constexpr int bq_smem_n(bool i24) {
-    return TC_WARPS * (TC_STAGES * (i24 ? BQ_STAGE_N24 : BQ_STAGE_N16) + (i24 ? BQ_PLANE : 0));
+    return TC_WARPS * (BQ_STAGES * (i24 ? BQ_STAGE_N24 : BQ_STAGE_N16) + (i24 ? BQ_PLANE : 0));
 }
 constexpr int bq_smem_t(bool i24) {
-    return TC_WARPS * (TC_STAGES * (i24 ? BQ_STAGE_T24 : BQ_STAGE_T16) + (i24 ? BQ_PLANE : 0));
+    return TC_WARPS * (BQ_STAGES * (i24 ? BQ_STAGE_T24 : BQ_STAGE_T16) + (i24 ? BQ_PLANE : 0));
 }
 
 // FP16 pairs 1024 + byte of the two 16-bit words of r: high bytes, low bytes
@@ -124,7 +136,7 @@ __device__ __forceinline__ void stage_bfp(uint8_t* sa, const uint8_t* base, int 
 // words); lane (g, t) accumulates rows 16i + g, 16i + g + 8 for right-hand
 // sides 2t, 2t+1.  Launch: bq_smem_n(I24) bytes of dynamic shared memory.
 template <bool I24>
-__global__ void __launch_bounds__(TC_WARPS * 32)
+__global__ void __launch_bounds__(TC_WARPS * 32, HLRC_BQ_MINB)
 k_nform_bfp(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
             const double* __restrict__ vx, const double* __restrict__ vt, OutMap om, double alpha, int add) {
     using O = TcOp<FMT_F16>;
@@ -135,8 +147,8 @@ k_nform_bfp(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
     const MSeg sg = segs[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * STAGE + (I24 ? BQ_PLANE : 0));
-    uint8_t* lo_plane = ring + TC_STAGES * STAGE;                          // 24-bit: this warp's widened bytes
+    uint8_t* ring = smem + warp * (BQ_STAGES * STAGE + (I24 ? BQ_PLANE : 0));
+    uint8_t* lo_plane = ring + BQ_STAGES * STAGE;                          // 24-bit: this warp's widened bytes
     const int ncols = int(sg.ncols);
     const uint8_t* base = A + size_t(sg.a16) * 16;
     const MCol* ctab = cols + sg.col0;
@@ -147,7 +159,7 @@ k_nform_bfp(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
     MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<BQ_STAGES>(
         (ncols + 31) / 32, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * STAGE;
@@ -278,8 +290,8 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     constexpr int STAGE = I24 ? BQ_STAGE_T24 : BQ_STAGE_T16;
-    uint8_t* ring = smem + warp * (TC_STAGES * STAGE + (I24 ? BQ_PLANE : 0));
-    uint8_t* lo_plane = ring + TC_STAGES * STAGE;             // 24-bit: this warp's widened bytes
+    uint8_t* ring = smem + warp * (BQ_STAGES * STAGE + (I24 ? BQ_PLANE : 0));
+    uint8_t* lo_plane = ring + BQ_STAGES * STAGE;             // 24-bit: this warp's widened bytes
     constexpr int TABOFF = I24 ? BQ_PLANE + 32 * BQ_LO_STRIDE : BQ_PLANE;   // column table of a stage
     // x entries of the lane: rows 16kt + 2t + {0, 1, 8, 9} (kt < 4), right-hand side g
     double xv[4][4];
@@ -317,7 +329,7 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
     // ldmatrix row of this lane: column + 8 for lanes 8-15 and 24-31, rows + 8 for lanes 16-31
     const int lcol = (lane & 7) + ((lane >> 3) & 1) * 8, lrow = ((lane >> 4) & 1) * 8;
     MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<BQ_STAGES>(
         (ncols + 31) / 32, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * STAGE;
@@ -386,7 +398,7 @@ __device__ __forceinline__ void ttform_bfp(const MSeg& sg, uint8_t* smem, const 
 // write disjoint outputs and run as two grids, each with its own stage
 // size).  Dynamic shared memory: bq_smem_t(I24).
 template <bool I24>
-__global__ void __launch_bounds__(TC_WARPS * 32)
+__global__ void __launch_bounds__(TC_WARPS * 32, HLRC_BQ_MINB)
 k_ttform_bfp(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const uint8_t* __restrict__ A,
              const double* __restrict__ vin, OutMap om, float* __restrict__ part, double alpha, int add) {
     extern __shared__ __align__(16) uint8_t smem[];
