@@ -38,15 +38,22 @@ def test_struct_layouts_match_header(tmp_path):
     structs = ["hlrc_block", "hlrc_h_desc", "hlrc_basis", "hlrc_uniform_block", "hlrc_uniform_desc",
                "hlrc_options", "hlrc_info", "hlrc_problem", "hlrc_tuning",
                "hlrc_h2_cluster", "hlrc_h2_desc"]
+    # the size of every struct and the offset of every field of the ctypes
+    # mirror, as the C compiler lays out the header
+    fields = [(s, f) for s in structs for f, *_ in getattr(_capi, s)._fields_]
     src = tmp_path / "sz.c"
-    src.write_text('#include <stdio.h>\n#include "hlrc.h"\nint main(void){\n' +
-                   "".join(f'printf("{s} %zu\\n", sizeof({s}));\n' for s in structs) + "return 0;}\n")
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "hlrc.h"\nint main(void){\n' +
+                   "".join(f'printf("{s} %zu\\n", sizeof({s}));\n' for s in structs) +
+                   "".join(f'printf("{s}.{f} %zu\\n", offsetof({s}, {f}));\n' for s, f in fields) +
+                   "return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     sizes = dict(zip(out[0::2], map(int, out[1::2])))
     for s in structs:
         assert C.sizeof(getattr(_capi, s)) == sizes[s], s
+    for s, f in fields:
+        assert getattr(getattr(_capi, s), f).offset == sizes[f"{s}.{f}"], (s, f)
 
 
 def _ll_desc(n=8):
