@@ -1569,14 +1569,11 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
             if (ws.profile) prof_end(M, s);
             if (tp.ngroups > 0) {
                 if (ws.profile) prof_begin(M, "ttfinish", tp.npart * 8, s);
-                const int b1 = fin_gpb(tp.ngroups1), b2 = fin_gpb(tp.ngroups);
                 if (tp.ngroups1 > 0)   // first level: runs of slots into the scratch part of the partials
-                    L(launch_k(ov, k_ttfinish_flat<1, double, false>, unsigned((tp.ngroups1 + b1 - 1) / b1), 256, 0,
-                               s, tp.groups1, tp.ngroups1, b1, static_cast<const double*>(ws.part),
-                               OutMap{ws.part, 1, 0, 1}, static_cast<double*>(nullptr), 1.0, 0));
-                L(launch_k(ov, k_ttfinish_flat<1, double, false>, unsigned((tp.ngroups + b2 - 1) / b2), 256, 0, s,
-                           tp.groups, tp.ngroups, b2, static_cast<const double*>(ws.part), OutMap{vout, 1, 0, 1},
-                           static_cast<double*>(nullptr), alpha, add));
+                    L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups1 + 7) / 8), 256, 0, s, tp.groups1, tp.ngroups1,
+                               static_cast<const double*>(ws.part), ws.part, 1.0, 0));
+                L(launch_k(ov, k_ttfinish_f64, unsigned((tp.ngroups + 7) / 8), 256, 0, s, tp.groups, tp.ngroups,
+                           static_cast<const double*>(ws.part), vout, alpha, add));
                 if (ws.profile) prof_end(M, s);
             }
             HLRC_AFTER_LAUNCH(stage_name(M, 2, st.idx));

@@ -419,6 +419,50 @@ k_ttform_f64(const TTSeg* __restrict__ segs, const TTChunk* __restrict__ chunks,
     }
 }
 
+// Sums the per-tile partials of multi-tile tile-T-form outputs in tile order
+// (one-vector products; a warp per output, lanes over its columns).
+__global__ void __launch_bounds__(256)
+k_ttfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,
+               double* __restrict__ out, double alpha, int add) {
+    pdl_trigger();
+    const int gid = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (gid >= ngroups) return;
+    const int lane = threadIdx.x & 31;
+    const TGroup g = groups[gid];
+    pdl_wait();
+    for (uint32_t j = lane; j < g.nc; j += 32) {
+        // four interleaved partial sums keep four loads in flight; they are
+        // combined in a fixed order, so the result is deterministic
+        const double* p = part + size_t(g.slot0) + j;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        uint32_t i = 0;
+        // sixteen loads in flight, then the same sums in the same order
+        for (; i + 16 <= g.nslots; i += 16) {
+            double v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = p[size_t(i + q) * g.nc];
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) {
+                s0 += v[q];
+                s1 += v[q + 1];
+                s2 += v[q + 2];
+                s3 += v[q + 3];
+            }
+        }
+        for (; i + 4 <= g.nslots; i += 4) {
+            s0 += p[size_t(i) * g.nc];
+            s1 += p[size_t(i + 1) * g.nc];
+            s2 += p[size_t(i + 2) * g.nc];
+            s3 += p[size_t(i + 3) * g.nc];
+        }
+        for (; i < g.nslots; ++i) s0 += p[size_t(i) * g.nc];
+        const double s = (s0 + s1) + (s2 + s3);
+        double* o = out + g.out + j;
+        if (add) *o += alpha * s;
+        else *o = s;
+    }
+}
+
 // Sums the partial slots of multi-unit T-form outputs in slot order.
 __global__ void __launch_bounds__(256)
 k_tfinish_f64(const TGroup* __restrict__ groups, int ngroups, const double* __restrict__ part,

@@ -38,22 +38,22 @@ struct OutMap {            // output element (i, r) lives at base[i * rs + r * c
     int nr;                // valid right-hand sides
 };
 
-// Finish of the tile T-form with a flat thread map: a CTA takes gpb (at most
-// FIN_GROUPS, fin_gpb) consecutive groups, and each thread one vector of VEC
-// entries (output
-// column j, right-hand sides k .. k+VEC-1) of them, NR right-hand sides per
-// partial entry (1 for one-vector products, MR_RB for the multi-vector
-// kernels).  Slot i of a group holds its entries at
-// part[(slot0 + i*nc + j)*NR + k].  Each entry is summed in a fixed order:
-// four FP64 accumulators, slot a going to accumulator a mod 4 when
-// a < (nslots rounded down to a multiple of 4) and to the first otherwise,
-// each accumulator taking its slots in increasing order; the result is
-// (s0 + s1) + (s2 + s3).  The loads of FIN_BATCH slots are issued before
-// their sums, so a short group (a few slots of a few columns, the common
-// case) costs one round trip, and the short groups of a CTA fill its
+// Finish of the multi-vector tile T-form with a flat thread map: a CTA takes
+// gpb (at most FIN_GROUPS, fin_gpb) consecutive groups, and each thread one
+// vector of VEC entries of them (output column j, right-hand sides k ..
+// k+VEC-1), NR right-hand sides per partial entry.  Slot i of a group holds
+// its entries at part[(slot0 + i*nc + j)*NR + k].  Each entry is summed in a
+// fixed order: four FP64 accumulators, slot a going to accumulator a mod 4
+// when a < (nslots rounded down to a multiple of 4) and to the first
+// otherwise, each accumulator taking its slots in increasing order; the
+// result is (s0 + s1) + (s2 + s3).  The loads of FIN_BATCH slots are issued
+// before their sums, so a short group (a few slots of a few columns, the
+// common case) costs one round trip, and the short groups of a CTA fill its
 // threads together.  TO_PART writes the sums (as T) to
 // part_out[(out + j)*NR + k] (the first level of long outputs); otherwise
-// they go to the output map, with alpha/add.
+// they go to the output map, with alpha/add.  (The one-vector finish,
+// k_ttfinish_f64, keeps a warp per output: for one vector that measured
+// faster.)
 constexpr int FIN_GROUPS = 32;
 constexpr int FIN_BATCH = 8;
 
