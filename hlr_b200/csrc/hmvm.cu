@@ -705,9 +705,9 @@ hlrc_status enable_tc_smem(int dev) {
     std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), dev) != done.end()) return HLRC_OK;
     HLRC_CUDA(cudaFuncSetAttribute(k_ttform_mr<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_TT)));
+                                   tc_smem_bytes(TC_STAGE_TT, TC_STAGES_TT)));
     HLRC_CUDA(cudaFuncSetAttribute(k_ttform_mr<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   tc_smem_bytes(TC_STAGE_TT)));
+                                   tc_smem_bytes(TC_STAGE_TT, TC_STAGES_TT)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tc_smem_bytes(TC_STAGE_N16, TC_STAGES_N16)));
     HLRC_CUDA(cudaFuncSetAttribute(k_nform_tc<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1702,11 +1702,13 @@ hlrc_status run_multi(hlrc_hmat M, const Workspace& ws, double alpha_in, int op,
                     const int n32 = tp.nmseg[FMT_F32];
                     float* fpart = reinterpret_cast<float*>(ws.mr_part);
                     if (tp.nmseg[FMT_BF16] > 0) {
-                        k_ttform_mr<FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
+                        k_ttform_mr<FMT_BF16><<<n32 + tp.nmseg[FMT_BF16], TC_WARPS * 32,
+                                               tc_smem_bytes(TC_STAGE_TT, TC_STAGES_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_BF16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
                         ++nl;
                     } else if (n32 + tp.nmseg[FMT_F16] > 0) {
-                        k_ttform_mr<FMT_F16><<<n32 + tp.nmseg[FMT_F16], TC_WARPS * 32, tc_smem_bytes(TC_STAGE_TT), s>>>(
+                        k_ttform_mr<FMT_F16><<<n32 + tp.nmseg[FMT_F16], TC_WARPS * 32,
+                                               tc_smem_bytes(TC_STAGE_TT, TC_STAGES_TT), s>>>(
                             tp.mseg[FMT_F32], n32, tp.mseg[FMT_F16], tp.mcol, M->store, vec(tp.in), om, fpart, alpha, add);
                         ++nl;
                     }

@@ -58,6 +58,17 @@ constexpr int TC_STAGES_N16 = HLRC_N16_STAGES;   // ring depth of the 16-bit N-f
 #ifndef HLRC_N16_MINB
 #define HLRC_N16_MINB 1
 #endif
+// The 8-vector tile T-form: one ring stage per warp and at least 6 CTAs per
+// SM.  On a 4-member batched problem (mixed store) it took 0.193 ms against
+// 0.206 ms with two stages; on one n = 32768 matrix the product time was the
+// same (197 us) either way.  The ring depth changes no sum.
+#ifndef HLRC_TT_STAGES
+#define HLRC_TT_STAGES 1
+#endif
+constexpr int TC_STAGES_TT = HLRC_TT_STAGES;     // ring depth of the 8-vector tile T-form
+#ifndef HLRC_TT_MINB
+#define HLRC_TT_MINB 6
+#endif
 
 // dynamic shared memory of a launch: one ring of `nst` stages per warp
 constexpr int tc_smem_bytes(int stage, int nst = TC_STAGES) { return TC_WARPS * nst * stage; }
@@ -261,7 +272,7 @@ __device__ __forceinline__ void ttform_tc(const MSeg& sg, uint8_t* smem, const M
     using O = TcOp<FMT>;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T16);
+    uint8_t* ring = smem + warp * (TC_STAGES_TT * TC_STAGE_T16);
     // x entries of the lane: rows 16kt + 2t + {0, 1, 8, 9} (kt < 4), right-hand side g
     double xv[4][4];
     int E = 0;
@@ -293,7 +304,7 @@ __device__ __forceinline__ void ttform_tc(const MSeg& sg, uint8_t* smem, const M
     // ldmatrix row of this lane: column + 8 for lanes 8-15 and 24-31, rows + 8 for lanes 16-31
     const int lcol = (lane & 7) + ((lane >> 3) & 1) * 8, lrow = ((lane >> 4) & 1) * 8;
     MCol mc = warp * 32 + lane < ncols ? ld_mcol(ctab + warp * 32 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<TC_STAGES_TT>(
         (ncols + 31) / 32, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_T16;
@@ -453,7 +464,7 @@ __device__ __forceinline__ void ttform_d32(const MSeg& sg, uint8_t* smem, const 
                                            const OutMap& om, float* __restrict__ part, double alpha, int add) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    uint8_t* ring = smem + warp * (TC_STAGES * TC_STAGE_T32);
+    uint8_t* ring = smem + warp * (TC_STAGES_TT * TC_STAGE_T32);
     // x of the lane: rows 8j + 2t + b (j < 8, b < 2), right-hand side g
     double xv[16];
 #pragma unroll
@@ -468,7 +479,7 @@ __device__ __forceinline__ void ttform_d32(const MSeg& sg, uint8_t* smem, const 
     const MCol* ctab = cols + sg.col0;
     const int nj = (sg.rows + 7) / 8;
     MCol mc = (lane < 16 && warp * 16 + lane < ncols) ? ld_mcol(ctab + warp * 16 + lane) : MCol{0u, 0.f};
-    warp_stream(
+    warp_stream<TC_STAGES_TT>(
         (ncols + 15) / 16, warp,
         [&](int slot, int st) {
             uint8_t* sa = ring + slot * TC_STAGE_T32;
@@ -573,10 +584,10 @@ k_nform_d32(const MSeg* __restrict__ segs, const MCol* __restrict__ cols, const 
 // One tile T-form pass of a reduced-precision store in one grid: the first
 // n32 CTAs take the FP32 runs (FP64 tensor cores), the others the runs of the
 // 16-bit format F16.  The outputs of the two formats are disjoint.  Dynamic
-// shared memory: tc_smem_bytes(TC_STAGE_TT).
+// shared memory: tc_smem_bytes(TC_STAGE_TT, TC_STAGES_TT).
 constexpr int TC_STAGE_TT = TC_STAGE_T16 > TC_STAGE_T32 ? TC_STAGE_T16 : TC_STAGE_T32;
 template <int F16>
-__global__ void __launch_bounds__(TC_WARPS * 32)
+__global__ void __launch_bounds__(TC_WARPS * 32, HLRC_TT_MINB)
 k_ttform_mr(const MSeg* __restrict__ segs32, int n32, const MSeg* __restrict__ segs16, const MCol* __restrict__ cols,
             const uint8_t* __restrict__ A, const double* __restrict__ vin, OutMap om, float* __restrict__ part,
             double alpha, int add) {
