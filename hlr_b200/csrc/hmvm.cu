@@ -191,6 +191,7 @@ struct hlrc_hmat_s {
     std::vector<Stage> stages[3];
     std::vector<Stage> stages_mr[3];   // multi-vector products, when they differ (H^2: no tree sweeps)
     std::vector<Stage> stages_nf[3];   // one-vector products with side stages, when present
+    bool nf_multi = false;             // multi-vector products take stages_nf too
     Workspace side_ws;                 // the handle's side stream and events (side stages only)
     hlrc_info info{};
     // multi-RHS workspace (FP64 plans, allocated at upload when max_nrhs > 1):
@@ -1161,6 +1162,7 @@ hlrc_status upload_plan(Plan& p, const hlrc_options& o, hlrc_hmat* out) {
         hp->stages_mr[op] = p.stages_mr[op];
         hp->stages_nf[op] = p.stages_nf[op];
     }
+    hp->nf_multi = p.nf_multi;
     if (has_side(hp->stages_nf)) {
         if (const hlrc_status ss = side_create(hp->side_ws); ss != HLRC_OK) {
             cleanup();
@@ -1628,9 +1630,14 @@ hlrc_status run_single(hlrc_hmat M, const Workspace& ws, double alpha_in, int op
 
 // The stages of a multi-vector product: the level passes where the
 // one-vector product sweeps trees.
+// The 8-vector DMMA and tensor-core passes are compute-heavy, so the near
+// field beside them hides nothing: multi-vector products keep the fused pass
+// unless the plan asked for the side stream explicitly (near_field = 2).  On
+// a uniform-H matrix (sphere, 32768 triangles, 32 vectors) the fused pass
+// took 337 us against 354 us.
 const std::vector<Stage>& mr_stages(hlrc_hmat M, int op) {
     if (!M->stages_mr[op].empty()) return M->stages_mr[op];
-    return M->stages_nf[op].empty() ? M->stages[op] : M->stages_nf[op];
+    return M->stages_nf[op].empty() || !M->nf_multi ? M->stages[op] : M->stages_nf[op];
 }
 
 // Can the product for `op` run in blocks of MR_RB right-hand sides?  Needs

@@ -1221,6 +1221,7 @@ hlrc_status plan_h(const hlrc_h_desc& d, const hlrc_options& o, Plan& p, double 
             nbld.finish();
         }
         p.stages_nf[HLRC_OP_N] = {{1, 2, 1}, {2, 0}, {1, 3}};
+        p.nf_multi = g_knobs.near_field == 2;
     }
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}};
     p.stages[HLRC_OP_T] = {{2, 1}, {1, 1}, {2, 2}};
@@ -1511,6 +1512,7 @@ hlrc_status plan_uniform(const hlrc_uniform_desc& d, const hlrc_options& o, Plan
             nbld.finish();
         }
         p.stages_nf[HLRC_OP_N] = {{1, 3, 1}, {2, 0}, {1, 0}, {1, 4}};
+        p.nf_multi = g_knobs.near_field == 2;
     }
     p.stages[HLRC_OP_N] = {{2, 0}, {1, 0}, {1, 1}};
     p.stages[HLRC_OP_T].clear();  // uniform_lrmatrix::uni_apply_add asserts on apply_transposed
@@ -2110,6 +2112,7 @@ hlrc_status plan_h2(const hlrc_h2_desc& d, const hlrc_options& o, Plan& p) {
         const Stage lu{1, int(p.npasses.size()) - 1};
         std::vector<Stage>& nf = p.stages_nf[HLRC_OP_N];
         nf = {Stage{1, dxi, 1}};
+        p.nf_multi = g_knobs.near_field == 2;
         for (const Stage& sg : p.stages[HLRC_OP_N])
             nf.push_back(sg.kind == n_out.kind && sg.idx == n_out.idx ? lu : sg);
     }

@@ -151,6 +151,7 @@ struct Plan {
     // one-vector products with the near field on a side stream
     // (hlrc_options.near_field): replaces stages[op] there when not empty
     std::vector<Stage> stages_nf[3];
+    bool nf_multi = false;         // multi-vector products take stages_nf too (near_field = 2 asked for)
     // accounting (per product, one rhs)
     int64_t n_dense = 0, n_lowrank = 0, n_row_tiles = 0, n_col_tiles = 0;
     int64_t matrix_bytes = 0, algorithmic_bytes = 0, flops = 0;

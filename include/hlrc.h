@@ -198,12 +198,14 @@ typedef struct hlrc_options {
      * device (an on_device build); FP64 stores are filled on the device,
      * other precisions copy the leaves to the host first                   */
     int32_t leaves_on_device;
-    /* near_field (one-vector products of op N): 1 = the dense leaves' D x is
-     * summed in the last pass with the low-rank part (as HLR's mul_vec sums
-     * every block of a row, tbb/detail/arith.hh:95-124); 2 = D x is its own
-     * pass, launched on a side stream at the start of the product and joined
+    /* near_field (products of op N): 1 = the dense leaves' D x is summed in
+     * the last pass with the low-rank part (as HLR's mul_vec sums every
+     * block of a row, tbb/detail/arith.hh:95-124); 2 = D x is its own pass,
+     * launched on a side stream at the start of the product and joined
      * before the pass that adds the low-rank part to y, so that it overlaps
-     * the dependent low-rank passes; 0 = default (2).  With 2, D x is added
+     * the dependent low-rank passes, in one- and 8-vector products; 0 =
+     * default: 2 for one-vector products, 1 for multi-vector ones (their
+     * passes are compute-heavy: nothing to overlap).  With 2, D x is added
      * first, then the low-rank part, per row tile; the 64-vector product of
      * 16-bit stores always takes the fused pass.                          */
     int32_t near_field;
