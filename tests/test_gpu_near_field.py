@@ -166,10 +166,11 @@ def test_graph_replay_profiles_the_side_pass(kind):
 
 @pytest.mark.parametrize("prec", ["f64", "mixed", "bfp"])
 def test_side_stream_in_eight_vector_products(prec):
-    """The 8-vector kernels take the same split: D X on the side stream after
-    x is staged, U T after the join.  Against the fused plan the result
-    differs by summation order only; against the oracle, by the store's
-    precision."""
+    """With near_field = 2 asked for explicitly, the 8-vector kernels take
+    the same split (by default they keep the fused pass): D X on the side
+    stream after x is staged, U T after the join.  Against the fused plan the
+    result differs by summation order only; against the oracle, by the
+    store's precision."""
     hm = CASES["h"]()
     M1 = hlr.upload(hm, precision=prec, max_nrhs=8, plan={"near_field": 1})
     M2 = hlr.upload(hm, precision=prec, max_nrhs=8, plan={"near_field": 2})
