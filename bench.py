@@ -3,12 +3,14 @@
 Default workload (one step = one product on one GPU): FP64 H-matrix of the 3D
 exponential covariance exp(-r/0.1) + 1e-4 nugget on n = 131072 points
 uniform in [0,1]^3 (seed 1), BSP cluster tree leaf 64, eta = 2, ACA + SVD
-eps = 1e-6, one right-hand side x ~ N(0,1).  Synthetic inputs, built on the
-host by the library's own construction.
+eps = 1e-6, one right-hand side x ~ N(0,1).  Synthetic inputs, built by the
+library's own construction (the leaves on the GPU; --host-build on the host).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config c2|c1|c3|c2s|c4|c5] [--precision P] [--nrhs K]
                     [--no-cpu-baseline] [--no-autotune] [--no-graph] [--h2] [--shard]
+                    [--tune-plan] [--plan k=v,...] [--members N] [--host-build]
+                    [--reduced bfp,mixed|none]
 
 Prints one JSON line on rank 0.  Under torchrun (N > 1) every rank runs an
 independent replica of the product on its own GPU (weak scaling), time = max
